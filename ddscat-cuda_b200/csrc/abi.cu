@@ -1,0 +1,422 @@
+// C ABI of the B200 DDA library: the 15 entry points of
+// ddscat_cuda_unified/cuda/ddscat_matvec_cuda.h:11-51 with the reference's
+// argument checks, return codes, last_error() text convention and state
+// lifetime (device state owned from prepare until release or the next
+// prepare; the solution stays resident for EVALQ/SCAT).
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+#include "ddscat_matvec_cuda.h"
+#include "solvers.h"
+
+namespace ddb {
+
+static std::string g_last_error;
+void set_error(const char* where, const char* what) {
+  char b[1024];
+  std::snprintf(b, sizeof(b), "%s: %s", where, what);
+  g_last_error = b;
+}
+void set_cuda_error(const char* where, cudaError_t e) { set_error(where, cudaGetErrorString(e)); }
+const char* last_error_text() { return g_last_error.c_str(); }
+void clear_error() { g_last_error.clear(); }
+int check_launch(const char* where) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) { set_cuda_error(where, e); return 1; }
+  return 0;
+}
+
+using C = float2;
+
+struct State {
+  bool ready = false;
+  bool solution_valid = false;
+  Engine<float> eng;
+  VecOps<float> ops;
+  cudaStream_t stream = 0;
+  C *d_xf = nullptr, *d_yf = nullptr, *d_adia = nullptr, *d_aoff = nullptr;  // full 3*NAT
+  C *d_b = nullptr, *d_sx = nullptr, *d_sy = nullptr, *d_work = nullptr;     // compact
+  bool aoff_zero = false;
+  int verbose = 0;
+};
+static State s;
+
+static void release_state() {
+  if (s.ready || s.eng.green) {
+    cudaFree(s.d_xf); cudaFree(s.d_yf); cudaFree(s.d_adia); cudaFree(s.d_aoff);
+    cudaFree(s.d_b); cudaFree(s.d_sx); cudaFree(s.d_sy); cudaFree(s.d_work);
+    s.ops.release();
+    s.eng.release();
+  }
+  const int verbose = s.verbose;
+  s = State{};
+  s.verbose = verbose;
+}
+
+static int env_verbose() {
+  const char* v = std::getenv("DDSCAT_B200_VERBOSE");
+  return (v && *v && *v != '0') ? 1 : 0;
+}
+
+static int slices_build() {
+#ifdef DDSCAT_B200_SLICES
+  return 1;
+#else
+  return 0;
+#endif
+}
+
+static int allocate_runtime() {
+  const size_t n = (size_t)3 * s.eng.g.nat, cn = (size_t)3 * s.eng.g.nat0;
+  if (cn > (size_t)0x7fffffff) { set_error("allocate runtime", "3*NAT0 exceeds solver int range"); return 204; }
+  cudaError_t e = cudaSuccess;
+  auto M = [&](C** p, size_t cnt) { if (e == cudaSuccess) e = cudaMalloc((void**)p, cnt * sizeof(C)); };
+  M(&s.d_xf, n); M(&s.d_yf, n); M(&s.d_adia, n); M(&s.d_aoff, n);
+  M(&s.d_b, cn); M(&s.d_sx, cn); M(&s.d_sy, cn); M(&s.d_work, 13 * cn);
+  if (e != cudaSuccess) { set_cuda_error("allocate runtime", e); return 204; }
+  if (s.ops.init(s.stream)) return 204;
+  s.eng.stream = s.stream;
+  s.eng.slices_layout = slices_build();
+  if (s.eng.ensure_workspace(1)) return 204;
+  return 0;
+}
+
+static bool all_zero(const void* p, size_t bytes) {
+  const unsigned char* c = (const unsigned char*)p;
+  for (size_t i = 0; i < bytes; ++i)
+    if (c[i]) return false;
+  return true;
+}
+
+static int upload_operators(const void* adia, const void* aoff) {
+  const size_t b = (size_t)3 * s.eng.g.nat * sizeof(C);
+  cudaError_t e = cudaMemcpy(s.d_adia, adia, b, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(s.d_aoff, aoff, b, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) { set_cuda_error("operator H2D", e); return 1; }
+  s.aoff_zero = all_zero(aoff, b);  // zero CXAOFF contributes nothing: skip its reads
+  return 0;
+}
+
+static int upload_full_to_compact(const void* host, C* compact) {
+  const size_t b = (size_t)3 * s.eng.g.nat * sizeof(C);
+  cudaError_t e = cudaMemcpy(s.d_xf, host, b, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) { set_cuda_error("full vector H2D", e); return 1; }
+  v_gather<float>(s.d_xf, compact, s.eng.occ, s.eng.g.nat, s.eng.g.nat0, s.stream);
+  return check_launch("full->compact gather");
+}
+
+static int download_compact_to_full(const C* compact, void* host) {
+  const size_t b = (size_t)3 * s.eng.g.nat * sizeof(C);
+  cudaError_t e = cudaMemsetAsync(s.d_xf, 0, b, s.stream);
+  if (e != cudaSuccess) { set_cuda_error("solution compact D2H", e); return 1; }
+  v_scatter<float>(compact, s.d_xf, s.eng.occ, s.eng.g.nat, s.eng.g.nat0, s.stream);
+  if (check_launch("compact->full scatter")) return 1;
+  e = cudaMemcpy(host, s.d_xf, b, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) { set_cuda_error("solution compact D2H", e); return 1; }
+  return 0;
+}
+
+typedef int (*SolveFn)(SolveIO<float>&);
+
+struct SolverCodes {
+  const char* name;
+  int invalid, workspace, h2d, d2h;
+  bool publish_on_maxit;  // PBCGST writes x back before returning 87
+};
+
+static int run_solver(const SolverCodes& sc, SolveFn fn, const void* b, void* x, const void* adia, const void* aoff,
+                      int ndim, int maxit, float tol, int* itout, float* tole, int* ncout) {
+  clear_error();
+  if (!s.ready || !b || !x || !adia || !aoff || !itout || !tole || !ncout || ndim != 3 * s.eng.g.nat || maxit <= 0 ||
+      tol <= 0.f) {
+    set_error(sc.name, "invalid argument");
+    return sc.invalid;
+  }
+  if (!s.d_work) { set_error(sc.name, "Krylov workspace missing"); return sc.workspace; }
+  s.solution_valid = false;
+  if (upload_full_to_compact(b, s.d_b)) return sc.h2d;
+  if (upload_full_to_compact(x, s.d_sx)) return sc.h2d;
+  if (upload_operators(adia, aoff)) return sc.h2d;
+  SolveIO<float> io;
+  io.eng = &s.eng; io.ops = &s.ops; io.stream = s.stream;
+  io.n = 3 * s.eng.g.nat0;
+  io.b = s.d_b; io.x = s.d_sx;
+  io.adia = s.d_adia; io.aoff = s.aoff_zero ? nullptr : s.d_aoff; io.a_full = 1;
+  io.work = s.d_work; io.sy = s.d_sy;
+  io.maxit = maxit; io.tol = (double)tol; io.verbose = s.verbose;
+  const int rc = fn(io);
+  if (rc != 0 && !(rc == 87 && sc.publish_on_maxit)) return rc;
+  std::string keep = g_last_error;
+  if (download_compact_to_full(s.d_sx, x)) return sc.d2h;
+  s.solution_valid = true;
+  *itout = io.itno;
+  *tole = (float)io.tole;
+  *ncout = io.ncompte;
+  if (rc) g_last_error = keep;
+  return rc;
+}
+
+// ---- far-field quadrature (cu:849-875) ----
+struct IntDir {
+  float k[3];
+  double w[5];
+};
+static long lround_half_away(double v) { return v >= 0 ? (long)std::floor(v + 0.5) : -(long)std::floor(-v + 0.5); }
+static int make_integration_dirs(const float ak[3], const C e01[3], float etasca, int nat0, std::vector<IntDir>& dirs) {
+  const double pi = 4.0 * std::atan(1.0);
+  const double ak2 = (double)ak[0] * ak[0] + (double)ak[1] * ak[1] + (double)ak[2] * ak[2], akk = std::sqrt(ak2);
+  double a1[3] = {(double)e01[0].x, (double)e01[1].x, (double)e01[2].x};
+  const double einc = std::sqrt(a1[0] * a1[0] + a1[1] * a1[1] + a1[2] * a1[2]);
+  if (!(einc > 0.0)) { set_error("GPU SCAT", "CXE01_TF is pure imaginary"); return 1; }
+  for (double& v : a1) v *= akk / einc;
+  const double a2[3] = {(ak[1] * a1[2] - ak[2] * a1[1]) / akk, (ak[2] * a1[0] - ak[0] * a1[2]) / akk,
+                        (ak[0] * a1[1] - ak[1] * a1[0]) / akk};
+  const double x = akk * std::cbrt(3.0 * (double)nat0 / (4.0 * pi)), theta0 = 2.0 * pi / (1.0 + x), afac = 1.0;
+  const int ntheta = 1 + (int)lround_half_away((2.0 * (3.0 + x) / (double)etasca) * (1.0 + afac / (pi + theta0)) /
+                                               (1.0 + afac * theta0 / ((pi + theta0) * (pi + theta0))));
+  double theta = 0.0, thetau = 0.0;
+  dirs.clear();
+  for (int ic = 1; ic <= ntheta; ++ic) {
+    const double thetal = theta;
+    theta = thetau;
+    if (ic < ntheta) {
+      const double si = (double)ic * (pi + afac * pi / (theta0 + pi)) / (double)(ntheta - 1), term = si - afac - theta0;
+      thetau = 0.5 * (term + std::sqrt(term * term + 4.0 * theta0 * si));
+    } else {
+      thetau = pi;
+    }
+    const double domega = 2.0 * pi * (std::cos(0.5 * (thetal + theta)) - std::cos(0.5 * (theta + thetau)));
+    const double ct = std::cos(theta), st = std::sin(theta), ct2 = ct * ct;
+    int nphi = (ic == 1 || ic == ntheta) ? 1 : (int)lround_half_away(4.0 * pi * st / (thetau - thetal));
+    if (nphi < 3 && ic != 1 && ic != ntheta) nphi = 3;
+    const double w = domega / (double)nphi, dphi = 2.0 * pi / (double)nphi;
+    for (int ip = 1; ip <= nphi; ++ip) {
+      const double phi = dphi * ((double)ip - 0.5 * (double)(ic % 2)), sp = std::sin(phi), cp = std::cos(phi);
+      IntDir d{};
+      for (int k = 0; k < 3; ++k) d.k[k] = (float)(ct * (double)ak[k] + st * (cp * a1[k] + sp * a2[k]));
+      d.w[0] = w; d.w[1] = w * ct; d.w[2] = w * st * cp; d.w[3] = w * st * sp; d.w[4] = w * ct2;
+      dirs.push_back(d);
+    }
+  }
+  return 0;
+}
+
+}  // namespace ddb
+
+using namespace ddb;
+
+extern "C" {
+
+DDSCAT_CUDA_API int ddscat_cuda_release(void) {
+  release_state();
+  clear_error();
+  return 0;
+}
+
+DDSCAT_CUDA_API const char* ddscat_cuda_last_error(void) { return last_error_text(); }
+
+DDSCAT_CUDA_API int ddscat_cuda_prepare_green_f32(int nx, int ny, int nz, int ipbc, int nat, int nat0, int idipint,
+                                                  float gamma, float pyd, float pzd, float akx, float aky, float akz,
+                                                  float dx1, float dx2, float dx3, const int16_t* iocc) {
+  clear_error();
+  if (nx <= 0 || ny <= 0 || nz <= 0 || nat <= 0 || nat0 <= 0 || nat0 > nat || (ipbc != 0 && ipbc != 1) ||
+      (idipint != 0 && idipint != 1) || !iocc || (long long)nx * ny * nz != (long long)nat) {
+    set_error("prepare_green", "invalid argument");
+    return 201;
+  }
+  if (ipbc && gamma <= 0.f) { set_error("prepare_green", "GAMMA must be >0 for PBC"); return 202; }
+  if (!s.verbose) s.verbose = env_verbose();
+  release_state();
+  int rc = s.eng.init_geometry(nx, ny, nz, ipbc, nat, nat0, iocc);
+  if (rc) { release_state(); return rc == 2 ? 208 : 204; }
+  GreenArgs<float> ga;
+  ga.idipint = idipint; ga.gamma = gamma; ga.pyd = pyd; ga.pzd = pzd;
+  ga.ak[0] = akx; ga.ak[1] = aky; ga.ak[2] = akz;
+  ga.dx[0] = dx1; ga.dx[1] = dx2; ga.dx[2] = dx3;
+  rc = s.eng.build_green(ga);
+  if (rc) { release_state(); return 220 + rc; }
+  rc = allocate_runtime();
+  if (rc) { release_state(); return rc; }
+  s.ready = true;
+  return 0;
+}
+
+DDSCAT_CUDA_API int ddscat_cuda_prepare_f32(int nx, int ny, int nz, int ipbc, int nat, int nat0, const void* green,
+                                            const int16_t* iocc) {
+  clear_error();
+  if (nx <= 0 || ny <= 0 || nz <= 0 || nat <= 0 || nat0 <= 0 || nat0 > nat || (ipbc != 0 && ipbc != 1) || !green ||
+      !iocc || (long long)nx * ny * nz != (long long)nat) {
+    set_error("prepare", "invalid argument");
+    return 1;
+  }
+  if (!s.verbose) s.verbose = env_verbose();
+  release_state();
+  int rc = s.eng.init_geometry(nx, ny, nz, ipbc, nat, nat0, iocc);
+  if (rc) { release_state(); return rc == 2 ? 6 : 2; }
+  if (allocate_runtime()) { release_state(); return 2; }
+  if (s.eng.upload_green(green)) { release_state(); return 4; }
+  s.ready = true;
+  return 0;
+}
+
+DDSCAT_CUDA_API int ddscat_cuda_apply_f32(int cwhat, const void* x, void* y, const void* adia, const void* aoff) {
+  if (!s.ready) { set_error("apply", "not prepared"); return 10; }
+  if ((cwhat != 'N' && cwhat != 'C') || !x || !y || !adia || !aoff) { set_error("apply", "invalid argument"); return 11; }
+  const size_t b = (size_t)3 * s.eng.g.nat * sizeof(C);
+  cudaError_t e = cudaMemcpy(s.d_xf, x, b, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) { set_cuda_error("x H2D", e); return 12; }
+  e = cudaMemcpy(s.d_adia, adia, b, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) { set_cuda_error("adia H2D", e); return 13; }
+  e = cudaMemcpy(s.d_aoff, aoff, b, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) { set_cuda_error("aoff H2D", e); return 14; }
+  s.aoff_zero = all_zero(aoff, b);
+  MvArgs<float> a;
+  a.x = s.d_xf; a.y = s.d_yf; a.io_full = 1;
+  a.adia = s.d_adia; a.aoff = s.aoff_zero ? nullptr : s.d_aoff; a.a_full = 1;
+  a.conj = (cwhat == 'C'); a.nrhs = 1;
+  int rc = s.eng.matvec(a);
+  if (rc) return rc;
+  e = cudaMemcpy(y, s.d_yf, b, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) { set_cuda_error("y D2H", e); return 15; }
+  return 0;
+}
+
+#define SOLVER_ENTRY(fname, fn, nm, inv, ws, h2d, d2h, pub)                                                          \
+  DDSCAT_CUDA_API int fname(const void* b, void* x, const void* adia, const void* aoff, int ndim, int maxit, float tol, \
+                            int* itno, float* tole, int* ncompte) {                                                   \
+    static const SolverCodes sc{nm, inv, ws, h2d, d2h, pub};                                                          \
+    return run_solver(sc, fn<float>, b, x, adia, aoff, ndim, maxit, tol, itno, tole, ncompte);                        \
+  }
+SOLVER_ENTRY(ddscat_cuda_solve_gpbicg_f32, solve_gpbicg, "GPBICG", 30, 29, 31, 40, false)
+SOLVER_ENTRY(ddscat_cuda_solve_qmrccg_f32, solve_qmrccg, "QMRCCG", 50, 29, 51, 61, false)
+SOLVER_ENTRY(ddscat_cuda_solve_pbcgst_f32, solve_pbcgst, "PBCGST", 70, 29, 71, 86, true)
+SOLVER_ENTRY(ddscat_cuda_solve_pbcgs2_f32, solve_pbcgs2, "PBCGS2", 90, 29, 91, 107, false)
+SOLVER_ENTRY(ddscat_cuda_solve_petrkp_f32, solve_petrkp, "PETRKP", 110, 29, 111, 124, false)
+SOLVER_ENTRY(ddscat_cuda_solve_bicgstab4_f32, solve_bicgstab4, "BiCGStab4", 130, 131, 131, 145, false)
+SOLVER_ENTRY(ddscat_cuda_solve_gpbicgstab2_f32, solve_gpbicgstab2, "GPBiCGStab2", 150, 151, 151, 173, false)
+SOLVER_ENTRY(ddscat_cuda_solve_gpbicgstab4_f32, solve_gpbicgstab4, "GPBiCGStab4", 180, 181, 181, 207, false)
+#undef SOLVER_ENTRY
+
+DDSCAT_CUDA_API int ddscat_cuda_evalq_f32(int use_resident, const void* e_compact, const void* p_compact,
+                                          const void* adia_compact, const void* aoff_compact, float akx, float aky,
+                                          float akz, float e02, double* cabs, double* cext, double* cpha) {
+  clear_error();
+  if (!s.ready || !cabs || !cext || !cpha || !(e02 > 0.f)) { set_error("GPU EVALQ", "invalid argument"); return 300; }
+  const size_t cn = (size_t)3 * s.eng.g.nat0, cb = cn * sizeof(C);
+  const C *ad = s.d_adia, *ao = s.aoff_zero ? nullptr : s.d_aoff;
+  int a_full = 1;
+  if (use_resident) {
+    if (!s.solution_valid) { set_error("GPU EVALQ", "no resident final polarization published by solver"); return 301; }
+  } else {
+    if (!e_compact || !p_compact || !adia_compact || !aoff_compact) {
+      set_error("GPU EVALQ", "missing compact host arrays");
+      return 302;
+    }
+    cudaError_t e = cudaMemcpy(s.d_b, e_compact, cb, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(s.d_sx, p_compact, cb, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) { set_cuda_error("GPU EVALQ E/P H2D", e); return 303; }
+    s.solution_valid = true;
+    C* tad = s.d_work;  // compact operator copies live in the Krylov workspace
+    C* tao = s.d_work + cn;
+    e = cudaMemcpy(tad, adia_compact, cb, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(tao, aoff_compact, cb, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) { set_cuda_error("GPU EVALQ ADIA/AOFF H2D", e); return 305; }
+    ad = tad;
+    ao = all_zero(aoff_compact, cb) ? nullptr : tao;
+    a_full = 0;
+  }
+  const double ak2 = (double)akx * akx + (double)aky * aky + (double)akz * akz, akk = std::sqrt(ak2), ak3 = akk * ak2;
+  double2 zabs, zep;
+  int rc = evalq_compute<float>(s.eng, s.ops, s.d_b, s.d_sx, ad, ao, a_full, s.d_sy, ak3, &zabs, &zep);
+  if (rc) return rc;
+  const double pi = 4.0 * std::atan(1.0);
+  *cabs = -4.0 * pi * akk * zabs.y / (double)e02;
+  *cext = 4.0 * pi * akk * zep.y / (double)e02;
+  *cpha = 2.0 * pi * akk * zep.x / (double)e02;
+  return 0;
+}
+
+DDSCAT_CUDA_API int ddscat_cuda_scat_f32(int jpbc, int ndir, const float* ak, const float* aks, const float* dx,
+                                         const float* em1, const float* em2, float e02, float etasca, const void* e01v,
+                                         const float* x0, double* cbksca, double* csca, double* cscag, double* cscag2,
+                                         int* navg, void* f1v, void* f2v) {
+  clear_error();
+  if (!s.ready || !s.solution_valid || !ak || !dx || !x0 || !cbksca || !csca || !cscag || !cscag2 || !navg ||
+      !(e02 > 0.f)) {
+    set_error("GPU SCAT", "invalid state/argument");
+    return 320;
+  }
+  if (ndir > 0 && (!aks || !em1 || !em2 || !f1v || !f2v)) {
+    set_error("GPU SCAT", "missing selected-direction arrays");
+    return 321;
+  }
+  const double ak2 = (double)ak[0] * ak[0] + (double)ak[1] * ak[1] + (double)ak[2] * ak[2], akk = std::sqrt(ak2),
+               ak3 = akk * ak2;
+  *cbksca = 0.0; *csca = 0.0; cscag[0] = cscag[1] = cscag[2] = 0.0; *cscag2 = 0.0; *navg = 0;
+  if (jpbc == 0) {
+    if (!e01v || !(etasca > 0.f)) {
+      set_error("GPU SCAT", "finite-target integration needs CXE01 and ETASCA>0");
+      return 323;
+    }
+    std::vector<IntDir> idirs;
+    if (make_integration_dirs(ak, (const C*)e01v, etasca, s.eng.g.nat0, idirs)) return 324;
+    const int nd = (int)idirs.size();
+    *navg = nd;
+    std::vector<float> hd((size_t)3 * nd);
+    for (int i = 0; i < nd; ++i)
+      for (int k = 0; k < 3; ++k) hd[3 * i + k] = idirs[i].k[k];
+    std::vector<double2> sums((size_t)3 * nd);
+    int rc = farfield_sums<float>(s.eng, s.d_sx, hd.data(), nd, dx, x0, sums.data(), s.stream);
+    if (rc) return rc;
+    double acc[5] = {0, 0, 0, 0, 0}, back = 0.0;
+    for (int i = 0; i < nd; ++i) {
+      const double nx = hd[3 * i] / akk, ny = hd[3 * i + 1] / akk, nz = hd[3 * i + 2] / akk;
+      const double2 sx = sums[3 * i], sy = sums[3 * i + 1], sz = sums[3 * i + 2];
+      const double ndr = nx * sx.x + ny * sy.x + nz * sz.x, ndi = nx * sx.y + ny * sy.y + nz * sz.y;
+      const double exr = sx.x - nx * ndr, exi = sx.y - nx * ndi, eyr = sy.x - ny * ndr, eyi = sy.y - ny * ndi;
+      const double ezr = sz.x - nz * ndr, ezi = sz.y - nz * ndi;
+      const double es2 = exr * exr + exi * exi + eyr * eyr + eyi * eyi + ezr * ezr + ezi * ezi;
+      for (int k = 0; k < 5; ++k) acc[k] += es2 * idirs[i].w[k];
+      if (i == nd - 1) back = es2;
+    }
+    const double fac = ak2 * ak2 / (double)e02;
+    *csca = fac * acc[0];
+    cscag[0] = fac * acc[1];
+    cscag[1] = fac * acc[2];
+    cscag[2] = fac * acc[3];
+    *cscag2 = fac * acc[4];
+    *cbksca = fac * back;
+  }
+  if (ndir > 0) {
+    std::vector<double2> sums((size_t)3 * ndir);
+    int rc = farfield_sums<float>(s.eng, s.d_sx, aks, ndir, dx, x0, sums.data(), s.stream);
+    if (rc) return rc == 325 ? 330 : rc;
+    const double term = ak3 / std::sqrt((double)e02);
+    C* h1 = (C*)f1v;
+    C* h2 = (C*)f2v;
+    for (int i = 0; i < ndir; ++i) {
+      const double2 sx = sums[3 * i], sy = sums[3 * i + 1], sz = sums[3 * i + 2];
+      const double a1r = em1[3 * i] * sx.x + em1[3 * i + 1] * sy.x + em1[3 * i + 2] * sz.x;
+      const double a1i = em1[3 * i] * sx.y + em1[3 * i + 1] * sy.y + em1[3 * i + 2] * sz.y;
+      const double a2r = em2[3 * i] * sx.x + em2[3 * i + 1] * sy.x + em2[3 * i + 2] * sz.x;
+      const double a2i = em2[3 * i] * sx.y + em2[3 * i + 1] * sy.y + em2[3 * i + 2] * sz.y;
+      h1[i] = make_float2((float)(term * a1r), (float)(term * a1i));
+      h2[i] = make_float2((float)(term * a2r), (float)(term * a2i));
+    }
+  }
+  return 0;
+}
+
+// ---- library extensions (declared in ddscat_b200.h) ----
+DDSCAT_CUDA_API int ddscat_b200_set_verbose(int level) {
+  s.verbose = level;
+  return 0;
+}
+
+DDSCAT_CUDA_API int ddscat_b200_layout(void) { return slices_build(); }
+
+}  // extern "C"

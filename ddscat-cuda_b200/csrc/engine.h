@@ -1,0 +1,122 @@
+// Internal interfaces of the B200 DDA library (not part of the C ABI).
+//
+// Data layout in HBM
+//   polarisation / field vectors: full  v[m*NAT + j]   (the ABI layout)
+//                                 compact v[m*NAT0 + q], q = rank of occupied site j
+//   zhat  : z-spectrum, [rhs][comp][kz < Mz][iy < ny][ix < nx]
+//   slab  : xy spectrum of a batch of kz planes, [rhs][comp][kz][iy < ny][kx < Mx]
+//   green : octant [6][nz+1][ny+1][nx+1] (IPBC=0) or full [6][Mz][My][Mx] (IPBC=1)
+// The MATVEC is a z-first pipeline: z-forward (pad-skip, compact scatter fused)
+// -> per kz batch { x-forward, y-forward * Green * y-inverse, x-inverse } ->
+// z-inverse with the diagonal / off-diagonal CXZC terms and compact gather fused.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+#include "common.cuh"
+#include "fft.cuh"
+
+namespace ddb {
+
+// ---------------------------------------------------------------- errors
+void set_error(const char* where, const char* what);
+void set_cuda_error(const char* where, cudaError_t e);
+const char* last_error_text();
+void clear_error();
+int check_launch(const char* where);
+
+// ---------------------------------------------------------------- geometry
+struct Geometry {
+  int nx = 0, ny = 0, nz = 0, Mx = 0, My = 0, Mz = 0;
+  int nat = 0, nat0 = 0, ipbc = 0;
+  size_t ngrid() const { return (size_t)Mx * My * Mz; }
+  size_t octant() const { return (size_t)(nx + 1) * (ny + 1) * (nz + 1); }
+  size_t green_count() const { return ipbc == 0 ? 6 * octant() : 6 * ngrid(); }
+};
+
+// Arguments of one MATVEC launch sequence over `nrhs` right-hand sides.
+template <typename T> struct MvArgs {
+  const cplx<T>* x = nullptr;  // input, RHS r at x + r*x_rs
+  size_t x_rs = 0;
+  cplx<T>* y = nullptr;        // output, RHS r at y + r*y_rs
+  size_t y_rs = 0;
+  int io_full = 0;             // 1: x,y are full 3*NAT vectors; 0: compact 3*NAT0
+  const cplx<T>* adia = nullptr;
+  const cplx<T>* aoff = nullptr;  // null => no off-diagonal site block
+  size_t a_rs = 0;                // per-RHS stride of adia/aoff (0 = shared)
+  int a_full = 1;                 // adia/aoff layout: 1 full, 0 compact
+  int conj = 0;                   // CWHAT='C'
+  const int* mask = nullptr;      // device per-RHS flags (nonzero = compute)
+  int nrhs = 1;
+};
+
+template <typename T> struct GreenArgs {
+  int idipint = 0;
+  double gamma = 0, pyd = 0, pzd = 0;
+  double ak[3] = {0, 0, 0};
+  double dx[3] = {1, 1, 1};
+};
+
+// The MATVEC engine for one prepared target (one Green tensor).
+template <typename T> struct Engine {
+  using C = cplx<T>;
+  Geometry g;
+  FftPlan px, py, pz;
+  C *twx = nullptr, *twy = nullptr, *twz = nullptr;
+  C* green = nullptr;
+  int* occ = nullptr;      // [nat0]
+  int* inv = nullptr;      // [nat], -1 for vacuum
+  int16_t* iocc = nullptr; // [nat]
+  // MATVEC workspace
+  C* zhat = nullptr;
+  int zcap = 0;            // RHS capacity of zhat
+  C* slab = nullptr;
+  int slab_nr = 0, slab_B = 0;  // slab = slab_nr RHS x slab_B planes
+  size_t slab_budget_elems = 0;
+  int slices_layout = 0;
+  cudaStream_t stream = 0;
+  size_t bytes_allocated = 0;
+
+  int init_geometry(int nx, int ny, int nz, int ipbc, int nat, int nat0, const int16_t* iocc_host);
+  int build_green(const GreenArgs<T>& ga);          // on-GPU direct sum + FFT to the octant
+  int upload_green(const void* host_green);         // CPU-supplied CXZC (ddscat_cuda_prepare_f32)
+  int ensure_workspace(int nrhs);
+  int matvec(const MvArgs<T>& a);
+  void release();
+};
+
+// ---------------------------------------------------------------- vector kernels
+template <typename T> struct VecOps {
+  using C = cplx<T>;
+  cudaStream_t stream = 0;
+  double2* d_red = nullptr;    // reduction partials
+  double2* d_out = nullptr;    // device results
+  unsigned* d_count = nullptr; // last-block counters
+  double2* h_out = nullptr;    // pinned host copy
+  int nblocks = 0;
+  int init(cudaStream_t s);
+  void release();
+  // results of up to 8 dots, each sum over conj(a)*b (conj=1) or a*b (conj=0)
+  int dots(int n, int k, const C* const* a, const C* const* b, const int* conjf, double2* host_out);
+  double2 dotc(int n, const C* a, const C* b, int* err);
+  double2 dotu(int n, const C* a, const C* b, int* err);
+  double nrm2(int n, const C* a, int* err);
+  double norm_diff(int n, const C* a, const C* b, int* err);             // ||a-b||
+  double norm_gap(int n, const C* a, const C* b, const C* c, int* err);  // ||a-b-c||
+};
+
+// elementwise launches (stream-ordered)
+template <typename T> void v_copy(cplx<T>* d, const cplx<T>* a, int n, cudaStream_t s);
+template <typename T> void v_zero(cplx<T>* d, int n, cudaStream_t s);
+template <typename T> void v_diff(cplx<T>* d, const cplx<T>* a, const cplx<T>* b, int n, cudaStream_t s);  // d=a-b
+// d = za*a + zb*b + zd*d   (any pointer may alias d; null a/b skip the term)
+template <typename T>
+void v_lincomb(cplx<T>* d, double2 zd, const cplx<T>* a, double2 za, const cplx<T>* b, double2 zb, int n, cudaStream_t s);
+// d = a / adia_full[c*nat + occ[k]] (the DIAGL left preconditioner)
+template <typename T>
+void v_precon(cplx<T>* d, const cplx<T>* a, const cplx<T>* adia_full, const int* occ, int nat, int nat0, cudaStream_t s);
+template <typename T> void v_gather(const cplx<T>* full, cplx<T>* compact, const int* occ, int nat, int nat0, cudaStream_t s);
+template <typename T> void v_scatter(const cplx<T>* compact, cplx<T>* full, const int* occ, int nat, int nat0, cudaStream_t s);
+
+}  // namespace ddb

@@ -1,0 +1,463 @@
+// FFT-accelerated DDA MATVEC, z-first pipeline (sm_100a).
+//
+// y = CXADIA o x - (G * x) + CXAOFF 3x3 site blocks, unoccupied sites zeroed;
+// CWHAT='C' conjugates x on input and y on output.  This is the operator of
+// ddscat_cuda_unified/fortran/cprod_cuda.f90:446-607 evaluated as in
+// ddscat_cuda_unified/cuda/ddscat_matvec_cuda.cu:104-118 (pad, FFT(+i), Green
+// 3x3 multiply from the octant with sign flips, FFT(-i), finish with 1/ngrid),
+// but organised per axis so the zero-padded half is never transformed on the
+// forward side and never produced on the inverse side:
+//   k_zfwd    : compact/full x -> z-FFT(+i) of n_z inputs -> zhat (M_z planes)
+//   k_xfwd    : zhat plane rows (n_x inputs) -> x-FFT(+i) -> slab rows (M_x)
+//   k_ygreen  : slab columns (n_y inputs) -> y-FFT(+i) -> Green -> y-FFT(-i),
+//               keep n_y outputs
+//   k_xinv    : slab rows -> x-FFT(-i), keep n_x -> zhat
+//   k_zinv_fin: zhat columns -> z-FFT(-i), keep n_z -> finish -> y
+#include <algorithm>
+#include <cstdlib>
+#include "engine.h"
+
+namespace ddb {
+
+template <typename T> struct MvParams {
+  int nx, ny, nz, Mx, My, Mz, nat, nat0;
+  const cplx<T>* x;
+  size_t x_rs;
+  cplx<T>* y;
+  size_t y_rs;
+  const cplx<T>* adia;
+  const cplx<T>* aoff;
+  size_t a_rs;
+  int io_full, a_full, conj;
+  const int* inv;
+  const int16_t* iocc;
+  const int* mask;
+  int rhs0;  // global index of local RHS 0 (for the mask)
+  cplx<T>* zhat;
+  size_t zhat_rs;
+  cplx<T>* slab;
+  int kz0, nplanes;  // planes kz0 .. kz0+nplanes-1 live in the slab
+  int slab_rhs0;     // local RHS index of slab RHS 0 (relative to zhat)
+  const cplx<T>* green;
+  int ipbc;
+  FftPlan px, py, pz;
+  const cplx<T>* twx;
+  const cplx<T>* twy;
+  const cplx<T>* twz;
+  int tz, ry, ty;  // tile widths
+  T inv_ngrid;
+};
+
+template <typename T> __device__ __forceinline__ bool rhs_off(const MvParams<T>& P, int rl) {
+  return P.mask != nullptr && P.mask[P.rhs0 + rl] == 0;
+}
+
+// ---------------------------------------------------------------- z forward
+template <typename T> __global__ void __launch_bounds__(256) k_zfwd(MvParams<T> P) {
+  using C = cplx<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int TX = P.tz;
+  C* A = reinterpret_cast<C*>(smem_raw);
+  C* B = A + (size_t)TX * P.Mz;
+  const int ix0 = blockIdx.x * TX, iy = blockIdx.y;
+  const int rl = blockIdx.z / 3, c = blockIdx.z % 3;
+  if (rhs_off(P, rl)) return;
+  const C* x = P.x + (size_t)rl * P.x_rs;
+  const size_t S = P.io_full ? (size_t)P.nat : (size_t)P.nat0;
+  const int tot = TX * P.Mz;
+  for (int t = threadIdx.x; t < tot; t += blockDim.x) {
+    const int l = t % TX, e = t / TX, ix = ix0 + l;
+    C v = mk<C>(0, 0);
+    if (e < P.nz && ix < P.nx) {
+      const size_t j = (size_t)ix + (size_t)P.nx * ((size_t)iy + (size_t)P.ny * e);
+      if (P.io_full) {
+        v = x[c * S + j];
+      } else {
+        const int q = P.inv[j];
+        if (q >= 0) v = x[c * S + q];
+      }
+      if (P.conj) v.y = -v.y;
+    }
+    A[e * TX + l] = v;
+  }
+  __syncthreads();
+  C* R = fft_tile<+1>(A, B, Lay{1, TX}, TX, P.pz, P.twz);
+  C* zh = P.zhat + (size_t)rl * P.zhat_rs + (size_t)c * P.Mz * P.ny * P.nx;
+  for (int t = threadIdx.x; t < tot; t += blockDim.x) {
+    const int l = t % TX, e = t / TX, ix = ix0 + l;
+    if (ix < P.nx) zh[((size_t)e * P.ny + iy) * P.nx + ix] = R[e * TX + l];
+  }
+}
+
+// ---------------------------------------------------------------- x forward
+template <typename T> __global__ void __launch_bounds__(256) k_xfwd(MvParams<T> P) {
+  using C = cplx<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int RY = P.ry, LD = P.Mx + 1;
+  C* A = reinterpret_cast<C*>(smem_raw);
+  C* B = A + (size_t)RY * LD;
+  const int iy0 = blockIdx.x * RY, kzl = blockIdx.y, kz = P.kz0 + kzl;
+  const int rs = blockIdx.z / 3, c = blockIdx.z % 3, rl = P.slab_rhs0 + rs;
+  if (rhs_off(P, rl)) return;
+  const C* zh = P.zhat + (size_t)rl * P.zhat_rs + ((size_t)c * P.Mz + kz) * P.ny * P.nx;
+  const int tot = RY * P.Mx;
+  for (int t = threadIdx.x; t < tot; t += blockDim.x) {
+    const int e = t % P.Mx, l = t / P.Mx, iy = iy0 + l;
+    C v = mk<C>(0, 0);
+    if (e < P.nx && iy < P.ny) v = zh[(size_t)iy * P.nx + e];
+    A[l * LD + e] = v;
+  }
+  __syncthreads();
+  C* R = fft_tile<+1>(A, B, Lay{LD, 1}, RY, P.px, P.twx);
+  C* sl = P.slab + (((size_t)rs * 3 + c) * P.nplanes + kzl) * P.ny * P.Mx;
+  for (int t = threadIdx.x; t < tot; t += blockDim.x) {
+    const int e = t % P.Mx, l = t / P.Mx, iy = iy0 + l;
+    if (iy < P.ny) sl[(size_t)iy * P.Mx + e] = R[l * LD + e];
+  }
+}
+
+// Green tensor at spectral point (kx,ky,kz): symmetric 3x3 (a11,a12,a13,a22,a23,a33)
+template <typename T>
+__device__ __forceinline__ void green_at(const MvParams<T>& P, int kx, int ky, int kz, cplx<T> a[6]) {
+  if (P.ipbc == 0) {
+    const T sx = kx <= P.nx ? (T)1 : (T)-1, sy = ky <= P.ny ? (T)1 : (T)-1, sz = kz <= P.nz ? (T)1 : (T)-1;
+    const int irx = min(kx, P.Mx - kx), iry = min(ky, P.My - ky), irz = min(kz, P.Mz - kz);
+    const size_t cx = P.nx + 1, cy = P.ny + 1, cz = P.nz + 1;
+    const size_t b = (size_t)irx + cx * ((size_t)iry + cy * irz), st = cx * cy * cz;
+    a[0] = P.green[b];
+    a[1] = cscale(P.green[b + st], sx * sy);
+    a[2] = cscale(P.green[b + 2 * st], sx * sz);
+    a[3] = P.green[b + 3 * st];
+    a[4] = cscale(P.green[b + 4 * st], sy * sz);
+    a[5] = P.green[b + 5 * st];
+  } else {
+    const size_t st = (size_t)P.Mx * P.My * P.Mz;
+    const size_t k = (size_t)kx + (size_t)P.Mx * ((size_t)ky + (size_t)P.My * kz);
+#pragma unroll
+    for (int m = 0; m < 6; ++m) a[m] = P.green[k + m * st];
+  }
+}
+
+// ---------------------------------------------------------------- y forward * Green * y inverse
+template <typename T> __global__ void __launch_bounds__(256) k_ygreen(MvParams<T> P) {
+  using C = cplx<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int TX = P.ty, My = P.My;
+  C* D = reinterpret_cast<C*>(smem_raw);  // [3][My][TX]
+  C* S = D + (size_t)3 * My * TX;         // scratch [My][TX]
+  const int kx0 = blockIdx.x * TX, kzl = blockIdx.y, kz = P.kz0 + kzl;
+  const int rs = blockIdx.z, rl = P.slab_rhs0 + rs;
+  if (rhs_off(P, rl)) return;
+  const size_t plane = (size_t)P.ny * P.Mx;
+  C* sl0 = P.slab + ((size_t)rs * 3 * P.nplanes + kzl) * plane;
+  const size_t cstride = (size_t)P.nplanes * plane;
+  const int tot = TX * My;
+  for (int t = threadIdx.x; t < 3 * tot; t += blockDim.x) {
+    const int c = t / tot, u = t % tot, l = u % TX, e = u / TX, kx = kx0 + l;
+    C v = mk<C>(0, 0);
+    if (e < P.ny && kx < P.Mx) v = sl0[c * cstride + (size_t)e * P.Mx + kx];
+    D[(size_t)c * tot + u] = v;
+  }
+  __syncthreads();
+  for (int c = 0; c < 3; ++c) {
+    C* Dc = D + (size_t)c * tot;
+    C* R = fft_tile<+1>(Dc, S, Lay{1, TX}, TX, P.py, P.twy);
+    if (R != Dc) {
+      for (int u = threadIdx.x; u < tot; u += blockDim.x) Dc[u] = R[u];
+      __syncthreads();
+    }
+  }
+  for (int u = threadIdx.x; u < tot; u += blockDim.x) {
+    const int l = u % TX, ky = u / TX, kx = kx0 + l;
+    if (kx >= P.Mx) continue;
+    C a[6];
+    green_at(P, kx, ky, kz, a);
+    const C px = D[u], py = D[tot + u], pz = D[2 * tot + u];
+    D[u] = cadd(cadd(cmul(a[0], px), cmul(a[1], py)), cmul(a[2], pz));
+    D[tot + u] = cadd(cadd(cmul(a[1], px), cmul(a[3], py)), cmul(a[4], pz));
+    D[2 * tot + u] = cadd(cadd(cmul(a[2], px), cmul(a[4], py)), cmul(a[5], pz));
+  }
+  __syncthreads();
+  for (int c = 0; c < 3; ++c) {
+    C* Dc = D + (size_t)c * tot;
+    C* R = fft_tile<-1>(Dc, S, Lay{1, TX}, TX, P.py, P.twy);
+    if (R != Dc) {
+      for (int u = threadIdx.x; u < tot; u += blockDim.x) Dc[u] = R[u];
+      __syncthreads();
+    }
+  }
+  const int totn = TX * P.ny;
+  for (int t = threadIdx.x; t < 3 * totn; t += blockDim.x) {
+    const int c = t / totn, u = t % totn, l = u % TX, e = u / TX, kx = kx0 + l;
+    if (kx < P.Mx) sl0[c * cstride + (size_t)e * P.Mx + kx] = D[(size_t)c * tot + u];
+  }
+}
+
+// ---------------------------------------------------------------- x inverse
+template <typename T> __global__ void __launch_bounds__(256) k_xinv(MvParams<T> P) {
+  using C = cplx<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int RY = P.ry, LD = P.Mx + 1;
+  C* A = reinterpret_cast<C*>(smem_raw);
+  C* B = A + (size_t)RY * LD;
+  const int iy0 = blockIdx.x * RY, kzl = blockIdx.y, kz = P.kz0 + kzl;
+  const int rs = blockIdx.z / 3, c = blockIdx.z % 3, rl = P.slab_rhs0 + rs;
+  if (rhs_off(P, rl)) return;
+  const C* sl = P.slab + (((size_t)rs * 3 + c) * P.nplanes + kzl) * P.ny * P.Mx;
+  const int tot = RY * P.Mx;
+  for (int t = threadIdx.x; t < tot; t += blockDim.x) {
+    const int e = t % P.Mx, l = t / P.Mx, iy = iy0 + l;
+    C v = mk<C>(0, 0);
+    if (iy < P.ny) v = sl[(size_t)iy * P.Mx + e];
+    A[l * LD + e] = v;
+  }
+  __syncthreads();
+  C* R = fft_tile<-1>(A, B, Lay{LD, 1}, RY, P.px, P.twx);
+  C* zh = P.zhat + (size_t)rl * P.zhat_rs + ((size_t)c * P.Mz + kz) * P.ny * P.nx;
+  const int totn = RY * P.nx;
+  for (int t = threadIdx.x; t < totn; t += blockDim.x) {
+    const int e = t % P.nx, l = t / P.nx, iy = iy0 + l;
+    if (iy < P.ny) zh[(size_t)iy * P.nx + e] = R[l * LD + e];
+  }
+}
+
+// ---------------------------------------------------------------- z inverse + finish
+template <typename T> __global__ void __launch_bounds__(256) k_zinv_fin(MvParams<T> P) {
+  using C = cplx<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int TX = P.tz;
+  C* A = reinterpret_cast<C*>(smem_raw);
+  C* B = A + (size_t)TX * P.Mz;
+  const int ix0 = blockIdx.x * TX, iy = blockIdx.y;
+  const int rl = blockIdx.z / 3, c = blockIdx.z % 3;
+  if (rhs_off(P, rl)) return;
+  const C* zh = P.zhat + (size_t)rl * P.zhat_rs + (size_t)c * P.Mz * P.ny * P.nx;
+  const int tot = TX * P.Mz;
+  for (int t = threadIdx.x; t < tot; t += blockDim.x) {
+    const int l = t % TX, e = t / TX, ix = ix0 + l;
+    C v = mk<C>(0, 0);
+    if (ix < P.nx) v = zh[((size_t)e * P.ny + iy) * P.nx + ix];
+    A[e * TX + l] = v;
+  }
+  __syncthreads();
+  C* R = fft_tile<-1>(A, B, Lay{1, TX}, TX, P.pz, P.twz);
+  const C* x = P.x + (size_t)rl * P.x_rs;
+  C* y = P.y + (size_t)rl * P.y_rs;
+  const C* ad = P.adia + (size_t)rl * P.a_rs;
+  const C* ao = P.aoff ? P.aoff + (size_t)rl * P.a_rs : nullptr;
+  const size_t S = P.io_full ? (size_t)P.nat : (size_t)P.nat0;
+  const size_t SA = P.a_full ? (size_t)P.nat : (size_t)P.nat0;
+  const int totn = TX * P.nz;
+  for (int t = threadIdx.x; t < totn; t += blockDim.x) {
+    const int l = t % TX, iz = t / TX, ix = ix0 + l;
+    if (ix >= P.nx) continue;
+    const size_t j = (size_t)ix + (size_t)P.nx * ((size_t)iy + (size_t)P.ny * iz);
+    size_t q;
+    if (P.io_full) {
+      q = j;
+      if (P.iocc[j] == 0) { y[c * S + q] = mk<C>(0, 0); continue; }
+    } else {
+      const int qq = P.inv[j];
+      if (qq < 0) continue;
+      q = (size_t)qq;
+    }
+    const size_t qa = P.a_full ? j : q;
+    C xc = x[c * S + q];
+    if (P.conj) xc.y = -xc.y;
+    C w = cscale(R[iz * TX + l], P.inv_ngrid);
+    C yv = csub(cmul(ad[c * SA + qa], xc), w);
+    if (ao) {
+      C x1 = x[q], x2 = x[S + q], x3 = x[2 * S + q];
+      if (P.conj) { x1.y = -x1.y; x2.y = -x2.y; x3.y = -x3.y; }
+      const C a23 = ao[qa], a31 = ao[SA + qa], a12 = ao[2 * SA + qa];
+      if (c == 0) yv = cadd(yv, cadd(cmul(a31, x3), cmul(a12, x2)));
+      else if (c == 1) yv = cadd(yv, cadd(cmul(a12, x1), cmul(a23, x3)));
+      else yv = cadd(yv, cadd(cmul(a23, x2), cmul(a31, x1)));
+    }
+    if (P.conj) yv.y = -yv.y;
+    y[c * S + q] = yv;
+  }
+}
+
+// ---------------------------------------------------------------- host side
+static int env_int(const char* name, int dflt) {
+  const char* v = std::getenv(name);
+  if (!v || !*v) return dflt;
+  return std::atoi(v);
+}
+
+template <typename T> static cplx<T>* upload_twiddles(int n, size_t& bytes) {
+  std::vector<cplx<T>> h(n);
+  const double pi = 3.14159265358979323846;
+  for (int m = 0; m < n; ++m) {
+    const double a = -2.0 * pi * (double)m / (double)n;
+    h[m] = mk<cplx<T>>(std::cos(a), std::sin(a));
+  }
+  cplx<T>* d = nullptr;
+  if (cudaMalloc((void**)&d, n * sizeof(cplx<T>)) != cudaSuccess) return nullptr;
+  cudaMemcpy(d, h.data(), n * sizeof(cplx<T>), cudaMemcpyHostToDevice);
+  bytes += n * sizeof(cplx<T>);
+  return d;
+}
+
+template <typename T>
+int Engine<T>::init_geometry(int nx, int ny, int nz, int ipbc, int nat, int nat0, const int16_t* iocc_host) {
+  g.nx = nx; g.ny = ny; g.nz = nz;
+  g.Mx = 2 * nx; g.My = 2 * ny; g.Mz = 2 * nz;
+  g.nat = nat; g.nat0 = nat0; g.ipbc = ipbc;
+  px = make_fft_plan(g.Mx);
+  py = make_fft_plan(g.My);
+  pz = make_fft_plan(g.Mz);
+  if (px.nstages < 0 || py.nstages < 0 || pz.nstages < 0) {
+    set_error("prepare", "FFT length has too many prime factors");
+    return 1;
+  }
+  twx = upload_twiddles<T>(g.Mx, bytes_allocated);
+  twy = upload_twiddles<T>(g.My, bytes_allocated);
+  twz = upload_twiddles<T>(g.Mz, bytes_allocated);
+  if (!twx || !twy || !twz) { set_error("prepare", "twiddle allocation failed"); return 1; }
+  std::vector<int> occ_h, inv_h((size_t)nat, -1);
+  occ_h.reserve(nat0);
+  for (int j = 0; j < nat; ++j)
+    if (iocc_host[j] != 0) { inv_h[j] = (int)occ_h.size(); occ_h.push_back(j); }
+  if ((int)occ_h.size() != nat0) {
+    char msg[160];
+    std::snprintf(msg, sizeof(msg), "IOCC contains %zu occupied sites but NAT0=%d", occ_h.size(), nat0);
+    set_error("occupied-index map", msg);
+    return 2;
+  }
+  cudaError_t e;
+  e = cudaMalloc((void**)&occ, (size_t)nat0 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&inv, (size_t)nat * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&iocc, (size_t)nat * sizeof(int16_t));
+  if (e != cudaSuccess) { set_cuda_error("prepare: index maps", e); return 3; }
+  bytes_allocated += (size_t)nat0 * 4 + (size_t)nat * 6;
+  cudaMemcpy(occ, occ_h.data(), (size_t)nat0 * sizeof(int), cudaMemcpyHostToDevice);
+  cudaMemcpy(inv, inv_h.data(), (size_t)nat * sizeof(int), cudaMemcpyHostToDevice);
+  e = cudaMemcpy(iocc, iocc_host, (size_t)nat * sizeof(int16_t), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) { set_cuda_error("prepare: index map H2D", e); return 3; }
+  e = cudaMalloc((void**)&green, g.green_count() * sizeof(C));
+  if (e != cudaSuccess) { set_cuda_error("malloc resident Green", e); return 4; }
+  bytes_allocated += g.green_count() * sizeof(C);
+  // slab budget: FFT3D keeps up to 64 MiB of xy spectrum per batch (fits the
+  // 126 MB L2 together with the Green octant traffic); SLICES keeps 4 planes.
+  const int mb = env_int("DDSCAT_B200_SLAB_MB", 64);
+  slab_budget_elems = (size_t)mb * 1024 * 1024 / sizeof(C);
+  return 0;
+}
+
+template <typename T> int Engine<T>::ensure_workspace(int nrhs) {
+  const size_t per_rhs_z = (size_t)3 * g.Mz * g.ny * g.nx;
+  const size_t per_plane = (size_t)3 * g.ny * g.Mx;  // one kz plane, 3 comps, one RHS
+  if (nrhs <= zcap && zhat) return 0;
+  if (zhat) { cudaFree(zhat); bytes_allocated -= (size_t)zcap * per_rhs_z * sizeof(C); zhat = nullptr; }
+  if (slab) { cudaFree(slab); bytes_allocated -= (size_t)slab_nr * slab_B * per_plane * sizeof(C); slab = nullptr; }
+  zcap = nrhs;
+  cudaError_t e = cudaMalloc((void**)&zhat, (size_t)zcap * per_rhs_z * sizeof(C));
+  if (e != cudaSuccess) { zcap = 0; set_cuda_error("malloc z-spectrum workspace", e); return 1; }
+  bytes_allocated += (size_t)zcap * per_rhs_z * sizeof(C);
+  if (slices_layout) {
+    slab_nr = 1;
+    slab_B = std::min(4, g.Mz);
+  } else {
+    const size_t full_rhs = per_plane * g.Mz;
+    if (full_rhs * zcap <= slab_budget_elems) { slab_nr = zcap; slab_B = g.Mz; }
+    else if (full_rhs <= slab_budget_elems) { slab_nr = (int)std::max<size_t>(1, slab_budget_elems / full_rhs); slab_B = g.Mz; }
+    else { slab_nr = 1; slab_B = (int)std::max<size_t>(1, slab_budget_elems / per_plane); }
+  }
+  e = cudaMalloc((void**)&slab, (size_t)slab_nr * slab_B * per_plane * sizeof(C));
+  if (e != cudaSuccess) { set_cuda_error("malloc xy-slab workspace", e); return 1; }
+  bytes_allocated += (size_t)slab_nr * slab_B * per_plane * sizeof(C);
+  return 0;
+}
+
+template <typename T> static void set_smem(const void* f) {
+  cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+}
+
+template <typename T> int Engine<T>::matvec(const MvArgs<T>& a) {
+  static bool attr_done = false;
+  if (!attr_done) {
+    set_smem<T>((const void*)k_zfwd<T>);
+    set_smem<T>((const void*)k_xfwd<T>);
+    set_smem<T>((const void*)k_ygreen<T>);
+    set_smem<T>((const void*)k_xinv<T>);
+    set_smem<T>((const void*)k_zinv_fin<T>);
+    attr_done = true;
+  }
+  {
+    // z-spectrum capacity: all RHS of the call if they fit the budget
+    const size_t per_rhs_z = (size_t)3 * g.Mz * g.ny * g.nx * sizeof(C);
+    const size_t budget = (size_t)env_int("DDSCAT_B200_ZHAT_MB", 16384) * 1024 * 1024;
+    const int want = (int)std::max<size_t>(1, std::min<size_t>((size_t)a.nrhs, budget / per_rhs_z));
+    if (ensure_workspace(want)) return 1;
+  }
+  MvParams<T> P{};
+  P.nx = g.nx; P.ny = g.ny; P.nz = g.nz; P.Mx = g.Mx; P.My = g.My; P.Mz = g.Mz;
+  P.nat = g.nat; P.nat0 = g.nat0;
+  P.x_rs = a.x_rs; P.y_rs = a.y_rs; P.a_rs = a.a_rs;
+  P.io_full = a.io_full; P.a_full = a.a_full; P.conj = a.conj;
+  P.inv = inv; P.iocc = iocc; P.mask = a.mask;
+  P.zhat = zhat; P.zhat_rs = (size_t)3 * g.Mz * g.ny * g.nx;
+  P.slab = slab;
+  P.green = green; P.ipbc = g.ipbc;
+  P.px = px; P.py = py; P.pz = pz;
+  P.twx = twx; P.twy = twy; P.twz = twz;
+  P.inv_ngrid = (T)(1.0 / (double)g.ngrid());
+  const int tile_elems = (sizeof(C) == 8) ? 4096 : 2048;  // complex elements per 32 KiB tile
+  P.tz = std::max(1, std::min(32, tile_elems / g.Mz));
+  P.ry = std::max(1, std::min(16, tile_elems / (g.Mx + 1)));
+  P.ty = std::max(1, std::min(32, (tile_elems / 2) / g.My));
+  const size_t sm_z = (size_t)2 * P.tz * g.Mz * sizeof(C);
+  const size_t sm_x = (size_t)2 * P.ry * (g.Mx + 1) * sizeof(C);
+  const size_t sm_y = (size_t)4 * P.ty * g.My * sizeof(C);
+  const int threads = 256;
+  for (int r0 = 0; r0 < a.nrhs; r0 += zcap) {
+    const int nr = std::min(zcap, a.nrhs - r0);
+    P.rhs0 = r0;
+    P.x = a.x + (size_t)r0 * a.x_rs;
+    P.y = a.y + (size_t)r0 * a.y_rs;
+    P.adia = a.adia + (size_t)r0 * a.a_rs;
+    P.aoff = a.aoff ? a.aoff + (size_t)r0 * a.a_rs : nullptr;
+    dim3 gz((unsigned)ceil_div(g.nx, P.tz), (unsigned)g.ny, (unsigned)(3 * nr));
+    k_zfwd<T><<<gz, threads, sm_z, stream>>>(P);
+    if (check_launch("MATVEC z-forward")) return 21;
+    for (int rs = 0; rs < nr; rs += slab_nr) {
+      const int nrs = std::min(slab_nr, nr - rs);
+      P.slab_rhs0 = rs;
+      for (int kz0 = 0; kz0 < g.Mz; kz0 += slab_B) {
+        P.kz0 = kz0;
+        P.nplanes = std::min(slab_B, g.Mz - kz0);
+        dim3 gx((unsigned)ceil_div(g.ny, P.ry), (unsigned)P.nplanes, (unsigned)(3 * nrs));
+        k_xfwd<T><<<gx, threads, sm_x, stream>>>(P);
+        if (check_launch("MATVEC x-forward")) return 22;
+        dim3 gy((unsigned)ceil_div(g.Mx, P.ty), (unsigned)P.nplanes, (unsigned)nrs);
+        k_ygreen<T><<<gy, threads, sm_y, stream>>>(P);
+        if (check_launch("MATVEC y-Green")) return 23;
+        k_xinv<T><<<gx, threads, sm_x, stream>>>(P);
+        if (check_launch("MATVEC x-inverse")) return 24;
+      }
+    }
+    k_zinv_fin<T><<<gz, threads, sm_z, stream>>>(P);
+    if (check_launch("MATVEC z-inverse/finish")) return 25;
+  }
+  return 0;
+}
+
+template <typename T> int Engine<T>::upload_green(const void* host_green) {
+  cudaError_t e = cudaMemcpy(green, host_green, g.green_count() * sizeof(C), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) { set_cuda_error("green H2D", e); return 4; }
+  return 0;
+}
+
+template <typename T> void Engine<T>::release() {
+  cudaFree(twx); cudaFree(twy); cudaFree(twz);
+  cudaFree(green); cudaFree(occ); cudaFree(inv); cudaFree(iocc);
+  cudaFree(zhat); cudaFree(slab);
+  *this = Engine<T>{};
+}
+
+template struct Engine<float>;
+template struct Engine<double>;
+
+}  // namespace ddb

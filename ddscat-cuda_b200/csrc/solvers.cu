@@ -1,0 +1,1116 @@
+// Krylov solvers behind the ddscat_cuda_solve_*_f32 entry points.
+//
+// Each routine restates the corresponding reference routine of
+// ddscat_cuda_unified/cuda/ddscat_matvec_cuda.cu (line ranges at each
+// function) on compact 3*NAT0 device vectors: FP32 vectors, FP64 recurrence
+// scalars, FP64 inner products, the reliable-residual policy (true residual
+// every 20 iterations and on claimed convergence, restart when the recursion
+// gap >= 1e-3 or on false convergence, cu:543-556), the same MATVEC counting
+// and the same error codes.  Scalars are combined on the host from the
+// device-reduced inner products (one small D2H per product, no full-vector
+// transfers inside the loops).
+#include <complex>
+#include "engine.h"
+#include "solvers.h"
+
+namespace ddb {
+
+using Z = std::complex<double>;
+static inline double2 dz(Z z) { return make_double2(z.real(), z.imag()); }
+static inline Z zd(double2 v) { return Z(v.x, v.y); }
+
+constexpr int RELIABLE_PERIOD = 20;
+constexpr double RELIABLE_GAP = 1.0e-3;
+
+template <typename T> struct Ctx {
+  using C = cplx<T>;
+  SolveIO<T>& io;
+  int n;
+  int nc = 0;
+  int err = 0;
+  explicit Ctx(SolveIO<T>& s) : io(s), n(s.n) {}
+  cudaStream_t st() const { return io.stream; }
+  int mv(const C* in, C* out, int conj = 0) {
+    MvArgs<T> a;
+    a.x = in; a.y = out; a.io_full = 0;
+    a.adia = io.adia; a.aoff = io.aoff; a.a_full = io.a_full; a.conj = conj; a.nrhs = 1;
+    int rc = io.eng->matvec(a);
+    if (!rc) ++nc;
+    if (!rc && io.verbose) std::printf("CUDA MATVEC %d [%c]\n", nc, conj ? 'C' : 'N');
+    return rc;
+  }
+  Z dotc(const C* a, const C* b) { return zd(io.ops->dotc(n, a, b, &err)); }
+  Z dotu(const C* a, const C* b) { return zd(io.ops->dotu(n, a, b, &err)); }
+  double nrm(const C* a) { return io.ops->nrm2(n, a, &err); }
+  // d = zd*d + za*a + zb*b
+  void lin(C* d, Z zdd, const C* a = nullptr, Z za = 0.0, const C* b = nullptr, Z zb = 0.0) {
+    v_lincomb<T>(d, dz(zdd), a, dz(za), b, dz(zb), n, st());
+  }
+  void copy(C* d, const C* a) { v_copy<T>(d, a, n, st()); }
+  void zero(C* d) { v_zero<T>(d, n, st()); }
+  void diff(C* d, const C* a, const C* b) { v_diff<T>(d, a, b, n, st()); }
+  C* w(int slot) { return io.work + (size_t)slot * n; }
+  // cu:543-556
+  int reliable(const char* name, const C* rhs, const C* xcur, const C* rrec, double rhsnorm, double recursive,
+               double tol, double& true_res, bool& converged, bool& restart) {
+    if (rhsnorm <= 0.0) { set_error(name, "reliable residual: zero RHS norm"); return 1; }
+    int rc = mv(xcur, io.sy);
+    if (rc) return rc;
+    const double tr = io.ops->norm_diff(n, rhs, io.sy, &err);
+    const double gapn = io.ops->norm_gap(n, rhs, io.sy, rrec, &err);
+    if (err) return 1;
+    true_res = tr / rhsnorm;
+    const double gap = tr > 0.0 ? gapn / tr : (gapn == 0.0 ? 0.0 : INFINITY);
+    converged = true_res <= tol;
+    restart = gap >= RELIABLE_GAP || (recursive <= tol && !converged);
+    if (io.verbose) std::printf(" %s reliable: true=%14.6E gap=%14.6E%s\n", name, true_res, gap, restart ? " RESTART" : "");
+    return 0;
+  }
+};
+
+#define CK(code)                         \
+  do {                                   \
+    if (c.err) return (code);            \
+    if (check_launch(name)) return (code); \
+  } while (0)
+#define MV(in, out, code)            \
+  do {                               \
+    int _rc = c.mv((in), (out));     \
+    if (_rc) return _rc;             \
+  } while (0)
+
+// ---------------------------------------------------------------- PBCGS2 (cu:459-480, cu:1168-1278)
+template <typename T> int solve_pbcgs2(SolveIO<T>& io) {
+  using C = cplx<T>;
+  const char* name = "PBCGS2";
+  Ctx<T> c(io);
+  C *rr = c.w(0), *r[3] = {c.w(1), c.w(2), c.w(3)}, *u[3] = {c.w(4), c.w(5), c.w(6)};
+  C *XP = c.w(7), *BP = c.w(8), *X = c.w(9);
+  // init: rr=r0=BP=b, XP=x0, the rest 0 (cu:462)
+  c.copy(XP, io.x);
+  c.copy(rr, io.b); c.copy(r[0], io.b); c.copy(BP, io.b);
+  c.zero(r[1]); c.zero(r[2]); c.zero(u[0]); c.zero(u[1]); c.zero(u[2]); c.zero(X);
+  const double rnrm0 = c.nrm(r[0]);
+  CK(92);
+  double rnrm = rnrm0, mxnrmx = rnrm0, mxnrmr = rnrm0;
+  Z alpha = 0.0, omega = 1.0, sigma = 1.0, rho0 = 1.0, rho1 = 0.0, beta;
+  double resid = rnrm0 > 0.0 ? 1.0 : 0.0;
+  int it = 0;
+  while (resid > io.tol && it < io.maxit) {
+    ++it;
+    rho0 = -(omega * rho0);
+    for (int k = 1; k <= 2; ++k) {
+      rho1 = c.dotc(rr, r[k - 1]);
+      CK(94);
+      if (rho0 == Z(0.0)) { set_error(name, "ZBCG2 breakdown: RHO0 == 0"); return 95; }
+      beta = alpha * (rho1 / rho0);
+      rho0 = rho1;
+      for (int j = 0; j < k; ++j) c.lin(u[j], -beta, r[j], 1.0);
+      MV(u[k - 1], u[k], 96);
+      sigma = c.dotc(rr, u[k]);
+      CK(97);
+      if (sigma == Z(0.0)) { set_error(name, "ZBCG2 breakdown: SIGMA == 0"); return 98; }
+      alpha = rho1 / sigma;
+      c.lin(X, 1.0, u[0], alpha);
+      for (int j = 0; j < k; ++j) c.lin(r[j], 1.0, u[j + 1], -alpha);
+      MV(r[k - 1], r[k], 99);
+      rnrm = c.nrm(r[0]);
+      CK(100);
+      mxnrmx = std::max(mxnrmx, rnrm);
+      mxnrmr = std::max(mxnrmr, rnrm);
+    }
+    // Hermitian Gram matrix Z[i][j] = r_i^H r_j (lower triangle computed, cu:1215-1220)
+    Z Zm[3][3];
+    {
+      const C* A6[6] = {r[0], r[1], r[1], r[2], r[2], r[2]};
+      const C* B6[6] = {r[0], r[0], r[1], r[0], r[1], r[2]};
+      const int cj[6] = {1, 1, 1, 1, 1, 1};
+      double2 o[6];
+      if (io.ops->dots(c.n, 6, A6, B6, cj, o)) return 101;
+      Zm[0][0] = zd(o[0]); Zm[1][0] = zd(o[1]); Zm[1][1] = zd(o[2]);
+      Zm[2][0] = zd(o[3]); Zm[2][1] = zd(o[4]); Zm[2][2] = zd(o[5]);
+      Zm[0][1] = std::conj(Zm[1][0]); Zm[0][2] = std::conj(Zm[2][0]); Zm[1][2] = std::conj(Zm[2][1]);
+    }
+    // convex polynomial (cu:471-472)
+    if (Zm[1][1] == Z(0.0)) { set_error(name, "ZBCG2 convex-polynomial breakdown"); return 102; }
+    Z y0[3] = {-1.0, Zm[1][0] / Zm[1][1], 0.0};
+    Z yl[3] = {0.0, Zm[1][2] / Zm[1][1], -1.0};
+    auto matv = [&](const Z* v, Z* o) { for (int i = 0; i < 3; ++i) { o[i] = 0.0; for (int j = 0; j < 3; ++j) o[i] += Zm[i][j] * v[j]; } };
+    auto inner = [](const Z* a, const Z* b) { Z s = 0.0; for (int i = 0; i < 3; ++i) s += std::conj(a[i]) * b[i]; return s; };
+    Z zy0[3], zyl[3];
+    matv(y0, zy0);
+    matv(yl, zyl);
+    const double k0 = std::sqrt(std::abs(inner(y0, zy0))), kl = std::sqrt(std::abs(inner(yl, zyl)));
+    if (k0 == 0.0 || kl == 0.0) { set_error(name, "ZBCG2 convex-polynomial breakdown"); return 102; }
+    const Z vr = inner(yl, zy0) / (k0 * kl);
+    const double avr = std::abs(vr);
+    if (avr == 0.0) { set_error(name, "ZBCG2 convex-polynomial breakdown"); return 102; }
+    const Z hg = vr * (std::max(avr, 0.7) / avr);
+    const Z fac = hg * (k0 / kl);
+    for (int i = 0; i < 3; ++i) y0[i] -= fac * yl[i];
+    const Z Y1 = y0[1], Y2 = y0[2];
+    omega = y0[2];
+    matv(y0, zy0);
+    rnrm = std::sqrt(std::abs(inner(y0, zy0)));
+    mxnrmx = std::max(mxnrmx, rnrm);
+    mxnrmr = std::max(mxnrmr, rnrm);
+    // u0 -= Y1 u1 + Y2 u2 ; X += Y1 r0 + Y2 r1 ; r0 -= Y1 r1 + Y2 r2
+    c.lin(u[0], 1.0, u[1], -Y1, u[2], -Y2);
+    c.lin(X, 1.0, r[0], Y1, r[1], Y2);
+    c.lin(r[0], 1.0, r[1], -Y1, r[2], -Y2);
+    CK(103);
+    const double delta = 1.0e-2;
+    const bool xpdt = rnrm < delta * rnrm0 && rnrm0 < mxnrmx;
+    const bool rcmp = (rnrm < delta * mxnrmr && rnrm0 < mxnrmr) || xpdt;
+    resid = rnrm0 > 0.0 ? rnrm / rnrm0 : 0.0;
+    if ((it % RELIABLE_PERIOD) == 0 || resid <= io.tol) {
+      double tres;
+      bool conv, rest;
+      int rc = c.reliable("PBCGS2", BP, X, r[0], rnrm0, resid, io.tol, tres, conv, rest);
+      if (rc) return rc == 1 ? 104 : rc;
+      if (conv) { resid = tres; break; }
+      if (rest) {
+        c.diff(r[0], BP, io.sy);        // r0 = BP - A X
+        c.lin(XP, 1.0, X, 1.0);          // XP += X
+        c.zero(X);
+        c.copy(BP, r[0]);
+        c.copy(rr, r[0]);
+        c.zero(r[1]); c.zero(r[2]); c.zero(u[0]); c.zero(u[1]); c.zero(u[2]);
+        rnrm = mxnrmx = mxnrmr = tres * rnrm0;
+        alpha = 0.0; omega = 1.0; sigma = 1.0; rho0 = 1.0;
+        resid = tres;
+        CK(104);
+        if (io.verbose) std::printf(" PBCGS2 reliable restart at iteration %d\n", it);
+        continue;
+      }
+    }
+    if (rcmp) {
+      MV(X, io.sy, 104);
+      c.diff(r[0], BP, io.sy);
+      if (xpdt) {
+        c.lin(XP, 1.0, X, 1.0);
+        c.zero(X);
+        c.copy(BP, r[0]);
+      }
+      mxnrmr = rnrm;
+      if (xpdt) mxnrmx = rnrm;
+      CK(104);
+    }
+    if (io.verbose) std::printf(" PBCGS2 iteration=%6d residual=%14.6E\n", it, resid);
+  }
+  // X = X + XP and one final true residual against the original b (cu:1259-1264)
+  c.lin(X, 1.0, XP, 1.0);
+  MV(X, io.sy, 105);
+  c.diff(r[0], io.b, io.sy);
+  rnrm = c.nrm(r[0]);
+  CK(106);
+  resid = rnrm0 > 0.0 ? rnrm / rnrm0 : INFINITY;
+  c.copy(io.x, X);
+  CK(107);
+  io.itno = it; io.tole = resid; io.ncompte = c.nc;
+  return 0;  // ZBCG2 reports non-convergence through TOLE only (cu:1275-1277)
+}
+
+// ---------------------------------------------------------------- QMRCCG (cu:434-443, cu:1071-1103)
+template <typename T> int solve_qmrccg(SolveIO<T>& io) {
+  using C = cplx<T>;
+  const char* name = "QMRCCG";
+  Ctx<T> c(io);
+  C *r = c.w(0), *p = c.w(1), *ap = c.w(2), *q = c.w(3), *d = c.w(4), *s = c.w(5);
+  C *vt = c.w(6), *wt = c.w(7), *atw = c.w(8), *xs = c.w(9);
+  const double bnorm = c.nrm(io.b);
+  CK(52);
+  if (bnorm == 0.0) { set_error(name, "zero RHS norm"); return 52; }
+  c.copy(xs, io.x);
+  MV(xs, io.sy, 53);
+  c.diff(r, io.b, io.sy);
+  c.zero(p); c.zero(ap); c.zero(q); c.zero(d); c.zero(s); c.zero(atw);
+  c.copy(vt, r); c.copy(wt, r);
+  Z lambda, kappa, theta, gamma, ksi, rho, eps, mu, tau;
+  auto init_scalars = [&]() -> int {
+    const C* A3[3] = {vt, wt, vt};
+    const C* B3[3] = {vt, wt, wt};
+    const int cj[3] = {1, 1, 0};
+    double2 o[3];
+    if (io.ops->dots(c.n, 3, A3, B3, cj, o)) return 54;
+    const double gn = std::sqrt(std::max(0.0, o[0].x)), kn = std::sqrt(std::max(0.0, o[1].x));
+    rho = zd(o[2]);
+    int rc = c.mv(wt, io.sy);
+    if (rc) return rc;
+    c.copy(atw, io.sy);
+    eps = c.dotu(vt, atw);
+    if (c.err) return 54;
+    lambda = 1.0; kappa = -1.0; theta = -1.0; gamma = gn; ksi = kn; mu = 0.0;
+    if (rho == Z(0.0) || gamma == Z(0.0) || ksi == Z(0.0)) {
+      char msg[80];
+      std::snprintf(msg, sizeof(msg), "breakdown at step %d", rho == Z(0.0) ? 5 : (gamma == Z(0.0) ? 6 : 7));
+      set_error(name, msg);
+      return 55;
+    }
+    tau = eps / rho;
+    return 0;
+  };
+  int rc = init_scalars();
+  if (rc) return rc;
+  double resid = c.nrm(r) / bnorm;
+  CK(55);
+  int it = 0;
+  while (it < io.maxit && resid > io.tol) {
+    ++it;
+    // p = vt/gamma - mu p ; q = (atw - gamma mu q)/ksi
+    c.lin(p, -mu, vt, 1.0 / gamma);
+    c.lin(q, -(gamma * mu) / ksi, atw, 1.0 / ksi);
+    MV(p, io.sy, 56);
+    c.copy(ap, io.sy);
+    c.lin(vt, -(tau / gamma), io.sy, 1.0);
+    c.lin(wt, -(tau / ksi), q, 1.0);
+    double gn, kn;
+    Z new_rho;
+    {
+      const C* A3[3] = {vt, wt, vt};
+      const C* B3[3] = {vt, wt, wt};
+      const int cj[3] = {1, 1, 0};
+      double2 o[3];
+      if (io.ops->dots(c.n, 3, A3, B3, cj, o)) return 57;
+      gn = std::sqrt(std::max(0.0, o[0].x));
+      kn = std::sqrt(std::max(0.0, o[1].x));
+      new_rho = zd(o[2]);
+    }
+    MV(wt, io.sy, 57);
+    c.copy(atw, io.sy);
+    const Z new_eps = c.dotu(vt, atw);
+    CK(57);
+    // scalar recurrence (cu:442)
+    const Z gamma0 = gamma, ksi0 = ksi, rho0 = rho, tau0 = tau, kappa0 = kappa;
+    gamma = gn; ksi = kn; rho = new_rho; eps = new_eps;
+    int st = 0;
+    if (gamma == Z(0.0)) st = 6;
+    else if (ksi == Z(0.0)) st = 7;
+    Z den = gamma * tau * rho0;
+    if (!st && den == Z(0.0)) st = 12;
+    if (!st) {
+      mu = gamma0 * ksi0 * rho / den;
+      if (rho == Z(0.0)) st = 13;
+    }
+    if (!st) {
+      tau = eps / rho - gamma * mu;
+      const double at0 = std::norm(tau0), ag = std::norm(gamma);
+      const Z den2 = lambda * at0 + ag;
+      if (den2 == Z(0.0)) st = 14;
+      else {
+        theta = ((1.0 - lambda) * at0) / den2;
+        kappa = -(gamma0 * std::conj(tau0) * kappa0) / den2;
+        lambda = (lambda * at0) / den2;
+      }
+    }
+    if (st) {
+      char msg[80];
+      std::snprintf(msg, sizeof(msg), "breakdown at step %d", st);
+      set_error(name, msg);
+      return 58;
+    }
+    // d = theta d + kappa p ; s = theta s + kappa ap ; x += d ; r -= s
+    c.lin(d, theta, p, kappa);
+    c.lin(s, theta, ap, kappa);
+    c.lin(xs, 1.0, d, 1.0);
+    c.lin(r, 1.0, s, -1.0);
+    resid = c.nrm(r) / bnorm;
+    CK(59);
+    if (io.verbose) std::printf(" QMRCCG iteration=%6d residual=%14.6E\n", it, resid);
+    if ((it % RELIABLE_PERIOD) == 0 || resid <= io.tol) {
+      double tres;
+      bool conv, rest;
+      rc = c.reliable("QMRCCG", io.b, xs, r, bnorm, resid, io.tol, tres, conv, rest);
+      if (rc) return rc == 1 ? 59 : rc;
+      if (conv) { resid = tres; break; }
+      if (rest) {
+        c.diff(io.sy, io.b, io.sy);
+        c.copy(r, io.sy);
+        c.zero(p); c.zero(ap); c.zero(q); c.zero(d); c.zero(s); c.zero(atw);
+        c.copy(vt, io.sy); c.copy(wt, io.sy);
+        if ((rc = init_scalars())) return rc;
+        resid = tres;
+      }
+    }
+  }
+  if (resid > io.tol) {
+    double tres;
+    bool conv, rest;
+    rc = c.reliable("QMRCCG", io.b, xs, r, bnorm, resid, io.tol, tres, conv, rest);
+    if (rc) return rc == 1 ? 60 : rc;
+    resid = tres;
+  }
+  c.copy(io.x, xs);
+  CK(61);
+  io.itno = it; io.tole = resid; io.ncompte = c.nc;
+  return 0;
+}
+
+// ---------------------------------------------------------------- PBCGST (cu:445-457, cu:1105-1165)
+template <typename T> int solve_pbcgst(SolveIO<T>& io) {
+  using C = cplx<T>;
+  const char* name = "PBCGST";
+  Ctx<T> c(io);
+  C *r = c.w(0), *rt = c.w(1), *p = c.w(2), *sv = c.w(3), *v = c.w(4), *t = c.w(5), *xs = c.w(6), *rtrue = c.w(7);
+  const Engine<T>& E = *io.eng;
+  auto precon = [&](C* dst, const C* src) { v_precon<T>(dst, src, io.adia, E.occ, E.g.nat, E.g.nat0, c.st()); };
+  c.copy(xs, io.x);
+  const double bnorm = c.nrm(io.b);
+  CK(72);
+  int total_it = 0, restart = 0;
+  double resid = 1.0;
+  bool converged = false;
+  while (total_it < io.maxit && !converged) {
+    if (restart > 0 && io.verbose) std::printf(" restart PBCGST CUDA: %d\n", restart);
+    MV(xs, io.sy, 73);
+    c.diff(rtrue, io.b, io.sy);
+    precon(r, rtrue);
+    c.copy(rt, r);
+    c.zero(p);
+    c.zero(v);
+    Z rho = 1.0, alpha = 1.0, omega = 1.0;
+    for (int local = 0; local < 5 && total_it < io.maxit && !converged; ++local) {
+      const Z new_rho = c.dotc(rt, r);
+      CK(74);
+      const Z kap = rho * omega;
+      if (kap == Z(0.0)) { set_error(name, "hard breakdown at step 6 (rho0*omega == 0)"); return 75; }
+      const Z beta = new_rho * alpha / kap;
+      rho = new_rho;
+      // p = r + beta (p - omega v)
+      c.lin(p, beta, v, -beta * omega);
+      c.lin(p, 1.0, r, 1.0);
+      MV(p, io.sy, 76);
+      precon(v, io.sy);
+      const Z xi = c.dotc(rt, v);
+      CK(77);
+      if (xi == Z(0.0)) { set_error(name, "hard breakdown at step 10 (rtilde^H v == 0)"); return 78; }
+      alpha = rho / xi;
+      c.copy(sv, r);
+      c.lin(sv, 1.0, v, -alpha);
+      const double snorm = c.nrm(sv);
+      CK(79);
+      if (snorm < 1.19209e-7) {  // PIM step 12 soft breakdown: accept x += alpha p, restart
+        c.lin(xs, 1.0, p, alpha);
+        ++total_it;
+        if (io.verbose) std::printf(" PBCGST CUDA soft breakdown: restarting from updated x at iteration %d\n", total_it);
+        break;
+      }
+      MV(sv, io.sy, 80);
+      precon(t, io.sy);
+      Z tt, ts;
+      {
+        const C* A2[2] = {t, t};
+        const C* B2[2] = {t, sv};
+        const int cj[2] = {1, 1};
+        double2 o[2];
+        if (io.ops->dots(c.n, 2, A2, B2, cj, o)) return 81;
+        tt = zd(o[0]);
+        ts = zd(o[1]);
+      }
+      if (tt == Z(0.0)) { set_error(name, "hard breakdown at step 14 (t^H t == 0)"); return 82; }
+      omega = ts / tt;
+      c.lin(xs, 1.0, p, alpha, sv, omega);
+      c.copy(r, sv);
+      c.lin(r, 1.0, t, -omega);
+      ++total_it;
+      MV(xs, io.sy, 84);
+      c.diff(rtrue, io.b, io.sy);
+      const double trn = c.nrm(rtrue);
+      CK(84);
+      resid = bnorm > 0.0 ? trn / bnorm : INFINITY;
+      if (io.verbose) std::printf(" PBCGST iteration=%6d residual=%14.6E\n", total_it, resid);
+      if (resid <= io.tol) converged = true;
+    }
+    ++restart;
+  }
+  if (!converged) {
+    MV(xs, io.sy, 85);
+    c.diff(rtrue, io.b, io.sy);
+    const double trn = c.nrm(rtrue);
+    CK(85);
+    resid = bnorm > 0.0 ? trn / bnorm : INFINITY;
+  }
+  c.copy(io.x, xs);
+  CK(86);
+  io.itno = total_it; io.tole = resid; io.ncompte = c.nc;
+  if (!converged) { set_error(name, "MAXIT reached before requested tolerance"); return 87; }
+  return 0;
+}
+
+// ---------------------------------------------------------------- PETRKP (cu:482-493, cu:1280-1357)
+template <typename T> int solve_petrkp(SolveIO<T>& io) {
+  using C = cplx<T>;
+  const char* name = "PETRKP";
+  Ctx<T> c(io);
+  C *ace = c.w(0), *gi = c.w(1), *pi = c.w(2), *qi = c.w(3), *axi = c.w(4), *rv = c.w(5), *xs = c.w(6);
+  c.copy(xs, io.x);
+  const double bb = c.dotc(io.b, io.b).real();
+  CK(112);
+  {
+    int rc = c.mv(io.b, io.sy, 1);  // ACE = A^H b
+    if (rc) return rc;
+  }
+  c.copy(ace, io.sy); c.copy(gi, io.sy); c.copy(pi, io.sy);
+  MV(pi, io.sy, 113);
+  c.copy(qi, io.sy);
+  double gg = c.dotc(gi, gi).real(), qq = c.dotc(qi, qi).real();
+  CK(114);
+  if (qq == 0.0) { set_error(name, "breakdown: ||QI|| == 0 while computing initial alpha"); return 115; }
+  double alpha = gg / qq;
+  c.lin(xs, 1.0, pi, alpha);
+  MV(xs, io.sy, 116);
+  c.copy(axi, io.sy);
+  double resid = 1.0;
+  int it;
+  for (it = 1; it <= io.maxit; ++it) {
+    const double oldgg = gg;
+    {
+      int rc = c.mv(axi, io.sy, 1);  // A^H A x
+      if (rc) return rc;
+    }
+    c.diff(gi, ace, io.sy);
+    gg = c.dotc(gi, gi).real();
+    CK(118);
+    if (oldgg == 0.0) { set_error(name, "breakdown: previous ||GI|| == 0 while computing beta"); return 119; }
+    const double beta = gg / oldgg;
+    c.lin(pi, beta, gi, 1.0);
+    MV(pi, io.sy, 120);
+    c.copy(qi, io.sy);
+    qq = c.dotc(qi, qi).real();
+    CK(120);
+    if (qq == 0.0) { set_error(name, "breakdown: ||QI|| == 0 while computing alpha"); return 121; }
+    alpha = gg / qq;
+    c.lin(xs, 1.0, pi, alpha);
+    if (it != 10 * (it / 10)) {
+      c.lin(axi, 1.0, qi, alpha);
+    } else {
+      MV(xs, io.sy, 122);
+      c.copy(axi, io.sy);
+    }
+    c.diff(rv, axi, io.b);
+    const double rr = c.dotc(rv, rv).real();
+    CK(123);
+    resid = bb > 0.0 ? std::sqrt(std::max(rr, 0.0) / bb) : INFINITY;
+    if (io.verbose) std::printf(" PETRKP iteration=%6d residual=%14.6E\n", it, resid);
+    if (resid < io.tol) break;
+  }
+  c.copy(io.x, xs);
+  CK(124);
+  io.itno = it <= io.maxit ? it : io.maxit; io.tole = resid; io.ncompte = c.nc;
+  return 0;
+}
+
+// ---------------------------------------------------------------- GPBICG (cu:420-432, cu:1031-1069)
+template <typename T> int solve_gpbicg(SolveIO<T>& io) {
+  using C = cplx<T>;
+  const char* name = "GPBICG";
+  Ctx<T> c(io);
+  C *r0 = c.w(0), *p = c.w(1), *r = c.w(2), *yv = c.w(3), *t = c.w(4), *ap = c.w(5), *at = c.w(6);
+  C *u = c.w(7), *wv = c.w(8), *zv = c.w(9), *xsol = c.w(10), *told = c.w(11), *tmp = c.w(12);
+  c.copy(xsol, io.x);
+  const double bnorm = c.nrm(io.b);
+  CK(32);
+  if (bnorm == 0.0) { set_error(name, "zero RHS norm"); return 32; }
+  MV(xsol, io.sy, 32);
+  c.diff(r0, io.b, io.sy);
+  c.copy(r, r0);
+  c.zero(p); c.zero(t); c.zero(u); c.zero(wv); c.zero(zv); c.zero(yv); c.zero(told);
+  Z r0rn = c.dotc(r0, r0), beta = 0.0, alpha = 0.0, dzeta = 0.0, eta = 0.0;
+  double resid = c.nrm(r) / bnorm;
+  CK(32);
+  int it = 0;
+  bool first = true;
+  while (it < io.maxit && resid > io.tol) {
+    ++it;
+    // p = r + beta (p - u)
+    c.lin(p, beta, u, -beta);
+    c.lin(p, 1.0, r, 1.0);
+    MV(p, io.sy, 33);
+    c.copy(ap, io.sy);
+    const Z g0 = c.dotc(r0, ap);
+    CK(34);
+    if (g0 == Z(0.0)) { set_error(name, "alpha breakdown"); return 34; }
+    alpha = r0rn / g0;
+    // y = (t - r) + alpha (ap - w) ; told = t ; t = r - alpha ap
+    c.copy(yv, t);
+    c.lin(yv, 1.0, r, -1.0);
+    c.lin(yv, 1.0, ap, alpha, wv, -alpha);
+    c.copy(told, t);
+    c.copy(t, r);
+    c.lin(t, 1.0, ap, -alpha);
+    MV(t, io.sy, 35);
+    c.copy(at, io.sy);
+    Z g1, g4;
+    {
+      const C* A2[2] = {at, at};
+      const C* B2[2] = {at, t};
+      const int cj[2] = {1, 1};
+      double2 o[2];
+      if (io.ops->dots(c.n, 2, A2, B2, cj, o)) return 35;
+      g1 = zd(o[0]);
+      g4 = zd(o[1]);
+    }
+    if (first) {
+      if (g1 == Z(0.0)) { set_error(name, "dzeta/eta breakdown"); return 36; }
+      eta = 0.0;
+      dzeta = g4 / g1;
+    } else {
+      const C* A3[3] = {yv, at, yv};
+      const C* B3[3] = {yv, yv, t};
+      const int cj[3] = {1, 1, 1};
+      double2 o[3];
+      if (io.ops->dots(c.n, 3, A3, B3, cj, o)) return 35;
+      const Z g2 = zd(o[0]), g3 = zd(o[1]), g5 = zd(o[2]);
+      const Z den = g1 * g2 - g3 * std::conj(g3);
+      if (den == Z(0.0)) { set_error(name, "dzeta/eta breakdown"); return 36; }
+      dzeta = (g2 * g4 - g5 * g3) / den;
+      eta = (g1 * g5 - std::conj(g3) * g4) / den;
+    }
+    // u = dz ap + eta (told - r + beta u) ; z = dz r + eta z - alpha u ; x += alpha p + z ; r = t - eta y - dz at
+    c.copy(tmp, told);
+    c.lin(tmp, 1.0, r, -1.0);
+    c.lin(tmp, 1.0, u, beta);
+    c.lin(u, 0.0, ap, dzeta, tmp, eta);
+    c.lin(zv, eta, r, dzeta, u, -alpha);
+    c.lin(xsol, 1.0, p, alpha, zv, 1.0);
+    c.copy(r, t);
+    c.lin(r, 1.0, yv, -eta, at, -dzeta);
+    resid = c.nrm(r) / bnorm;
+    CK(37);
+    if (io.verbose) std::printf(" GPBICG iteration=%6d residual=%14.6E\n", it, resid);
+    if ((it % RELIABLE_PERIOD) == 0 || resid <= io.tol) {
+      double tres;
+      bool conv, rest;
+      int rc = c.reliable("GPBICG", io.b, xsol, r, bnorm, resid, io.tol, tres, conv, rest);
+      if (rc) return rc == 1 ? 37 : rc;
+      if (conv) { resid = tres; break; }
+      if (rest) {
+        c.diff(io.sy, io.b, io.sy);
+        c.copy(r0, io.sy); c.copy(r, io.sy);
+        c.zero(p); c.zero(yv); c.zero(t); c.zero(ap); c.zero(at); c.zero(u); c.zero(wv); c.zero(zv); c.zero(told);
+        r0rn = c.dotc(r0, r0);
+        CK(37);
+        beta = 0.0;
+        first = true;
+        resid = tres;
+        continue;
+      }
+    }
+    const Z g0b = c.dotc(r0, r);
+    CK(39);
+    if (r0rn == Z(0.0) || dzeta == Z(0.0)) { set_error(name, "beta breakdown"); return 39; }
+    beta = (alpha * g0b / dzeta) / r0rn;
+    r0rn = g0b;
+    c.lin(wv, 0.0, at, 1.0, ap, beta);
+    first = false;
+  }
+  if (resid > io.tol) {
+    double tres;
+    bool conv, rest;
+    int rc = c.reliable("GPBICG", io.b, xsol, r, bnorm, resid, io.tol, tres, conv, rest);
+    if (rc) return rc == 1 ? 40 : rc;
+    resid = tres;
+  }
+  c.copy(io.x, xsol);
+  CK(40);
+  io.itno = it; io.tole = resid; io.ncompte = c.nc;
+  return 0;
+}
+
+// ---------------------------------------------------------------- BiCGStab(4) (cu:1363-1433)
+template <typename T> int solve_bicgstab4(SolveIO<T>& io) {
+  using C = cplx<T>;
+  const char* name = "BiCGStab4";
+  Ctx<T> c(io);
+  C* r[5] = {c.w(0), c.w(3), c.w(4), c.w(5), c.w(6)};
+  C* u[5] = {c.w(1), c.w(7), c.w(8), c.w(9), c.w(10)};
+  C* rtil = c.w(2);
+  C* x = io.x;
+  MV(x, io.sy, 132);
+  c.diff(r[0], io.b, io.sy);
+  const double bnorm = c.nrm(io.b);
+  double rnorm = c.nrm(r[0]);
+  CK(132);
+  if (bnorm == 0.0) { set_error(name, "zero RHS norm"); return 133; }
+  double resid = rnorm / bnorm;
+  if (resid <= io.tol) { io.itno = 0; io.tole = resid; io.ncompte = c.nc; return 0; }
+  if (rnorm < 1e-30) { set_error(name, "cannot start from zero residual"); return 133; }
+  c.lin(rtil, 0.0, r[0], 1.0 / rnorm);
+  c.zero(u[0]);
+  Z rho = 1.0, alpha = 0.0, omega = 1.0;
+  int it;
+  for (it = 1; it <= io.maxit; ++it) {
+    rho = -omega * rho;
+    for (int j = 0; j < 4; ++j) {
+      if (std::abs(rho) < 1e-30) { set_error(name, "breakdown: rho is zero"); return 135; }
+      const Z rho1 = c.dotc(rtil, r[j]);
+      CK(135);
+      const Z beta = alpha * rho1 / rho;
+      rho = rho1;
+      for (int i = 0; i <= j; ++i) c.lin(u[i], -beta, r[i], 1.0);
+      MV(u[j], u[j + 1], 136);
+      const Z den = c.dotc(rtil, u[j + 1]);
+      CK(137);
+      if (std::abs(den) < 1e-30) { set_error(name, "breakdown: <rtilde,u> is zero"); return 137; }
+      alpha = rho / den;
+      for (int i = 0; i <= j; ++i) c.lin(r[i], 1.0, u[i + 1], -alpha);
+      MV(r[j], r[j + 1], 138);
+      c.lin(x, 1.0, u[0], alpha);
+    }
+    Z tau[4][4], gp[5], gam[5], gpp[5];
+    double sigma[5] = {0, 0, 0, 0, 0};
+    for (auto& row : tau) for (auto& zz : row) zz = 0.0;
+    for (int i = 0; i < 5; ++i) gp[i] = gam[i] = gpp[i] = 0.0;
+    for (int j = 1; j <= 4; ++j) {
+      for (int i = 1; i < j; ++i) {
+        const Z dd = c.dotc(r[i], r[j]);
+        CK(140);
+        tau[j - 1][i - 1] = dd / sigma[i];
+        c.lin(r[j], 1.0, r[i], -tau[j - 1][i - 1]);
+      }
+      sigma[j] = c.dotc(r[j], r[j]).real();
+      CK(141);
+      if (!(sigma[j] > 1e-30)) { set_error(name, "breakdown in MR polynomial"); return 141; }
+      gp[j] = c.dotc(r[j], r[0]) / sigma[j];
+      CK(141);
+    }
+    omega = gam[4] = gp[4];
+    for (int j = 3; j >= 1; --j) {
+      gam[j] = gp[j];
+      for (int i = j + 1; i <= 4; ++i) gam[j] -= tau[i - 1][j - 1] * gam[i];
+    }
+    for (int j = 1; j < 4; ++j) {
+      gpp[j] = gam[j + 1];
+      for (int i = j + 1; i < 4; ++i) gpp[j] += tau[i - 1][j - 1] * gam[i + 1];
+    }
+    c.lin(x, 1.0, r[0], gam[1]);
+    c.lin(r[0], 1.0, r[4], -gp[4]);
+    c.lin(u[0], 1.0, u[4], -gam[4]);
+    for (int j = 1; j < 4; ++j) {
+      c.lin(x, 1.0, r[j], gpp[j]);
+      c.lin(r[0], 1.0, r[j], -gp[j]);
+      c.lin(u[0], 1.0, u[j], -gam[j]);
+    }
+    rnorm = c.nrm(r[0]);
+    CK(143);
+    resid = rnorm / bnorm;
+    if (io.verbose) std::printf(" BiCGStab(4) iteration=%6d residual=%14.6E\n", it, resid);
+    if ((it % RELIABLE_PERIOD) == 0 || resid <= io.tol) {
+      double tres;
+      bool conv, rest;
+      int rc = c.reliable("BiCGStab(4)", io.b, x, r[0], bnorm, resid, io.tol, tres, conv, rest);
+      if (rc) return rc == 1 ? 144 : rc;
+      if (conv) { resid = tres; break; }
+      if (rest) {
+        c.diff(r[0], io.b, io.sy);
+        rnorm = tres * bnorm;
+        if (!(rnorm > 0.0)) { set_error(name, "reliable restart produced zero residual"); return 144; }
+        c.lin(rtil, 0.0, r[0], 1.0 / rnorm);
+        c.zero(u[0]);
+        rho = 1.0; alpha = 0.0; omega = 1.0;
+        resid = tres;
+      }
+    }
+  }
+  MV(x, io.sy, 144);
+  c.diff(r[0], io.b, io.sy);
+  rnorm = c.nrm(r[0]);
+  CK(144);
+  resid = rnorm / bnorm;
+  io.itno = it <= io.maxit ? it : io.maxit; io.tole = resid; io.ncompte = c.nc;
+  return 0;
+}
+
+// Gaussian elimination with partial pivoting and the 1e-30 breakdown test of cu:349-359
+static bool solve_small(Z* a, Z* b, int n, int ld) {
+  for (int k = 0; k < n; ++k) {
+    int piv = k;
+    double best = std::abs(a[k * ld + k]);
+    for (int i = k + 1; i < n; ++i) {
+      const double v = std::abs(a[i * ld + k]);
+      if (v > best) { best = v; piv = i; }
+    }
+    if (best < 1e-30) return false;
+    if (piv != k) {
+      for (int j = k; j < n; ++j) std::swap(a[k * ld + j], a[piv * ld + j]);
+      std::swap(b[k], b[piv]);
+    }
+    for (int i = k + 1; i < n; ++i) {
+      const Z f = a[i * ld + k] / a[k * ld + k];
+      a[i * ld + k] = 0.0;
+      for (int j = k + 1; j < n; ++j) a[i * ld + j] -= f * a[k * ld + j];
+      b[i] -= f * b[k];
+    }
+  }
+  for (int i = n - 1; i >= 0; --i) {
+    Z v = b[i];
+    for (int j = i + 1; j < n; ++j) v -= a[i * ld + j] * b[j];
+    if (std::abs(a[i * ld + i]) < 1e-30) return false;
+    b[i] = v / a[i * ld + i];
+  }
+  return true;
+}
+
+// ---------------------------------------------------------------- GPBiCGStab(2) (cu:1435-1491)
+template <typename T> int solve_gpbicgstab2(SolveIO<T>& io) {
+  using C = cplx<T>;
+  const char* name = "GPBiCGStab2";
+  Ctx<T> c(io);
+  C *r0 = c.w(0), *p0 = c.w(1), *rt = c.w(2), *z = c.w(3), *yv = c.w(4), *u = c.w(5), *hs = c.w(6), *hq0 = c.w(7),
+    *hq1 = c.w(8), *work = c.w(9);
+  C* x = io.x;
+  MV(x, io.sy, 152);
+  c.diff(r0, io.b, io.sy);
+  const double bnorm = c.nrm(io.b);
+  double rnorm = c.nrm(r0);
+  CK(152);
+  if (bnorm == 0.0) { set_error(name, "zero RHS norm"); return 153; }
+  c.copy(rt, r0); c.copy(p0, r0); c.zero(z);
+  bool fresh = true;
+  double resid = rnorm / bnorm;
+  Z rho, sigma, alpha, beta;
+  int it;
+  for (it = 1; it <= io.maxit && resid > io.tol; ++it) {
+    if (fresh) {
+      rho = c.dotc(rt, r0);
+      MV(p0, work, 154);
+      sigma = c.dotc(rt, work);
+      CK(154);
+      if (std::abs(sigma) < 1e-30) { set_error("GP2", "sigma1 zero"); return 154; }
+      alpha = rho / sigma;
+      c.lin(x, 1.0, p0, alpha);
+      c.lin(r0, 1.0, work, -alpha);
+      MV(r0, hs, 155);
+      rho = c.dotc(rt, hs);
+      CK(155);
+      beta = rho / sigma;
+      c.lin(p0, -beta, r0, 1.0);
+      c.lin(work, -beta, hs, 1.0);
+      MV(work, hq1, 156);
+      sigma = c.dotc(rt, hq1);
+      CK(156);
+      if (std::abs(sigma) < 1e-30) { set_error("GP2", "sigma2 zero"); return 156; }
+      alpha = rho / sigma;
+      c.lin(x, 1.0, p0, alpha);
+      c.lin(r0, 1.0, work, -alpha);
+      c.lin(hs, 1.0, hq1, -alpha);
+      MV(hs, hq0, 157);
+      rho = c.dotc(rt, hq0);
+      CK(157);
+      beta = rho / sigma;
+      c.lin(p0, -beta, r0, 1.0);
+      c.lin(work, -beta, hs, 1.0);
+      c.lin(hq1, -beta, hq0, 1.0);
+      Z mat[3][3], rhs[3];
+      mat[0][0] = c.dotc(hs, hs); mat[0][1] = c.dotc(hs, hq0); mat[1][1] = c.dotc(hq0, hq0);
+      rhs[0] = c.dotc(hs, r0); rhs[1] = c.dotc(hq0, r0);
+      CK(159);
+      mat[1][0] = std::conj(mat[0][1]);
+      if (!solve_small(&mat[0][0], rhs, 2, 3)) { set_error("GP2", "initial 2x2 minimization breakdown"); return 159; }
+      const Z z1 = rhs[0], z2 = rhs[1];
+      c.lin(z, 0.0, r0, z1, hs, z2);
+      c.lin(x, 1.0, z, 1.0);
+      c.lin(yv, 0.0, hs, z1, hq0, z2);
+      c.lin(u, 0.0, work, z1, hq1, z2);
+      c.lin(r0, 1.0, yv, -1.0);
+      c.lin(p0, 1.0, u, -1.0);
+      c.copy(hq0, work);
+      fresh = false;
+    } else {
+      rho = c.dotc(rt, r0);
+      MV(p0, work, 161);
+      sigma = c.dotc(rt, work);
+      CK(161);
+      if (std::abs(sigma) < 1e-30) { set_error("GP2", "sigma1 zero"); return 161; }
+      alpha = rho / sigma;
+      c.lin(x, 1.0, p0, alpha);
+      c.lin(z, 1.0, u, -alpha);
+      c.lin(yv, 1.0, hq0, -alpha, work, alpha);
+      c.lin(r0, 1.0, work, -alpha);
+      c.lin(hs, 1.0, hq1, -alpha);
+      MV(r0, hq1, 162);
+      rho = c.dotc(rt, hq1);
+      CK(162);
+      beta = rho / sigma;
+      c.lin(p0, -beta, r0, 1.0);
+      c.lin(work, -beta, hq1, 1.0);
+      c.lin(hq0, -beta, hs, 1.0);
+      c.lin(u, -beta, yv, 1.0);
+      MV(work, hs, 163);
+      sigma = c.dotc(rt, hs);
+      CK(163);
+      if (std::abs(sigma) < 1e-30) { set_error("GP2", "sigma2 zero"); return 163; }
+      alpha = rho / sigma;
+      c.lin(x, 1.0, p0, alpha);
+      c.lin(z, 1.0, u, -alpha);
+      c.lin(yv, 1.0, hq0, -alpha, work, alpha);
+      c.lin(r0, 1.0, work, -alpha);
+      c.lin(hq1, 1.0, hs, -alpha);
+      MV(hq1, hq0, 164);
+      rho = c.dotc(rt, hq0);
+      CK(164);
+      beta = rho / sigma;
+      c.lin(p0, -beta, r0, 1.0);
+      c.lin(work, -beta, hq1, 1.0);
+      c.lin(hs, -beta, hq0, 1.0);
+      c.lin(u, -beta, yv, 1.0);
+      Z mat[3][3], rhs[3];
+      {
+        const C* A9[8] = {hq1, hq1, hq1, hq0, hq0, yv, hq1, hq0};
+        const C* B9[8] = {hq1, hq0, yv, hq0, yv, yv, r0, r0};
+        const int cj[8] = {1, 1, 1, 1, 1, 1, 1, 1};
+        double2 o[8];
+        if (io.ops->dots(c.n, 8, A9, B9, cj, o)) return 166;
+        mat[0][0] = zd(o[0]); mat[0][1] = zd(o[1]); mat[0][2] = zd(o[2]);
+        mat[1][1] = zd(o[3]); mat[1][2] = zd(o[4]); mat[2][2] = zd(o[5]);
+        rhs[0] = zd(o[6]); rhs[1] = zd(o[7]);
+        rhs[2] = c.dotc(yv, r0);
+        CK(166);
+      }
+      mat[1][0] = std::conj(mat[0][1]); mat[2][0] = std::conj(mat[0][2]); mat[2][1] = std::conj(mat[1][2]);
+      if (!solve_small(&mat[0][0], rhs, 3, 3)) { set_error("GP2", "3x3 minimization breakdown"); return 166; }
+      const Z z1 = rhs[0], z2 = rhs[1], eta = rhs[2];
+      c.lin(z, eta, r0, z1, hq1, z2);
+      c.lin(x, 1.0, z, 1.0);
+      c.lin(yv, eta, hq1, z1, hq0, z2);
+      c.lin(u, eta, work, z1, hs, z2);
+      c.lin(r0, 1.0, yv, -1.0);
+      c.lin(p0, 1.0, u, -1.0);
+      // restore fixed histories: hs=r1, hq0=p1, hq1=p2 (cu:1474)
+      c.copy(hq0, hs);
+      c.copy(hs, hq1);
+      c.copy(hq1, hq0);
+      c.copy(hq0, work);
+    }
+    rnorm = c.nrm(r0);
+    CK(169);
+    resid = rnorm / bnorm;
+    if (io.verbose) std::printf(" GPBiCGStab(2) iteration=%6d residual=%14.6E\n", it, resid);
+    if ((it % RELIABLE_PERIOD) == 0 || resid <= io.tol) {
+      double tres;
+      bool conv, rest;
+      int rc = c.reliable("GPBiCGStab(2)", io.b, x, r0, bnorm, resid, io.tol, tres, conv, rest);
+      if (rc) return rc == 1 ? 170 : rc;
+      if (conv) { resid = tres; break; }
+      if (rest) {
+        c.diff(r0, io.b, io.sy);
+        c.copy(rt, r0); c.copy(p0, r0); c.zero(z);
+        fresh = true;
+        resid = tres;
+      }
+    }
+  }
+  if (resid > io.tol) {
+    MV(x, io.sy, 172);
+    c.diff(r0, io.b, io.sy);
+    rnorm = c.nrm(r0);
+    CK(172);
+    resid = rnorm / bnorm;
+  }
+  io.itno = it <= io.maxit ? it : io.maxit; io.tole = resid; io.ncompte = c.nc;
+  return 0;
+}
+
+// ---------------------------------------------------------------- GPBiCGStab(4) (cu:1493-1570)
+template <typename T> int solve_gpbicgstab4(SolveIO<T>& io) {
+  using C = cplx<T>;
+  const char* name = "GPBiCGStab4";
+  Ctx<T> c(io);
+  C *r0 = c.w(0), *p0 = c.w(1), *rt = c.w(2), *z = c.w(3), *yv = c.w(4), *u = c.w(5);
+  C* hs[3] = {c.w(6), c.w(7), c.w(8)};
+  C* hq[4] = {c.w(9), c.w(10), c.w(11), c.w(12)};
+  C* work = io.sy;  // the MATVEC staging vector doubles as `work`, as in the reference
+  C* x = io.x;
+  MV(x, io.sy, 182);
+  c.diff(r0, io.b, io.sy);
+  const double bnorm = c.nrm(io.b);
+  double rnorm = c.nrm(r0);
+  CK(182);
+  if (bnorm == 0.0) { set_error("GP4", "zero RHS norm"); return 183; }
+  c.copy(rt, r0); c.copy(p0, r0); c.zero(z);
+  bool fresh = true;
+  double resid = rnorm / bnorm;
+  Z rho, sigma, alpha, beta, zeta[4], eta;
+  auto restore = [&]() {
+    c.copy(hq[0], hs[0]); c.copy(hs[0], hq[3]); c.copy(hq[3], hq[0]);
+    c.copy(hq[0], hs[1]); c.copy(hs[1], hq[2]); c.copy(hq[2], hq[0]);
+    c.copy(hq[0], hs[2]); c.copy(hs[2], hq[1]); c.copy(hq[1], hq[0]); c.copy(hq[0], work);
+  };
+  auto gram = [&](C* const* rr, int with_y, Z* mat, Z* rhs, int ld) -> int {
+    for (int i = 0; i < 4; ++i) {
+      for (int j = 0; j < 4; ++j) mat[i * ld + j] = c.dotc(rr[i + 1], rr[j + 1]);
+      if (with_y) {
+        mat[i * ld + 4] = c.dotc(rr[i + 1], yv);
+        mat[4 * ld + i] = std::conj(mat[i * ld + 4]);
+      }
+      rhs[i] = c.dotc(rr[i + 1], rr[0]);
+    }
+    if (with_y) {
+      mat[4 * ld + 4] = c.dotc(yv, yv);
+      rhs[4] = c.dotc(yv, rr[0]);
+    }
+    return c.err;
+  };
+  int it;
+  for (it = 1; it <= io.maxit && resid > io.tol; ++it) {
+    if (fresh) {
+      C* rr[5] = {r0, hq[3], hq[2], hq[1], hq[0]};
+      C* pp[5] = {p0, work, hs[2], hs[1], hs[0]};
+      rho = c.dotc(rt, rr[0]);
+      CK(184);
+      for (int j = 1; j <= 4; ++j) {
+        MV(pp[j - 1], pp[j], 184);
+        sigma = c.dotc(rt, pp[j]);
+        CK(184);
+        if (std::abs(sigma) < 1e-30) { set_error("GP4", "initial sigma zero"); return 184; }
+        alpha = rho / sigma;
+        c.lin(x, 1.0, pp[0], alpha);
+        for (int i = 0; i < j; ++i) c.lin(rr[i], 1.0, pp[i + 1], -alpha);
+        MV(rr[j - 1], rr[j], 185);
+        rho = c.dotc(rt, rr[j]);
+        CK(185);
+        beta = rho / sigma;
+        for (int i = 0; i <= j; ++i) c.lin(pp[i], -beta, rr[i], 1.0);
+      }
+      Z mat[5][5], rhs[5];
+      for (auto& row : mat) for (auto& v : row) v = 0.0;
+      for (auto& v : rhs) v = 0.0;
+      if (gram(rr, 0, &mat[0][0], rhs, 5)) return 187;
+      if (!solve_small(&mat[0][0], rhs, 4, 5)) { set_error("GP4", "initial 4x4 minimization breakdown"); return 187; }
+      for (int i = 0; i < 4; ++i) zeta[i] = rhs[i];
+      c.lin(z, 0.0, rr[0], zeta[0]);
+      for (int i = 1; i < 4; ++i) c.lin(z, 1.0, rr[i], zeta[i]);
+      c.lin(x, 1.0, z, 1.0);
+      c.lin(yv, 0.0, rr[1], zeta[0]);
+      c.lin(u, 0.0, pp[1], zeta[0]);
+      for (int i = 1; i < 4; ++i) { c.lin(yv, 1.0, rr[i + 1], zeta[i]); c.lin(u, 1.0, pp[i + 1], zeta[i]); }
+      c.lin(r0, 1.0, yv, -1.0);
+      c.lin(p0, 1.0, u, -1.0);
+      restore();
+      fresh = false;
+    } else {
+      rho = c.dotc(rt, r0);
+      // j = 1
+      MV(p0, work, 190);
+      sigma = c.dotc(rt, work);
+      CK(190);
+      if (std::abs(sigma) < 1e-30) { set_error("GP4", "sigma1 zero"); return 190; }
+      alpha = rho / sigma;
+      c.lin(x, 1.0, p0, alpha); c.lin(z, 1.0, u, -alpha); c.lin(yv, 1.0, hq[0], -alpha, work, alpha);
+      c.lin(r0, 1.0, work, -alpha);
+      for (int i = 0; i < 3; ++i) c.lin(hs[i], 1.0, hq[i + 1], -alpha);
+      MV(r0, hq[3], 191);
+      rho = c.dotc(rt, hq[3]);
+      CK(191);
+      beta = rho / sigma;
+      c.lin(p0, -beta, r0, 1.0); c.lin(work, -beta, hq[3], 1.0);
+      for (int i = 0; i < 3; ++i) c.lin(hq[i], -beta, hs[i], 1.0);
+      c.lin(u, -beta, yv, 1.0);
+      // j = 2
+      MV(work, hs[2], 193);
+      sigma = c.dotc(rt, hs[2]);
+      CK(193);
+      if (std::abs(sigma) < 1e-30) { set_error("GP4", "sigma2 zero"); return 193; }
+      alpha = rho / sigma;
+      c.lin(x, 1.0, p0, alpha); c.lin(z, 1.0, u, -alpha); c.lin(yv, 1.0, hq[0], -alpha, work, alpha);
+      c.lin(r0, 1.0, work, -alpha); c.lin(hq[3], 1.0, hs[2], -alpha);
+      for (int i = 0; i < 2; ++i) c.lin(hs[i], 1.0, hq[i + 1], -alpha);
+      MV(hq[3], hq[2], 194);
+      rho = c.dotc(rt, hq[2]);
+      CK(194);
+      beta = rho / sigma;
+      c.lin(p0, -beta, r0, 1.0); c.lin(work, -beta, hq[3], 1.0); c.lin(hs[2], -beta, hq[2], 1.0);
+      for (int i = 0; i < 2; ++i) c.lin(hq[i], -beta, hs[i], 1.0);
+      c.lin(u, -beta, yv, 1.0);
+      // j = 3
+      MV(hs[2], hs[1], 196);
+      sigma = c.dotc(rt, hs[1]);
+      CK(196);
+      if (std::abs(sigma) < 1e-30) { set_error("GP4", "sigma3 zero"); return 196; }
+      alpha = rho / sigma;
+      c.lin(x, 1.0, p0, alpha); c.lin(z, 1.0, u, -alpha); c.lin(yv, 1.0, hq[0], -alpha, work, alpha);
+      c.lin(r0, 1.0, work, -alpha); c.lin(hq[3], 1.0, hs[2], -alpha); c.lin(hq[2], 1.0, hs[1], -alpha);
+      c.lin(hs[0], 1.0, hq[1], -alpha);
+      MV(hq[2], hq[1], 197);
+      rho = c.dotc(rt, hq[1]);
+      CK(197);
+      beta = rho / sigma;
+      c.lin(p0, -beta, r0, 1.0); c.lin(work, -beta, hq[3], 1.0); c.lin(hs[2], -beta, hq[2], 1.0);
+      c.lin(hs[1], -beta, hq[1], 1.0); c.lin(hq[0], -beta, hs[0], 1.0); c.lin(u, -beta, yv, 1.0);
+      // j = 4
+      MV(hs[1], hs[0], 199);
+      sigma = c.dotc(rt, hs[0]);
+      CK(199);
+      if (std::abs(sigma) < 1e-30) { set_error("GP4", "sigma4 zero"); return 199; }
+      alpha = rho / sigma;
+      c.lin(x, 1.0, p0, alpha); c.lin(z, 1.0, u, -alpha); c.lin(yv, 1.0, hq[0], -alpha, work, alpha);
+      c.lin(r0, 1.0, work, -alpha); c.lin(hq[3], 1.0, hs[2], -alpha); c.lin(hq[2], 1.0, hs[1], -alpha);
+      c.lin(hq[1], 1.0, hs[0], -alpha);
+      MV(hq[1], hq[0], 200);
+      rho = c.dotc(rt, hq[0]);
+      CK(200);
+      beta = rho / sigma;
+      c.lin(p0, -beta, r0, 1.0); c.lin(work, -beta, hq[3], 1.0); c.lin(hs[2], -beta, hq[2], 1.0);
+      c.lin(hs[1], -beta, hq[1], 1.0); c.lin(hs[0], -beta, hq[0], 1.0); c.lin(u, -beta, yv, 1.0);
+      C* rr[5] = {r0, hq[3], hq[2], hq[1], hq[0]};
+      C* pp[5] = {p0, work, hs[2], hs[1], hs[0]};
+      Z mat[5][5], rhs[5];
+      for (auto& row : mat) for (auto& v : row) v = 0.0;
+      for (auto& v : rhs) v = 0.0;
+      if (gram(rr, 1, &mat[0][0], rhs, 5)) return 202;
+      if (!solve_small(&mat[0][0], rhs, 5, 5)) { set_error("GP4", "5x5 minimization breakdown"); return 202; }
+      for (int i = 0; i < 4; ++i) zeta[i] = rhs[i];
+      eta = rhs[4];
+      c.lin(z, eta);
+      for (int i = 0; i < 4; ++i) c.lin(z, 1.0, rr[i], zeta[i]);
+      c.lin(x, 1.0, z, 1.0);
+      c.lin(yv, eta);
+      c.lin(u, eta);
+      for (int i = 0; i < 4; ++i) { c.lin(yv, 1.0, rr[i + 1], zeta[i]); c.lin(u, 1.0, pp[i + 1], zeta[i]); }
+      c.lin(r0, 1.0, yv, -1.0);
+      c.lin(p0, 1.0, u, -1.0);
+      restore();
+    }
+    rnorm = c.nrm(r0);
+    CK(205);
+    resid = rnorm / bnorm;
+    if (io.verbose) std::printf(" GPBiCGStab(4) iteration=%6d residual=%14.6E\n", it, resid);
+    if ((it % RELIABLE_PERIOD) == 0 || resid <= io.tol) {
+      double tres;
+      bool conv, rest;
+      int rc = c.reliable("GPBiCGStab(4)", io.b, x, r0, bnorm, resid, io.tol, tres, conv, rest);
+      if (rc) return rc == 1 ? 206 : rc;
+      if (conv) { resid = tres; break; }
+      if (rest) {
+        c.diff(r0, io.b, io.sy);
+        c.copy(rt, r0); c.copy(p0, r0); c.zero(z);
+        fresh = true;
+        resid = tres;
+      } else {
+        c.copy(work, hq[0]);  // the check overwrote `work` (the MATVEC staging vector)
+      }
+    }
+  }
+  MV(x, io.sy, 206);
+  c.diff(r0, io.b, io.sy);
+  rnorm = c.nrm(r0);
+  CK(206);
+  resid = rnorm / bnorm;
+  io.itno = it <= io.maxit ? it : io.maxit; io.tole = resid; io.ncompte = c.nc;
+  return 0;
+}
+
+#define DDB_SOLVERS(T)                                   \
+  template int solve_pbcgs2<T>(SolveIO<T>&);             \
+  template int solve_qmrccg<T>(SolveIO<T>&);             \
+  template int solve_pbcgst<T>(SolveIO<T>&);             \
+  template int solve_petrkp<T>(SolveIO<T>&);             \
+  template int solve_gpbicg<T>(SolveIO<T>&);             \
+  template int solve_bicgstab4<T>(SolveIO<T>&);          \
+  template int solve_gpbicgstab2<T>(SolveIO<T>&);        \
+  template int solve_gpbicgstab4<T>(SolveIO<T>&);
+DDB_SOLVERS(float)
+DDB_SOLVERS(double)
+#undef DDB_SOLVERS
+
+}  // namespace ddb

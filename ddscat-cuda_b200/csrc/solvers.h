@@ -1,0 +1,49 @@
+// Solver interface shared by the C ABI and the solver implementations.
+#pragma once
+#include "engine.h"
+
+namespace ddb {
+
+template <typename T> struct SolveIO {
+  Engine<T>* eng = nullptr;
+  VecOps<T>* ops = nullptr;
+  cudaStream_t stream = 0;
+  int n = 0;                        // 3*NAT0
+  const cplx<T>* b = nullptr;       // compact right-hand side
+  cplx<T>* x = nullptr;             // compact: initial guess in, solution out
+  const cplx<T>* adia = nullptr;    // CXADIA (layout a_full)
+  const cplx<T>* aoff = nullptr;    // CXAOFF or null
+  int a_full = 1;
+  cplx<T>* work = nullptr;          // 13*n scratch
+  cplx<T>* sy = nullptr;            // n: MATVEC output staging
+  int maxit = 0;
+  double tol = 0.0;
+  int verbose = 0;
+  int itno = 0;
+  double tole = 0.0;
+  int ncompte = 0;
+};
+
+template <typename T> int solve_pbcgs2(SolveIO<T>& io);
+template <typename T> int solve_qmrccg(SolveIO<T>& io);
+template <typename T> int solve_pbcgst(SolveIO<T>& io);
+template <typename T> int solve_petrkp(SolveIO<T>& io);
+template <typename T> int solve_gpbicg(SolveIO<T>& io);
+template <typename T> int solve_bicgstab4(SolveIO<T>& io);
+template <typename T> int solve_gpbicgstab2(SolveIO<T>& io);
+template <typename T> int solve_gpbicgstab4(SolveIO<T>& io);
+
+// post-processing (post.cu)
+template <typename T>
+int evalq_compute(Engine<T>& eng, VecOps<T>& ops, const cplx<T>* e, const cplx<T>* p, const cplx<T>* adia,
+                  const cplx<T>* aoff, int a_full, cplx<T>* qbuf, double ak3, double2* zabs, double2* zep);
+
+struct FarDir {
+  double k[3];
+};
+// S[d][c] = sum_j P_c(j) exp(-i k_d . r_j), r_j = ((i+1)+x0)*dx; FP64 sums.
+template <typename T>
+int farfield_sums(Engine<T>& eng, const cplx<T>* p, const float* dirs_host, int ndir, const float dx[3], const float x0[3],
+                  double2* sums_host, cudaStream_t s);
+
+}  // namespace ddb

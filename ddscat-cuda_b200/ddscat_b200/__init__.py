@@ -1,0 +1,201 @@
+"""Thin ctypes binding of the B200 DDA library (used by tests and bench).
+
+It calls the C ABI declared in ``include/ddscat_matvec_cuda.h`` and
+``include/ddscat_b200.h`` with host NumPy arrays, the same way the DDSCAT
+Fortran bridge does (``ddscat_cuda_unified/fortran/cuda_matvec_bridge.f90``):
+full-grid component-major complex64 vectors of length 3*NAT.  There is no CPU
+fallback: if the CUDA library is not built, :func:`load` raises.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+ROOT_DIR = os.path.dirname(PKG_DIR)
+LIB_DIR = os.path.join(ROOT_DIR, "lib")
+LIB_NAMES = {"fft3d": "libddscat_matvec_cuda.so", "slices": "libddscat_matvec_cuda_slice.so"}
+
+SOLVERS = ("gpbicg", "qmrccg", "pbcgst", "pbcgs2", "petrkp", "bicgstab4", "gpbicgstab2", "gpbicgstab4")
+
+# every symbol the C headers declare (checked by the CPU test suite)
+EXPORTS = (
+    ["ddscat_cuda_prepare_green_f32", "ddscat_cuda_prepare_f32", "ddscat_cuda_apply_f32"]
+    + [f"ddscat_cuda_solve_{s}_f32" for s in SOLVERS]
+    + ["ddscat_cuda_evalq_f32", "ddscat_cuda_scat_f32", "ddscat_cuda_release", "ddscat_cuda_last_error"]
+    + ["ddscat_b200_set_verbose", "ddscat_b200_layout"]
+)
+
+
+class DDSCATError(RuntimeError):
+    def __init__(self, where, code, msg):
+        super().__init__(f"{where} failed with status {code}: {msg}")
+        self.code = code
+        self.msg = msg
+
+
+def lib_path(layout="fft3d"):
+    return os.path.join(LIB_DIR, LIB_NAMES[layout])
+
+
+_P = ct.c_void_p
+_I = ct.c_int
+_F = ct.c_float
+_D = ct.POINTER(ct.c_double)
+
+
+def _declare(lib):
+    f = lib.ddscat_cuda_prepare_green_f32
+    f.argtypes = [_I] * 7 + [_F] * 9 + [_P]
+    f.restype = _I
+    f = lib.ddscat_cuda_prepare_f32
+    f.argtypes = [_I] * 6 + [_P, _P]
+    f.restype = _I
+    f = lib.ddscat_cuda_apply_f32
+    f.argtypes = [_I, _P, _P, _P, _P]
+    f.restype = _I
+    for s in SOLVERS:
+        f = getattr(lib, f"ddscat_cuda_solve_{s}_f32")
+        f.argtypes = [_P, _P, _P, _P, _I, _I, _F, ct.POINTER(_I), ct.POINTER(_F), ct.POINTER(_I)]
+        f.restype = _I
+    f = lib.ddscat_cuda_evalq_f32
+    f.argtypes = [_I, _P, _P, _P, _P, _F, _F, _F, _F, _D, _D, _D]
+    f.restype = _I
+    f = lib.ddscat_cuda_scat_f32
+    f.argtypes = [_I, _I, _P, _P, _P, _P, _P, _F, _F, _P, _P, _D, _D, _D, _D, ct.POINTER(_I), _P, _P]
+    f.restype = _I
+    lib.ddscat_cuda_release.argtypes = []
+    lib.ddscat_cuda_release.restype = _I
+    lib.ddscat_cuda_last_error.argtypes = []
+    lib.ddscat_cuda_last_error.restype = ct.c_char_p
+    lib.ddscat_b200_set_verbose.argtypes = [_I]
+    lib.ddscat_b200_set_verbose.restype = _I
+    lib.ddscat_b200_layout.argtypes = []
+    lib.ddscat_b200_layout.restype = _I
+
+
+_LIBS = {}
+
+
+def load(layout="fft3d"):
+    """Load (once) the built library for ``layout`` ('fft3d' or 'slices')."""
+    if layout in _LIBS:
+        return _LIBS[layout]
+    path = lib_path(layout)
+    if not os.path.exists(path):
+        raise OSError(f"B200 DDA library not built: {path} is missing (run `make -C ddscat-cuda_b200`)")
+    lib = ct.CDLL(path, mode=ct.RTLD_LOCAL)
+    _declare(lib)
+    _LIBS[layout] = lib
+    return lib
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ct.c_void_p) if a is not None else None
+
+
+def _c64(a, n=None):
+    a = np.ascontiguousarray(np.asarray(a), dtype=np.complex64)
+    if n is not None and a.size != n:
+        raise ValueError(f"expected {n} elements, got {a.size}")
+    return a
+
+
+@dataclass
+class SolveOut:
+    rc: int
+    x: np.ndarray
+    itno: int
+    tole: float
+    ncompte: int
+
+
+class DDA:
+    """One prepared target on the current CUDA device (the library keeps a
+    single global state, like the reference)."""
+
+    def __init__(self, layout="fft3d"):
+        self.lib = load(layout)
+        self.layout = layout
+        self.nat = self.nat0 = 0
+
+    def _err(self):
+        return self.lib.ddscat_cuda_last_error().decode(errors="replace")
+
+    def _check(self, where, rc):
+        if rc != 0:
+            raise DDSCATError(where, rc, self._err())
+
+    def prepare_green(self, nx, ny, nz, iocc, ak, dx=(1.0, 1.0, 1.0), ipbc=0, idipint=0, gamma=0.0, pyd=0.0, pzd=0.0,
+                      nat=None, nat0=None):
+        iocc = np.ascontiguousarray(np.asarray(iocc), dtype=np.int16)
+        self.nat = nx * ny * nz if nat is None else nat
+        self.nat0 = int(np.count_nonzero(iocc)) if nat0 is None else nat0
+        rc = self.lib.ddscat_cuda_prepare_green_f32(nx, ny, nz, ipbc, self.nat, self.nat0, idipint, gamma, pyd, pzd,
+                                                    float(ak[0]), float(ak[1]), float(ak[2]), float(dx[0]),
+                                                    float(dx[1]), float(dx[2]), _ptr(iocc))
+        self._check("prepare_green", rc)
+        return rc
+
+    def prepare(self, nx, ny, nz, iocc, green, ipbc=0):
+        iocc = np.ascontiguousarray(np.asarray(iocc), dtype=np.int16)
+        self.nat = nx * ny * nz
+        self.nat0 = int(np.count_nonzero(iocc))
+        g = _c64(green)
+        rc = self.lib.ddscat_cuda_prepare_f32(nx, ny, nz, ipbc, self.nat, self.nat0, _ptr(g), _ptr(iocc))
+        self._check("prepare", rc)
+        return rc
+
+    def apply(self, x, adia, aoff, cwhat="N"):
+        n = 3 * self.nat
+        x, adia, aoff = _c64(x, n), _c64(adia, n), _c64(aoff, n)
+        y = np.empty(n, dtype=np.complex64)
+        rc = self.lib.ddscat_cuda_apply_f32(ord(cwhat), _ptr(x), _ptr(y), _ptr(adia), _ptr(aoff))
+        self._check("apply", rc)
+        return y
+
+    def solve(self, name, b, adia, aoff, x0=None, maxit=300, tol=1e-5, check=True):
+        n = 3 * self.nat
+        b, adia, aoff = _c64(b, n), _c64(adia, n), _c64(aoff, n)
+        x = np.zeros(n, dtype=np.complex64) if x0 is None else _c64(x0, n).copy()
+        it, tole, nc = _I(0), _F(0.0), _I(0)
+        fn = getattr(self.lib, f"ddscat_cuda_solve_{name}_f32")
+        rc = fn(_ptr(b), _ptr(x), _ptr(adia), _ptr(aoff), n, maxit, tol, ct.byref(it), ct.byref(tole), ct.byref(nc))
+        if check:
+            self._check(name, rc)
+        return SolveOut(rc, x, it.value, float(tole.value), nc.value)
+
+    def evalq(self, ak, e02=1.0, use_resident=1, e=None, p=None, adia=None, aoff=None):
+        cabs, cext, cpha = ct.c_double(), ct.c_double(), ct.c_double()
+        arrs = [None if a is None else _c64(a) for a in (e, p, adia, aoff)]
+        rc = self.lib.ddscat_cuda_evalq_f32(use_resident, *[_ptr(a) for a in arrs], float(ak[0]), float(ak[1]),
+                                            float(ak[2]), e02, ct.byref(cabs), ct.byref(cext), ct.byref(cpha))
+        self._check("evalq", rc)
+        return cabs.value, cext.value, cpha.value
+
+    def scat(self, ak, e01, x0, dx=(1.0, 1.0, 1.0), etasca=0.5, e02=1.0, jpbc=0, aks=None, em1=None, em2=None):
+        akf = np.ascontiguousarray(ak, dtype=np.float32)
+        dxf = np.ascontiguousarray(dx, dtype=np.float32)
+        x0f = np.ascontiguousarray(x0, dtype=np.float32)
+        e01c = _c64(e01, 3)
+        ndir = 0 if aks is None else int(np.asarray(aks).size // 3)
+        aksf = None if aks is None else np.ascontiguousarray(aks, dtype=np.float32).reshape(-1)
+        em1f = None if em1 is None else np.ascontiguousarray(em1, dtype=np.float32).reshape(-1)
+        em2f = None if em2 is None else np.ascontiguousarray(em2, dtype=np.float32).reshape(-1)
+        f1 = np.zeros(max(ndir, 1), dtype=np.complex64)
+        f2 = np.zeros(max(ndir, 1), dtype=np.complex64)
+        cb, cs, cg2 = ct.c_double(), ct.c_double(), ct.c_double()
+        cg = (ct.c_double * 3)()
+        navg = _I(0)
+        rc = self.lib.ddscat_cuda_scat_f32(jpbc, ndir, _ptr(akf), _ptr(aksf), _ptr(dxf), _ptr(em1f), _ptr(em2f), e02,
+                                           etasca, _ptr(e01c), _ptr(x0f), ct.byref(cb), ct.byref(cs),
+                                           ct.cast(cg, _D), ct.byref(cg2), ct.byref(navg), _ptr(f1), _ptr(f2))
+        self._check("scat", rc)
+        return {"cbksca": cb.value, "csca": cs.value, "cscag": [cg[0], cg[1], cg[2]], "cscag2": cg2.value,
+                "navg": navg.value, "f1": f1[:ndir], "f2": f2[:ndir]}
+
+    def release(self):
+        return self.lib.ddscat_cuda_release()

@@ -1,0 +1,157 @@
+"""Seeded synthetic DDA problems (harness code, not the solve path).
+
+The reference takes the target occupancy (TARELL), the incident field (EVALE)
+and the polarisabilities (ALPHADIAG/EVALA) from upstream DDSCAT routines that
+are not part of it.  This module restates them from published formulas so
+tests and the benchmark can build inputs with the shapes of the DDSCAT
+configurations:
+
+* occupancy: site (i,j,k) is occupied iff sum_a ((i_a + 1/2 - n_a/2)/r_a)^2 <= 1
+  (r_a = semi-axes in lattice units);
+* lattice-dispersion-relation polarisability (Draine & Goodman 1993, ApJ 405,
+  685): alpha = alpha_CM / (1 + (alpha_CM/d^3) [(b1 + m^2 b2 + m^2 b3 S)(kd)^2
+  - (2/3) i (kd)^3]), b1=-1.891531, b2=0.1648469, b3=-1.7700004,
+  S = sum_j (a_j e_j)^2, alpha_CM = (3/4pi)(m^2-1)/(m^2+2); CXADIA = 1/alpha;
+* incident field E_j = e0 exp(i k.r_j), r_j = ((i+1)+x0)*d, x0 = -(n+1)/2
+  (target centred at the origin).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+B1, B2, B3 = -1.891531, 0.1648469, -1.7700004
+
+
+def ellipsoid_occupancy(nx, ny, nz, semi=None):
+    """int16 IOCC of length nx*ny*nz (component order j = ix + nx*(iy + ny*iz))."""
+    if semi is None:
+        semi = (nx / 2.0, ny / 2.0, nz / 2.0)
+    ix = (np.arange(nx) + 0.5 - nx / 2.0) / semi[0]
+    iy = (np.arange(ny) + 0.5 - ny / 2.0) / semi[1]
+    iz = (np.arange(nz) + 0.5 - nz / 2.0) / semi[2]
+    r2 = iz[:, None, None] ** 2 + iy[None, :, None] ** 2 + ix[None, None, :] ** 2
+    return (r2 <= 1.0).astype(np.int16).reshape(-1)
+
+
+def ldr_alpha(m, kd, khat, ehat):
+    """LDR polarisability (lattice units d=1) for refractive index m."""
+    eps = complex(m) ** 2
+    acm = (3.0 / (4.0 * math.pi)) * (eps - 1.0) / (eps + 2.0)
+    S = float(np.sum((np.asarray(khat) * np.real(np.asarray(ehat))) ** 2))
+    corr = (B1 + eps * B2 + eps * B3 * S) * kd ** 2 - (2.0 / 3.0) * 1j * kd ** 3
+    return acm / (1.0 + acm * corr)
+
+
+def euler_rotation(beta, theta, phi):
+    """Rotation R = Rz(phi) Ry(theta) Rz(beta) (ZYZ Euler angles)."""
+    def rz(a):
+        c, s = math.cos(a), math.sin(a)
+        return np.array([[c, -s, 0.0], [s, c, 0.0], [0.0, 0.0, 1.0]])
+
+    def ry(a):
+        c, s = math.cos(a), math.sin(a)
+        return np.array([[c, 0.0, s], [0.0, 1.0, 0.0], [-s, 0.0, c]])
+
+    return rz(phi) @ ry(theta) @ rz(beta)
+
+
+def random_orientations(count, seed=0):
+    """Euler angles uniform on SO(3): beta, phi ~ U[0,2pi), cos(theta) ~ U[-1,1]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        beta = rng.uniform(0.0, 2.0 * math.pi)
+        ct = rng.uniform(-1.0, 1.0)
+        phi = rng.uniform(0.0, 2.0 * math.pi)
+        out.append((beta, math.acos(ct), phi))
+    return out
+
+
+@dataclass
+class Incidence:
+    """One right-hand side: wave vector k (lattice units) and polarisation e."""
+    k: np.ndarray
+    e: np.ndarray
+
+
+@dataclass
+class Problem:
+    nx: int
+    ny: int
+    nz: int
+    iocc: np.ndarray
+    m: complex
+    kd: float
+    aeff: float
+    x0: tuple
+    incid: list = field(default_factory=list)
+
+    @property
+    def nat(self):
+        return self.nx * self.ny * self.nz
+
+    @property
+    def nat0(self):
+        return int(np.count_nonzero(self.iocc))
+
+    @property
+    def occ(self):
+        return np.flatnonzero(self.iocc)
+
+    def positions(self):
+        j = np.arange(self.nat)
+        ix, iy, iz = j % self.nx, (j // self.nx) % self.ny, j // (self.nx * self.ny)
+        return np.stack([ix + 1 + self.x0[0], iy + 1 + self.x0[1], iz + 1 + self.x0[2]], axis=1)
+
+    def rhs(self, r):
+        """Full complex64 b (3*NAT) for right-hand side r, zero on vacuum sites."""
+        inc = self.incid[r]
+        ph = np.exp(1j * (self.positions() @ inc.k))
+        b = (inc.e[:, None] * ph[None, :]) * (self.iocc != 0)[None, :]
+        return b.reshape(-1).astype(np.complex64)
+
+    def adia(self, r, m=None):
+        """Full CXADIA (3*NAT) for right-hand side r (uniform 1/alpha, homogeneous)."""
+        inc = self.incid[r]
+        khat = inc.k / np.linalg.norm(inc.k)
+        a = ldr_alpha(self.m if m is None else m, self.kd, khat, inc.e)
+        return np.full(3 * self.nat, 1.0 / a, dtype=np.complex64)
+
+    def aoff(self):
+        return np.zeros(3 * self.nat, dtype=np.complex64)
+
+
+def make_problem(nx, ny=None, nz=None, m=1.5 + 0.01j, x=5.0, semi=None, orientations=None, iocc=None):
+    """Ellipsoid (sphere by default) of size parameter x = k*aeff; one RHS per
+    (orientation, polarisation) with k along x before rotation and
+    polarisations y and z."""
+    ny = nx if ny is None else ny
+    nz = nx if nz is None else nz
+    if iocc is None:
+        iocc = ellipsoid_occupancy(nx, ny, nz, semi)
+    nat0 = int(np.count_nonzero(iocc))
+    aeff = (3.0 * nat0 / (4.0 * math.pi)) ** (1.0 / 3.0)
+    kd = x / aeff
+    x0 = (-(nx + 1) / 2.0, -(ny + 1) / 2.0, -(nz + 1) / 2.0)
+    p = Problem(nx, ny, nz, np.asarray(iocc, dtype=np.int16), complex(m), kd, aeff, x0)
+    if orientations is None:
+        orientations = [(0.0, 0.0, 0.0)]
+    for ang in orientations:
+        R = euler_rotation(*ang)
+        k = kd * (R @ np.array([1.0, 0.0, 0.0]))
+        for e in (R @ np.array([0.0, 1.0, 0.0]), R @ np.array([0.0, 0.0, 1.0])):
+            p.incid.append(Incidence(k=k, e=e.astype(np.complex128)))
+    return p
+
+
+def voxel_problem(n, p_occ=0.6, m1=1.5 + 0.01j, m2=1.2 + 0.0j, x=8.0, seed=0):
+    """Two-material random voxel target: each voxel occupied with probability
+    p_occ, material 1 with probability 1/2.  Returns (Problem, material map)."""
+    rng = np.random.default_rng(seed)
+    occ = rng.random(n ** 3) < p_occ
+    mat = np.where(rng.random(n ** 3) < 0.5, 1, 2) * occ
+    prob = make_problem(n, m=m1, x=x, iocc=occ.astype(np.int16))
+    return prob, mat

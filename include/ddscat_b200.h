@@ -1,0 +1,24 @@
+/* Extensions of the B200 DDA library beyond the reference ABI.
+ *
+ * These entry points have no counterpart in ddscat_cuda_unified/cuda/
+ * ddscat_matvec_cuda.h; they are new symbols only, and the 15 reference entry
+ * points in ddscat_matvec_cuda.h keep their behaviour.
+ */
+#pragma once
+#include <stdint.h>
+#include "ddscat_matvec_cuda.h"
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Per-iteration progress lines on stdout (the reference always prints them;
+ * here they are off unless level != 0 or DDSCAT_B200_VERBOSE is set). */
+DDSCAT_CUDA_API int ddscat_b200_set_verbose(int level);
+
+/* 0 for the FFT3D build (libddscat_matvec_cuda.so), 1 for the SLICES build
+ * (libddscat_matvec_cuda_slice.so). */
+DDSCAT_CUDA_API int ddscat_b200_layout(void);
+
+#ifdef __cplusplus
+}
+#endif

@@ -1,0 +1,142 @@
+"""Generate golden fixtures by running the REFERENCE library on a B200.
+
+The reference backend (ddscat_cuda_unified/cuda/ddscat_matvec_cuda.cu) is built
+unmodified by oracle/Makefile into oracle/_ref/.  This script calls it through
+its own C ABI on small seeded inputs and stores inputs and outputs in
+tests/golden/reference_fixtures.npz.  tests/test_oracle_pinned.py then checks
+the CPU oracle against these outputs (no GPU needed), which pins the oracle to
+the reference's actual behaviour.
+
+Run on a GPU machine:  python tests/golden/make_reference_fixtures.py
+"""
+import ctypes as ct
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "ddscat-cuda_b200"))
+
+from ddscat_b200 import targets  # noqa: E402
+import ddscat_b200 as D  # noqa: E402
+from oracle import ddscat_oracle as O  # noqa: E402
+
+OUT = os.path.join(HERE, "reference_fixtures.npz")
+
+
+def ref_lib(layout="fft3d"):
+    path = os.path.join(ROOT, "oracle", "_ref", f"libddscat_ref_{layout}.so")
+    lib = ct.CDLL(path, mode=ct.RTLD_LOCAL)
+    _declare_ref(lib)  # the reference exports the same 15 names and signatures
+    return lib
+
+
+def _declare_ref(lib):
+    _P, _I, _F = ct.c_void_p, ct.c_int, ct.c_float
+    _D = ct.POINTER(ct.c_double)
+    lib.ddscat_cuda_prepare_green_f32.argtypes = [_I] * 7 + [_F] * 9 + [_P]
+    lib.ddscat_cuda_prepare_f32.argtypes = [_I] * 6 + [_P, _P]
+    lib.ddscat_cuda_apply_f32.argtypes = [_I, _P, _P, _P, _P]
+    for s in D.SOLVERS:
+        getattr(lib, f"ddscat_cuda_solve_{s}_f32").argtypes = [_P, _P, _P, _P, _I, _I, _F, ct.POINTER(_I),
+                                                                ct.POINTER(_F), ct.POINTER(_I)]
+    lib.ddscat_cuda_evalq_f32.argtypes = [_I, _P, _P, _P, _P, _F, _F, _F, _F, _D, _D, _D]
+    lib.ddscat_cuda_scat_f32.argtypes = [_I, _I, _P, _P, _P, _P, _P, _F, _F, _P, _P, _D, _D, _D, _D, ct.POINTER(_I),
+                                         _P, _P]
+    lib.ddscat_cuda_last_error.restype = ct.c_char_p
+
+
+def _p(a):
+    return a.ctypes.data_as(ct.c_void_p)
+
+
+def main():
+    lib = ref_lib("fft3d")
+    fx = {}
+    # ---- A: MATVEC on a random 7x6x5 grid (prepare_green, both CWHAT), IDIPINT 0 and 1
+    rng = np.random.default_rng(20261203)
+    for idip in (0, 1):
+        nx, ny, nz = 7, 6, 5
+        nat = nx * ny * nz
+        iocc = (rng.random(nat) < 0.75).astype(np.int16)
+        ak = (rng.normal(size=3) * 0.4).astype(np.float32)
+        x = (rng.normal(size=3 * nat) + 1j * rng.normal(size=3 * nat)).astype(np.complex64)
+        x[np.tile(iocc == 0, 3)] = 0  # DDSCAT passes zeros on vacuum sites
+        adia = (rng.normal(size=3 * nat) + 1j * rng.normal(size=3 * nat)).astype(np.complex64)
+        aoff = (0.3 * (rng.normal(size=3 * nat) + 1j * rng.normal(size=3 * nat))).astype(np.complex64)
+        rc = lib.ddscat_cuda_prepare_green_f32(nx, ny, nz, 0, nat, int(iocc.sum()), idip, 0.0, 0.0, 0.0, *map(float, ak), 1.0,
+                                               1.0, 1.0, _p(iocc))
+        assert rc == 0, lib.ddscat_cuda_last_error()
+        for cw in "NC":
+            y = np.empty_like(x)
+            assert lib.ddscat_cuda_apply_f32(ord(cw), _p(x), _p(y), _p(adia), _p(aoff)) == 0
+            fx[f"A{idip}_y{cw}"] = y
+        fx.update({f"A{idip}_dims": np.array([nx, ny, nz]), f"A{idip}_iocc": iocc, f"A{idip}_ak": ak,
+                   f"A{idip}_x": x, f"A{idip}_adia": adia, f"A{idip}_aoff": aoff})
+    # ---- B: 12^3 sphere, LDR, all eight solvers + EVALQ + SCAT
+    n = 12
+    prob = targets.make_problem(n, m=1.5 + 0.01j, x=2.0)
+    k = prob.incid[0].k.astype(np.float32)
+    iocc = prob.iocc
+    b, adia, aoff = prob.rhs(0), prob.adia(0), prob.aoff()
+    rc = lib.ddscat_cuda_prepare_green_f32(n, n, n, 0, prob.nat, prob.nat0, 0, 0.0, 0.0, 0.0, *map(float, k), 1.0, 1.0, 1.0,
+                                           _p(iocc))
+    assert rc == 0, lib.ddscat_cuda_last_error()
+    fx.update({"B_n": np.array([n]), "B_iocc": iocc, "B_k": k, "B_b": b, "B_adia": adia, "B_aoff": aoff,
+               "B_e": prob.incid[0].e.astype(np.complex64), "B_x0": np.array(prob.x0, dtype=np.float32)})
+    for s in D.SOLVERS:
+        xs = np.zeros_like(b)
+        it, tole, nc = ct.c_int(), ct.c_float(), ct.c_int()
+        rc = getattr(lib, f"ddscat_cuda_solve_{s}_f32")(_p(b), _p(xs), _p(adia), _p(aoff), b.size, 300, 1e-5,
+                                                        ct.byref(it), ct.byref(tole), ct.byref(nc))
+        fx[f"B_{s}_rc"] = np.array([rc])
+        fx[f"B_{s}_x"] = xs
+        fx[f"B_{s}_meta"] = np.array([it.value, tole.value, nc.value], dtype=np.float64)
+        if s == "qmrccg":
+            cabs, cext, cpha = ct.c_double(), ct.c_double(), ct.c_double()
+            assert lib.ddscat_cuda_evalq_f32(1, None, None, None, None, *map(float, k), 1.0, ct.byref(cabs), ct.byref(cext),
+                                             ct.byref(cpha)) == 0
+            fx["B_evalq"] = np.array([cabs.value, cext.value, cpha.value])
+            th = np.deg2rad(np.arange(0.0, 181.0, 30.0))
+            kk = float(np.linalg.norm(k))
+            aks = np.array([[kk * np.cos(t), kk * np.sin(t), 0.0] for t in th], dtype=np.float32)
+            em1 = np.array([[-np.sin(t), np.cos(t), 0.0] for t in th], dtype=np.float32)
+            em2 = np.array([[0.0, 0.0, 1.0] for t in th], dtype=np.float32)
+            dx = np.ones(3, dtype=np.float32)
+            x0 = np.array(prob.x0, dtype=np.float32)
+            e01 = prob.incid[0].e.astype(np.complex64)
+            f1 = np.zeros(len(th), dtype=np.complex64)
+            f2 = np.zeros(len(th), dtype=np.complex64)
+            cb, cs, cg2 = ct.c_double(), ct.c_double(), ct.c_double()
+            cg = (ct.c_double * 3)()
+            navg = ct.c_int()
+            rc = lib.ddscat_cuda_scat_f32(0, len(th), _p(k), _p(aks), _p(dx), _p(em1), _p(em2), 1.0, 3.0, _p(e01),
+                                          _p(x0), ct.byref(cb), ct.byref(cs), ct.cast(cg, ct.POINTER(ct.c_double)),
+                                          ct.byref(cg2), ct.byref(navg), _p(f1), _p(f2))
+            assert rc == 0, lib.ddscat_cuda_last_error()
+            fx["B_scat"] = np.array([cb.value, cs.value, cg[0], cg[1], cg[2], cg2.value, navg.value])
+            fx.update({"B_aks": aks, "B_em1": em1, "B_em2": em2, "B_f1": f1, "B_f2": f2})
+    lib.ddscat_cuda_release()
+    # ---- C: prepare_f32 with a CPU-supplied octant (FP64 oracle octant rounded to c64)
+    nx, ny, nz = 6, 5, 4
+    nat = nx * ny * nz
+    iocc = np.ones(nat, dtype=np.int16)
+    gp = O.GreenParams(nx, ny, nz, ak=(0.3, -0.2, 0.5))
+    oct6 = O.green_octant(gp).astype(np.complex64)
+    x = (rng.normal(size=3 * nat) + 1j * rng.normal(size=3 * nat)).astype(np.complex64)
+    adia = np.full(3 * nat, 1.7 - 0.4j, dtype=np.complex64)
+    aoff = np.zeros(3 * nat, dtype=np.complex64)
+    assert lib.ddscat_cuda_prepare_f32(nx, ny, nz, 0, nat, nat, _p(oct6), _p(iocc)) == 0
+    y = np.empty_like(x)
+    assert lib.ddscat_cuda_apply_f32(ord("N"), _p(x), _p(y), _p(adia), _p(aoff)) == 0
+    fx.update({"C_dims": np.array([nx, ny, nz]), "C_oct": oct6, "C_x": x, "C_adia": adia, "C_y": y})
+    lib.ddscat_cuda_release()
+    np.savez_compressed(OUT, **fx)
+    print("wrote", OUT, len(fx), "arrays")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,113 @@
+"""GPU parity of the MATVEC and the Green build against the FP64 oracle,
+through the C ABI (ddscat_cuda_prepare_green_f32 / prepare_f32 / apply_f32).
+
+Tolerance: complex-FP32 bulk arithmetic, so the relative L2 error of y must be
+<= 2e-5 and the max-norm error <= 1e-4 of max|y| (the FFT error grows like
+eps_f32 * log2(M))."""
+import numpy as np
+import pytest
+
+import ddscat_b200 as D
+from oracle import ddscat_oracle as O
+
+RTOL_L2 = 2e-5
+RTOL_MAX = 1e-4
+
+
+def _case(dims, idipint, seed=11, occ_p=0.7):
+    nx, ny, nz = dims
+    rng = np.random.default_rng(seed)
+    nat = nx * ny * nz
+    iocc = (rng.random(nat) < occ_p).astype(np.int16)
+    iocc[0] = 1
+    ak = tuple(rng.normal(size=3) * 0.4)
+    x = (rng.normal(size=3 * nat) + 1j * rng.normal(size=3 * nat)).astype(np.complex64)
+    adia = (rng.normal(size=3 * nat) + 1j * rng.normal(size=3 * nat)).astype(np.complex64)
+    aoff = (0.3 * (rng.normal(size=3 * nat) + 1j * rng.normal(size=3 * nat))).astype(np.complex64)
+    gp = O.GreenParams(nx, ny, nz, idipint=idipint, ak=tuple(float(np.float32(a)) for a in ak))
+    return iocc, ak, x, adia, aoff, gp
+
+
+def _err(y, yr):
+    l2 = np.linalg.norm(y - yr) / np.linalg.norm(yr)
+    mx = np.abs(y - yr).max() / np.abs(yr).max()
+    return l2, mx
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("layout", ["fft3d", "slices"])
+@pytest.mark.parametrize("dims,idipint", [((4, 4, 4), 0), ((5, 3, 4), 0), ((6, 5, 7), 1), ((7, 11, 13), 0),
+                                          ((8, 8, 8), 0), ((12, 10, 9), 1), ((16, 16, 16), 0), ((24, 18, 30), 0),
+                                          ((32, 32, 32), 0)])
+def test_apply_matches_oracle(layout, dims, idipint):
+    iocc, ak, x, adia, aoff, gp = _case(dims, idipint)
+    dda = D.DDA(layout)
+    dda.prepare_green(*dims, iocc, ak, idipint=idipint)
+    op = O.Operator.from_params(gp, iocc)
+    for cwhat in "NC":
+        y = dda.apply(x, adia, aoff, cwhat)
+        yr = op.apply_full(x, adia, aoff, cwhat)
+        l2, mx = _err(y, yr)
+        assert l2 <= RTOL_L2 and mx <= RTOL_MAX, (cwhat, l2, mx)
+        # unoccupied sites are exactly zero (cu:117)
+        assert np.all(y.reshape(3, -1)[:, iocc == 0] == 0)
+    dda.release()
+
+
+@pytest.mark.gpu
+def test_prepare_with_cpu_green_matches_gpu_green():
+    dims = (10, 9, 8)
+    iocc, ak, x, adia, aoff, gp = _case(dims, 0, seed=5)
+    dda = D.DDA()
+    dda.prepare_green(*dims, iocc, ak)
+    y1 = dda.apply(x, adia, aoff)
+    oct6 = O.green_octant(gp).astype(np.complex64)
+    dda.prepare(*dims, iocc, oct6)
+    y2 = dda.apply(x, adia, aoff)
+    yr = O.Operator.from_octant(*dims, oct6.astype(np.complex128), iocc).apply_full(x, adia, aoff)
+    assert _err(y2, yr)[0] <= RTOL_L2
+    assert _err(y1, y2)[0] <= RTOL_L2
+    dda.release()
+
+
+@pytest.mark.gpu
+def test_pbc_green_matches_oracle():
+    """IPBC=1 (periodic in y): full-tensor Green build and MATVEC branch."""
+    dims = (4, 3, 3)
+    rng = np.random.default_rng(2)
+    nat = 36
+    iocc = np.ones(nat, dtype=np.int16)
+    ak = (0.6, 0.25, 0.0)
+    x = (rng.normal(size=3 * nat) + 1j * rng.normal(size=3 * nat)).astype(np.complex64)
+    adia = np.full(3 * nat, 2.0 + 0.5j, dtype=np.complex64)
+    aoff = np.zeros(3 * nat, dtype=np.complex64)
+    gamma, pyd = 5e-2, 3.0
+    dda = D.DDA()
+    dda.prepare_green(*dims, iocc, ak, ipbc=1, gamma=gamma, pyd=pyd, pzd=0.0)
+    y = dda.apply(x, adia, aoff)
+    gp = O.GreenParams(*dims, ipbc=1, gamma=gamma, pyd=pyd, pzd=0.0,
+                       ak=tuple(float(np.float32(a)) for a in ak))
+    op = O.Operator.from_params(gp, iocc)
+    yr = op.apply_full(x, adia, aoff)
+    assert _err(y, yr)[0] <= 1e-4
+    dda.release()
+
+
+@pytest.mark.gpu
+def test_apply_is_linear_and_symmetric():
+    """Size-independent properties at a larger grid: A(a x + b z) = a Ax + b Az
+    and z^T A x = x^T A z (complex symmetry)."""
+    dims = (40, 36, 32)
+    iocc, ak, x, adia, aoff, gp = _case(dims, 0, seed=3, occ_p=1.0)
+    rng = np.random.default_rng(4)
+    z = (rng.normal(size=x.size) + 1j * rng.normal(size=x.size)).astype(np.complex64)
+    dda = D.DDA()
+    dda.prepare_green(*dims, iocc, ak)
+    ax, az = dda.apply(x, adia, aoff), dda.apply(z, adia, aoff)
+    a, b = 0.3 - 0.7j, 1.1 + 0.2j
+    lin = dda.apply((a * x + b * z).astype(np.complex64), adia, aoff)
+    assert np.linalg.norm(lin - (a * ax + b * az)) / np.linalg.norm(lin) < 5e-6
+    s1 = np.dot(z.astype(np.complex128), ax.astype(np.complex128))
+    s2 = np.dot(x.astype(np.complex128), az.astype(np.complex128))
+    assert abs(s1 - s2) / abs(s1) < 1e-5
+    dda.release()
