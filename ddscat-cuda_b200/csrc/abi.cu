@@ -419,4 +419,46 @@ DDSCAT_CUDA_API int ddscat_b200_set_verbose(int level) {
 
 DDSCAT_CUDA_API int ddscat_b200_layout(void) { return slices_build(); }
 
+DDSCAT_CUDA_API int ddscat_b200_matvec_timing(int nrhs, int iters, int cwhat, float* ms_per_call) {
+  clear_error();
+  if (!s.ready || nrhs <= 0 || iters <= 0 || !ms_per_call || (cwhat != 'N' && cwhat != 'C')) {
+    set_error("matvec_timing", "invalid argument");
+    return 400;
+  }
+  const size_t cn = (size_t)3 * s.eng.g.nat0;
+  C *x = nullptr, *y = nullptr, *ad = nullptr;
+  cudaError_t e = cudaMalloc((void**)&x, cn * nrhs * sizeof(C));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&y, cn * nrhs * sizeof(C));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&ad, cn * nrhs * sizeof(C));
+  if (e != cudaSuccess) { cudaFree(x); cudaFree(y); cudaFree(ad); set_cuda_error("matvec_timing", e); return 401; }
+  {
+    std::vector<C> h(cn);
+    for (size_t i = 0; i < cn; ++i) h[i] = make_float2((float)((i * 2654435761u) % 1000) * 1e-3f, (float)(i % 7) * 0.1f);
+    for (int r = 0; r < nrhs; ++r) {
+      cudaMemcpy(x + r * cn, h.data(), cn * sizeof(C), cudaMemcpyHostToDevice);
+      cudaMemcpy(ad + r * cn, h.data(), cn * sizeof(C), cudaMemcpyHostToDevice);
+    }
+  }
+  MvArgs<float> a;
+  a.x = x; a.x_rs = cn; a.y = y; a.y_rs = cn; a.io_full = 0;
+  a.adia = ad; a.a_rs = cn; a.a_full = 0; a.aoff = nullptr; a.conj = (cwhat == 'C'); a.nrhs = nrhs;
+  int rc = 0;
+  for (int w = 0; w < 3 && !rc; ++w) rc = s.eng.matvec(a);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, s.stream);
+  for (int i = 0; i < iters && !rc; ++i) rc = s.eng.matvec(a);
+  cudaEventRecord(e1, s.stream);
+  e = cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(x); cudaFree(y); cudaFree(ad);
+  if (!rc && e != cudaSuccess) { set_cuda_error("matvec_timing", e); rc = 402; }
+  *ms_per_call = ms / iters;
+  return rc;
+}
+
 }  // extern "C"

@@ -5,7 +5,8 @@
 //                                 compact v[m*NAT0 + q], q = rank of occupied site j
 //   zhat  : z-spectrum, [rhs][comp][kz < Mz][iy < ny][ix < nx]
 //   slab  : xy spectrum of a batch of kz planes, [rhs][comp][kz][iy < ny][kx < Mx]
-//   green : octant [6][nz+1][ny+1][nx+1] (IPBC=0) or full [6][Mz][My][Mx] (IPBC=1)
+//   green : point-interleaved [point][6], points = octant (nz+1)(ny+1)(nx+1) (IPBC=0)
+//           or the full Mz*My*Mx grid (IPBC=1); 6 = (xx,xy,xz,yy,yz,zz)
 // The MATVEC is a z-first pipeline: z-forward (pad-skip, compact scatter fused)
 // -> per kz batch { x-forward, y-forward * Green * y-inverse, x-inverse } ->
 // z-inverse with the diagonal / off-diagonal CXZC terms and compact gather fused.
@@ -75,12 +76,14 @@ template <typename T> struct Engine {
   int slab_nr = 0, slab_B = 0;  // slab = slab_nr RHS x slab_B planes
   size_t slab_budget_elems = 0;
   int slices_layout = 0;
+  int xpipe = 0;           // 1: x-first transposed pipeline (power-of-two grids)
   cudaStream_t stream = 0;
   size_t bytes_allocated = 0;
 
   int init_geometry(int nx, int ny, int nz, int ipbc, int nat, int nat0, const int16_t* iocc_host);
   int build_green(const GreenArgs<T>& ga);          // on-GPU direct sum + FFT to the octant
   int upload_green(const void* host_green);         // CPU-supplied CXZC (ddscat_cuda_prepare_f32)
+  int interleave_green(const C* planar_dev);        // planar [6][P] -> green [P][6]
   int ensure_workspace(int nrhs);
   int matvec(const MvArgs<T>& a);
   void release();
@@ -118,5 +121,10 @@ template <typename T>
 void v_precon(cplx<T>* d, const cplx<T>* a, const cplx<T>* adia_full, const int* occ, int nat, int nat0, cudaStream_t s);
 template <typename T> void v_gather(const cplx<T>* full, cplx<T>* compact, const int* occ, int nat, int nat0, cudaStream_t s);
 template <typename T> void v_scatter(const cplx<T>* compact, cplx<T>* full, const int* occ, int nat, int nat0, cudaStream_t s);
+
+// x-first transposed pipeline (matvec_x.cu)
+template <typename T> bool xpipe_supported(const Geometry& g);
+template <typename T> int matvec_xpipe(Engine<T>& E, const MvArgs<T>& a);
+template <typename T> int interleave_green_zfast(Engine<T>& E, const cplx<T>* planar);
 
 }  // namespace ddb

@@ -1,0 +1,125 @@
+// Register-resident line FFT for power-of-two lengths N = E*T in {16..512}.
+//
+// A line is held by T threads, thread t owning elements t + T*i (i < E).  The
+// transform is the four-step factorisation N = E*T: an E-point DFT in
+// registers over i, a twiddle W_N^{t p}, one transpose through shared memory,
+// and T-point DFTs in registers.  With E = m*T (m = 1 or 2) the output lands
+// in the same index map (thread t owns X[t + T*i]), so a forward transform,
+// a pointwise operation and an inverse transform chain without moving data,
+// pad-skip loads read only i with t + T*i < n, and truncated stores write only
+// the first n outputs.  In-register DFTs of 16 and 32 points are themselves
+// four-step products of 4- and 8-point butterflies with exact constant
+// twiddles.  Convention as in fft.cuh: DIR = +1 is exp(+i...), unnormalised.
+#pragma once
+#include "fft.cuh"
+
+namespace ddb {
+
+#include "w32.inc"
+
+// W_K^m for DIR: exp(DIR * 2*pi*i*m/K), K divides 32
+template <int K, int DIR, typename C> DDB_HD C wk(int m) {
+  const int q = (m * (32 / K)) & 31;
+  return mk<C>(w32re(q), DIR < 0 ? w32im(q) : -w32im(q));
+}
+
+template <int K, int DIR, typename C> __device__ __forceinline__ void dftr(C* v) {
+  if constexpr (K == 1) {
+  } else if constexpr (K == 2) {
+    bfly2<DIR>(v);
+  } else if constexpr (K == 4) {
+    bfly4<DIR>(v);
+  } else if constexpr (K == 8) {
+    bfly8<DIR>(v);
+  } else {
+    // K = K1*K2: element K2*a + b ; output c + K1*d
+    constexpr int K1 = (K == 16) ? 4 : 8;
+    constexpr int K2 = K / K1;
+    C Y[K2][K1];
+#pragma unroll
+    for (int b = 0; b < K2; ++b) {
+      C t[K1];
+#pragma unroll
+      for (int a = 0; a < K1; ++a) t[a] = v[K2 * a + b];
+      dftr<K1, DIR>(t);
+#pragma unroll
+      for (int c = 0; c < K1; ++c) Y[b][c] = (b * c == 0) ? t[c] : cmul(t[c], wk<K, DIR, C>(b * c));
+    }
+#pragma unroll
+    for (int c = 0; c < K1; ++c) {
+      C t[K2];
+#pragma unroll
+      for (int b = 0; b < K2; ++b) t[b] = Y[b][c];
+      dftr<K2, DIR>(t);
+#pragma unroll
+      for (int d = 0; d < K2; ++d) v[c + K1 * d] = t[d];
+    }
+  }
+}
+
+// per-line scratch size (complex elements) for the transpose, before padding
+template <int E, int T> constexpr int line_scratch() { return T * (E + 1) + 1; }
+
+// Line stride (complex elements) for L lines per block whose threads are
+// interleaved line-fastest (column passes) or thread-fastest (row passes):
+// the smallest stride >= T*(E+1) for which the 16 lanes of a half-warp hit 16
+// distinct 8-byte bank pairs in both the transpose write and read.
+inline int line_stride(int E, int T, int L, bool line_fastest) {
+  const int base = T * (E + 1);
+  for (int pad = 0; pad < 32; ++pad) {
+    const int LS = base + pad;
+    bool ok = true;
+    for (int phase = 0; phase < 2 && ok; ++phase) {
+      unsigned used = 0;
+      for (int lane = 0; lane < 16 && ok; ++lane) {
+        int l, t;
+        if (line_fastest) { l = lane % L; t = lane / L; } else { t = lane % T; l = lane / T; }
+        if (l >= L || t >= T) continue;
+        // write: t*(E+1) + p (p = 0); read: s*(E+1) + t (s = 0)
+        const int a = (l * LS + (phase == 0 ? t * (E + 1) : t)) & 15;
+        if (used & (1u << a)) ok = false;
+        used |= 1u << a;
+      }
+    }
+    if (ok) return LS;
+  }
+  return base + 1;
+}
+
+// One length-E*T transform of the line held in v by thread t (0 <= t < T).
+// `sl` is this line's shared scratch; `tw` the N-entry table exp(-2*pi*i*m/N).
+// BLOCK_SYNC selects __syncthreads (line spread over warps) or __syncwarp.
+template <int E, int T, int DIR, bool BLOCK_SYNC, typename C>
+__device__ __forceinline__ void line_fft(C (&v)[E], C* sl, int t, const C* __restrict__ tw) {
+  constexpr int M = E / T;
+  static_assert(M * T == E && M >= 1, "E must be a multiple of T");
+  dftr<E, DIR>(v);
+#pragma unroll
+  for (int p = 1; p < E; ++p) v[p] = cmul(v[p], twid<DIR>(tw, t * p));
+#pragma unroll
+  for (int p = 0; p < E; ++p) sl[t * (E + 1) + p] = v[p];
+  if (BLOCK_SYNC) __syncthreads(); else __syncwarp();
+#pragma unroll
+  for (int j = 0; j < M; ++j) {
+    C u[T];
+#pragma unroll
+    for (int s = 0; s < T; ++s) u[s] = sl[s * (E + 1) + t + T * j];
+    dftr<T, DIR>(u);
+#pragma unroll
+    for (int q = 0; q < T; ++q) v[j + M * q] = u[q];
+  }
+  if (BLOCK_SYNC) __syncthreads(); else __syncwarp();
+}
+
+// (E, T) shape for a supported power-of-two length, E*T = N
+template <int N> struct RegShape;
+template <> struct RegShape<16> { static constexpr int E = 4, T = 4; };
+template <> struct RegShape<32> { static constexpr int E = 8, T = 4; };
+template <> struct RegShape<64> { static constexpr int E = 8, T = 8; };
+template <> struct RegShape<128> { static constexpr int E = 16, T = 8; };
+template <> struct RegShape<256> { static constexpr int E = 16, T = 16; };
+template <> struct RegShape<512> { static constexpr int E = 32, T = 16; };
+
+inline bool reg_supported(int n) { return n == 16 || n == 32 || n == 64 || n == 128 || n == 256 || n == 512; }
+
+}  // namespace ddb

@@ -313,8 +313,10 @@ template <typename T> int Engine<T>::build_green(const GreenArgs<T>& ga) {
       const int TX = std::max(1, std::min(32, 4096 / Mz));
       const size_t sm = (size_t)2 * TX * Mz * sizeof(double2);
       cudaFuncSetAttribute((const void*)k_green_col<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-      k_green_col<C><<<dim3((unsigned)ceil_div(W, TX), 6), 256, sm>>>(a2, green, Mz, W, nzo, plz, twz_d, TX);
+      C* planar = reinterpret_cast<C*>(a1);  // a1 is free now and larger than the result
+      k_green_col<C><<<dim3((unsigned)ceil_div(W, TX), 6), 256, sm>>>(a2, planar, Mz, W, nzo, plz, twz_d, TX);
       if (check_launch("Green z FFT")) rc = 6;
+      if (!rc && interleave_green(planar)) rc = 6;
     }
     e = cudaDeviceSynchronize();
     if (!rc && e != cudaSuccess) { set_cuda_error("Green build synchronize", e); rc = 7; }

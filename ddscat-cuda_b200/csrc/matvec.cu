@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <cstdlib>
 #include "engine.h"
+#include "fftreg.cuh"
 
 namespace ddb {
 
@@ -45,6 +46,7 @@ template <typename T> struct MvParams {
   const cplx<T>* twy;
   const cplx<T>* twz;
   int tz, ry, ty;  // tile widths
+  int lsz, lsx, lsy;  // register-path line strides (complex elements)
   T inv_ngrid;
 };
 
@@ -119,23 +121,33 @@ template <typename T> __global__ void __launch_bounds__(256) k_xfwd(MvParams<T> 
 // Green tensor at spectral point (kx,ky,kz): symmetric 3x3 (a11,a12,a13,a22,a23,a33)
 template <typename T>
 __device__ __forceinline__ void green_at(const MvParams<T>& P, int kx, int ky, int kz, cplx<T> a[6]) {
+  // Green storage is point-interleaved: g[point*6 + m], m = (xx,xy,xz,yy,yz,zz)
+  size_t b;
+  T sxy = (T)1, sxz = (T)1, syz = (T)1;
   if (P.ipbc == 0) {
     const T sx = kx <= P.nx ? (T)1 : (T)-1, sy = ky <= P.ny ? (T)1 : (T)-1, sz = kz <= P.nz ? (T)1 : (T)-1;
     const int irx = min(kx, P.Mx - kx), iry = min(ky, P.My - ky), irz = min(kz, P.Mz - kz);
-    const size_t cx = P.nx + 1, cy = P.ny + 1, cz = P.nz + 1;
-    const size_t b = (size_t)irx + cx * ((size_t)iry + cy * irz), st = cx * cy * cz;
-    a[0] = P.green[b];
-    a[1] = cscale(P.green[b + st], sx * sy);
-    a[2] = cscale(P.green[b + 2 * st], sx * sz);
-    a[3] = P.green[b + 3 * st];
-    a[4] = cscale(P.green[b + 4 * st], sy * sz);
-    a[5] = P.green[b + 5 * st];
+    b = (size_t)irx + (size_t)(P.nx + 1) * ((size_t)iry + (size_t)(P.ny + 1) * irz);
+    sxy = sx * sy; sxz = sx * sz; syz = sy * sz;
   } else {
-    const size_t st = (size_t)P.Mx * P.My * P.Mz;
-    const size_t k = (size_t)kx + (size_t)P.Mx * ((size_t)ky + (size_t)P.My * kz);
-#pragma unroll
-    for (int m = 0; m < 6; ++m) a[m] = P.green[k + m * st];
+    b = (size_t)kx + (size_t)P.Mx * ((size_t)ky + (size_t)P.My * kz);
   }
+  const cplx<T>* gp = P.green + 6 * b;
+  if constexpr (sizeof(cplx<T>) == 8) {
+    const float4* g4 = reinterpret_cast<const float4*>(gp);  // 48-byte point record, 16-byte aligned
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      const float4 q = __ldg(g4 + m);
+      a[2 * m] = mk<cplx<T>>(q.x, q.y);
+      a[2 * m + 1] = mk<cplx<T>>(q.z, q.w);
+    }
+  } else {
+#pragma unroll
+    for (int m = 0; m < 6; ++m) a[m] = gp[m];
+  }
+  a[1] = cscale(a[1], sxy);
+  a[2] = cscale(a[2], sxz);
+  a[4] = cscale(a[4], syz);
 }
 
 // ---------------------------------------------------------------- y forward * Green * y inverse
@@ -279,6 +291,270 @@ template <typename T> __global__ void __launch_bounds__(256) k_zinv_fin(MvParams
   }
 }
 
+
+// ================================================================ register path
+// Power-of-two axis lengths 16..512 use register-resident line transforms
+// (fftreg.cuh): each pass is one coalesced global read, one shared-memory
+// transpose per transform and one coalesced global write.  Column passes put
+// L = blockDim/T adjacent columns in the fast thread index (coalescing along
+// the contiguous axis); row passes put the T threads of a row adjacent.
+
+template <typename T>
+__device__ __forceinline__ void finish_site(const MvParams<T>& P, int rl, int c, int ix, int iy, int iz, cplx<T> wraw) {
+  using C = cplx<T>;
+  const C* x = P.x + (size_t)rl * P.x_rs;
+  C* y = P.y + (size_t)rl * P.y_rs;
+  const C* ad = P.adia + (size_t)rl * P.a_rs;
+  const C* ao = P.aoff ? P.aoff + (size_t)rl * P.a_rs : nullptr;
+  const size_t S = P.io_full ? (size_t)P.nat : (size_t)P.nat0;
+  const size_t SA = P.a_full ? (size_t)P.nat : (size_t)P.nat0;
+  const size_t j = (size_t)ix + (size_t)P.nx * ((size_t)iy + (size_t)P.ny * iz);
+  size_t q;
+  if (P.io_full) {
+    q = j;
+    if (P.iocc[j] == 0) { y[c * S + q] = mk<C>(0, 0); return; }
+  } else {
+    const int qq = P.inv[j];
+    if (qq < 0) return;
+    q = (size_t)qq;
+  }
+  const size_t qa = P.a_full ? j : q;
+  C xc = x[c * S + q];
+  if (P.conj) xc.y = -xc.y;
+  const C w = cscale(wraw, P.inv_ngrid);
+  C yv = csub(cmul(ad[c * SA + qa], xc), w);
+  if (ao) {
+    C x1 = x[q], x2 = x[S + q], x3 = x[2 * S + q];
+    if (P.conj) { x1.y = -x1.y; x2.y = -x2.y; x3.y = -x3.y; }
+    const C a23 = ao[qa], a31 = ao[SA + qa], a12 = ao[2 * SA + qa];
+    if (c == 0) yv = cadd(yv, cadd(cmul(a31, x3), cmul(a12, x2)));
+    else if (c == 1) yv = cadd(yv, cadd(cmul(a12, x1), cmul(a23, x3)));
+    else yv = cadd(yv, cadd(cmul(a23, x2), cmul(a31, x1)));
+  }
+  if (P.conj) yv.y = -yv.y;
+  y[c * S + q] = yv;
+}
+
+template <typename T, int N> __global__ void __launch_bounds__(256) k_zfwd_r(MvParams<T> P) {
+  using C = cplx<T>;
+  constexpr int E = RegShape<N>::E, TT = RegShape<N>::T;
+  const int LS = P.lsz;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* sm = reinterpret_cast<C*>(smem_raw);
+  C* tws = sm + (size_t)(blockDim.x / TT) * LS;  // N twiddles after the line scratches
+  const int L = blockDim.x / TT, l = threadIdx.x % L, t = threadIdx.x / L;
+  const int ix = blockIdx.x * L + l, iy = blockIdx.y;
+  const int rl = blockIdx.z / 3, c = blockIdx.z % 3;
+  if (rhs_off(P, rl)) return;
+  for (int u = threadIdx.x; u < N; u += blockDim.x) tws[u] = P.twz[u];
+  __syncthreads();
+  const C* x = P.x + (size_t)rl * P.x_rs;
+  const size_t S = P.io_full ? (size_t)P.nat : (size_t)P.nat0;
+  C v[E];
+#pragma unroll
+  for (int i = 0; i < E; ++i) {
+    const int iz = t + TT * i;
+    v[i] = mk<C>(0, 0);
+    if (iz < P.nz && ix < P.nx) {
+      const size_t j = (size_t)ix + (size_t)P.nx * ((size_t)iy + (size_t)P.ny * iz);
+      if (P.io_full) {
+        v[i] = x[c * S + j];
+      } else {
+        const int q = P.inv[j];
+        if (q >= 0) v[i] = x[c * S + q];
+      }
+      if (P.conj) v[i].y = -v[i].y;
+    }
+  }
+  line_fft<E, TT, +1, true>(v, sm + l * LS, t, tws);
+  if (ix < P.nx) {
+    C* zh = P.zhat + (size_t)rl * P.zhat_rs + (size_t)c * P.Mz * P.ny * P.nx + (size_t)iy * P.nx + ix;
+#pragma unroll
+    for (int i = 0; i < E; ++i) zh[(size_t)(t + TT * i) * P.ny * P.nx] = v[i];
+  }
+}
+
+template <typename T, int N> __global__ void __launch_bounds__(256) k_xfwd_r(MvParams<T> P) {
+  using C = cplx<T>;
+  constexpr int E = RegShape<N>::E, TT = RegShape<N>::T;
+  const int LS = P.lsx;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* sm = reinterpret_cast<C*>(smem_raw);
+  C* tws = sm + (size_t)(blockDim.x / TT) * LS;  // N twiddles after the line scratches
+  const int RL = blockDim.x / TT, t = threadIdx.x % TT, l = threadIdx.x / TT;
+  const int iy = blockIdx.x * RL + l, kzl = blockIdx.y, kz = P.kz0 + kzl;
+  const int rs = blockIdx.z / 3, c = blockIdx.z % 3, rl = P.slab_rhs0 + rs;
+  if (rhs_off(P, rl)) return;
+  for (int u = threadIdx.x; u < N; u += blockDim.x) tws[u] = P.twx[u];
+  __syncthreads();
+  const C* zh = P.zhat + (size_t)rl * P.zhat_rs + ((size_t)c * P.Mz + kz) * P.ny * P.nx + (size_t)iy * P.nx;
+  C v[E];
+#pragma unroll
+  for (int i = 0; i < E; ++i) {
+    const int ix = t + TT * i;
+    v[i] = (ix < P.nx && iy < P.ny) ? zh[ix] : mk<C>(0, 0);
+  }
+  line_fft<E, TT, +1, false>(v, sm + l * LS, t, tws);
+  if (iy < P.ny) {
+    C* sl = P.slab + (((size_t)rs * 3 + c) * P.nplanes + kzl) * P.ny * P.Mx + (size_t)iy * P.Mx;
+#pragma unroll
+    for (int i = 0; i < E; ++i) sl[t + TT * i] = v[i];
+  }
+}
+
+template <typename T, int N> __global__ void __launch_bounds__(384) k_ygreen_r(MvParams<T> P) {
+  // Thread (l, t, c): column l of the block's L columns, line thread t, field
+  // component c.  (1) forward y-FFT of every component's column into its line
+  // region (the same region serves as the transpose scratch), (2) Green 3x3
+  // multiply with one thread per spectral point, (3) inverse y-FFTs, truncated
+  // store.  Grid: x = RHS (so consecutive blocks share the Green tile in L2),
+  // y = column tile, z = plane.
+  using C = cplx<T>;
+  constexpr int E = RegShape<N>::E, TT = RegShape<N>::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int LS = P.lsy;
+  const int L = blockDim.x / (3 * TT);
+  const int l = threadIdx.x % L, t = (threadIdx.x / L) % TT, c = threadIdx.x / (L * TT);
+  C* tws = reinterpret_cast<C*>(smem_raw);  // N twiddles
+  C* lines = tws + N;                        // [3][L][LS]
+  C* my = lines + (size_t)(c * L + l) * LS;
+  for (int u = threadIdx.x; u < N; u += blockDim.x) tws[u] = P.twy[u];
+  const int rs = blockIdx.x, kx0 = blockIdx.y * L, kx = kx0 + l, kzl = blockIdx.z, kz = P.kz0 + kzl;
+  const int rl = P.slab_rhs0 + rs;
+  if (rhs_off(P, rl)) return;
+  __syncthreads();
+  const size_t plane = (size_t)P.ny * P.Mx, cstride = (size_t)P.nplanes * plane;
+  C* col = P.slab + ((size_t)rs * 3 * P.nplanes + kzl) * plane + c * cstride + kx;
+  C v[E];
+#pragma unroll
+  for (int i = 0; i < E; ++i) {
+    const int iy = t + TT * i;
+    v[i] = (iy < P.ny && kx < P.Mx) ? col[(size_t)iy * P.Mx] : mk<C>(0, 0);
+  }
+  line_fft<E, TT, +1, true>(v, my, t, tws);
+#pragma unroll
+  for (int i = 0; i < E; ++i) my[t + TT * i] = v[i];
+  __syncthreads();
+  for (int u = threadIdx.x; u < N * L; u += blockDim.x) {
+    const int ll = u % L, ky = u / L, kxx = kx0 + ll;
+    if (kxx >= P.Mx) continue;
+    C a[6];
+    green_at(P, kxx, ky, kz, a);
+    C* p0 = lines + (size_t)ll * LS + ky;
+    C* p1 = p0 + (size_t)L * LS;
+    C* p2 = p1 + (size_t)L * LS;
+    const C px = *p0, py = *p1, pz = *p2;
+    *p0 = cadd(cadd(cmul(a[0], px), cmul(a[1], py)), cmul(a[2], pz));
+    *p1 = cadd(cadd(cmul(a[1], px), cmul(a[3], py)), cmul(a[4], pz));
+    *p2 = cadd(cadd(cmul(a[2], px), cmul(a[4], py)), cmul(a[5], pz));
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < E; ++i) v[i] = my[t + TT * i];
+  __syncthreads();  // the region is reused as transpose scratch below
+  line_fft<E, TT, -1, true>(v, my, t, tws);
+  if (kx < P.Mx) {
+#pragma unroll
+    for (int i = 0; i < E; ++i) {
+      const int iy = t + TT * i;
+      if (iy < P.ny) col[(size_t)iy * P.Mx] = v[i];
+    }
+  }
+}
+
+template <typename T, int N> __global__ void __launch_bounds__(256) k_xinv_r(MvParams<T> P) {
+  using C = cplx<T>;
+  constexpr int E = RegShape<N>::E, TT = RegShape<N>::T;
+  const int LS = P.lsx;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* sm = reinterpret_cast<C*>(smem_raw);
+  C* tws = sm + (size_t)(blockDim.x / TT) * LS;  // N twiddles after the line scratches
+  const int RL = blockDim.x / TT, t = threadIdx.x % TT, l = threadIdx.x / TT;
+  const int iy = blockIdx.x * RL + l, kzl = blockIdx.y, kz = P.kz0 + kzl;
+  const int rs = blockIdx.z / 3, c = blockIdx.z % 3, rl = P.slab_rhs0 + rs;
+  if (rhs_off(P, rl)) return;
+  for (int u = threadIdx.x; u < N; u += blockDim.x) tws[u] = P.twx[u];
+  __syncthreads();
+  const C* sl = P.slab + (((size_t)rs * 3 + c) * P.nplanes + kzl) * P.ny * P.Mx + (size_t)iy * P.Mx;
+  C v[E];
+#pragma unroll
+  for (int i = 0; i < E; ++i) v[i] = (iy < P.ny) ? sl[t + TT * i] : mk<C>(0, 0);
+  line_fft<E, TT, -1, false>(v, sm + l * LS, t, tws);
+  if (iy < P.ny) {
+    C* zh = P.zhat + (size_t)rl * P.zhat_rs + ((size_t)c * P.Mz + kz) * P.ny * P.nx + (size_t)iy * P.nx;
+#pragma unroll
+    for (int i = 0; i < E; ++i) {
+      const int ix = t + TT * i;
+      if (ix < P.nx) zh[ix] = v[i];
+    }
+  }
+}
+
+template <typename T, int N> __global__ void __launch_bounds__(256) k_zinv_fin_r(MvParams<T> P) {
+  using C = cplx<T>;
+  constexpr int E = RegShape<N>::E, TT = RegShape<N>::T;
+  const int LS = P.lsz;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* sm = reinterpret_cast<C*>(smem_raw);
+  C* tws = sm + (size_t)(blockDim.x / TT) * LS;  // N twiddles after the line scratches
+  const int L = blockDim.x / TT, l = threadIdx.x % L, t = threadIdx.x / L;
+  const int ix = blockIdx.x * L + l, iy = blockIdx.y;
+  const int rl = blockIdx.z / 3, c = blockIdx.z % 3;
+  if (rhs_off(P, rl)) return;
+  for (int u = threadIdx.x; u < N; u += blockDim.x) tws[u] = P.twz[u];
+  __syncthreads();
+  const C* zh = P.zhat + (size_t)rl * P.zhat_rs + (size_t)c * P.Mz * P.ny * P.nx + (size_t)iy * P.nx + ix;
+  C v[E];
+#pragma unroll
+  for (int i = 0; i < E; ++i) v[i] = (ix < P.nx) ? zh[(size_t)(t + TT * i) * P.ny * P.nx] : mk<C>(0, 0);
+  line_fft<E, TT, -1, true>(v, sm + l * LS, t, tws);
+  if (ix < P.nx) {
+#pragma unroll
+    for (int i = 0; i < E; ++i) {
+      const int iz = t + TT * i;
+      if (iz < P.nz) finish_site(P, rl, c, ix, iy, iz, v[i]);
+    }
+  }
+}
+
+enum class Pass { ZF, XF, YG, XI, ZI };
+
+template <typename T, int N> static const void* reg_kernel(Pass p) {
+  switch (p) {
+    case Pass::ZF: return (const void*)k_zfwd_r<T, N>;
+    case Pass::XF: return (const void*)k_xfwd_r<T, N>;
+    case Pass::YG: return (const void*)k_ygreen_r<T, N>;
+    case Pass::XI: return (const void*)k_xinv_r<T, N>;
+    default: return (const void*)k_zinv_fin_r<T, N>;
+  }
+}
+
+// Register kernel for this pass and axis length, or null (generic path).
+template <typename T> static const void* pick_reg(Pass p, int n) {
+  if (std::getenv("DDSCAT_B200_GENERIC_FFT")) return nullptr;
+  if (sizeof(T) == 8) return nullptr;  // FP64 engine: generic path (register budget)
+  if (p == Pass::YG && n == 512) return nullptr;
+  switch (n) {
+    case 16: return reg_kernel<T, 16>(p);
+    case 32: return reg_kernel<T, 32>(p);
+    case 64: return reg_kernel<T, 64>(p);
+    case 128: return reg_kernel<T, 128>(p);
+    case 256: return reg_kernel<T, 256>(p);
+    case 512: return reg_kernel<T, 512>(p);
+    default: return nullptr;
+  }
+}
+
+static int reg_T(int n) { return n <= 32 ? 4 : (n <= 128 ? 8 : 16); }
+static int reg_E(int n) { return n / reg_T(n); }
+
+template <typename T> static int launch_k(const void* f, dim3 g, int threads, size_t sm, cudaStream_t st, MvParams<T>& P) {
+  void* args[] = {(void*)&P};
+  cudaError_t e = cudaLaunchKernel(f, g, dim3(threads), args, sm, st);
+  if (e != cudaSuccess) { set_cuda_error("MATVEC launch", e); return 1; }
+  return 0;
+}
+
 // ---------------------------------------------------------------- host side
 static int env_int(const char* name, int dflt) {
   const char* v = std::getenv(name);
@@ -308,6 +584,7 @@ int Engine<T>::init_geometry(int nx, int ny, int nz, int ipbc, int nat, int nat0
   px = make_fft_plan(g.Mx);
   py = make_fft_plan(g.My);
   pz = make_fft_plan(g.Mz);
+  xpipe = xpipe_supported<T>(g) ? 1 : 0;
   if (px.nstages < 0 || py.nstages < 0 || pz.nstages < 0) {
     set_error("prepare", "FFT length has too many prime factors");
     return 1;
@@ -339,16 +616,18 @@ int Engine<T>::init_geometry(int nx, int ny, int nz, int ipbc, int nat, int nat0
   e = cudaMalloc((void**)&green, g.green_count() * sizeof(C));
   if (e != cudaSuccess) { set_cuda_error("malloc resident Green", e); return 4; }
   bytes_allocated += g.green_count() * sizeof(C);
-  // slab budget: FFT3D keeps up to 64 MiB of xy spectrum per batch (fits the
-  // 126 MB L2 together with the Green octant traffic); SLICES keeps 4 planes.
-  const int mb = env_int("DDSCAT_B200_SLAB_MB", 64);
+  // slab budget: FFT3D keeps the xy spectrum of all kz planes of up to 4 GiB
+  // worth of RHS per batch (one Green pass per batch); SLICES keeps 4 planes.
+  const int mb = env_int("DDSCAT_B200_SLAB_MB", 4096);
   slab_budget_elems = (size_t)mb * 1024 * 1024 / sizeof(C);
   return 0;
 }
 
 template <typename T> int Engine<T>::ensure_workspace(int nrhs) {
   const size_t per_rhs_z = (size_t)3 * g.Mz * g.ny * g.nx;
-  const size_t per_plane = (size_t)3 * g.ny * g.Mx;  // one kz plane, 3 comps, one RHS
+  // one middle-stage plane, 3 comps, one RHS: a kz plane (z-first) or a kx column plane (x-first)
+  const size_t per_plane = xpipe ? (size_t)3 * g.My * g.nz : (size_t)3 * g.ny * g.Mx;
+  const int nplanes_all = xpipe ? g.Mx : g.Mz;
   if (nrhs <= zcap && zhat) return 0;
   if (zhat) { cudaFree(zhat); bytes_allocated -= (size_t)zcap * per_rhs_z * sizeof(C); zhat = nullptr; }
   if (slab) { cudaFree(slab); bytes_allocated -= (size_t)slab_nr * slab_B * per_plane * sizeof(C); slab = nullptr; }
@@ -357,12 +636,13 @@ template <typename T> int Engine<T>::ensure_workspace(int nrhs) {
   if (e != cudaSuccess) { zcap = 0; set_cuda_error("malloc z-spectrum workspace", e); return 1; }
   bytes_allocated += (size_t)zcap * per_rhs_z * sizeof(C);
   if (slices_layout) {
+    // bounded memory: the middle stage holds max(4, planes/16) planes of one RHS
     slab_nr = 1;
-    slab_B = std::min(4, g.Mz);
+    slab_B = std::min(nplanes_all, std::max(4, nplanes_all / 16));
   } else {
-    const size_t full_rhs = per_plane * g.Mz;
-    if (full_rhs * zcap <= slab_budget_elems) { slab_nr = zcap; slab_B = g.Mz; }
-    else if (full_rhs <= slab_budget_elems) { slab_nr = (int)std::max<size_t>(1, slab_budget_elems / full_rhs); slab_B = g.Mz; }
+    const size_t full_rhs = per_plane * nplanes_all;
+    if (full_rhs * zcap <= slab_budget_elems) { slab_nr = zcap; slab_B = nplanes_all; }
+    else if (full_rhs <= slab_budget_elems) { slab_nr = (int)std::max<size_t>(1, slab_budget_elems / full_rhs); slab_B = nplanes_all; }
     else { slab_nr = 1; slab_B = (int)std::max<size_t>(1, slab_budget_elems / per_plane); }
   }
   e = cudaMalloc((void**)&slab, (size_t)slab_nr * slab_B * per_plane * sizeof(C));
@@ -392,6 +672,7 @@ template <typename T> int Engine<T>::matvec(const MvArgs<T>& a) {
     const int want = (int)std::max<size_t>(1, std::min<size_t>((size_t)a.nrhs, budget / per_rhs_z));
     if (ensure_workspace(want)) return 1;
   }
+  if (xpipe) return matvec_xpipe<T>(*this, a);
   MvParams<T> P{};
   P.nx = g.nx; P.ny = g.ny; P.nz = g.nz; P.Mx = g.Mx; P.My = g.My; P.Mz = g.Mz;
   P.nat = g.nat; P.nat0 = g.nat0;
@@ -408,10 +689,35 @@ template <typename T> int Engine<T>::matvec(const MvArgs<T>& a) {
   P.tz = std::max(1, std::min(32, tile_elems / g.Mz));
   P.ry = std::max(1, std::min(16, tile_elems / (g.Mx + 1)));
   P.ty = std::max(1, std::min(32, (tile_elems / 2) / g.My));
+  const int threads = 256;
+  // per-pass kernel, grid geometry and shared memory: register path or generic
+  const void* fz_r = pick_reg<T>(Pass::ZF, g.Mz);
+  const void* fx_r = pick_reg<T>(Pass::XF, g.Mx);
+  const void* fy_r = pick_reg<T>(Pass::YG, g.My);
+  const void* fxi_r = pick_reg<T>(Pass::XI, g.Mx);
+  const void* fzi_r = pick_reg<T>(Pass::ZI, g.Mz);
+  // block sizes of the register passes (threads): z columns, x rows, y columns
+  const int thz = env_int("DDSCAT_B200_TH_Z", 256), thx = env_int("DDSCAT_B200_TH_X", 256);
+  const int Ly = std::max(1, env_int("DDSCAT_B200_LY", 4));  // y-pass columns per block
+  const int thy = 3 * reg_T(g.My) * Ly;
+  const int Lz = thz / reg_T(g.Mz), Rx = thx / reg_T(g.Mx);
+  P.lsz = line_stride(reg_E(g.Mz), reg_T(g.Mz), Lz, true);
+  P.lsx = line_stride(reg_E(g.Mx), reg_T(g.Mx), Rx, false);
+  P.lsy = std::max(line_stride(reg_E(g.My), reg_T(g.My), Ly, true), g.My);
+  const size_t smz_r = ((size_t)Lz * P.lsz + g.Mz) * sizeof(C);
+  const size_t smx_r = ((size_t)Rx * P.lsx + g.Mx) * sizeof(C);
+  const size_t smy_r = ((size_t)3 * Ly * P.lsy + g.My) * sizeof(C);
   const size_t sm_z = (size_t)2 * P.tz * g.Mz * sizeof(C);
   const size_t sm_x = (size_t)2 * P.ry * (g.Mx + 1) * sizeof(C);
   const size_t sm_y = (size_t)4 * P.ty * g.My * sizeof(C);
-  const int threads = 256;
+  {
+    static std::vector<const void*> attr_set;  // kernels whose smem limit is raised
+    for (const void* f : {fz_r, fx_r, fy_r, fxi_r, fzi_r}) {
+      if (!f || std::find(attr_set.begin(), attr_set.end(), f) != attr_set.end()) continue;
+      cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+      attr_set.push_back(f);
+    }
+  }
   for (int r0 = 0; r0 < a.nrhs; r0 += zcap) {
     const int nr = std::min(zcap, a.nrhs - r0);
     P.rhs0 = r0;
@@ -419,34 +725,77 @@ template <typename T> int Engine<T>::matvec(const MvArgs<T>& a) {
     P.y = a.y + (size_t)r0 * a.y_rs;
     P.adia = a.adia + (size_t)r0 * a.a_rs;
     P.aoff = a.aoff ? a.aoff + (size_t)r0 * a.a_rs : nullptr;
-    dim3 gz((unsigned)ceil_div(g.nx, P.tz), (unsigned)g.ny, (unsigned)(3 * nr));
-    k_zfwd<T><<<gz, threads, sm_z, stream>>>(P);
-    if (check_launch("MATVEC z-forward")) return 21;
+    if (fz_r) {
+      if (launch_k<T>(fz_r, dim3((unsigned)ceil_div(g.nx, Lz), (unsigned)g.ny, (unsigned)(3 * nr)), thz, smz_r, stream, P)) return 21;
+    } else {
+      dim3 gz((unsigned)ceil_div(g.nx, P.tz), (unsigned)g.ny, (unsigned)(3 * nr));
+      k_zfwd<T><<<gz, threads, sm_z, stream>>>(P);
+      if (check_launch("MATVEC z-forward")) return 21;
+    }
     for (int rs = 0; rs < nr; rs += slab_nr) {
       const int nrs = std::min(slab_nr, nr - rs);
       P.slab_rhs0 = rs;
       for (int kz0 = 0; kz0 < g.Mz; kz0 += slab_B) {
         P.kz0 = kz0;
         P.nplanes = std::min(slab_B, g.Mz - kz0);
-        dim3 gx((unsigned)ceil_div(g.ny, P.ry), (unsigned)P.nplanes, (unsigned)(3 * nrs));
-        k_xfwd<T><<<gx, threads, sm_x, stream>>>(P);
-        if (check_launch("MATVEC x-forward")) return 22;
-        dim3 gy((unsigned)ceil_div(g.Mx, P.ty), (unsigned)P.nplanes, (unsigned)nrs);
-        k_ygreen<T><<<gy, threads, sm_y, stream>>>(P);
-        if (check_launch("MATVEC y-Green")) return 23;
-        k_xinv<T><<<gx, threads, sm_x, stream>>>(P);
-        if (check_launch("MATVEC x-inverse")) return 24;
+        if (fx_r) {
+          if (launch_k<T>(fx_r, dim3((unsigned)ceil_div(g.ny, Rx), (unsigned)P.nplanes, (unsigned)(3 * nrs)), thx, smx_r, stream, P)) return 22;
+        } else {
+          dim3 gx((unsigned)ceil_div(g.ny, P.ry), (unsigned)P.nplanes, (unsigned)(3 * nrs));
+          k_xfwd<T><<<gx, threads, sm_x, stream>>>(P);
+          if (check_launch("MATVEC x-forward")) return 22;
+        }
+        if (fy_r) {
+          if (launch_k<T>(fy_r, dim3((unsigned)nrs, (unsigned)ceil_div(g.Mx, Ly), (unsigned)P.nplanes), thy, smy_r, stream, P)) return 23;
+        } else {
+          dim3 gy((unsigned)ceil_div(g.Mx, P.ty), (unsigned)P.nplanes, (unsigned)nrs);
+          k_ygreen<T><<<gy, threads, sm_y, stream>>>(P);
+          if (check_launch("MATVEC y-Green")) return 23;
+        }
+        if (fxi_r) {
+          if (launch_k<T>(fxi_r, dim3((unsigned)ceil_div(g.ny, Rx), (unsigned)P.nplanes, (unsigned)(3 * nrs)), thx, smx_r, stream, P)) return 24;
+        } else {
+          dim3 gx((unsigned)ceil_div(g.ny, P.ry), (unsigned)P.nplanes, (unsigned)(3 * nrs));
+          k_xinv<T><<<gx, threads, sm_x, stream>>>(P);
+          if (check_launch("MATVEC x-inverse")) return 24;
+        }
       }
     }
-    k_zinv_fin<T><<<gz, threads, sm_z, stream>>>(P);
-    if (check_launch("MATVEC z-inverse/finish")) return 25;
+    if (fzi_r) {
+      if (launch_k<T>(fzi_r, dim3((unsigned)ceil_div(g.nx, Lz), (unsigned)g.ny, (unsigned)(3 * nr)), thz, smz_r, stream, P)) return 25;
+    } else {
+      dim3 gz((unsigned)ceil_div(g.nx, P.tz), (unsigned)g.ny, (unsigned)(3 * nr));
+      k_zinv_fin<T><<<gz, threads, sm_z, stream>>>(P);
+      if (check_launch("MATVEC z-inverse/finish")) return 25;
+    }
   }
   return 0;
 }
 
+template <typename C> __global__ void k_interleave6(const C* src, C* dst, size_t npts) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < 6 * npts; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t m = i / npts, p = i - m * npts;
+    dst[p * 6 + m] = src[i];
+  }
+}
+
+// planar [6][points] (CXZC / build layout) -> point-interleaved [points][6] in `green`
+template <typename T> int Engine<T>::interleave_green(const C* planar_dev) {
+  if (xpipe) return interleave_green_zfast<T>(*this, planar_dev);
+  const size_t npts = g.green_count() / 6;
+  k_interleave6<C><<<(unsigned)std::min<size_t>(ceil_div(6 * npts, 256), 148 * 32), 256, 0, stream>>>(planar_dev, green, npts);
+  return check_launch("Green interleave");
+}
+
 template <typename T> int Engine<T>::upload_green(const void* host_green) {
-  cudaError_t e = cudaMemcpy(green, host_green, g.green_count() * sizeof(C), cudaMemcpyHostToDevice);
-  if (e != cudaSuccess) { set_cuda_error("green H2D", e); return 4; }
+  C* tmp = nullptr;
+  cudaError_t e = cudaMalloc((void**)&tmp, g.green_count() * sizeof(C));
+  if (e == cudaSuccess) e = cudaMemcpy(tmp, host_green, g.green_count() * sizeof(C), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) { cudaFree(tmp); set_cuda_error("green H2D", e); return 4; }
+  int rc = interleave_green(tmp);
+  e = cudaStreamSynchronize(stream);
+  cudaFree(tmp);
+  if (rc || e != cudaSuccess) { if (!rc) set_cuda_error("green interleave", e); return 4; }
   return 0;
 }
 

@@ -1,0 +1,484 @@
+// x-first, transposed-layout MATVEC pipeline for power-of-two grids (sm_100a).
+//
+// Same operator as matvec.cu (cprod_cuda.f90:446-607 / ddscat_matvec_cuda.cu:
+// 104-118), organised so that every pass transforms along the contiguous axis
+// of its input with the T threads of a line inside one warp (register line
+// FFTs, fftreg.cuh), and the axis change is done by a shared-memory tile
+// transpose on the load or store side, keeping global accesses in 128-byte
+// segments:
+//   XF : x (compact or full) rows  -> x-FFT(+i), pad-skip -> A[c][iz][kx][iy]
+//   YF : A y-rows (n_y)            -> y-FFT(+i)           -> B[c][kx][ky][iz]
+//   ZG : B z-rows (n_z)            -> z-FFT(+i) * Green * z-FFT(-i), keep n_z
+//   YI : B (transposed load)       -> y-FFT(-i), keep n_y -> A
+//   XI : A (transposed load)       -> x-FFT(-i), keep n_x -> finish -> y
+// The Green octant is stored z-fastest, [irx][iry][irz][6], so a z-line reads
+// contiguous 48-byte records, and each record is loaded once for kz and its
+// mirror M_z - kz.  The ZG grid runs RHS-fastest so consecutive blocks reuse
+// the Green tile from L2.  The middle passes run over kx batches (all of M_x for
+// the FFT3D build, 4 columns for the SLICES build).
+#include <algorithm>
+#include <cstdlib>
+#include "engine.h"
+#include "fftreg.cuh"
+
+namespace ddb {
+
+template <typename T> struct XParams {
+  int nx, ny, nz, Mx, My, Mz, nat, nat0;
+  const cplx<T>* x;
+  size_t x_rs;
+  cplx<T>* y;
+  size_t y_rs;
+  const cplx<T>* adia;
+  const cplx<T>* aoff;
+  size_t a_rs;
+  int io_full, a_full, conj;
+  const int* inv;
+  const int16_t* iocc;
+  const int* mask;
+  int rhs0;
+  cplx<T>* A;  // [rl][c][iz][kx][iy]
+  size_t A_rs;
+  cplx<T>* B;  // [rb][c][kxl][ky][iz] for kx in [kx0, kx0 + nkx)
+  int kx0, nkx, b_rhs0;
+  const cplx<T>* green;  // [irx][iry][irz][6] (IPBC=0) or [kx][ky][kz][6] (IPBC=1)
+  int ipbc;
+  const cplx<T>* twx;
+  const cplx<T>* twy;
+  const cplx<T>* twz;
+  int lsx, lsy, lsz;  // line strides of the x, y, z passes
+  T inv_ngrid;
+};
+
+template <typename T> __device__ __forceinline__ bool xoff(const XParams<T>& P, int rl) {
+  return P.mask != nullptr && P.mask[P.rhs0 + rl] == 0;
+}
+
+template <typename T, int N> __device__ __forceinline__ void load_tw(cplx<T>* tws, const cplx<T>* tw) {
+  for (int u = threadIdx.x; u < N; u += blockDim.x) tws[u] = tw[u];
+}
+
+// ------------------------------------------------------------- XF: x forward
+// block: RL rows (iy) x T threads, thread-fastest; grid (ceil(ny/RL), nz, 3*nr)
+template <typename T, int N> __global__ void __launch_bounds__(256) kx_xf(XParams<T> P) {
+  using C = cplx<T>;
+  constexpr int E = RegShape<N>::E, TT = RegShape<N>::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int RL = blockDim.x / TT, t = threadIdx.x % TT, l = threadIdx.x / TT;
+  C* tws = reinterpret_cast<C*>(smem_raw);
+  C* tile = tws + N;                        // [kx][RL+1]
+  C* lines = tile + (size_t)N * (RL + 1);   // RL * lsx
+  const int iy0 = blockIdx.x * RL, iy = iy0 + l, iz = blockIdx.y;
+  const int rl = blockIdx.z / 3, c = blockIdx.z % 3;
+  if (xoff(P, rl)) return;
+  load_tw<T, N>(tws, P.twx);
+  __syncthreads();
+  const C* x = P.x + (size_t)rl * P.x_rs;
+  const size_t S = P.io_full ? (size_t)P.nat : (size_t)P.nat0;
+  C v[E];
+#pragma unroll
+  for (int i = 0; i < E; ++i) {
+    const int ix = t + TT * i;
+    v[i] = mk<C>(0, 0);
+    if (ix < P.nx && iy < P.ny) {
+      const size_t j = (size_t)ix + (size_t)P.nx * ((size_t)iy + (size_t)P.ny * iz);
+      if (P.io_full) {
+        v[i] = x[c * S + j];
+      } else {
+        const int q = P.inv[j];
+        if (q >= 0) v[i] = x[c * S + q];
+      }
+      if (P.conj) v[i].y = -v[i].y;
+    }
+  }
+  line_fft<E, TT, +1, false>(v, lines + (size_t)l * P.lsx, t, tws);
+#pragma unroll
+  for (int i = 0; i < E; ++i) tile[(t + TT * i) * (RL + 1) + l] = v[i];
+  __syncthreads();
+  C* A = P.A + (size_t)rl * P.A_rs + (((size_t)c * P.nz + iz) * P.Mx) * P.ny;
+  for (int u = threadIdx.x; u < N * RL; u += blockDim.x) {
+    const int kx = u / RL, ll = u % RL;
+    if (iy0 + ll < P.ny) A[(size_t)kx * P.ny + iy0 + ll] = tile[kx * (RL + 1) + ll];
+  }
+}
+
+// ------------------------------------------------------------- YF: y forward
+// block: RL z-lines (iz) x T; grid (ceil(nz/RL), nkx, 3*nrb)
+template <typename T, int N> __global__ void __launch_bounds__(256) kx_yf(XParams<T> P) {
+  using C = cplx<T>;
+  constexpr int E = RegShape<N>::E, TT = RegShape<N>::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int RL = blockDim.x / TT, t = threadIdx.x % TT, l = threadIdx.x / TT;
+  C* tws = reinterpret_cast<C*>(smem_raw);
+  C* tile = tws + N;
+  C* lines = tile + (size_t)N * (RL + 1);
+  const int iz0 = blockIdx.x * RL, iz = iz0 + l, kxl = blockIdx.y, kx = P.kx0 + kxl;
+  const int rb = blockIdx.z / 3, c = blockIdx.z % 3, rl = P.b_rhs0 + rb;
+  if (xoff(P, rl)) return;
+  load_tw<T, N>(tws, P.twy);
+  __syncthreads();
+  const C* A = P.A + (size_t)rl * P.A_rs + (((size_t)c * P.nz + iz) * P.Mx + kx) * P.ny;
+  C v[E];
+#pragma unroll
+  for (int i = 0; i < E; ++i) {
+    const int iy = t + TT * i;
+    v[i] = (iy < P.ny && iz < P.nz) ? A[iy] : mk<C>(0, 0);
+  }
+  line_fft<E, TT, +1, false>(v, lines + (size_t)l * P.lsy, t, tws);
+#pragma unroll
+  for (int i = 0; i < E; ++i) tile[(t + TT * i) * (RL + 1) + l] = v[i];
+  __syncthreads();
+  C* B = P.B + (((size_t)rb * 3 + c) * P.nkx + kxl) * (size_t)P.My * P.nz;
+  for (int u = threadIdx.x; u < N * RL; u += blockDim.x) {
+    const int ky = u / RL, ll = u % RL;
+    if (iz0 + ll < P.nz) B[(size_t)ky * P.nz + iz0 + ll] = tile[ky * (RL + 1) + ll];
+  }
+}
+
+// Green record at (kx, ky, kz) for the z-fastest layout, without the kz sign.
+template <typename T>
+__device__ __forceinline__ const cplx<T>* green_rec(const XParams<T>& P, int kx, int ky, int kz, T& sxy, T& sxz,
+                                                    T& syz) {
+  size_t b;
+  if (P.ipbc == 0) {
+    const T sx = kx <= P.nx ? (T)1 : (T)-1, sy = ky <= P.ny ? (T)1 : (T)-1;
+    const int irx = min(kx, P.Mx - kx), iry = min(ky, P.My - ky);
+    b = ((size_t)irx * (P.ny + 1) + iry) * (P.nz + 1) + kz;
+    sxy = sx * sy; sxz = sx; syz = sy;  // times sz, applied by the caller
+  } else {
+    b = ((size_t)kx * P.My + ky) * P.Mz + kz;
+    sxy = sxz = syz = (T)1;
+  }
+  return P.green + 6 * b;
+}
+
+template <typename T> __device__ __forceinline__ void load_rec(const cplx<T>* gp, cplx<T> a[6]) {
+  if constexpr (sizeof(cplx<T>) == 8) {
+    const float4* g4 = reinterpret_cast<const float4*>(gp);
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      const float4 q = __ldg(g4 + m);
+      a[2 * m] = mk<cplx<T>>(q.x, q.y);
+      a[2 * m + 1] = mk<cplx<T>>(q.z, q.w);
+    }
+  } else {
+#pragma unroll
+    for (int m = 0; m < 6; ++m) a[m] = gp[m];
+  }
+}
+
+template <typename C, typename R>
+__device__ __forceinline__ void green_apply(const C a[6], R sxy, R sxz, R syz, C& px, C& py, C& pz) {
+  const C a12 = cscale(a[1], sxy), a13 = cscale(a[2], sxz), a23 = cscale(a[4], syz);
+  const C x = px, y = py, z = pz;
+  px = cadd(cadd(cmul(a[0], x), cmul(a12, y)), cmul(a13, z));
+  py = cadd(cadd(cmul(a12, x), cmul(a[3], y)), cmul(a23, z));
+  pz = cadd(cadd(cmul(a13, x), cmul(a23, y)), cmul(a[5], z));
+}
+
+// ------------------------------------------------------------- ZG: z * Green * z^-1
+// block: RL lines x T threads x 3 components, thread-fastest within a line;
+// lines are (kx, ky) pairs p = kxl*My + ky.  grid (nrb, ceil(nkx*My/RL))
+template <typename T, int N> __global__ void __launch_bounds__(384) kx_zg(XParams<T> P) {
+  using C = cplx<T>;
+  using R = T;
+  constexpr int E = RegShape<N>::E, TT = RegShape<N>::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int RL = blockDim.x / (3 * TT);
+  const int t = threadIdx.x % TT, l = (threadIdx.x / TT) % RL, c = threadIdx.x / (TT * RL);
+  C* tws = reinterpret_cast<C*>(smem_raw);
+  C* lines = tws + N;  // [3][RL][lsz]
+  C* my = lines + (size_t)(c * RL + l) * P.lsz;
+  const int rb = blockIdx.x, rl = P.b_rhs0 + rb;
+  if (xoff(P, rl)) return;
+  load_tw<T, N>(tws, P.twz);
+  __syncthreads();
+  const int nlines = P.nkx * P.My;
+  const int p = blockIdx.y * RL + l;
+  const bool live = p < nlines;
+  C* row = P.B + (((size_t)rb * 3 + c) * P.nkx) * (size_t)P.My * P.nz + (size_t)p * P.nz;
+  C v[E];
+#pragma unroll
+  for (int i = 0; i < E; ++i) {
+    const int iz = t + TT * i;
+    v[i] = (live && iz < P.nz) ? row[iz] : mk<C>(0, 0);
+  }
+  line_fft<E, TT, +1, false>(v, my, t, tws);
+#pragma unroll
+  for (int i = 0; i < E; ++i) my[t + TT * i] = v[i];
+  __syncthreads();
+  // Green: one thread per (line, kz <= Mz/2); the record serves kz and Mz-kz
+  const int half = N / 2 + 1;
+  for (int u = threadIdx.x; u < RL * half; u += blockDim.x) {
+    const int ll = u / half, kz = u % half, pl = blockIdx.y * RL + ll;
+    if (pl >= nlines) continue;
+    const int kx = P.kx0 + pl / P.My, ky = pl % P.My;
+    R sxy, sxz, syz;
+    C a[6];
+    load_rec<T>(green_rec(P, kx, ky, kz, sxy, sxz, syz), a);
+    C* L0 = lines + (size_t)ll * P.lsz;
+    C* L1 = L0 + (size_t)RL * P.lsz;
+    C* L2 = L1 + (size_t)RL * P.lsz;
+    if (P.ipbc == 0) {
+      green_apply(a, sxy, sxz, syz, L0[kz], L1[kz], L2[kz]);  // kz <= nz: sz = +1
+      const int km = N - kz;
+      if (kz > 0 && km != kz) green_apply(a, sxy, -sxz, -syz, L0[km], L1[km], L2[km]);  // sz = -1
+    } else {
+      green_apply(a, sxy, sxz, syz, L0[kz], L1[kz], L2[kz]);
+      const int km = N - kz;
+      if (kz > 0 && km != kz) {
+        load_rec<T>(green_rec(P, kx, ky, km, sxy, sxz, syz), a);
+        green_apply(a, sxy, sxz, syz, L0[km], L1[km], L2[km]);
+      }
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < E; ++i) v[i] = my[t + TT * i];
+  __syncwarp();
+  line_fft<E, TT, -1, false>(v, my, t, tws);
+  if (live) {
+#pragma unroll
+    for (int i = 0; i < E; ++i) {
+      const int iz = t + TT * i;
+      if (iz < P.nz) row[iz] = v[i];
+    }
+  }
+}
+
+// ------------------------------------------------------------- YI: y inverse
+// block: RL z-lines x T; grid (ceil(nz/RL), nkx, 3*nrb)
+template <typename T, int N> __global__ void __launch_bounds__(256) kx_yi(XParams<T> P) {
+  using C = cplx<T>;
+  constexpr int E = RegShape<N>::E, TT = RegShape<N>::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int RL = blockDim.x / TT, t = threadIdx.x % TT, l = threadIdx.x / TT;
+  C* tws = reinterpret_cast<C*>(smem_raw);
+  C* tile = tws + N;
+  C* lines = tile + (size_t)N * (RL + 1);
+  const int iz0 = blockIdx.x * RL, iz = iz0 + l, kxl = blockIdx.y, kx = P.kx0 + kxl;
+  const int rb = blockIdx.z / 3, c = blockIdx.z % 3, rl = P.b_rhs0 + rb;
+  if (xoff(P, rl)) return;
+  load_tw<T, N>(tws, P.twy);
+  const C* B = P.B + (((size_t)rb * 3 + c) * P.nkx + kxl) * (size_t)P.My * P.nz;
+  for (int u = threadIdx.x; u < N * RL; u += blockDim.x) {
+    const int ky = u / RL, ll = u % RL;
+    tile[ky * (RL + 1) + ll] = (iz0 + ll < P.nz) ? B[(size_t)ky * P.nz + iz0 + ll] : mk<C>(0, 0);
+  }
+  __syncthreads();
+  C v[E];
+#pragma unroll
+  for (int i = 0; i < E; ++i) v[i] = tile[(t + TT * i) * (RL + 1) + l];
+  line_fft<E, TT, -1, false>(v, lines + (size_t)l * P.lsy, t, tws);
+  if (iz < P.nz) {
+    C* A = P.A + (size_t)rl * P.A_rs + (((size_t)c * P.nz + iz) * P.Mx + kx) * P.ny;
+#pragma unroll
+    for (int i = 0; i < E; ++i) {
+      const int iy = t + TT * i;
+      if (iy < P.ny) A[iy] = v[i];
+    }
+  }
+}
+
+// ------------------------------------------------------------- XI: x inverse + finish
+template <typename T>
+__device__ __forceinline__ void xfinish(const XParams<T>& P, int rl, int c, int ix, int iy, int iz, cplx<T> wraw) {
+  using C = cplx<T>;
+  const C* x = P.x + (size_t)rl * P.x_rs;
+  C* y = P.y + (size_t)rl * P.y_rs;
+  const C* ad = P.adia + (size_t)rl * P.a_rs;
+  const C* ao = P.aoff ? P.aoff + (size_t)rl * P.a_rs : nullptr;
+  const size_t S = P.io_full ? (size_t)P.nat : (size_t)P.nat0;
+  const size_t SA = P.a_full ? (size_t)P.nat : (size_t)P.nat0;
+  const size_t j = (size_t)ix + (size_t)P.nx * ((size_t)iy + (size_t)P.ny * iz);
+  size_t q;
+  if (P.io_full) {
+    q = j;
+    if (P.iocc[j] == 0) { y[c * S + q] = mk<C>(0, 0); return; }
+  } else {
+    const int qq = P.inv[j];
+    if (qq < 0) return;
+    q = (size_t)qq;
+  }
+  const size_t qa = P.a_full ? j : q;
+  C xc = x[c * S + q];
+  if (P.conj) xc.y = -xc.y;
+  C yv = csub(cmul(ad[c * SA + qa], xc), cscale(wraw, P.inv_ngrid));
+  if (ao) {
+    C x1 = x[q], x2 = x[S + q], x3 = x[2 * S + q];
+    if (P.conj) { x1.y = -x1.y; x2.y = -x2.y; x3.y = -x3.y; }
+    const C a23 = ao[qa], a31 = ao[SA + qa], a12 = ao[2 * SA + qa];
+    if (c == 0) yv = cadd(yv, cadd(cmul(a31, x3), cmul(a12, x2)));
+    else if (c == 1) yv = cadd(yv, cadd(cmul(a12, x1), cmul(a23, x3)));
+    else yv = cadd(yv, cadd(cmul(a23, x2), cmul(a31, x1)));
+  }
+  if (P.conj) yv.y = -yv.y;
+  y[c * S + q] = yv;
+}
+
+// block: RL rows (iy) x T; grid (ceil(ny/RL), nz, 3*nr)
+template <typename T, int N> __global__ void __launch_bounds__(256) kx_xi(XParams<T> P) {
+  using C = cplx<T>;
+  constexpr int E = RegShape<N>::E, TT = RegShape<N>::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int RL = blockDim.x / TT, t = threadIdx.x % TT, l = threadIdx.x / TT;
+  C* tws = reinterpret_cast<C*>(smem_raw);
+  C* tile = tws + N;
+  C* lines = tile + (size_t)N * (RL + 1);
+  const int iy0 = blockIdx.x * RL, iy = iy0 + l, iz = blockIdx.y;
+  const int rl = blockIdx.z / 3, c = blockIdx.z % 3;
+  if (xoff(P, rl)) return;
+  load_tw<T, N>(tws, P.twx);
+  const C* A = P.A + (size_t)rl * P.A_rs + (((size_t)c * P.nz + iz) * P.Mx) * P.ny;
+  for (int u = threadIdx.x; u < N * RL; u += blockDim.x) {
+    const int kx = u / RL, ll = u % RL;
+    tile[kx * (RL + 1) + ll] = (iy0 + ll < P.ny) ? A[(size_t)kx * P.ny + iy0 + ll] : mk<C>(0, 0);
+  }
+  __syncthreads();
+  C v[E];
+#pragma unroll
+  for (int i = 0; i < E; ++i) v[i] = tile[(t + TT * i) * (RL + 1) + l];
+  line_fft<E, TT, -1, false>(v, lines + (size_t)l * P.lsx, t, tws);
+  if (iy < P.ny) {
+#pragma unroll
+    for (int i = 0; i < E; ++i) {
+      const int ix = t + TT * i;
+      if (ix < P.nx) xfinish(P, rl, c, ix, iy, iz, v[i]);
+    }
+  }
+}
+
+// ------------------------------------------------------------- host side
+enum class XPass { XF, YF, ZG, YI, XI };
+
+template <typename T, int N> static const void* xk(XPass p) {
+  switch (p) {
+    case XPass::XF: return (const void*)kx_xf<T, N>;
+    case XPass::YF: return (const void*)kx_yf<T, N>;
+    case XPass::ZG: return (const void*)kx_zg<T, N>;
+    case XPass::YI: return (const void*)kx_yi<T, N>;
+    default: return (const void*)kx_xi<T, N>;
+  }
+}
+
+template <typename T> static const void* xkernel(XPass p, int n) {
+  switch (n) {
+    case 16: return xk<T, 16>(p);
+    case 32: return xk<T, 32>(p);
+    case 64: return xk<T, 64>(p);
+    case 128: return xk<T, 128>(p);
+    case 256: return xk<T, 256>(p);
+    case 512: return xk<T, 512>(p);
+    default: return nullptr;
+  }
+}
+
+static int rT(int n) { return n <= 32 ? 4 : (n <= 128 ? 8 : 16); }
+
+template <typename T> static int xlaunch(const void* f, dim3 g, int th, size_t sm, cudaStream_t st, XParams<T>& P) {
+  static std::vector<const void*> raised;
+  if (std::find(raised.begin(), raised.end(), f) == raised.end()) {
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    raised.push_back(f);
+  }
+  void* args[] = {(void*)&P};
+  cudaError_t e = cudaLaunchKernel(f, g, dim3(th), args, sm, st);
+  if (e != cudaSuccess) { set_cuda_error("MATVEC launch", e); return 1; }
+  return 0;
+}
+
+template <typename T> bool xpipe_supported(const Geometry& g) {
+  if (std::getenv("DDSCAT_B200_ZFIRST")) return false;
+  if (sizeof(T) == 8) return false;  // the FP64 engine keeps the generic z-first pipeline
+  auto ok = [](int n) { return reg_supported(n); };
+  return ok(g.Mx) && ok(g.My) && ok(g.Mz);
+}
+
+template <typename T>
+int matvec_xpipe(Engine<T>& E, const MvArgs<T>& a) {
+  using C = cplx<T>;
+  const Geometry& g = E.g;
+  XParams<T> P{};
+  P.nx = g.nx; P.ny = g.ny; P.nz = g.nz; P.Mx = g.Mx; P.My = g.My; P.Mz = g.Mz;
+  P.nat = g.nat; P.nat0 = g.nat0;
+  P.x_rs = a.x_rs; P.y_rs = a.y_rs; P.a_rs = a.a_rs;
+  P.io_full = a.io_full; P.a_full = a.a_full; P.conj = a.conj;
+  P.inv = E.inv; P.iocc = E.iocc; P.mask = a.mask;
+  P.A = E.zhat; P.A_rs = (size_t)3 * g.nz * g.Mx * g.ny;
+  P.B = E.slab;
+  P.green = E.green; P.ipbc = g.ipbc;
+  P.twx = E.twx; P.twy = E.twy; P.twz = E.twz;
+  P.inv_ngrid = (T)(1.0 / (double)g.ngrid());
+  const int TX = rT(g.Mx), TY = rT(g.My), TZ = rT(g.Mz);
+  const int RX = 256 / TX, RY = 256 / TY;
+  const int RZ = std::max(1, 128 / TZ);  // ZG: 3*TZ*RZ threads
+  P.lsx = line_stride(g.Mx / TX, TX, RX, false);
+  P.lsy = line_stride(g.My / TY, TY, RY, false);
+  P.lsz = std::max(line_stride(g.Mz / TZ, TZ, RZ, false), g.Mz);
+  const size_t smx = ((size_t)g.Mx + (size_t)g.Mx * (RX + 1) + (size_t)RX * P.lsx) * sizeof(C);
+  const size_t smy = ((size_t)g.My + (size_t)g.My * (RY + 1) + (size_t)RY * P.lsy) * sizeof(C);
+  const size_t smz = ((size_t)g.Mz + (size_t)3 * RZ * P.lsz) * sizeof(C);
+  const void* fxf = xkernel<T>(XPass::XF, g.Mx);
+  const void* fyf = xkernel<T>(XPass::YF, g.My);
+  const void* fzg = xkernel<T>(XPass::ZG, g.Mz);
+  const void* fyi = xkernel<T>(XPass::YI, g.My);
+  const void* fxi = xkernel<T>(XPass::XI, g.Mx);
+  for (int r0 = 0; r0 < a.nrhs; r0 += E.zcap) {
+    const int nr = std::min(E.zcap, a.nrhs - r0);
+    P.rhs0 = r0;
+    P.x = a.x + (size_t)r0 * a.x_rs;
+    P.y = a.y + (size_t)r0 * a.y_rs;
+    P.adia = a.adia + (size_t)r0 * a.a_rs;
+    P.aoff = a.aoff ? a.aoff + (size_t)r0 * a.a_rs : nullptr;
+    if (xlaunch<T>(fxf, dim3((unsigned)ceil_div(g.ny, RX), (unsigned)g.nz, (unsigned)(3 * nr)), 256, smx, E.stream, P))
+      return 21;
+    for (int rb0 = 0; rb0 < nr; rb0 += E.slab_nr) {
+      const int nrb = std::min(E.slab_nr, nr - rb0);
+      P.b_rhs0 = rb0;
+      for (int kx0 = 0; kx0 < g.Mx; kx0 += E.slab_B) {
+        P.kx0 = kx0;
+        P.nkx = std::min(E.slab_B, g.Mx - kx0);
+        if (xlaunch<T>(fyf, dim3((unsigned)ceil_div(g.nz, RY), (unsigned)P.nkx, (unsigned)(3 * nrb)), 256, smy,
+                       E.stream, P))
+          return 22;
+        if (xlaunch<T>(fzg, dim3((unsigned)nrb, (unsigned)ceil_div((size_t)P.nkx * g.My, RZ)), 3 * TZ * RZ, smz,
+                       E.stream, P))
+          return 23;
+        if (xlaunch<T>(fyi, dim3((unsigned)ceil_div(g.nz, RY), (unsigned)P.nkx, (unsigned)(3 * nrb)), 256, smy,
+                       E.stream, P))
+          return 24;
+      }
+    }
+    if (xlaunch<T>(fxi, dim3((unsigned)ceil_div(g.ny, RX), (unsigned)g.nz, (unsigned)(3 * nr)), 256, smx, E.stream, P))
+      return 25;
+  }
+  return 0;
+}
+
+// planar [6][Z][Y][X] (build / CXZC layout) -> [X][Y][Z][6]
+template <typename C> __global__ void k_interleave6_zfast(const C* src, C* dst, int X, int Y, int Z) {
+  const size_t npts = (size_t)X * Y * Z;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < 6 * npts; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t m = i / npts, p = i - m * npts;
+    const size_t ix = p % X, iy = (p / X) % Y, iz = p / ((size_t)X * Y);
+    dst[((ix * Y + iy) * Z + iz) * 6 + m] = src[i];
+  }
+}
+
+template <typename T> int interleave_green_zfast(Engine<T>& E, const cplx<T>* planar) {
+  const Geometry& g = E.g;
+  const int X = g.ipbc == 0 ? g.nx + 1 : g.Mx, Y = g.ipbc == 0 ? g.ny + 1 : g.My, Z = g.ipbc == 0 ? g.nz + 1 : g.Mz;
+  const size_t n = (size_t)6 * X * Y * Z;
+  k_interleave6_zfast<cplx<T>><<<(unsigned)std::min<size_t>(ceil_div(n, 256), 148 * 32), 256, 0, E.stream>>>(
+      planar, E.green, X, Y, Z);
+  return check_launch("Green interleave (z-fastest)");
+}
+
+template bool xpipe_supported<float>(const Geometry&);
+template bool xpipe_supported<double>(const Geometry&);
+template int matvec_xpipe<float>(Engine<float>&, const MvArgs<float>&);
+template int matvec_xpipe<double>(Engine<double>&, const MvArgs<double>&);
+template int interleave_green_zfast<float>(Engine<float>&, const float2*);
+template int interleave_green_zfast<double>(Engine<double>&, const double2*);
+
+}  // namespace ddb

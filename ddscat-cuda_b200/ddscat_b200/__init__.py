@@ -26,7 +26,7 @@ EXPORTS = (
     ["ddscat_cuda_prepare_green_f32", "ddscat_cuda_prepare_f32", "ddscat_cuda_apply_f32"]
     + [f"ddscat_cuda_solve_{s}_f32" for s in SOLVERS]
     + ["ddscat_cuda_evalq_f32", "ddscat_cuda_scat_f32", "ddscat_cuda_release", "ddscat_cuda_last_error"]
-    + ["ddscat_b200_set_verbose", "ddscat_b200_layout"]
+    + ["ddscat_b200_set_verbose", "ddscat_b200_layout", "ddscat_b200_matvec_timing"]
 )
 
 
@@ -75,6 +75,8 @@ def _declare(lib):
     lib.ddscat_b200_set_verbose.restype = _I
     lib.ddscat_b200_layout.argtypes = []
     lib.ddscat_b200_layout.restype = _I
+    lib.ddscat_b200_matvec_timing.argtypes = [_I, _I, _I, ct.POINTER(_F)]
+    lib.ddscat_b200_matvec_timing.restype = _I
 
 
 _LIBS = {}
@@ -196,6 +198,11 @@ class DDA:
         self._check("scat", rc)
         return {"cbksca": cb.value, "csca": cs.value, "cscag": [cg[0], cg[1], cg[2]], "cscag2": cg2.value,
                 "navg": navg.value, "f1": f1[:ndir], "f2": f2[:ndir]}
+
+    def matvec_ms(self, nrhs=1, iters=10, cwhat="N"):
+        ms = _F(0.0)
+        self._check("matvec_timing", self.lib.ddscat_b200_matvec_timing(nrhs, iters, ord(cwhat), ct.byref(ms)))
+        return ms.value
 
     def release(self):
         return self.lib.ddscat_cuda_release()

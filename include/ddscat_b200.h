@@ -19,6 +19,13 @@ DDSCAT_CUDA_API int ddscat_b200_set_verbose(int level);
  * (libddscat_matvec_cuda_slice.so). */
 DDSCAT_CUDA_API int ddscat_b200_layout(void);
 
+/* Times the device-resident MATVEC of the prepared target: nrhs right-hand
+ * sides per call (compact layout, per-RHS CXADIA, no CXAOFF), `iters` calls
+ * after 3 warm-up calls, CUDA events on the library stream.  Writes the mean
+ * milliseconds per call.  Allocates its own scratch vectors.  Codes: 400
+ * invalid / not prepared, 401 allocation, 402 CUDA failure. */
+DDSCAT_CUDA_API int ddscat_b200_matvec_timing(int nrhs, int iters, int cwhat, float *ms_per_call);
+
 #ifdef __cplusplus
 }
 #endif

@@ -38,7 +38,8 @@ def _err(y, yr):
 @pytest.mark.parametrize("layout", ["fft3d", "slices"])
 @pytest.mark.parametrize("dims,idipint", [((4, 4, 4), 0), ((5, 3, 4), 0), ((6, 5, 7), 1), ((7, 11, 13), 0),
                                           ((8, 8, 8), 0), ((12, 10, 9), 1), ((16, 16, 16), 0), ((24, 18, 30), 0),
-                                          ((32, 32, 32), 0)])
+                                          ((32, 32, 32), 0), ((16, 8, 32), 1), ((64, 32, 16), 0), ((8, 64, 16), 0),
+                                          ((128, 16, 8), 1), ((64, 64, 64), 0)])
 def test_apply_matches_oracle(layout, dims, idipint):
     iocc, ak, x, adia, aoff, gp = _case(dims, idipint)
     dda = D.DDA(layout)
@@ -55,8 +56,8 @@ def test_apply_matches_oracle(layout, dims, idipint):
 
 
 @pytest.mark.gpu
-def test_prepare_with_cpu_green_matches_gpu_green():
-    dims = (10, 9, 8)
+@pytest.mark.parametrize("dims", [(10, 9, 8), (16, 8, 8)])
+def test_prepare_with_cpu_green_matches_gpu_green(dims):
     iocc, ak, x, adia, aoff, gp = _case(dims, 0, seed=5)
     dda = D.DDA()
     dda.prepare_green(*dims, iocc, ak)
@@ -71,11 +72,12 @@ def test_prepare_with_cpu_green_matches_gpu_green():
 
 
 @pytest.mark.gpu
-def test_pbc_green_matches_oracle():
-    """IPBC=1 (periodic in y): full-tensor Green build and MATVEC branch."""
-    dims = (4, 3, 3)
+@pytest.mark.parametrize("dims", [(4, 3, 3), (8, 8, 8)])
+def test_pbc_green_matches_oracle(dims):
+    """IPBC=1 (periodic in y): full-tensor Green build and MATVEC branch
+    (a generic-length grid and a power-of-two grid)."""
     rng = np.random.default_rng(2)
-    nat = 36
+    nat = int(np.prod(dims))
     iocc = np.ones(nat, dtype=np.int16)
     ak = (0.6, 0.25, 0.0)
     x = (rng.normal(size=3 * nat) + 1j * rng.normal(size=3 * nat)).astype(np.complex64)
