@@ -1,0 +1,447 @@
+#!/usr/bin/env python3
+"""Benchmark of the DDA solve hot path: time-to-residual 1e-5 per right-hand
+side, FP64-checked, on the 128^3 sphere workload (m = 1.33+0.05i, x = 20,
+QMRCCG, tol 1e-5).
+
+A step solves one batch of R right-hand sides (orientations x 2 polarisations,
+Euler angles uniform on SO(3) from a per-rank seed) until every RHS has an
+FP64-recomputed true residual ||b - A x|| / ||b|| <= tol (RHS that pass the
+FP32-MATVEC check but not the FP64 one are re-solved from their current x with
+a tighter tolerance inside the step).  `value` is RHS per second with inputs
+resident in HBM; `e2e` is the same metric through the C ABI with pinned host
+buffers (H2D of b, x0, CXADIA and D2H of x inside the timed region).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference implementation of the path: the
+reference CUDA library built unmodified from its sources (oracle/_ref), called
+through its own C ABI one RHS at a time, on the same inputs.
+"""
+import argparse
+import contextlib
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "ddscat-cuda_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "time-to-residual 1e-5 per RHS (FP64-checked), as RHS solved per second"
+UNIT = "RHS/s"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=128)
+    ap.add_argument("--orient", type=int, default=8, help="orientations per rank (x2 polarisations = RHS per step)")
+    ap.add_argument("--solver", default="qmrccg", choices=["qmrccg", "pbcgs2"])
+    ap.add_argument("--tol", type=float, default=1e-5)
+    ap.add_argument("--maxit", type=int, default=4000)
+    ap.add_argument("--ref-rhs", type=int, default=2, help="RHS per step of the reference arm")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ helpers
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-f", self.path], stdout=subprocess.DEVNULL,
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9 or not f[0].isdigit() or int(f[0]) != self.idx:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+@contextlib.contextmanager
+def quiet_stdout():
+    """Silence C-level stdout (the reference library prints per-MATVEC lines)."""
+    sys.stdout.flush()
+    saved = os.dup(1)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    try:
+        yield
+    finally:
+        sys.stdout.flush()
+        os.dup2(saved, 1)
+        os.close(devnull)
+        os.close(saved)
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    return world, rank, local, pg
+
+
+def barrier(pg, local):
+    if pg is not None:
+        pg.barrier(device_ids=[local])
+
+
+def max_over_ranks(pg, value):
+    if pg is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def workload(args, rank):
+    from ddscat_b200 import targets
+
+    orients = targets.random_orientations(args.orient, seed=1000 + rank)
+    prob = targets.make_problem(args.n, m=1.33 + 0.05j, x=20.0, orientations=orients)
+    R = len(prob.incid)
+    b = np.stack([prob.rhs(r) for r in range(R)])
+    adia = np.stack([prob.adia(r) for r in range(R)])
+    return prob, b, adia
+
+
+def config(args, prob, R, world):
+    return {"workload": f"{args.n}^3 sphere, m=1.33+0.05i, x=20, {args.solver.upper()} tol {args.tol:g}, "
+                        f"{args.orient} orientations x 2 polarisations per rank",
+            "n": args.n, "nat": prob.nat, "nat0": prob.nat0, "rhs_per_rank": R, "solver": args.solver,
+            "tol": args.tol, "fp64_check": "GPU all-FP64 MATVEC true residual, every RHS, every step",
+            "l2": "inputs larger than L2 (each RHS vector 3*NAT*8 B > 50 MB; working set > 1 GB)",
+            "parallelism": f"replicas x{world} (independent RHS batches per GPU)"}
+
+
+def algorithmic_bytes_per_matvec(prob, rhs_per_call):
+    """8 B x [4*3*Mx*My*nz + 12*NAT0 + 6*(nx+1)(ny+1)(nz+1)/R] per RHS MATVEC:
+    the half-padded spectrum round trip, x/y/CXADIA/CXAOFF, and the Green octant
+    amortised over the RHS of one batched MATVEC."""
+    nx, ny, nz = prob.nx, prob.ny, prob.nz
+    return 8.0 * (12.0 * (2 * nx) * (2 * ny) * nz + 12.0 * prob.nat0 +
+                  6.0 * (nx + 1) * (ny + 1) * (nz + 1) / max(rhs_per_call, 1.0))
+
+
+def load_profile_traffic(n):
+    """DRAM bytes per RHS-MATVEC from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", f"matvec_{n}cubed_ncu.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_rhs_matvec:"):
+            try:
+                return float(line.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        return float(json.load(open(path))["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_baseline(prob, ncompte_mean):
+    """CPU restatement (the oracle, test infrastructure) timed on the host:
+    a bounded sample of 3 MATVECs of the complex64 FFT operator at the full
+    size (scipy.fft on all host threads, a random Green spectrum of the true
+    shape), scaled by the GPU run's mean MATVEC count per RHS."""
+    from oracle import ddscat_oracle as O
+
+    nx, ny, nz = prob.nx, prob.ny, prob.nz
+    rng = np.random.default_rng(0)
+    shape = (6, 2 * nz, 2 * ny, 2 * nx)
+    g = (rng.standard_normal(shape, dtype=np.float32) + 1j * rng.standard_normal(shape, dtype=np.float32))
+    op = O.Operator(nx, ny, nz, g.astype(np.complex64), prob.iocc, dtype=np.complex64)
+    occ = op.occ
+    xc = O.gather_compact(prob.rhs(0), occ, prob.nat).astype(np.complex64)
+    ac = O.gather_compact(prob.adia(0), occ, prob.nat).astype(np.complex64)
+    oc = np.zeros_like(ac)
+    op.apply_compact(xc, ac, oc)  # warm-up (plans, page faults)
+    t0 = time.perf_counter()
+    nmv = 3
+    for _ in range(nmv):
+        op.apply_compact(xc, ac, oc)
+    t_mv = (time.perf_counter() - t0) / nmv
+    per_rhs = t_mv * ncompte_mean
+    return {"value": 1.0 / per_rhs, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+            "sample": f"{nmv} MATVECs of the complex64 oracle FFT operator at {nx}^3 (scipy.fft, "
+                      f"{os.cpu_count()} threads), {t_mv:.3f} s each, scaled by {ncompte_mean:.1f} MATVECs per RHS"}
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(args):
+    import torch
+
+    import ddscat_b200 as D
+
+    world, rank, local, pg = dist_init()
+    prob, b, adia = workload(args, rank)
+    R = b.shape[0]
+    dda = D.DDA("fft3d")
+    dda.prepare_green(prob.nx, prob.ny, prob.nz, prob.iocc, prob.incid[0].k)
+    dev = torch.device("cuda", local)
+    bd = torch.from_numpy(b).to(dev)
+    ad = torch.from_numpy(adia).to(dev)
+    xd = torch.zeros_like(bd)
+    stats = {"iters": [], "ncompte": [], "res64": [], "resolves": 0, "mv_ms": 0.0, "mv_rhs": 0, "mv_calls": 0}
+
+    def solve_to_fp64(bx, xx, ax, on_device):
+        """One step: batched solve, FP64 true residuals, re-solve failures."""
+        out = dda.solve_batch(args.solver, bx, xx, ax, None, maxit=args.maxit, tol=args.tol)
+        ms, rhs, calls = dda.last_solve_stats()
+        stats["mv_ms"] += ms
+        stats["mv_rhs"] += rhs
+        stats["mv_calls"] += calls
+        res = dda.residual_f64(bx, xx, ax)
+        tol = args.tol
+        rounds = 0
+        while np.any(res > args.tol) and rounds < 4:
+            bad = np.flatnonzero(res > args.tol)
+            tol *= 0.5
+            sub = (lambda a: a[bad].contiguous()) if on_device else (lambda a: np.ascontiguousarray(a[bad]))
+            xs = sub(xx)
+            o2 = dda.solve_batch(args.solver, sub(bx), xs, sub(ax), None, maxit=args.maxit, tol=tol)
+            xx[bad] = xs
+            out.itno[bad] += o2.itno
+            out.ncompte[bad] += o2.ncompte
+            res[bad] = dda.residual_f64(sub(bx), xs, sub(ax))
+            stats["resolves"] += len(bad)
+            rounds += 1
+        return out, res
+
+    def step_dev(record):
+        xd.zero_()
+        out, res = solve_to_fp64(bd, xd, ad, True)
+        if record:
+            stats["iters"] += list(out.itno)
+            stats["ncompte"] += list(out.ncompte)
+            stats["res64"] += list(res)
+        return out
+
+    for _ in range(args.warmup):
+        step_dev(False)
+    stats.update(mv_ms=0.0, mv_rhs=0, mv_calls=0)
+    clocks = ClockSampler(local)
+    barrier(pg, local)
+    torch.cuda.synchronize()
+    clocks.start()
+    l0 = dda.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step_dev(True)
+    e1.record()
+    torch.cuda.synchronize()
+    barrier(pg, local)
+    launches = dda.launch_count() - l0
+    clk = clocks.stop()
+    elapsed = max_over_ranks(pg, e0.elapsed_time(e1) / 1000.0)
+    total_rhs = R * args.steps * world
+    value = total_rhs / elapsed
+    mv_stats = (stats["mv_ms"], stats["mv_rhs"], stats["mv_calls"])
+
+    # end-to-end through the C ABI with pinned host buffers
+    bh = torch.from_numpy(b).pin_memory()
+    ah = torch.from_numpy(adia).pin_memory()
+    xh = torch.zeros_like(bh).pin_memory()
+    bhn, ahn, xhn = bh.numpy(), ah.numpy(), xh.numpy()
+    step_host = lambda: solve_to_fp64(bhn, xhn, ahn, False)  # noqa: E731
+    xhn[...] = 0
+    step_host()  # warm-up of the host path
+    barrier(pg, local)
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record()
+    for _ in range(args.steps):
+        xhn[...] = 0
+        step_host()
+    f1.record()
+    torch.cuda.synchronize()
+    barrier(pg, local)
+    e2e_elapsed = max_over_ranks(pg, f0.elapsed_time(f1) / 1000.0)
+    vec = 3 * prob.nat * 8
+    h2d = R * vec * 3 * 2  # b, x0, CXADIA into the solve and again into the FP64 check
+    d2h = R * vec
+
+    if rank == 0:
+        ncm = float(np.mean(stats["ncompte"]))
+        rhs_per_call = mv_stats[1] / max(mv_stats[2], 1)
+        alg = algorithmic_bytes_per_matvec(prob, rhs_per_call)
+        ms_per_rhs_mv = mv_stats[0] / max(mv_stats[1], 1)
+        achieved = alg / (ms_per_rhs_mv * 1e-3) / 1e9
+        peak, peak_kind = measured_peak()
+        traffic = load_profile_traffic(args.n)
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            cpu = cpu_baseline(prob, ncm)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": elapsed * 1000.0 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c64 (FP32 complex bulk, FP64 dots and checks)",
+            "data": "synthetic (seeded sphere target and incident fields)", "config": config(args, prob, R, world),
+            "ms_per_rhs": elapsed * 1000.0 / (R * args.steps),
+            "iterations_mean": float(np.mean(stats["iters"])), "matvecs_per_rhs_mean": ncm,
+            "fp64_residual_max": float(np.max(stats["res64"])), "fp64_resolved_rhs": stats["resolves"],
+            "roofline": {"bound": "hbm", "kernel": "MATVEC (5 register-FFT passes, all RHS of one batched call)",
+                         "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": achieved / peak,
+                         "traffic": None if traffic is None else traffic,
+                         "algorithmic_bytes_per_rhs_matvec": alg, "ms_per_rhs_matvec": ms_per_rhs_mv,
+                         "rhs_per_matvec_call": rhs_per_call},
+            "cpu_baseline": cpu,
+            "e2e": {"value": total_rhs / e2e_elapsed, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches, "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    dda.release()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+# ------------------------------------------------------------------ reference arm
+def run_reference(args):
+    import ctypes as ct
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import torch
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    path = os.path.join(ROOT, "oracle", "_ref", "libddscat_ref_fft3d.so")
+    if not os.path.exists(path):
+        print(json.dumps({"impl": "reference", "unavailable": f"reference library not built ({path})"}))
+        return
+    lib = ct.CDLL(path, mode=ct.RTLD_LOCAL)
+    P = lambda a: a.ctypes.data_as(ct.c_void_p)  # noqa: E731
+    lib.ddscat_cuda_prepare_green_f32.argtypes = [ct.c_int] * 7 + [ct.c_float] * 9 + [ct.c_void_p]
+    fn = getattr(lib, f"ddscat_cuda_solve_{args.solver}_f32")
+    fn.argtypes = [ct.c_void_p] * 4 + [ct.c_int, ct.c_int, ct.c_float] + [ct.c_void_p] * 3
+    prob, b, adia = workload(args, 0)
+    aoff = np.zeros(b.shape[1], dtype=np.complex64)
+    nref = min(args.ref_rhs, b.shape[0])
+    k = prob.incid[0].k
+    with quiet_stdout():
+        rc = lib.ddscat_cuda_prepare_green_f32(prob.nx, prob.ny, prob.nz, 0, prob.nat, prob.nat0, 0, 0.0, 0.0, 0.0,
+                                               float(k[0]), float(k[1]), float(k[2]), 1.0, 1.0, 1.0, P(prob.iocc))
+    if rc != 0:
+        print(json.dumps({"impl": "reference", "unavailable": f"reference prepare_green failed with status {rc}"}))
+        return
+    iters = []
+
+    def step(record):
+        for r in range(nref):
+            x = np.zeros(b.shape[1], dtype=np.complex64)
+            it, tole, nc = ct.c_int(), ct.c_float(), ct.c_int()
+            rr = fn(P(b[r]), P(x), P(adia[r]), P(aoff), b.shape[1], args.maxit, args.tol, ct.byref(it),
+                    ct.byref(tole), ct.byref(nc))
+            if rr != 0:
+                raise RuntimeError(f"reference solve failed with status {rr}")
+            if record:
+                iters.append(it.value)
+
+    with quiet_stdout():
+        for _ in range(args.warmup):
+            step(False)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            step(True)
+        e1.record()
+        torch.cuda.synchronize()
+    elapsed = e0.elapsed_time(e1) / 1000.0
+    value = nref * args.steps / elapsed
+    sample = (f"reference ddscat_matvec_cuda.cu built unmodified (oracle/Makefile), {args.solver.upper()} through its "
+              f"own C ABI with host buffers, one RHS at a time, {nref} RHS per step (RHS 0..{nref - 1} of the "
+              f"workload); the reference implementation of this path runs on the GPU, its host side on 1 thread")
+    cfg = config(args, prob, b.shape[0], world)
+    cfg["reference_rhs_per_step"] = nref
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": elapsed * 1000.0 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c64 (FP32 complex bulk, FP64 dots)",
+            "data": "synthetic (seeded sphere target and incident fields)", "config": cfg, "impl": "reference",
+            "iterations_mean": float(np.mean(iters)),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -10,7 +10,8 @@
 #include <cstring>
 #include <string>
 #include <vector>
-#include "ddscat_matvec_cuda.h"
+#include "ddscat_b200.h"
+#include "batch.h"
 #include "solvers.h"
 
 namespace ddb {
@@ -24,6 +25,8 @@ void set_error(const char* where, const char* what) {
 void set_cuda_error(const char* where, cudaError_t e) { set_error(where, cudaGetErrorString(e)); }
 const char* last_error_text() { return g_last_error.c_str(); }
 void clear_error() { g_last_error.clear(); }
+static unsigned long long g_launches = 0;
+void note_launch(unsigned long long k) { g_launches += k; }
 int check_launch(const char* where) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) { set_cuda_error(where, e); return 1; }
@@ -42,10 +45,56 @@ struct State {
   C *d_b = nullptr, *d_sx = nullptr, *d_sy = nullptr, *d_work = nullptr;     // compact
   bool aoff_zero = false;
   int verbose = 0;
+  // how the target was prepared (for the all-FP64 engine built on demand)
+  int prep_kind = 0;  // 1 prepare_green, 2 prepare (CPU Green)
+  GreenArgs<float> green_args;
+  std::vector<float2> cpu_green;  // CXZC copy for prepare_f32
+  int16_t* h_iocc = nullptr;
 };
 static State s;
 
+// batched-solve buffers and statistics (library extension)
+struct BatchState {
+  int R = 0, cap = 0, n = 0;
+  C *b = nullptr, *x = nullptr, *adia = nullptr, *aoff = nullptr, *work = nullptr;
+  BatchOps<float> ops;
+  double matvec_ms = 0.0;
+  long long matvec_rhs = 0;
+  int matvec_calls = 0;
+};
+static BatchState bs;
+static void release_batch() {
+  cudaFree(bs.b); cudaFree(bs.x); cudaFree(bs.adia); cudaFree(bs.aoff); cudaFree(bs.work);
+  bs.ops.release();
+  const double ms = bs.matvec_ms;
+  const long long mr = bs.matvec_rhs;
+  const int mc = bs.matvec_calls;
+  bs = BatchState{};
+  bs.matvec_ms = ms; bs.matvec_rhs = mr; bs.matvec_calls = mc;
+}
+
+// all-FP64 engine of the prepared target (FP64 true residuals / FP64 solves)
+struct F64State {
+  bool ready = false;
+  Engine<double> eng;
+  VecOps<double> ops;
+  double2 *x = nullptr, *y = nullptr, *b = nullptr, *ad = nullptr, *ao = nullptr;
+};
+static F64State f64;
+static void release_f64() {
+  if (f64.ready) {
+    cudaFree(f64.x); cudaFree(f64.y); cudaFree(f64.b); cudaFree(f64.ad); cudaFree(f64.ao);
+    f64.ops.release();
+    f64.eng.release();
+  }
+  f64 = F64State{};
+}
+
 static void release_state() {
+  release_batch();
+  release_f64();
+  delete[] s.h_iocc;
+  s.h_iocc = nullptr;
   if (s.ready || s.eng.green) {
     cudaFree(s.d_xf); cudaFree(s.d_yf); cudaFree(s.d_adia); cudaFree(s.d_aoff);
     cudaFree(s.d_b); cudaFree(s.d_sx); cudaFree(s.d_sy); cudaFree(s.d_work);
@@ -53,6 +102,7 @@ static void release_state() {
     s.eng.release();
   }
   const int verbose = s.verbose;
+  s.cpu_green.clear();
   s = State{};
   s.verbose = verbose;
 }
@@ -205,6 +255,90 @@ static int make_integration_dirs(const float ak[3], const C e01[3], float etasca
   return 0;
 }
 
+// ---- batched solve ----
+static bool is_device_ptr(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) { cudaGetLastError(); return false; }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+static int ensure_batch(int R) {
+  const int n = 3 * s.eng.g.nat0;
+  if (bs.n == n && bs.cap >= R && bs.work) {  // reuse the vectors; reductions sized for R
+    if (bs.R != R) {
+      bs.ops.release();
+      if (bs.ops.init(R, n, s.stream)) return 1;
+      bs.R = R;
+    }
+    return 0;
+  }
+  release_batch();
+  const size_t v = (size_t)R * n;
+  cudaError_t e = cudaMalloc((void**)&bs.b, v * sizeof(C));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&bs.x, v * sizeof(C));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&bs.adia, v * sizeof(C));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&bs.aoff, v * sizeof(C));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&bs.work, (size_t)BATCH_WORK_VECTORS * v * sizeof(C));
+  if (e != cudaSuccess) { release_batch(); set_cuda_error("batched solve workspace", e); return 1; }
+  if (bs.ops.init(R, n, s.stream)) { release_batch(); return 1; }
+  bs.R = R;
+  bs.cap = R;
+  bs.n = n;
+  return 0;
+}
+
+// full (3*NAT) RHS r of a host or device array -> compact slot
+static int to_compact(const void* src, bool dev, int r, C* dst) {
+  const size_t full = (size_t)3 * s.eng.g.nat;
+  const C* f = (const C*)src + (size_t)r * full;
+  if (!dev) {
+    cudaError_t e = cudaMemcpyAsync(s.d_xf, f, full * sizeof(C), cudaMemcpyHostToDevice, s.stream);
+    if (e != cudaSuccess) { set_cuda_error("batched solve H2D", e); return 1; }
+    f = s.d_xf;
+  }
+  v_gather<float>(f, dst + (size_t)r * bs.n, s.eng.occ, s.eng.g.nat, s.eng.g.nat0, s.stream);
+  return check_launch("batched solve gather");
+}
+
+
+// ---- all-FP64 engine ----
+template <typename Src> __global__ void k_to_f64(const Src* a, double2* b, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    b[i] = to_d(a[i]);
+}
+
+static int ensure_f64() {
+  if (f64.ready) return 0;
+  const Geometry& g = s.eng.g;
+  int rc = f64.eng.init_geometry(g.nx, g.ny, g.nz, g.ipbc, g.nat, g.nat0, s.h_iocc);
+  if (rc) { release_f64(); return 1; }
+  if (s.prep_kind == 1) {
+    GreenArgs<double> ga;
+    ga.idipint = s.green_args.idipint; ga.gamma = s.green_args.gamma;
+    ga.pyd = s.green_args.pyd; ga.pzd = s.green_args.pzd;
+    for (int k = 0; k < 3; ++k) { ga.ak[k] = s.green_args.ak[k]; ga.dx[k] = s.green_args.dx[k]; }
+    if (f64.eng.build_green(ga)) { release_f64(); return 1; }
+  } else {
+    // CPU-supplied complex-float Green: widen to complex double
+    const size_t gc = g.green_count();
+    std::vector<double2> h(gc);
+    for (size_t i = 0; i < gc; ++i) h[i] = make_double2(s.cpu_green[i].x, s.cpu_green[i].y);
+    if (f64.eng.upload_green(h.data())) { release_f64(); return 1; }
+  }
+  const size_t cn = (size_t)3 * g.nat0;
+  cudaError_t e = cudaMalloc((void**)&f64.x, cn * sizeof(double2));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&f64.y, cn * sizeof(double2));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&f64.b, cn * sizeof(double2));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&f64.ad, cn * sizeof(double2));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&f64.ao, cn * sizeof(double2));
+  if (e != cudaSuccess) { set_cuda_error("FP64 engine", e); release_f64(); return 1; }
+  if (f64.ops.init(s.stream)) { release_f64(); return 1; }
+  f64.eng.stream = s.stream;
+  f64.ready = true;
+  return 0;
+}
+
+
 }  // namespace ddb
 
 using namespace ddb;
@@ -241,6 +375,10 @@ DDSCAT_CUDA_API int ddscat_cuda_prepare_green_f32(int nx, int ny, int nz, int ip
   if (rc) { release_state(); return 220 + rc; }
   rc = allocate_runtime();
   if (rc) { release_state(); return rc; }
+  s.prep_kind = 1;
+  s.green_args = ga;
+  s.h_iocc = new int16_t[nat];
+  std::memcpy(s.h_iocc, iocc, (size_t)nat * sizeof(int16_t));
   s.ready = true;
   return 0;
 }
@@ -259,6 +397,10 @@ DDSCAT_CUDA_API int ddscat_cuda_prepare_f32(int nx, int ny, int nz, int ipbc, in
   if (rc) { release_state(); return rc == 2 ? 6 : 2; }
   if (allocate_runtime()) { release_state(); return 2; }
   if (s.eng.upload_green(green)) { release_state(); return 4; }
+  s.prep_kind = 2;
+  s.cpu_green.assign((const float2*)green, (const float2*)green + s.eng.g.green_count());
+  s.h_iocc = new int16_t[nat];
+  std::memcpy(s.h_iocc, iocc, (size_t)nat * sizeof(int16_t));
   s.ready = true;
   return 0;
 }
@@ -418,6 +560,121 @@ DDSCAT_CUDA_API int ddscat_b200_set_verbose(int level) {
 }
 
 DDSCAT_CUDA_API int ddscat_b200_layout(void) { return slices_build(); }
+
+DDSCAT_CUDA_API unsigned long long ddscat_b200_launch_count(void) { return g_launches; }
+
+DDSCAT_CUDA_API int ddscat_b200_solve_batch_f32(int solver, int nrhs, const void* b, void* x, const void* adia,
+                                                const void* aoff, int maxit, float tol, int* itno, float* tole,
+                                                int* ncompte, int* status) {
+  clear_error();
+  if (!s.ready || nrhs <= 0 || !b || !x || !adia || maxit <= 0 || !(tol > 0.f) || !itno || !tole || !ncompte ||
+      !status) {
+    set_error("batched solve", "invalid argument or not prepared");
+    return 500;
+  }
+  if (solver != DDSCAT_B200_QMRCCG && solver != DDSCAT_B200_PBCGS2) {
+    set_error("batched solve", "unsupported solver (QMRCCG=1, PBCGS2=2)");
+    return 501;
+  }
+  const bool dev = is_device_ptr(b);
+  if (is_device_ptr(x) != dev || is_device_ptr(adia) != dev || (aoff && is_device_ptr(aoff) != dev)) {
+    set_error("batched solve", "b, x, adia, aoff must all be host or all be device pointers");
+    return 502;
+  }
+  if (ensure_batch(nrhs)) return 503;
+  const size_t full = (size_t)3 * s.eng.g.nat;
+  bool use_aoff = aoff != nullptr;
+  if (use_aoff && !dev) use_aoff = !all_zero(aoff, nrhs * full * sizeof(C));
+  for (int r = 0; r < nrhs; ++r) {
+    if (to_compact(b, dev, r, bs.b) || to_compact(x, dev, r, bs.x) || to_compact(adia, dev, r, bs.adia)) return 504;
+    if (use_aoff && to_compact(aoff, dev, r, bs.aoff)) return 504;
+  }
+  BatchIO<float> io;
+  io.eng = &s.eng; io.ops = &bs.ops; io.R = nrhs; io.n = bs.n;
+  io.b = bs.b; io.x = bs.x; io.adia = bs.adia; io.aoff = use_aoff ? bs.aoff : nullptr;
+  io.work = bs.work; io.nwork = BATCH_WORK_VECTORS;
+  io.maxit = maxit; io.tol = (double)tol; io.verbose = s.verbose;
+  BatchResult res;
+  const int rc = solver == DDSCAT_B200_QMRCCG ? solve_batch_qmrccg<float>(io, res) : solve_batch_pbcgs2<float>(io, res);
+  bs.matvec_ms = io.matvec_ms;
+  bs.matvec_rhs = io.matvec_rhs;
+  bs.matvec_calls = io.matvec_calls;
+  if (rc) return rc == 1 ? 505 : rc;
+  // solutions back to the caller's full layout (zeros on vacuum sites)
+  for (int r = 0; r < nrhs; ++r) {
+    C* dst = dev ? (C*)x + (size_t)r * full : s.d_xf;
+    cudaError_t e = cudaMemsetAsync(dst, 0, full * sizeof(C), s.stream);
+    if (e != cudaSuccess) { set_cuda_error("batched solve output", e); return 506; }
+    v_scatter<float>(bs.x + (size_t)r * bs.n, dst, s.eng.occ, s.eng.g.nat, s.eng.g.nat0, s.stream);
+    if (check_launch("batched solve scatter")) return 506;
+    if (!dev) {
+      e = cudaMemcpyAsync((C*)x + (size_t)r * full, s.d_xf, full * sizeof(C), cudaMemcpyDeviceToHost, s.stream);
+      if (e != cudaSuccess) { set_cuda_error("batched solve D2H", e); return 506; }
+    }
+  }
+  cudaError_t e = cudaStreamSynchronize(s.stream);
+  if (e != cudaSuccess) { set_cuda_error("batched solve", e); return 506; }
+  int worst = 0;
+  for (int r = 0; r < nrhs; ++r) {
+    itno[r] = res.itno[r];
+    tole[r] = (float)res.tole[r];
+    ncompte[r] = res.ncompte[r];
+    status[r] = res.status[r];
+    if (res.status[r] && !worst) worst = res.status[r];
+  }
+  if (worst) {
+    char msg[128];
+    std::snprintf(msg, sizeof(msg), "at least one right-hand side broke down (first status %d)", worst);
+    set_error("batched solve", msg);
+  }
+  return 0;
+}
+
+DDSCAT_CUDA_API int ddscat_b200_last_solve_stats(double* matvec_ms, long long* rhs_matvecs, int* matvec_calls) {
+  if (matvec_ms) *matvec_ms = bs.matvec_ms;
+  if (rhs_matvecs) *rhs_matvecs = bs.matvec_rhs;
+  if (matvec_calls) *matvec_calls = bs.matvec_calls;
+  return 0;
+}
+
+DDSCAT_CUDA_API int ddscat_b200_residual_f64(int nrhs, const void* b, const void* x, const void* adia, const void* aoff,
+                                             double* resid) {
+  clear_error();
+  if (!s.ready || nrhs <= 0 || !b || !x || !adia || !resid) { set_error("FP64 residual", "invalid argument"); return 510; }
+  const bool dev = is_device_ptr(b);
+  if (ensure_f64()) return 511;
+  const size_t full = (size_t)3 * s.eng.g.nat, cn = (size_t)3 * s.eng.g.nat0;
+  const unsigned gb = (unsigned)std::min<size_t>(ceil_div(cn, 256), 148 * 16);
+  C* tmp = s.d_sy;  // compact float staging
+  for (int r = 0; r < nrhs; ++r) {
+    const void* srcs[4] = {b, x, adia, aoff};
+    double2* dsts[4] = {f64.b, f64.x, f64.ad, f64.ao};
+    for (int k = 0; k < 4; ++k) {
+      if (!srcs[k]) continue;
+      const C* f = (const C*)srcs[k] + (size_t)r * full;
+      if (!dev) {
+        cudaError_t e = cudaMemcpyAsync(s.d_xf, f, full * sizeof(C), cudaMemcpyHostToDevice, s.stream);
+        if (e != cudaSuccess) { set_cuda_error("FP64 residual H2D", e); return 512; }
+        f = s.d_xf;
+      }
+      v_gather<float>(f, tmp, s.eng.occ, s.eng.g.nat, s.eng.g.nat0, s.stream);
+      k_to_f64<C><<<gb, 256, 0, s.stream>>>(tmp, dsts[k], cn);
+      note_launch();
+      if (check_launch("FP64 residual widen")) return 512;
+    }
+    MvArgs<double> a;
+    a.x = f64.x; a.y = f64.y; a.io_full = 0;
+    a.adia = f64.ad; a.aoff = aoff ? f64.ao : nullptr; a.a_full = 0; a.nrhs = 1;
+    int rc = f64.eng.matvec(a);
+    if (rc) return rc;
+    int err = 0;
+    const double bn = f64.ops.nrm2((int)cn, f64.b, &err);
+    const double rn = f64.ops.norm_diff((int)cn, f64.b, f64.y, &err);
+    if (err) return 513;
+    resid[r] = bn > 0.0 ? rn / bn : INFINITY;
+  }
+  return 0;
+}
 
 DDSCAT_CUDA_API int ddscat_b200_matvec_timing(int nrhs, int iters, int cwhat, float* ms_per_call) {
   clear_error();

@@ -1,0 +1,681 @@
+// Batched multi-RHS Krylov solves (sm_100a): masked per-RHS vector kernels,
+// per-RHS FP64 inner products in one launch, and the QMRCCG / PBCGS2
+// recurrences of solvers.cu run for every RHS in lock-step.  Host syncs (one
+// small D2H per group of inner products) are shared by all RHS of the batch.
+#include <algorithm>
+#include <complex>
+#include "batch.h"
+
+namespace ddb {
+
+using Z = std::complex<double>;
+static inline double2 dz(Z z) { return make_double2(z.real(), z.imag()); }
+static inline Z zd2(double2 v) { return Z(v.x, v.y); }
+
+constexpr int BT = 256;
+
+template <typename C>
+__global__ void __launch_bounds__(BT) kb_lin(int n, C* d, const double2* cd, const C* a, const double2* ca, const C* b,
+                                             const double2* cb, const int* mask) {
+  const int r = blockIdx.y;
+  if (mask && !mask[r]) return;
+  const size_t off = (size_t)r * n;
+  const double2 zd = cd ? cd[r] : make_double2(0.0, 0.0);
+  const double2 za = ca ? ca[r] : make_double2(0.0, 0.0);
+  const double2 zb = cb ? cb[r] : make_double2(0.0, 0.0);
+  const bool keep = cd && !(zd.x == 0.0 && zd.y == 0.0);
+  const bool d1 = zd.x == 1.0 && zd.y == 0.0, a1 = za.x == 1.0 && za.y == 0.0, b1 = zb.x == 1.0 && zb.y == 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    C v = mk<C>(0, 0);
+    if (keep) v = d1 ? d[off + i] : zmulv(zd, d[off + i]);
+    if (a) v = cadd(v, a1 ? a[off + i] : zmulv(za, a[off + i]));
+    if (b) v = cadd(v, b1 ? b[off + i] : zmulv(zb, b[off + i]));
+    d[off + i] = v;
+  }
+}
+
+template <typename T> struct BDot {
+  const cplx<T>* a[8];
+  const cplx<T>* b[8];
+  const cplx<T>* c[8];
+  int conj[8];
+  int K, mode;  // mode 0: products; 1: (|a-b|^2, |a-b-c|^2)
+};
+
+__device__ __forceinline__ double2 wsum2(double2 v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v.x += __shfl_down_sync(0xffffffffu, v.x, o);
+    v.y += __shfl_down_sync(0xffffffffu, v.y, o);
+  }
+  return v;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(BT) kb_dots(int n, BDot<T> sp, const int* mask, double2* part, double2* out,
+                                              unsigned* cnt) {
+  __shared__ double2 ws[8][BT / 32];
+  __shared__ bool last;
+  const int r = blockIdx.y;
+  if (mask && !mask[r]) return;
+  const size_t off = (size_t)r * n;
+  double2 acc[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) acc[k] = make_double2(0.0, 0.0);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (sp.mode == 0) {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        if (k >= sp.K) break;
+        const double2 a = to_d(sp.a[k][off + i]), b = to_d(sp.b[k][off + i]);
+        if (sp.conj[k]) { acc[k].x += a.x * b.x + a.y * b.y; acc[k].y += a.x * b.y - a.y * b.x; }
+        else { acc[k].x += a.x * b.x - a.y * b.y; acc[k].y += a.x * b.y + a.y * b.x; }
+      }
+    } else {
+      const double2 a = to_d(sp.a[0][off + i]), b = to_d(sp.b[0][off + i]), c = to_d(sp.c[0][off + i]);
+      const double dr = a.x - b.x, di = a.y - b.y;
+      acc[0].x += dr * dr + di * di;
+      const double er = dr - c.x, ei = di - c.y;
+      acc[1].x += er * er + ei * ei;
+    }
+  }
+  const int K = sp.mode == 0 ? sp.K : 2;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int k = 0; k < K; ++k) {
+    const double2 v = wsum2(acc[k]);
+    if (lane == 0) ws[k][wid] = v;
+  }
+  __syncthreads();
+  double2* P = part + ((size_t)r * 8) * gridDim.x;
+  if (threadIdx.x < 32) {
+    for (int k = 0; k < K; ++k) {
+      double2 v = lane < BT / 32 ? ws[k][lane] : make_double2(0.0, 0.0);
+      v = wsum2(v);
+      if (lane == 0) P[(size_t)k * gridDim.x + blockIdx.x] = v;
+    }
+  }
+  __threadfence();
+  if (threadIdx.x == 0) last = atomicInc(cnt + r, gridDim.x - 1) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int k = 0; k < K; ++k) {
+    double2 v = make_double2(0.0, 0.0);
+    for (int bi = threadIdx.x; bi < (int)gridDim.x; bi += blockDim.x) {
+      const volatile double* pp = reinterpret_cast<volatile double*>(P + (size_t)k * gridDim.x + bi);
+      v.x += pp[0];
+      v.y += pp[1];
+    }
+    v = wsum2(v);
+    if (lane == 0) ws[k][wid] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    for (int k = 0; k < K; ++k) {
+      double2 v = lane < BT / 32 ? ws[k][lane] : make_double2(0.0, 0.0);
+      v = wsum2(v);
+      if (lane == 0) out[(size_t)r * 8 + k] = v;
+    }
+  }
+}
+
+template <typename T> int BatchOps<T>::init(int R_, int n_, cudaStream_t s) {
+  R = R_;
+  n = n_;
+  stream = s;
+  nb = (int)std::max<size_t>(1, std::min<size_t>(ceil_div(n, BT), std::max(1, 592 / std::max(1, R))));
+  coef_cap = (size_t)3 * R * 96;
+  cudaError_t e = cudaMalloc((void**)&d_part, (size_t)R * 8 * nb * sizeof(double2));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&d_out, (size_t)R * 8 * sizeof(double2));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&d_cnt, (size_t)R * sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&h_out, (size_t)R * 8 * sizeof(double2));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&h_coef, coef_cap * sizeof(double2));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&d_coef, coef_cap * sizeof(double2));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&h_mask, (size_t)MASKS * R * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&d_masks, (size_t)MASKS * R * sizeof(int));
+  if (e != cudaSuccess) { set_cuda_error("batch buffers", e); return 1; }
+  cudaMemset(d_cnt, 0, (size_t)R * sizeof(unsigned));
+  return 0;
+}
+
+template <typename T> void BatchOps<T>::release() {
+  cudaFree(d_part); cudaFree(d_out); cudaFree(d_cnt); cudaFree(d_coef); cudaFree(d_masks);
+  if (h_out) cudaFreeHost(h_out);
+  if (h_coef) cudaFreeHost(h_coef);
+  if (h_mask) cudaFreeHost(h_mask);
+  *this = BatchOps<T>{};
+}
+
+template <typename T> const int* BatchOps<T>::mask(const std::vector<int>& m) {
+  if (mask_pos >= (size_t)MASKS) {  // ring full: wait for pending copies, then reuse
+    cudaStreamSynchronize(stream);
+    mask_pos = 0;
+  }
+  int* h = h_mask + mask_pos * R;
+  int* d = d_masks + mask_pos * R;
+  for (int r = 0; r < R; ++r) h[r] = m[r];
+  cudaMemcpyAsync(d, h, (size_t)R * sizeof(int), cudaMemcpyHostToDevice, stream);
+  ++mask_pos;
+  return d;
+}
+
+template <typename T>
+int BatchOps<T>::lin(C* d, const double2* zd, const C* a, const double2* za, const C* b, const double2* zb,
+                     const int* msk) {
+  if (coef_pos + 3 * (size_t)R > coef_cap) {
+    cudaStreamSynchronize(stream);
+    coef_pos = 0;
+  }
+  double2* h = h_coef + coef_pos;
+  double2* dc = d_coef + coef_pos;
+  const double2* src[3] = {zd, za, zb};
+  for (int k = 0; k < 3; ++k)
+    for (int r = 0; r < R; ++r) h[k * R + r] = src[k] ? src[k][r] : make_double2(0.0, 0.0);
+  cudaMemcpyAsync(dc, h, (size_t)3 * R * sizeof(double2), cudaMemcpyHostToDevice, stream);
+  coef_pos += 3 * (size_t)R;
+  const unsigned gx = (unsigned)std::max<size_t>(1, std::min<size_t>(ceil_div(n, BT), std::max(1, 2368 / R)));
+  kb_lin<C><<<dim3(gx, R), BT, 0, stream>>>(n, d, zd ? dc : nullptr, a, za ? dc + R : nullptr, b, zb ? dc + 2 * R : nullptr,
+                                            msk);
+  note_launch();
+  return check_launch("batched vector update");
+}
+
+template <typename T> int BatchOps<T>::copy(C* d, const C* a, const int* msk) {
+  std::vector<double2> one(R, make_double2(1.0, 0.0));
+  return lin(d, nullptr, a, one.data(), nullptr, nullptr, msk);
+}
+
+template <typename T> int BatchOps<T>::zero(C* d, const int* msk) {
+  return lin(d, nullptr, nullptr, nullptr, nullptr, nullptr, msk);
+}
+
+template <typename T>
+int BatchOps<T>::dots(int K, const C* const* a, const C* const* b, const int* conj, const int* msk,
+                      std::vector<double2>& out) {
+  BDot<T> sp{};
+  sp.K = K;
+  sp.mode = 0;
+  for (int k = 0; k < K; ++k) { sp.a[k] = a[k]; sp.b[k] = b[k]; sp.conj[k] = conj[k]; }
+  kb_dots<T><<<dim3(nb, R), BT, 0, stream>>>(n, sp, msk, d_part, d_out, d_cnt);
+  note_launch();
+  if (check_launch("batched inner products")) return 1;
+  cudaError_t e = cudaMemcpyAsync(h_out, d_out, (size_t)R * 8 * sizeof(double2), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) { set_cuda_error("batched inner products D2H", e); return 1; }
+  reset_ring();
+  out.assign((size_t)R * K, make_double2(0, 0));
+  for (int r = 0; r < R; ++r)
+    for (int k = 0; k < K; ++k) out[(size_t)r * K + k] = h_out[(size_t)r * 8 + k];
+  return 0;
+}
+
+template <typename T>
+int BatchOps<T>::diff_norms(const C* a, const C* b, const C* c, const int* msk, std::vector<double2>& out) {
+  BDot<T> sp{};
+  sp.K = 2;
+  sp.mode = 1;
+  sp.a[0] = a; sp.b[0] = b; sp.c[0] = c;
+  kb_dots<T><<<dim3(nb, R), BT, 0, stream>>>(n, sp, msk, d_part, d_out, d_cnt);
+  note_launch();
+  if (check_launch("batched residual norms")) return 1;
+  cudaError_t e = cudaMemcpyAsync(h_out, d_out, (size_t)R * 8 * sizeof(double2), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) { set_cuda_error("batched residual norms D2H", e); return 1; }
+  reset_ring();
+  out.assign((size_t)R * 2, make_double2(0, 0));
+  for (int r = 0; r < R; ++r) {
+    out[(size_t)r * 2] = h_out[(size_t)r * 8];
+    out[(size_t)r * 2 + 1] = h_out[(size_t)r * 8 + 1];
+  }
+  return 0;
+}
+
+// --------------------------------------------------------------------------
+// shared solver plumbing
+template <typename T> struct BCtx {
+  using C = cplx<T>;
+  BatchIO<T>& io;
+  BatchOps<T>& ops;
+  int R, n;
+  std::vector<int> nc;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+  explicit BCtx(BatchIO<T>& s) : io(s), ops(*s.ops), R(s.R), n(s.n), nc(s.R, 0) {}
+  ~BCtx() {
+    for (auto& p : ev) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
+  }
+  C* w(int slot) { return io.work + (size_t)slot * R * n; }
+  // MATVEC of `in` into `out` for RHS in mask m (host copy hm for counting)
+  int mv(const C* in, C* out, const std::vector<int>& hm) {
+    int cnt = 0;
+    for (int r = 0; r < R; ++r) cnt += hm[r] ? 1 : 0;
+    if (!cnt) return 0;
+    const int* dm = ops.mask(hm);
+    MvArgs<T> a;
+    a.x = in; a.x_rs = n; a.y = out; a.y_rs = n; a.io_full = 0;
+    a.adia = io.adia; a.aoff = io.aoff; a.a_rs = n; a.a_full = 0;
+    a.conj = 0; a.mask = dm; a.nrhs = R;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, ops.stream);
+    int rc = io.eng->matvec(a);
+    cudaEventRecord(e1, ops.stream);
+    ev.push_back({e0, e1});
+    if (rc) return rc;
+    for (int r = 0; r < R; ++r) nc[r] += hm[r] ? 1 : 0;
+    io.matvec_rhs += cnt;
+    io.matvec_calls += 1;
+    return 0;
+  }
+  void finish_timing() {
+    cudaStreamSynchronize(ops.stream);
+    double ms = 0.0;
+    for (auto& p : ev) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, p.first, p.second);
+      ms += t;
+    }
+    io.matvec_ms += ms;
+  }
+  static std::vector<double2> vals(const std::vector<Z>& z) {
+    std::vector<double2> o(z.size());
+    for (size_t i = 0; i < z.size(); ++i) o[i] = dz(z[i]);
+    return o;
+  }
+  static std::vector<double2> cst(int R, Z v) { return std::vector<double2>(R, dz(v)); }
+};
+
+static bool any_of(const std::vector<int>& m) {
+  for (int v : m)
+    if (v) return true;
+  return false;
+}
+
+// --------------------------------------------------------------------------
+// QMRCCG (per RHS: solvers.cu solve_qmrccg, reference cu:434-443, cu:1071-1103)
+template <typename T> int solve_batch_qmrccg(BatchIO<T>& io, BatchResult& res) {
+  using C = cplx<T>;
+  BCtx<T> c(io);
+  BatchOps<T>& ops = c.ops;
+  const int R = io.R;
+  C *r = c.w(0), *p = c.w(1), *ap = c.w(2), *q = c.w(3), *d = c.w(4), *s = c.w(5);
+  C *vt = c.w(6), *wt = c.w(7), *atw = c.w(8), *sy = c.w(9), *xs = io.x;
+  const std::vector<double2> one = BCtx<T>::cst(R, 1.0), mone = BCtx<T>::cst(R, -1.0);
+  res.itno.assign(R, 0); res.ncompte.assign(R, 0); res.status.assign(R, 0); res.tole.assign(R, 0.0);
+  std::vector<int> live(R, 1);  // not failed, not converged
+  std::vector<double> bnorm(R), resid(R);
+  std::vector<Z> lambda(R), kappa(R), theta(R), gamma(R), ksi(R), rho(R), eps(R), mu(R), tau(R);
+  std::vector<double2> o;
+  const C* A1[3];
+  const C* B1[3];
+  int cj[3];
+  // ||b||
+  A1[0] = io.b; B1[0] = io.b; cj[0] = 1;
+  if (ops.dots(1, A1, B1, cj, nullptr, o)) return 1;
+  for (int i = 0; i < R; ++i) {
+    bnorm[i] = std::sqrt(std::max(0.0, o[i].x));
+    if (bnorm[i] == 0.0) { res.status[i] = 52; live[i] = 0; }
+  }
+  const int* M = ops.mask(live);
+  int rc = c.mv(xs, sy, live);
+  if (rc) return rc;
+  ops.lin(r, nullptr, io.b, one.data(), sy, mone.data(), M);
+  for (C* v : {p, ap, q, d, s, atw}) ops.zero(v, M);
+  ops.copy(vt, r, M);
+  ops.copy(wt, r, M);
+  auto init_scalars = [&](const std::vector<int>& set) -> int {
+    const int* Ms = ops.mask(set);
+    const C* A3[3] = {vt, wt, vt};
+    const C* B3[3] = {vt, wt, wt};
+    const int c3[3] = {1, 1, 0};
+    std::vector<double2> o3, o1;
+    if (ops.dots(3, A3, B3, c3, Ms, o3)) return 1;
+    int rc2 = c.mv(wt, atw, set);
+    if (rc2) return rc2;
+    const C* A1b[1] = {vt};
+    const C* B1b[1] = {atw};
+    const int c1[1] = {0};
+    if (ops.dots(1, A1b, B1b, c1, Ms, o1)) return 1;
+    for (int i = 0; i < R; ++i) {
+      if (!set[i]) continue;
+      const double gn = std::sqrt(std::max(0.0, o3[3 * i].x)), kn = std::sqrt(std::max(0.0, o3[3 * i + 1].x));
+      rho[i] = zd2(o3[3 * i + 2]);
+      eps[i] = zd2(o1[i]);
+      lambda[i] = 1.0; kappa[i] = -1.0; theta[i] = -1.0; gamma[i] = gn; ksi[i] = kn; mu[i] = 0.0;
+      if (rho[i] == Z(0.0) || gamma[i] == Z(0.0) || ksi[i] == Z(0.0)) { res.status[i] = 55; live[i] = 0; continue; }
+      tau[i] = eps[i] / rho[i];
+    }
+    return 0;
+  };
+  if ((rc = init_scalars(live))) return rc;
+  {
+    const C* Ar[1] = {r};
+    const int c1[1] = {1};
+    if (ops.dots(1, Ar, Ar, c1, ops.mask(live), o)) return 1;
+    for (int i = 0; i < R; ++i)
+      if (live[i]) resid[i] = std::sqrt(std::max(0.0, o[i].x)) / bnorm[i];
+  }
+  std::vector<int> it(R, 0);
+  for (;;) {
+    std::vector<int> I(R, 0);
+    for (int i = 0; i < R; ++i) I[i] = live[i] && it[i] < io.maxit && resid[i] > io.tol;
+    if (!any_of(I)) break;
+    for (int i = 0; i < R; ++i) it[i] += I[i];
+    const int* MI = ops.mask(I);
+    std::vector<double2> cmu(R), cgam(R), cq(R), cksi(R), ctg(R), ctk(R), cth(R), cka(R);
+    for (int i = 0; i < R; ++i) {
+      if (!I[i]) continue;
+      cmu[i] = dz(-mu[i]); cgam[i] = dz(1.0 / gamma[i]);
+      cq[i] = dz(-(gamma[i] * mu[i]) / ksi[i]); cksi[i] = dz(1.0 / ksi[i]);
+    }
+    ops.lin(p, cmu.data(), vt, cgam.data(), nullptr, nullptr, MI);
+    ops.lin(q, cq.data(), atw, cksi.data(), nullptr, nullptr, MI);
+    if ((rc = c.mv(p, ap, I))) return rc;
+    for (int i = 0; i < R; ++i) {
+      if (!I[i]) continue;
+      ctg[i] = dz(-(tau[i] / gamma[i]));
+      ctk[i] = dz(-(tau[i] / ksi[i]));
+    }
+    ops.lin(vt, ctg.data(), ap, one.data(), nullptr, nullptr, MI);
+    ops.lin(wt, ctk.data(), q, one.data(), nullptr, nullptr, MI);
+    std::vector<double2> o3, o1;
+    {
+      const C* A3[3] = {vt, wt, vt};
+      const C* B3[3] = {vt, wt, wt};
+      const int c3[3] = {1, 1, 0};
+      if (ops.dots(3, A3, B3, c3, MI, o3)) return 1;
+    }
+    if ((rc = c.mv(wt, atw, I))) return rc;
+    {
+      const C* A1b[1] = {vt};
+      const C* B1b[1] = {atw};
+      const int c1[1] = {0};
+      if (ops.dots(1, A1b, B1b, c1, MI, o1)) return 1;
+    }
+    for (int i = 0; i < R; ++i) {
+      if (!I[i]) continue;
+      const Z gamma0 = gamma[i], ksi0 = ksi[i], rho0 = rho[i], tau0 = tau[i], kappa0 = kappa[i];
+      gamma[i] = std::sqrt(std::max(0.0, o3[3 * i].x));
+      ksi[i] = std::sqrt(std::max(0.0, o3[3 * i + 1].x));
+      rho[i] = zd2(o3[3 * i + 2]);
+      eps[i] = zd2(o1[i]);
+      int st = 0;
+      if (gamma[i] == Z(0.0)) st = 6;
+      else if (ksi[i] == Z(0.0)) st = 7;
+      const Z den = gamma[i] * tau[i] * rho0;
+      if (!st && den == Z(0.0)) st = 12;
+      if (!st) { mu[i] = gamma0 * ksi0 * rho[i] / den; if (rho[i] == Z(0.0)) st = 13; }
+      if (!st) {
+        tau[i] = eps[i] / rho[i] - gamma[i] * mu[i];
+        const double at0 = std::norm(tau0), ag = std::norm(gamma[i]);
+        const Z den2 = lambda[i] * at0 + ag;
+        if (den2 == Z(0.0)) st = 14;
+        else {
+          theta[i] = ((1.0 - lambda[i]) * at0) / den2;
+          kappa[i] = -(gamma0 * std::conj(tau0) * kappa0) / den2;
+          lambda[i] = (lambda[i] * at0) / den2;
+        }
+      }
+      if (st) { res.status[i] = 58; live[i] = 0; I[i] = 0; }
+      cth[i] = dz(theta[i]);
+      cka[i] = dz(kappa[i]);
+    }
+    MI = ops.mask(I);
+    ops.lin(d, cth.data(), p, cka.data(), nullptr, nullptr, MI);
+    ops.lin(s, cth.data(), ap, cka.data(), nullptr, nullptr, MI);
+    ops.lin(xs, one.data(), d, one.data(), nullptr, nullptr, MI);
+    ops.lin(r, one.data(), s, mone.data(), nullptr, nullptr, MI);
+    {
+      const C* Ar[1] = {r};
+      const int c1[1] = {1};
+      if (ops.dots(1, Ar, Ar, c1, MI, o)) return 1;
+      for (int i = 0; i < R; ++i)
+        if (I[i]) resid[i] = std::sqrt(std::max(0.0, o[i].x)) / bnorm[i];
+    }
+    std::vector<int> CK(R, 0);
+    for (int i = 0; i < R; ++i) CK[i] = I[i] && ((it[i] % 20) == 0 || resid[i] <= io.tol);
+    if (any_of(CK)) {
+      if ((rc = c.mv(xs, sy, CK))) return rc;
+      std::vector<double2> nn;
+      if (ops.diff_norms(io.b, sy, r, ops.mask(CK), nn)) return 1;
+      std::vector<int> RS(R, 0);
+      for (int i = 0; i < R; ++i) {
+        if (!CK[i]) continue;
+        const double tr = std::sqrt(std::max(0.0, nn[2 * i].x)), gapn = std::sqrt(std::max(0.0, nn[2 * i + 1].x));
+        const double tres = tr / bnorm[i];
+        const double gap = tr > 0.0 ? gapn / tr : (gapn == 0.0 ? 0.0 : INFINITY);
+        const bool conv = tres <= io.tol;
+        const bool rest = gap >= 1.0e-3 || (resid[i] <= io.tol && !conv);
+        if (conv) { resid[i] = tres; live[i] = 0; continue; }
+        if (rest) { RS[i] = 1; resid[i] = tres; }
+      }
+      if (any_of(RS)) {
+        const int* MR = ops.mask(RS);
+        ops.lin(sy, mone.data(), io.b, one.data(), nullptr, nullptr, MR);  // sy = b - A x
+        ops.copy(r, sy, MR);
+        for (C* v : {p, ap, q, d, s, atw}) ops.zero(v, MR);
+        ops.copy(vt, sy, MR);
+        ops.copy(wt, sy, MR);
+        if ((rc = init_scalars(RS))) return rc;
+      }
+    }
+  }
+  // RHS that stopped at MAXIT: one final true residual (cu:1099)
+  std::vector<int> F(R, 0);
+  for (int i = 0; i < R; ++i) F[i] = res.status[i] == 0 && resid[i] > io.tol;
+  if (any_of(F)) {
+    if ((rc = c.mv(xs, sy, F))) return rc;
+    std::vector<double2> nn;
+    if (ops.diff_norms(io.b, sy, r, ops.mask(F), nn)) return 1;
+    for (int i = 0; i < R; ++i)
+      if (F[i]) resid[i] = std::sqrt(std::max(0.0, nn[2 * i].x)) / bnorm[i];
+  }
+  c.finish_timing();
+  for (int i = 0; i < R; ++i) { res.itno[i] = it[i]; res.tole[i] = resid[i]; res.ncompte[i] = c.nc[i]; }
+  return 0;
+}
+
+// --------------------------------------------------------------------------
+// PBCGS2 (per RHS: solvers.cu solve_pbcgs2, reference cu:459-480, cu:1168-1278)
+template <typename T> int solve_batch_pbcgs2(BatchIO<T>& io, BatchResult& res) {
+  using C = cplx<T>;
+  BCtx<T> c(io);
+  BatchOps<T>& ops = c.ops;
+  const int R = io.R;
+  C *rr = c.w(0), *r[3] = {c.w(1), c.w(2), c.w(3)}, *u[3] = {c.w(4), c.w(5), c.w(6)};
+  C *XP = c.w(7), *BP = c.w(8), *X = c.w(9), *sy = c.w(10);
+  const std::vector<double2> one = BCtx<T>::cst(R, 1.0), mone = BCtx<T>::cst(R, -1.0);
+  res.itno.assign(R, 0); res.ncompte.assign(R, 0); res.status.assign(R, 0); res.tole.assign(R, 0.0);
+  std::vector<int> live(R, 1);
+  const int* MA = ops.mask(live);
+  ops.copy(XP, io.x, MA);
+  ops.copy(rr, io.b, MA); ops.copy(r[0], io.b, MA); ops.copy(BP, io.b, MA);
+  for (C* v : {r[1], r[2], u[0], u[1], u[2], X}) ops.zero(v, MA);
+  std::vector<double2> o;
+  {
+    const C* A1[1] = {r[0]};
+    const int c1[1] = {1};
+    if (ops.dots(1, A1, A1, c1, MA, o)) return 1;
+  }
+  std::vector<double> rnrm0(R), rnrm(R), mxx(R), mxr(R), resid(R);
+  std::vector<Z> alpha(R, 0.0), omega(R, 1.0), sigma(R, 1.0), rho0(R, 1.0), rho1(R, 0.0), beta(R, 0.0);
+  for (int i = 0; i < R; ++i) {
+    rnrm0[i] = std::sqrt(std::max(0.0, o[i].x));
+    rnrm[i] = mxx[i] = mxr[i] = rnrm0[i];
+    resid[i] = rnrm0[i] > 0.0 ? 1.0 : 0.0;
+  }
+  std::vector<int> it(R, 0);
+  int rc;
+  for (;;) {
+    std::vector<int> I(R, 0);
+    for (int i = 0; i < R; ++i) I[i] = live[i] && resid[i] > io.tol && it[i] < io.maxit;
+    if (!any_of(I)) break;
+    for (int i = 0; i < R; ++i)
+      if (I[i]) { it[i]++; rho0[i] = -(omega[i] * rho0[i]); }
+    const int* MI = ops.mask(I);
+    for (int k = 1; k <= 2; ++k) {
+      {
+        const C* A1[1] = {rr};
+        const C* B1[1] = {r[k - 1]};
+        const int c1[1] = {1};
+        if (ops.dots(1, A1, B1, c1, MI, o)) return 1;
+      }
+      std::vector<double2> cb(R), ca(R), cma(R);
+      for (int i = 0; i < R; ++i) {
+        if (!I[i]) continue;
+        rho1[i] = zd2(o[i]);
+        if (rho0[i] == Z(0.0)) { res.status[i] = 95; live[i] = 0; I[i] = 0; continue; }
+        beta[i] = alpha[i] * (rho1[i] / rho0[i]);
+        rho0[i] = rho1[i];
+        cb[i] = dz(-beta[i]);
+      }
+      MI = ops.mask(I);
+      for (int j = 0; j < k; ++j) ops.lin(u[j], cb.data(), r[j], one.data(), nullptr, nullptr, MI);
+      if ((rc = c.mv(u[k - 1], u[k], I))) return rc;
+      {
+        const C* A1[1] = {rr};
+        const C* B1[1] = {u[k]};
+        const int c1[1] = {1};
+        if (ops.dots(1, A1, B1, c1, MI, o)) return 1;
+      }
+      for (int i = 0; i < R; ++i) {
+        if (!I[i]) continue;
+        sigma[i] = zd2(o[i]);
+        if (sigma[i] == Z(0.0)) { res.status[i] = 98; live[i] = 0; I[i] = 0; continue; }
+        alpha[i] = rho1[i] / sigma[i];
+        ca[i] = dz(alpha[i]);
+        cma[i] = dz(-alpha[i]);
+      }
+      MI = ops.mask(I);
+      ops.lin(X, one.data(), u[0], ca.data(), nullptr, nullptr, MI);
+      for (int j = 0; j < k; ++j) ops.lin(r[j], one.data(), u[j + 1], cma.data(), nullptr, nullptr, MI);
+      if ((rc = c.mv(r[k - 1], r[k], I))) return rc;
+      {
+        const C* A1[1] = {r[0]};
+        const int c1[1] = {1};
+        if (ops.dots(1, A1, A1, c1, MI, o)) return 1;
+      }
+      for (int i = 0; i < R; ++i) {
+        if (!I[i]) continue;
+        rnrm[i] = std::sqrt(std::max(0.0, o[i].x));
+        mxx[i] = std::max(mxx[i], rnrm[i]);
+        mxr[i] = std::max(mxr[i], rnrm[i]);
+      }
+    }
+    {
+      const C* A6[6] = {r[0], r[1], r[1], r[2], r[2], r[2]};
+      const C* B6[6] = {r[0], r[0], r[1], r[0], r[1], r[2]};
+      const int c6[6] = {1, 1, 1, 1, 1, 1};
+      if (ops.dots(6, A6, B6, c6, MI, o)) return 1;
+    }
+    std::vector<double2> cy1(R), cy2(R), cmy1(R), cmy2(R);
+    std::vector<int> XPDT(R, 0), RCMP(R, 0);
+    for (int i = 0; i < R; ++i) {
+      if (!I[i]) continue;
+      Z Zm[3][3];
+      Zm[0][0] = zd2(o[6 * i]); Zm[1][0] = zd2(o[6 * i + 1]); Zm[1][1] = zd2(o[6 * i + 2]);
+      Zm[2][0] = zd2(o[6 * i + 3]); Zm[2][1] = zd2(o[6 * i + 4]); Zm[2][2] = zd2(o[6 * i + 5]);
+      Zm[0][1] = std::conj(Zm[1][0]); Zm[0][2] = std::conj(Zm[2][0]); Zm[1][2] = std::conj(Zm[2][1]);
+      auto matv = [&](const Z* v, Z* out) {
+        for (int a = 0; a < 3; ++a) { out[a] = 0.0; for (int b = 0; b < 3; ++b) out[a] += Zm[a][b] * v[b]; }
+      };
+      auto inner = [](const Z* a, const Z* b) { Z sum = 0.0; for (int k = 0; k < 3; ++k) sum += std::conj(a[k]) * b[k]; return sum; };
+      if (Zm[1][1] == Z(0.0)) { res.status[i] = 102; live[i] = 0; I[i] = 0; continue; }
+      Z y0[3] = {-1.0, Zm[1][0] / Zm[1][1], 0.0}, yl[3] = {0.0, Zm[1][2] / Zm[1][1], -1.0}, zy0[3], zyl[3];
+      matv(y0, zy0);
+      matv(yl, zyl);
+      const double k0 = std::sqrt(std::abs(inner(y0, zy0))), kl = std::sqrt(std::abs(inner(yl, zyl)));
+      if (k0 == 0.0 || kl == 0.0) { res.status[i] = 102; live[i] = 0; I[i] = 0; continue; }
+      const Z vr = inner(yl, zy0) / (k0 * kl);
+      const double avr = std::abs(vr);
+      if (avr == 0.0) { res.status[i] = 102; live[i] = 0; I[i] = 0; continue; }
+      const Z fac = vr * (std::max(avr, 0.7) / avr) * (k0 / kl);
+      for (int a = 0; a < 3; ++a) y0[a] -= fac * yl[a];
+      omega[i] = y0[2];
+      matv(y0, zy0);
+      rnrm[i] = std::sqrt(std::abs(inner(y0, zy0)));
+      mxx[i] = std::max(mxx[i], rnrm[i]);
+      mxr[i] = std::max(mxr[i], rnrm[i]);
+      cy1[i] = dz(y0[1]); cy2[i] = dz(y0[2]); cmy1[i] = dz(-y0[1]); cmy2[i] = dz(-y0[2]);
+      XPDT[i] = rnrm[i] < 1.0e-2 * rnrm0[i] && rnrm0[i] < mxx[i];
+      RCMP[i] = (rnrm[i] < 1.0e-2 * mxr[i] && rnrm0[i] < mxr[i]) || XPDT[i];
+      resid[i] = rnrm0[i] > 0.0 ? rnrm[i] / rnrm0[i] : 0.0;
+    }
+    MI = ops.mask(I);
+    ops.lin(u[0], one.data(), u[1], cmy1.data(), u[2], cmy2.data(), MI);
+    ops.lin(X, one.data(), r[0], cy1.data(), r[1], cy2.data(), MI);
+    ops.lin(r[0], one.data(), r[1], cmy1.data(), r[2], cmy2.data(), MI);
+    std::vector<int> CK(R, 0), RS(R, 0);
+    for (int i = 0; i < R; ++i) CK[i] = I[i] && ((it[i] % 20) == 0 || resid[i] <= io.tol);
+    if (any_of(CK)) {
+      if ((rc = c.mv(X, sy, CK))) return rc;
+      std::vector<double2> nn;
+      if (ops.diff_norms(BP, sy, r[0], ops.mask(CK), nn)) return 1;
+      for (int i = 0; i < R; ++i) {
+        if (!CK[i]) continue;
+        const double tr = std::sqrt(std::max(0.0, nn[2 * i].x)), gapn = std::sqrt(std::max(0.0, nn[2 * i + 1].x));
+        const double tres = tr / rnrm0[i];
+        const double gap = tr > 0.0 ? gapn / tr : (gapn == 0.0 ? 0.0 : INFINITY);
+        const bool conv = tres <= io.tol;
+        const bool rest = gap >= 1.0e-3 || (resid[i] <= io.tol && !conv);
+        if (conv) { resid[i] = tres; live[i] = 0; I[i] = 0; continue; }
+        if (rest) { RS[i] = 1; resid[i] = tres; I[i] = 0; }
+      }
+      if (any_of(RS)) {
+        const int* MR = ops.mask(RS);
+        // r0 = BP - A X  (sy holds A X)
+        ops.lin(r[0], nullptr, BP, one.data(), sy, mone.data(), MR);
+        ops.lin(XP, one.data(), X, one.data(), nullptr, nullptr, MR);
+        ops.zero(X, MR);
+        ops.copy(BP, r[0], MR);
+        ops.copy(rr, r[0], MR);
+        for (C* v : {r[1], r[2], u[0], u[1], u[2]}) ops.zero(v, MR);
+        for (int i = 0; i < R; ++i)
+          if (RS[i]) {
+            rnrm[i] = mxx[i] = mxr[i] = resid[i] * rnrm0[i];
+            alpha[i] = 0.0; omega[i] = 1.0; sigma[i] = 1.0; rho0[i] = 1.0;
+          }
+      }
+    }
+    std::vector<int> RC(R, 0), XD(R, 0);
+    for (int i = 0; i < R; ++i) { RC[i] = I[i] && RCMP[i]; XD[i] = RC[i] && XPDT[i]; }
+    if (any_of(RC)) {
+      if ((rc = c.mv(X, sy, RC))) return rc;
+      const int* MC = ops.mask(RC);
+      ops.lin(r[0], nullptr, BP, one.data(), sy, mone.data(), MC);
+      if (any_of(XD)) {
+        const int* MX = ops.mask(XD);
+        ops.lin(XP, one.data(), X, one.data(), nullptr, nullptr, MX);
+        ops.zero(X, MX);
+        ops.copy(BP, r[0], MX);
+      }
+      for (int i = 0; i < R; ++i)
+        if (RC[i]) { mxr[i] = rnrm[i]; if (XD[i]) mxx[i] = rnrm[i]; }
+    }
+  }
+  // X += XP and one final true residual against b (cu:1259-1264)
+  std::vector<int> F(R, 0);
+  for (int i = 0; i < R; ++i) F[i] = res.status[i] == 0;
+  const int* MF = ops.mask(F);
+  ops.lin(X, one.data(), XP, one.data(), nullptr, nullptr, MF);
+  if ((rc = c.mv(X, sy, F))) return rc;
+  std::vector<double2> nn;
+  if (ops.diff_norms(io.b, sy, io.b, MF, nn)) return 1;
+  ops.copy(io.x, X, MF);
+  c.finish_timing();
+  for (int i = 0; i < R; ++i) {
+    res.itno[i] = it[i];
+    res.ncompte[i] = c.nc[i];
+    res.tole[i] = F[i] ? (rnrm0[i] > 0.0 ? std::sqrt(std::max(0.0, nn[2 * i].x)) / rnrm0[i] : INFINITY) : resid[i];
+  }
+  return 0;
+}
+
+template struct BatchOps<float>;
+template struct BatchOps<double>;
+template int solve_batch_qmrccg<float>(BatchIO<float>&, BatchResult&);
+template int solve_batch_qmrccg<double>(BatchIO<double>&, BatchResult&);
+template int solve_batch_pbcgs2<float>(BatchIO<float>&, BatchResult&);
+template int solve_batch_pbcgs2<double>(BatchIO<double>&, BatchResult&);
+
+}  // namespace ddb

@@ -299,6 +299,7 @@ template <typename T> int Engine<T>::build_green(const GreenArgs<T>& ga) {
     const size_t smx = (size_t)2 * 6 * (Mx + 1) * sizeof(double2);
     cudaFuncSetAttribute((const void*)k_green_x, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     k_green_x<<<dim3(My, Mz), 256, smx>>>(p, px, twx_d, a1, nxo, d_status);
+    note_launch();
     if (check_launch("Green direct sum + x FFT")) rc = 4;
     const FftPlan ply = make_fft_plan(My), plz = make_fft_plan(Mz);
     if (!rc) {
@@ -306,6 +307,7 @@ template <typename T> int Engine<T>::build_green(const GreenArgs<T>& ga) {
       const size_t sm = (size_t)2 * TX * My * sizeof(double2);
       cudaFuncSetAttribute((const void*)k_green_col<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
       k_green_col<double2><<<dim3((unsigned)ceil_div(nxo, TX), 6 * Mz), 256, sm>>>(a1, a2, My, nxo, nyo, ply, twy_d, TX);
+      note_launch();
       if (check_launch("Green y FFT")) rc = 5;
     }
     if (!rc) {
@@ -315,6 +317,7 @@ template <typename T> int Engine<T>::build_green(const GreenArgs<T>& ga) {
       cudaFuncSetAttribute((const void*)k_green_col<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
       C* planar = reinterpret_cast<C*>(a1);  // a1 is free now and larger than the result
       k_green_col<C><<<dim3((unsigned)ceil_div(W, TX), 6), 256, sm>>>(a2, planar, Mz, W, nzo, plz, twz_d, TX);
+      note_launch();
       if (check_launch("Green z FFT")) rc = 6;
       if (!rc && interleave_green(planar)) rc = 6;
     }

@@ -550,6 +550,7 @@ static int reg_E(int n) { return n / reg_T(n); }
 
 template <typename T> static int launch_k(const void* f, dim3 g, int threads, size_t sm, cudaStream_t st, MvParams<T>& P) {
   void* args[] = {(void*)&P};
+  note_launch();
   cudaError_t e = cudaLaunchKernel(f, g, dim3(threads), args, sm, st);
   if (e != cudaSuccess) { set_cuda_error("MATVEC launch", e); return 1; }
   return 0;
@@ -730,6 +731,7 @@ template <typename T> int Engine<T>::matvec(const MvArgs<T>& a) {
     } else {
       dim3 gz((unsigned)ceil_div(g.nx, P.tz), (unsigned)g.ny, (unsigned)(3 * nr));
       k_zfwd<T><<<gz, threads, sm_z, stream>>>(P);
+      note_launch();
       if (check_launch("MATVEC z-forward")) return 21;
     }
     for (int rs = 0; rs < nr; rs += slab_nr) {
@@ -743,6 +745,7 @@ template <typename T> int Engine<T>::matvec(const MvArgs<T>& a) {
         } else {
           dim3 gx((unsigned)ceil_div(g.ny, P.ry), (unsigned)P.nplanes, (unsigned)(3 * nrs));
           k_xfwd<T><<<gx, threads, sm_x, stream>>>(P);
+          note_launch();
           if (check_launch("MATVEC x-forward")) return 22;
         }
         if (fy_r) {
@@ -750,6 +753,7 @@ template <typename T> int Engine<T>::matvec(const MvArgs<T>& a) {
         } else {
           dim3 gy((unsigned)ceil_div(g.Mx, P.ty), (unsigned)P.nplanes, (unsigned)nrs);
           k_ygreen<T><<<gy, threads, sm_y, stream>>>(P);
+          note_launch();
           if (check_launch("MATVEC y-Green")) return 23;
         }
         if (fxi_r) {
@@ -757,6 +761,7 @@ template <typename T> int Engine<T>::matvec(const MvArgs<T>& a) {
         } else {
           dim3 gx((unsigned)ceil_div(g.ny, P.ry), (unsigned)P.nplanes, (unsigned)(3 * nrs));
           k_xinv<T><<<gx, threads, sm_x, stream>>>(P);
+          note_launch();
           if (check_launch("MATVEC x-inverse")) return 24;
         }
       }
@@ -766,6 +771,7 @@ template <typename T> int Engine<T>::matvec(const MvArgs<T>& a) {
     } else {
       dim3 gz((unsigned)ceil_div(g.nx, P.tz), (unsigned)g.ny, (unsigned)(3 * nr));
       k_zinv_fin<T><<<gz, threads, sm_z, stream>>>(P);
+      note_launch();
       if (check_launch("MATVEC z-inverse/finish")) return 25;
     }
   }
@@ -784,6 +790,7 @@ template <typename T> int Engine<T>::interleave_green(const C* planar_dev) {
   if (xpipe) return interleave_green_zfast<T>(*this, planar_dev);
   const size_t npts = g.green_count() / 6;
   k_interleave6<C><<<(unsigned)std::min<size_t>(ceil_div(6 * npts, 256), 148 * 32), 256, 0, stream>>>(planar_dev, green, npts);
+  note_launch();
   return check_launch("Green interleave");
 }
 

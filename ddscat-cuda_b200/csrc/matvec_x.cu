@@ -382,6 +382,7 @@ template <typename T> static int xlaunch(const void* f, dim3 g, int th, size_t s
     raised.push_back(f);
   }
   void* args[] = {(void*)&P};
+  note_launch();
   cudaError_t e = cudaLaunchKernel(f, g, dim3(th), args, sm, st);
   if (e != cudaSuccess) { set_cuda_error("MATVEC launch", e); return 1; }
   return 0;
@@ -471,6 +472,7 @@ template <typename T> int interleave_green_zfast(Engine<T>& E, const cplx<T>* pl
   const size_t n = (size_t)6 * X * Y * Z;
   k_interleave6_zfast<cplx<T>><<<(unsigned)std::min<size_t>(ceil_div(n, 256), 148 * 32), 256, 0, E.stream>>>(
       planar, E.green, X, Y, Z);
+  note_launch();
   return check_launch("Green interleave (z-fastest)");
 }
 

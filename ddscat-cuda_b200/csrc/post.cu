@@ -46,6 +46,7 @@ int evalq_compute(Engine<T>& eng, VecOps<T>& ops, const cplx<T>* e, const cplx<T
   const int nat0 = eng.g.nat0;
   k_evalq_q<<<(unsigned)ceil_div(nat0, 256), 256, 0, ops.stream>>>(p, qbuf, adia, aoff, eng.occ, eng.g.nat, nat0, a_full,
                                                                    ak3 / 1.5);
+  note_launch();
   if (check_launch("GPU EVALQ local alpha^-1 P")) return 306;
   const cplx<T>* A[2] = {p, e};
   const cplx<T>* B[2] = {qbuf, p};
@@ -179,6 +180,7 @@ int farfield_sums(Engine<T>& eng, const cplx<T>* p, const float* dirs_host, int 
   if (e != cudaSuccess) { set_cuda_error("SCAT workspace", e); rc = 322; }
   if (!rc) {
     k_pack_coords<<<(unsigned)ceil_div(nat0, 256), 256, 0, s>>>(eng.occ, nat0, nx, ny, coords);
+    note_launch();
     std::vector<double> hd((size_t)3 * chunk);
     const size_t sm = (size_t)FF_DIRS * ntab * sizeof(float2);
     cudaFuncSetAttribute((const void*)k_ff_partial<cplx<T>>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
@@ -188,9 +190,12 @@ int farfield_sums(Engine<T>& eng, const cplx<T>* p, const float* dirs_host, int 
       cudaMemcpyAsync(d_dirs, hd.data(), (size_t)3 * cnt * sizeof(double), cudaMemcpyHostToDevice, s);
       k_ff_tables<<<(unsigned)std::min<size_t>(ceil_div((size_t)cnt * ntab, 256), 4096), 256, 0, s>>>(
           d_dirs, cnt, nx, ny, nz, dx[0], dx[1], dx[2], x0[0], x0[1], x0[2], tab);
+      note_launch();
       dim3 grid((unsigned)nblocks, (unsigned)ceil_div(cnt, FF_DIRS));
       k_ff_partial<cplx<T>><<<grid, FF_THREADS, sm, s>>>(p, coords, nat0, cnt, nx, ny, nz, tab, sites_per_block, partials);
+      note_launch();
       k_ff_final<<<(unsigned)ceil_div((size_t)cnt * 3, 128), 128, 0, s>>>(partials, nblocks, cnt * 3, sums);
+      note_launch();
       if (check_launch("SCAT far-field sums")) { rc = 325; break; }
       e = cudaMemcpyAsync(sums_host + (size_t)3 * off, sums, (size_t)3 * cnt * sizeof(double2), cudaMemcpyDeviceToHost, s);
       if (e == cudaSuccess) e = cudaStreamSynchronize(s);

@@ -128,6 +128,7 @@ template <typename T> static int run_dots(VecOps<T>& o, int n, DotSpec<T>& sp, d
   const int need = (int)ceil_div((size_t)std::max(n, 1), RED_THREADS);
   if (need < nb) nb = need;
   k_dots<T><<<nb, RED_THREADS, 0, o.stream>>>(n, sp, o.d_red, o.d_out, o.d_count);
+  note_launch();
   if (check_launch("FP64 inner product")) return 1;
   cudaError_t e = cudaMemcpyAsync(o.h_out, o.d_out, sp.k * sizeof(double2), cudaMemcpyDeviceToHost, o.stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(o.stream);
@@ -224,24 +225,32 @@ template <typename C> __global__ void k_scatter(const C* compact, C* full, const
 
 static inline unsigned grid_for(size_t n) { return (unsigned)std::min<size_t>(ceil_div(std::max<size_t>(n, 1), 256), 148 * 16); }
 
-template <typename T> void v_copy(cplx<T>* d, const cplx<T>* a, int n, cudaStream_t s) { k_copy<<<grid_for(n), 256, 0, s>>>(d, a, n); }
+template <typename T> void v_copy(cplx<T>* d, const cplx<T>* a, int n, cudaStream_t s) {
+  k_copy<<<grid_for(n), 256, 0, s>>>(d, a, n);
+  note_launch();
+}
 template <typename T> void v_zero(cplx<T>* d, int n, cudaStream_t s) { k_zero<<<grid_for(n), 256, 0, s>>>(d, n); }
 template <typename T> void v_diff(cplx<T>* d, const cplx<T>* a, const cplx<T>* b, int n, cudaStream_t s) {
   k_diff<<<grid_for(n), 256, 0, s>>>(d, a, b, n);
+  note_launch();
 }
 template <typename T>
 void v_lincomb(cplx<T>* d, double2 zd, const cplx<T>* a, double2 za, const cplx<T>* b, double2 zb, int n, cudaStream_t s) {
   k_lincomb<<<grid_for(n), 256, 0, s>>>(d, zd, a, za, b, zb, n);
+  note_launch();
 }
 template <typename T>
 void v_precon(cplx<T>* d, const cplx<T>* a, const cplx<T>* adia_full, const int* occ, int nat, int nat0, cudaStream_t s) {
   k_precon<<<grid_for((size_t)3 * nat0), 256, 0, s>>>(d, a, adia_full, occ, nat, nat0);
+  note_launch();
 }
 template <typename T> void v_gather(const cplx<T>* full, cplx<T>* compact, const int* occ, int nat, int nat0, cudaStream_t s) {
   k_gather<<<grid_for((size_t)3 * nat0), 256, 0, s>>>(full, compact, occ, nat, nat0);
+  note_launch();
 }
 template <typename T> void v_scatter(const cplx<T>* compact, cplx<T>* full, const int* occ, int nat, int nat0, cudaStream_t s) {
   k_scatter<<<grid_for((size_t)3 * nat0), 256, 0, s>>>(compact, full, occ, nat, nat0);
+  note_launch();
 }
 
 #define DDB_INST(T)                                                                                              \

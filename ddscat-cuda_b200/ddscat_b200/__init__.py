@@ -26,7 +26,8 @@ EXPORTS = (
     ["ddscat_cuda_prepare_green_f32", "ddscat_cuda_prepare_f32", "ddscat_cuda_apply_f32"]
     + [f"ddscat_cuda_solve_{s}_f32" for s in SOLVERS]
     + ["ddscat_cuda_evalq_f32", "ddscat_cuda_scat_f32", "ddscat_cuda_release", "ddscat_cuda_last_error"]
-    + ["ddscat_b200_set_verbose", "ddscat_b200_layout", "ddscat_b200_matvec_timing"]
+    + ["ddscat_b200_set_verbose", "ddscat_b200_layout", "ddscat_b200_matvec_timing", "ddscat_b200_solve_batch_f32",
+       "ddscat_b200_last_solve_stats", "ddscat_b200_residual_f64", "ddscat_b200_launch_count"]
 )
 
 
@@ -77,6 +78,14 @@ def _declare(lib):
     lib.ddscat_b200_layout.restype = _I
     lib.ddscat_b200_matvec_timing.argtypes = [_I, _I, _I, ct.POINTER(_F)]
     lib.ddscat_b200_matvec_timing.restype = _I
+    lib.ddscat_b200_solve_batch_f32.argtypes = [_I, _I, _P, _P, _P, _P, _I, _F, _P, _P, _P, _P]
+    lib.ddscat_b200_solve_batch_f32.restype = _I
+    lib.ddscat_b200_last_solve_stats.argtypes = [_D, ct.POINTER(ct.c_longlong), ct.POINTER(_I)]
+    lib.ddscat_b200_last_solve_stats.restype = _I
+    lib.ddscat_b200_residual_f64.argtypes = [_I, _P, _P, _P, _P, _D]
+    lib.ddscat_b200_residual_f64.restype = _I
+    lib.ddscat_b200_launch_count.argtypes = []
+    lib.ddscat_b200_launch_count.restype = ct.c_ulonglong
 
 
 _LIBS = {}
@@ -104,6 +113,27 @@ def _c64(a, n=None):
     if n is not None and a.size != n:
         raise ValueError(f"expected {n} elements, got {a.size}")
     return a
+
+
+BATCH_SOLVERS = {"qmrccg": 1, "pbcgs2": 2}
+
+
+def _vptr(a):
+    """Pointer of a host NumPy array or of a CUDA tensor (``data_ptr()``)."""
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return ct.c_void_p(a.data_ptr())
+    return a.ctypes.data_as(ct.c_void_p)
+
+
+@dataclass
+class BatchOut:
+    rc: int
+    itno: np.ndarray
+    tole: np.ndarray
+    ncompte: np.ndarray
+    status: np.ndarray
 
 
 @dataclass
@@ -199,10 +229,45 @@ class DDA:
         return {"cbksca": cb.value, "csca": cs.value, "cscag": [cg[0], cg[1], cg[2]], "cscag2": cg2.value,
                 "navg": navg.value, "f1": f1[:ndir], "f2": f2[:ndir]}
 
+    def solve_batch(self, name, b, x, adia, aoff=None, maxit=300, tol=1e-5, check=True):
+        """Batched solve; b, x (in/out), adia, aoff are (nrhs, 3*NAT) complex64
+        host arrays, or CUDA tensors of the same shape (device-resident path)."""
+        nrhs = int(b.shape[0])
+        for a in (b, x, adia) + (() if aoff is None else (aoff,)):
+            if tuple(a.shape) != (nrhs, 3 * self.nat):
+                raise ValueError(f"expected shape {(nrhs, 3 * self.nat)}, got {tuple(a.shape)}")
+            if not hasattr(a, "data_ptr") and (a.dtype != np.complex64 or not a.flags.c_contiguous):
+                raise ValueError("host arrays must be C-contiguous complex64")
+        it = np.zeros(nrhs, dtype=np.int32)
+        tole = np.zeros(nrhs, dtype=np.float32)
+        nc = np.zeros(nrhs, dtype=np.int32)
+        st = np.zeros(nrhs, dtype=np.int32)
+        rc = self.lib.ddscat_b200_solve_batch_f32(BATCH_SOLVERS[name], nrhs, _vptr(b), _vptr(x), _vptr(adia),
+                                                  _vptr(aoff), maxit, tol, _ptr(it), _ptr(tole), _ptr(nc), _ptr(st))
+        if check:
+            self._check("solve_batch", rc)
+        return BatchOut(rc, it, tole, nc, st)
+
+    def last_solve_stats(self):
+        ms, rhs, calls = ct.c_double(), ct.c_longlong(), _I()
+        self.lib.ddscat_b200_last_solve_stats(ct.byref(ms), ct.byref(rhs), ct.byref(calls))
+        return ms.value, rhs.value, calls.value
+
+    def residual_f64(self, b, x, adia, aoff=None):
+        nrhs = int(b.shape[0])
+        out = np.zeros(nrhs, dtype=np.float64)
+        rc = self.lib.ddscat_b200_residual_f64(nrhs, _vptr(b), _vptr(x), _vptr(adia), _vptr(aoff),
+                                               out.ctypes.data_as(_D))
+        self._check("residual_f64", rc)
+        return out
+
     def matvec_ms(self, nrhs=1, iters=10, cwhat="N"):
         ms = _F(0.0)
         self._check("matvec_timing", self.lib.ddscat_b200_matvec_timing(nrhs, iters, ord(cwhat), ct.byref(ms)))
         return ms.value
+
+    def launch_count(self):
+        return int(self.lib.ddscat_b200_launch_count())
 
     def release(self):
         return self.lib.ddscat_cuda_release()

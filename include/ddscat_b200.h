@@ -19,12 +19,47 @@ DDSCAT_CUDA_API int ddscat_b200_set_verbose(int level);
  * (libddscat_matvec_cuda_slice.so). */
 DDSCAT_CUDA_API int ddscat_b200_layout(void);
 
+/* Number of CUDA kernels this library has launched since it was loaded. */
+DDSCAT_CUDA_API unsigned long long ddscat_b200_launch_count(void);
+
 /* Times the device-resident MATVEC of the prepared target: nrhs right-hand
  * sides per call (compact layout, per-RHS CXADIA, no CXAOFF), `iters` calls
  * after 3 warm-up calls, CUDA events on the library stream.  Writes the mean
  * milliseconds per call.  Allocates its own scratch vectors.  Codes: 400
  * invalid / not prepared, 401 allocation, 402 CUDA failure. */
 DDSCAT_CUDA_API int ddscat_b200_matvec_timing(int nrhs, int iters, int cwhat, float *ms_per_call);
+
+/* Batched solve of nrhs systems A_r x_r = b_r that share the prepared target
+ * and Green tensor (same |k|; CXADIA/CXAOFF may differ per right-hand side,
+ * e.g. per orientation and polarisation).  b, x (initial guess in, solution
+ * out), adia and aoff are arrays of nrhs full vectors (3*NAT complex float
+ * each, RHS r at element offset r*3*NAT), all host pointers or all device
+ * pointers; aoff may be NULL (no off-diagonal site blocks).  Each RHS follows
+ * the recurrence of the single-RHS entry point of the same solver (reliable
+ * residual every 20 iterations, restart policy, MATVEC count); every kernel
+ * launch covers all RHS still iterating.  Per-RHS outputs: itno, tole
+ * (achieved true relative residual), ncompte, status (0, or the error code
+ * the single-RHS entry point would have returned for that RHS).
+ * solver: DDSCAT_B200_QMRCCG or DDSCAT_B200_PBCGS2.
+ * Codes: 500 invalid argument / not prepared, 501 solver, 502 mixed pointer
+ * kinds, 503 workspace allocation, 504 input transfer, 505 solver failure,
+ * 506 output transfer. */
+#define DDSCAT_B200_QMRCCG 1
+#define DDSCAT_B200_PBCGS2 2
+DDSCAT_CUDA_API int ddscat_b200_solve_batch_f32(int solver, int nrhs, const void *b, void *x, const void *adia,
+                                                const void *aoff, int maxit, float tol, int *itno, float *tole,
+                                                int *ncompte, int *status);
+
+/* CUDA-event time spent in MATVECs during the last batched solve, the number
+ * of single-RHS MATVECs it performed and the number of batched MATVEC calls. */
+DDSCAT_CUDA_API int ddscat_b200_last_solve_stats(double *matvec_ms, long long *rhs_matvecs, int *matvec_calls);
+
+/* FP64 true relative residuals ||b_r - A x_r|| / ||b_r|| with the operator
+ * evaluated entirely in FP64 on the GPU (FP64 Green tensor, FP64 FFTs).
+ * Arrays as in ddscat_b200_solve_batch_f32; aoff may be NULL.  Codes: 510
+ * invalid, 511 FP64 engine setup, 512 transfer, 513 reduction. */
+DDSCAT_CUDA_API int ddscat_b200_residual_f64(int nrhs, const void *b, const void *x, const void *adia,
+                                             const void *aoff, double *resid);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,94 @@
+"""GPU tests of the batched multi-RHS solve (ddscat_b200_solve_batch_f32) and
+the all-FP64 residual check (ddscat_b200_residual_f64).
+
+Each RHS of a batch must behave like the single-RHS entry point of the same
+solver: TOLE <= TOL, iteration count within max(1, 10 %) of the single solve
+(reductions are grouped differently, so the last bit can differ), solution
+within 20*TOL, and an FP64 true residual <= 1.2*TOL."""
+import numpy as np
+import pytest
+
+import ddscat_b200 as D
+from ddscat_b200 import targets
+from oracle import ddscat_oracle as O
+
+TOL = 1e-5
+
+
+def _batch_inputs(prob):
+    R = len(prob.incid)
+    b = np.stack([prob.rhs(r) for r in range(R)])
+    adia = np.stack([prob.adia(r) for r in range(R)])
+    return b, adia
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [12, 16])
+@pytest.mark.parametrize("name", ["qmrccg", "pbcgs2"])
+def test_batch_matches_single(name, n):
+    orients = targets.random_orientations(3, seed=1)
+    prob = targets.make_problem(n, m=1.33 + 0.05j, x=2.0, semi=(n / 2, 0.8 * n / 2, 0.6 * n / 2),
+                                orientations=orients)
+    R = len(prob.incid)
+    dda = D.DDA()
+    dda.prepare_green(n, n, n, prob.iocc, prob.incid[0].k)
+    b, adia = _batch_inputs(prob)
+    x = np.zeros_like(b)
+    out = dda.solve_batch(name, b, x, adia, None, maxit=400, tol=TOL)
+    assert np.all(out.status == 0)
+    assert np.all(out.tole <= TOL)
+    res64 = dda.residual_f64(b, x, adia)
+    assert np.all(res64 <= 1.2 * TOL), res64
+    for r in range(R):
+        single = dda.solve(name, b[r], adia[r], prob.aoff(), maxit=400, tol=TOL)
+        assert abs(single.itno - out.itno[r]) <= max(1, 0.1 * single.itno), (r, single.itno, out.itno[r])
+        assert np.linalg.norm(single.x - x[r]) / np.linalg.norm(single.x) < 20 * TOL
+    ms, rhs, calls = dda.last_solve_stats()
+    assert rhs == int(out.ncompte.sum()) and calls > 0 and ms > 0
+    dda.release()
+
+
+@pytest.mark.gpu
+def test_batch_device_pointers_and_breakdown_mask():
+    torch = pytest.importorskip("torch")
+    n = 16
+    prob = targets.make_problem(n, m=1.5 + 0.01j, x=2.0, orientations=targets.random_orientations(2, seed=3))
+    dda = D.DDA()
+    dda.prepare_green(n, n, n, prob.iocc, prob.incid[0].k)
+    b, adia = _batch_inputs(prob)
+    b[1] = 0  # a zero right-hand side is rejected for that RHS only (QMRCCG code 52)
+    xh = np.zeros_like(b)
+    host = dda.solve_batch("qmrccg", b, xh, adia, maxit=300, tol=TOL)
+    assert host.status[1] == 52 and np.all(np.delete(host.status, 1) == 0)
+    bd = torch.from_numpy(b).cuda()
+    ad = torch.from_numpy(adia).cuda()
+    xd = torch.zeros_like(bd)
+    dev = dda.solve_batch("qmrccg", bd, xd, ad, maxit=300, tol=TOL)
+    np.testing.assert_array_equal(dev.itno, host.itno)
+    np.testing.assert_array_equal(dev.status, host.status)
+    assert np.allclose(xd.cpu().numpy(), xh, rtol=0, atol=1e-6 * np.abs(xh).max())
+    dda.release()
+
+
+@pytest.mark.gpu
+def test_residual_f64_matches_oracle():
+    n = 12
+    prob = targets.make_problem(n, m=1.5 + 0.01j, x=2.0)
+    rng = np.random.default_rng(5)
+    dda = D.DDA()
+    dda.prepare_green(n, n, n, prob.iocc, prob.incid[0].k)
+    b, adia = _batch_inputs(prob)
+    x = (rng.normal(size=b.shape) + 1j * rng.normal(size=b.shape)).astype(np.complex64) * 0.1
+    x[:, np.tile(prob.iocc == 0, 3)] = 0
+    aoff = (0.05 * (rng.normal(size=b.shape) + 1j * rng.normal(size=b.shape))).astype(np.complex64)
+    got = dda.residual_f64(b, x, adia, aoff)
+    gp = O.GreenParams(n, n, n, ak=tuple(float(np.float32(a)) for a in prob.incid[0].k))
+    op = O.Operator.from_params(gp, prob.iocc)
+    for r in range(b.shape[0]):
+        y = op.apply_full(x[r], adia[r], aoff[r])
+        occ = op.occ
+        bc = O.gather_compact(b[r], occ, op.nat).astype(np.complex128)  # float64 norms
+        yc = O.gather_compact(y, occ, op.nat)
+        ref = np.linalg.norm(bc - yc) / np.linalg.norm(bc)
+        assert abs(got[r] - ref) <= 1e-9 * ref
+    dda.release()
