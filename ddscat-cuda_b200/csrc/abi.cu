@@ -339,6 +339,10 @@ static int ensure_f64() {
 }
 
 
+// The prepared FP32 engine, or null before a successful prepare (read-only
+// access for entry points defined in other translation units).
+const Engine<float>* prepared_engine() { return s.ready ? &s.eng : nullptr; }
+
 }  // namespace ddb
 
 using namespace ddb;

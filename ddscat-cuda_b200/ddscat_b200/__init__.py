@@ -27,7 +27,8 @@ EXPORTS = (
     + [f"ddscat_cuda_solve_{s}_f32" for s in SOLVERS]
     + ["ddscat_cuda_evalq_f32", "ddscat_cuda_scat_f32", "ddscat_cuda_release", "ddscat_cuda_last_error"]
     + ["ddscat_b200_set_verbose", "ddscat_b200_layout", "ddscat_b200_matvec_timing", "ddscat_b200_solve_batch_f32",
-       "ddscat_b200_last_solve_stats", "ddscat_b200_residual_f64", "ddscat_b200_launch_count"]
+       "ddscat_b200_last_solve_stats", "ddscat_b200_residual_f64", "ddscat_b200_launch_count",
+       "ddscat_b200_apply_noalloc_f32"]
 )
 
 
@@ -84,6 +85,8 @@ def _declare(lib):
     lib.ddscat_b200_last_solve_stats.restype = _I
     lib.ddscat_b200_residual_f64.argtypes = [_I, _P, _P, _P, _P, _D]
     lib.ddscat_b200_residual_f64.restype = _I
+    lib.ddscat_b200_apply_noalloc_f32.argtypes = [_I, _P, _P, _P, _P, _P]
+    lib.ddscat_b200_apply_noalloc_f32.restype = _I
     lib.ddscat_b200_launch_count.argtypes = []
     lib.ddscat_b200_launch_count.restype = ct.c_ulonglong
 

@@ -61,6 +61,25 @@ DDSCAT_CUDA_API int ddscat_b200_last_solve_stats(double *matvec_ms, long long *r
 DDSCAT_CUDA_API int ddscat_b200_residual_f64(int nrhs, const void *b, const void *x, const void *adia,
                                              const void *aoff, double *resid);
 
+/* MATVEC that allocates no device memory; no counterpart in the reference.
+ * For callers that cannot call cudaMalloc where they need the operator (inside
+ * CUDA stream capture, in allocation-free real-time loops, or with all device
+ * memory handed to their own pool): y = A x (cwhat 'N') or A^H x ('C') for the
+ * prepared target, with x, y, adia and aoff caller-owned DEVICE vectors in the
+ * full layout of ddscat_cuda_apply_f32 (3*NAT complex floats; aoff may be
+ * NULL), launched on `stream` (a cudaStream_t, NULL for the legacy default
+ * stream).  The MATVEC scratch is a fixed 48 MiB array in the library's device
+ * image, so only targets with NAT <= 349,525 sites (e.g. 64^3) are accepted;
+ * every GPU that loads the library holds that array until exit.  All calls
+ * share it and it keeps the last call's contents (nothing needs to start at
+ * zero); calls that overlap on the GPU race, so serialise them.  The first call
+ * on a device (and the first after each prepare) does one-time set-up and
+ * should come before any stream capture.  Codes: 600 invalid argument or not
+ * prepared, 601 target larger than the fixed scratch, 602 scratch address
+ * lookup failed, 21-25 kernel launch failure. */
+DDSCAT_CUDA_API int ddscat_b200_apply_noalloc_f32(int cwhat, const void *x, void *y, const void *adia,
+                                                  const void *aoff, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,71 @@
+"""The allocation-free MATVEC entry point, ddscat_b200_apply_noalloc_f32.
+
+It exists for callers that cannot allocate device memory where they need the
+operator (code inside CUDA stream capture, allocation-free real-time loops,
+applications that give all device memory to their own pool).  It must return
+the same y as ddscat_cuda_apply_f32 on the same inputs (FP32 tolerance 2e-5
+relative, as in test_gpu_matvec.py) on two calls in a row, leave the free
+device memory unchanged, and reject targets larger than its fixed scratch.
+This file is named to be collected last."""
+import ctypes as ct
+
+import numpy as np
+import pytest
+
+import ddscat_b200 as D
+
+RTOL = 2e-5
+
+
+def _inputs(dims, seed):
+    rng = np.random.default_rng(seed)
+    nat = int(np.prod(dims))
+    iocc = (rng.random(nat) < 0.8).astype(np.int16)
+    iocc[0] = 1
+    ak = tuple(rng.normal(size=3) * 0.4)
+    c = lambda s=1.0: (s * (rng.normal(size=3 * nat) + 1j * rng.normal(size=3 * nat))).astype(np.complex64)  # noqa: E731
+    return iocc, ak, c(), c(), c(), c(0.3)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dims", [(16, 16, 16), (12, 10, 9)])
+def test_apply_noalloc_matches_apply(dims):
+    torch = pytest.importorskip("torch")
+    iocc, ak, x1, x2, adia, aoff = _inputs(dims, 7)
+    dda = D.DDA()
+    dda.prepare_green(*dims, iocc, ak)
+    lib = dda.lib
+    dev = torch.device("cuda", torch.cuda.current_device())
+    xd1, xd2 = torch.from_numpy(x1).to(dev), torch.from_numpy(x2).to(dev)
+    ad, od = torch.from_numpy(adia).to(dev), torch.from_numpy(aoff).to(dev)
+    yd1, yd2 = torch.empty_like(xd1), torch.empty_like(xd1)
+    p = lambda t: ct.c_void_p(t.data_ptr())  # noqa: E731
+    # first call on this device: one-time set-up (scratch address lookup)
+    assert lib.ddscat_b200_apply_noalloc_f32(ord("N"), p(xd1), p(yd1), p(ad), p(od), None) == 0
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    # two calls in a row, different inputs and CWHAT
+    assert lib.ddscat_b200_apply_noalloc_f32(ord("N"), p(xd1), p(yd1), p(ad), p(od), None) == 0
+    assert lib.ddscat_b200_apply_noalloc_f32(ord("C"), p(xd2), p(yd2), p(ad), p(od), None) == 0
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    for yd, xh, cw in ((yd1, x1, "N"), (yd2, x2, "C")):
+        ref = dda.apply(xh, adia, aoff, cw)
+        got = yd.cpu().numpy()
+        assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= RTOL
+    dda.release()
+
+
+@pytest.mark.gpu
+def test_apply_noalloc_rejects_large_target():
+    torch = pytest.importorskip("torch")
+    dims = (72, 72, 72)  # NAT = 373,248 > 349,525
+    nat = int(np.prod(dims))
+    dda = D.DDA()
+    dda.prepare_green(*dims, np.ones(nat, dtype=np.int16), (0.3, 0.0, 0.0))
+    t = torch.zeros(3 * nat, dtype=torch.complex64, device="cuda")
+    p = ct.c_void_p(t.data_ptr())
+    rc = dda.lib.ddscat_b200_apply_noalloc_f32(ord("N"), p, p, p, None, None)
+    assert rc == 601
+    assert b"at most" in dda.lib.ddscat_cuda_last_error()
+    dda.release()
