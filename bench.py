@@ -51,7 +51,9 @@ def parse_args():
     ap.add_argument("--solver", default="qmrccg", choices=["qmrccg", "pbcgs2"])
     ap.add_argument("--tol", type=float, default=1e-5)
     ap.add_argument("--maxit", type=int, default=4000)
-    ap.add_argument("--ref-rhs", type=int, default=2, help="RHS per step of the reference arm")
+    ap.add_argument("--policy", default="replace", choices=["replace", "restart"],
+                    help="reliable-residual policy of the batched solve: residual replacement or restart")
+    ap.add_argument("--ref-rhs", type=int, default=0, help="RHS per step of the reference arm (0: the whole batch)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -173,7 +175,8 @@ def config(args, prob, R, world):
             "n": args.n, "nat": prob.nat, "nat0": prob.nat0, "rhs_per_rank": R, "solver": args.solver,
             "tol": args.tol, "fp64_check": "GPU all-FP64 MATVEC true residual, every RHS, every step",
             "l2": "inputs larger than L2 (each RHS vector 3*NAT*8 B > 50 MB; working set > 1 GB)",
-            "parallelism": f"replicas x{world} (independent RHS batches per GPU)"}
+            "parallelism": f"replicas x{world} (independent RHS batches per GPU)",
+            "reliable_residual_policy": getattr(args, "policy", "restart")}
 
 
 def algorithmic_bytes_per_matvec(prob, rhs_per_call):
@@ -253,7 +256,8 @@ def run_ours(args):
 
     def solve_to_fp64(bx, xx, ax, on_device):
         """One step: batched solve, FP64 true residuals, re-solve failures."""
-        out = dda.solve_batch(args.solver, bx, xx, ax, None, maxit=args.maxit, tol=args.tol)
+        rep = args.policy == "replace"
+        out = dda.solve_batch(args.solver, bx, xx, ax, None, maxit=args.maxit, tol=args.tol, replace=rep)
         ms, rhs, calls = dda.last_solve_stats()
         stats["mv_ms"] += ms
         stats["mv_rhs"] += rhs
@@ -266,7 +270,7 @@ def run_ours(args):
             tol *= 0.5
             sub = (lambda a: a[bad].contiguous()) if on_device else (lambda a: np.ascontiguousarray(a[bad]))
             xs = sub(xx)
-            o2 = dda.solve_batch(args.solver, sub(bx), xs, sub(ax), None, maxit=args.maxit, tol=tol)
+            o2 = dda.solve_batch(args.solver, sub(bx), xs, sub(ax), None, maxit=args.maxit, tol=tol, replace=rep)
             xx[bad] = xs
             out.itno[bad] += o2.itno
             out.ncompte[bad] += o2.ncompte
@@ -387,7 +391,7 @@ def run_reference(args):
     fn.argtypes = [ct.c_void_p] * 4 + [ct.c_int, ct.c_int, ct.c_float] + [ct.c_void_p] * 3
     prob, b, adia = workload(args, 0)
     aoff = np.zeros(b.shape[1], dtype=np.complex64)
-    nref = min(args.ref_rhs, b.shape[0])
+    nref = b.shape[0] if args.ref_rhs <= 0 else min(args.ref_rhs, b.shape[0])
     k = prob.incid[0].k
     with quiet_stdout():
         rc = lib.ddscat_cuda_prepare_green_f32(prob.nx, prob.ny, prob.nz, 0, prob.nat, prob.nat0, 0, 0.0, 0.0, 0.0,
@@ -397,8 +401,8 @@ def run_reference(args):
         return
     iters = []
 
-    def step(record):
-        for r in range(nref):
+    def step(record, count=nref):
+        for r in range(count):
             x = np.zeros(b.shape[1], dtype=np.complex64)
             it, tole, nc = ct.c_int(), ct.c_float(), ct.c_int()
             rr = fn(P(b[r]), P(x), P(adia[r]), P(aoff), b.shape[1], args.maxit, args.tol, ct.byref(it),
@@ -410,7 +414,7 @@ def run_reference(args):
 
     with quiet_stdout():
         for _ in range(args.warmup):
-            step(False)
+            step(False, 1)  # warm-up: one RHS per step
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -422,9 +426,10 @@ def run_reference(args):
     value = nref * args.steps / elapsed
     sample = (f"reference ddscat_matvec_cuda.cu built unmodified (oracle/Makefile), {args.solver.upper()} through its "
               f"own C ABI with host buffers, one RHS at a time, {nref} RHS per step (RHS 0..{nref - 1} of the "
-              f"workload); the reference implementation of this path runs on the GPU, its host side on 1 thread")
+              f"workload), its own restart policy; the reference implementation of this path runs on the GPU, its host side on 1 thread")
     cfg = config(args, prob, b.shape[0], world)
     cfg["reference_rhs_per_step"] = nref
+    cfg["reliable_residual_policy"] = "restart (the reference's own)"
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed * 1000.0 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c64 (FP32 complex bulk, FP64 dots)",

@@ -438,7 +438,7 @@ template <typename T> int solve_batch_qmrccg(BatchIO<T>& io, BatchResult& res) {
       if ((rc = c.mv(xs, sy, CK))) return rc;
       std::vector<double2> nn;
       if (ops.diff_norms(io.b, sy, r, ops.mask(CK), nn)) return 1;
-      std::vector<int> RS(R, 0);
+      std::vector<int> RS(R, 0), RP(R, 0);
       for (int i = 0; i < R; ++i) {
         if (!CK[i]) continue;
         const double tr = std::sqrt(std::max(0.0, nn[2 * i].x)), gapn = std::sqrt(std::max(0.0, nn[2 * i + 1].x));
@@ -447,7 +447,13 @@ template <typename T> int solve_batch_qmrccg(BatchIO<T>& io, BatchResult& res) {
         const bool conv = tres <= io.tol;
         const bool rest = gap >= 1.0e-3 || (resid[i] <= io.tol && !conv);
         if (conv) { resid[i] = tres; live[i] = 0; continue; }
-        if (rest) { RS[i] = 1; resid[i] = tres; }
+        if (rest && io.replace) { RP[i] = 1; resid[i] = tres; }
+        else if (rest) { RS[i] = 1; resid[i] = tres; }
+      }
+      if (any_of(RP)) {
+        // residual replacement: r = b - A x; the Lanczos vectors and scalars
+        // do not depend on r, so the iterates are unchanged
+        ops.lin(r, nullptr, io.b, one.data(), sy, mone.data(), ops.mask(RP));
       }
       if (any_of(RS)) {
         const int* MR = ops.mask(RS);
@@ -605,7 +611,7 @@ template <typename T> int solve_batch_pbcgs2(BatchIO<T>& io, BatchResult& res) {
     ops.lin(u[0], one.data(), u[1], cmy1.data(), u[2], cmy2.data(), MI);
     ops.lin(X, one.data(), r[0], cy1.data(), r[1], cy2.data(), MI);
     ops.lin(r[0], one.data(), r[1], cmy1.data(), r[2], cmy2.data(), MI);
-    std::vector<int> CK(R, 0), RS(R, 0);
+    std::vector<int> CK(R, 0), RS(R, 0), RP(R, 0);
     for (int i = 0; i < R; ++i) CK[i] = I[i] && ((it[i] % 20) == 0 || resid[i] <= io.tol);
     if (any_of(CK)) {
       if ((rc = c.mv(X, sy, CK))) return rc;
@@ -619,7 +625,15 @@ template <typename T> int solve_batch_pbcgs2(BatchIO<T>& io, BatchResult& res) {
         const bool conv = tres <= io.tol;
         const bool rest = gap >= 1.0e-3 || (resid[i] <= io.tol && !conv);
         if (conv) { resid[i] = tres; live[i] = 0; I[i] = 0; continue; }
-        if (rest) { RS[i] = 1; resid[i] = tres; I[i] = 0; }
+        if (rest && io.replace) { RP[i] = 1; resid[i] = tres; }
+        else if (rest) { RS[i] = 1; resid[i] = tres; I[i] = 0; }
+      }
+      if (any_of(RP)) {
+        // residual replacement: r0 = BP - A X, shadow residual and search
+        // directions kept
+        ops.lin(r[0], nullptr, BP, one.data(), sy, mone.data(), ops.mask(RP));
+        for (int i = 0; i < R; ++i)
+          if (RP[i]) { rnrm[i] = resid[i] * rnrm0[i]; mxr[i] = std::max(mxr[i], rnrm[i]); }
       }
       if (any_of(RS)) {
         const int* MR = ops.mask(RS);

@@ -67,6 +67,11 @@ template <typename T> struct BatchIO {
   int maxit = 0;
   double tol = 0.0;
   int verbose = 0;
+  // Reliable-residual policy at a check that finds no convergence: 0 restarts
+  // the Krylov process from the true residual when the gap test fails (the
+  // single-RHS entry points); 1 replaces the recursive residual by the true
+  // one and keeps the Krylov state (residual replacement).
+  int replace = 0;
   double matvec_ms = 0.0;         // CUDA-event time of the MATVECs inside the solve
   long long matvec_rhs = 0;       // RHS-MATVECs performed
   int matvec_calls = 0;

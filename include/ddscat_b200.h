@@ -40,12 +40,17 @@ DDSCAT_CUDA_API int ddscat_b200_matvec_timing(int nrhs, int iters, int cwhat, fl
  * launch covers all RHS still iterating.  Per-RHS outputs: itno, tole
  * (achieved true relative residual), ncompte, status (0, or the error code
  * the single-RHS entry point would have returned for that RHS).
- * solver: DDSCAT_B200_QMRCCG or DDSCAT_B200_PBCGS2.
+ * solver: DDSCAT_B200_QMRCCG or DDSCAT_B200_PBCGS2, optionally OR'ed with
+ * DDSCAT_B200_REPLACE_RESIDUAL: at a reliable-residual check that finds the
+ * RHS unconverged with a large gap, replace the recursive residual by the
+ * true one and keep the Krylov state, instead of restarting the solver from
+ * the true residual (convergence is still declared on the true residual).
  * Codes: 500 invalid argument / not prepared, 501 solver, 502 mixed pointer
  * kinds, 503 workspace allocation, 504 input transfer, 505 solver failure,
  * 506 output transfer. */
 #define DDSCAT_B200_QMRCCG 1
 #define DDSCAT_B200_PBCGS2 2
+#define DDSCAT_B200_REPLACE_RESIDUAL 0x100
 DDSCAT_CUDA_API int ddscat_b200_solve_batch_f32(int solver, int nrhs, const void *b, void *x, const void *adia,
                                                 const void *aoff, int maxit, float tol, int *itno, float *tole,
                                                 int *ncompte, int *status);

@@ -92,3 +92,25 @@ def test_residual_f64_matches_oracle():
         ref = np.linalg.norm(bc - yc) / np.linalg.norm(bc)
         assert abs(got[r] - ref) <= 1e-9 * ref
     dda.release()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["qmrccg", "pbcgs2"])
+def test_batch_residual_replacement(name):
+    """Residual replacement instead of restarts (DDSCAT_B200_REPLACE_RESIDUAL):
+    every RHS still converges on its true residual, passes the FP64 check and
+    agrees with the restart-policy solution."""
+    n = 24
+    prob = targets.make_problem(n, m=1.33 + 0.05j, x=6.0, orientations=targets.random_orientations(3, seed=7))
+    dda = D.DDA()
+    dda.prepare_green(n, n, n, prob.iocc, prob.incid[0].k)
+    b, adia = _batch_inputs(prob)
+    xr, xp = np.zeros_like(b), np.zeros_like(b)
+    rest = dda.solve_batch(name, b, xr, adia, maxit=2000, tol=TOL)
+    rep = dda.solve_batch(name, b, xp, adia, maxit=2000, tol=TOL, replace=True)
+    assert np.all(rep.status == 0) and np.all(rep.tole <= TOL)
+    assert np.all(dda.residual_f64(b, xp, adia) <= 1.2 * TOL)
+    for r in range(b.shape[0]):
+        assert np.linalg.norm(xp[r] - xr[r]) / np.linalg.norm(xr[r]) < 20 * TOL
+    assert rest.itno.sum() > 0 and rep.itno.sum() > 0
+    dda.release()
