@@ -137,23 +137,29 @@ def dist_init():
 
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900),
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
         pg = dist
     return world, rank, local, pg
 
 
 def barrier(pg, local):
-    if pg is not None:
+    if pg is None:
+        return
+    if pg.get_backend() == "nccl":
         pg.barrier(device_ids=[local])
+    else:
+        pg.barrier()
 
 
 def max_over_ranks(pg, value):
+    """Max of a per-rank scalar (the slowest rank's time) over the job."""
     if pg is None:
         return value
     import torch
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dev = "cuda" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
 
