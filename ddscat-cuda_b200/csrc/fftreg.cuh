@@ -57,6 +57,62 @@ template <int K, int DIR, typename C> __device__ __forceinline__ void dftr(C* v)
   }
 }
 
+// DFT of K points whose upper half v[K/2..K-1] is zero (not read): the
+// zero-padded half of a forward DDA transform.  Same output as dftr<K>.
+template <int K, int DIR, typename C> __device__ __forceinline__ void dftr_h(C* v) {
+  if constexpr (K == 2) {
+    v[1] = v[0];
+  } else if constexpr (K == 4) {
+    const C a = v[0], b = v[1], bi = cmuli(v[1], (float)DIR);
+    v[0] = cadd(a, b);
+    v[2] = csub(a, b);
+    v[1] = cadd(a, bi);
+    v[3] = csub(a, bi);
+  } else if constexpr (K == 8) {
+    C e[4] = {v[0], v[2], v[0], v[0]};
+    C o[4] = {v[1], v[3], v[1], v[1]};
+    dftr_h<4, DIR>(e);
+    dftr_h<4, DIR>(o);
+    using R = decltype(v[0].x);
+    const R h = (R)0.70710678118654752440;
+    C o1 = o[1], o3 = o[3];
+    C t1 = mk<C>((double)(h * (o1.x - (R)DIR * o1.y)), (double)(h * (o1.y + (R)DIR * o1.x)));
+    C t2 = cmuli(o[2], (float)DIR);
+    C t3 = mk<C>((double)(h * (-o3.x - (R)DIR * o3.y)), (double)(h * (-o3.y + (R)DIR * o3.x)));
+    v[0] = cadd(e[0], o[0]);
+    v[4] = csub(e[0], o[0]);
+    v[1] = cadd(e[1], t1);
+    v[5] = csub(e[1], t1);
+    v[2] = cadd(e[2], t2);
+    v[6] = csub(e[2], t2);
+    v[3] = cadd(e[3], t3);
+    v[7] = csub(e[3], t3);
+  } else {
+    // K = K1*K2, element K2*a + b is zero for a >= K1/2
+    constexpr int K1 = (K == 16) ? 4 : 8;
+    constexpr int K2 = K / K1;
+    C Y[K2][K1];
+#pragma unroll
+    for (int b = 0; b < K2; ++b) {
+      C t[K1];
+#pragma unroll
+      for (int a = 0; a < K1 / 2; ++a) t[a] = v[K2 * a + b];
+      dftr_h<K1, DIR>(t);
+#pragma unroll
+      for (int c = 0; c < K1; ++c) Y[b][c] = (b * c == 0) ? t[c] : cmul(t[c], wk<K, DIR, C>(b * c));
+    }
+#pragma unroll
+    for (int c = 0; c < K1; ++c) {
+      C t[K2];
+#pragma unroll
+      for (int b = 0; b < K2; ++b) t[b] = Y[b][c];
+      dftr<K2, DIR>(t);
+#pragma unroll
+      for (int d = 0; d < K2; ++d) v[c + K1 * d] = t[d];
+    }
+  }
+}
+
 // per-line scratch size (complex elements) for the transpose, before padding
 template <int E, int T> constexpr int line_scratch() { return T * (E + 1) + 1; }
 
@@ -89,11 +145,13 @@ inline int line_stride(int E, int T, int L, bool line_fastest) {
 // One length-E*T transform of the line held in v by thread t (0 <= t < T).
 // `sl` is this line's shared scratch; `tw` the N-entry table exp(-2*pi*i*m/N).
 // BLOCK_SYNC selects __syncthreads (line spread over warps) or __syncwarp.
-template <int E, int T, int DIR, bool BLOCK_SYNC, typename C>
+// HALF_IN: elements t + T*i with i >= E/2 (the upper half of the line) are
+// zero and are not read.
+template <int E, int T, int DIR, bool BLOCK_SYNC, bool HALF_IN = false, typename C>
 __device__ __forceinline__ void line_fft(C (&v)[E], C* sl, int t, const C* __restrict__ tw) {
   constexpr int M = E / T;
   static_assert(M * T == E && M >= 1, "E must be a multiple of T");
-  dftr<E, DIR>(v);
+  if constexpr (HALF_IN) dftr_h<E, DIR>(v); else dftr<E, DIR>(v);
 #pragma unroll
   for (int p = 1; p < E; ++p) v[p] = cmul(v[p], twid<DIR>(tw, t * p));
 #pragma unroll

@@ -47,6 +47,7 @@ template <typename T> struct XParams {
   const cplx<T>* twy;
   const cplx<T>* twz;
   int lsx, lsy, lsz;  // line strides of the x, y, z passes
+  int my_log2;        // log2(My)
   T inv_ngrid;
 };
 
@@ -58,80 +59,96 @@ template <typename T, int N> __device__ __forceinline__ void load_tw(cplx<T>* tw
   for (int u = threadIdx.x; u < N; u += blockDim.x) tws[u] = tw[u];
 }
 
+// Compile-time shape of a pass over axis length N = 2n (M = 2n always in this
+// pipeline): E elements per thread, TT threads per line, H = E/2 elements per
+// thread inside the n real points, RL lines per 256-thread row block.
+template <int N> struct XShape {
+  static constexpr int E = RegShape<N>::E, TT = RegShape<N>::T, H = E / 2;
+  static constexpr int RL = 256 / TT;
+  static constexpr int RZ = (128 / TT) > 1 ? 128 / TT : 1;  // ZG lines per block (3*TT*RZ threads)
+  static constexpr int ZG_MINB = E >= 32 ? 2 : 3;             // ZG blocks per SM the registers must allow
+};
+
 // ------------------------------------------------------------- XF: x forward
-// block: RL rows (iy) x T threads, thread-fastest; grid (ceil(ny/RL), nz, 3*nr)
+// block: RL rows (iy) x TT threads, thread-fastest; grid (ceil(ny/RL), nz, 3*nr)
 template <typename T, int N> __global__ void __launch_bounds__(256) kx_xf(XParams<T> P) {
   using C = cplx<T>;
-  constexpr int E = RegShape<N>::E, TT = RegShape<N>::T;
+  using S_ = XShape<N>;
+  constexpr int E = S_::E, TT = S_::TT, H = S_::H, RL = S_::RL;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int RL = blockDim.x / TT, t = threadIdx.x % TT, l = threadIdx.x / TT;
+  const int t = threadIdx.x % TT, l = threadIdx.x / TT;
   C* tws = reinterpret_cast<C*>(smem_raw);
-  C* tile = tws + N;                        // [kx][RL+1]
-  C* lines = tile + (size_t)N * (RL + 1);   // RL * lsx
+  C* tile = tws + N;   // [kx][RL+1], aliases the line scratch
+  C* lines = tws + N;  // RL * lsx
   const int iy0 = blockIdx.x * RL, iy = iy0 + l, iz = blockIdx.y;
-  const int rl = blockIdx.z / 3, c = blockIdx.z % 3;
+  const int rl = blockIdx.z / 3, c = blockIdx.z - 3 * (blockIdx.z / 3);
   if (xoff(P, rl)) return;
   load_tw<T, N>(tws, P.twx);
   __syncthreads();
-  const C* x = P.x + (size_t)rl * P.x_rs;
-  const size_t S = P.io_full ? (size_t)P.nat : (size_t)P.nat0;
+  const int S = P.io_full ? P.nat : P.nat0;
+  const C* x = P.x + (size_t)rl * P.x_rs + (size_t)c * S;
+  const int jrow = P.nx * (iy + P.ny * iz);
   C v[E];
 #pragma unroll
-  for (int i = 0; i < E; ++i) {
-    const int ix = t + TT * i;
+  for (int i = 0; i < H; ++i) {
+    const int ix = t + TT * i;  // < nx = N/2
     v[i] = mk<C>(0, 0);
-    if (ix < P.nx && iy < P.ny) {
-      const size_t j = (size_t)ix + (size_t)P.nx * ((size_t)iy + (size_t)P.ny * iz);
+    if (iy < P.ny) {
       if (P.io_full) {
-        v[i] = x[c * S + j];
+        v[i] = x[jrow + ix];
       } else {
-        const int q = P.inv[j];
-        if (q >= 0) v[i] = x[c * S + q];
+        const int q = P.inv[jrow + ix];
+        if (q >= 0) v[i] = x[q];
       }
       if (P.conj) v[i].y = -v[i].y;
     }
   }
-  line_fft<E, TT, +1, false>(v, lines + (size_t)l * P.lsx, t, tws);
+  line_fft<E, TT, +1, false, true>(v, lines + (size_t)l * P.lsx, t, tws);
+  __syncthreads();  // all line scratch consumed before the tile reuses it
 #pragma unroll
   for (int i = 0; i < E; ++i) tile[(t + TT * i) * (RL + 1) + l] = v[i];
   __syncthreads();
-  C* A = P.A + (size_t)rl * P.A_rs + (((size_t)c * P.nz + iz) * P.Mx) * P.ny;
-  for (int u = threadIdx.x; u < N * RL; u += blockDim.x) {
+  C* A = P.A + (size_t)rl * P.A_rs + ((size_t)(c * P.nz + iz) * P.Mx) * P.ny + iy0;
+  const int ny = P.ny;
+#pragma unroll 4
+  for (int u = threadIdx.x; u < N * RL; u += 256) {
     const int kx = u / RL, ll = u % RL;
-    if (iy0 + ll < P.ny) A[(size_t)kx * P.ny + iy0 + ll] = tile[kx * (RL + 1) + ll];
+    if (iy0 + ll < ny) A[kx * ny + ll] = tile[kx * (RL + 1) + ll];
   }
 }
 
 // ------------------------------------------------------------- YF: y forward
-// block: RL z-lines (iz) x T; grid (ceil(nz/RL), nkx, 3*nrb)
+// block: RL z-lines (iz) x TT; grid (ceil(nz/RL), nkx, 3*nrb)
 template <typename T, int N> __global__ void __launch_bounds__(256) kx_yf(XParams<T> P) {
   using C = cplx<T>;
-  constexpr int E = RegShape<N>::E, TT = RegShape<N>::T;
+  using S_ = XShape<N>;
+  constexpr int E = S_::E, TT = S_::TT, H = S_::H, RL = S_::RL;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int RL = blockDim.x / TT, t = threadIdx.x % TT, l = threadIdx.x / TT;
+  const int t = threadIdx.x % TT, l = threadIdx.x / TT;
   C* tws = reinterpret_cast<C*>(smem_raw);
   C* tile = tws + N;
-  C* lines = tile + (size_t)N * (RL + 1);
+  C* lines = tws + N;
   const int iz0 = blockIdx.x * RL, iz = iz0 + l, kxl = blockIdx.y, kx = P.kx0 + kxl;
-  const int rb = blockIdx.z / 3, c = blockIdx.z % 3, rl = P.b_rhs0 + rb;
+  const int rb = blockIdx.z / 3, c = blockIdx.z - 3 * (blockIdx.z / 3), rl = P.b_rhs0 + rb;
   if (xoff(P, rl)) return;
   load_tw<T, N>(tws, P.twy);
   __syncthreads();
-  const C* A = P.A + (size_t)rl * P.A_rs + (((size_t)c * P.nz + iz) * P.Mx + kx) * P.ny;
+  const C* A = P.A + (size_t)rl * P.A_rs + ((size_t)(c * P.nz + iz) * P.Mx + kx) * P.ny;
   C v[E];
+  const bool zin = iz < P.nz;
 #pragma unroll
-  for (int i = 0; i < E; ++i) {
-    const int iy = t + TT * i;
-    v[i] = (iy < P.ny && iz < P.nz) ? A[iy] : mk<C>(0, 0);
-  }
-  line_fft<E, TT, +1, false>(v, lines + (size_t)l * P.lsy, t, tws);
+  for (int i = 0; i < H; ++i) v[i] = zin ? A[t + TT * i] : mk<C>(0, 0);  // iy < ny = N/2
+  line_fft<E, TT, +1, false, true>(v, lines + (size_t)l * P.lsy, t, tws);
+  __syncthreads();
 #pragma unroll
   for (int i = 0; i < E; ++i) tile[(t + TT * i) * (RL + 1) + l] = v[i];
   __syncthreads();
-  C* B = P.B + (((size_t)rb * 3 + c) * P.nkx + kxl) * (size_t)P.My * P.nz;
-  for (int u = threadIdx.x; u < N * RL; u += blockDim.x) {
+  const int nz = P.nz;
+  C* B = P.B + ((size_t)(rb * 3 + c) * P.nkx + kxl) * (size_t)P.My * nz + iz0;
+#pragma unroll 4
+  for (int u = threadIdx.x; u < N * RL; u += 256) {
     const int ky = u / RL, ll = u % RL;
-    if (iz0 + ll < P.nz) B[(size_t)ky * P.nz + iz0 + ll] = tile[ky * (RL + 1) + ll];
+    if (iz0 + ll < nz) B[ky * nz + ll] = tile[ky * (RL + 1) + ll];
   }
 }
 
@@ -177,14 +194,16 @@ __device__ __forceinline__ void green_apply(const C a[6], R sxy, R sxz, R syz, C
 }
 
 // ------------------------------------------------------------- ZG: z * Green * z^-1
-// block: RL lines x T threads x 3 components, thread-fastest within a line;
-// lines are (kx, ky) pairs p = kxl*My + ky.  grid (nrb, ceil(nkx*My/RL))
-template <typename T, int N> __global__ void __launch_bounds__(384) kx_zg(XParams<T> P) {
+// block: RZ lines x TT threads x 3 components, thread-fastest within a line;
+// lines are (kx, ky) pairs p = kxl*My + ky.  grid (nrb, ceil(nkx*My/RZ))
+template <typename T, int N>
+__global__ void __launch_bounds__(3 * XShape<N>::TT * XShape<N>::RZ, XShape<N>::ZG_MINB) kx_zg(XParams<T> P) {
   using C = cplx<T>;
   using R = T;
-  constexpr int E = RegShape<N>::E, TT = RegShape<N>::T;
+  using S_ = XShape<N>;
+  constexpr int E = S_::E, TT = S_::TT, H = S_::H, RL = S_::RZ;
+  constexpr int GT = 3 * TT;  // Green-phase threads per line
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int RL = blockDim.x / (3 * TT);
   const int t = threadIdx.x % TT, l = (threadIdx.x / TT) % RL, c = threadIdx.x / (TT * RL);
   C* tws = reinterpret_cast<C*>(smem_raw);
   C* lines = tws + N;  // [3][RL][lsz]
@@ -196,39 +215,40 @@ template <typename T, int N> __global__ void __launch_bounds__(384) kx_zg(XParam
   const int nlines = P.nkx * P.My;
   const int p = blockIdx.y * RL + l;
   const bool live = p < nlines;
-  C* row = P.B + (((size_t)rb * 3 + c) * P.nkx) * (size_t)P.My * P.nz + (size_t)p * P.nz;
+  C* row = P.B + ((size_t)(rb * 3 + c) * P.nkx) * (size_t)P.My * P.nz + (size_t)p * P.nz;
   C v[E];
 #pragma unroll
-  for (int i = 0; i < E; ++i) {
-    const int iz = t + TT * i;
-    v[i] = (live && iz < P.nz) ? row[iz] : mk<C>(0, 0);
-  }
-  line_fft<E, TT, +1, false>(v, my, t, tws);
+  for (int i = 0; i < H; ++i) v[i] = live ? row[t + TT * i] : mk<C>(0, 0);  // iz < nz = N/2
+  line_fft<E, TT, +1, false, true>(v, my, t, tws);
 #pragma unroll
   for (int i = 0; i < E; ++i) my[t + TT * i] = v[i];
   __syncthreads();
-  // Green: one thread per (line, kz <= Mz/2); the record serves kz and Mz-kz
-  const int half = N / 2 + 1;
-  for (int u = threadIdx.x; u < RL * half; u += blockDim.x) {
-    const int ll = u / half, kz = u % half, pl = blockIdx.y * RL + ll;
-    if (pl >= nlines) continue;
-    const int kx = P.kx0 + pl / P.My, ky = pl % P.My;
-    R sxy, sxz, syz;
-    C a[6];
-    load_rec<T>(green_rec(P, kx, ky, kz, sxy, sxz, syz), a);
-    C* L0 = lines + (size_t)ll * P.lsz;
-    C* L1 = L0 + (size_t)RL * P.lsz;
-    C* L2 = L1 + (size_t)RL * P.lsz;
-    if (P.ipbc == 0) {
-      green_apply(a, sxy, sxz, syz, L0[kz], L1[kz], L2[kz]);  // kz <= nz: sz = +1
-      const int km = N - kz;
-      if (kz > 0 && km != kz) green_apply(a, sxy, -sxz, -syz, L0[km], L1[km], L2[km]);  // sz = -1
-    } else {
-      green_apply(a, sxy, sxz, syz, L0[kz], L1[kz], L2[kz]);
-      const int km = N - kz;
-      if (kz > 0 && km != kz) {
-        load_rec<T>(green_rec(P, kx, ky, km, sxy, sxz, syz), a);
-        green_apply(a, sxy, sxz, syz, L0[km], L1[km], L2[km]);
+  // Green: GT threads per line, kz = 0..N/2; the record serves kz and N - kz
+  {
+    const int gl = threadIdx.x / GT, gk = threadIdx.x - GT * (threadIdx.x / GT);
+    const int pl = blockIdx.y * RL + gl;
+    if (pl < nlines) {
+      const int kx = P.kx0 + (pl >> P.my_log2), ky = pl & (P.My - 1);
+      C* L0 = lines + (size_t)gl * P.lsz;
+      C* L1 = L0 + (size_t)RL * P.lsz;
+      C* L2 = L1 + (size_t)RL * P.lsz;
+      if (P.ipbc == 0) {
+        R sxy, sxz, syz;
+        const C* rec0 = green_rec(P, kx, ky, 0, sxy, sxz, syz);
+        for (int kz = gk; kz <= N / 2; kz += GT) {
+          C a[6];
+          load_rec<T>(rec0 + 6 * kz, a);
+          green_apply(a, sxy, sxz, syz, L0[kz], L1[kz], L2[kz]);  // kz <= nz: sz = +1
+          const int km = N - kz;
+          if (kz > 0 && km != kz) green_apply(a, sxy, -sxz, -syz, L0[km], L1[km], L2[km]);  // sz = -1
+        }
+      } else {
+        for (int kz = gk; kz < N; kz += GT) {
+          R sxy, sxz, syz;
+          C a[6];
+          load_rec<T>(green_rec(P, kx, ky, kz, sxy, sxz, syz), a);
+          green_apply(a, sxy, sxz, syz, L0[kz], L1[kz], L2[kz]);
+        }
       }
     }
   }
@@ -239,112 +259,107 @@ template <typename T, int N> __global__ void __launch_bounds__(384) kx_zg(XParam
   line_fft<E, TT, -1, false>(v, my, t, tws);
   if (live) {
 #pragma unroll
-    for (int i = 0; i < E; ++i) {
-      const int iz = t + TT * i;
-      if (iz < P.nz) row[iz] = v[i];
-    }
+    for (int i = 0; i < H; ++i) row[t + TT * i] = v[i];  // keep iz < nz
   }
 }
 
 // ------------------------------------------------------------- YI: y inverse
-// block: RL z-lines x T; grid (ceil(nz/RL), nkx, 3*nrb)
+// block: RL z-lines x TT; grid (ceil(nz/RL), nkx, 3*nrb)
 template <typename T, int N> __global__ void __launch_bounds__(256) kx_yi(XParams<T> P) {
   using C = cplx<T>;
-  constexpr int E = RegShape<N>::E, TT = RegShape<N>::T;
+  using S_ = XShape<N>;
+  constexpr int E = S_::E, TT = S_::TT, H = S_::H, RL = S_::RL;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int RL = blockDim.x / TT, t = threadIdx.x % TT, l = threadIdx.x / TT;
+  const int t = threadIdx.x % TT, l = threadIdx.x / TT;
   C* tws = reinterpret_cast<C*>(smem_raw);
   C* tile = tws + N;
-  C* lines = tile + (size_t)N * (RL + 1);
+  C* lines = tws + N;
   const int iz0 = blockIdx.x * RL, iz = iz0 + l, kxl = blockIdx.y, kx = P.kx0 + kxl;
-  const int rb = blockIdx.z / 3, c = blockIdx.z % 3, rl = P.b_rhs0 + rb;
+  const int rb = blockIdx.z / 3, c = blockIdx.z - 3 * (blockIdx.z / 3), rl = P.b_rhs0 + rb;
   if (xoff(P, rl)) return;
   load_tw<T, N>(tws, P.twy);
-  const C* B = P.B + (((size_t)rb * 3 + c) * P.nkx + kxl) * (size_t)P.My * P.nz;
-  for (int u = threadIdx.x; u < N * RL; u += blockDim.x) {
+  const int nz = P.nz;
+  const C* B = P.B + ((size_t)(rb * 3 + c) * P.nkx + kxl) * (size_t)P.My * nz + iz0;
+#pragma unroll 4
+  for (int u = threadIdx.x; u < N * RL; u += 256) {
     const int ky = u / RL, ll = u % RL;
-    tile[ky * (RL + 1) + ll] = (iz0 + ll < P.nz) ? B[(size_t)ky * P.nz + iz0 + ll] : mk<C>(0, 0);
+    tile[ky * (RL + 1) + ll] = (iz0 + ll < nz) ? B[ky * nz + ll] : mk<C>(0, 0);
   }
   __syncthreads();
   C v[E];
 #pragma unroll
   for (int i = 0; i < E; ++i) v[i] = tile[(t + TT * i) * (RL + 1) + l];
+  __syncthreads();  // the tile is consumed before the line scratch reuses it
   line_fft<E, TT, -1, false>(v, lines + (size_t)l * P.lsy, t, tws);
-  if (iz < P.nz) {
-    C* A = P.A + (size_t)rl * P.A_rs + (((size_t)c * P.nz + iz) * P.Mx + kx) * P.ny;
+  if (iz < nz) {
+    C* A = P.A + (size_t)rl * P.A_rs + ((size_t)(c * nz + iz) * P.Mx + kx) * P.ny;
 #pragma unroll
-    for (int i = 0; i < E; ++i) {
-      const int iy = t + TT * i;
-      if (iy < P.ny) A[iy] = v[i];
-    }
+    for (int i = 0; i < H; ++i) A[t + TT * i] = v[i];  // keep iy < ny
   }
 }
 
 // ------------------------------------------------------------- XI: x inverse + finish
-template <typename T>
-__device__ __forceinline__ void xfinish(const XParams<T>& P, int rl, int c, int ix, int iy, int iz, cplx<T> wraw) {
-  using C = cplx<T>;
-  const C* x = P.x + (size_t)rl * P.x_rs;
-  C* y = P.y + (size_t)rl * P.y_rs;
-  const C* ad = P.adia + (size_t)rl * P.a_rs;
-  const C* ao = P.aoff ? P.aoff + (size_t)rl * P.a_rs : nullptr;
-  const size_t S = P.io_full ? (size_t)P.nat : (size_t)P.nat0;
-  const size_t SA = P.a_full ? (size_t)P.nat : (size_t)P.nat0;
-  const size_t j = (size_t)ix + (size_t)P.nx * ((size_t)iy + (size_t)P.ny * iz);
-  size_t q;
-  if (P.io_full) {
-    q = j;
-    if (P.iocc[j] == 0) { y[c * S + q] = mk<C>(0, 0); return; }
-  } else {
-    const int qq = P.inv[j];
-    if (qq < 0) return;
-    q = (size_t)qq;
-  }
-  const size_t qa = P.a_full ? j : q;
-  C xc = x[c * S + q];
-  if (P.conj) xc.y = -xc.y;
-  C yv = csub(cmul(ad[c * SA + qa], xc), cscale(wraw, P.inv_ngrid));
-  if (ao) {
-    C x1 = x[q], x2 = x[S + q], x3 = x[2 * S + q];
-    if (P.conj) { x1.y = -x1.y; x2.y = -x2.y; x3.y = -x3.y; }
-    const C a23 = ao[qa], a31 = ao[SA + qa], a12 = ao[2 * SA + qa];
-    if (c == 0) yv = cadd(yv, cadd(cmul(a31, x3), cmul(a12, x2)));
-    else if (c == 1) yv = cadd(yv, cadd(cmul(a12, x1), cmul(a23, x3)));
-    else yv = cadd(yv, cadd(cmul(a23, x2), cmul(a31, x1)));
-  }
-  if (P.conj) yv.y = -yv.y;
-  y[c * S + q] = yv;
-}
-
-// block: RL rows (iy) x T; grid (ceil(ny/RL), nz, 3*nr)
+// block: RL rows (iy) x TT; grid (ceil(ny/RL), nz, 3*nr)
 template <typename T, int N> __global__ void __launch_bounds__(256) kx_xi(XParams<T> P) {
   using C = cplx<T>;
-  constexpr int E = RegShape<N>::E, TT = RegShape<N>::T;
+  using S_ = XShape<N>;
+  constexpr int E = S_::E, TT = S_::TT, H = S_::H, RL = S_::RL;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int RL = blockDim.x / TT, t = threadIdx.x % TT, l = threadIdx.x / TT;
+  const int t = threadIdx.x % TT, l = threadIdx.x / TT;
   C* tws = reinterpret_cast<C*>(smem_raw);
   C* tile = tws + N;
-  C* lines = tile + (size_t)N * (RL + 1);
+  C* lines = tws + N;
   const int iy0 = blockIdx.x * RL, iy = iy0 + l, iz = blockIdx.y;
-  const int rl = blockIdx.z / 3, c = blockIdx.z % 3;
+  const int rl = blockIdx.z / 3, c = blockIdx.z - 3 * (blockIdx.z / 3);
   if (xoff(P, rl)) return;
   load_tw<T, N>(tws, P.twx);
-  const C* A = P.A + (size_t)rl * P.A_rs + (((size_t)c * P.nz + iz) * P.Mx) * P.ny;
-  for (int u = threadIdx.x; u < N * RL; u += blockDim.x) {
+  const int ny = P.ny;
+  const C* A = P.A + (size_t)rl * P.A_rs + ((size_t)(c * P.nz + iz) * P.Mx) * ny + iy0;
+#pragma unroll 4
+  for (int u = threadIdx.x; u < N * RL; u += 256) {
     const int kx = u / RL, ll = u % RL;
-    tile[kx * (RL + 1) + ll] = (iy0 + ll < P.ny) ? A[(size_t)kx * P.ny + iy0 + ll] : mk<C>(0, 0);
+    tile[kx * (RL + 1) + ll] = (iy0 + ll < ny) ? A[kx * ny + ll] : mk<C>(0, 0);
   }
   __syncthreads();
   C v[E];
 #pragma unroll
   for (int i = 0; i < E; ++i) v[i] = tile[(t + TT * i) * (RL + 1) + l];
+  __syncthreads();
   line_fft<E, TT, -1, false>(v, lines + (size_t)l * P.lsx, t, tws);
-  if (iy < P.ny) {
+  if (iy >= ny) return;
+  // finish (cu:116-118): y = CXADIA x - w/ngrid [+ CXAOFF terms], conj for 'C'
+  const int S = P.io_full ? P.nat : P.nat0;
+  const int SA = P.a_full ? P.nat : P.nat0;
+  const C* x = P.x + (size_t)rl * P.x_rs;
+  C* y = P.y + (size_t)rl * P.y_rs + (size_t)c * S;
+  const C* ad = P.adia + (size_t)rl * P.a_rs + (size_t)c * SA;
+  const C* ao = P.aoff ? P.aoff + (size_t)rl * P.a_rs : nullptr;
+  const int jrow = P.nx * (iy + ny * iz);
 #pragma unroll
-    for (int i = 0; i < E; ++i) {
-      const int ix = t + TT * i;
-      if (ix < P.nx) xfinish(P, rl, c, ix, iy, iz, v[i]);
+  for (int i = 0; i < H; ++i) {
+    const int j = jrow + t + TT * i;  // ix < nx
+    int q;
+    if (P.io_full) {
+      q = j;
+      if (P.iocc[j] == 0) { y[q] = mk<C>(0, 0); continue; }
+    } else {
+      q = P.inv[j];
+      if (q < 0) continue;
     }
+    const int qa = P.a_full ? j : q;
+    C xc = x[(size_t)c * S + q];
+    if (P.conj) xc.y = -xc.y;
+    C yv = csub(cmul(ad[qa], xc), cscale(v[i], P.inv_ngrid));
+    if (ao) {
+      C x1 = x[q], x2 = x[S + q], x3 = x[2 * (size_t)S + q];
+      if (P.conj) { x1.y = -x1.y; x2.y = -x2.y; x3.y = -x3.y; }
+      const C a23 = ao[qa], a31 = ao[SA + qa], a12 = ao[2 * (size_t)SA + qa];
+      if (c == 0) yv = cadd(yv, cadd(cmul(a31, x3), cmul(a12, x2)));
+      else if (c == 1) yv = cadd(yv, cadd(cmul(a12, x1), cmul(a23, x3)));
+      else yv = cadd(yv, cadd(cmul(a23, x2), cmul(a31, x1)));
+    }
+    if (P.conj) yv.y = -yv.y;
+    y[q] = yv;
   }
 }
 
@@ -416,8 +431,11 @@ int matvec_xpipe(Engine<T>& E, const MvArgs<T>& a) {
   P.lsx = line_stride(g.Mx / TX, TX, RX, false);
   P.lsy = line_stride(g.My / TY, TY, RY, false);
   P.lsz = std::max(line_stride(g.Mz / TZ, TZ, RZ, false), g.Mz);
-  const size_t smx = ((size_t)g.Mx + (size_t)g.Mx * (RX + 1) + (size_t)RX * P.lsx) * sizeof(C);
-  const size_t smy = ((size_t)g.My + (size_t)g.My * (RY + 1) + (size_t)RY * P.lsy) * sizeof(C);
+  // the transpose tile and the line scratch share one region
+  const size_t smx = ((size_t)g.Mx + std::max((size_t)g.Mx * (RX + 1), (size_t)RX * P.lsx)) * sizeof(C);
+  const size_t smy = ((size_t)g.My + std::max((size_t)g.My * (RY + 1), (size_t)RY * P.lsy)) * sizeof(C);
+  P.my_log2 = 0;
+  while ((1 << P.my_log2) < g.My) ++P.my_log2;
   const size_t smz = ((size_t)g.Mz + (size_t)3 * RZ * P.lsz) * sizeof(C);
   const void* fxf = xkernel<T>(XPass::XF, g.Mx);
   const void* fyf = xkernel<T>(XPass::YF, g.My);
