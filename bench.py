@@ -53,6 +53,9 @@ def parse_args():
     ap.add_argument("--maxit", type=int, default=4000)
     ap.add_argument("--policy", default="replace", choices=["replace", "restart"],
                     help="reliable-residual policy of the batched solve: residual replacement or restart")
+    ap.add_argument("--qmr-form", default="symmetric", choices=["symmetric", "two-product"],
+                    help="QMRCCG: one MATVEC per iteration (left Lanczos vectors = right ones, A^T = A) or the "
+                         "reference's two-product form")
     ap.add_argument("--ref-rhs", type=int, default=0, help="RHS per step of the reference arm (0: the whole batch)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -182,7 +185,8 @@ def config(args, prob, R, world):
             "tol": args.tol, "fp64_check": "GPU all-FP64 MATVEC true residual, every RHS, every step",
             "l2": "inputs larger than L2 (each RHS vector 3*NAT*8 B > 50 MB; working set > 1 GB)",
             "parallelism": f"replicas x{world} (independent RHS batches per GPU)",
-            "reliable_residual_policy": getattr(args, "policy", "restart")}
+            "reliable_residual_policy": getattr(args, "policy", "restart"),
+            "qmr_form": getattr(args, "qmr_form", "two-product") if args.solver == "qmrccg" else None}
 
 
 def algorithmic_bytes_per_matvec(prob, rhs_per_call):
@@ -263,7 +267,9 @@ def run_ours(args):
     def solve_to_fp64(bx, xx, ax, on_device):
         """One step: batched solve, FP64 true residuals, re-solve failures."""
         rep = args.policy == "replace"
-        out = dda.solve_batch(args.solver, bx, xx, ax, None, maxit=args.maxit, tol=args.tol, replace=rep)
+        sym = args.solver == "qmrccg" and args.qmr_form == "symmetric"
+        out = dda.solve_batch(args.solver, bx, xx, ax, None, maxit=args.maxit, tol=args.tol, replace=rep,
+                              symmetric=sym)
         ms, rhs, calls = dda.last_solve_stats()
         stats["mv_ms"] += ms
         stats["mv_rhs"] += rhs
@@ -276,7 +282,8 @@ def run_ours(args):
             tol *= 0.5
             sub = (lambda a: a[bad].contiguous()) if on_device else (lambda a: np.ascontiguousarray(a[bad]))
             xs = sub(xx)
-            o2 = dda.solve_batch(args.solver, sub(bx), xs, sub(ax), None, maxit=args.maxit, tol=tol, replace=rep)
+            o2 = dda.solve_batch(args.solver, sub(bx), xs, sub(ax), None, maxit=args.maxit, tol=tol, replace=rep,
+                                 symmetric=sym)
             xx[bad] = xs
             out.itno[bad] += o2.itno
             out.ncompte[bad] += o2.ncompte
@@ -436,6 +443,7 @@ def run_reference(args):
     cfg = config(args, prob, b.shape[0], world)
     cfg["reference_rhs_per_step"] = nref
     cfg["reliable_residual_policy"] = "restart (the reference's own)"
+    cfg["qmr_form"] = "two-product (the reference's own)" if args.solver == "qmrccg" else None
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed * 1000.0 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c64 (FP32 complex bulk, FP64 dots)",

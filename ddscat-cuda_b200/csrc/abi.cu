@@ -577,7 +577,12 @@ DDSCAT_CUDA_API int ddscat_b200_solve_batch_f32(int solver, int nrhs, const void
     return 500;
   }
   const int replace = (solver & DDSCAT_B200_REPLACE_RESIDUAL) != 0;
-  solver &= ~DDSCAT_B200_REPLACE_RESIDUAL;
+  const int sym = (solver & DDSCAT_B200_QMR_SYMMETRIC) != 0;
+  solver &= ~(DDSCAT_B200_REPLACE_RESIDUAL | DDSCAT_B200_QMR_SYMMETRIC);
+  if (sym && solver != DDSCAT_B200_QMRCCG) {
+    set_error("batched solve", "DDSCAT_B200_QMR_SYMMETRIC applies to QMRCCG only");
+    return 501;
+  }
   if (solver != DDSCAT_B200_QMRCCG && solver != DDSCAT_B200_PBCGS2) {
     set_error("batched solve", "unsupported solver (QMRCCG=1, PBCGS2=2)");
     return 501;
@@ -599,7 +604,7 @@ DDSCAT_CUDA_API int ddscat_b200_solve_batch_f32(int solver, int nrhs, const void
   io.eng = &s.eng; io.ops = &bs.ops; io.R = nrhs; io.n = bs.n;
   io.b = bs.b; io.x = bs.x; io.adia = bs.adia; io.aoff = use_aoff ? bs.aoff : nullptr;
   io.work = bs.work; io.nwork = BATCH_WORK_VECTORS;
-  io.maxit = maxit; io.tol = (double)tol; io.verbose = s.verbose; io.replace = replace;
+  io.maxit = maxit; io.tol = (double)tol; io.verbose = s.verbose; io.replace = replace; io.sym = sym;
   BatchResult res;
   const int rc = solver == DDSCAT_B200_QMRCCG ? solve_batch_qmrccg<float>(io, res) : solve_batch_pbcgs2<float>(io, res);
   bs.matvec_ms = io.matvec_ms;

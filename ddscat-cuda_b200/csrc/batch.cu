@@ -305,6 +305,11 @@ template <typename T> int solve_batch_qmrccg(BatchIO<T>& io, BatchResult& res) {
   std::vector<int> live(R, 1);  // not failed, not converged
   std::vector<double> bnorm(R), resid(R);
   std::vector<Z> lambda(R), kappa(R), theta(R), gamma(R), ksi(R), rho(R), eps(R), mu(R), tau(R);
+  // sym: the left Lanczos vectors equal the right ones (wt0 = vt0 = r0 and
+  // A^T = A, so wt_k = vt_k and q_k = A p_k for every k): wt is not stored,
+  // q is kept by its recurrence as A p, and one MATVEC (A vt) per iteration
+  // remains.  Same iterates as the two-product form in exact arithmetic.
+  const bool sym = io.sym != 0;
   std::vector<double2> o;
   const C* A1[3];
   const C* B1[3];
@@ -322,9 +327,32 @@ template <typename T> int solve_batch_qmrccg(BatchIO<T>& io, BatchResult& res) {
   ops.lin(r, nullptr, io.b, one.data(), sy, mone.data(), M);
   for (C* v : {p, ap, q, d, s, atw}) ops.zero(v, M);
   ops.copy(vt, r, M);
-  ops.copy(wt, r, M);
+  if (!sym) ops.copy(wt, r, M);
   auto init_scalars = [&](const std::vector<int>& set) -> int {
     const int* Ms = ops.mask(set);
+    if (sym) {
+      const C* A2[2] = {vt, vt};
+      const C* B2[2] = {vt, vt};
+      const int c2[2] = {1, 0};
+      std::vector<double2> o2, o1;
+      if (ops.dots(2, A2, B2, c2, Ms, o2)) return 1;
+      int rc2 = c.mv(vt, atw, set);
+      if (rc2) return rc2;
+      const C* A1b[1] = {vt};
+      const C* B1b[1] = {atw};
+      const int c1[1] = {0};
+      if (ops.dots(1, A1b, B1b, c1, Ms, o1)) return 1;
+      for (int i = 0; i < R; ++i) {
+        if (!set[i]) continue;
+        const double gn = std::sqrt(std::max(0.0, o2[2 * i].x));
+        rho[i] = zd2(o2[2 * i + 1]);
+        eps[i] = zd2(o1[i]);
+        lambda[i] = 1.0; kappa[i] = -1.0; theta[i] = -1.0; gamma[i] = gn; ksi[i] = gn; mu[i] = 0.0;
+        if (rho[i] == Z(0.0) || gamma[i] == Z(0.0)) { res.status[i] = 55; live[i] = 0; continue; }
+        tau[i] = eps[i] / rho[i];
+      }
+      return 0;
+    }
     const C* A3[3] = {vt, wt, vt};
     const C* B3[3] = {vt, wt, wt};
     const int c3[3] = {1, 1, 0};
@@ -370,22 +398,33 @@ template <typename T> int solve_batch_qmrccg(BatchIO<T>& io, BatchResult& res) {
     }
     ops.lin(p, cmu.data(), vt, cgam.data(), nullptr, nullptr, MI);
     ops.lin(q, cq.data(), atw, cksi.data(), nullptr, nullptr, MI);
-    if ((rc = c.mv(p, ap, I))) return rc;
+    if (!sym && (rc = c.mv(p, ap, I))) return rc;
+    const C* Ap = sym ? q : ap;  // A p
     for (int i = 0; i < R; ++i) {
       if (!I[i]) continue;
       ctg[i] = dz(-(tau[i] / gamma[i]));
       ctk[i] = dz(-(tau[i] / ksi[i]));
     }
-    ops.lin(vt, ctg.data(), ap, one.data(), nullptr, nullptr, MI);
-    ops.lin(wt, ctk.data(), q, one.data(), nullptr, nullptr, MI);
+    ops.lin(vt, ctg.data(), Ap, one.data(), nullptr, nullptr, MI);
+    if (!sym) ops.lin(wt, ctk.data(), q, one.data(), nullptr, nullptr, MI);
+    const C* W = sym ? vt : wt;  // left Lanczos vector
     std::vector<double2> o3, o1;
     {
-      const C* A3[3] = {vt, wt, vt};
-      const C* B3[3] = {vt, wt, wt};
+      const C* A3[3] = {vt, W, vt};
+      const C* B3[3] = {vt, W, W};
       const int c3[3] = {1, 1, 0};
-      if (ops.dots(3, A3, B3, c3, MI, o3)) return 1;
+      if (sym) {
+        const C* A2[2] = {vt, vt};
+        const int c2[2] = {1, 0};
+        std::vector<double2> o2;
+        if (ops.dots(2, A2, A2, c2, MI, o2)) return 1;
+        o3.resize((size_t)3 * R);
+        for (int i = 0; i < R; ++i) { o3[3 * i] = o3[3 * i + 1] = o2[2 * i]; o3[3 * i + 2] = o2[2 * i + 1]; }
+      } else if (ops.dots(3, A3, B3, c3, MI, o3)) {
+        return 1;
+      }
     }
-    if ((rc = c.mv(wt, atw, I))) return rc;
+    if ((rc = c.mv(W, atw, I))) return rc;
     {
       const C* A1b[1] = {vt};
       const C* B1b[1] = {atw};
@@ -422,7 +461,7 @@ template <typename T> int solve_batch_qmrccg(BatchIO<T>& io, BatchResult& res) {
     }
     MI = ops.mask(I);
     ops.lin(d, cth.data(), p, cka.data(), nullptr, nullptr, MI);
-    ops.lin(s, cth.data(), ap, cka.data(), nullptr, nullptr, MI);
+    ops.lin(s, cth.data(), Ap, cka.data(), nullptr, nullptr, MI);
     ops.lin(xs, one.data(), d, one.data(), nullptr, nullptr, MI);
     ops.lin(r, one.data(), s, mone.data(), nullptr, nullptr, MI);
     {
@@ -461,7 +500,7 @@ template <typename T> int solve_batch_qmrccg(BatchIO<T>& io, BatchResult& res) {
         ops.copy(r, sy, MR);
         for (C* v : {p, ap, q, d, s, atw}) ops.zero(v, MR);
         ops.copy(vt, sy, MR);
-        ops.copy(wt, sy, MR);
+        if (!sym) ops.copy(wt, sy, MR);
         if ((rc = init_scalars(RS))) return rc;
       }
     }

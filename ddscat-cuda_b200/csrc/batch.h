@@ -72,6 +72,10 @@ template <typename T> struct BatchIO {
   // single-RHS entry points); 1 replaces the recursive residual by the true
   // one and keeps the Krylov state (residual replacement).
   int replace = 0;
+  // QMRCCG only: 1 = one MATVEC per iteration (left Lanczos vectors equal the
+  // right ones since A^T = A and both start from r0), 0 = the reference's
+  // two-product form.
+  int sym = 0;
   double matvec_ms = 0.0;         // CUDA-event time of the MATVECs inside the solve
   long long matvec_rhs = 0;       // RHS-MATVECs performed
   int matvec_calls = 0;

@@ -69,6 +69,47 @@ template <int N> struct XShape {
   static constexpr int ZG_MINB = E >= 32 ? 2 : 3;             // ZG blocks per SM the registers must allow
 };
 
+// Tile <-> global moves of the row passes: N rows of RL consecutive elements
+// (row stride ld in global, RL+1 in the tile), two elements per 16-byte access.
+// Rows hold `valid` elements (RL or fewer at the grid edge; always even,
+// since every axis length n = N/2 >= 8 and RL are even).  The global base and
+// ld are even in elements, so every pair is 16-byte aligned.
+template <int RL, int N, typename C>
+__device__ __forceinline__ void store_pairs(C* g, int ld, int valid, const C* tile) {
+  constexpr int RP = RL / 2;
+#pragma unroll 4
+  for (int u = threadIdx.x; u < N * RP; u += 256) {
+    const int r = u / RP, ll = 2 * (u % RP);
+    if (ll < valid) {
+      const C a = tile[r * (RL + 1) + ll], b = tile[r * (RL + 1) + ll + 1];
+      if constexpr (sizeof(C) == 8) {
+        *reinterpret_cast<float4*>(g + (size_t)r * ld + ll) = make_float4(a.x, a.y, b.x, b.y);
+      } else {
+        g[(size_t)r * ld + ll] = a;
+        g[(size_t)r * ld + ll + 1] = b;
+      }
+    }
+  }
+}
+template <int RL, int N, typename C>
+__device__ __forceinline__ void load_pairs(const C* g, int ld, int valid, C* tile) {
+  constexpr int RP = RL / 2;
+#pragma unroll 4
+  for (int u = threadIdx.x; u < N * RP; u += 256) {
+    const int r = u / RP, ll = 2 * (u % RP);
+    if constexpr (sizeof(C) == 8) {
+      float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (ll < valid) q = __ldg(reinterpret_cast<const float4*>(g + (size_t)r * ld + ll));
+      tile[r * (RL + 1) + ll] = mk<C>(q.x, q.y);
+      tile[r * (RL + 1) + ll + 1] = mk<C>(q.z, q.w);
+    } else {
+      const bool ok = ll < valid;
+      tile[r * (RL + 1) + ll] = ok ? g[(size_t)r * ld + ll] : mk<C>(0, 0);
+      tile[r * (RL + 1) + ll + 1] = ok ? g[(size_t)r * ld + ll + 1] : mk<C>(0, 0);
+    }
+  }
+}
+
 // ------------------------------------------------------------- XF: x forward
 // block: RL rows (iy) x TT threads, thread-fastest; grid (ceil(ny/RL), nz, 3*nr)
 template <typename T, int N> __global__ void __launch_bounds__(256) kx_xf(XParams<T> P) {
@@ -109,12 +150,7 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_xf(XParam
   for (int i = 0; i < E; ++i) tile[(t + TT * i) * (RL + 1) + l] = v[i];
   __syncthreads();
   C* A = P.A + (size_t)rl * P.A_rs + ((size_t)(c * P.nz + iz) * P.Mx) * P.ny + iy0;
-  const int ny = P.ny;
-#pragma unroll 4
-  for (int u = threadIdx.x; u < N * RL; u += 256) {
-    const int kx = u / RL, ll = u % RL;
-    if (iy0 + ll < ny) A[kx * ny + ll] = tile[kx * (RL + 1) + ll];
-  }
+  store_pairs<RL, N>(A, P.ny, P.ny - iy0, tile);
 }
 
 // ------------------------------------------------------------- YF: y forward
@@ -143,13 +179,8 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_yf(XParam
 #pragma unroll
   for (int i = 0; i < E; ++i) tile[(t + TT * i) * (RL + 1) + l] = v[i];
   __syncthreads();
-  const int nz = P.nz;
-  C* B = P.B + ((size_t)(rb * 3 + c) * P.nkx + kxl) * (size_t)P.My * nz + iz0;
-#pragma unroll 4
-  for (int u = threadIdx.x; u < N * RL; u += 256) {
-    const int ky = u / RL, ll = u % RL;
-    if (iz0 + ll < nz) B[ky * nz + ll] = tile[ky * (RL + 1) + ll];
-  }
+  C* B = P.B + ((size_t)(rb * 3 + c) * P.nkx + kxl) * (size_t)P.My * P.nz + iz0;
+  store_pairs<RL, N>(B, P.nz, P.nz - iz0, tile);
 }
 
 // Green record at (kx, ky, kz) for the z-fastest layout, without the kz sign.
@@ -280,11 +311,7 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_yi(XParam
   load_tw<T, N>(tws, P.twy);
   const int nz = P.nz;
   const C* B = P.B + ((size_t)(rb * 3 + c) * P.nkx + kxl) * (size_t)P.My * nz + iz0;
-#pragma unroll 4
-  for (int u = threadIdx.x; u < N * RL; u += 256) {
-    const int ky = u / RL, ll = u % RL;
-    tile[ky * (RL + 1) + ll] = (iz0 + ll < nz) ? B[ky * nz + ll] : mk<C>(0, 0);
-  }
+  load_pairs<RL, N>(B, nz, nz - iz0, tile);
   __syncthreads();
   C v[E];
 #pragma unroll
@@ -315,11 +342,7 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_xi(XParam
   load_tw<T, N>(tws, P.twx);
   const int ny = P.ny;
   const C* A = P.A + (size_t)rl * P.A_rs + ((size_t)(c * P.nz + iz) * P.Mx) * ny + iy0;
-#pragma unroll 4
-  for (int u = threadIdx.x; u < N * RL; u += 256) {
-    const int kx = u / RL, ll = u % RL;
-    tile[kx * (RL + 1) + ll] = (iy0 + ll < ny) ? A[kx * ny + ll] : mk<C>(0, 0);
-  }
+  load_pairs<RL, N>(A, ny, ny - iy0, tile);
   __syncthreads();
   C v[E];
 #pragma unroll

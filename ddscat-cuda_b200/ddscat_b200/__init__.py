@@ -120,6 +120,7 @@ def _c64(a, n=None):
 
 BATCH_SOLVERS = {"qmrccg": 1, "pbcgs2": 2}
 REPLACE_RESIDUAL = 0x100  # DDSCAT_B200_REPLACE_RESIDUAL
+QMR_SYMMETRIC = 0x200  # DDSCAT_B200_QMR_SYMMETRIC
 
 
 def _vptr(a):
@@ -233,11 +234,13 @@ class DDA:
         return {"cbksca": cb.value, "csca": cs.value, "cscag": [cg[0], cg[1], cg[2]], "cscag2": cg2.value,
                 "navg": navg.value, "f1": f1[:ndir], "f2": f2[:ndir]}
 
-    def solve_batch(self, name, b, x, adia, aoff=None, maxit=300, tol=1e-5, check=True, replace=False):
+    def solve_batch(self, name, b, x, adia, aoff=None, maxit=300, tol=1e-5, check=True, replace=False,
+                    symmetric=False):
         """Batched solve; b, x (in/out), adia, aoff are (nrhs, 3*NAT) complex64
         host arrays, or CUDA tensors of the same shape (device-resident path).
         replace=True selects residual replacement instead of restarts at the
-        reliable-residual checks."""
+        reliable-residual checks; symmetric=True (QMRCCG) uses one MATVEC per
+        iteration (left Lanczos vectors equal to the right ones)."""
         nrhs = int(b.shape[0])
         for a in (b, x, adia) + (() if aoff is None else (aoff,)):
             if tuple(a.shape) != (nrhs, 3 * self.nat):
@@ -248,7 +251,7 @@ class DDA:
         tole = np.zeros(nrhs, dtype=np.float32)
         nc = np.zeros(nrhs, dtype=np.int32)
         st = np.zeros(nrhs, dtype=np.int32)
-        code = BATCH_SOLVERS[name] | (REPLACE_RESIDUAL if replace else 0)
+        code = BATCH_SOLVERS[name] | (REPLACE_RESIDUAL if replace else 0) | (QMR_SYMMETRIC if symmetric else 0)
         rc = self.lib.ddscat_b200_solve_batch_f32(code, nrhs, _vptr(b), _vptr(x), _vptr(adia),
                                                   _vptr(aoff), maxit, tol, _ptr(it), _ptr(tole), _ptr(nc), _ptr(st))
         if check:

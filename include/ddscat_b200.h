@@ -45,12 +45,19 @@ DDSCAT_CUDA_API int ddscat_b200_matvec_timing(int nrhs, int iters, int cwhat, fl
  * RHS unconverged with a large gap, replace the recursive residual by the
  * true one and keep the Krylov state, instead of restarting the solver from
  * the true residual (convergence is still declared on the true residual).
+ * QMRCCG may also be OR'ed with DDSCAT_B200_QMR_SYMMETRIC: the reference's
+ * QMRCCG starts its left and right Lanczos vectors equal (both r0) and the DDA
+ * matrix is complex symmetric, so the left vectors stay equal to the right
+ * ones and A p equals the recurrence vector q; this variant drops the second
+ * MATVEC of each iteration (one MATVEC per iteration instead of two; same
+ * iterates in exact arithmetic).
  * Codes: 500 invalid argument / not prepared, 501 solver, 502 mixed pointer
  * kinds, 503 workspace allocation, 504 input transfer, 505 solver failure,
  * 506 output transfer. */
 #define DDSCAT_B200_QMRCCG 1
 #define DDSCAT_B200_PBCGS2 2
 #define DDSCAT_B200_REPLACE_RESIDUAL 0x100
+#define DDSCAT_B200_QMR_SYMMETRIC 0x200
 DDSCAT_CUDA_API int ddscat_b200_solve_batch_f32(int solver, int nrhs, const void *b, void *x, const void *adia,
                                                 const void *aoff, int maxit, float tol, int *itno, float *tole,
                                                 int *ncompte, int *status);

@@ -114,3 +114,27 @@ def test_batch_residual_replacement(name):
         assert np.linalg.norm(xp[r] - xr[r]) / np.linalg.norm(xr[r]) < 20 * TOL
     assert rest.itno.sum() > 0 and rep.itno.sum() > 0
     dda.release()
+
+
+@pytest.mark.gpu
+def test_batch_qmrccg_symmetric_form():
+    """One-MATVEC QMRCCG (DDSCAT_B200_QMR_SYMMETRIC): same iterates as the
+    two-product form up to rounding, half the MATVECs per iteration."""
+    n = 24
+    prob = targets.make_problem(n, m=1.33 + 0.05j, x=6.0, orientations=targets.random_orientations(3, seed=9))
+    dda = D.DDA()
+    dda.prepare_green(n, n, n, prob.iocc, prob.incid[0].k)
+    b, adia = _batch_inputs(prob)
+    for replace in (False, True):
+        x2, x1 = np.zeros_like(b), np.zeros_like(b)
+        two = dda.solve_batch("qmrccg", b, x2, adia, maxit=2000, tol=TOL, replace=replace)
+        one = dda.solve_batch("qmrccg", b, x1, adia, maxit=2000, tol=TOL, replace=replace, symmetric=True)
+        assert np.all(one.status == 0) and np.all(one.tole <= TOL)
+        assert np.all(dda.residual_f64(b, x1, adia) <= 1.2 * TOL)
+        for r in range(b.shape[0]):
+            assert np.linalg.norm(x1[r] - x2[r]) / np.linalg.norm(x2[r]) < 20 * TOL
+            # 1 MATVEC per iteration + init + checks, against 2 per iteration
+            assert one.ncompte[r] <= 0.6 * two.ncompte[r] * one.itno[r] / max(two.itno[r], 1) + 20
+    with pytest.raises(D.DDSCATError):
+        dda.solve_batch("pbcgs2", b, np.zeros_like(b), adia, maxit=10, tol=TOL, symmetric=True)
+    dda.release()
