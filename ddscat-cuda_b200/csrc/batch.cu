@@ -119,6 +119,113 @@ __global__ void __launch_bounds__(BT) kb_dots(int n, BDot<T> sp, const int* mask
   }
 }
 
+// Block partial sums of NK (<= 2) FP64 accumulators into part[r][k0 + k][block],
+// and the last block of RHS r (in completion order) folds all partials in a
+// fixed order into out[r][k0 + k]: deterministic for a given grid.
+template <int NK>
+__device__ __forceinline__ void block_sums(const double2 (&acc)[NK], int k0, int r, double2* part, double2* out,
+                                           unsigned* cnt) {
+  __shared__ double2 ws[NK][BT / 32];
+  __shared__ bool last;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < NK; ++k) {
+    const double2 v = wsum2(acc[k]);
+    if (lane == 0) ws[k][wid] = v;
+  }
+  __syncthreads();
+  double2* P = part + ((size_t)r * 8) * gridDim.x;
+  if (threadIdx.x < 32) {
+#pragma unroll
+    for (int k = 0; k < NK; ++k) {
+      double2 v = lane < BT / 32 ? ws[k][lane] : make_double2(0.0, 0.0);
+      v = wsum2(v);
+      if (lane == 0) P[(size_t)(k0 + k) * gridDim.x + blockIdx.x] = v;
+    }
+  }
+  __threadfence();
+  if (threadIdx.x == 0) last = atomicInc(cnt + r, gridDim.x - 1) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+#pragma unroll
+  for (int k = 0; k < NK; ++k) {
+    double2 v = make_double2(0.0, 0.0);
+    for (int bi = threadIdx.x; bi < (int)gridDim.x; bi += blockDim.x) {
+      const volatile double* pp = reinterpret_cast<volatile double*>(P + (size_t)(k0 + k) * gridDim.x + bi);
+      v.x += pp[0];
+      v.y += pp[1];
+    }
+    v = wsum2(v);
+    __syncthreads();
+    if (lane == 0) ws[k][wid] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+#pragma unroll
+    for (int k = 0; k < NK; ++k) {
+      double2 v = lane < BT / 32 ? ws[k][lane] : make_double2(0.0, 0.0);
+      v = wsum2(v);
+      if (lane == 0) out[(size_t)r * 8 + k0 + k] = v;
+    }
+  }
+}
+
+// One-MATVEC QMRCCG, first vector step of an iteration, per RHS r in mask:
+//   p = cp p + cv vt ; q = cq q + cw atw ; vt = ct vt + q
+// with sums |vt|^2 and vt^T vt into out slots k0, k0+1.  Same element
+// arithmetic as the separate kb_lin updates it replaces.
+template <typename C>
+__global__ void __launch_bounds__(BT) kq_pqv(int n, C* p, C* q, C* vt, const C* atw, const double2* co,
+                                             const int* mask, int k0, double2* part, double2* out, unsigned* cnt) {
+  const int r = blockIdx.y, R = gridDim.y;
+  if (mask && !mask[r]) return;
+  const size_t off = (size_t)r * n;
+  const double2 cp = co[r], cv = co[R + r], cq = co[2 * R + r], cw = co[3 * R + r], ct = co[4 * R + r];
+  double2 acc[2] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
+  for (int i = blockIdx.x * BT + threadIdx.x; i < n; i += gridDim.x * BT) {
+    const C v0 = vt[off + i];
+    const C pn = cadd(zmulv(cp, p[off + i]), zmulv(cv, v0));
+    const C qn = cadd(zmulv(cq, q[off + i]), zmulv(cw, atw[off + i]));
+    const C vn = cadd(zmulv(ct, v0), qn);
+    p[off + i] = pn;
+    q[off + i] = qn;
+    vt[off + i] = vn;
+    const double2 a = to_d(vn);
+    acc[0].x += a.x * a.x + a.y * a.y;
+    acc[1].x += a.x * a.x - a.y * a.y;
+    acc[1].y += 2.0 * a.x * a.y;
+  }
+  block_sums<2>(acc, k0, r, part, out, cnt);
+}
+
+// One-MATVEC QMRCCG, last vector step of an iteration, per RHS r in mask:
+//   d = th d + ka p ; s = th s + ka q ; x = x + d ; r = r - s
+// with the sum |r|^2 into out slot k0.
+template <typename C>
+__global__ void __launch_bounds__(BT) kq_dsxr(int n, C* d, C* s, C* x, C* rv, const C* p, const C* q,
+                                              const double2* co, const int* mask, int k0, double2* part,
+                                              double2* out, unsigned* cnt) {
+  const int r = blockIdx.y, R = gridDim.y;
+  if (mask && !mask[r]) return;
+  const size_t off = (size_t)r * n;
+  const double2 th = co[r], ka = co[R + r];
+  double2 acc[1] = {make_double2(0.0, 0.0)};
+  for (int i = blockIdx.x * BT + threadIdx.x; i < n; i += gridDim.x * BT) {
+    const C dn = cadd(zmulv(th, d[off + i]), zmulv(ka, p[off + i]));
+    const C sn = cadd(zmulv(th, s[off + i]), zmulv(ka, q[off + i]));
+    const C xn = cadd(x[off + i], dn);
+    const C rn = csub(rv[off + i], sn);
+    d[off + i] = dn;
+    s[off + i] = sn;
+    x[off + i] = xn;
+    rv[off + i] = rn;
+    const double2 a = to_d(rn);
+    acc[0].x += a.x * a.x + a.y * a.y;
+  }
+  block_sums<1>(acc, k0, r, part, out, cnt);
+}
+
 template <typename T> int BatchOps<T>::init(int R_, int n_, cudaStream_t s) {
   R = R_;
   n = n_;
@@ -178,6 +285,46 @@ int BatchOps<T>::lin(C* d, const double2* zd, const C* a, const double2* za, con
                                             msk);
   note_launch();
   return check_launch("batched vector update");
+}
+
+template <typename T> const double2* BatchOps<T>::upload(const std::vector<const double2*>& cols) {
+  const size_t need = cols.size() * (size_t)R;
+  if (coef_pos + need > coef_cap) {
+    cudaStreamSynchronize(stream);
+    coef_pos = 0;
+  }
+  double2* h = h_coef + coef_pos;
+  double2* dc = d_coef + coef_pos;
+  for (size_t k = 0; k < cols.size(); ++k)
+    for (int r = 0; r < R; ++r) h[k * R + r] = cols[k][r];
+  cudaMemcpyAsync(dc, h, need * sizeof(double2), cudaMemcpyHostToDevice, stream);
+  coef_pos += need;
+  return dc;
+}
+
+template <typename T>
+int BatchOps<T>::qmr_pqv(C* p, C* q, C* vt, const C* atw, const double2* cp, const double2* cv, const double2* cq,
+                         const double2* cw, const double2* ct, const int* msk) {
+  const double2* co = upload({cp, cv, cq, cw, ct});
+  kq_pqv<C><<<dim3(nb, R), BT, 0, stream>>>(n, p, q, vt, atw, co, msk, 2, d_part, d_out, d_cnt);
+  note_launch();
+  return check_launch("batched QMR p/q/v update");
+}
+
+template <typename T>
+int BatchOps<T>::qmr_dsxr(C* d, C* s, C* x, C* r, const C* p, const C* q, const double2* th, const double2* ka,
+                          const int* msk, std::vector<double2>& rr) {
+  const double2* co = upload({th, ka});
+  kq_dsxr<C><<<dim3(nb, R), BT, 0, stream>>>(n, d, s, x, r, p, q, co, msk, 0, d_part, d_out, d_cnt);
+  note_launch();
+  if (check_launch("batched QMR d/s/x/r update")) return 1;
+  cudaError_t e = cudaMemcpyAsync(h_out, d_out, (size_t)R * 8 * sizeof(double2), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) { set_cuda_error("batched QMR update D2H", e); return 1; }
+  reset_ring();
+  rr.assign((size_t)R, make_double2(0, 0));
+  for (int i = 0; i < R; ++i) rr[i] = h_out[(size_t)i * 8];
+  return 0;
 }
 
 template <typename T> int BatchOps<T>::copy(C* d, const C* a, const int* msk) {
@@ -396,33 +543,27 @@ template <typename T> int solve_batch_qmrccg(BatchIO<T>& io, BatchResult& res) {
       cmu[i] = dz(-mu[i]); cgam[i] = dz(1.0 / gamma[i]);
       cq[i] = dz(-(gamma[i] * mu[i]) / ksi[i]); cksi[i] = dz(1.0 / ksi[i]);
     }
-    ops.lin(p, cmu.data(), vt, cgam.data(), nullptr, nullptr, MI);
-    ops.lin(q, cq.data(), atw, cksi.data(), nullptr, nullptr, MI);
-    if (!sym && (rc = c.mv(p, ap, I))) return rc;
-    const C* Ap = sym ? q : ap;  // A p
     for (int i = 0; i < R; ++i) {
       if (!I[i]) continue;
       ctg[i] = dz(-(tau[i] / gamma[i]));
       ctk[i] = dz(-(tau[i] / ksi[i]));
     }
-    ops.lin(vt, ctg.data(), Ap, one.data(), nullptr, nullptr, MI);
-    if (!sym) ops.lin(wt, ctk.data(), q, one.data(), nullptr, nullptr, MI);
+    const C* Ap = sym ? q : ap;  // A p
     const C* W = sym ? vt : wt;  // left Lanczos vector
     std::vector<double2> o3, o1;
-    {
+    if (sym) {
+      // one fused pass: p, q (= A p), vt and the sums |vt|^2, vt^T vt
+      if (ops.qmr_pqv(p, q, vt, atw, cmu.data(), cgam.data(), cq.data(), cksi.data(), ctg.data(), MI)) return 1;
+    } else {
+      ops.lin(p, cmu.data(), vt, cgam.data(), nullptr, nullptr, MI);
+      ops.lin(q, cq.data(), atw, cksi.data(), nullptr, nullptr, MI);
+      if ((rc = c.mv(p, ap, I))) return rc;
+      ops.lin(vt, ctg.data(), Ap, one.data(), nullptr, nullptr, MI);
+      ops.lin(wt, ctk.data(), q, one.data(), nullptr, nullptr, MI);
       const C* A3[3] = {vt, W, vt};
       const C* B3[3] = {vt, W, W};
       const int c3[3] = {1, 1, 0};
-      if (sym) {
-        const C* A2[2] = {vt, vt};
-        const int c2[2] = {1, 0};
-        std::vector<double2> o2;
-        if (ops.dots(2, A2, A2, c2, MI, o2)) return 1;
-        o3.resize((size_t)3 * R);
-        for (int i = 0; i < R; ++i) { o3[3 * i] = o3[3 * i + 1] = o2[2 * i]; o3[3 * i + 2] = o2[2 * i + 1]; }
-      } else if (ops.dots(3, A3, B3, c3, MI, o3)) {
-        return 1;
-      }
+      if (ops.dots(3, A3, B3, c3, MI, o3)) return 1;
     }
     if ((rc = c.mv(W, atw, I))) return rc;
     {
@@ -430,6 +571,14 @@ template <typename T> int solve_batch_qmrccg(BatchIO<T>& io, BatchResult& res) {
       const C* B1b[1] = {atw};
       const int c1[1] = {0};
       if (ops.dots(1, A1b, B1b, c1, MI, o1)) return 1;
+    }
+    if (sym) {
+      o3.assign((size_t)3 * R, make_double2(0, 0));
+      for (int i = 0; i < R; ++i) {
+        if (!I[i]) continue;
+        o3[3 * i] = o3[3 * i + 1] = ops.slot(i, 2);
+        o3[3 * i + 2] = ops.slot(i, 3);
+      }
     }
     for (int i = 0; i < R; ++i) {
       if (!I[i]) continue;
@@ -460,17 +609,20 @@ template <typename T> int solve_batch_qmrccg(BatchIO<T>& io, BatchResult& res) {
       cka[i] = dz(kappa[i]);
     }
     MI = ops.mask(I);
-    ops.lin(d, cth.data(), p, cka.data(), nullptr, nullptr, MI);
-    ops.lin(s, cth.data(), Ap, cka.data(), nullptr, nullptr, MI);
-    ops.lin(xs, one.data(), d, one.data(), nullptr, nullptr, MI);
-    ops.lin(r, one.data(), s, mone.data(), nullptr, nullptr, MI);
-    {
+    if (sym) {
+      // one fused pass: d, s, x, r and |r|^2
+      if (ops.qmr_dsxr(d, s, xs, r, p, Ap, cth.data(), cka.data(), MI, o)) return 1;
+    } else {
+      ops.lin(d, cth.data(), p, cka.data(), nullptr, nullptr, MI);
+      ops.lin(s, cth.data(), Ap, cka.data(), nullptr, nullptr, MI);
+      ops.lin(xs, one.data(), d, one.data(), nullptr, nullptr, MI);
+      ops.lin(r, one.data(), s, mone.data(), nullptr, nullptr, MI);
       const C* Ar[1] = {r};
       const int c1[1] = {1};
       if (ops.dots(1, Ar, Ar, c1, MI, o)) return 1;
-      for (int i = 0; i < R; ++i)
-        if (I[i]) resid[i] = std::sqrt(std::max(0.0, o[i].x)) / bnorm[i];
     }
+    for (int i = 0; i < R; ++i)
+      if (I[i]) resid[i] = std::sqrt(std::max(0.0, o[i].x)) / bnorm[i];
     std::vector<int> CK(R, 0);
     for (int i = 0; i < R; ++i) CK[i] = I[i] && ((it[i] % 20) == 0 || resid[i] <= io.tol);
     if (any_of(CK)) {

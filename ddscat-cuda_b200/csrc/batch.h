@@ -44,6 +44,15 @@ template <typename T> struct BatchOps {
   int dots(int K, const C* const* a, const C* const* b, const int* conj, const int* mask, std::vector<double2>& out);
   // ||a - b||^2 and ||a - b - c||^2 per RHS (FP64)
   int diff_norms(const C* a, const C* b, const C* c, const int* mask, std::vector<double2>& out);
+  // fused steps of the one-MATVEC QMRCCG iteration (see kq_pqv / kq_dsxr):
+  // qmr_pqv leaves |vt|^2 and vt^T vt in output slots 2 and 3 (read them with
+  // slot() after the next synchronising call); qmr_dsxr returns |r|^2 per RHS
+  int qmr_pqv(C* p, C* q, C* vt, const C* atw, const double2* cp, const double2* cv, const double2* cq,
+              const double2* cw, const double2* ct, const int* mask);
+  int qmr_dsxr(C* d, C* s, C* x, C* r, const C* p, const C* q, const double2* th, const double2* ka,
+               const int* mask, std::vector<double2>& rr);
+  double2 slot(int r, int k) const { return h_out[(size_t)r * 8 + k]; }
+  const double2* upload(const std::vector<const double2*>& cols);
   // after a stream sync every pending coefficient copy has landed; masks wrap on
   // their own (a mask pointer stays valid for MASKS-1 further uploads)
   void reset_ring() { coef_pos = 0; }
