@@ -22,6 +22,7 @@ template <> struct cplx_t<double> { using type = double2; };
 template <typename T> using cplx = typename cplx_t<T>::type;
 
 template <typename C> DDB_HD C mk(double re, double im) { C c; c.x = re; c.y = im; return c; }
+template <typename C, typename R> DDB_HD C mk2(R re, R im) { C c; c.x = re; c.y = im; return c; }
 DDB_HD float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 DDB_HD double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 DDB_HD float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
@@ -34,6 +35,39 @@ DDB_HD float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); 
 DDB_HD double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
 // multiply by i*s (s = +1 or -1 selects the sign of the rotation)
 DDB_HD float2 cmuli(float2 a, float s) { return make_float2(-a.y * s, a.x * s); }
+
+// Packed complex add / subtract: one Blackwell f32x2 instruction for both
+// lanes (IEEE round-to-nearest per lane, identical results to two scalar
+// adds).  Used by the FFT butterflies, where adds dominate; elsewhere the
+// scalar forms are kept so the compiler can contract products into FMAs.
+__device__ __forceinline__ float2 vadd(float2 a, float2 b) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+  float2 c;
+  asm("add.rn.f32x2 %0, %1, %2;"
+      : "=l"(reinterpret_cast<uint64_t&>(c))
+      : "l"(reinterpret_cast<const uint64_t&>(a)), "l"(reinterpret_cast<const uint64_t&>(b)));
+  return c;
+#else
+  return make_float2(a.x + b.x, a.y + b.y);
+#endif
+}
+__device__ __forceinline__ float2 vsub(float2 a, float2 b) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+  float2 c;
+  asm("sub.rn.f32x2 %0, %1, %2;"
+      : "=l"(reinterpret_cast<uint64_t&>(c))
+      : "l"(reinterpret_cast<const uint64_t&>(a)), "l"(reinterpret_cast<const uint64_t&>(b)));
+  return c;
+#else
+  return make_float2(a.x - b.x, a.y - b.y);
+#endif
+}
+__device__ __forceinline__ double2 vadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 vsub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+// a + s*i*b and a - s*i*b (s = +-1): the rotated term stays scalar, where the
+// swap and sign fold into the adds for free
+template <int S, typename C> __device__ __forceinline__ C addrot(C a, C b) { return mk2<C>(a.x - S * b.y, a.y + S * b.x); }
+template <int S, typename C> __device__ __forceinline__ C subrot(C a, C b) { return mk2<C>(a.x + S * b.y, a.y - S * b.x); }
 DDB_HD double2 cmuli(double2 a, double s) { return make_double2(-a.y * s, a.x * s); }
 DDB_HD double2 to_d(float2 a) { return make_double2((double)a.x, (double)a.y); }
 DDB_HD double2 to_d(double2 a) { return a; }

@@ -45,16 +45,16 @@ inline FftPlan make_fft_plan(int n) {
 // ---- butterflies: in-register R-point DFTs, W = exp(dir*2*pi*i/R) ---------
 template <int DIR, typename C> __device__ __forceinline__ void bfly2(C* v) {
   C a = v[0], b = v[1];
-  v[0] = cadd(a, b);
-  v[1] = csub(a, b);
+  v[0] = vadd(a, b);
+  v[1] = vsub(a, b);
 }
 template <int DIR, typename C> __device__ __forceinline__ void bfly4(C* v) {
-  C s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
-  C s13 = cadd(v[1], v[3]), d13 = cmuli(csub(v[1], v[3]), (float)DIR);
-  v[0] = cadd(s02, s13);
-  v[2] = csub(s02, s13);
-  v[1] = cadd(d02, d13);
-  v[3] = csub(d02, d13);
+  const C s02 = vadd(v[0], v[2]), d02 = vsub(v[0], v[2]);
+  const C s13 = vadd(v[1], v[3]), t13 = vsub(v[1], v[3]);
+  v[0] = vadd(s02, s13);
+  v[2] = vsub(s02, s13);
+  v[1] = addrot<DIR>(d02, t13);  // d02 + DIR*i*t13
+  v[3] = subrot<DIR>(d02, t13);
 }
 template <int DIR, typename C> __device__ __forceinline__ void bfly8(C* v) {
   C e[4] = {v[0], v[2], v[4], v[6]};
@@ -66,16 +66,15 @@ template <int DIR, typename C> __device__ __forceinline__ void bfly8(C* v) {
   // W8^1 = (1 + dir*i)/sqrt2, W8^2 = dir*i, W8^3 = (-1 + dir*i)/sqrt2
   C o1 = o[1], o3 = o[3];
   C t1 = mk<C>((double)(h * (o1.x - (R)DIR * o1.y)), (double)(h * (o1.y + (R)DIR * o1.x)));
-  C t2 = cmuli(o[2], (float)DIR);
   C t3 = mk<C>((double)(h * (-o3.x - (R)DIR * o3.y)), (double)(h * (-o3.y + (R)DIR * o3.x)));
-  v[0] = cadd(e[0], o[0]);
-  v[4] = csub(e[0], o[0]);
-  v[1] = cadd(e[1], t1);
-  v[5] = csub(e[1], t1);
-  v[2] = cadd(e[2], t2);
-  v[6] = csub(e[2], t2);
-  v[3] = cadd(e[3], t3);
-  v[7] = csub(e[3], t3);
+  v[0] = vadd(e[0], o[0]);
+  v[4] = vsub(e[0], o[0]);
+  v[1] = vadd(e[1], t1);
+  v[5] = vsub(e[1], t1);
+  v[2] = addrot<DIR>(e[2], o[2]);  // e2 + W8^2 o2, W8^2 = DIR*i
+  v[6] = subrot<DIR>(e[2], o[2]);
+  v[3] = vadd(e[3], t3);
+  v[7] = vsub(e[3], t3);
 }
 template <int DIR, typename C> __device__ __forceinline__ void bfly3(C* v) {
   using R = decltype(v[0].x);

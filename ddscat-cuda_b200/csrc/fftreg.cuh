@@ -63,11 +63,11 @@ template <int K, int DIR, typename C> __device__ __forceinline__ void dftr_h(C* 
   if constexpr (K == 2) {
     v[1] = v[0];
   } else if constexpr (K == 4) {
-    const C a = v[0], b = v[1], bi = cmuli(v[1], (float)DIR);
-    v[0] = cadd(a, b);
-    v[2] = csub(a, b);
-    v[1] = cadd(a, bi);
-    v[3] = csub(a, bi);
+    const C a = v[0], b = v[1];
+    v[0] = vadd(a, b);
+    v[2] = vsub(a, b);
+    v[1] = addrot<DIR>(a, b);  // a + DIR*i*b
+    v[3] = subrot<DIR>(a, b);
   } else if constexpr (K == 8) {
     C e[4] = {v[0], v[2], v[0], v[0]};
     C o[4] = {v[1], v[3], v[1], v[1]};
@@ -77,16 +77,15 @@ template <int K, int DIR, typename C> __device__ __forceinline__ void dftr_h(C* 
     const R h = (R)0.70710678118654752440;
     C o1 = o[1], o3 = o[3];
     C t1 = mk<C>((double)(h * (o1.x - (R)DIR * o1.y)), (double)(h * (o1.y + (R)DIR * o1.x)));
-    C t2 = cmuli(o[2], (float)DIR);
     C t3 = mk<C>((double)(h * (-o3.x - (R)DIR * o3.y)), (double)(h * (-o3.y + (R)DIR * o3.x)));
-    v[0] = cadd(e[0], o[0]);
-    v[4] = csub(e[0], o[0]);
-    v[1] = cadd(e[1], t1);
-    v[5] = csub(e[1], t1);
-    v[2] = cadd(e[2], t2);
-    v[6] = csub(e[2], t2);
-    v[3] = cadd(e[3], t3);
-    v[7] = csub(e[3], t3);
+    v[0] = vadd(e[0], o[0]);
+    v[4] = vsub(e[0], o[0]);
+    v[1] = vadd(e[1], t1);
+    v[5] = vsub(e[1], t1);
+    v[2] = addrot<DIR>(e[2], o[2]);
+    v[6] = subrot<DIR>(e[2], o[2]);
+    v[3] = vadd(e[3], t3);
+    v[7] = vsub(e[3], t3);
   } else {
     // K = K1*K2, element K2*a + b is zero for a >= K1/2
     constexpr int K1 = (K == 16) ? 4 : 8;
