@@ -71,6 +71,7 @@ template <typename T> struct Engine {
   int* occ = nullptr;      // [nat0]
   int* inv = nullptr;      // [nat], -1 for vacuum
   int16_t* iocc = nullptr; // [nat]
+  int* rowq = nullptr;     // [nat/nx + 1]: occupied sites before each x row (row = iy + ny*iz)
   // MATVEC workspace
   C* zhat = nullptr;
   int zcap = 0;            // RHS capacity of zhat

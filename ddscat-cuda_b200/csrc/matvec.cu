@@ -604,14 +604,25 @@ int Engine<T>::init_geometry(int nx, int ny, int nz, int ipbc, int nat, int nat0
     set_error("occupied-index map", msg);
     return 2;
   }
+  // compact index of the first occupied site of every x row: the sites of
+  // consecutive rows occupy one contiguous compact range
+  const int nrows = nat / nx;
+  std::vector<int> rowq_h((size_t)nrows + 1, 0);
+  for (int r = 0; r < nrows; ++r) {
+    int c = 0;
+    for (int ix = 0; ix < nx; ++ix) c += iocc_host[(size_t)r * nx + ix] != 0;
+    rowq_h[r + 1] = rowq_h[r] + c;
+  }
   cudaError_t e;
   e = cudaMalloc((void**)&occ, (size_t)nat0 * sizeof(int));
   if (e == cudaSuccess) e = cudaMalloc((void**)&inv, (size_t)nat * sizeof(int));
   if (e == cudaSuccess) e = cudaMalloc((void**)&iocc, (size_t)nat * sizeof(int16_t));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&rowq, ((size_t)nrows + 1) * sizeof(int));
   if (e != cudaSuccess) { set_cuda_error("prepare: index maps", e); return 3; }
-  bytes_allocated += (size_t)nat0 * 4 + (size_t)nat * 6;
+  bytes_allocated += (size_t)nat0 * 4 + (size_t)nat * 6 + ((size_t)nrows + 1) * 4;
   cudaMemcpy(occ, occ_h.data(), (size_t)nat0 * sizeof(int), cudaMemcpyHostToDevice);
   cudaMemcpy(inv, inv_h.data(), (size_t)nat * sizeof(int), cudaMemcpyHostToDevice);
+  cudaMemcpy(rowq, rowq_h.data(), ((size_t)nrows + 1) * sizeof(int), cudaMemcpyHostToDevice);
   e = cudaMemcpy(iocc, iocc_host, (size_t)nat * sizeof(int16_t), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) { set_cuda_error("prepare: index map H2D", e); return 3; }
   e = cudaMalloc((void**)&green, g.green_count() * sizeof(C));
@@ -808,7 +819,7 @@ template <typename T> int Engine<T>::upload_green(const void* host_green) {
 
 template <typename T> void Engine<T>::release() {
   cudaFree(twx); cudaFree(twy); cudaFree(twz);
-  cudaFree(green); cudaFree(occ); cudaFree(inv); cudaFree(iocc);
+  cudaFree(green); cudaFree(occ); cudaFree(inv); cudaFree(iocc); cudaFree(rowq);
   cudaFree(zhat); cudaFree(slab);
   *this = Engine<T>{};
 }

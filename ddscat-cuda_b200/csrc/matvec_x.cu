@@ -35,6 +35,7 @@ template <typename T> struct XParams {
   int io_full, a_full, conj;
   const int* inv;
   const int16_t* iocc;
+  const int* rowq;  // compact index of the first occupied site of each x row
   const int* mask;
   int rhs0;
   cplx<T>* A;  // [rl][c][iz][kx][iy]
@@ -48,6 +49,7 @@ template <typename T> struct XParams {
   const cplx<T>* twz;
   int lsx, lsy, lsz;  // line strides of the x, y, z passes
   int my_log2;        // log2(My)
+  int tlx;            // tile / line scratch elements of the x passes
   T inv_ngrid;
 };
 
@@ -110,6 +112,27 @@ __device__ __forceinline__ void load_pairs(const C* g, int ld, int valid, C* til
   }
 }
 
+// Copy cnt (<= MAXC) contiguous elements from global to shared memory with the
+// whole 256-thread block, eight loads in flight per thread.
+template <int MAXC, typename C> __device__ __forceinline__ void stage_chunk(C* dst, const C* src, int cnt) {
+  constexpr int IT = (MAXC + 255) / 256;
+  constexpr int G = IT < 8 ? IT : 8;
+#pragma unroll 1
+  for (int k0 = 0; k0 < IT; k0 += G) {
+    C tmp[G];
+#pragma unroll
+    for (int k = 0; k < G; ++k) {
+      const int u = threadIdx.x + 256 * (k0 + k);
+      if (u < cnt) tmp[k] = src[u];
+    }
+#pragma unroll
+    for (int k = 0; k < G; ++k) {
+      const int u = threadIdx.x + 256 * (k0 + k);
+      if (u < cnt) dst[u] = tmp[k];
+    }
+  }
+}
+
 // ------------------------------------------------------------- XF: x forward
 // block: RL rows (iy) x TT threads, thread-fastest; grid (ceil(ny/RL), nz, 3*nr)
 template <typename T, int N> __global__ void __launch_bounds__(256) kx_xf(XParams<T> P) {
@@ -130,19 +153,28 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_xf(XParam
   const C* x = P.x + (size_t)rl * P.x_rs + (size_t)c * S;
   const int jrow = P.nx * (iy + P.ny * iz);
   C v[E];
+  if (P.io_full) {
 #pragma unroll
-  for (int i = 0; i < H; ++i) {
-    const int ix = t + TT * i;  // < nx = N/2
-    v[i] = mk<C>(0, 0);
-    if (iy < P.ny) {
-      if (P.io_full) {
-        v[i] = x[jrow + ix];
-      } else {
-        const int q = P.inv[jrow + ix];
-        if (q >= 0) v[i] = x[q];
-      }
-      if (P.conj) v[i].y = -v[i].y;
-    }
+    for (int i = 0; i < H; ++i) v[i] = iy < P.ny ? x[jrow + t + TT * i] : mk<C>(0, 0);  // ix < nx = N/2
+  } else {
+    // the block's rows hold one contiguous compact range [q0, q0 + cnt): copy
+    // it to shared memory (coalesced) while the inv lookups are in flight,
+    // then gather from there
+    const int r0 = iy0 + P.ny * iz, nrows = min(RL, P.ny - iy0);
+    const int q0 = P.rowq[r0], cnt = P.rowq[r0 + nrows] - q0;
+    int qi[H];
+#pragma unroll
+    for (int i = 0; i < H; ++i) qi[i] = iy < P.ny ? P.inv[jrow + t + TT * i] : -1;
+    C* chunk = lines;  // at most RL*nx elements; consumed before the FFT uses the scratch
+    stage_chunk<RL * (N / 2)>(chunk, x + q0, cnt);
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < H; ++i) v[i] = qi[i] >= 0 ? chunk[qi[i] - q0] : mk<C>(0, 0);
+    __syncthreads();
+  }
+  if (P.conj) {
+#pragma unroll
+    for (int i = 0; i < H; ++i) v[i].y = -v[i].y;
   }
   line_fft<E, TT, +1, false, true>(v, lines + (size_t)l * P.lsx, t, tws);
   __syncthreads();  // all line scratch consumed before the tile reuses it
@@ -266,12 +298,25 @@ __global__ void __launch_bounds__(3 * XShape<N>::TT * XShape<N>::RZ, XShape<N>::
       if (P.ipbc == 0) {
         R sxy, sxz, syz;
         const C* rec0 = green_rec(P, kx, ky, 0, sxy, sxz, syz);
-        for (int kz = gk; kz <= N / 2; kz += GT) {
-          C a[6];
-          load_rec<T>(rec0 + 6 * kz, a);
-          green_apply(a, sxy, sxz, syz, L0[kz], L1[kz], L2[kz]);  // kz <= nz: sz = +1
-          const int km = N - kz;
-          if (kz > 0 && km != kz) green_apply(a, sxy, -sxz, -syz, L0[km], L1[km], L2[km]);  // sz = -1
+        // records kz = gk + GT*j: up to 3 loads in flight before the first use
+        constexpr int NIT = (N / 2 + GT) / GT;
+#pragma unroll
+        for (int j0 = 0; j0 < NIT; j0 += 3) {
+          C a[3][6];
+#pragma unroll
+          for (int j = 0; j < 3; ++j) {
+            const int kz = gk + GT * (j0 + j);
+            if (j0 + j < NIT && kz <= N / 2) load_rec<T>(rec0 + 6 * kz, a[j]);
+          }
+#pragma unroll
+          for (int j = 0; j < 3; ++j) {
+            const int kz = gk + GT * (j0 + j);
+            if (j0 + j < NIT && kz <= N / 2) {
+              green_apply(a[j], sxy, sxz, syz, L0[kz], L1[kz], L2[kz]);  // kz <= nz: sz = +1
+              const int km = N - kz;
+              if (kz > 0 && km != kz) green_apply(a[j], sxy, -sxz, -syz, L0[km], L1[km], L2[km]);  // sz = -1
+            }
+          }
         }
       } else {
         for (int kz = gk; kz < N; kz += GT) {
@@ -326,21 +371,54 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_yi(XParam
 }
 
 // ------------------------------------------------------------- XI: x inverse + finish
+constexpr int XI_STAGE_MAX = 2048;  // largest staged chunk of the XI pass (elements)
+
 // block: RL rows (iy) x TT; grid (ceil(ny/RL), nz, 3*nr)
+// shared memory: twiddles [N] | tile / line scratch [tlx] | x chunk | CXADIA chunk
 template <typename T, int N> __global__ void __launch_bounds__(256) kx_xi(XParams<T> P) {
   using C = cplx<T>;
   using S_ = XShape<N>;
   constexpr int E = S_::E, TT = S_::TT, H = S_::H, RL = S_::RL;
+  constexpr int MAXC = RL * (N / 2);
+  constexpr bool STAGE = MAXC <= XI_STAGE_MAX;  // larger rows keep direct loads (shared memory)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int t = threadIdx.x % TT, l = threadIdx.x / TT;
   C* tws = reinterpret_cast<C*>(smem_raw);
   C* tile = tws + N;
   C* lines = tws + N;
+  C* xs = tws + N + P.tlx;
+  C* as = xs + MAXC;
   const int iy0 = blockIdx.x * RL, iy = iy0 + l, iz = blockIdx.y;
   const int rl = blockIdx.z / 3, c = blockIdx.z - 3 * (blockIdx.z / 3);
   if (xoff(P, rl)) return;
   load_tw<T, N>(tws, P.twx);
   const int ny = P.ny;
+  const int S = P.io_full ? P.nat : P.nat0;
+  const int SA = P.a_full ? P.nat : P.nat0;
+  const C* x = P.x + (size_t)rl * P.x_rs;
+  const C* ad = P.adia + (size_t)rl * P.a_rs + (size_t)c * SA;
+  // The rows of this block hold one contiguous range of sites (full layout) or
+  // of compact indices (compact layout): when x and CXADIA share the layout,
+  // both ranges are staged in shared memory together with the A tile, so the
+  // finish reads no global memory.
+  const int r0 = iy0 + ny * iz, nrows = min(RL, ny - iy0);
+  const bool chunked = STAGE && P.io_full == P.a_full;
+  int q0 = 0, cnt = 0;
+  if (chunked) {
+    if (P.io_full) { q0 = P.nx * r0; cnt = nrows * P.nx; }
+    else { q0 = P.rowq[r0]; cnt = P.rowq[r0 + nrows] - q0; }
+  }
+  const int jrow = P.nx * (iy + ny * iz);
+  int qi[H];  // x / y index of each kept element, -1 for vacuum
+#pragma unroll
+  for (int i = 0; i < H; ++i) {
+    const int j = jrow + t + TT * i;  // ix < nx
+    qi[i] = iy < ny ? (P.io_full ? (P.iocc[j] != 0 ? j : -1) : P.inv[j]) : -1;
+  }
+  if (chunked) {
+    stage_chunk<MAXC>(xs, x + (size_t)c * S + q0, cnt);
+    stage_chunk<MAXC>(as, ad + q0, cnt);
+  }
   const C* A = P.A + (size_t)rl * P.A_rs + ((size_t)(c * P.nz + iz) * P.Mx) * ny + iy0;
   load_pairs<RL, N>(A, ny, ny - iy0, tile);
   __syncthreads();
@@ -351,28 +429,22 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_xi(XParam
   line_fft<E, TT, -1, false>(v, lines + (size_t)l * P.lsx, t, tws);
   if (iy >= ny) return;
   // finish (cu:116-118): y = CXADIA x - w/ngrid [+ CXAOFF terms], conj for 'C'
-  const int S = P.io_full ? P.nat : P.nat0;
-  const int SA = P.a_full ? P.nat : P.nat0;
-  const C* x = P.x + (size_t)rl * P.x_rs;
   C* y = P.y + (size_t)rl * P.y_rs + (size_t)c * S;
-  const C* ad = P.adia + (size_t)rl * P.a_rs + (size_t)c * SA;
   const C* ao = P.aoff ? P.aoff + (size_t)rl * P.a_rs : nullptr;
-  const int jrow = P.nx * (iy + ny * iz);
 #pragma unroll
   for (int i = 0; i < H; ++i) {
-    const int j = jrow + t + TT * i;  // ix < nx
-    int q;
-    if (P.io_full) {
-      q = j;
-      if (P.iocc[j] == 0) { y[q] = mk<C>(0, 0); continue; }
-    } else {
-      q = P.inv[j];
-      if (q < 0) continue;
+    const int j = jrow + t + TT * i;
+    const int q = qi[i];
+    if (q < 0) {
+      if (P.io_full) y[j] = mk<C>(0, 0);
+      continue;
     }
-    const int qa = P.a_full ? j : q;
-    C xc = x[(size_t)c * S + q];
+    int qa = q;
+    if (!chunked) qa = P.a_full ? j : P.inv[j];
+    C xc = chunked ? xs[q - q0] : x[(size_t)c * S + q];
+    const C av = chunked ? as[q - q0] : ad[qa];
     if (P.conj) xc.y = -xc.y;
-    C yv = csub(cmul(ad[qa], xc), cscale(v[i], P.inv_ngrid));
+    C yv = csub(cmul(av, xc), cscale(v[i], P.inv_ngrid));
     if (ao) {
       C x1 = x[q], x2 = x[S + q], x3 = x[2 * (size_t)S + q];
       if (P.conj) { x1.y = -x1.y; x2.y = -x2.y; x3.y = -x3.y; }
@@ -442,7 +514,7 @@ int matvec_xpipe(Engine<T>& E, const MvArgs<T>& a) {
   P.nat = g.nat; P.nat0 = g.nat0;
   P.x_rs = a.x_rs; P.y_rs = a.y_rs; P.a_rs = a.a_rs;
   P.io_full = a.io_full; P.a_full = a.a_full; P.conj = a.conj;
-  P.inv = E.inv; P.iocc = E.iocc; P.mask = a.mask;
+  P.inv = E.inv; P.iocc = E.iocc; P.rowq = E.rowq; P.mask = a.mask;
   P.A = E.zhat; P.A_rs = (size_t)3 * g.nz * g.Mx * g.ny;
   P.B = E.slab;
   P.green = E.green; P.ipbc = g.ipbc;
@@ -455,7 +527,9 @@ int matvec_xpipe(Engine<T>& E, const MvArgs<T>& a) {
   P.lsy = line_stride(g.My / TY, TY, RY, false);
   P.lsz = std::max(line_stride(g.Mz / TZ, TZ, RZ, false), g.Mz);
   // the transpose tile and the line scratch share one region
-  const size_t smx = ((size_t)g.Mx + std::max((size_t)g.Mx * (RX + 1), (size_t)RX * P.lsx)) * sizeof(C);
+  P.tlx = (int)std::max((size_t)g.Mx * (RX + 1), (size_t)RX * P.lsx);
+  const size_t smx = ((size_t)g.Mx + P.tlx) * sizeof(C);
+  const size_t smxi = smx + ((size_t)RX * g.nx <= (size_t)XI_STAGE_MAX ? (size_t)2 * RX * g.nx * sizeof(C) : 0);
   const size_t smy = ((size_t)g.My + std::max((size_t)g.My * (RY + 1), (size_t)RY * P.lsy)) * sizeof(C);
   P.my_log2 = 0;
   while ((1 << P.my_log2) < g.My) ++P.my_log2;
@@ -491,7 +565,7 @@ int matvec_xpipe(Engine<T>& E, const MvArgs<T>& a) {
           return 24;
       }
     }
-    if (xlaunch<T>(fxi, dim3((unsigned)ceil_div(g.ny, RX), (unsigned)g.nz, (unsigned)(3 * nr)), 256, smx, E.stream, P))
+    if (xlaunch<T>(fxi, dim3((unsigned)ceil_div(g.ny, RX), (unsigned)g.nz, (unsigned)(3 * nr)), 256, smxi, E.stream, P))
       return 25;
   }
   return 0;
