@@ -730,3 +730,17 @@ DDSCAT_CUDA_API int ddscat_b200_matvec_timing(int nrhs, int iters, int cwhat, fl
 }
 
 }  // extern "C"
+
+extern "C" DDSCAT_CUDA_API int ddscat_b200_mueller_f32(int ndir, const float* ak, const void* e01, const void* e02,
+                                                       const float* em2, const void* f11, const void* f21,
+                                                       const void* f12, const void* f22, void* s1234, double* smat) {
+  clear_error();
+  if (ndir <= 0 || !ak || !e01 || !e02 || !em2 || !f11 || !f21 || !f12 || !f22 || !smat) {
+    set_error("Mueller", "invalid argument");
+    return 700;
+  }
+  return mueller_compute(ndir, ak, static_cast<const float2*>(e01), static_cast<const float2*>(e02), em2,
+                         static_cast<const float2*>(f11), static_cast<const float2*>(f21),
+                         static_cast<const float2*>(f12), static_cast<const float2*>(f22),
+                         static_cast<float2*>(s1234), smat);
+}

@@ -206,6 +206,113 @@ int farfield_sums(Engine<T>& eng, const cplx<T>* p, const float* dirs_host, int 
   return rc;
 }
 
+// --------------------------------------------------------------------------
+// Amplitude matrix (S1..S4) and Mueller matrix (S_ij) per scattering direction,
+// the step DDSCAT's GETMUELLER performs after SCAT (not in the reference).
+// Definitions of Bohren & Huffman (1983), section 3.2 and eq. 3.16; f_ml as
+// ddscat_cuda_scat_f32 returns them (k times the physical amplitude), so
+// S = -i f.  DDSCAT's basis has EM2 = n x EM1 (phi-hat); Bohren & Huffman's
+// perpendicular vector is -EM2 for scattered and incident light, and
+// e_par,i = khat x e_perp,i.  With g_1l = f_1l and g_2l = -f_2l:
+//   S2 = -i sum_l g_1l conj(e0l).e_par   S3 = -i sum_l g_1l conj(e0l).e_perp
+//   S4 = -i sum_l g_2l conj(e0l).e_par   S1 = -i sum_l g_2l conj(e0l).e_perp
+struct MuellerIn {
+  double kh[3];
+  double2 e0c[2][3];  // conj(e01), conj(e02)
+};
+
+__device__ __forceinline__ double2 zmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__device__ __forceinline__ double2 zmulc(double2 a, double2 b) { return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y); }  // a conj(b)
+
+__global__ void k_mueller(int ndir, MuellerIn in, const float* em2, const float2* f11, const float2* f21,
+                          const float2* f12, const float2* f22, float2* s_out, double* m_out) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= ndir) return;
+  const double ep[3] = {-(double)em2[3 * d], -(double)em2[3 * d + 1], -(double)em2[3 * d + 2]};  // e_perp = -EM2
+  const double ea[3] = {in.kh[1] * ep[2] - in.kh[2] * ep[1], in.kh[2] * ep[0] - in.kh[0] * ep[2],
+                        in.kh[0] * ep[1] - in.kh[1] * ep[0]};
+  double2 cpar[2], cperp[2];
+  for (int l = 0; l < 2; ++l) {
+    cpar[l] = make_double2(0.0, 0.0);
+    cperp[l] = make_double2(0.0, 0.0);
+    for (int k = 0; k < 3; ++k) {
+      cpar[l].x += ea[k] * in.e0c[l][k].x; cpar[l].y += ea[k] * in.e0c[l][k].y;
+      cperp[l].x += ep[k] * in.e0c[l][k].x; cperp[l].y += ep[k] * in.e0c[l][k].y;
+    }
+  }
+  const double2 a11 = to_d(f11[d]), a12 = to_d(f12[d]);
+  const double2 a21 = make_double2(-(double)f21[d].x, -(double)f21[d].y);  // g_2l = -f_2l
+  const double2 a22 = make_double2(-(double)f22[d].x, -(double)f22[d].y);
+  auto mi = [](double2 z) { return make_double2(z.y, -z.x); };  // -i z
+  auto add = [](double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); };
+  const double2 S2 = mi(add(zmul(a11, cpar[0]), zmul(a12, cpar[1])));
+  const double2 S3 = mi(add(zmul(a11, cperp[0]), zmul(a12, cperp[1])));
+  const double2 S4 = mi(add(zmul(a21, cpar[0]), zmul(a22, cpar[1])));
+  const double2 S1 = mi(add(zmul(a21, cperp[0]), zmul(a22, cperp[1])));
+  if (s_out) {
+    s_out[4 * d] = make_float2((float)S1.x, (float)S1.y);
+    s_out[4 * d + 1] = make_float2((float)S2.x, (float)S2.y);
+    s_out[4 * d + 2] = make_float2((float)S3.x, (float)S3.y);
+    s_out[4 * d + 3] = make_float2((float)S4.x, (float)S4.y);
+  }
+  const double q1 = zabs2(S1), q2 = zabs2(S2), q3 = zabs2(S3), q4 = zabs2(S4);
+  const double2 s23 = zmulc(S2, S3), s14 = zmulc(S1, S4), s24 = zmulc(S2, S4), s13 = zmulc(S1, S3);
+  const double2 s12 = zmulc(S1, S2), s34 = zmulc(S3, S4);
+  double* M = m_out + (size_t)16 * d;
+  M[0] = 0.5 * (q2 + q1 + q4 + q3);
+  M[1] = 0.5 * (q2 - q1 + q4 - q3);
+  M[2] = s23.x + s14.x;
+  M[3] = s23.y - s14.y;
+  M[4] = 0.5 * (q2 - q1 - q4 + q3);
+  M[5] = 0.5 * (q2 + q1 - q4 - q3);
+  M[6] = s23.x - s14.x;
+  M[7] = s23.y + s14.y;
+  M[8] = s24.x + s13.x;
+  M[9] = s24.x - s13.x;
+  M[10] = s12.x + s34.x;
+  M[11] = -s12.y - s34.y;   // Im(S2 S1* + S4 S3*)
+  M[12] = -s24.y + s13.y;   // Im(S4 S2* + S1 S3*)
+  M[13] = -s24.y - s13.y;   // Im(S4 S2* - S1 S3*)
+  M[14] = s12.y - s34.y;    // Im(S1 S2* - S3 S4*)
+  M[15] = s12.x - s34.x;
+}
+
+int mueller_compute(int ndir, const float* ak, const float2* e01, const float2* e02, const float* em2,
+                    const float2* f11, const float2* f21, const float2* f12, const float2* f22, float2* s_out,
+                    double* m_out) {
+  MuellerIn in{};
+  const double kk = std::sqrt((double)ak[0] * ak[0] + (double)ak[1] * ak[1] + (double)ak[2] * ak[2]);
+  if (!(kk > 0.0)) { set_error("Mueller", "zero incident wave vector"); return 700; }
+  for (int k = 0; k < 3; ++k) {
+    in.kh[k] = ak[k] / kk;
+    in.e0c[0][k] = make_double2(e01[k].x, -e01[k].y);
+    in.e0c[1][k] = make_double2(e02[k].x, -e02[k].y);
+  }
+  const size_t off_f = ((size_t)ndir * 3 * sizeof(float) + 15) & ~(size_t)15;  // 16-byte aligned f block
+  const size_t nb = off_f + (size_t)ndir * (8 * sizeof(float2) + 16 * sizeof(double));
+  unsigned char* buf = nullptr;
+  cudaError_t e = cudaMalloc((void**)&buf, nb);
+  if (e != cudaSuccess) { set_cuda_error("Mueller workspace", e); return 701; }
+  float* d_em2 = reinterpret_cast<float*>(buf);
+  float2* d_f = reinterpret_cast<float2*>(buf + off_f);
+  float2* d_s = d_f + (size_t)4 * ndir;
+  double* d_m = reinterpret_cast<double*>(d_s + (size_t)4 * ndir);
+  const float2* hf[4] = {f11, f21, f12, f22};
+  e = cudaMemcpy(d_em2, em2, (size_t)ndir * 3 * sizeof(float), cudaMemcpyHostToDevice);
+  for (int k = 0; k < 4 && e == cudaSuccess; ++k)
+    e = cudaMemcpy(d_f + (size_t)k * ndir, hf[k], (size_t)ndir * sizeof(float2), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) { cudaFree(buf); set_cuda_error("Mueller H2D", e); return 702; }
+  k_mueller<<<(unsigned)ceil_div(ndir, 128), 128>>>(ndir, in, d_em2, d_f, d_f + ndir, d_f + 2 * (size_t)ndir,
+                                                    d_f + 3 * (size_t)ndir, d_s, d_m);
+  note_launch();
+  if (check_launch("Mueller kernel")) { cudaFree(buf); return 703; }
+  if (s_out) e = cudaMemcpy(s_out, d_s, (size_t)ndir * 4 * sizeof(float2), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(m_out, d_m, (size_t)ndir * 16 * sizeof(double), cudaMemcpyDeviceToHost);
+  cudaFree(buf);
+  if (e != cudaSuccess) { set_cuda_error("Mueller D2H", e); return 702; }
+  return 0;
+}
+
 template int evalq_compute<float>(Engine<float>&, VecOps<float>&, const float2*, const float2*, const float2*,
                                   const float2*, int, float2*, double, double2*, double2*);
 template int evalq_compute<double>(Engine<double>&, VecOps<double>&, const double2*, const double2*, const double2*,

@@ -46,4 +46,9 @@ template <typename T>
 int farfield_sums(Engine<T>& eng, const cplx<T>* p, const float* dirs_host, int ndir, const float dx[3], const float x0[3],
                   double2* sums_host, cudaStream_t s);
 
+// Amplitude and Mueller matrices per scattering direction from f_ml (host in / out).
+int mueller_compute(int ndir, const float* ak, const float2* e01, const float2* e02, const float* em2,
+                    const float2* f11, const float2* f21, const float2* f12, const float2* f22, float2* s_out,
+                    double* m_out);
+
 }  // namespace ddb

@@ -28,7 +28,7 @@ EXPORTS = (
     + ["ddscat_cuda_evalq_f32", "ddscat_cuda_scat_f32", "ddscat_cuda_release", "ddscat_cuda_last_error"]
     + ["ddscat_b200_set_verbose", "ddscat_b200_layout", "ddscat_b200_matvec_timing", "ddscat_b200_solve_batch_f32",
        "ddscat_b200_last_solve_stats", "ddscat_b200_residual_f64", "ddscat_b200_launch_count",
-       "ddscat_b200_apply_noalloc_f32"]
+       "ddscat_b200_apply_noalloc_f32", "ddscat_b200_mueller_f32"]
 )
 
 
@@ -87,6 +87,8 @@ def _declare(lib):
     lib.ddscat_b200_residual_f64.restype = _I
     lib.ddscat_b200_apply_noalloc_f32.argtypes = [_I, _P, _P, _P, _P, _P]
     lib.ddscat_b200_apply_noalloc_f32.restype = _I
+    lib.ddscat_b200_mueller_f32.argtypes = [_I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _D]
+    lib.ddscat_b200_mueller_f32.restype = _I
     lib.ddscat_b200_launch_count.argtypes = []
     lib.ddscat_b200_launch_count.restype = ct.c_ulonglong
 
@@ -275,6 +277,21 @@ class DDA:
         ms = _F(0.0)
         self._check("matvec_timing", self.lib.ddscat_b200_matvec_timing(nrhs, iters, ord(cwhat), ct.byref(ms)))
         return ms.value
+
+    def mueller(self, ak, e01, e02, em2, f11, f21, f12, f22):
+        """(S1..S4 per direction (ndir, 4) complex64, Mueller S_ij (ndir, 4, 4)) from
+        the f1/f2 outputs of scat() for the two incident polarisations."""
+        f = [_c64(v) for v in (f11, f21, f12, f22)]
+        ndir = f[0].size
+        akf = np.ascontiguousarray(ak, dtype=np.float32)
+        e1, e2 = _c64(e01, 3), _c64(e02, 3)
+        em2f = np.ascontiguousarray(em2, dtype=np.float32).reshape(ndir, 3)
+        s = np.zeros((ndir, 4), dtype=np.complex64)
+        m = np.zeros((ndir, 4, 4), dtype=np.float64)
+        rc = self.lib.ddscat_b200_mueller_f32(ndir, _ptr(akf), _ptr(e1), _ptr(e2), _ptr(em2f), *[_ptr(v) for v in f],
+                                              _ptr(s), m.ctypes.data_as(_D))
+        self._check("mueller", rc)
+        return s, m
 
     def launch_count(self):
         return int(self.lib.ddscat_b200_launch_count())

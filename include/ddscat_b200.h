@@ -92,6 +92,22 @@ DDSCAT_CUDA_API int ddscat_b200_residual_f64(int nrhs, const void *b, const void
 DDSCAT_CUDA_API int ddscat_b200_apply_noalloc_f32(int cwhat, const void *x, void *y, const void *adia,
                                                   const void *aoff, void *stream);
 
+/* Amplitude matrix (S1..S4) and 4x4 Mueller matrix S_ij per scattering
+ * direction, the step DDSCAT's GETMUELLER performs after SCAT (GETMUELLER is not
+ * part of the reference; this restates the definitions of Bohren & Huffman 1983,
+ * section 3.2 and eq. 3.16).  f11, f21 are the f1, f2 outputs of
+ * ddscat_cuda_scat_f32 for incident polarisation e01; f12, f22 those for e02
+ * (ndir complex floats each, same EM1/EM2 and AKS).  em2 (ndir x 3) is EM2 of
+ * the SCAT call, in DDSCAT's convention EM2 = n x EM1 (phi-hat when EM1 is
+ * theta-hat); Bohren & Huffman's perpendicular vector is -EM2, for incident and
+ * scattered light, and e_par,i = khat x e_perp,i.
+ * Outputs: s1234 (ndir x 4 complex floats S1, S2, S3, S4, may be NULL) and smat
+ * (ndir x 16 doubles, S_ij row-major).  Host pointers.  Codes: 700 invalid
+ * argument, 701 allocation, 702 transfer, 703 kernel launch. */
+DDSCAT_CUDA_API int ddscat_b200_mueller_f32(int ndir, const float *ak, const void *e01, const void *e02,
+                                            const float *em2, const void *f11, const void *f21, const void *f12,
+                                            const void *f22, void *s1234, double *smat);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1499,3 +1499,67 @@ def scat(p_c, occ, nx, ny, jpbc, ak, aks, dx, em1, em2, e02, etasca, e01, x0):
         out["f1"] = term * np.sum(em1 * s, axis=1)
         out["f2"] = term * np.sum(em2 * s, axis=1)
     return out
+
+
+# --------------------------------------------------------------------------
+# Amplitude and Mueller matrices (the S_ij step DDSCAT's GETMUELLER performs
+# after SCAT; GETMUELLER itself is not in the reference).  Restated from the
+# definitions of Bohren & Huffman (1983), "Absorption and Scattering of Light by
+# Small Particles", section 3.2 (amplitude matrix) and eq. 3.16 (Mueller
+# matrix), with DDSCAT's f_ml as the reference SCAT returns them: f_ml is the
+# amplitude along the scattered basis vector e_m (m = 1: EM1, m = 2: EM2) for
+# incident polarisation e0l (l = 1: E01, l = 2: E02), in the normalisation of
+# ddscat_cuda_scat_f32 (term = |k|^3/sqrt(E02), cu:994), i.e. k times the
+# physical scattering amplitude, so that S = -i f.
+
+def amplitude_matrix(ak, e01, e02, em2, f11, f21, f12, f22):
+    """S1..S4 per direction (ndir, 4) complex128, in the order (S1, S2, S3, S4).
+
+    EM1/EM2 are DDSCAT's scattered basis vectors as passed to SCAT, with
+    EM2 = n x EM1 (theta-hat and phi-hat).  Bohren & Huffman use e_par,s =
+    theta-hat and e_perp,s = -phi-hat = -EM2, and the same perpendicular vector
+    for the incident light, e_perp,i = -EM2, with e_par,i = khat x e_perp,i.
+    With a_l = conj(e0l) . E_inc the scattered field components are
+    E_par = sum_l f_1l a_l and E_perp = -sum_l f_2l a_l, so with g_1l = f_1l,
+    g_2l = -f_2l:
+      S2 = -i sum_l g_1l conj(e0l).e_par,i   S3 = -i sum_l g_1l conj(e0l).e_perp,i
+      S4 = -i sum_l g_2l conj(e0l).e_par,i   S1 = -i sum_l g_2l conj(e0l).e_perp,i
+    """
+    k = np.asarray(ak, dtype=np.float64)
+    khat = k / np.linalg.norm(k)
+    eperp = -np.asarray(em2, dtype=np.float64).reshape(-1, 3)
+    epar = np.cross(khat[None, :], eperp)
+    e0 = [np.conj(np.asarray(e01, dtype=np.complex128)), np.conj(np.asarray(e02, dtype=np.complex128))]
+    cpar = [epar @ e for e in e0]     # conj(e0l) . e_par,i
+    cperp = [eperp @ e for e in e0]   # conj(e0l) . e_perp,i
+    g1 = [np.asarray(f11, dtype=np.complex128), np.asarray(f12, dtype=np.complex128)]    # l = 1, 2
+    g2 = [-np.asarray(f21, dtype=np.complex128), -np.asarray(f22, dtype=np.complex128)]
+    S2 = -1j * (g1[0] * cpar[0] + g1[1] * cpar[1])
+    S3 = -1j * (g1[0] * cperp[0] + g1[1] * cperp[1])
+    S4 = -1j * (g2[0] * cpar[0] + g2[1] * cpar[1])
+    S1 = -1j * (g2[0] * cperp[0] + g2[1] * cperp[1])
+    return np.stack([S1, S2, S3, S4], axis=1)
+
+
+def mueller_from_amplitude(S):
+    """(ndir, 4, 4) Mueller matrix S_ij from (S1, S2, S3, S4), Bohren & Huffman eq. 3.16."""
+    S1, S2, S3, S4 = (S[:, k] for k in range(4))
+    a1, a2, a3, a4 = (np.abs(s) ** 2 for s in (S1, S2, S3, S4))
+    M = np.empty((S.shape[0], 4, 4))
+    M[:, 0, 0] = 0.5 * (a2 + a1 + a4 + a3)
+    M[:, 0, 1] = 0.5 * (a2 - a1 + a4 - a3)
+    M[:, 0, 2] = np.real(S2 * np.conj(S3) + S1 * np.conj(S4))
+    M[:, 0, 3] = np.imag(S2 * np.conj(S3) - S1 * np.conj(S4))
+    M[:, 1, 0] = 0.5 * (a2 - a1 - a4 + a3)
+    M[:, 1, 1] = 0.5 * (a2 + a1 - a4 - a3)
+    M[:, 1, 2] = np.real(S2 * np.conj(S3) - S1 * np.conj(S4))
+    M[:, 1, 3] = np.imag(S2 * np.conj(S3) + S1 * np.conj(S4))
+    M[:, 2, 0] = np.real(S2 * np.conj(S4) + S1 * np.conj(S3))
+    M[:, 2, 1] = np.real(S2 * np.conj(S4) - S1 * np.conj(S3))
+    M[:, 2, 2] = np.real(S1 * np.conj(S2) + S3 * np.conj(S4))
+    M[:, 2, 3] = np.imag(S2 * np.conj(S1) + S4 * np.conj(S3))
+    M[:, 3, 0] = np.imag(S4 * np.conj(S2) + S1 * np.conj(S3))
+    M[:, 3, 1] = np.imag(S4 * np.conj(S2) - S1 * np.conj(S3))
+    M[:, 3, 2] = np.imag(S1 * np.conj(S2) - S3 * np.conj(S4))
+    M[:, 3, 3] = np.real(S1 * np.conj(S2) - S3 * np.conj(S4))
+    return M

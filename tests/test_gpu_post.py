@@ -87,3 +87,66 @@ def test_energy_conservation_on_gpu():
     sc = dda.scat(k, prob.incid[0].e, prob.x0, etasca=0.2)
     assert cext == pytest.approx(cabs + sc["csca"], rel=3e-3)
     dda.release()
+
+
+def _plane_dirs(kk, phi, th_deg):
+    """Scattering directions for incidence along x in the plane at azimuth phi,
+    with DDSCAT's basis EM1 = theta-hat, EM2 = n x EM1 (= phi-hat)."""
+    aks, em1, em2 = [], [], []
+    for t in np.deg2rad(th_deg):
+        n = np.array([math.cos(t), math.sin(t) * math.cos(phi), math.sin(t) * math.sin(phi)])
+        e1 = np.array([-math.sin(t), math.cos(t) * math.cos(phi), math.cos(t) * math.sin(phi)])
+        aks.append(kk * n)
+        em1.append(e1)
+        em2.append(np.cross(n, e1))
+    return (np.array(a, dtype=np.float32) for a in (aks, em1, em2))
+
+
+@pytest.mark.gpu
+def test_mueller_matches_oracle():
+    rng = np.random.default_rng(17)
+    nd = 200
+    k = np.array([0.7, 0.2, -0.3])
+    e01 = np.array([0.1 + 0.2j, 0.9, 0.3j])
+    e01 /= np.linalg.norm(e01)
+    e02 = np.cross(k / np.linalg.norm(k), np.conj(e01))
+    em2 = rng.normal(size=(nd, 3)).astype(np.float32)
+    f = [(rng.normal(size=nd) + 1j * rng.normal(size=nd)).astype(np.complex64) for _ in range(4)]
+    dda = D.DDA()
+    s, m = dda.mueller(k, e01, e02, em2, *f)
+    sref = O.amplitude_matrix(k.astype(np.float32), e01.astype(np.complex64), e02.astype(np.complex64), em2, *f)
+    mref = O.mueller_from_amplitude(sref)
+    assert np.abs(s - sref).max() <= 1e-5 * np.abs(sref).max()
+    assert np.abs(m - mref).max() <= 1e-5 * np.abs(mref).max()
+
+
+@pytest.mark.gpu
+def test_mueller_of_dda_sphere():
+    """S_ij of a solved DDA sphere in its mirror plane (incidence along x,
+    scattering plane x-y): S3 = S4 = 0 by symmetry, so the off-block elements
+    vanish, S11 = S22, S33 = S44, S12 = S21, S34 = -S43; forward, S33 = S11 and
+    S12 = 0; and sum_ij S_ij^2 = 4 S11^2 (a pure Mueller matrix)."""
+    n = 16
+    prob = targets.make_problem(n, m=1.33 + 0.05j, x=2.5)
+    dda = D.DDA()
+    dda.prepare_green(n, n, n, prob.iocc, prob.incid[0].k)
+    k = prob.incid[0].k
+    aks, em1, em2 = _plane_dirs(np.linalg.norm(k), 0.0, np.arange(0, 181, 5.0))
+    f = {}
+    for l in (0, 1):
+        inc = prob.incid[l]
+        dda.solve("qmrccg", prob.rhs(l), prob.adia(l), prob.aoff(), maxit=500, tol=1e-6)
+        sc = dda.scat(k, inc.e, prob.x0, etasca=3.0, aks=aks, em1=em1, em2=em2)
+        f[l] = (sc["f1"], sc["f2"])
+    s, m = dda.mueller(k, prob.incid[0].e, prob.incid[1].e, em2, f[0][0], f[0][1], f[1][0], f[1][1])
+    s11 = m[:, 0, 0]
+    assert np.all(s11 > 0)
+    for i, j in [(0, 2), (0, 3), (1, 2), (1, 3), (2, 0), (2, 1), (3, 0), (3, 1)]:
+        assert np.abs(m[:, i, j]).max() <= 1e-4 * s11.max(), (i, j)
+    assert np.allclose(m[:, 1, 1], s11, rtol=1e-4, atol=1e-6 * s11.max())
+    assert np.allclose(m[:, 3, 3], m[:, 2, 2], rtol=1e-4, atol=1e-6 * s11.max())
+    assert np.allclose(m[:, 0, 1], m[:, 1, 0], atol=1e-6 * s11.max())
+    assert np.allclose(m[:, 2, 3], -m[:, 3, 2], atol=1e-6 * s11.max())
+    assert abs(m[0, 2, 2] - s11[0]) <= 1e-4 * s11[0] and abs(m[0, 0, 1]) <= 1e-4 * s11[0]
+    assert np.allclose(np.sum(m ** 2, axis=(1, 2)), 4 * s11 ** 2, rtol=1e-5)
+    dda.release()

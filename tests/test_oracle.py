@@ -166,3 +166,36 @@ def test_optical_theorem():
     cabs, cext, _ = O.evalq(b, res.x, adia, aoff, ak, 1.0)
     sc = O.scat(res.x, op.occ, prob.nx, prob.ny, 0, ak, [], (1, 1, 1), [], [], 1.0, 0.2, prob.incid[0].e, prob.x0)
     assert cext == pytest.approx(cabs + sc["csca"], rel=2e-3)
+
+
+def test_mueller_identities():
+    """Bohren & Huffman eq. 3.16 from a single amplitude matrix: the Mueller
+    matrix is 'pure', so sum_ij S_ij^2 = 4 S_11^2; with S3 = S4 = 0 (sphere)
+    the off-block elements vanish, S11 = S22, S33 = S44, S12 = S21, S34 = -S43."""
+    rng = np.random.default_rng(3)
+    S = rng.normal(size=(50, 4)) + 1j * rng.normal(size=(50, 4))
+    M = O.mueller_from_amplitude(S)
+    assert np.allclose(np.sum(M ** 2, axis=(1, 2)), 4 * M[:, 0, 0] ** 2, rtol=1e-12)
+    S[:, 2:] = 0
+    M = O.mueller_from_amplitude(S)
+    for i, j in [(0, 2), (0, 3), (1, 2), (1, 3), (2, 0), (2, 1), (3, 0), (3, 1)]:
+        assert np.allclose(M[:, i, j], 0)
+    assert np.allclose(M[:, 0, 0], M[:, 1, 1]) and np.allclose(M[:, 2, 2], M[:, 3, 3])
+    assert np.allclose(M[:, 0, 1], M[:, 1, 0]) and np.allclose(M[:, 2, 3], -M[:, 3, 2])
+
+
+def test_amplitude_matrix_forward_direction():
+    """Forward scattering by an isotropic scatterer keeps the incident
+    polarisation, f_ml = f0 (e_m . e0l), so S1 = S2 = -i f0 and S3 = S4 = 0
+    for any azimuth of the scattering plane (DDSCAT basis EM2 = n x EM1)."""
+    k = np.array([2.0, 0.0, 0.0])
+    e01 = np.array([0, 1, 0], dtype=complex)
+    e02 = np.array([0, 0, 1], dtype=complex)
+    f0 = 0.3 - 0.7j
+    for phi in np.linspace(0, np.pi, 5):
+        em1 = np.array([0.0, np.cos(phi), np.sin(phi)])  # theta-hat at theta = 0
+        em2 = np.cross(k / 2, em1)
+        f = [[f0 * np.dot(em, e) for e in (e01, e02)] for em in (em1, em2)]
+        S = O.amplitude_matrix(k, e01, e02, em2[None, :], [f[0][0]], [f[1][0]], [f[0][1]], [f[1][1]])
+        assert np.allclose(S[0, 0], S[0, 1]) and np.allclose(S[0, 2:], 0)
+        assert np.allclose(S[0, 0], -1j * f0)
