@@ -343,6 +343,9 @@ static int ensure_f64() {
 // access for entry points defined in other translation units).
 const Engine<float>* prepared_engine() { return s.ready ? &s.eng : nullptr; }
 
+int make_inputs(const Engine<float>& eng, int nrhs, const float* k, const float2* e0, const float* x0, int nmat,
+                const float2* mref, const int16_t* icomp_host, float2* b, float2* adia, cudaStream_t st);
+
 }  // namespace ddb
 
 using namespace ddb;
@@ -743,4 +746,40 @@ extern "C" DDSCAT_CUDA_API int ddscat_b200_mueller_f32(int ndir, const float* ak
                          static_cast<const float2*>(f11), static_cast<const float2*>(f21),
                          static_cast<const float2*>(f12), static_cast<const float2*>(f22),
                          static_cast<float2*>(s1234), smat);
+}
+
+extern "C" DDSCAT_CUDA_API int ddscat_b200_make_inputs_f32(int nrhs, const float* k, const void* e0, const float* x0,
+                                                           int nmat, const void* m, const int16_t* icomp, void* b,
+                                                           void* adia) {
+  clear_error();
+  if (!s.ready || nrhs <= 0 || nmat <= 0 || !k || !e0 || !x0 || !m || (!b && !adia)) {
+    set_error("make_inputs", "invalid argument or not prepared");
+    return 610;
+  }
+  const bool dev = is_device_ptr(b ? b : adia);
+  if ((b && is_device_ptr(b) != dev) || (adia && is_device_ptr(adia) != dev)) {
+    set_error("make_inputs", "b and adia must both be host or both be device pointers");
+    return 610;
+  }
+  const size_t full = (size_t)3 * s.eng.g.nat;
+  float2 *db = static_cast<float2*>(b), *da = static_cast<float2*>(adia);
+  float2* tmp = nullptr;
+  if (!dev) {
+    const size_t per = (size_t)nrhs * full;
+    cudaError_t e = cudaMalloc((void**)&tmp, per * sizeof(float2) * ((b ? 1 : 0) + (adia ? 1 : 0)));
+    if (e != cudaSuccess) { set_cuda_error("make_inputs staging", e); return 612; }
+    db = b ? tmp : nullptr;
+    da = adia ? tmp + (b ? per : 0) : nullptr;
+  }
+  int rc = make_inputs(s.eng, nrhs, k, static_cast<const float2*>(e0), x0, nmat, static_cast<const float2*>(m),
+                       icomp, db, da, s.stream);
+  if (!rc && !dev) {
+    const size_t bytes = (size_t)nrhs * full * sizeof(float2);
+    cudaError_t e = cudaSuccess;
+    if (b) e = cudaMemcpy(b, db, bytes, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && adia) e = cudaMemcpy(adia, da, bytes, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) { set_cuda_error("make_inputs D2H", e); rc = 612; }
+  }
+  cudaFree(tmp);
+  return rc;
 }

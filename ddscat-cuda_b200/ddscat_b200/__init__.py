@@ -28,7 +28,7 @@ EXPORTS = (
     + ["ddscat_cuda_evalq_f32", "ddscat_cuda_scat_f32", "ddscat_cuda_release", "ddscat_cuda_last_error"]
     + ["ddscat_b200_set_verbose", "ddscat_b200_layout", "ddscat_b200_matvec_timing", "ddscat_b200_solve_batch_f32",
        "ddscat_b200_last_solve_stats", "ddscat_b200_residual_f64", "ddscat_b200_launch_count",
-       "ddscat_b200_apply_noalloc_f32", "ddscat_b200_mueller_f32"]
+       "ddscat_b200_apply_noalloc_f32", "ddscat_b200_mueller_f32", "ddscat_b200_make_inputs_f32"]
 )
 
 
@@ -89,6 +89,8 @@ def _declare(lib):
     lib.ddscat_b200_apply_noalloc_f32.restype = _I
     lib.ddscat_b200_mueller_f32.argtypes = [_I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _D]
     lib.ddscat_b200_mueller_f32.restype = _I
+    lib.ddscat_b200_make_inputs_f32.argtypes = [_I, _P, _P, _P, _I, _P, _P, _P, _P]
+    lib.ddscat_b200_make_inputs_f32.restype = _I
     lib.ddscat_b200_launch_count.argtypes = []
     lib.ddscat_b200_launch_count.restype = ct.c_ulonglong
 
@@ -277,6 +279,26 @@ class DDA:
         ms = _F(0.0)
         self._check("matvec_timing", self.lib.ddscat_b200_matvec_timing(nrhs, iters, ord(cwhat), ct.byref(ms)))
         return ms.value
+
+    def make_inputs(self, ks, es, x0, m, icomp=None, b=None, adia=None):
+        """b and CXADIA (nrhs, 3*NAT) for wave vectors ks (nrhs, 3) and
+        polarisations es (nrhs, 3) on the GPU.  m: refractive index or list of
+        them; icomp: NAT material indices (1-based, 0 vacuum) or None.  b / adia:
+        optional preallocated outputs (NumPy arrays or CUDA tensors); NumPy
+        arrays are returned when none are given."""
+        kf = np.ascontiguousarray(ks, dtype=np.float32).reshape(-1, 3)
+        nrhs = kf.shape[0]
+        ef = _c64(es, 3 * nrhs)
+        x0f = np.ascontiguousarray(x0, dtype=np.float32)
+        mf = _c64(np.atleast_1d(m))
+        ic = None if icomp is None else np.ascontiguousarray(icomp, dtype=np.int16)
+        if b is None and adia is None:
+            b = np.zeros((nrhs, 3 * self.nat), dtype=np.complex64)
+            adia = np.zeros_like(b)
+        rc = self.lib.ddscat_b200_make_inputs_f32(nrhs, _ptr(kf), _ptr(ef), _ptr(x0f), int(mf.size), _ptr(mf),
+                                                  _ptr(ic), _vptr(b), _vptr(adia))
+        self._check("make_inputs", rc)
+        return b, adia
 
     def mueller(self, ak, e01, e02, em2, f11, f21, f12, f22):
         """(S1..S4 per direction (ndir, 4) complex64, Mueller S_ij (ndir, 4, 4)) from

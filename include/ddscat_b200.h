@@ -108,6 +108,21 @@ DDSCAT_CUDA_API int ddscat_b200_mueller_f32(int ndir, const float *ak, const voi
                                             const float *em2, const void *f11, const void *f21, const void *f12,
                                             const void *f22, void *s1234, double *smat);
 
+/* Right-hand sides and CXADIA for nrhs incident waves, generated on the GPU
+ * for the prepared target (DDSCAT computes them on the host in EVALE and
+ * ALPHADIAG; no counterpart in the reference ABI).  k: nrhs x 3 wave vectors in
+ * lattice units; e0: nrhs x 3 complex polarisations; x0: the SCAT origin
+ * offset (r_j = (ix+1, iy+1, iz+1) + x0); m: nmat complex refractive indices;
+ * icomp: NAT material indices 1..nmat (0 = vacuum) or NULL for material 1 on
+ * every occupied site.  Writes b = e0 exp(i k.r_j) on occupied sites (0 on
+ * vacuum) and adia = 1/alpha_LDR (Draine & Goodman 1993) of each site's
+ * material, as nrhs full vectors (3*NAT complex floats each, the input layout
+ * of ddscat_b200_solve_batch_f32); either output may be NULL; both host or both
+ * device pointers.  Codes: 610 invalid argument / not prepared, 611 material
+ * index out of range, 612 allocation or transfer, 613 kernel failure. */
+DDSCAT_CUDA_API int ddscat_b200_make_inputs_f32(int nrhs, const float *k, const void *e0, const float *x0, int nmat,
+                                                const void *m, const int16_t *icomp, void *b, void *adia);
+
 #ifdef __cplusplus
 }
 #endif
