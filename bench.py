@@ -58,6 +58,7 @@ def parse_args():
                          "reference's two-product form")
     ap.add_argument("--ref-rhs", type=int, default=0, help="RHS per step of the reference arm (0: the whole batch)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-q-check", action="store_true", help="skip the all-FP64 reference solve and Q errors")
     return ap.parse_args()
 
 
@@ -355,6 +356,34 @@ def run_ours(args):
     h2d = R * vec * 3  # b, x0 and CXADIA
     d2h = R * vec      # x
 
+    # Q errors of the FP32 solutions against the same batch solved all-FP64 on
+    # the GPU (outside the timed regions; every rank checks its own batch)
+    qerr = None
+    if not args.no_q_check:
+        nat = prob.nat
+        occ = prob.occ
+
+        def compact(v):
+            return np.concatenate([v[c * nat:(c + 1) * nat][occ] for c in range(3)])
+
+        x32 = xd.cpu().numpy()
+        x64 = np.zeros(b.shape, dtype=np.complex128)
+        o64 = dda.solve_batch_f64(args.solver, b, x64, adia, None, maxit=args.maxit, tol=1e-8,
+                                  replace=args.policy == "replace",
+                                  symmetric=args.solver == "qmrccg" and args.qmr_form == "symmetric")
+        worst = {"cabs": 0.0, "cext": 0.0, "cpha": 0.0}
+        zero = np.zeros(3 * prob.nat0, dtype=np.complex64)
+        for r in range(R):
+            k = prob.incid[r].k
+            ec, ac = compact(b[r]), compact(adia[r])
+            q32 = dda.evalq(k, use_resident=0, e=ec, p=compact(x32[r]), adia=ac, aoff=zero)
+            q64 = dda.evalq(k, use_resident=0, e=ec, p=compact(x64[r]).astype(np.complex64), adia=ac, aoff=zero)
+            for key, a, c in zip(("cabs", "cext", "cpha"), q32, q64):
+                worst[key] = max(worst[key], abs(a - c) / max(abs(c), 1e-300))
+        qerr = {"cabs_max_rel": worst["cabs"], "cext_max_rel": worst["cext"], "cpha_max_rel": worst["cpha"],
+                "rhs": R, "fp64_solve": f"{args.solver.upper()} all-FP64 on the GPU, tol 1e-8",
+                "fp64_iterations_mean": float(np.mean(o64.itno))}
+
     if rank == 0:
         ncm = float(np.mean(stats["ncompte"]))
         rhs_per_call = mv_stats[1] / max(mv_stats[2], 1)
@@ -384,6 +413,7 @@ def run_ours(args):
             "e2e": {"value": total_rhs / e2e_elapsed, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches, "clocks": clk,
+            "q_error_vs_fp64": qerr,
         }
         print(json.dumps(line), flush=True)
     dda.release()

@@ -90,8 +90,22 @@ static void release_f64() {
   f64 = F64State{};
 }
 
+// all-FP64 batched solve (complex128 vectors, FP64 engine)
+struct Batch64 {
+  int R = 0, cap = 0, n = 0;
+  double2 *b = nullptr, *x = nullptr, *adia = nullptr, *aoff = nullptr, *work = nullptr, *full = nullptr;
+  BatchOps<double> ops;
+};
+static Batch64 b64;
+static void release_b64() {
+  cudaFree(b64.b); cudaFree(b64.x); cudaFree(b64.adia); cudaFree(b64.aoff); cudaFree(b64.work); cudaFree(b64.full);
+  b64.ops.release();
+  b64 = Batch64{};
+}
+
 static void release_state() {
   release_batch();
+  release_b64();
   release_f64();
   delete[] s.h_iocc;
   s.h_iocc = nullptr;
@@ -338,6 +352,48 @@ static int ensure_f64() {
   return 0;
 }
 
+
+static int ensure_b64(int R) {
+  const int n = 3 * s.eng.g.nat0;
+  if (b64.n == n && b64.cap >= R && b64.work) {
+    if (b64.R != R) {
+      b64.ops.release();
+      if (b64.ops.init(R, n, s.stream)) return 1;
+      b64.R = R;
+    }
+    return 0;
+  }
+  release_b64();
+  const size_t v = (size_t)R * n;
+  cudaError_t e = cudaMalloc((void**)&b64.b, v * sizeof(double2));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&b64.x, v * sizeof(double2));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&b64.adia, v * sizeof(double2));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&b64.aoff, v * sizeof(double2));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&b64.work, (size_t)BATCH_WORK_VECTORS * v * sizeof(double2));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&b64.full, (size_t)3 * s.eng.g.nat * sizeof(double2));
+  if (e != cudaSuccess) { release_b64(); set_cuda_error("FP64 batched solve workspace", e); return 1; }
+  if (b64.ops.init(R, n, s.stream)) { release_b64(); return 1; }
+  b64.R = R;
+  b64.cap = R;
+  b64.n = n;
+  return 0;
+}
+
+// complex-float full RHS r (host or device) -> complex-double compact slot
+static int widen_to_compact(const void* src, bool dev, int r, double2* dst) {
+  const size_t full = (size_t)3 * s.eng.g.nat, cn = (size_t)3 * s.eng.g.nat0;
+  const C* f = (const C*)src + (size_t)r * full;
+  if (!dev) {
+    cudaError_t e = cudaMemcpyAsync(s.d_xf, f, full * sizeof(C), cudaMemcpyHostToDevice, s.stream);
+    if (e != cudaSuccess) { set_cuda_error("FP64 batched solve H2D", e); return 1; }
+    f = s.d_xf;
+  }
+  v_gather<float>(f, s.d_sy, s.eng.occ, s.eng.g.nat, s.eng.g.nat0, s.stream);
+  const unsigned gb = (unsigned)std::min<size_t>(ceil_div(cn, 256), 148 * 16);
+  k_to_f64<C><<<gb, 256, 0, s.stream>>>(s.d_sy, dst, cn);
+  note_launch();
+  return check_launch("FP64 batched solve widen");
+}
 
 // The prepared FP32 engine, or null before a successful prepare (read-only
 // access for entry points defined in other translation units).
@@ -782,4 +838,78 @@ extern "C" DDSCAT_CUDA_API int ddscat_b200_make_inputs_f32(int nrhs, const float
   }
   cudaFree(tmp);
   return rc;
+}
+
+extern "C" DDSCAT_CUDA_API int ddscat_b200_solve_batch_f64(int solver, int nrhs, const void* b, void* x,
+                                                           const void* adia, const void* aoff, int maxit, double tol,
+                                                           int* itno, double* tole, int* ncompte, int* status) {
+  clear_error();
+  if (!s.ready || nrhs <= 0 || !b || !x || !adia || maxit <= 0 || !(tol > 0.0) || !itno || !tole || !ncompte ||
+      !status) {
+    set_error("FP64 batched solve", "invalid argument or not prepared");
+    return 520;
+  }
+  const int replace = (solver & DDSCAT_B200_REPLACE_RESIDUAL) != 0;
+  const int sym = (solver & DDSCAT_B200_QMR_SYMMETRIC) != 0;
+  solver &= ~(DDSCAT_B200_REPLACE_RESIDUAL | DDSCAT_B200_QMR_SYMMETRIC);
+  if ((solver != DDSCAT_B200_QMRCCG && solver != DDSCAT_B200_PBCGS2) || (sym && solver != DDSCAT_B200_QMRCCG)) {
+    set_error("FP64 batched solve", "unsupported solver or flag");
+    return 521;
+  }
+  const bool dev = is_device_ptr(b);
+  if (is_device_ptr(x) != dev || is_device_ptr(adia) != dev || (aoff && is_device_ptr(aoff) != dev)) {
+    set_error("FP64 batched solve", "b, x, adia, aoff must all be host or all be device pointers");
+    return 522;
+  }
+  if (ensure_f64() || ensure_b64(nrhs)) return 523;
+  const size_t full = (size_t)3 * s.eng.g.nat;
+  for (int r = 0; r < nrhs; ++r) {
+    if (widen_to_compact(b, dev, r, b64.b + (size_t)r * b64.n) ||
+        widen_to_compact(adia, dev, r, b64.adia + (size_t)r * b64.n) ||
+        (aoff && widen_to_compact(aoff, dev, r, b64.aoff + (size_t)r * b64.n)))
+      return 524;
+    const double2* xf = (const double2*)x + (size_t)r * full;
+    if (!dev) {
+      cudaError_t e = cudaMemcpyAsync(b64.full, xf, full * sizeof(double2), cudaMemcpyHostToDevice, s.stream);
+      if (e != cudaSuccess) { set_cuda_error("FP64 batched solve H2D", e); return 524; }
+      xf = b64.full;
+    }
+    v_gather<double>(xf, b64.x + (size_t)r * b64.n, s.eng.occ, s.eng.g.nat, s.eng.g.nat0, s.stream);
+    if (check_launch("FP64 batched solve gather")) return 524;
+  }
+  BatchIO<double> io;
+  io.eng = &f64.eng; io.ops = &b64.ops; io.R = nrhs; io.n = b64.n;
+  io.b = b64.b; io.x = b64.x; io.adia = b64.adia; io.aoff = aoff ? b64.aoff : nullptr;
+  io.work = b64.work; io.nwork = BATCH_WORK_VECTORS;
+  io.maxit = maxit; io.tol = tol; io.verbose = s.verbose; io.replace = replace; io.sym = sym;
+  BatchResult res;
+  const int rc = solver == DDSCAT_B200_QMRCCG ? solve_batch_qmrccg<double>(io, res) : solve_batch_pbcgs2<double>(io, res);
+  if (rc) return rc == 1 ? 525 : rc;
+  for (int r = 0; r < nrhs; ++r) {
+    double2* dst = dev ? (double2*)x + (size_t)r * full : b64.full;
+    cudaError_t e = cudaMemsetAsync(dst, 0, full * sizeof(double2), s.stream);
+    if (e != cudaSuccess) { set_cuda_error("FP64 batched solve output", e); return 526; }
+    v_scatter<double>(b64.x + (size_t)r * b64.n, dst, s.eng.occ, s.eng.g.nat, s.eng.g.nat0, s.stream);
+    if (check_launch("FP64 batched solve scatter")) return 526;
+    if (!dev) {
+      e = cudaMemcpyAsync((double2*)x + (size_t)r * full, b64.full, full * sizeof(double2), cudaMemcpyDeviceToHost,
+                          s.stream);
+      if (e != cudaSuccess) { set_cuda_error("FP64 batched solve D2H", e); return 526; }
+    }
+  }
+  cudaError_t e = cudaStreamSynchronize(s.stream);
+  if (e != cudaSuccess) { set_cuda_error("FP64 batched solve", e); return 526; }
+  int worst = 0;
+  for (int r = 0; r < nrhs; ++r) {
+    itno[r] = res.itno[r];
+    tole[r] = res.tole[r];
+    ncompte[r] = res.ncompte[r];
+    status[r] = res.status[r];
+    if (res.status[r] && !worst) worst = res.status[r];
+  }
+  if (worst) {
+    set_error("FP64 batched solve", "at least one right-hand side stopped on a breakdown (see status)");
+    return worst;
+  }
+  return 0;
 }

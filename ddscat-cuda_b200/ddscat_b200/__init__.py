@@ -28,7 +28,8 @@ EXPORTS = (
     + ["ddscat_cuda_evalq_f32", "ddscat_cuda_scat_f32", "ddscat_cuda_release", "ddscat_cuda_last_error"]
     + ["ddscat_b200_set_verbose", "ddscat_b200_layout", "ddscat_b200_matvec_timing", "ddscat_b200_solve_batch_f32",
        "ddscat_b200_last_solve_stats", "ddscat_b200_residual_f64", "ddscat_b200_launch_count",
-       "ddscat_b200_apply_noalloc_f32", "ddscat_b200_mueller_f32", "ddscat_b200_make_inputs_f32"]
+       "ddscat_b200_apply_noalloc_f32", "ddscat_b200_mueller_f32", "ddscat_b200_make_inputs_f32",
+       "ddscat_b200_solve_batch_f64"]
 )
 
 
@@ -47,6 +48,7 @@ _P = ct.c_void_p
 _I = ct.c_int
 _F = ct.c_float
 _D = ct.POINTER(ct.c_double)
+_D2 = ct.c_double
 
 
 def _declare(lib):
@@ -91,6 +93,8 @@ def _declare(lib):
     lib.ddscat_b200_mueller_f32.restype = _I
     lib.ddscat_b200_make_inputs_f32.argtypes = [_I, _P, _P, _P, _I, _P, _P, _P, _P]
     lib.ddscat_b200_make_inputs_f32.restype = _I
+    lib.ddscat_b200_solve_batch_f64.argtypes = [_I, _I, _P, _P, _P, _P, _I, _D2, _P, _P, _P, _P]
+    lib.ddscat_b200_solve_batch_f64.restype = _I
     lib.ddscat_b200_launch_count.argtypes = []
     lib.ddscat_b200_launch_count.restype = ct.c_ulonglong
 
@@ -260,6 +264,24 @@ class DDA:
                                                   _vptr(aoff), maxit, tol, _ptr(it), _ptr(tole), _ptr(nc), _ptr(st))
         if check:
             self._check("solve_batch", rc)
+        return BatchOut(rc, it, tole, nc, st)
+
+    def solve_batch_f64(self, name, b, x, adia, aoff=None, maxit=1000, tol=1e-9, check=True, replace=False,
+                        symmetric=False):
+        """All-FP64 batched solve; b, adia, aoff complex64 (nrhs, 3*NAT), x
+        complex128 (nrhs, 3*NAT) in/out; NumPy arrays or CUDA tensors."""
+        nrhs = int(b.shape[0])
+        if not hasattr(x, "data_ptr") and (x.dtype != np.complex128 or not x.flags.c_contiguous):
+            raise ValueError("x must be a C-contiguous complex128 array")
+        it = np.zeros(nrhs, dtype=np.int32)
+        tole = np.zeros(nrhs, dtype=np.float64)
+        nc = np.zeros(nrhs, dtype=np.int32)
+        st = np.zeros(nrhs, dtype=np.int32)
+        code = BATCH_SOLVERS[name] | (REPLACE_RESIDUAL if replace else 0) | (QMR_SYMMETRIC if symmetric else 0)
+        rc = self.lib.ddscat_b200_solve_batch_f64(code, nrhs, _vptr(b), _vptr(x), _vptr(adia), _vptr(aoff), maxit,
+                                                  float(tol), _ptr(it), _ptr(tole), _ptr(nc), _ptr(st))
+        if check:
+            self._check("solve_batch_f64", rc)
         return BatchOut(rc, it, tole, nc, st)
 
     def last_solve_stats(self):

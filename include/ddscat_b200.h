@@ -123,6 +123,20 @@ DDSCAT_CUDA_API int ddscat_b200_mueller_f32(int ndir, const float *ak, const voi
 DDSCAT_CUDA_API int ddscat_b200_make_inputs_f32(int nrhs, const float *k, const void *e0, const float *x0, int nmat,
                                                 const void *m, const int16_t *icomp, void *b, void *adia);
 
+/* All-FP64 batched solve: the recurrence of ddscat_b200_solve_batch_f32 (same
+ * solver codes and flags) with complex-double vectors, an FP64 Green tensor and
+ * FP64 FFTs, as the reference solution against which FP32 results (Q values,
+ * residuals) are checked.  b, adia, aoff: nrhs complex-float full vectors (as
+ * for the FP32 entry point, widened on the GPU); x: nrhs complex-DOUBLE full
+ * vectors, initial guess in, solution out; all host or all device pointers.
+ * tole is the achieved true relative residual.  Codes: 520 invalid argument /
+ * not prepared, 521 solver or flag, 522 mixed pointer kinds, 523 workspace,
+ * 524 input transfer, 525 solver failure, 526 output transfer; a breakdown of
+ * any RHS returns that RHS's status code. */
+DDSCAT_CUDA_API int ddscat_b200_solve_batch_f64(int solver, int nrhs, const void *b, void *x, const void *adia,
+                                                const void *aoff, int maxit, double tol, int *itno, double *tole,
+                                                int *ncompte, int *status);
+
 #ifdef __cplusplus
 }
 #endif
