@@ -1,0 +1,99 @@
+"""The small configurations at their full sizes (seeded synthetic inputs with
+the shapes the configurations name).
+
+C1: sphere on a 32^3 lattice, m = 1.50+0.01i, x = 5, one orientation, two
+    polarisations, PBCGS2 at tol 1e-5; Q values against the all-FP64 GPU solve
+    (<= 1e-4), Cext = Cabs + Csca, and S_ij on 0..180 deg at 1 deg in two
+    scattering planes (physical symmetries of a sphere in its mirror planes).
+C3: triaxial ellipsoid 1 : 0.8 : 0.6 on a 64^3 lattice, m = 1.60+0.02i, x = 12,
+    64 orientations uniform on SO(3) from seed 0 x 2 polarisations = 128 RHS in
+    one batched PBCGS2 solve at tol 1e-5 (inputs generated on the GPU); every
+    RHS passes the FP64 residual check and a sample matches single-RHS solves."""
+import math
+
+import numpy as np
+import pytest
+
+import ddscat_b200 as D
+from ddscat_b200 import targets
+from oracle import ddscat_oracle as O
+
+TOL = 1e-5
+
+
+def _compact(v, prob):
+    return np.concatenate([v[c * prob.nat:(c + 1) * prob.nat][prob.occ] for c in range(3)])
+
+
+@pytest.mark.gpu
+def test_c1_sphere_32():
+    n = 32
+    prob = targets.make_problem(n, m=1.50 + 0.01j, x=5.0)
+    dda = D.DDA()
+    dda.prepare_green(n, n, n, prob.iocc, prob.incid[0].k)
+    k = prob.incid[0].k
+    b = np.stack([prob.rhs(r) for r in range(2)])
+    adia = np.stack([prob.adia(r) for r in range(2)])
+    x64 = np.zeros(b.shape, dtype=np.complex128)
+    dda.solve_batch_f64("pbcgs2", b, x64, adia, maxit=2000, tol=1e-9)
+    # scattering directions: 0..180 deg at 1 deg in the planes phi = 0 and 90 deg
+    kk = np.linalg.norm(k)
+    aks, em1, em2 = [], [], []
+    for phi in (0.0, math.pi / 2):
+        for t in np.deg2rad(np.arange(0, 181, 1.0)):
+            nv = np.array([math.cos(t), math.sin(t) * math.cos(phi), math.sin(t) * math.sin(phi)])
+            e1 = np.array([-math.sin(t), math.cos(t) * math.cos(phi), math.cos(t) * math.sin(phi)])
+            aks.append(kk * nv)
+            em1.append(e1)
+            em2.append(np.cross(nv, e1))
+    aks, em1, em2 = (np.array(a, dtype=np.float32) for a in (aks, em1, em2))
+    f = []
+    zero = np.zeros(3 * prob.nat0, dtype=np.complex64)
+    for r in range(2):
+        out = dda.solve("pbcgs2", b[r], adia[r], prob.aoff(), maxit=1000, tol=TOL)
+        assert out.tole <= TOL
+        cabs, cext, _ = dda.evalq(k)
+        sc = dda.scat(k, prob.incid[r].e, prob.x0, etasca=0.5, aks=aks, em1=em1, em2=em2)
+        f.append((sc["f1"], sc["f2"]))
+        ec, ac = _compact(b[r], prob), _compact(adia[r], prob)
+        q64 = dda.evalq(k, use_resident=0, e=ec, p=_compact(x64[r], prob).astype(np.complex64), adia=ac, aoff=zero)
+        assert abs(cabs - q64[0]) <= 1e-4 * abs(q64[0]) and abs(cext - q64[1]) <= 1e-4 * abs(q64[1])
+        assert cext == pytest.approx(cabs + sc["csca"], rel=5e-3)
+    s, m = dda.mueller(k, prob.incid[0].e, prob.incid[1].e, em2, f[0][0], f[0][1], f[1][0], f[1][1])
+    s11 = m[:, 0, 0]
+    assert np.all(s11 > 0)
+    # both planes are mirror planes of the lattice sphere: S3 = S4 = 0
+    for i, j in [(0, 2), (0, 3), (1, 2), (1, 3), (2, 0), (2, 1), (3, 0), (3, 1)]:
+        assert np.abs(m[:, i, j]).max() <= 1e-4 * s11.max()
+    # the cubic lattice sphere looks the same in both planes
+    assert np.allclose(m[:181], m[181:], atol=1e-4 * s11.max())
+    dda.release()
+
+
+@pytest.mark.gpu
+def test_c3_ellipsoid_64_batch_128():
+    torch = pytest.importorskip("torch")
+    n = 64
+    orients = targets.random_orientations(64, seed=0)
+    prob = targets.make_problem(n, m=1.60 + 0.02j, x=12.0, semi=(n / 2, 0.8 * n / 2, 0.6 * n / 2),
+                                orientations=orients)
+    R = len(prob.incid)
+    assert R == 128
+    ks = np.array([inc.k for inc in prob.incid])
+    es = np.array([inc.e for inc in prob.incid])
+    dda = D.DDA()
+    dda.prepare_green(n, n, n, prob.iocc, prob.incid[0].k)
+    bd = torch.zeros((R, 3 * prob.nat), dtype=torch.complex64, device="cuda")
+    ad = torch.zeros_like(bd)
+    dda.make_inputs(ks, es, prob.x0, prob.m, b=bd, adia=ad)
+    xd = torch.zeros_like(bd)
+    out = dda.solve_batch("pbcgs2", bd, xd, ad, maxit=1000, tol=TOL)
+    assert np.all(out.status == 0) and np.all(out.tole <= TOL)
+    r64 = dda.residual_f64(bd, xd, ad)
+    assert np.all(r64 <= 1.2 * TOL), r64.max()
+    for r in (0, 37, 127):
+        single = dda.solve("pbcgs2", bd[r].cpu().numpy(), ad[r].cpu().numpy(), prob.aoff(), maxit=1000, tol=TOL)
+        assert abs(single.itno - out.itno[r]) <= max(1, 0.1 * single.itno)
+        x = xd[r].cpu().numpy()
+        assert np.linalg.norm(single.x - x) / np.linalg.norm(single.x) < 20 * TOL
+    dda.release()
