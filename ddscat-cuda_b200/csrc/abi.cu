@@ -395,6 +395,28 @@ static int widen_to_compact(const void* src, bool dev, int r, double2* dst) {
   return check_launch("FP64 batched solve widen");
 }
 
+// ---- adjoint gradient ----
+// g[r][site j] = -sum_c lam_c(j) dadia_c(j) p_c(j): the derivative of s^T P
+// with respect to a parameter that enters A only through CXADIA at site j
+// (A^T = A, so lam = A^-1 s is the adjoint solution).  FP64 accumulation.
+__global__ void k_adjoint_grad(int n, int nat0, const C* lam, const C* dad, const C* p, const int* occ, C* g,
+                               size_t g_rs) {
+  const int r = blockIdx.y;
+  const size_t off = (size_t)r * n;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nat0; q += gridDim.x * blockDim.x) {
+    double gr = 0.0, gi = 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const size_t i = off + (size_t)c * nat0 + q;
+      const double2 l = to_d(lam[i]), d = to_d(dad[i]), v = to_d(p[i]);
+      const double tr = l.x * d.x - l.y * d.y, ti = l.x * d.y + l.y * d.x;
+      gr -= tr * v.x - ti * v.y;
+      gi -= tr * v.y + ti * v.x;
+    }
+    g[(size_t)r * g_rs + occ[q]] = make_float2((float)gr, (float)gi);
+  }
+}
+
 // The prepared FP32 engine, or null before a successful prepare (read-only
 // access for entry points defined in other translation units).
 const Engine<float>* prepared_engine() { return s.ready ? &s.eng : nullptr; }
@@ -851,7 +873,8 @@ extern "C" DDSCAT_CUDA_API int ddscat_b200_solve_batch_f64(int solver, int nrhs,
   }
   const int replace = (solver & DDSCAT_B200_REPLACE_RESIDUAL) != 0;
   const int sym = (solver & DDSCAT_B200_QMR_SYMMETRIC) != 0;
-  solver &= ~(DDSCAT_B200_REPLACE_RESIDUAL | DDSCAT_B200_QMR_SYMMETRIC);
+  const bool in64 = (solver & DDSCAT_B200_INPUTS_F64) != 0;
+  solver &= ~(DDSCAT_B200_REPLACE_RESIDUAL | DDSCAT_B200_QMR_SYMMETRIC | DDSCAT_B200_INPUTS_F64);
   if ((solver != DDSCAT_B200_QMRCCG && solver != DDSCAT_B200_PBCGS2) || (sym && solver != DDSCAT_B200_QMRCCG)) {
     set_error("FP64 batched solve", "unsupported solver or flag");
     return 521;
@@ -863,10 +886,23 @@ extern "C" DDSCAT_CUDA_API int ddscat_b200_solve_batch_f64(int solver, int nrhs,
   }
   if (ensure_f64() || ensure_b64(nrhs)) return 523;
   const size_t full = (size_t)3 * s.eng.g.nat;
+  // complex-double full RHS r (host or device) -> compact slot
+  auto gather64 = [&](const void* src, int r, double2* dst) -> int {
+    const double2* f = (const double2*)src + (size_t)r * full;
+    if (!dev) {
+      cudaError_t e = cudaMemcpyAsync(b64.full, f, full * sizeof(double2), cudaMemcpyHostToDevice, s.stream);
+      if (e != cudaSuccess) { set_cuda_error("FP64 batched solve H2D", e); return 1; }
+      f = b64.full;
+    }
+    v_gather<double>(f, dst, s.eng.occ, s.eng.g.nat, s.eng.g.nat0, s.stream);
+    return check_launch("FP64 batched solve gather");
+  };
+  auto load = [&](const void* src, int r, double2* dst) -> int {
+    return in64 ? gather64(src, r, dst) : widen_to_compact(src, dev, r, dst);
+  };
   for (int r = 0; r < nrhs; ++r) {
-    if (widen_to_compact(b, dev, r, b64.b + (size_t)r * b64.n) ||
-        widen_to_compact(adia, dev, r, b64.adia + (size_t)r * b64.n) ||
-        (aoff && widen_to_compact(aoff, dev, r, b64.aoff + (size_t)r * b64.n)))
+    if (load(b, r, b64.b + (size_t)r * b64.n) || load(adia, r, b64.adia + (size_t)r * b64.n) ||
+        (aoff && load(aoff, r, b64.aoff + (size_t)r * b64.n)))
       return 524;
     const double2* xf = (const double2*)x + (size_t)r * full;
     if (!dev) {
@@ -911,5 +947,98 @@ extern "C" DDSCAT_CUDA_API int ddscat_b200_solve_batch_f64(int solver, int nrhs,
     set_error("FP64 batched solve", "at least one right-hand side stopped on a breakdown (see status)");
     return worst;
   }
+  return 0;
+}
+
+extern "C" DDSCAT_CUDA_API int ddscat_b200_adjoint_f32(int nrhs, const void* p, const void* src, const void* adia,
+                                                       const void* dadia, int maxit, float tol, void* grad, void* lam,
+                                                       int* itno, float* tole) {
+  clear_error();
+  if (!s.ready || nrhs <= 0 || !p || !src || !adia || !dadia || !grad || maxit <= 0 || !(tol > 0.f) || !itno ||
+      !tole) {
+    set_error("adjoint", "invalid argument or not prepared");
+    return 530;
+  }
+  const bool dev = is_device_ptr(p);
+  if (is_device_ptr(src) != dev || is_device_ptr(adia) != dev || is_device_ptr(dadia) != dev ||
+      is_device_ptr(grad) != dev || (lam && is_device_ptr(lam) != dev)) {
+    set_error("adjoint", "all arrays must be host or all device pointers");
+    return 531;
+  }
+  if (ensure_batch(nrhs)) return 532;
+  const size_t full = (size_t)3 * s.eng.g.nat, nat = (size_t)s.eng.g.nat;
+  C* pc = bs.work + (size_t)(BATCH_WORK_VECTORS - 2) * nrhs * bs.n;  // outside the solver's slots
+  C* dc = bs.aoff;
+  for (int r = 0; r < nrhs; ++r) {
+    if (to_compact(src, dev, r, bs.b) || to_compact(adia, dev, r, bs.adia)) return 533;
+  }
+  cudaError_t e = cudaMemsetAsync(bs.x, 0, (size_t)nrhs * bs.n * sizeof(C), s.stream);
+  if (e != cudaSuccess) { set_cuda_error("adjoint", e); return 533; }
+  // adjoint solve A lam = s: one-MATVEC QMRCCG with residual replacement
+  BatchIO<float> io;
+  io.eng = &s.eng; io.ops = &bs.ops; io.R = nrhs; io.n = bs.n;
+  io.b = bs.b; io.x = bs.x; io.adia = bs.adia; io.aoff = nullptr;
+  io.work = bs.work; io.nwork = BATCH_WORK_VECTORS - 2;
+  io.maxit = maxit; io.tol = (double)tol; io.verbose = s.verbose; io.replace = 1; io.sym = 1;
+  BatchResult res;
+  const int rc = solve_batch_qmrccg<float>(io, res);
+  if (rc) return rc == 1 ? 534 : rc;
+  for (int r = 0; r < nrhs; ++r) {
+    itno[r] = res.itno[r];
+    tole[r] = (float)res.tole[r];
+    if (res.status[r]) {
+      set_error("adjoint", "adjoint solve broke down for at least one right-hand side");
+      return res.status[r];
+    }
+  }
+  // forward solutions and dCXADIA/dparameter, compact
+  for (int r = 0; r < nrhs; ++r) {
+    const C* pf = (const C*)p + (size_t)r * full;
+    const C* df = (const C*)dadia + (size_t)r * full;
+    for (int k = 0; k < 2; ++k) {
+      const C* f = k == 0 ? pf : df;
+      if (!dev) {
+        e = cudaMemcpyAsync(s.d_xf, f, full * sizeof(C), cudaMemcpyHostToDevice, s.stream);
+        if (e != cudaSuccess) { set_cuda_error("adjoint H2D", e); return 533; }
+        f = s.d_xf;
+      }
+      v_gather<float>(f, (k == 0 ? pc : dc) + (size_t)r * bs.n, s.eng.occ, s.eng.g.nat, s.eng.g.nat0, s.stream);
+      if (check_launch("adjoint gather")) return 533;
+    }
+  }
+  // gradient per site (zero on vacuum)
+  C* gd = dev ? static_cast<C*>(grad) : s.d_xf;  // host: stage nat sites per RHS in the full-vector buffer
+  const unsigned gx = (unsigned)std::min<size_t>(ceil_div((size_t)s.eng.g.nat0, 256), 1184);
+  for (int r0 = 0; r0 < nrhs; r0 += dev ? nrhs : 3) {
+    const int nr = dev ? nrhs : std::min(3, nrhs - r0);  // the host staging buffer holds 3 x NAT
+    e = cudaMemsetAsync(gd + (dev ? 0 : 0), 0, (size_t)nr * nat * sizeof(C), s.stream);
+    if (e != cudaSuccess) { set_cuda_error("adjoint", e); return 535; }
+    k_adjoint_grad<<<dim3(gx, (unsigned)nr), 256, 0, s.stream>>>(bs.n, s.eng.g.nat0, bs.x + (size_t)r0 * bs.n,
+                                                                 dc + (size_t)r0 * bs.n, pc + (size_t)r0 * bs.n,
+                                                                 s.eng.occ, gd, nat);
+    note_launch();
+    if (check_launch("adjoint gradient")) return 535;
+    if (!dev) {
+      e = cudaMemcpyAsync((C*)grad + (size_t)r0 * nat, gd, (size_t)nr * nat * sizeof(C), cudaMemcpyDeviceToHost,
+                          s.stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s.stream);
+      if (e != cudaSuccess) { set_cuda_error("adjoint D2H", e); return 535; }
+    }
+  }
+  if (lam) {
+    for (int r = 0; r < nrhs; ++r) {
+      C* dst = dev ? (C*)lam + (size_t)r * full : s.d_xf;
+      e = cudaMemsetAsync(dst, 0, full * sizeof(C), s.stream);
+      if (e != cudaSuccess) { set_cuda_error("adjoint", e); return 535; }
+      v_scatter<float>(bs.x + (size_t)r * bs.n, dst, s.eng.occ, s.eng.g.nat, s.eng.g.nat0, s.stream);
+      if (check_launch("adjoint scatter")) return 535;
+      if (!dev) {
+        e = cudaMemcpyAsync((C*)lam + (size_t)r * full, s.d_xf, full * sizeof(C), cudaMemcpyDeviceToHost, s.stream);
+        if (e != cudaSuccess) { set_cuda_error("adjoint D2H", e); return 535; }
+      }
+    }
+  }
+  e = cudaStreamSynchronize(s.stream);
+  if (e != cudaSuccess) { set_cuda_error("adjoint", e); return 535; }
   return 0;
 }

@@ -29,7 +29,7 @@ EXPORTS = (
     + ["ddscat_b200_set_verbose", "ddscat_b200_layout", "ddscat_b200_matvec_timing", "ddscat_b200_solve_batch_f32",
        "ddscat_b200_last_solve_stats", "ddscat_b200_residual_f64", "ddscat_b200_launch_count",
        "ddscat_b200_apply_noalloc_f32", "ddscat_b200_mueller_f32", "ddscat_b200_make_inputs_f32",
-       "ddscat_b200_solve_batch_f64"]
+       "ddscat_b200_solve_batch_f64", "ddscat_b200_adjoint_f32"]
 )
 
 
@@ -95,6 +95,8 @@ def _declare(lib):
     lib.ddscat_b200_make_inputs_f32.restype = _I
     lib.ddscat_b200_solve_batch_f64.argtypes = [_I, _I, _P, _P, _P, _P, _I, _D2, _P, _P, _P, _P]
     lib.ddscat_b200_solve_batch_f64.restype = _I
+    lib.ddscat_b200_adjoint_f32.argtypes = [_I, _P, _P, _P, _P, _I, _F, _P, _P, _P, _P]
+    lib.ddscat_b200_adjoint_f32.restype = _I
     lib.ddscat_b200_launch_count.argtypes = []
     lib.ddscat_b200_launch_count.restype = ct.c_ulonglong
 
@@ -129,6 +131,7 @@ def _c64(a, n=None):
 BATCH_SOLVERS = {"qmrccg": 1, "pbcgs2": 2}
 REPLACE_RESIDUAL = 0x100  # DDSCAT_B200_REPLACE_RESIDUAL
 QMR_SYMMETRIC = 0x200  # DDSCAT_B200_QMR_SYMMETRIC
+INPUTS_F64 = 0x400  # DDSCAT_B200_INPUTS_F64
 
 
 def _vptr(a):
@@ -268,9 +271,14 @@ class DDA:
 
     def solve_batch_f64(self, name, b, x, adia, aoff=None, maxit=1000, tol=1e-9, check=True, replace=False,
                         symmetric=False):
-        """All-FP64 batched solve; b, adia, aoff complex64 (nrhs, 3*NAT), x
-        complex128 (nrhs, 3*NAT) in/out; NumPy arrays or CUDA tensors."""
+        """All-FP64 batched solve; b, adia, aoff complex64 or complex128
+        (nrhs, 3*NAT), x complex128 (nrhs, 3*NAT) in/out; NumPy arrays or CUDA
+        tensors."""
         nrhs = int(b.shape[0])
+        in64 = str(b.dtype).endswith("complex128")
+        for a in (adia,) + (() if aoff is None else (aoff,)):
+            if str(a.dtype).endswith("complex128") != in64:
+                raise ValueError("b, adia and aoff must share one precision")
         if not hasattr(x, "data_ptr") and (x.dtype != np.complex128 or not x.flags.c_contiguous):
             raise ValueError("x must be a C-contiguous complex128 array")
         it = np.zeros(nrhs, dtype=np.int32)
@@ -278,11 +286,27 @@ class DDA:
         nc = np.zeros(nrhs, dtype=np.int32)
         st = np.zeros(nrhs, dtype=np.int32)
         code = BATCH_SOLVERS[name] | (REPLACE_RESIDUAL if replace else 0) | (QMR_SYMMETRIC if symmetric else 0)
+        code |= INPUTS_F64 if in64 else 0
         rc = self.lib.ddscat_b200_solve_batch_f64(code, nrhs, _vptr(b), _vptr(x), _vptr(adia), _vptr(aoff), maxit,
                                                   float(tol), _ptr(it), _ptr(tole), _ptr(nc), _ptr(st))
         if check:
             self._check("solve_batch_f64", rc)
         return BatchOut(rc, it, tole, nc, st)
+
+    def adjoint(self, p, src, adia, dadia, maxit=1000, tol=1e-5, want_lam=False):
+        """Per-site derivatives of s^T P (see ddscat_b200_adjoint_f32); all
+        arguments (nrhs, 3*NAT) complex64 NumPy arrays.  Returns (grad (nrhs,
+        NAT) complex64, lam or None, itno, tole)."""
+        p, src, adia, dadia = (np.ascontiguousarray(a, dtype=np.complex64) for a in (p, src, adia, dadia))
+        nrhs = p.shape[0]
+        grad = np.zeros((nrhs, self.nat), dtype=np.complex64)
+        lam = np.zeros_like(p) if want_lam else None
+        it = np.zeros(nrhs, dtype=np.int32)
+        tole = np.zeros(nrhs, dtype=np.float32)
+        rc = self.lib.ddscat_b200_adjoint_f32(nrhs, _ptr(p), _ptr(src), _ptr(adia), _ptr(dadia), maxit, tol,
+                                              _ptr(grad), _ptr(lam), _ptr(it), _ptr(tole))
+        self._check("adjoint", rc)
+        return grad, lam, it, tole
 
     def last_solve_stats(self):
         ms, rhs, calls = ct.c_double(), ct.c_longlong(), _I()

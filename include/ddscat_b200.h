@@ -58,6 +58,7 @@ DDSCAT_CUDA_API int ddscat_b200_matvec_timing(int nrhs, int iters, int cwhat, fl
 #define DDSCAT_B200_PBCGS2 2
 #define DDSCAT_B200_REPLACE_RESIDUAL 0x100
 #define DDSCAT_B200_QMR_SYMMETRIC 0x200
+#define DDSCAT_B200_INPUTS_F64 0x400
 DDSCAT_CUDA_API int ddscat_b200_solve_batch_f32(int solver, int nrhs, const void *b, void *x, const void *adia,
                                                 const void *aoff, int maxit, float tol, int *itno, float *tole,
                                                 int *ncompte, int *status);
@@ -129,6 +130,8 @@ DDSCAT_CUDA_API int ddscat_b200_make_inputs_f32(int nrhs, const float *k, const 
  * residuals) are checked.  b, adia, aoff: nrhs complex-float full vectors (as
  * for the FP32 entry point, widened on the GPU); x: nrhs complex-DOUBLE full
  * vectors, initial guess in, solution out; all host or all device pointers.
+ * With DDSCAT_B200_INPUTS_F64 OR'ed into solver, b, adia and aoff are
+ * complex-double full vectors too.
  * tole is the achieved true relative residual.  Codes: 520 invalid argument /
  * not prepared, 521 solver or flag, 522 mixed pointer kinds, 523 workspace,
  * 524 input transfer, 525 solver failure, 526 output transfer; a breakdown of
@@ -136,6 +139,26 @@ DDSCAT_CUDA_API int ddscat_b200_make_inputs_f32(int nrhs, const float *k, const 
 DDSCAT_CUDA_API int ddscat_b200_solve_batch_f64(int solver, int nrhs, const void *b, void *x, const void *adia,
                                                 const void *aoff, int maxit, double tol, int *itno, double *tole,
                                                 int *ncompte, int *status);
+
+/* Adjoint gradient (no counterpart in the reference).  For nrhs forward
+ * solutions P_r of A_r P_r = E_r and adjoint sources s_r, solves the adjoint
+ * systems A_r lam_r = s_r (A^T = A: the same complex-symmetric operator, one
+ * batched one-MATVEC QMRCCG solve with residual replacement, tolerance tol) and
+ * returns per site j the derivative of the holomorphic functional F_r = s_r^T P_r
+ * with respect to a site parameter that enters A only through CXADIA:
+ *   grad[r][j] = -sum_c lam_r[c][j] * dadia_r[c][j] * P_r[c][j],
+ * dadia_r = dCXADIA/dparameter (e.g. the derivative of the LDR 1/alpha with
+ * respect to the permittivity).  s_r = conj(E_r) gives dCext: Cext = 4 pi k
+ * Im(F)/E02; s_r = the far-field weights of ddscat_cuda_scat_f32 gives the
+ * derivative of a scattering amplitude.  p, src, adia, dadia, lam (optional):
+ * nrhs full vectors (3*NAT complex floats); grad: nrhs x NAT complex floats
+ * (zero on vacuum sites); all host or all device pointers.  itno / tole: the
+ * adjoint solves' iterations and achieved residuals.  Codes: 530 invalid
+ * argument / not prepared, 531 mixed pointer kinds, 532 workspace, 533 input
+ * transfer, 534 solver failure, 535 gradient or output failure. */
+DDSCAT_CUDA_API int ddscat_b200_adjoint_f32(int nrhs, const void *p, const void *src, const void *adia,
+                                            const void *dadia, int maxit, float tol, void *grad, void *lam, int *itno,
+                                            float *tole);
 
 #ifdef __cplusplus
 }
