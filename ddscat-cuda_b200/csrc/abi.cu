@@ -10,13 +10,17 @@
 #include <cstring>
 #include <string>
 #include <vector>
+#include <atomic>
+#include <mutex>
 #include "ddscat_b200.h"
 #include "batch.h"
 #include "solvers.h"
 
 namespace ddb {
 
-static std::string g_last_error;
+// error text of the calling host thread (the multi-target solve runs targets
+// on several threads; single-threaded callers see the reference behaviour)
+static thread_local std::string g_last_error;
 void set_error(const char* where, const char* what) {
   char b[1024];
   std::snprintf(b, sizeof(b), "%s: %s", where, what);
@@ -25,8 +29,17 @@ void set_error(const char* where, const char* what) {
 void set_cuda_error(const char* where, cudaError_t e) { set_error(where, cudaGetErrorString(e)); }
 const char* last_error_text() { return g_last_error.c_str(); }
 void clear_error() { g_last_error.clear(); }
-static unsigned long long g_launches = 0;
+static std::atomic<unsigned long long> g_launches{0};
 void note_launch(unsigned long long k) { g_launches += k; }
+// raise the dynamic shared-memory limit of kernel f once per process (thread-safe)
+void raise_smem_limit(const void* f) {
+  static std::mutex mu;
+  static std::vector<const void*> done;
+  std::lock_guard<std::mutex> lock(mu);
+  if (std::find(done.begin(), done.end(), f) != done.end()) return;
+  cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  done.push_back(f);
+}
 int check_launch(const char* where) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) { set_cuda_error(where, e); return 1; }
@@ -646,7 +659,7 @@ DDSCAT_CUDA_API int ddscat_b200_set_verbose(int level) {
 
 DDSCAT_CUDA_API int ddscat_b200_layout(void) { return slices_build(); }
 
-DDSCAT_CUDA_API unsigned long long ddscat_b200_launch_count(void) { return g_launches; }
+DDSCAT_CUDA_API unsigned long long ddscat_b200_launch_count(void) { return g_launches.load(); }
 
 DDSCAT_CUDA_API int ddscat_b200_solve_batch_f32(int solver, int nrhs, const void* b, void* x, const void* adia,
                                                 const void* aoff, int maxit, float tol, int* itno, float* tole,

@@ -26,6 +26,7 @@ void set_cuda_error(const char* where, cudaError_t e);
 const char* last_error_text();
 void clear_error();
 int check_launch(const char* where);
+void raise_smem_limit(const void* f);  // thread-safe, once per kernel
 // count of kernels this library launched (reported by ddscat_b200_launch_count)
 void note_launch(unsigned long long k = 1);
 

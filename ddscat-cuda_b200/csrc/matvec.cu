@@ -663,20 +663,13 @@ template <typename T> int Engine<T>::ensure_workspace(int nrhs) {
   return 0;
 }
 
-template <typename T> static void set_smem(const void* f) {
-  cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-}
 
 template <typename T> int Engine<T>::matvec(const MvArgs<T>& a) {
-  static bool attr_done = false;
-  if (!attr_done) {
-    set_smem<T>((const void*)k_zfwd<T>);
-    set_smem<T>((const void*)k_xfwd<T>);
-    set_smem<T>((const void*)k_ygreen<T>);
-    set_smem<T>((const void*)k_xinv<T>);
-    set_smem<T>((const void*)k_zinv_fin<T>);
-    attr_done = true;
-  }
+  raise_smem_limit((const void*)k_zfwd<T>);
+  raise_smem_limit((const void*)k_xfwd<T>);
+  raise_smem_limit((const void*)k_ygreen<T>);
+  raise_smem_limit((const void*)k_xinv<T>);
+  raise_smem_limit((const void*)k_zinv_fin<T>);
   {
     // z-spectrum capacity: all RHS of the call if they fit the budget
     const size_t per_rhs_z = (size_t)3 * g.Mz * g.ny * g.nx * sizeof(C);
@@ -722,14 +715,8 @@ template <typename T> int Engine<T>::matvec(const MvArgs<T>& a) {
   const size_t sm_z = (size_t)2 * P.tz * g.Mz * sizeof(C);
   const size_t sm_x = (size_t)2 * P.ry * (g.Mx + 1) * sizeof(C);
   const size_t sm_y = (size_t)4 * P.ty * g.My * sizeof(C);
-  {
-    static std::vector<const void*> attr_set;  // kernels whose smem limit is raised
-    for (const void* f : {fz_r, fx_r, fy_r, fxi_r, fzi_r}) {
-      if (!f || std::find(attr_set.begin(), attr_set.end(), f) != attr_set.end()) continue;
-      cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-      attr_set.push_back(f);
-    }
-  }
+  for (const void* f : {fz_r, fx_r, fy_r, fxi_r, fzi_r})
+    if (f) raise_smem_limit(f);
   for (int r0 = 0; r0 < a.nrhs; r0 += zcap) {
     const int nr = std::min(zcap, a.nrhs - r0);
     P.rhs0 = r0;

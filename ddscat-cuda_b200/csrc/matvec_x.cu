@@ -486,11 +486,7 @@ template <typename T> static const void* xkernel(XPass p, int n) {
 static int rT(int n) { return n <= 32 ? 4 : (n <= 128 ? 8 : 16); }
 
 template <typename T> static int xlaunch(const void* f, dim3 g, int th, size_t sm, cudaStream_t st, XParams<T>& P) {
-  static std::vector<const void*> raised;
-  if (std::find(raised.begin(), raised.end(), f) == raised.end()) {
-    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    raised.push_back(f);
-  }
+  raise_smem_limit(f);
   void* args[] = {(void*)&P};
   note_launch();
   cudaError_t e = cudaLaunchKernel(f, g, dim3(th), args, sm, st);

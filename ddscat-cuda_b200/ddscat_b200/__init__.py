@@ -29,7 +29,7 @@ EXPORTS = (
     + ["ddscat_b200_set_verbose", "ddscat_b200_layout", "ddscat_b200_matvec_timing", "ddscat_b200_solve_batch_f32",
        "ddscat_b200_last_solve_stats", "ddscat_b200_residual_f64", "ddscat_b200_launch_count",
        "ddscat_b200_apply_noalloc_f32", "ddscat_b200_mueller_f32", "ddscat_b200_make_inputs_f32",
-       "ddscat_b200_solve_batch_f64", "ddscat_b200_adjoint_f32"]
+       "ddscat_b200_solve_batch_f64", "ddscat_b200_adjoint_f32", "ddscat_b200_multi_solve_f32"]
 )
 
 
@@ -97,6 +97,8 @@ def _declare(lib):
     lib.ddscat_b200_solve_batch_f64.restype = _I
     lib.ddscat_b200_adjoint_f32.argtypes = [_I, _P, _P, _P, _P, _I, _F, _P, _P, _P, _P]
     lib.ddscat_b200_adjoint_f32.restype = _I
+    lib.ddscat_b200_multi_solve_f32.argtypes = [_I, _P, _P, _P, _P, _P, _P, _P, _I, _I, _F, _I, _P, _P, _P, _P]
+    lib.ddscat_b200_multi_solve_f32.restype = _I
     lib.ddscat_b200_launch_count.argtypes = []
     lib.ddscat_b200_launch_count.restype = ct.c_ulonglong
 
@@ -307,6 +309,41 @@ class DDA:
                                               _ptr(grad), _ptr(lam), _ptr(it), _ptr(tole))
         self._check("adjoint", rc)
         return grad, lam, it, tole
+
+    def multi_solve(self, targets_, name="qmrccg", maxit=1000, tol=1e-5, replace=True, symmetric=True, nthreads=0,
+                    check=True):
+        """Solve many targets of uneven size together.  targets_: list of dicts
+        with dims (nx, ny, nz), iocc (NAT int16), ak (3,), b, x, adia
+        ((nrhs, 3*NAT) complex64 host arrays; x in/out).  Returns BatchOut over
+        all RHS in target order."""
+        nt = len(targets_)
+        dims = np.ascontiguousarray([t["dims"] for t in targets_], dtype=np.int32).reshape(-1)
+        occs = [np.ascontiguousarray(t["iocc"], dtype=np.int16) for t in targets_]
+        aks = np.ascontiguousarray([t["ak"] for t in targets_], dtype=np.float32).reshape(-1)
+        nr = np.ascontiguousarray([t["b"].shape[0] for t in targets_], dtype=np.int32)
+        for t in targets_:
+            for key in ("b", "x", "adia"):
+                a = t[key]
+                if a.dtype != np.complex64 or not a.flags.c_contiguous:
+                    raise ValueError(f"{key} must be a C-contiguous complex64 array")
+        P = ct.c_void_p * nt
+        po = P(*[a.ctypes.data for a in occs])
+        pb = P(*[t["b"].ctypes.data for t in targets_])
+        px = P(*[t["x"].ctypes.data for t in targets_])
+        pa = P(*[t["adia"].ctypes.data for t in targets_])
+        total = int(nr.sum())
+        it = np.zeros(total, dtype=np.int32)
+        tole = np.zeros(total, dtype=np.float32)
+        nc = np.zeros(total, dtype=np.int32)
+        st = np.zeros(total, dtype=np.int32)
+        code = BATCH_SOLVERS[name] | (REPLACE_RESIDUAL if replace else 0) | (QMR_SYMMETRIC if symmetric else 0)
+        rc = self.lib.ddscat_b200_multi_solve_f32(nt, _ptr(dims), ct.cast(po, ct.c_void_p), _ptr(aks), _ptr(nr),
+                                                  ct.cast(pb, ct.c_void_p), ct.cast(px, ct.c_void_p),
+                                                  ct.cast(pa, ct.c_void_p), code, maxit, tol, nthreads, _ptr(it),
+                                                  _ptr(tole), _ptr(nc), _ptr(st))
+        if check:
+            self._check("multi_solve", rc)
+        return BatchOut(rc, it, tole, nc, st)
 
     def last_solve_stats(self):
         ms, rhs, calls = ct.c_double(), ct.c_longlong(), _I()

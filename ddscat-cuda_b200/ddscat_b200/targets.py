@@ -124,6 +124,32 @@ class Problem:
         return np.zeros(3 * self.nat, dtype=np.complex64)
 
 
+def fft_friendly(n):
+    """Smallest m >= n of the form 2^a 3^b 5^c: DDSCAT extends each grid
+    dimension this way so that the padded FFT lengths 2m factor into small
+    radices; the extra planes are vacuum."""
+    m = max(1, int(n))
+    while True:
+        k = m
+        for f in (2, 3, 5):
+            while k % f == 0:
+                k //= f
+        if k == 1:
+            return m
+        m += 1
+
+
+def embed_ellipsoid(sides, semi):
+    """(grid dims, IOCC) of an ellipsoid filling a box of the given lattice
+    sides, placed in a grid extended to FFT-friendly sizes (vacuum padding)."""
+    sx, sy, sz = (int(v) for v in sides)
+    gx, gy, gz = fft_friendly(sx), fft_friendly(sy), fft_friendly(sz)
+    box = ellipsoid_occupancy(sx, sy, sz, semi).reshape(sz, sy, sx)
+    occ = np.zeros((gz, gy, gx), dtype=np.int16)
+    occ[:sz, :sy, :sx] = box
+    return (gx, gy, gz), occ.reshape(-1)
+
+
 def make_problem(nx, ny=None, nz=None, m=1.5 + 0.01j, x=5.0, semi=None, orientations=None, iocc=None):
     """Ellipsoid (sphere by default) of size parameter x = k*aeff; one RHS per
     (orientation, polarisation) with k along x before rotation and

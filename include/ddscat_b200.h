@@ -160,6 +160,24 @@ DDSCAT_CUDA_API int ddscat_b200_adjoint_f32(int nrhs, const void *p, const void 
                                             const void *dadia, int maxit, float tol, void *grad, void *lam, int *itno,
                                             float *tole);
 
+/* Many targets of uneven size solved together (no counterpart in the
+ * reference, whose state holds one target).  Target t has lattice dims[3t..3t+2],
+ * occupancy iocc[t] (int16, NAT_t), wave vector ak[3t..3t+2] (lattice units;
+ * point dipoles, IPBC = 0, unit spacing) and nrhs[t] right-hand sides: b[t],
+ * x[t] (initial guess in, solution out) and adia[t] are host arrays of nrhs[t]
+ * full vectors (3*NAT_t complex floats each).  Each target gets its own
+ * engine, Green tensor and CUDA stream; nthreads host threads (0: up to 8)
+ * drive the targets' batched solves concurrently, largest first.  solver and
+ * flags as for ddscat_b200_solve_batch_f32; per-RHS outputs in target order.
+ * The FFT3D layout is used in both libraries.  Codes: 540 invalid argument,
+ * 541 solver or flag, 542 workspace, 543 geometry or Green build, 544 input
+ * transfer, 545 solver failure, 546 output transfer; a breakdown returns that
+ * RHS's status code. */
+DDSCAT_CUDA_API int ddscat_b200_multi_solve_f32(int ntarget, const int *dims, const int16_t *const *iocc,
+                                                const float *ak, const int *nrhs, const void *const *b, void *const *x,
+                                                const void *const *adia, int solver, int maxit, float tol,
+                                                int nthreads, int *itno, float *tole, int *ncompte, int *status);
+
 #ifdef __cplusplus
 }
 #endif
