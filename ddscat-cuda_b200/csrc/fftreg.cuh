@@ -151,8 +151,18 @@ __device__ __forceinline__ void line_fft(C (&v)[E], C* sl, int t, const C* __res
   constexpr int M = E / T;
   static_assert(M * T == E && M >= 1, "E must be a multiple of T");
   if constexpr (HALF_IN) dftr_h<E, DIR>(v); else dftr<E, DIR>(v);
+  // twiddles W^(t p), p = 1..E-1: the powers of two come from the table, the
+  // others are products of at most four of them (fewer shared-memory loads)
+  C w[E];
 #pragma unroll
-  for (int p = 1; p < E; ++p) v[p] = cmul(v[p], twid<DIR>(tw, t * p));
+  for (int b = 1; b < E; b <<= 1) w[b] = twid<DIR>(tw, t * b);
+#pragma unroll
+  for (int p = 3; p < E; ++p) {
+    const int hb = 1 << (31 - __clz(p));  // highest set bit of p
+    if (p != hb) w[p] = cmul(w[hb], w[p - hb]);
+  }
+#pragma unroll
+  for (int p = 1; p < E; ++p) v[p] = cmul(v[p], w[p]);
 #pragma unroll
   for (int p = 0; p < E; ++p) sl[t * (E + 1) + p] = v[p];
   if (BLOCK_SYNC) __syncthreads(); else __syncwarp();
