@@ -112,41 +112,65 @@ template <int K, int DIR, typename C> __device__ __forceinline__ void dftr_h(C* 
   }
 }
 
-// per-line scratch size (complex elements) for the transpose, before padding
-template <int E, int T> constexpr int line_scratch() { return T * (E + 1) + 1; }
+// Transpose scratch of one line: T rows of E elements.  Row stride E + 1, or
+// E + 2 with PAIR (even, so that element pairs are 16-byte aligned and each
+// pair is written with one 128-bit store).
+template <int E, bool PAIR = false> constexpr int row_stride() { return PAIR ? E + 2 : E + 1; }
+template <int E, int T, bool PAIR = false> constexpr int line_scratch() { return T * row_stride<E, PAIR>() + 2; }
 
 // Line stride (complex elements) for L lines per block whose threads are
-// interleaved line-fastest (column passes) or thread-fastest (row passes):
-// the smallest stride >= T*(E+1) for which the 16 lanes of a half-warp hit 16
-// distinct 8-byte bank pairs in both the transpose write and read.
-inline int line_stride(int E, int T, int L, bool line_fastest) {
-  const int base = T * (E + 1);
-  for (int pad = 0; pad < 32; ++pad) {
+// interleaved line-fastest (column passes) or thread-fastest (row passes): the
+// smallest stride >= T*rowstride for which the transpose is free of
+// shared-memory bank conflicts where one exists.  Reads: the 16 lanes of a
+// half-warp load 8-byte elements at s*rs + t and must hit 16 distinct 8-byte
+// bank pairs.  Writes: without pair, the 16 lanes of a half-warp store 8 bytes
+// at t*rs + p; with pair (even strides only), the 8 lanes of a quarter-warp
+// store 16 bytes and must hit 8 distinct 16-byte bank groups.
+inline int line_stride(int E, int T, int L, bool line_fastest, bool pair = false) {
+  const int RS = pair ? E + 2 : E + 1;
+  const int base = T * RS;
+  auto lane_lt = [&](int lane, int& l, int& t) {
+    if (line_fastest) { l = lane % L; t = lane / L; } else { t = lane % T; l = lane / T; }
+    return l < L && t < T;
+  };
+  for (int pad = 0; pad < 64; pad += pair ? 2 : 1) {
     const int LS = base + pad;
     bool ok = true;
-    for (int phase = 0; phase < 2 && ok; ++phase) {
+    const int wl = pair ? 8 : 16;  // lanes per write wavefront
+    for (int q = 0; q < 32 / wl && ok; ++q) {
       unsigned used = 0;
-      for (int lane = 0; lane < 16 && ok; ++lane) {
+      for (int k = 0; k < wl && ok; ++k) {
         int l, t;
-        if (line_fastest) { l = lane % L; t = lane / L; } else { t = lane % T; l = lane / T; }
-        if (l >= L || t >= T) continue;
-        // write: t*(E+1) + p (p = 0); read: s*(E+1) + t (s = 0)
-        const int a = (l * LS + (phase == 0 ? t * (E + 1) : t)) & 15;
+        if (!lane_lt(wl * q + k, l, t)) continue;
+        const int a = l * LS + t * RS;
+        const int g = pair ? (a / 2) & 7 : a & 15;
+        if (used & (1u << g)) ok = false;
+        used |= 1u << g;
+      }
+    }
+    for (int h = 0; h < 2 && ok; ++h) {
+      unsigned used = 0;
+      for (int k = 0; k < 16 && ok; ++k) {
+        int l, t;
+        if (!lane_lt(16 * h + k, l, t)) continue;
+        const int a = (l * LS + t) & 15;
         if (used & (1u << a)) ok = false;
         used |= 1u << a;
       }
     }
     if (ok) return LS;
   }
-  return base + 1;
+  return base + (pair ? 2 : 1);
 }
 
 // One length-E*T transform of the line held in v by thread t (0 <= t < T).
 // `sl` is this line's shared scratch; `tw` the N-entry table exp(-2*pi*i*m/N).
 // BLOCK_SYNC selects __syncthreads (line spread over warps) or __syncwarp.
 // HALF_IN: elements t + T*i with i >= E/2 (the upper half of the line) are
-// zero and are not read.
-template <int E, int T, int DIR, bool BLOCK_SYNC, bool HALF_IN = false, typename C>
+// zero and are not read.  PAIR: transpose rows of stride E + 2 written with
+// 128-bit stores (complex-float lines; the line stride must come from
+// line_stride(..., pair = true)).
+template <int E, int T, int DIR, bool BLOCK_SYNC, bool HALF_IN = false, bool PAIR = false, typename C>
 __device__ __forceinline__ void line_fft(C (&v)[E], C* sl, int t, const C* __restrict__ tw) {
   constexpr int M = E / T;
   static_assert(M * T == E && M >= 1, "E must be a multiple of T");
@@ -163,14 +187,22 @@ __device__ __forceinline__ void line_fft(C (&v)[E], C* sl, int t, const C* __res
   }
 #pragma unroll
   for (int p = 1; p < E; ++p) v[p] = cmul(v[p], w[p]);
+  constexpr bool P2 = PAIR && sizeof(C) == 8;
+  constexpr int RS = row_stride<E, P2>();
+  if constexpr (P2) {
 #pragma unroll
-  for (int p = 0; p < E; ++p) sl[t * (E + 1) + p] = v[p];
+    for (int p = 0; p < E; p += 2)
+      *reinterpret_cast<float4*>(sl + t * RS + p) = make_float4(v[p].x, v[p].y, v[p + 1].x, v[p + 1].y);
+  } else {
+#pragma unroll
+    for (int p = 0; p < E; ++p) sl[t * RS + p] = v[p];
+  }
   if (BLOCK_SYNC) __syncthreads(); else __syncwarp();
 #pragma unroll
   for (int j = 0; j < M; ++j) {
     C u[T];
 #pragma unroll
-    for (int s = 0; s < T; ++s) u[s] = sl[s * (E + 1) + t + T * j];
+    for (int s = 0; s < T; ++s) u[s] = sl[s * RS + t + T * j];
     dftr<T, DIR>(u);
 #pragma unroll
     for (int q = 0; q < T; ++q) v[j + M * q] = u[q];

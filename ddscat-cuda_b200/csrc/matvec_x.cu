@@ -69,6 +69,7 @@ template <int N> struct XShape {
   static constexpr int RL = 256 / TT;
   static constexpr int RZ = (128 / TT) > 1 ? 128 / TT : 1;  // ZG lines per block (3*TT*RZ threads)
   static constexpr int ZG_MINB = E >= 32 ? 2 : 3;             // ZG blocks per SM the registers must allow
+  static constexpr bool PAIR = TT >= 8;                      // 128-bit transpose stores (conflict-free for TT >= 8)
 };
 
 // Tile <-> global moves of the row passes: N rows of RL consecutive elements
@@ -176,7 +177,7 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_xf(XParam
 #pragma unroll
     for (int i = 0; i < H; ++i) v[i].y = -v[i].y;
   }
-  line_fft<E, TT, +1, false, true>(v, lines + (size_t)l * P.lsx, t, tws);
+  line_fft<E, TT, +1, false, true, S_::PAIR>(v, lines + (size_t)l * P.lsx, t, tws);
   __syncthreads();  // all line scratch consumed before the tile reuses it
 #pragma unroll
   for (int i = 0; i < E; ++i) tile[(t + TT * i) * (RL + 1) + l] = v[i];
@@ -206,7 +207,7 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_yf(XParam
   const bool zin = iz < P.nz;
 #pragma unroll
   for (int i = 0; i < H; ++i) v[i] = zin ? A[t + TT * i] : mk<C>(0, 0);  // iy < ny = N/2
-  line_fft<E, TT, +1, false, true>(v, lines + (size_t)l * P.lsy, t, tws);
+  line_fft<E, TT, +1, false, true, S_::PAIR>(v, lines + (size_t)l * P.lsy, t, tws);
   __syncthreads();
 #pragma unroll
   for (int i = 0; i < E; ++i) tile[(t + TT * i) * (RL + 1) + l] = v[i];
@@ -282,7 +283,7 @@ __global__ void __launch_bounds__(3 * XShape<N>::TT * XShape<N>::RZ, XShape<N>::
   C v[E];
 #pragma unroll
   for (int i = 0; i < H; ++i) v[i] = live ? row[t + TT * i] : mk<C>(0, 0);  // iz < nz = N/2
-  line_fft<E, TT, +1, false, true>(v, my, t, tws);
+  line_fft<E, TT, +1, false, true, S_::PAIR>(v, my, t, tws);
 #pragma unroll
   for (int i = 0; i < E; ++i) my[t + TT * i] = v[i];
   __syncthreads();
@@ -332,7 +333,7 @@ __global__ void __launch_bounds__(3 * XShape<N>::TT * XShape<N>::RZ, XShape<N>::
 #pragma unroll
   for (int i = 0; i < E; ++i) v[i] = my[t + TT * i];
   __syncwarp();
-  line_fft<E, TT, -1, false>(v, my, t, tws);
+  line_fft<E, TT, -1, false, false, S_::PAIR>(v, my, t, tws);
   if (live) {
 #pragma unroll
     for (int i = 0; i < H; ++i) row[t + TT * i] = v[i];  // keep iz < nz
@@ -362,7 +363,7 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_yi(XParam
 #pragma unroll
   for (int i = 0; i < E; ++i) v[i] = tile[(t + TT * i) * (RL + 1) + l];
   __syncthreads();  // the tile is consumed before the line scratch reuses it
-  line_fft<E, TT, -1, false>(v, lines + (size_t)l * P.lsy, t, tws);
+  line_fft<E, TT, -1, false, false, S_::PAIR>(v, lines + (size_t)l * P.lsy, t, tws);
   if (iz < nz) {
     C* A = P.A + (size_t)rl * P.A_rs + ((size_t)(c * nz + iz) * P.Mx + kx) * P.ny;
 #pragma unroll
@@ -426,7 +427,7 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_xi(XParam
 #pragma unroll
   for (int i = 0; i < E; ++i) v[i] = tile[(t + TT * i) * (RL + 1) + l];
   __syncthreads();
-  line_fft<E, TT, -1, false>(v, lines + (size_t)l * P.lsx, t, tws);
+  line_fft<E, TT, -1, false, false, S_::PAIR>(v, lines + (size_t)l * P.lsx, t, tws);
   if (iy >= ny) return;
   // finish (cu:116-118): y = CXADIA x - w/ngrid [+ CXAOFF terms], conj for 'C'
   C* y = P.y + (size_t)rl * P.y_rs + (size_t)c * S;
@@ -519,9 +520,10 @@ int matvec_xpipe(Engine<T>& E, const MvArgs<T>& a) {
   const int TX = rT(g.Mx), TY = rT(g.My), TZ = rT(g.Mz);
   const int RX = 256 / TX, RY = 256 / TY;
   const int RZ = std::max(1, 128 / TZ);  // ZG: 3*TZ*RZ threads
-  P.lsx = line_stride(g.Mx / TX, TX, RX, false);
-  P.lsy = line_stride(g.My / TY, TY, RY, false);
-  P.lsz = std::max(line_stride(g.Mz / TZ, TZ, RZ, false), g.Mz);
+  // must match XShape<N>::PAIR
+  P.lsx = line_stride(g.Mx / TX, TX, RX, false, TX >= 8);
+  P.lsy = line_stride(g.My / TY, TY, RY, false, TY >= 8);
+  P.lsz = std::max(line_stride(g.Mz / TZ, TZ, RZ, false, TZ >= 8), g.Mz);
   // the transpose tile and the line scratch share one region
   P.tlx = (int)std::max((size_t)g.Mx * (RX + 1), (size_t)RX * P.lsx);
   const size_t smx = ((size_t)g.Mx + P.tlx) * sizeof(C);
