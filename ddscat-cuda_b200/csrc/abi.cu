@@ -781,6 +781,15 @@ DDSCAT_CUDA_API int ddscat_b200_residual_f64(int nrhs, const void* b, const void
   return 0;
 }
 
+DDSCAT_CUDA_API int ddscat_b200_autotune_f32(int iters, float* default_ms, float* best_ms) {
+  clear_error();
+  if (!s.ready || iters <= 0 || !default_ms || !best_ms) {
+    set_error("autotune", "invalid argument or not prepared");
+    return 410;
+  }
+  return autotune_engine(s.eng, iters, default_ms, best_ms) ? 411 : 0;
+}
+
 DDSCAT_CUDA_API int ddscat_b200_matvec_timing(int nrhs, int iters, int cwhat, float* ms_per_call) {
   clear_error();
   if (!s.ready || nrhs <= 0 || iters <= 0 || !ms_per_call || (cwhat != 'N' && cwhat != 'C')) {

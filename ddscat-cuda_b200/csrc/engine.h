@@ -81,6 +81,10 @@ template <typename T> struct Engine {
   size_t slab_budget_elems = 0;
   int slices_layout = 0;
   int xpipe = 0;           // 1: x-first transposed pipeline (power-of-two grids)
+  // launch shapes of the z-first pipeline (set from the environment at
+  // prepare, changed by the autotuner): register-pass block sizes, y-pass
+  // columns per block, complex elements per generic-pass tile (0: default)
+  int tune_thz = 256, tune_thx = 256, tune_ly = 4, tune_tile = 0;
   cudaStream_t stream = 0;
   size_t bytes_allocated = 0;
 
@@ -128,6 +132,9 @@ template <typename T> void v_scatter(const cplx<T>* compact, cplx<T>* full, cons
 
 // x-first transposed pipeline (matvec_x.cu)
 template <typename T> bool xpipe_supported(const Geometry& g);
+// Times the MATVEC of a prepared FP32 engine under the launch shapes that apply
+// to its grid and keeps the fastest; default_ms / best_ms per call.
+int autotune_engine(Engine<float>& e, int iters, float* default_ms, float* best_ms);
 template <typename T> int matvec_xpipe(Engine<T>& E, const MvArgs<T>& a);
 template <typename T> int interleave_green_zfast(Engine<T>& E, const cplx<T>* planar);
 

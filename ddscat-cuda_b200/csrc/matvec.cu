@@ -586,6 +586,10 @@ int Engine<T>::init_geometry(int nx, int ny, int nz, int ipbc, int nat, int nat0
   py = make_fft_plan(g.My);
   pz = make_fft_plan(g.Mz);
   xpipe = xpipe_supported<T>(g) ? 1 : 0;
+  tune_thz = env_int("DDSCAT_B200_TH_Z", 256);
+  tune_thx = env_int("DDSCAT_B200_TH_X", 256);
+  tune_ly = std::max(1, env_int("DDSCAT_B200_LY", 4));
+  tune_tile = env_int("DDSCAT_B200_TILE", 0);
   if (px.nstages < 0 || py.nstages < 0 || pz.nstages < 0) {
     set_error("prepare", "FFT length has too many prime factors");
     return 1;
@@ -690,7 +694,7 @@ template <typename T> int Engine<T>::matvec(const MvArgs<T>& a) {
   P.px = px; P.py = py; P.pz = pz;
   P.twx = twx; P.twy = twy; P.twz = twz;
   P.inv_ngrid = (T)(1.0 / (double)g.ngrid());
-  const int tile_elems = (sizeof(C) == 8) ? 4096 : 2048;  // complex elements per 32 KiB tile
+  const int tile_elems = tune_tile > 0 ? tune_tile : ((sizeof(C) == 8) ? 4096 : 2048);  // 32 KiB by default
   P.tz = std::max(1, std::min(32, tile_elems / g.Mz));
   P.ry = std::max(1, std::min(16, tile_elems / (g.Mx + 1)));
   P.ty = std::max(1, std::min(32, (tile_elems / 2) / g.My));
@@ -702,8 +706,8 @@ template <typename T> int Engine<T>::matvec(const MvArgs<T>& a) {
   const void* fxi_r = pick_reg<T>(Pass::XI, g.Mx);
   const void* fzi_r = pick_reg<T>(Pass::ZI, g.Mz);
   // block sizes of the register passes (threads): z columns, x rows, y columns
-  const int thz = env_int("DDSCAT_B200_TH_Z", 256), thx = env_int("DDSCAT_B200_TH_X", 256);
-  const int Ly = std::max(1, env_int("DDSCAT_B200_LY", 4));  // y-pass columns per block
+  const int thz = tune_thz, thx = tune_thx;
+  const int Ly = tune_ly;  // y-pass columns per block
   const int thy = 3 * reg_T(g.My) * Ly;
   const int Lz = thz / reg_T(g.Mz), Rx = thx / reg_T(g.Mx);
   P.lsz = line_stride(reg_E(g.Mz), reg_T(g.Mz), Lz, true);
@@ -809,6 +813,84 @@ template <typename T> void Engine<T>::release() {
   cudaFree(green); cudaFree(occ); cudaFree(inv); cudaFree(iocc); cudaFree(rowq);
   cudaFree(zhat); cudaFree(slab);
   *this = Engine<T>{};
+}
+
+// ---------------------------------------------------------------- autotuner
+// Candidate launch shapes are those that change a kernel this grid uses:
+// power-of-two axes run register passes (block sizes, y columns per block),
+// the other axes run generic Stockham passes (tile size).  Each candidate is
+// timed with CUDA events over `iters` single-RHS MATVECs after two warm-up
+// calls; the x-first pipeline has no launch-shape choices and is left alone.
+int autotune_engine(Engine<float>& e, int iters, float* default_ms, float* best_ms) {
+  using C = float2;
+  const Geometry& g = e.g;
+  const size_t cn = (size_t)3 * g.nat0;
+  C *x = nullptr, *y = nullptr, *ad = nullptr;
+  cudaError_t err = cudaMalloc((void**)&x, cn * sizeof(C));
+  if (err == cudaSuccess) err = cudaMalloc((void**)&y, cn * sizeof(C));
+  if (err == cudaSuccess) err = cudaMalloc((void**)&ad, cn * sizeof(C));
+  if (err != cudaSuccess) { cudaFree(x); cudaFree(y); cudaFree(ad); set_cuda_error("autotune", err); return 1; }
+  cudaMemsetAsync(x, 0, cn * sizeof(C), e.stream);
+  cudaMemsetAsync(ad, 0, cn * sizeof(C), e.stream);
+  MvArgs<float> a;
+  a.x = x; a.x_rs = cn; a.y = y; a.y_rs = cn; a.io_full = 0;
+  a.adia = ad; a.a_rs = cn; a.a_full = 0; a.aoff = nullptr; a.conj = 0; a.nrhs = 1;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  auto time_it = [&](float* ms) -> int {
+    for (int w = 0; w < 2; ++w)
+      if (e.matvec(a)) return 1;
+    cudaEventRecord(e0, e.stream);
+    for (int i = 0; i < iters; ++i)
+      if (e.matvec(a)) return 1;
+    cudaEventRecord(e1, e.stream);
+    if (cudaEventSynchronize(e1) != cudaSuccess) return 1;
+    cudaEventElapsedTime(ms, e0, e1);
+    *ms /= iters;
+    return 0;
+  };
+  struct Shape { int thz, thx, ly, tile; };
+  const Shape def{e.tune_thz, e.tune_thx, e.tune_ly, e.tune_tile};
+  std::vector<Shape> cands{def};
+  if (!e.xpipe) {
+    const bool rz = reg_supported(g.Mz), rx = reg_supported(g.Mx), ry = reg_supported(g.My);
+    const std::vector<int> thzs = rz ? std::vector<int>{128, 256} : std::vector<int>{def.thz};
+    const std::vector<int> thxs = rx ? std::vector<int>{128, 256} : std::vector<int>{def.thx};
+    std::vector<int> lys{def.ly};
+    if (ry)
+      for (int ly : {1, 2, 4, 8})
+        if (3 * reg_T(g.My) * ly <= 384) lys.push_back(ly);
+    std::vector<int> tiles{def.tile};
+    if (!(rz && rx && ry)) tiles = {0, 1024, 4096};
+    for (int a1 : thzs)
+      for (int a2 : thxs)
+        for (int a3 : lys)
+          for (int a4 : tiles) cands.push_back({a1, a2, a3, a4});
+  }
+  int rc = 0;
+  float dms = 0.f, bms = 0.f;
+  Shape best = def;
+  for (size_t k = 0; k < cands.size() && !rc; ++k) {
+    e.tune_thz = cands[k].thz; e.tune_thx = cands[k].thx; e.tune_ly = cands[k].ly; e.tune_tile = cands[k].tile;
+    float ms = 0.f;
+    if (time_it(&ms)) {
+      if (k == 0) { rc = 1; break; }  // the default shape must run
+      cudaGetLastError();             // a rejected candidate (launch limits) is skipped
+      continue;
+    }
+    if (k == 0) { dms = bms = ms; continue; }
+    if (ms < bms) { bms = ms; best = cands[k]; }
+  }
+  e.tune_thz = best.thz; e.tune_thx = best.thx; e.tune_ly = best.ly; e.tune_tile = best.tile;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(x); cudaFree(y); cudaFree(ad);
+  if (rc) return 1;
+  *default_ms = dms;
+  *best_ms = bms;
+  clear_error();
+  return 0;
 }
 
 template struct Engine<float>;

@@ -44,7 +44,8 @@ struct Target {
 
 int multi_solve(int nt, const int* dims, const int16_t* const* iocc, const float* ak, const int* nrhs,
                 const void* const* b, void* const* x, const void* const* adia, int solver, int replace, int sym,
-                int maxit, float tol, int nthreads, int* itno, float* tole, int* ncompte, int* status) {
+                int autotune, int maxit, float tol, int nthreads, int* itno, float* tole, int* ncompte,
+                int* status) {
   const bool verbose = std::getenv("DDSCAT_B200_VERBOSE") != nullptr;
   auto now = []() { return std::chrono::steady_clock::now(); };
   const auto t0 = now();
@@ -67,6 +68,10 @@ int multi_solve(int nt, const int* dims, const int16_t* const* iocc, const float
     for (int k = 0; k < 3; ++k) ga.ak[k] = ak[3 * i + k];
     rc = t.eng.build_green(ga);
     if (rc) { cleanup(); return 543; }
+    if (autotune) {
+      float d = 0.f, bst = 0.f;
+      if (autotune_engine(t.eng, 3, &d, &bst)) { cleanup(); return 543; }
+    }
     t.eng.stream = t.st;
     t.R = nrhs[i];
     t.n = 3 * nat0;
@@ -184,12 +189,13 @@ extern "C" DDSCAT_CUDA_API int ddscat_b200_multi_solve_f32(int ntarget, const in
     }
   const int replace = (solver & DDSCAT_B200_REPLACE_RESIDUAL) != 0;
   const int sym = (solver & DDSCAT_B200_QMR_SYMMETRIC) != 0;
-  solver &= ~(DDSCAT_B200_REPLACE_RESIDUAL | DDSCAT_B200_QMR_SYMMETRIC);
+  const int tune = (solver & DDSCAT_B200_AUTOTUNE) != 0;
+  solver &= ~(DDSCAT_B200_REPLACE_RESIDUAL | DDSCAT_B200_QMR_SYMMETRIC | DDSCAT_B200_AUTOTUNE);
   if ((solver != DDSCAT_B200_QMRCCG && solver != DDSCAT_B200_PBCGS2) || (sym && solver != DDSCAT_B200_QMRCCG)) {
     set_error("multi-target solve", "unsupported solver or flag");
     return 541;
   }
   if (nthreads <= 0) nthreads = std::min(ntarget, 8);
-  return multi_solve(ntarget, dims, iocc, ak, nrhs, b, x, adia, solver, replace, sym, maxit, tol, nthreads, itno,
-                     tole, ncompte, status);
+  return multi_solve(ntarget, dims, iocc, ak, nrhs, b, x, adia, solver, replace, sym, tune, maxit, tol, nthreads,
+                     itno, tole, ncompte, status);
 }

@@ -29,7 +29,8 @@ EXPORTS = (
     + ["ddscat_b200_set_verbose", "ddscat_b200_layout", "ddscat_b200_matvec_timing", "ddscat_b200_solve_batch_f32",
        "ddscat_b200_last_solve_stats", "ddscat_b200_residual_f64", "ddscat_b200_launch_count",
        "ddscat_b200_apply_noalloc_f32", "ddscat_b200_mueller_f32", "ddscat_b200_make_inputs_f32",
-       "ddscat_b200_solve_batch_f64", "ddscat_b200_adjoint_f32", "ddscat_b200_multi_solve_f32"]
+       "ddscat_b200_solve_batch_f64", "ddscat_b200_adjoint_f32", "ddscat_b200_multi_solve_f32",
+       "ddscat_b200_autotune_f32"]
 )
 
 
@@ -99,6 +100,8 @@ def _declare(lib):
     lib.ddscat_b200_adjoint_f32.restype = _I
     lib.ddscat_b200_multi_solve_f32.argtypes = [_I, _P, _P, _P, _P, _P, _P, _P, _I, _I, _F, _I, _P, _P, _P, _P]
     lib.ddscat_b200_multi_solve_f32.restype = _I
+    lib.ddscat_b200_autotune_f32.argtypes = [_I, _P, _P]
+    lib.ddscat_b200_autotune_f32.restype = _I
     lib.ddscat_b200_launch_count.argtypes = []
     lib.ddscat_b200_launch_count.restype = ct.c_ulonglong
 
@@ -134,6 +137,7 @@ BATCH_SOLVERS = {"qmrccg": 1, "pbcgs2": 2}
 REPLACE_RESIDUAL = 0x100  # DDSCAT_B200_REPLACE_RESIDUAL
 QMR_SYMMETRIC = 0x200  # DDSCAT_B200_QMR_SYMMETRIC
 INPUTS_F64 = 0x400  # DDSCAT_B200_INPUTS_F64
+AUTOTUNE = 0x800  # DDSCAT_B200_AUTOTUNE
 
 
 def _vptr(a):
@@ -311,7 +315,7 @@ class DDA:
         return grad, lam, it, tole
 
     def multi_solve(self, targets_, name="qmrccg", maxit=1000, tol=1e-5, replace=True, symmetric=True, nthreads=0,
-                    check=True):
+                    check=True, autotune=False):
         """Solve many targets of uneven size together.  targets_: list of dicts
         with dims (nx, ny, nz), iocc (NAT int16), ak (3,), b, x, adia
         ((nrhs, 3*NAT) complex64 host arrays; x in/out).  Returns BatchOut over
@@ -337,6 +341,7 @@ class DDA:
         nc = np.zeros(total, dtype=np.int32)
         st = np.zeros(total, dtype=np.int32)
         code = BATCH_SOLVERS[name] | (REPLACE_RESIDUAL if replace else 0) | (QMR_SYMMETRIC if symmetric else 0)
+        code |= AUTOTUNE if autotune else 0
         rc = self.lib.ddscat_b200_multi_solve_f32(nt, _ptr(dims), ct.cast(po, ct.c_void_p), _ptr(aks), _ptr(nr),
                                                   ct.cast(pb, ct.c_void_p), ct.cast(px, ct.c_void_p),
                                                   ct.cast(pa, ct.c_void_p), code, maxit, tol, nthreads, _ptr(it),
@@ -397,6 +402,12 @@ class DDA:
                                               _ptr(s), m.ctypes.data_as(_D))
         self._check("mueller", rc)
         return s, m
+
+    def autotune(self, iters=5):
+        """Tune the prepared target's FFT launch shapes; returns (default ms, best ms) per MATVEC."""
+        d, b = _F(0.0), _F(0.0)
+        self._check("autotune", self.lib.ddscat_b200_autotune_f32(iters, ct.byref(d), ct.byref(b)))
+        return d.value, b.value
 
     def launch_count(self):
         return int(self.lib.ddscat_b200_launch_count())

@@ -29,6 +29,15 @@ DDSCAT_CUDA_API unsigned long long ddscat_b200_launch_count(void);
  * invalid / not prepared, 401 allocation, 402 CUDA failure. */
 DDSCAT_CUDA_API int ddscat_b200_matvec_timing(int nrhs, int iters, int cwhat, float *ms_per_call);
 
+/* FFT launch-shape autotuner for the prepared target: times `iters` MATVECs
+ * (after two warm-up calls) under every launch shape that changes a kernel the
+ * grid uses (register-pass block sizes and y-pass columns per block on
+ * power-of-two axes, generic Stockham tile sizes on the others; the x-first
+ * pipeline of all-power-of-two grids has none) and keeps the fastest for the
+ * rest of the target's life.  Writes the default and the chosen shape's time
+ * per call.  Codes: 410 invalid argument / not prepared, 411 failure. */
+DDSCAT_CUDA_API int ddscat_b200_autotune_f32(int iters, float *default_ms, float *best_ms);
+
 /* Batched solve of nrhs systems A_r x_r = b_r that share the prepared target
  * and Green tensor (same |k|; CXADIA/CXAOFF may differ per right-hand side,
  * e.g. per orientation and polarisation).  b, x (initial guess in, solution
@@ -59,6 +68,7 @@ DDSCAT_CUDA_API int ddscat_b200_matvec_timing(int nrhs, int iters, int cwhat, fl
 #define DDSCAT_B200_REPLACE_RESIDUAL 0x100
 #define DDSCAT_B200_QMR_SYMMETRIC 0x200
 #define DDSCAT_B200_INPUTS_F64 0x400
+#define DDSCAT_B200_AUTOTUNE 0x800
 DDSCAT_CUDA_API int ddscat_b200_solve_batch_f32(int solver, int nrhs, const void *b, void *x, const void *adia,
                                                 const void *aoff, int maxit, float tol, int *itno, float *tole,
                                                 int *ncompte, int *status);
@@ -168,7 +178,9 @@ DDSCAT_CUDA_API int ddscat_b200_adjoint_f32(int nrhs, const void *p, const void 
  * full vectors (3*NAT_t complex floats each).  Each target gets its own
  * engine, Green tensor and CUDA stream; nthreads host threads (0: up to 8)
  * drive the targets' batched solves concurrently, largest first.  solver and
- * flags as for ddscat_b200_solve_batch_f32; per-RHS outputs in target order.
+ * flags as for ddscat_b200_solve_batch_f32, plus DDSCAT_B200_AUTOTUNE: tune each
+ * target's FFT launch shapes before its solve (see ddscat_b200_autotune_f32);
+ * per-RHS outputs in target order.
  * The FFT3D layout is used in both libraries.  Codes: 540 invalid argument,
  * 541 solver or flag, 542 workspace, 543 geometry or Green build, 544 input
  * transfer, 545 solver failure, 546 output transfer; a breakdown returns that
