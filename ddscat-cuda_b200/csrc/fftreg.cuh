@@ -15,13 +15,17 @@
 
 namespace ddb {
 
-#include "w32.inc"
+#include "w96.inc"
 
-// W_K^m for DIR: exp(DIR * 2*pi*i*m/K), K divides 32
+// W_K^m for DIR: exp(DIR * 2*pi*i*m/K), K divides 96
 template <int K, int DIR, typename C> DDB_HD C wk(int m) {
-  const int q = (m * (32 / K)) & 31;
-  return mk<C>(w32re(q), DIR < 0 ? w32im(q) : -w32im(q));
+  static_assert(96 % K == 0, "in-register DFT sizes must divide 96");
+  const int q = (m * (96 / K)) % 96;
+  return mk<C>(w96re(q), DIR < 0 ? w96im(q) : -w96im(q));
 }
+
+// first factor of the four-step split K = K1 * K2 of an in-register DFT
+template <int K> constexpr int dft_split() { return (K == 16 || K == 12) ? 4 : 8; }
 
 template <int K, int DIR, typename C> __device__ __forceinline__ void dftr(C* v) {
   if constexpr (K == 1) {
@@ -31,9 +35,11 @@ template <int K, int DIR, typename C> __device__ __forceinline__ void dftr(C* v)
     bfly4<DIR>(v);
   } else if constexpr (K == 8) {
     bfly8<DIR>(v);
+  } else if constexpr (K == 3) {
+    bfly3<DIR>(v);
   } else {
-    // K = K1*K2: element K2*a + b ; output c + K1*d
-    constexpr int K1 = (K == 16) ? 4 : 8;
+    // K = K1*K2 (16 = 4*4, 32 = 8*4, 12 = 4*3, 24 = 8*3): element K2*a + b ; output c + K1*d
+    constexpr int K1 = dft_split<K>();
     constexpr int K2 = K / K1;
     C Y[K2][K1];
 #pragma unroll
@@ -88,7 +94,7 @@ template <int K, int DIR, typename C> __device__ __forceinline__ void dftr_h(C* 
     v[7] = vsub(e[3], t3);
   } else {
     // K = K1*K2, element K2*a + b is zero for a >= K1/2
-    constexpr int K1 = (K == 16) ? 4 : 8;
+    constexpr int K1 = dft_split<K>();
     constexpr int K2 = K / K1;
     C Y[K2][K1];
 #pragma unroll
@@ -218,7 +224,20 @@ template <> struct RegShape<64> { static constexpr int E = 8, T = 8; };
 template <> struct RegShape<128> { static constexpr int E = 16, T = 8; };
 template <> struct RegShape<256> { static constexpr int E = 16, T = 16; };
 template <> struct RegShape<512> { static constexpr int E = 32, T = 16; };
+// 3 * 2^k lengths (x-first pipeline only)
+template <> struct RegShape<48> { static constexpr int E = 12, T = 4; };
+template <> struct RegShape<96> { static constexpr int E = 24, T = 4; };
+template <> struct RegShape<192> { static constexpr int E = 24, T = 8; };
 
 inline bool reg_supported(int n) { return n == 16 || n == 32 || n == 64 || n == 128 || n == 256 || n == 512; }
+inline bool xreg_supported(int n) { return reg_supported(n) || n == 48 || n == 96 || n == 192; }
+// threads per line of the register shape of length n (RegShape<n>::T)
+inline int reg_threads(int n) {
+  switch (n) {
+    case 16: case 32: case 48: case 96: return 4;
+    case 64: case 128: case 192: return 8;
+    default: return 16;
+  }
+}
 
 }  // namespace ddb

@@ -48,7 +48,6 @@ template <typename T> struct XParams {
   const cplx<T>* twy;
   const cplx<T>* twz;
   int lsx, lsy, lsz;  // line strides of the x, y, z passes
-  int my_log2;        // log2(My)
   int tlx;            // tile / line scratch elements of the x passes
   T inv_ngrid;
 };
@@ -68,7 +67,7 @@ template <int N> struct XShape {
   static constexpr int E = RegShape<N>::E, TT = RegShape<N>::T, H = E / 2;
   static constexpr int RL = 256 / TT;
   static constexpr int RZ = (128 / TT) > 1 ? 128 / TT : 1;  // ZG lines per block (3*TT*RZ threads)
-  static constexpr int ZG_MINB = E >= 32 ? 2 : 3;             // ZG blocks per SM the registers must allow
+  static constexpr int ZG_MINB = E >= 24 ? 2 : 3;             // ZG blocks per SM the registers must allow
   static constexpr bool PAIR = TT >= 8;                      // 128-bit transpose stores (conflict-free for TT >= 8)
 };
 
@@ -292,7 +291,8 @@ __global__ void __launch_bounds__(3 * XShape<N>::TT * XShape<N>::RZ, XShape<N>::
     const int gl = threadIdx.x / GT, gk = threadIdx.x - GT * (threadIdx.x / GT);
     const int pl = blockIdx.y * RL + gl;
     if (pl < nlines) {
-      const int kx = P.kx0 + (pl >> P.my_log2), ky = pl & (P.My - 1);
+      const int kxl = pl / P.My;  // My need not be a power of two (3 * 2^k lengths)
+      const int kx = P.kx0 + kxl, ky = pl - kxl * P.My;
       C* L0 = lines + (size_t)gl * P.lsz;
       C* L1 = L0 + (size_t)RL * P.lsz;
       C* L2 = L1 + (size_t)RL * P.lsz;
@@ -476,15 +476,18 @@ template <typename T> static const void* xkernel(XPass p, int n) {
   switch (n) {
     case 16: return xk<T, 16>(p);
     case 32: return xk<T, 32>(p);
+    case 48: return xk<T, 48>(p);
     case 64: return xk<T, 64>(p);
+    case 96: return xk<T, 96>(p);
     case 128: return xk<T, 128>(p);
+    case 192: return xk<T, 192>(p);
     case 256: return xk<T, 256>(p);
     case 512: return xk<T, 512>(p);
     default: return nullptr;
   }
 }
 
-static int rT(int n) { return n <= 32 ? 4 : (n <= 128 ? 8 : 16); }
+static int rT(int n) { return reg_threads(n); }
 
 template <typename T> static int xlaunch(const void* f, dim3 g, int th, size_t sm, cudaStream_t st, XParams<T>& P) {
   raise_smem_limit(f);
@@ -498,7 +501,7 @@ template <typename T> static int xlaunch(const void* f, dim3 g, int th, size_t s
 template <typename T> bool xpipe_supported(const Geometry& g) {
   if (std::getenv("DDSCAT_B200_ZFIRST")) return false;
   if (sizeof(T) == 8) return false;  // the FP64 engine keeps the generic z-first pipeline
-  auto ok = [](int n) { return reg_supported(n); };
+  auto ok = [](int n) { return xreg_supported(n); };
   return ok(g.Mx) && ok(g.My) && ok(g.Mz);
 }
 
@@ -529,8 +532,6 @@ int matvec_xpipe(Engine<T>& E, const MvArgs<T>& a) {
   const size_t smx = ((size_t)g.Mx + P.tlx) * sizeof(C);
   const size_t smxi = smx + ((size_t)RX * g.nx <= (size_t)XI_STAGE_MAX ? (size_t)2 * RX * g.nx * sizeof(C) : 0);
   const size_t smy = ((size_t)g.My + std::max((size_t)g.My * (RY + 1), (size_t)RY * P.lsy)) * sizeof(C);
-  P.my_log2 = 0;
-  while ((1 << P.my_log2) < g.My) ++P.my_log2;
   const size_t smz = ((size_t)g.Mz + (size_t)3 * RZ * P.lsz) * sizeof(C);
   const void* fxf = xkernel<T>(XPass::XF, g.Mx);
   const void* fyf = xkernel<T>(XPass::YF, g.My);

@@ -39,7 +39,9 @@ def _err(y, yr):
 @pytest.mark.parametrize("dims,idipint", [((4, 4, 4), 0), ((5, 3, 4), 0), ((6, 5, 7), 1), ((7, 11, 13), 0),
                                           ((8, 8, 8), 0), ((12, 10, 9), 1), ((16, 16, 16), 0), ((24, 18, 30), 0),
                                           ((32, 32, 32), 0), ((16, 8, 32), 1), ((64, 32, 16), 0), ((8, 64, 16), 0),
-                                          ((128, 16, 8), 1), ((64, 64, 64), 0)])
+                                          ((128, 16, 8), 1), ((64, 64, 64), 0),
+                                          # 3 * 2^k padded lengths (x-first pipeline with 12/24-point DFTs)
+                                          ((24, 24, 24), 0), ((48, 24, 96), 1), ((96, 32, 24), 0), ((48, 48, 48), 0)])
 def test_apply_matches_oracle(layout, dims, idipint):
     iocc, ak, x, adia, aoff, gp = _case(dims, idipint)
     dda = D.DDA(layout)
