@@ -139,11 +139,27 @@ def fft_friendly(n):
         m += 1
 
 
-def embed_ellipsoid(sides, semi):
+FAST_SIDES = (8, 12, 16, 24, 32, 48, 64, 96, 128, 256)
+
+
+def fast_side(n):
+    """Smallest grid side >= n whose padded FFT length 2*side runs on the
+    x-first register pipeline (2^k and 3*2^k lengths); falls back to
+    fft_friendly above 256."""
+    for s in FAST_SIDES:
+        if s >= n:
+            return s
+    return fft_friendly(n)
+
+
+def embed_ellipsoid(sides, semi, grid="fast"):
     """(grid dims, IOCC) of an ellipsoid filling a box of the given lattice
-    sides, placed in a grid extended to FFT-friendly sizes (vacuum padding)."""
+    sides, placed in a grid extended with vacuum: grid='fast' picks the sides
+    of the fast MATVEC path (fast_side), grid='friendly' DDSCAT's 2^a 3^b 5^c
+    sizes (fft_friendly)."""
     sx, sy, sz = (int(v) for v in sides)
-    gx, gy, gz = fft_friendly(sx), fft_friendly(sy), fft_friendly(sz)
+    ext = fast_side if grid == "fast" else fft_friendly
+    gx, gy, gz = ext(sx), ext(sy), ext(sz)
     box = ellipsoid_occupancy(sx, sy, sz, semi).reshape(sz, sy, sx)
     occ = np.zeros((gz, gy, gx), dtype=np.int16)
     occ[:sz, :sy, :sx] = box
