@@ -56,6 +56,8 @@ def parse_args():
     ap.add_argument("--qmr-form", default="symmetric", choices=["symmetric", "two-product"],
                     help="QMRCCG: one MATVEC per iteration (left Lanczos vectors = right ones, A^T = A) or the "
                          "reference's two-product form")
+    ap.add_argument("--graph", default="on", choices=["on", "off"],
+                    help="QMRCCG symmetric form with replacement: device-driven iterations launched as a CUDA graph")
     ap.add_argument("--ref-rhs", type=int, default=0, help="RHS per step of the reference arm (0: the whole batch)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-q-check", action="store_true", help="skip the all-FP64 reference solve and Q errors")
@@ -187,7 +189,9 @@ def config(args, prob, R, world):
             "l2": "inputs larger than L2 (each RHS vector 3*NAT*8 B > 50 MB; working set > 1 GB)",
             "parallelism": f"replicas x{world} (independent RHS batches per GPU)",
             "reliable_residual_policy": getattr(args, "policy", "restart"),
-            "qmr_form": getattr(args, "qmr_form", "two-product") if args.solver == "qmrccg" else None}
+            "qmr_form": getattr(args, "qmr_form", "two-product") if args.solver == "qmrccg" else None,
+            "iteration_launch": ("CUDA graph, device-driven scalars" if getattr(args, "graph", "off") == "on"
+                                 and args.solver == "qmrccg" else "host-driven")}
 
 
 def algorithmic_bytes_per_matvec(prob, rhs_per_call):
@@ -269,8 +273,9 @@ def run_ours(args):
         """One step: batched solve, FP64 true residuals, re-solve failures."""
         rep = args.policy == "replace"
         sym = args.solver == "qmrccg" and args.qmr_form == "symmetric"
+        gr = sym and rep and args.graph == "on"
         out = dda.solve_batch(args.solver, bx, xx, ax, None, maxit=args.maxit, tol=args.tol, replace=rep,
-                              symmetric=sym)
+                              symmetric=sym, graph=gr)
         ms, rhs, calls = dda.last_solve_stats()
         stats["mv_ms"] += ms
         stats["mv_rhs"] += rhs
@@ -284,7 +289,7 @@ def run_ours(args):
             sub = (lambda a: a[bad].contiguous()) if on_device else (lambda a: np.ascontiguousarray(a[bad]))
             xs = sub(xx)
             o2 = dda.solve_batch(args.solver, sub(bx), xs, sub(ax), None, maxit=args.maxit, tol=tol, replace=rep,
-                                 symmetric=sym)
+                                 symmetric=sym, graph=gr)
             xx[bad] = xs
             out.itno[bad] += o2.itno
             out.ncompte[bad] += o2.ncompte

@@ -31,6 +31,7 @@ const char* last_error_text() { return g_last_error.c_str(); }
 void clear_error() { g_last_error.clear(); }
 static std::atomic<unsigned long long> g_launches{0};
 void note_launch(unsigned long long k) { g_launches += k; }
+unsigned long long launch_total() { return g_launches.load(); }
 // raise the dynamic shared-memory limit of kernel f once per process (thread-safe)
 void raise_smem_limit(const void* f) {
   static std::mutex mu;
@@ -672,7 +673,8 @@ DDSCAT_CUDA_API int ddscat_b200_solve_batch_f32(int solver, int nrhs, const void
   }
   const int replace = (solver & DDSCAT_B200_REPLACE_RESIDUAL) != 0;
   const int sym = (solver & DDSCAT_B200_QMR_SYMMETRIC) != 0;
-  solver &= ~(DDSCAT_B200_REPLACE_RESIDUAL | DDSCAT_B200_QMR_SYMMETRIC);
+  const int graph = (solver & DDSCAT_B200_GRAPH) != 0;
+  solver &= ~(DDSCAT_B200_REPLACE_RESIDUAL | DDSCAT_B200_QMR_SYMMETRIC | DDSCAT_B200_GRAPH);
   if (sym && solver != DDSCAT_B200_QMRCCG) {
     set_error("batched solve", "DDSCAT_B200_QMR_SYMMETRIC applies to QMRCCG only");
     return 501;
@@ -699,6 +701,7 @@ DDSCAT_CUDA_API int ddscat_b200_solve_batch_f32(int solver, int nrhs, const void
   io.b = bs.b; io.x = bs.x; io.adia = bs.adia; io.aoff = use_aoff ? bs.aoff : nullptr;
   io.work = bs.work; io.nwork = BATCH_WORK_VECTORS;
   io.maxit = maxit; io.tol = (double)tol; io.verbose = s.verbose; io.replace = replace; io.sym = sym;
+  io.graph = graph;
   BatchResult res;
   const int rc = solver == DDSCAT_B200_QMRCCG ? solve_batch_qmrccg<float>(io, res) : solve_batch_pbcgs2<float>(io, res);
   bs.matvec_ms = io.matvec_ms;

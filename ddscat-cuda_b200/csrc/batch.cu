@@ -439,6 +439,325 @@ static bool any_of(const std::vector<int>& m) {
 }
 
 // --------------------------------------------------------------------------
+// Device-driven one-MATVEC QMRCCG iteration (residual replacement), captured in
+// a CUDA graph.  The per-RHS scalar recurrence, the masks and the reliable-
+// residual bookkeeping run in single-thread kernels on FP64 state held on the
+// GPU, so an iteration needs no host round trip; the reliable-residual check
+// (a masked MATVEC, two norms and the replacement) sits in an IF conditional
+// node that k_qg_post arms only when some RHS needs a check.  The host
+// launches the graph repeatedly and reads the active-RHS count every few
+// launches.  Arithmetic is that of the host-driven form (FP64 scalars).
+struct QGState {
+  double2 *gamma, *ksi, *rho, *eps, *mu, *tau, *lambda, *kappa, *theta;
+  double2 *co;           // [7][R]: p/q/v coefficients (5), d/s coefficients (2)
+  double2 *one, *mone;   // [R]
+  double *bnorm, *resid;
+  int *it, *live, *status, *nc, *I, *CK, *RP;
+  int *active, *checks;  // [1] each
+};
+
+__device__ __forceinline__ double2 dmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__device__ __forceinline__ double2 ddiv(double2 a, double2 b) {
+  const double d = b.x * b.x + b.y * b.y;
+  return make_double2((a.x * b.x + a.y * b.y) / d, (a.y * b.x - a.x * b.y) / d);
+}
+__device__ __forceinline__ double2 dsc(double s, double2 a) { return make_double2(s * a.x, s * a.y); }
+__device__ __forceinline__ bool dz0(double2 a) { return a.x == 0.0 && a.y == 0.0; }
+
+// I = live and it < maxit and resid > tol; coefficients of the p/q/v step
+__global__ void k_qg_begin(int R, int maxit, double tol, QGState S) {
+  for (int r = threadIdx.x; r < R; r += blockDim.x) {
+    const int on = S.live[r] && S.it[r] < maxit && S.resid[r] > tol;
+    S.I[r] = on;
+    if (!on) continue;
+    S.it[r] += 1;
+    S.nc[r] += 1;
+    const double2 g = S.gamma[r], k = S.ksi[r], mu = S.mu[r], t = S.tau[r];
+    const double2 one = make_double2(1.0, 0.0);
+    S.co[r] = dsc(-1.0, mu);                          // -mu
+    S.co[R + r] = ddiv(one, g);                       // 1/gamma
+    S.co[2 * R + r] = dsc(-1.0, ddiv(dmul(g, mu), k));  // -(gamma mu)/ksi
+    S.co[3 * R + r] = ddiv(one, k);                   // 1/ksi
+    S.co[4 * R + r] = dsc(-1.0, ddiv(t, g));          // -(tau/gamma)
+  }
+}
+
+// scalar recurrence from |vt|^2, vt^T vt (out slots 2, 3) and vt^T A vt (slot 0)
+__global__ void k_qg_scalars(int R, QGState S, const double2* out) {
+  for (int r = threadIdx.x; r < R; r += blockDim.x) {
+    if (!S.I[r]) continue;
+    const double2 gamma0 = S.gamma[r], ksi0 = S.ksi[r], rho0 = S.rho[r], tau0 = S.tau[r], kappa0 = S.kappa[r];
+    const double g2 = out[(size_t)r * 8 + 2].x;
+    const double2 gam = make_double2(sqrt(fmax(0.0, g2)), 0.0);
+    const double2 ksi = gam;  // left Lanczos vectors equal the right ones
+    const double2 rho = out[(size_t)r * 8 + 3], eps = out[(size_t)r * 8];
+    S.gamma[r] = gam; S.ksi[r] = ksi; S.rho[r] = rho; S.eps[r] = eps;
+    int st = 0;
+    if (dz0(gam)) st = 6;
+    const double2 den = dmul(dmul(gam, S.tau[r]), rho0);
+    if (!st && dz0(den)) st = 12;
+    double2 mu = S.mu[r];
+    if (!st) { mu = ddiv(dmul(dmul(gamma0, ksi0), rho), den); if (dz0(rho)) st = 13; }
+    double2 theta = S.theta[r], kappa = kappa0, lambda = S.lambda[r], tau = S.tau[r];
+    if (!st) {
+      const double2 gm = dmul(gam, mu);
+      tau = ddiv(eps, rho);
+      tau = make_double2(tau.x - gm.x, tau.y - gm.y);
+      const double at0 = tau0.x * tau0.x + tau0.y * tau0.y, ag = gam.x * gam.x + gam.y * gam.y;
+      const double2 den2 = make_double2(lambda.x * at0 + ag, lambda.y * at0);
+      if (dz0(den2)) st = 14;
+      else {
+        theta = ddiv(make_double2((1.0 - lambda.x) * at0, -lambda.y * at0), den2);
+        kappa = dsc(-1.0, ddiv(dmul(dmul(gamma0, make_double2(tau0.x, -tau0.y)), kappa0), den2));
+        lambda = ddiv(make_double2(lambda.x * at0, lambda.y * at0), den2);
+      }
+    }
+    S.mu[r] = mu; S.tau[r] = tau; S.theta[r] = theta; S.kappa[r] = kappa; S.lambda[r] = lambda;
+    if (st) { S.status[r] = 58; S.live[r] = 0; S.I[r] = 0; }
+    S.co[5 * R + r] = theta;
+    S.co[6 * R + r] = kappa;
+  }
+}
+
+// recursive residual, the check mask and the IF condition of the check body
+__global__ void k_qg_post(int R, double tol, QGState S, const double2* out, cudaGraphConditionalHandle h) {
+  if (threadIdx.x != 0) return;
+  int any = 0;
+  for (int r = 0; r < R; ++r) {
+    int ck = 0;
+    if (S.I[r]) {
+      S.resid[r] = sqrt(fmax(0.0, out[(size_t)r * 8].x)) / S.bnorm[r];
+      ck = (S.it[r] % 20) == 0 || S.resid[r] <= tol;
+      if (ck) S.nc[r] += 1;
+    }
+    S.CK[r] = ck;
+    S.RP[r] = 0;
+    any |= ck;
+  }
+  if (any) *S.checks += 1;
+  cudaGraphSetConditional(h, any ? 1u : 0u);
+}
+
+// decisions of the reliable-residual check from |b - A x|^2, |b - A x - r|^2
+__global__ void k_qg_check(int R, double tol, QGState S, const double2* out) {
+  for (int r = threadIdx.x; r < R; r += blockDim.x) {
+    if (!S.CK[r]) continue;
+    const double tr = sqrt(fmax(0.0, out[(size_t)r * 8].x)), gapn = sqrt(fmax(0.0, out[(size_t)r * 8 + 1].x));
+    const double tres = tr / S.bnorm[r];
+    const double gap = tr > 0.0 ? gapn / tr : (gapn == 0.0 ? 0.0 : INFINITY);
+    const bool conv = tres <= tol;
+    const bool rest = gap >= 1.0e-3 || (S.resid[r] <= tol && !conv);
+    if (conv) { S.resid[r] = tres; S.live[r] = 0; continue; }
+    if (rest) { S.RP[r] = 1; S.resid[r] = tres; }
+  }
+}
+
+__global__ void k_qg_count(int R, int maxit, double tol, QGState S) {
+  if (threadIdx.x != 0) return;
+  int c = 0;
+  for (int r = 0; r < R; ++r) c += S.live[r] && S.it[r] < maxit && S.resid[r] > tol;
+  *S.active = c;
+}
+
+// Runs the iterations of the one-MATVEC QMRCCG with residual replacement from
+// the state the host-driven setup produced, until no RHS is active.
+template <typename T>
+static int qmr_graph_loop(BatchIO<T>& io, BatchOps<T>& ops, std::vector<int>& nc, cplx<T>* const* w,
+                          cplx<T>* xs, std::vector<Z>* sc, std::vector<double>& bnorm, std::vector<double>& resid,
+                          std::vector<int>& it, std::vector<int>& live, std::vector<int>& status) {
+  using C = cplx<T>;
+  const int R = io.R, n = io.n;
+  C *r = w[0], *p = w[1], *q = w[3], *d = w[4], *s = w[5], *vt = w[6], *atw = w[8], *sy = w[9];
+  // device state
+  const size_t nz2 = (size_t)(9 + 7 + 2) * R, nd = (size_t)2 * R, ni = (size_t)7 * R + 2;
+  unsigned char* blk = nullptr;
+  cudaError_t e = cudaMalloc((void**)&blk, nz2 * sizeof(double2) + nd * sizeof(double) + ni * sizeof(int));
+  if (e != cudaSuccess) { set_cuda_error("graph solve state", e); return 1; }
+  QGState S;
+  double2* z = reinterpret_cast<double2*>(blk);
+  double2** zp[9] = {&S.gamma, &S.ksi, &S.rho, &S.eps, &S.mu, &S.tau, &S.lambda, &S.kappa, &S.theta};
+  for (int k = 0; k < 9; ++k) *zp[k] = z + (size_t)k * R;
+  S.co = z + (size_t)9 * R;
+  S.one = z + (size_t)16 * R;
+  S.mone = z + (size_t)17 * R;
+  double* dd = reinterpret_cast<double*>(z + nz2);
+  S.bnorm = dd; S.resid = dd + R;
+  int* ii = reinterpret_cast<int*>(dd + nd);
+  int** ip[7] = {&S.it, &S.live, &S.status, &S.nc, &S.I, &S.CK, &S.RP};
+  for (int k = 0; k < 7; ++k) *ip[k] = ii + (size_t)k * R;
+  S.active = ii + (size_t)7 * R;
+  S.checks = S.active + 1;
+  {
+    std::vector<double2> hz(nz2, make_double2(0, 0));
+    for (int k = 0; k < 9; ++k)
+      for (int i = 0; i < R; ++i) hz[(size_t)k * R + i] = dz(sc[k][i]);
+    for (int i = 0; i < R; ++i) { hz[(size_t)16 * R + i] = make_double2(1, 0); hz[(size_t)17 * R + i] = make_double2(-1, 0); }
+    std::vector<double> hd(nd);
+    for (int i = 0; i < R; ++i) { hd[i] = bnorm[i]; hd[R + i] = resid[i]; }
+    std::vector<int> hi(ni, 0);
+    for (int i = 0; i < R; ++i) {
+      hi[i] = it[i]; hi[R + i] = live[i]; hi[2 * R + i] = status[i]; hi[3 * R + i] = nc[i];
+    }
+    e = cudaMemcpy(z, hz.data(), nz2 * sizeof(double2), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(dd, hd.data(), nd * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(ii, hi.data(), ni * sizeof(int), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) { cudaFree(blk); set_cuda_error("graph solve state", e); return 1; }
+  }
+  cudaStream_t st = nullptr, st2 = nullptr;
+  cudaStreamSynchronize(ops.stream);
+  e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { cudaFree(blk); set_cuda_error("graph solve streams", e); return 1; }
+  Engine<T>& eng = *io.eng;
+  const cudaStream_t eng_st = eng.stream;
+  MvArgs<T> mv;
+  mv.x = vt; mv.x_rs = n; mv.y = atw; mv.y_rs = n; mv.io_full = 0;
+  mv.adia = io.adia; mv.aoff = io.aoff; mv.a_rs = n; mv.a_full = 0; mv.conj = 0; mv.mask = S.live; mv.nrhs = R;
+  // MATVEC time of this batch (all RHS live), measured on this stream before the captured iterations
+  float per_call = 0.f;
+  int rc = 0;
+  {
+    eng.stream = st;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    rc = eng.matvec(mv);  // warm-up; A vt is recomputed by the first iteration anyway
+    cudaEventRecord(e0, st);
+    if (!rc) rc = eng.matvec(mv);
+    cudaEventRecord(e1, st);
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(&per_call, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  // (the two calls recomputed A vt, which atw already held)
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  unsigned long long kernels_a = 0, kernels_b = 0;
+  const double tol = io.tol;
+  const int maxit = io.maxit;
+  const unsigned gb = (unsigned)std::max<size_t>(1, std::min<size_t>(ceil_div(n, BT), std::max(1, 2368 / R)));
+  if (!rc) {
+    e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    cudaGraphConditionalHandle h = 0;
+    if (e == cudaSuccess) e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps);
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, graph, 0, cudaGraphCondAssignDefault);
+    const unsigned long long c0 = launch_total();
+    if (e == cudaSuccess) {
+      k_qg_begin<<<1, 256, 0, st>>>(R, maxit, tol, S);
+      note_launch();
+      kq_pqv<C><<<dim3(ops.nb, R), BT, 0, st>>>(n, p, q, vt, atw, S.co, S.I, 2, ops.d_part, ops.d_out, ops.d_cnt);
+      note_launch();
+      mv.x = vt; mv.y = atw; mv.mask = S.I;
+      rc = eng.matvec(mv);
+      BDot<T> sp{};
+      sp.K = 1; sp.mode = 0; sp.a[0] = vt; sp.b[0] = atw; sp.conj[0] = 0;
+      kb_dots<T><<<dim3(ops.nb, R), BT, 0, st>>>(n, sp, S.I, ops.d_part, ops.d_out, ops.d_cnt);
+      note_launch();
+      k_qg_scalars<<<1, 256, 0, st>>>(R, S, ops.d_out);
+      note_launch();
+      kq_dsxr<C><<<dim3(ops.nb, R), BT, 0, st>>>(n, d, s, xs, r, p, q, S.co + 5 * (size_t)R, S.I, 0, ops.d_part,
+                                                 ops.d_out, ops.d_cnt);
+      note_launch();
+      k_qg_post<<<1, 32, 0, st>>>(R, tol, S, ops.d_out, h);
+      note_launch();
+      kernels_a = launch_total() - c0;
+      // IF node: the reliable-residual check
+      e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps);
+      cudaGraphNodeParams cp{};
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = h;
+      cp.conditional.type = cudaGraphCondTypeIf;
+      cp.conditional.size = 1;
+      cudaGraphNode_t cnode = nullptr;
+      if (e == cudaSuccess) e = cudaGraphAddNode(&cnode, graph, deps, ndeps, &cp);
+      if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(st, &cnode, 1, cudaStreamSetCaptureDependencies);
+      if (e == cudaSuccess) {
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        e = cudaStreamBeginCaptureToGraph(st2, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+          const unsigned long long c1 = launch_total();
+          eng.stream = st2;
+          MvArgs<T> ck = mv;
+          ck.x = xs; ck.y = sy; ck.mask = S.CK;
+          if (!rc) rc = eng.matvec(ck);
+          BDot<T> dn{};
+          dn.K = 2; dn.mode = 1; dn.a[0] = io.b; dn.b[0] = sy; dn.c[0] = r;
+          kb_dots<T><<<dim3(ops.nb, R), BT, 0, st2>>>(n, dn, S.CK, ops.d_part, ops.d_out, ops.d_cnt);
+          note_launch();
+          k_qg_check<<<1, 256, 0, st2>>>(R, tol, S, ops.d_out);
+          note_launch();
+          kb_lin<C><<<dim3(gb, R), BT, 0, st2>>>(n, r, nullptr, io.b, S.one, sy, S.mone, S.RP);
+          note_launch();
+          kernels_b = launch_total() - c1;
+          cudaGraph_t body_out = nullptr;
+          e = cudaStreamEndCapture(st2, &body_out);
+          eng.stream = st;
+        }
+      }
+      if (e == cudaSuccess) {
+        k_qg_count<<<1, 32, 0, st>>>(R, maxit, tol, S);
+        note_launch();
+        kernels_a += 1;
+      }
+    }
+    cudaGraph_t g_out = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(st, &g_out);
+    if (e == cudaSuccess) e = e2;
+    graph = g_out;
+    if (e == cudaSuccess && !rc) e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e != cudaSuccess) { set_cuda_error("graph solve capture", e); rc = 1; }
+  }
+  // capture only recorded the launches: the counter counts executions below
+  if (!rc) {
+    int* h_active = nullptr;
+    e = cudaMallocHost((void**)&h_active, sizeof(int));
+    long long launches = 0;
+    const long long cap = (long long)maxit + 64;  // every RHS stops at maxit; the loop is bounded
+    while (e == cudaSuccess && launches < cap) {
+      for (int k = 0; k < 4 && e == cudaSuccess; ++k, ++launches) e = cudaGraphLaunch(exec, st);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(h_active, S.active, sizeof(int), cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess || *h_active == 0) break;
+    }
+    int checks = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&checks, S.checks, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) { set_cuda_error("graph solve", e); rc = 1; }
+    note_launch((unsigned long long)launches * kernels_a + (unsigned long long)checks * kernels_b);
+    cudaFreeHost(h_active);
+    if (!rc) {
+      std::vector<double> hd(nd);
+      std::vector<int> hi(ni);
+      std::vector<double2> hz(nz2);
+      e = cudaMemcpy(hd.data(), dd, nd * sizeof(double), cudaMemcpyDeviceToHost);
+      if (e == cudaSuccess) e = cudaMemcpy(hi.data(), ii, ni * sizeof(int), cudaMemcpyDeviceToHost);
+      if (e != cudaSuccess) { set_cuda_error("graph solve state", e); rc = 1; }
+      long long mv_rhs = 0;
+      for (int i = 0; i < R && !rc; ++i) {
+        resid[i] = hd[R + i];
+        it[i] = hi[i]; live[i] = hi[R + i]; status[i] = hi[2 * R + i];
+        mv_rhs += hi[3 * R + i] - nc[i];
+        nc[i] = hi[3 * R + i];
+      }
+      io.matvec_rhs += mv_rhs;
+      io.matvec_calls += (int)(launches + checks);
+      io.matvec_ms += (double)per_call * (double)mv_rhs / (double)R;
+    }
+  }
+  if (exec) cudaGraphExecDestroy(exec);
+  if (graph) cudaGraphDestroy(graph);
+  eng.stream = eng_st;
+  cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
+  cudaStreamDestroy(st2);
+  cudaFree(blk);
+  return rc;
+}
+
+// --------------------------------------------------------------------------
 // QMRCCG (per RHS: solvers.cu solve_qmrccg, reference cu:434-443, cu:1071-1103)
 template <typename T> int solve_batch_qmrccg(BatchIO<T>& io, BatchResult& res) {
   using C = cplx<T>;
@@ -531,7 +850,13 @@ template <typename T> int solve_batch_qmrccg(BatchIO<T>& io, BatchResult& res) {
       if (live[i]) resid[i] = std::sqrt(std::max(0.0, o[i].x)) / bnorm[i];
   }
   std::vector<int> it(R, 0);
-  for (;;) {
+  const bool use_graph = io.graph && sym && io.replace;
+  if (use_graph) {
+    C* wv[10] = {c.w(0), c.w(1), c.w(2), c.w(3), c.w(4), c.w(5), c.w(6), c.w(7), c.w(8), c.w(9)};
+    std::vector<Z> sc[9] = {gamma, ksi, rho, eps, mu, tau, lambda, kappa, theta};
+    if ((rc = qmr_graph_loop<T>(io, ops, c.nc, wv, xs, sc, bnorm, resid, it, live, res.status))) return rc;
+  }
+  for (; !use_graph;) {
     std::vector<int> I(R, 0);
     for (int i = 0; i < R; ++i) I[i] = live[i] && it[i] < io.maxit && resid[i] > io.tol;
     if (!any_of(I)) break;

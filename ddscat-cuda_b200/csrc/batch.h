@@ -85,6 +85,9 @@ template <typename T> struct BatchIO {
   // right ones since A^T = A and both start from r0), 0 = the reference's
   // two-product form.
   int sym = 0;
+  // QMRCCG with sym and replace: 1 = device-driven iterations launched as a
+  // CUDA graph (no host round trip per iteration)
+  int graph = 0;
   double matvec_ms = 0.0;         // CUDA-event time of the MATVECs inside the solve
   long long matvec_rhs = 0;       // RHS-MATVECs performed
   int matvec_calls = 0;

@@ -27,6 +27,7 @@ const char* last_error_text();
 void clear_error();
 int check_launch(const char* where);
 void raise_smem_limit(const void* f);  // thread-safe, once per kernel
+unsigned long long launch_total();     // kernels launched so far (note_launch counter)
 // count of kernels this library launched (reported by ddscat_b200_launch_count)
 void note_launch(unsigned long long k = 1);
 

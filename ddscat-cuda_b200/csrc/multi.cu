@@ -44,7 +44,7 @@ struct Target {
 
 int multi_solve(int nt, const int* dims, const int16_t* const* iocc, const float* ak, const int* nrhs,
                 const void* const* b, void* const* x, const void* const* adia, int solver, int replace, int sym,
-                int autotune, int maxit, float tol, int nthreads, int* itno, float* tole, int* ncompte,
+                int autotune, int graph, int maxit, float tol, int nthreads, int* itno, float* tole, int* ncompte,
                 int* status) {
   const bool verbose = std::getenv("DDSCAT_B200_VERBOSE") != nullptr;
   auto now = []() { return std::chrono::steady_clock::now(); };
@@ -116,7 +116,7 @@ int multi_solve(int nt, const int* dims, const int16_t* const* iocc, const float
       io.eng = &t.eng; io.ops = &t.ops; io.R = t.R; io.n = t.n;
       io.b = t.b; io.x = t.x; io.adia = t.adia; io.aoff = nullptr;
       io.work = t.work; io.nwork = BATCH_WORK_VECTORS;
-      io.maxit = maxit; io.tol = (double)tol; io.replace = replace; io.sym = sym;
+      io.maxit = maxit; io.tol = (double)tol; io.replace = replace; io.sym = sym; io.graph = graph;
       BatchResult res;
       int rc = solver == DDSCAT_B200_QMRCCG ? solve_batch_qmrccg<float>(io, res) : solve_batch_pbcgs2<float>(io, res);
       const int i = order[k];
@@ -190,12 +190,13 @@ extern "C" DDSCAT_CUDA_API int ddscat_b200_multi_solve_f32(int ntarget, const in
   const int replace = (solver & DDSCAT_B200_REPLACE_RESIDUAL) != 0;
   const int sym = (solver & DDSCAT_B200_QMR_SYMMETRIC) != 0;
   const int tune = (solver & DDSCAT_B200_AUTOTUNE) != 0;
-  solver &= ~(DDSCAT_B200_REPLACE_RESIDUAL | DDSCAT_B200_QMR_SYMMETRIC | DDSCAT_B200_AUTOTUNE);
+  const int graph = (solver & DDSCAT_B200_GRAPH) != 0;
+  solver &= ~(DDSCAT_B200_REPLACE_RESIDUAL | DDSCAT_B200_QMR_SYMMETRIC | DDSCAT_B200_AUTOTUNE | DDSCAT_B200_GRAPH);
   if ((solver != DDSCAT_B200_QMRCCG && solver != DDSCAT_B200_PBCGS2) || (sym && solver != DDSCAT_B200_QMRCCG)) {
     set_error("multi-target solve", "unsupported solver or flag");
     return 541;
   }
   if (nthreads <= 0) nthreads = std::min(ntarget, 8);
-  return multi_solve(ntarget, dims, iocc, ak, nrhs, b, x, adia, solver, replace, sym, tune, maxit, tol, nthreads,
-                     itno, tole, ncompte, status);
+  return multi_solve(ntarget, dims, iocc, ak, nrhs, b, x, adia, solver, replace, sym, tune, graph, maxit, tol,
+                     nthreads, itno, tole, ncompte, status);
 }

@@ -138,6 +138,7 @@ REPLACE_RESIDUAL = 0x100  # DDSCAT_B200_REPLACE_RESIDUAL
 QMR_SYMMETRIC = 0x200  # DDSCAT_B200_QMR_SYMMETRIC
 INPUTS_F64 = 0x400  # DDSCAT_B200_INPUTS_F64
 AUTOTUNE = 0x800  # DDSCAT_B200_AUTOTUNE
+GRAPH = 0x1000  # DDSCAT_B200_GRAPH
 
 
 def _vptr(a):
@@ -252,12 +253,13 @@ class DDA:
                 "navg": navg.value, "f1": f1[:ndir], "f2": f2[:ndir]}
 
     def solve_batch(self, name, b, x, adia, aoff=None, maxit=300, tol=1e-5, check=True, replace=False,
-                    symmetric=False):
+                    symmetric=False, graph=False):
         """Batched solve; b, x (in/out), adia, aoff are (nrhs, 3*NAT) complex64
         host arrays, or CUDA tensors of the same shape (device-resident path).
         replace=True selects residual replacement instead of restarts at the
         reliable-residual checks; symmetric=True (QMRCCG) uses one MATVEC per
-        iteration (left Lanczos vectors equal to the right ones)."""
+        iteration (left Lanczos vectors equal to the right ones); graph=True
+        (with both) runs the iterations device-driven as a CUDA graph."""
         nrhs = int(b.shape[0])
         for a in (b, x, adia) + (() if aoff is None else (aoff,)):
             if tuple(a.shape) != (nrhs, 3 * self.nat):
@@ -269,6 +271,7 @@ class DDA:
         nc = np.zeros(nrhs, dtype=np.int32)
         st = np.zeros(nrhs, dtype=np.int32)
         code = BATCH_SOLVERS[name] | (REPLACE_RESIDUAL if replace else 0) | (QMR_SYMMETRIC if symmetric else 0)
+        code |= GRAPH if graph else 0
         rc = self.lib.ddscat_b200_solve_batch_f32(code, nrhs, _vptr(b), _vptr(x), _vptr(adia),
                                                   _vptr(aoff), maxit, tol, _ptr(it), _ptr(tole), _ptr(nc), _ptr(st))
         if check:

@@ -59,7 +59,12 @@ DDSCAT_CUDA_API int ddscat_b200_autotune_f32(int iters, float *default_ms, float
  * matrix is complex symmetric, so the left vectors stay equal to the right
  * ones and A p equals the recurrence vector q; this variant drops the second
  * MATVEC of each iteration (one MATVEC per iteration instead of two; same
- * iterates in exact arithmetic).
+ * iterates in exact arithmetic).  QMRCCG with both flags may add
+ * DDSCAT_B200_GRAPH: the iterations then run device-driven (scalar
+ * recurrences, masks and reliable-residual decisions in FP64 on the GPU) as a
+ * captured CUDA graph with the reliable-residual check in a conditional node,
+ * so an iteration makes no host round trip; the host reads the active-RHS
+ * count every four graph launches.
  * Codes: 500 invalid argument / not prepared, 501 solver, 502 mixed pointer
  * kinds, 503 workspace allocation, 504 input transfer, 505 solver failure,
  * 506 output transfer. */
@@ -69,6 +74,7 @@ DDSCAT_CUDA_API int ddscat_b200_autotune_f32(int iters, float *default_ms, float
 #define DDSCAT_B200_QMR_SYMMETRIC 0x200
 #define DDSCAT_B200_INPUTS_F64 0x400
 #define DDSCAT_B200_AUTOTUNE 0x800
+#define DDSCAT_B200_GRAPH 0x1000
 DDSCAT_CUDA_API int ddscat_b200_solve_batch_f32(int solver, int nrhs, const void *b, void *x, const void *adia,
                                                 const void *aoff, int maxit, float tol, int *itno, float *tole,
                                                 int *ncompte, int *status);

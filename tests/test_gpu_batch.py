@@ -138,3 +138,29 @@ def test_batch_qmrccg_symmetric_form():
     with pytest.raises(D.DDSCATError):
         dda.solve_batch("pbcgs2", b, np.zeros_like(b), adia, maxit=10, tol=TOL, symmetric=True)
     dda.release()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [16, 24])
+def test_batch_qmrccg_graph_matches_host_driven(n):
+    """Device-driven iterations in a CUDA graph (DDSCAT_B200_GRAPH) follow the
+    host-driven one-MATVEC QMRCCG with residual replacement: iteration counts
+    within one, solutions within 20*TOL, FP64 residual <= 1.2*TOL."""
+    prob = targets.make_problem(n, m=1.33 + 0.05j, x=5.0, orientations=targets.random_orientations(4, seed=12))
+    dda = D.DDA()
+    dda.prepare_green(n, n, n, prob.iocc, prob.incid[0].k)
+    b, adia = _batch_inputs(prob)
+    xh, xg = np.zeros_like(b), np.zeros_like(b)
+    host = dda.solve_batch("qmrccg", b, xh, adia, maxit=2000, tol=TOL, replace=True, symmetric=True)
+    l0 = dda.launch_count()
+    gr = dda.solve_batch("qmrccg", b, xg, adia, maxit=2000, tol=TOL, replace=True, symmetric=True, graph=True)
+    assert dda.launch_count() > l0
+    assert np.all(gr.status == 0) and np.all(gr.tole <= TOL)
+    assert np.all(np.abs(gr.itno - host.itno) <= 1), (gr.itno, host.itno)
+    assert np.all(np.abs(gr.ncompte - host.ncompte) <= 2)
+    assert np.all(dda.residual_f64(b, xg, adia) <= 1.2 * TOL)
+    for r in range(b.shape[0]):
+        assert np.linalg.norm(xg[r] - xh[r]) / np.linalg.norm(xh[r]) < 20 * TOL
+    ms, rhs, calls = dda.last_solve_stats()
+    assert rhs == int(gr.ncompte.sum()) and ms > 0
+    dda.release()
