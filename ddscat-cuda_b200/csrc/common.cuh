@@ -89,4 +89,50 @@ DDB_HD bool zzero(double2 a) { return a.x == 0.0 && a.y == 0.0; }
 
 inline size_t ceil_div(size_t a, size_t b) { return (a + b - 1) / b; }
 
+// Bulk global -> shared copies completed on a shared-memory mbarrier (sm_90+
+// async proxy; no cluster multicast).  A CTA launched without a cluster is its
+// own one-CTA cluster, so its shared::cta addresses are valid shared::cluster
+// destinations.
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// one arrival that also announces `bytes` of transactions for the current phase
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+// bytes and both addresses multiples of 16
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+// Per-thread asynchronous 8-byte global -> shared copy (zero-fills when !ok;
+// src must still be a valid address); completed by cp_async_wait_all.
+__device__ __forceinline__ void cp_async8(void* dst, const void* src, bool ok) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(smem_addr(dst)), "l"(src), "r"(ok ? 8 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+// Wait for the phase of parity `par` to complete, at most `limit` polls;
+// returns false if it did not complete in that time.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t par, int limit) {
+  const uint32_t a = smem_addr(bar);
+  for (int k = 0; k < limit; ++k) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(a), "r"(par)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
 }  // namespace ddb

@@ -56,17 +56,29 @@ template <int DIR, typename C> __device__ __forceinline__ void bfly4(C* v) {
   v[1] = addrot<DIR>(d02, t13);  // d02 + DIR*i*t13
   v[3] = subrot<DIR>(d02, t13);
 }
+// W8^1 * o and W8^3 * o, W8 = exp(DIR*2*pi*i/8) = (1 + DIR*i)/sqrt2
+template <int DIR, typename C> __device__ __forceinline__ C w8_1(C o) {
+  using R = decltype(o.x);
+  const R h = (R)0.70710678118654752440;
+  return DIR > 0 ? mk2<C>(h * (o.x - o.y), h * (o.y + o.x)) : mk2<C>(h * (o.x + o.y), h * (o.y - o.x));
+}
+template <int DIR, typename C> __device__ __forceinline__ C w8_3(C o) {
+  using R = decltype(o.x);
+  const R h = (R)0.70710678118654752440, hn = (R)-0.70710678118654752440;
+  return DIR > 0 ? mk2<C>(hn * (o.x + o.y), h * (o.x - o.y)) : mk2<C>(h * (o.y - o.x), hn * (o.x + o.y));
+}
+// DIR*i*o
+template <int DIR, typename C> __device__ __forceinline__ C rot4(C o) {
+  using R = decltype(o.x);
+  const R m1 = (R)-1.0;
+  return DIR > 0 ? mk2<C>(m1 * o.y, o.x) : mk2<C>(o.y, m1 * o.x);
+}
 template <int DIR, typename C> __device__ __forceinline__ void bfly8(C* v) {
   C e[4] = {v[0], v[2], v[4], v[6]};
   C o[4] = {v[1], v[3], v[5], v[7]};
   bfly4<DIR>(e);
   bfly4<DIR>(o);
-  using R = decltype(v[0].x);
-  const R h = (R)0.70710678118654752440;
-  // W8^1 = (1 + dir*i)/sqrt2, W8^2 = dir*i, W8^3 = (-1 + dir*i)/sqrt2
-  C o1 = o[1], o3 = o[3];
-  C t1 = mk<C>((double)(h * (o1.x - (R)DIR * o1.y)), (double)(h * (o1.y + (R)DIR * o1.x)));
-  C t3 = mk<C>((double)(h * (-o3.x - (R)DIR * o3.y)), (double)(h * (-o3.y + (R)DIR * o3.x)));
+  const C t1 = w8_1<DIR>(o[1]), t3 = w8_3<DIR>(o[3]);
   v[0] = vadd(e[0], o[0]);
   v[4] = vsub(e[0], o[0]);
   v[1] = vadd(e[1], t1);
@@ -78,15 +90,15 @@ template <int DIR, typename C> __device__ __forceinline__ void bfly8(C* v) {
 }
 template <int DIR, typename C> __device__ __forceinline__ void bfly3(C* v) {
   using R = decltype(v[0].x);
-  const R c = (R)-0.5, s = (R)(DIR * 0.86602540378443864676);
-  C t = cadd(v[1], v[2]);
-  C d = csub(v[1], v[2]);
-  C a = v[0];
-  C m = mk<C>((double)(a.x + c * t.x), (double)(a.y + c * t.y));
-  C u = mk<C>((double)(-s * d.y), (double)(s * d.x));
-  v[0] = cadd(a, t);
-  v[1] = cadd(m, u);
-  v[2] = csub(m, u);
+  const R c = (R)-0.5, s = (R)(DIR * 0.86602540378443864676), ms = (R)(-DIR * 0.86602540378443864676);
+  const C t = vadd(v[1], v[2]);
+  const C d = vsub(v[1], v[2]);
+  const C a = v[0];
+  const C m = mk2<C>(a.x + c * t.x, a.y + c * t.y);
+  const C u = mk2<C>(ms * d.y, s * d.x);
+  v[0] = vadd(a, t);
+  v[1] = vadd(m, u);
+  v[2] = vsub(m, u);
 }
 template <int DIR, typename C> __device__ __forceinline__ void bfly5(C* v) {
   using R = decltype(v[0].x);

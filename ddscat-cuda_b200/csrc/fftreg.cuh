@@ -24,6 +24,23 @@ template <int K, int DIR, typename C> DDB_HD C wk(int m) {
   return mk<C>(w96re(q), DIR < 0 ? w96im(q) : -w96im(q));
 }
 
+// x * W_K^m: the multiples of pi/4 are a rotation, a negation or the radix-8
+// forms (m is a compile-time constant after unrolling, so the branches fold)
+template <int K, int DIR, typename C> __device__ __forceinline__ C cmul_wk(C x, int m) {
+  const int q = (m * (96 / K)) % 96;
+  using R = decltype(x.x);
+  const R m1 = (R)-1.0;
+  if (q == 0) return x;
+  if (q == 48) return mk2<C>(m1 * x.x, m1 * x.y);
+  if (q == 24) return rot4<DIR>(x);
+  if (q == 72) return rot4<-DIR>(x);
+  if (q == 12) return w8_1<DIR>(x);
+  if (q == 36) return w8_3<DIR>(x);
+  if (q == 60) return w8_3<-DIR>(x);  // exp(5 i pi/4) = exp(-3 i pi/4)
+  if (q == 84) return w8_1<-DIR>(x);  // exp(7 i pi/4) = exp(-i pi/4)
+  return cmul(x, wk<K, DIR, C>(m));
+}
+
 // first factor of the four-step split K = K1 * K2 of an in-register DFT
 template <int K> constexpr int dft_split() { return (K == 16 || K == 12) ? 4 : 8; }
 
@@ -49,7 +66,7 @@ template <int K, int DIR, typename C> __device__ __forceinline__ void dftr(C* v)
       for (int a = 0; a < K1; ++a) t[a] = v[K2 * a + b];
       dftr<K1, DIR>(t);
 #pragma unroll
-      for (int c = 0; c < K1; ++c) Y[b][c] = (b * c == 0) ? t[c] : cmul(t[c], wk<K, DIR, C>(b * c));
+      for (int c = 0; c < K1; ++c) Y[b][c] = cmul_wk<K, DIR>(t[c], b * c);
     }
 #pragma unroll
     for (int c = 0; c < K1; ++c) {
@@ -79,11 +96,7 @@ template <int K, int DIR, typename C> __device__ __forceinline__ void dftr_h(C* 
     C o[4] = {v[1], v[3], v[1], v[1]};
     dftr_h<4, DIR>(e);
     dftr_h<4, DIR>(o);
-    using R = decltype(v[0].x);
-    const R h = (R)0.70710678118654752440;
-    C o1 = o[1], o3 = o[3];
-    C t1 = mk<C>((double)(h * (o1.x - (R)DIR * o1.y)), (double)(h * (o1.y + (R)DIR * o1.x)));
-    C t3 = mk<C>((double)(h * (-o3.x - (R)DIR * o3.y)), (double)(h * (-o3.y + (R)DIR * o3.x)));
+    const C t1 = w8_1<DIR>(o[1]), t3 = w8_3<DIR>(o[3]);
     v[0] = vadd(e[0], o[0]);
     v[4] = vsub(e[0], o[0]);
     v[1] = vadd(e[1], t1);
@@ -104,7 +117,7 @@ template <int K, int DIR, typename C> __device__ __forceinline__ void dftr_h(C* 
       for (int a = 0; a < K1 / 2; ++a) t[a] = v[K2 * a + b];
       dftr_h<K1, DIR>(t);
 #pragma unroll
-      for (int c = 0; c < K1; ++c) Y[b][c] = (b * c == 0) ? t[c] : cmul(t[c], wk<K, DIR, C>(b * c));
+      for (int c = 0; c < K1; ++c) Y[b][c] = cmul_wk<K, DIR>(t[c], b * c);
     }
 #pragma unroll
     for (int c = 0; c < K1; ++c) {

@@ -93,43 +93,29 @@ __device__ __forceinline__ void store_pairs(C* g, int ld, int valid, const C* ti
     }
   }
 }
+// Global -> tile move of the column passes (the inverse of store_pairs): all
+// of a thread's copies are issued asynchronously at once (8-byte cp.async,
+// zero-filled beyond `valid`), so the block waits for one memory round trip;
+// completed by cp_async_wait_all + __syncthreads.
 template <int RL, int N, typename C>
-__device__ __forceinline__ void load_pairs(const C* g, int ld, int valid, C* tile) {
-  constexpr int RP = RL / 2;
-#pragma unroll 4
-  for (int u = threadIdx.x; u < N * RP; u += 256) {
-    const int r = u / RP, ll = 2 * (u % RP);
-    if constexpr (sizeof(C) == 8) {
-      float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (ll < valid) q = __ldg(reinterpret_cast<const float4*>(g + (size_t)r * ld + ll));
-      tile[r * (RL + 1) + ll] = mk<C>(q.x, q.y);
-      tile[r * (RL + 1) + ll + 1] = mk<C>(q.z, q.w);
-    } else {
-      const bool ok = ll < valid;
-      tile[r * (RL + 1) + ll] = ok ? g[(size_t)r * ld + ll] : mk<C>(0, 0);
-      tile[r * (RL + 1) + ll + 1] = ok ? g[(size_t)r * ld + ll + 1] : mk<C>(0, 0);
-    }
+__device__ __forceinline__ void load_tile_async(const C* g, int ld, int valid, C* tile) {
+  static_assert(sizeof(C) == 8 && (N * RL) % 256 == 0, "complex-float tiles of whole 256-thread rounds");
+#pragma unroll
+  for (int k = 0; k < N * RL / 256; ++k) {
+    const int u = threadIdx.x + 256 * k, r = u / RL, ll = u - r * RL;
+    const bool ok = ll < valid;
+    cp_async8(tile + r * (RL + 1) + ll, ok ? g + (size_t)r * ld + ll : g, ok);
   }
 }
 
-// Copy cnt (<= MAXC) contiguous elements from global to shared memory with the
-// whole 256-thread block, eight loads in flight per thread.
-template <int MAXC, typename C> __device__ __forceinline__ void stage_chunk(C* dst, const C* src, int cnt) {
-  constexpr int IT = (MAXC + 255) / 256;
-  constexpr int G = IT < 8 ? IT : 8;
-#pragma unroll 1
-  for (int k0 = 0; k0 < IT; k0 += G) {
-    C tmp[G];
+// Asynchronous copy of cnt (<= MAXC) contiguous elements from global to shared
+// memory with the whole 256-thread block (completed like load_tile_async).
+template <int MAXC, typename C> __device__ __forceinline__ void stage_chunk_async(C* dst, const C* src, int cnt) {
+  static_assert(sizeof(C) == 8, "complex float");
 #pragma unroll
-    for (int k = 0; k < G; ++k) {
-      const int u = threadIdx.x + 256 * (k0 + k);
-      if (u < cnt) tmp[k] = src[u];
-    }
-#pragma unroll
-    for (int k = 0; k < G; ++k) {
-      const int u = threadIdx.x + 256 * (k0 + k);
-      if (u < cnt) dst[u] = tmp[k];
-    }
+  for (int k = 0; k < (MAXC + 255) / 256; ++k) {
+    const int u = threadIdx.x + 256 * k;
+    if (u < cnt) cp_async8(dst + u, src + u, true);
   }
 }
 
@@ -166,7 +152,8 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_xf(XParam
 #pragma unroll
     for (int i = 0; i < H; ++i) qi[i] = iy < P.ny ? P.inv[jrow + t + TT * i] : -1;
     C* chunk = lines;  // at most RL*nx elements; consumed before the FFT uses the scratch
-    stage_chunk<RL * (N / 2)>(chunk, x + q0, cnt);
+    stage_chunk_async<RL * (N / 2)>(chunk, x + q0, cnt);
+    cp_async_wait_all();
     __syncthreads();
 #pragma unroll
     for (int i = 0; i < H; ++i) v[i] = qi[i] >= 0 ? chunk[qi[i] - q0] : mk<C>(0, 0);
@@ -340,6 +327,130 @@ __global__ void __launch_bounds__(3 * XShape<N>::TT * XShape<N>::RZ, XShape<N>::
   }
 }
 
+// ------------------------------------------------------------- ZG3: z * Green * z^-1, components in registers
+// Each thread holds the same z positions of all three components of its
+// (kx, ky) line, so the Green multiply runs in registers: shared memory only
+// carries the FFT transposes (half the shared-memory traffic of kx_zg, no
+// block barriers after the start).  With IPBC = 0 one thread copies the
+// block's Green octant lines (kz = 0..N/2, contiguous 48-byte records) into
+// shared memory with bulk asynchronous copies at the start, so they arrive
+// while the data loads and forward FFTs run; each thread then reads the
+// records of its own kz values there (kz > N/2 reads the record of N - kz).
+// For E <= 16 (registers: 3E complex per thread).
+// block: RZ lines x TT threads, thread-fastest; grid (nrb, ceil(nkx*My/RZ))
+// shared memory: twiddles [N] | FFT scratch [RZ][lsz] | Green [RZ][NR][6] | mbarrier
+template <int N> struct Z3Shape {
+  static constexpr int RZ = 128 / XShape<N>::TT;  // lines per 128-thread block
+  static constexpr int NR = N / 2 + 1;            // octant records per line
+  static constexpr bool OK = XShape<N>::E <= 16;
+};
+constexpr int ZG3_WAIT_POLLS = 1 << 20;  // bound on the mbarrier polls of one wait
+
+template <typename T>
+__device__ __forceinline__ void load_rec_s(const cplx<T>* sp, cplx<T> a[6]) {
+  if constexpr (sizeof(cplx<T>) == 8) {
+    const float4* s4 = reinterpret_cast<const float4*>(sp);
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      const float4 q = s4[m];
+      a[2 * m] = mk<cplx<T>>(q.x, q.y);
+      a[2 * m + 1] = mk<cplx<T>>(q.z, q.w);
+    }
+  } else {
+#pragma unroll
+    for (int m = 0; m < 6; ++m) a[m] = sp[m];
+  }
+}
+
+template <typename T, int N> __global__ void __launch_bounds__(128, 3) kx_zg3(XParams<T> P) {
+  using C = cplx<T>;
+  using R = T;
+  using S_ = XShape<N>;
+  constexpr int E = S_::E, TT = S_::TT, H = S_::H, RL = Z3Shape<N>::RZ, NR = Z3Shape<N>::NR;
+  static_assert(Z3Shape<N>::OK, "kx_zg3 holds 3*E complex values per thread");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int t = threadIdx.x % TT, l = threadIdx.x / TT;
+  C* tws = reinterpret_cast<C*>(smem_raw);
+  C* my = tws + N + (size_t)l * P.lsz;
+  C* sg = tws + N + (size_t)RL * P.lsz;  // 16-byte aligned: N and RL*lsz are even
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sg + (size_t)RL * NR * 6);
+  const int rb = blockIdx.x, rl = P.b_rhs0 + rb;
+  if (xoff(P, rl)) return;
+  const int nlines = P.nkx * P.My;
+  const int p0 = blockIdx.y * RL;
+  const bool pre = P.ipbc == 0;
+  if (pre && threadIdx.x == 0) {
+    const int nl = min(RL, nlines - p0);  // >= 1
+    mbar_init(bar, 1);
+    mbar_arrive_expect_tx(bar, (uint32_t)(nl * NR * 6 * sizeof(C)));
+    for (int j = 0; j < nl; ++j) {
+      const int pj = p0 + j, kxl = pj / P.My;
+      R s0, s1, s2;
+      bulk_g2s(sg + (size_t)j * NR * 6, green_rec(P, P.kx0 + kxl, pj - kxl * P.My, 0, s0, s1, s2),
+               (uint32_t)(NR * 6 * sizeof(C)), bar);
+    }
+  }
+  load_tw<T, N>(tws, P.twz);
+  __syncthreads();
+  const int p = p0 + l;
+  const bool live = p < nlines;
+  const size_t cs = (size_t)nlines * P.nz;  // component stride of B
+  C* row = P.B + (size_t)rb * 3 * cs + (size_t)(live ? p : 0) * P.nz;
+  C v[3][E];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+#pragma unroll
+    for (int i = 0; i < H; ++i) v[c][i] = live ? row[c * cs + t + TT * i] : mk<C>(0, 0);  // iz < nz = N/2
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) line_fft<E, TT, +1, false, true, S_::PAIR>(v[c], my, t, tws);
+  bool ok = true;
+  if (live) {
+    const int kxl = p / P.My;
+    const int kx = P.kx0 + kxl, ky = p - kxl * P.My;
+    if (pre) {
+      R sxy, sxz, syz;
+      const C* rec0 = green_rec(P, kx, ky, 0, sxy, sxz, syz);
+      const C* srec = sg + (size_t)l * NR * 6;
+      ok = mbar_wait(bar, 0, ZG3_WAIT_POLLS);  // else read the records from global memory
+#pragma unroll
+      for (int i0 = 0; i0 < E; i0 += 4) {
+        C a[4][6];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int kz = t + TT * (i0 + j);
+          const int r = kz <= N / 2 ? kz : N - kz;
+          if (ok) load_rec_s<T>(srec + 6 * r, a[j]); else load_rec<T>(rec0 + 6 * r, a[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int i = i0 + j;
+          const R s = t + TT * i <= N / 2 ? (R)1 : (R)-1;
+          green_apply(a[j], sxy, s * sxz, s * syz, v[0][i], v[1][i], v[2][i]);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < E; ++i) {
+        R sxy, sxz, syz;
+        C a[6];
+        load_rec<T>(green_rec(P, kx, ky, t + TT * i, sxy, sxz, syz), a);
+        green_apply(a, sxy, sxz, syz, v[0][i], v[1][i], v[2][i]);
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) line_fft<E, TT, -1, false, false, S_::PAIR>(v[c], my, t, tws);
+  if (live) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+#pragma unroll
+      for (int i = 0; i < H; ++i) row[c * cs + t + TT * i] = v[c][i];  // keep iz < nz
+    }
+  }
+  if (!ok) mbar_wait(bar, 0, ZG3_WAIT_POLLS);  // no copy may land after the block exits
+}
+
 // ------------------------------------------------------------- YI: y inverse
 // block: RL z-lines x TT; grid (ceil(nz/RL), nkx, 3*nrb)
 template <typename T, int N> __global__ void __launch_bounds__(256) kx_yi(XParams<T> P) {
@@ -357,7 +468,8 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_yi(XParam
   load_tw<T, N>(tws, P.twy);
   const int nz = P.nz;
   const C* B = P.B + ((size_t)(rb * 3 + c) * P.nkx + kxl) * (size_t)P.My * nz + iz0;
-  load_pairs<RL, N>(B, nz, nz - iz0, tile);
+  load_tile_async<RL, N>(B, nz, nz - iz0, tile);
+  cp_async_wait_all();
   __syncthreads();
   C v[E];
 #pragma unroll
@@ -417,11 +529,12 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_xi(XParam
     qi[i] = iy < ny ? (P.io_full ? (P.iocc[j] != 0 ? j : -1) : P.inv[j]) : -1;
   }
   if (chunked) {
-    stage_chunk<MAXC>(xs, x + (size_t)c * S + q0, cnt);
-    stage_chunk<MAXC>(as, ad + q0, cnt);
+    stage_chunk_async<MAXC>(xs, x + (size_t)c * S + q0, cnt);
+    stage_chunk_async<MAXC>(as, ad + q0, cnt);
   }
   const C* A = P.A + (size_t)rl * P.A_rs + ((size_t)(c * P.nz + iz) * P.Mx) * ny + iy0;
-  load_pairs<RL, N>(A, ny, ny - iy0, tile);
+  load_tile_async<RL, N>(A, ny, ny - iy0, tile);
+  cp_async_wait_all();
   __syncthreads();
   C v[E];
 #pragma unroll
@@ -460,30 +573,37 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_xi(XParam
 }
 
 // ------------------------------------------------------------- host side
-enum class XPass { XF, YF, ZG, YI, XI };
+enum class XPass { XF, YF, ZG, ZG3, YI, XI };
 
 template <typename T, int N> static const void* xk(XPass p) {
   switch (p) {
     case XPass::XF: return (const void*)kx_xf<T, N>;
     case XPass::YF: return (const void*)kx_yf<T, N>;
     case XPass::ZG: return (const void*)kx_zg<T, N>;
+    case XPass::ZG3:
+      if constexpr (Z3Shape<N>::OK) return (const void*)kx_zg3<T, N>;
+      return nullptr;
     case XPass::YI: return (const void*)kx_yi<T, N>;
     default: return (const void*)kx_xi<T, N>;
   }
 }
 
 template <typename T> static const void* xkernel(XPass p, int n) {
-  switch (n) {
-    case 16: return xk<T, 16>(p);
-    case 32: return xk<T, 32>(p);
-    case 48: return xk<T, 48>(p);
-    case 64: return xk<T, 64>(p);
-    case 96: return xk<T, 96>(p);
-    case 128: return xk<T, 128>(p);
-    case 192: return xk<T, 192>(p);
-    case 256: return xk<T, 256>(p);
-    case 512: return xk<T, 512>(p);
-    default: return nullptr;
+  if constexpr (sizeof(T) == 8) {
+    return nullptr;  // FP64 runs the z-first pipeline (xpipe_supported)
+  } else {
+    switch (n) {
+      case 16: return xk<T, 16>(p);
+      case 32: return xk<T, 32>(p);
+      case 48: return xk<T, 48>(p);
+      case 64: return xk<T, 64>(p);
+      case 96: return xk<T, 96>(p);
+      case 128: return xk<T, 128>(p);
+      case 192: return xk<T, 192>(p);
+      case 256: return xk<T, 256>(p);
+      case 512: return xk<T, 512>(p);
+      default: return nullptr;
+    }
   }
 }
 
@@ -523,16 +643,23 @@ int matvec_xpipe(Engine<T>& E, const MvArgs<T>& a) {
   const int TX = rT(g.Mx), TY = rT(g.My), TZ = rT(g.Mz);
   const int RX = 256 / TX, RY = 256 / TY;
   const int RZ = std::max(1, 128 / TZ);  // ZG: 3*TZ*RZ threads
+  // ZG3 (components in registers, E <= 16) unless DDSCAT_B200_ZG=1 selects ZG
+  const void* fzg3 = std::getenv("DDSCAT_B200_ZG") ? nullptr : xkernel<T>(XPass::ZG3, g.Mz);
+  const int RZ3 = 128 / TZ;  // ZG3: RZ3 lines of TZ threads
   // must match XShape<N>::PAIR
   P.lsx = line_stride(g.Mx / TX, TX, RX, false, TX >= 8);
   P.lsy = line_stride(g.My / TY, TY, RY, false, TY >= 8);
-  P.lsz = std::max(line_stride(g.Mz / TZ, TZ, RZ, false, TZ >= 8), g.Mz);
+  P.lsz = fzg3 ? line_stride(g.Mz / TZ, TZ, RZ3, false, TZ >= 8)
+               : std::max(line_stride(g.Mz / TZ, TZ, RZ, false, TZ >= 8), g.Mz);
   // the transpose tile and the line scratch share one region
   P.tlx = (int)std::max((size_t)g.Mx * (RX + 1), (size_t)RX * P.lsx);
   const size_t smx = ((size_t)g.Mx + P.tlx) * sizeof(C);
   const size_t smxi = smx + ((size_t)RX * g.nx <= (size_t)XI_STAGE_MAX ? (size_t)2 * RX * g.nx * sizeof(C) : 0);
   const size_t smy = ((size_t)g.My + std::max((size_t)g.My * (RY + 1), (size_t)RY * P.lsy)) * sizeof(C);
-  const size_t smz = ((size_t)g.Mz + (size_t)3 * RZ * P.lsz) * sizeof(C);
+  // ZG3: twiddles, FFT scratch, Green octant lines (IPBC = 0) and the mbarrier
+  const size_t smz =
+      fzg3 ? ((size_t)g.Mz + (size_t)RZ3 * P.lsz + (g.ipbc == 0 ? (size_t)RZ3 * 6 * (g.Mz / 2 + 1) : 0)) * sizeof(C) + 16
+           : ((size_t)g.Mz + (size_t)3 * RZ * P.lsz) * sizeof(C);
   const void* fxf = xkernel<T>(XPass::XF, g.Mx);
   const void* fyf = xkernel<T>(XPass::YF, g.My);
   const void* fzg = xkernel<T>(XPass::ZG, g.Mz);
@@ -556,8 +683,10 @@ int matvec_xpipe(Engine<T>& E, const MvArgs<T>& a) {
         if (xlaunch<T>(fyf, dim3((unsigned)ceil_div(g.nz, RY), (unsigned)P.nkx, (unsigned)(3 * nrb)), 256, smy,
                        E.stream, P))
           return 22;
-        if (xlaunch<T>(fzg, dim3((unsigned)nrb, (unsigned)ceil_div((size_t)P.nkx * g.My, RZ)), 3 * TZ * RZ, smz,
-                       E.stream, P))
+        if (fzg3 ? xlaunch<T>(fzg3, dim3((unsigned)nrb, (unsigned)ceil_div((size_t)P.nkx * g.My, RZ3)), 128, smz,
+                              E.stream, P)
+                 : xlaunch<T>(fzg, dim3((unsigned)nrb, (unsigned)ceil_div((size_t)P.nkx * g.My, RZ)), 3 * TZ * RZ,
+                              smz, E.stream, P))
           return 23;
         if (xlaunch<T>(fyi, dim3((unsigned)ceil_div(g.nz, RY), (unsigned)P.nkx, (unsigned)(3 * nrb)), 256, smy,
                        E.stream, P))
