@@ -182,21 +182,11 @@ inline int line_stride(int E, int T, int L, bool line_fastest, bool pair = false
   return base + (pair ? 2 : 1);
 }
 
-// One length-E*T transform of the line held in v by thread t (0 <= t < T).
-// `sl` is this line's shared scratch; `tw` the N-entry table exp(-2*pi*i*m/N).
-// BLOCK_SYNC selects __syncthreads (line spread over warps) or __syncwarp.
-// HALF_IN: elements t + T*i with i >= E/2 (the upper half of the line) are
-// zero and are not read.  PAIR: transpose rows of stride E + 2 written with
-// 128-bit stores (complex-float lines; the line stride must come from
-// line_stride(..., pair = true)).
-template <int E, int T, int DIR, bool BLOCK_SYNC, bool HALF_IN = false, bool PAIR = false, typename C>
-__device__ __forceinline__ void line_fft(C (&v)[E], C* sl, int t, const C* __restrict__ tw) {
-  constexpr int M = E / T;
-  static_assert(M * T == E && M >= 1, "E must be a multiple of T");
-  if constexpr (HALF_IN) dftr_h<E, DIR>(v); else dftr<E, DIR>(v);
-  // twiddles W^(t p), p = 1..E-1: the powers of two come from the table, the
-  // others are products of at most four of them (fewer shared-memory loads)
-  C w[E];
+// Four-step twiddles W^(t p), p = 1..E-1, of thread t for DIR: the powers of
+// two come from the table tw[m] = exp(-2*pi*i*m/N), the others are products
+// of at most four of them (fewer shared-memory loads).  w[0] is not set.
+template <int E, int DIR, typename C>
+__device__ __forceinline__ void line_twiddles(C (&w)[E], int t, const C* __restrict__ tw) {
 #pragma unroll
   for (int b = 1; b < E; b <<= 1) w[b] = twid<DIR>(tw, t * b);
 #pragma unroll
@@ -204,8 +194,30 @@ __device__ __forceinline__ void line_fft(C (&v)[E], C* sl, int t, const C* __res
     const int hb = 1 << (31 - __clz(p));  // highest set bit of p
     if (p != hb) w[p] = cmul(w[hb], w[p - hb]);
   }
+}
+
+// a * conj(w)
+template <typename C> __device__ __forceinline__ C cmulc(C a, C w) {
+  return mk2<C>(a.x * w.x + a.y * w.y, a.y * w.x - a.x * w.y);
+}
+
+// One length-E*T transform of the line held in v by thread t (0 <= t < T),
+// with the thread's twiddles w from line_twiddles: those of DIR, or with
+// CONJW those of -DIR, applied conjugated (so one set serves a forward and an
+// inverse transform; both give the same products as a set built for DIR).
+// `sl` is this line's shared scratch.  BLOCK_SYNC selects __syncthreads (line
+// spread over warps) or __syncwarp.  HALF_IN: elements t + T*i with i >= E/2
+// (the upper half of the line) are zero and are not read.  PAIR: transpose
+// rows of stride E + 2 written with 128-bit stores (complex-float lines; the
+// line stride must come from line_stride(..., pair = true)).
+template <int E, int T, int DIR, bool BLOCK_SYNC, bool HALF_IN = false, bool PAIR = false, bool CONJW = false,
+          typename C>
+__device__ __forceinline__ void line_fft_w(C (&v)[E], C* sl, int t, const C (&w)[E]) {
+  constexpr int M = E / T;
+  static_assert(M * T == E && M >= 1, "E must be a multiple of T");
+  if constexpr (HALF_IN) dftr_h<E, DIR>(v); else dftr<E, DIR>(v);
 #pragma unroll
-  for (int p = 1; p < E; ++p) v[p] = cmul(v[p], w[p]);
+  for (int p = 1; p < E; ++p) v[p] = CONJW ? cmulc(v[p], w[p]) : cmul(v[p], w[p]);
   constexpr bool P2 = PAIR && sizeof(C) == 8;
   constexpr int RS = row_stride<E, P2>();
   if constexpr (P2) {
@@ -227,6 +239,14 @@ __device__ __forceinline__ void line_fft(C (&v)[E], C* sl, int t, const C* __res
     for (int q = 0; q < T; ++q) v[j + M * q] = u[q];
   }
   if (BLOCK_SYNC) __syncthreads(); else __syncwarp();
+}
+
+// One length-E*T transform with its own twiddles (`tw` as in line_twiddles).
+template <int E, int T, int DIR, bool BLOCK_SYNC, bool HALF_IN = false, bool PAIR = false, typename C>
+__device__ __forceinline__ void line_fft(C (&v)[E], C* sl, int t, const C* __restrict__ tw) {
+  C w[E];
+  line_twiddles<E, DIR>(w, t, tw);
+  line_fft_w<E, T, DIR, BLOCK_SYNC, HALF_IN, PAIR>(v, sl, t, w);
 }
 
 // (E, T) shape for a supported power-of-two length, E*T = N

@@ -402,8 +402,11 @@ template <typename T, int N> __global__ void __launch_bounds__(128, 3) kx_zg3(XP
 #pragma unroll
     for (int i = 0; i < H; ++i) v[c][i] = live ? row[c * cs + t + TT * i] : mk<C>(0, 0);  // iz < nz = N/2
   }
+  // one twiddle set for the six transforms: forward, and conjugated for the inverse
+  C w[E];
+  line_twiddles<E, +1>(w, t, tws);
 #pragma unroll
-  for (int c = 0; c < 3; ++c) line_fft<E, TT, +1, false, true, S_::PAIR>(v[c], my, t, tws);
+  for (int c = 0; c < 3; ++c) line_fft_w<E, TT, +1, false, true, S_::PAIR>(v[c], my, t, w);
   bool ok = true;
   if (live) {
     const int kxl = p / P.My;
@@ -440,7 +443,7 @@ template <typename T, int N> __global__ void __launch_bounds__(128, 3) kx_zg3(XP
     }
   }
 #pragma unroll
-  for (int c = 0; c < 3; ++c) line_fft<E, TT, -1, false, false, S_::PAIR>(v[c], my, t, tws);
+  for (int c = 0; c < 3; ++c) line_fft_w<E, TT, -1, false, false, S_::PAIR, true>(v[c], my, t, w);
   if (live) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
