@@ -603,11 +603,17 @@ static int qmr_graph_loop(BatchIO<T>& io, BatchOps<T>& ops, std::vector<int>& nc
     if (e == cudaSuccess) e = cudaMemcpy(ii, hi.data(), ni * sizeof(int), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) { cudaFree(blk); set_cuda_error("graph solve state", e); return 1; }
   }
+  // partials of the MATVEC-fused vt^T A vt (x-first pipeline); else a separate sum kernel
+  double2* xpart = nullptr;
+  if (io.eng->xpipe) {
+    e = cudaMalloc((void**)&xpart, (size_t)R * xdot_blocks(io.eng->g) * sizeof(double2));
+    if (e != cudaSuccess) { cudaFree(blk); set_cuda_error("graph solve state", e); return 1; }
+  }
   cudaStream_t st = nullptr, st2 = nullptr;
   cudaStreamSynchronize(ops.stream);
   e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking);
-  if (e != cudaSuccess) { cudaFree(blk); set_cuda_error("graph solve streams", e); return 1; }
+  if (e != cudaSuccess) { cudaFree(blk); cudaFree(xpart); set_cuda_error("graph solve streams", e); return 1; }
   Engine<T>& eng = *io.eng;
   const cudaStream_t eng_st = eng.stream;
   MvArgs<T> mv;
@@ -652,11 +658,17 @@ static int qmr_graph_loop(BatchIO<T>& io, BatchOps<T>& ops, std::vector<int>& nc
       kq_pqv<C><<<dim3(ops.nb, R), BT, 0, st>>>(n, p, q, vt, atw, S.co, S.I, 2, ops.d_part, ops.d_out, ops.d_cnt);
       note_launch();
       mv.x = vt; mv.y = atw; mv.mask = S.I;
+      if (xpart) {  // vt^T A vt summed inside the last MATVEC pass
+        mv.dot_out = ops.d_out; mv.dot_part = xpart; mv.dot_cnt = ops.d_cnt; mv.dot_k = 0;
+      }
       rc = eng.matvec(mv);
-      BDot<T> sp{};
-      sp.K = 1; sp.mode = 0; sp.a[0] = vt; sp.b[0] = atw; sp.conj[0] = 0;
-      kb_dots<T><<<dim3(ops.nb, R), BT, 0, st>>>(n, sp, S.I, ops.d_part, ops.d_out, ops.d_cnt);
-      note_launch();
+      mv.dot_out = nullptr; mv.dot_part = nullptr; mv.dot_cnt = nullptr;
+      if (!xpart) {
+        BDot<T> sp{};
+        sp.K = 1; sp.mode = 0; sp.a[0] = vt; sp.b[0] = atw; sp.conj[0] = 0;
+        kb_dots<T><<<dim3(ops.nb, R), BT, 0, st>>>(n, sp, S.I, ops.d_part, ops.d_out, ops.d_cnt);
+        note_launch();
+      }
       k_qg_scalars<<<1, 256, 0, st>>>(R, S, ops.d_out);
       note_launch();
       kq_dsxr<C><<<dim3(ops.nb, R), BT, 0, st>>>(n, d, s, xs, r, p, q, S.co + 5 * (size_t)R, S.I, 0, ops.d_part,
@@ -754,6 +766,7 @@ static int qmr_graph_loop(BatchIO<T>& io, BatchOps<T>& ops, std::vector<int>& nc
   cudaStreamDestroy(st);
   cudaStreamDestroy(st2);
   cudaFree(blk);
+  cudaFree(xpart);
   return rc;
 }
 

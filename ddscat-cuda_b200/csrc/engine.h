@@ -54,6 +54,14 @@ template <typename T> struct MvArgs {
   int conj = 0;                   // CWHAT='C'
   const int* mask = nullptr;      // device per-RHS flags (nonzero = compute)
   int nrhs = 1;
+  // Optional, x-first pipeline only (conj = 0): the unconjugated FP64 sum
+  // over compact sites of x*y of RHS r into dot_out[8*r + dot_k], reduced in
+  // a fixed order inside the last MATVEC pass.  dot_part holds
+  // nrhs * xdot_blocks(g) partials; dot_cnt one zeroed counter per RHS.
+  double2* dot_out = nullptr;
+  double2* dot_part = nullptr;
+  unsigned* dot_cnt = nullptr;
+  int dot_k = 0;
 };
 
 template <typename T> struct GreenArgs {
@@ -137,6 +145,8 @@ template <typename T> bool xpipe_supported(const Geometry& g);
 // to its grid and keeps the fastest; default_ms / best_ms per call.
 int autotune_engine(Engine<float>& e, int iters, float* default_ms, float* best_ms);
 template <typename T> int matvec_xpipe(Engine<T>& E, const MvArgs<T>& a);
+// partials per RHS of the fused x*y sum of the x-first pipeline (MvArgs::dot_out)
+size_t xdot_blocks(const Geometry& g);
 template <typename T> int interleave_green_zfast(Engine<T>& E, const cplx<T>* planar);
 
 }  // namespace ddb

@@ -50,6 +50,10 @@ template <typename T> struct XParams {
   int lsx, lsy, lsz;  // line strides of the x, y, z passes
   int tlx;            // tile / line scratch elements of the x passes
   T inv_ngrid;
+  double2* dot_out;  // optional fused sum of x*y per RHS (MvArgs::dot_out)
+  double2* dot_part;
+  unsigned* dot_cnt;
+  int dot_k;
 };
 
 template <typename T> __device__ __forceinline__ bool xoff(const XParams<T>& P, int rl) {
@@ -486,6 +490,53 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_yi(XParam
   }
 }
 
+// Fused x*y sum of the XI pass: the block total goes to its partial slot; the
+// last block of RHS rg (in completion order) folds the nblk partials in a fixed
+// order into dot_out[8*rg + dot_k] (deterministic), and the counter wraps to 0.
+template <typename T> __device__ __forceinline__ void xdot_reduce(const XParams<T>& P, double2 v, int rg, int blk,
+                                                                  int nblk) {
+  __shared__ double2 ws[8];
+  __shared__ bool last;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  auto wsum = [](double2 a) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a.x += __shfl_down_sync(0xffffffffu, a.x, o);
+      a.y += __shfl_down_sync(0xffffffffu, a.y, o);
+    }
+    return a;
+  };
+  v = wsum(v);
+  if (lane == 0) ws[wid] = v;
+  __syncthreads();
+  double2* part = P.dot_part + (size_t)rg * nblk;
+  if (threadIdx.x == 0) {
+    double2 b = make_double2(0.0, 0.0);
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { b.x += ws[w].x; b.y += ws[w].y; }
+    part[blk] = b;
+    __threadfence();
+    last = atomicInc(P.dot_cnt + rg, (unsigned)nblk - 1) == (unsigned)nblk - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double2 a = make_double2(0.0, 0.0);
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
+    const volatile double* pp = reinterpret_cast<volatile double*>(part + b);
+    a.x += pp[0];
+    a.y += pp[1];
+  }
+  a = wsum(a);
+  __syncthreads();
+  if (lane == 0) ws[wid] = a;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double2 b = make_double2(0.0, 0.0);
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { b.x += ws[w].x; b.y += ws[w].y; }
+    P.dot_out[(size_t)rg * 8 + P.dot_k] = b;
+  }
+}
+
 // ------------------------------------------------------------- XI: x inverse + finish
 constexpr int XI_STAGE_MAX = 2048;  // largest staged chunk of the XI pass (elements)
 
@@ -544,12 +595,13 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_xi(XParam
   for (int i = 0; i < E; ++i) v[i] = tile[(t + TT * i) * (RL + 1) + l];
   __syncthreads();
   line_fft<E, TT, -1, false, false, S_::PAIR>(v, lines + (size_t)l * P.lsx, t, tws);
-  if (iy >= ny) return;
   // finish (cu:116-118): y = CXADIA x - w/ngrid [+ CXAOFF terms], conj for 'C'
   C* y = P.y + (size_t)rl * P.y_rs + (size_t)c * S;
   const C* ao = P.aoff ? P.aoff + (size_t)rl * P.a_rs : nullptr;
+  double2 dacc = make_double2(0.0, 0.0);  // x*y of this thread's sites (dot_out)
 #pragma unroll
   for (int i = 0; i < H; ++i) {
+    if (iy >= ny) break;
     const int j = jrow + t + TT * i;
     const int q = qi[i];
     if (q < 0) {
@@ -572,7 +624,15 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_xi(XParam
     }
     if (P.conj) yv.y = -yv.y;
     y[q] = yv;
+    if (P.dot_out) {  // conj = 0 here: xc is x
+      const double2 xd = to_d(xc), yd = to_d(yv);
+      dacc.x += xd.x * yd.x - xd.y * yd.y;
+      dacc.y += xd.x * yd.y + xd.y * yd.x;
+    }
   }
+  if (P.dot_out)
+    xdot_reduce(P, dacc, P.rhs0 + rl, (c * (int)gridDim.y + (int)blockIdx.y) * (int)gridDim.x + (int)blockIdx.x,
+                3 * (int)gridDim.y * (int)gridDim.x);
 }
 
 // ------------------------------------------------------------- host side
@@ -643,6 +703,8 @@ int matvec_xpipe(Engine<T>& E, const MvArgs<T>& a) {
   P.green = E.green; P.ipbc = g.ipbc;
   P.twx = E.twx; P.twy = E.twy; P.twz = E.twz;
   P.inv_ngrid = (T)(1.0 / (double)g.ngrid());
+  P.dot_out = a.dot_out; P.dot_part = a.dot_part; P.dot_cnt = a.dot_cnt; P.dot_k = a.dot_k;
+  if (a.dot_out && (a.conj || !a.dot_part || !a.dot_cnt)) { set_error("MATVEC", "fused x*y sum needs conj = 0"); return 25; }
   const int TX = rT(g.Mx), TY = rT(g.My), TZ = rT(g.Mz);
   const int RX = 256 / TX, RY = 256 / TY;
   const int RZ = std::max(1, 128 / TZ);  // ZG: 3*TZ*RZ threads
@@ -701,6 +763,8 @@ int matvec_xpipe(Engine<T>& E, const MvArgs<T>& a) {
   }
   return 0;
 }
+
+size_t xdot_blocks(const Geometry& g) { return (size_t)3 * g.nz * ceil_div(g.ny, 256 / reg_threads(g.Mx)); }
 
 // planar [6][Z][Y][X] (build / CXZC layout) -> [X][Y][Z][6]
 template <typename C> __global__ void k_interleave6_zfast(const C* src, C* dst, int X, int Y, int Z) {
