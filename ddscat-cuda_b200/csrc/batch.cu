@@ -226,6 +226,65 @@ __global__ void __launch_bounds__(BT) kq_dsxr(int n, C* d, C* s, C* x, C* rv, co
   block_sums<1>(acc, k0, r, part, out, cnt);
 }
 
+// One-MATVEC QMRCCG, the last vector step of iteration k fused with the first
+// of iteration k+1 (they read the same p and q), per RHS r in mask:
+//   d = th d + ka p ; s = th s + ka q ; x = x + d ; r = r - s          (k)
+//   p = cp p + cv vt ; q = cq q + cw atw ; vt = ct vt + q              (k+1)
+// with |r|^2 into out slot 0, |vt|^2 and vt^T vt into slots 2 and 3 (slot 1
+// is written 0).  co holds the five k+1 coefficients, then th and ka.  Same
+// element arithmetic and reduction grid as kq_dsxr and kq_pqv.
+template <typename C>
+__global__ void __launch_bounds__(BT) kq_dsxr_pqv(int n, C* __restrict__ d, C* __restrict__ s, C* __restrict__ x,
+                                                  C* __restrict__ rv, C* __restrict__ p, C* __restrict__ q,
+                                                  C* __restrict__ vt, const C* __restrict__ atw, const double2* co,
+                                                  const int* mask, double2* part, double2* out, unsigned* cnt) {
+  const int r = blockIdx.y, R = gridDim.y;
+  if (mask && !mask[r]) return;
+  const size_t off = (size_t)r * n;
+  d += off; s += off; x += off; rv += off; p += off; q += off; vt += off; atw += off;
+  const double2 cp = co[r], cv = co[R + r], cq = co[2 * R + r], cw = co[3 * R + r], ct = co[4 * R + r];
+  const double2 th = co[5 * R + r], ka = co[6 * R + r];
+  double2 acc[4] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0), make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
+  // two elements per thread and round: all sixteen loads are issued before the stores
+  const int stride = gridDim.x * BT;
+  for (int i0 = blockIdx.x * BT + threadIdx.x; i0 < n; i0 += 2 * stride) {
+    C p0[2], q0[2], v0[2], a0[2], d0[2], s0[2], x0[2], r0[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int i = i0 + k * stride;
+      if (i < n) {
+        p0[k] = p[i]; q0[k] = q[i]; v0[k] = vt[i]; a0[k] = atw[i];
+        d0[k] = d[i]; s0[k] = s[i]; x0[k] = x[i]; r0[k] = rv[i];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int i = i0 + k * stride;
+      if (i >= n) break;
+      const C dn = cadd(zmulv(th, d0[k]), zmulv(ka, p0[k]));
+      const C sn = cadd(zmulv(th, s0[k]), zmulv(ka, q0[k]));
+      const C xn = cadd(x0[k], dn);
+      const C rn = csub(r0[k], sn);
+      const C pn = cadd(zmulv(cp, p0[k]), zmulv(cv, v0[k]));
+      const C qn = cadd(zmulv(cq, q0[k]), zmulv(cw, a0[k]));
+      const C vn = cadd(zmulv(ct, v0[k]), qn);
+      d[i] = dn;
+      s[i] = sn;
+      x[i] = xn;
+      rv[i] = rn;
+      p[i] = pn;
+      q[i] = qn;
+      vt[i] = vn;
+      const double2 a = to_d(rn), b = to_d(vn);
+      acc[0].x += a.x * a.x + a.y * a.y;
+      acc[2].x += b.x * b.x + b.y * b.y;
+      acc[3].x += b.x * b.x - b.y * b.y;
+      acc[3].y += 2.0 * b.x * b.y;
+    }
+  }
+  block_sums<4>(acc, 0, r, part, out, cnt);
+}
+
 template <typename T> int BatchOps<T>::init(int R_, int n_, cudaStream_t s) {
   R = R_;
   n = n_;
@@ -386,6 +445,7 @@ template <typename T> struct BCtx {
   int R, n;
   std::vector<int> nc;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+  int last_cnt = 0;  // RHS of the latest MATVEC (its events are ev.back())
   explicit BCtx(BatchIO<T>& s) : io(s), ops(*s.ops), R(s.R), n(s.n), nc(s.R, 0) {}
   ~BCtx() {
     for (auto& p : ev) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
@@ -410,6 +470,7 @@ template <typename T> struct BCtx {
     ev.push_back({e0, e1});
     if (rc) return rc;
     for (int r = 0; r < R; ++r) nc[r] += hm[r] ? 1 : 0;
+    last_cnt = cnt;
     io.matvec_rhs += cnt;
     io.matvec_calls += 1;
     return 0;
@@ -464,6 +525,17 @@ __device__ __forceinline__ double2 ddiv(double2 a, double2 b) {
 __device__ __forceinline__ double2 dsc(double s, double2 a) { return make_double2(s * a.x, s * a.y); }
 __device__ __forceinline__ bool dz0(double2 a) { return a.x == 0.0 && a.y == 0.0; }
 
+// coefficients of the p/q/v step of RHS r from gamma, ksi, mu, tau
+__device__ __forceinline__ void qg_pqv_coefficients(int R, int r, const QGState& S) {
+  const double2 g = S.gamma[r], k = S.ksi[r], mu = S.mu[r], t = S.tau[r];
+  const double2 one = make_double2(1.0, 0.0);
+  S.co[r] = dsc(-1.0, mu);                            // -mu
+  S.co[R + r] = ddiv(one, g);                         // 1/gamma
+  S.co[2 * R + r] = dsc(-1.0, ddiv(dmul(g, mu), k));  // -(gamma mu)/ksi
+  S.co[3 * R + r] = ddiv(one, k);                     // 1/ksi
+  S.co[4 * R + r] = dsc(-1.0, ddiv(t, g));            // -(tau/gamma)
+}
+
 // I = live and it < maxit and resid > tol; coefficients of the p/q/v step
 __global__ void k_qg_begin(int R, int maxit, double tol, QGState S) {
   for (int r = threadIdx.x; r < R; r += blockDim.x) {
@@ -472,14 +544,22 @@ __global__ void k_qg_begin(int R, int maxit, double tol, QGState S) {
     if (!on) continue;
     S.it[r] += 1;
     S.nc[r] += 1;
-    const double2 g = S.gamma[r], k = S.ksi[r], mu = S.mu[r], t = S.tau[r];
-    const double2 one = make_double2(1.0, 0.0);
-    S.co[r] = dsc(-1.0, mu);                          // -mu
-    S.co[R + r] = ddiv(one, g);                       // 1/gamma
-    S.co[2 * R + r] = dsc(-1.0, ddiv(dmul(g, mu), k));  // -(gamma mu)/ksi
-    S.co[3 * R + r] = ddiv(one, k);                   // 1/ksi
-    S.co[4 * R + r] = dsc(-1.0, ddiv(t, g));          // -(tau/gamma)
+    qg_pqv_coefficients(R, r, S);
   }
+}
+
+// Start of the next iteration inside the captured body (its p/q/v step already
+// ran in kq_dsxr_pqv): I, iteration and MATVEC counts, and the active count.
+__global__ void k_qg_next(int R, int maxit, double tol, QGState S) {
+  if (threadIdx.x != 0) return;
+  int c = 0;
+  for (int r = 0; r < R; ++r) {
+    const int on = S.live[r] && S.it[r] < maxit && S.resid[r] > tol;
+    S.I[r] = on;
+    if (on) { S.it[r] += 1; S.nc[r] += 1; }
+    c += on;
+  }
+  *S.active = c;
 }
 
 // scalar recurrence from |vt|^2, vt^T vt (out slots 2, 3) and vt^T A vt (slot 0)
@@ -516,6 +596,7 @@ __global__ void k_qg_scalars(int R, QGState S, const double2* out) {
     if (st) { S.status[r] = 58; S.live[r] = 0; S.I[r] = 0; }
     S.co[5 * R + r] = theta;
     S.co[6 * R + r] = kappa;
+    if (!st) qg_pqv_coefficients(R, r, S);  // for the p/q/v step of the next iteration (kq_dsxr_pqv)
   }
 }
 
@@ -552,19 +633,14 @@ __global__ void k_qg_check(int R, double tol, QGState S, const double2* out) {
   }
 }
 
-__global__ void k_qg_count(int R, int maxit, double tol, QGState S) {
-  if (threadIdx.x != 0) return;
-  int c = 0;
-  for (int r = 0; r < R; ++r) c += S.live[r] && S.it[r] < maxit && S.resid[r] > tol;
-  *S.active = c;
-}
 
 // Runs the iterations of the one-MATVEC QMRCCG with residual replacement from
 // the state the host-driven setup produced, until no RHS is active.
 template <typename T>
 static int qmr_graph_loop(BatchIO<T>& io, BatchOps<T>& ops, std::vector<int>& nc, cplx<T>* const* w,
                           cplx<T>* xs, std::vector<Z>* sc, std::vector<double>& bnorm, std::vector<double>& resid,
-                          std::vector<int>& it, std::vector<int>& live, std::vector<int>& status) {
+                          std::vector<int>& it, std::vector<int>& live, std::vector<int>& status,
+                          double mv_ms_per_rhs) {
   using C = cplx<T>;
   const int R = io.R, n = io.n;
   C *r = w[0], *p = w[1], *q = w[3], *d = w[4], *s = w[5], *vt = w[6], *atw = w[8], *sy = w[9];
@@ -619,24 +695,10 @@ static int qmr_graph_loop(BatchIO<T>& io, BatchOps<T>& ops, std::vector<int>& nc
   MvArgs<T> mv;
   mv.x = vt; mv.x_rs = n; mv.y = atw; mv.y_rs = n; mv.io_full = 0;
   mv.adia = io.adia; mv.aoff = io.aoff; mv.a_rs = n; mv.a_full = 0; mv.conj = 0; mv.mask = S.live; mv.nrhs = R;
-  // MATVEC time of this batch (all RHS live), measured on this stream before the captured iterations
-  float per_call = 0.f;
+  // the MATVEC time of the iterations is estimated as mv_ms_per_rhs per RHS (the
+  // kernels inside the graph are not timed)
   int rc = 0;
-  {
-    eng.stream = st;
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    rc = eng.matvec(mv);  // warm-up; A vt is recomputed by the first iteration anyway
-    cudaEventRecord(e0, st);
-    if (!rc) rc = eng.matvec(mv);
-    cudaEventRecord(e1, st);
-    cudaEventSynchronize(e1);
-    cudaEventElapsedTime(&per_call, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-  }
-  // (the two calls recomputed A vt, which atw already held)
+  eng.stream = st;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   unsigned long long kernels_a = 0, kernels_b = 0;
@@ -653,10 +715,7 @@ static int qmr_graph_loop(BatchIO<T>& io, BatchOps<T>& ops, std::vector<int>& nc
     if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, graph, 0, cudaGraphCondAssignDefault);
     const unsigned long long c0 = launch_total();
     if (e == cudaSuccess) {
-      k_qg_begin<<<1, 256, 0, st>>>(R, maxit, tol, S);
-      note_launch();
-      kq_pqv<C><<<dim3(ops.nb, R), BT, 0, st>>>(n, p, q, vt, atw, S.co, S.I, 2, ops.d_part, ops.d_out, ops.d_cnt);
-      note_launch();
+      // body of iteration k: its p/q/v step ran at the end of k-1 (or in the prologue)
       mv.x = vt; mv.y = atw; mv.mask = S.I;
       if (xpart) {  // vt^T A vt summed inside the last MATVEC pass
         mv.dot_out = ops.d_out; mv.dot_part = xpart; mv.dot_cnt = ops.d_cnt; mv.dot_k = 0;
@@ -671,8 +730,8 @@ static int qmr_graph_loop(BatchIO<T>& io, BatchOps<T>& ops, std::vector<int>& nc
       }
       k_qg_scalars<<<1, 256, 0, st>>>(R, S, ops.d_out);
       note_launch();
-      kq_dsxr<C><<<dim3(ops.nb, R), BT, 0, st>>>(n, d, s, xs, r, p, q, S.co + 5 * (size_t)R, S.I, 0, ops.d_part,
-                                                 ops.d_out, ops.d_cnt);
+      kq_dsxr_pqv<C><<<dim3(ops.nb, R), BT, 0, st>>>(n, d, s, xs, r, p, q, vt, atw, S.co, S.I, ops.d_part,
+                                                     ops.d_out, ops.d_cnt);
       note_launch();
       k_qg_post<<<1, 32, 0, st>>>(R, tol, S, ops.d_out, h);
       note_launch();
@@ -711,7 +770,7 @@ static int qmr_graph_loop(BatchIO<T>& io, BatchOps<T>& ops, std::vector<int>& nc
         }
       }
       if (e == cudaSuccess) {
-        k_qg_count<<<1, 32, 0, st>>>(R, maxit, tol, S);
+        k_qg_next<<<1, 32, 0, st>>>(R, maxit, tol, S);
         note_launch();
         kernels_a += 1;
       }
@@ -725,6 +784,10 @@ static int qmr_graph_loop(BatchIO<T>& io, BatchOps<T>& ops, std::vector<int>& nc
   }
   // capture only recorded the launches: the counter counts executions below
   if (!rc) {
+    // prologue: the first iteration's start and p/q/v step
+    k_qg_begin<<<1, 256, 0, st>>>(R, maxit, tol, S);
+    kq_pqv<C><<<dim3(ops.nb, R), BT, 0, st>>>(n, p, q, vt, atw, S.co, S.I, 2, ops.d_part, ops.d_out, ops.d_cnt);
+    note_launch(2);
     int* h_active = nullptr;
     e = cudaMallocHost((void**)&h_active, sizeof(int));
     long long launches = 0;
@@ -756,7 +819,7 @@ static int qmr_graph_loop(BatchIO<T>& io, BatchOps<T>& ops, std::vector<int>& nc
       }
       io.matvec_rhs += mv_rhs;
       io.matvec_calls += (int)(launches + checks);
-      io.matvec_ms += (double)per_call * (double)mv_rhs / (double)R;
+      io.matvec_ms += mv_ms_per_rhs * (double)mv_rhs;
     }
   }
   if (exec) cudaGraphExecDestroy(exec);
@@ -867,7 +930,12 @@ template <typename T> int solve_batch_qmrccg(BatchIO<T>& io, BatchResult& res) {
   if (use_graph) {
     C* wv[10] = {c.w(0), c.w(1), c.w(2), c.w(3), c.w(4), c.w(5), c.w(6), c.w(7), c.w(8), c.w(9)};
     std::vector<Z> sc[9] = {gamma, ksi, rho, eps, mu, tau, lambda, kappa, theta};
-    if ((rc = qmr_graph_loop<T>(io, ops, c.nc, wv, xs, sc, bnorm, resid, it, live, res.status))) return rc;
+    // MATVEC time per RHS from the latest timed MATVEC of the setup (A vt0)
+    float t = 0.f;
+    cudaStreamSynchronize(ops.stream);
+    if (!c.ev.empty()) cudaEventElapsedTime(&t, c.ev.back().first, c.ev.back().second);
+    const double per_rhs = c.last_cnt > 0 ? (double)t / c.last_cnt : 0.0;
+    if ((rc = qmr_graph_loop<T>(io, ops, c.nc, wv, xs, sc, bnorm, resid, it, live, res.status, per_rhs))) return rc;
   }
   for (; !use_graph;) {
     std::vector<int> I(R, 0);
