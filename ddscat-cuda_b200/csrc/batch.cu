@@ -5,6 +5,8 @@
 #include <algorithm>
 #include <complex>
 #include "batch.h"
+#include <cstdio>
+#include <cstdlib>
 
 namespace ddb {
 
@@ -525,6 +527,18 @@ __device__ __forceinline__ double2 ddiv(double2 a, double2 b) {
 __device__ __forceinline__ double2 dsc(double s, double2 a) { return make_double2(s * a.x, s * a.y); }
 __device__ __forceinline__ bool dz0(double2 a) { return a.x == 0.0 && a.y == 0.0; }
 
+// Phase stamps of the captured iteration (DDSCAT_B200_VERBOSE): the global
+// timer at 7 points of iteration it, st[8*it + slot]; st[8*cap] counts the
+// iterations (bounded by cap).
+__global__ void k_qg_stamp(unsigned long long* st, int cap, int slot, int bump) {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  unsigned long long* n = st + 8 * (size_t)cap;
+  const unsigned long long it = *n;
+  if (it < (unsigned long long)cap) st[8 * it + slot] = t;
+  if (bump) *n = it + 1;
+}
+
 // coefficients of the p/q/v step of RHS r from gamma, ksi, mu, tau
 __device__ __forceinline__ void qg_pqv_coefficients(int R, int r, const QGState& S) {
   const double2 g = S.gamma[r], k = S.ksi[r], mu = S.mu[r], t = S.tau[r];
@@ -679,17 +693,30 @@ static int qmr_graph_loop(BatchIO<T>& io, BatchOps<T>& ops, std::vector<int>& nc
     if (e == cudaSuccess) e = cudaMemcpy(ii, hi.data(), ni * sizeof(int), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) { cudaFree(blk); set_cuda_error("graph solve state", e); return 1; }
   }
+  // phase stamps of the iterations (verbose only)
+  const bool verbose = std::getenv("DDSCAT_B200_VERBOSE") != nullptr;
+  const int scap = io.maxit + 64;
+  unsigned long long* stamps = nullptr;
+  if (verbose && cudaMalloc((void**)&stamps, (size_t)(8 * scap + 1) * sizeof(unsigned long long)) == cudaSuccess)
+    cudaMemset(stamps, 0, (size_t)(8 * scap + 1) * sizeof(unsigned long long));
+  auto stamp = [&](cudaStream_t s_, int slot, int bump) {
+    if (stamps) k_qg_stamp<<<1, 1, 0, s_>>>(stamps, scap, slot, bump);
+  };
   // partials of the MATVEC-fused vt^T A vt (x-first pipeline); else a separate sum kernel
   double2* xpart = nullptr;
   if (io.eng->xpipe) {
     e = cudaMalloc((void**)&xpart, (size_t)R * xdot_blocks(io.eng->g) * sizeof(double2));
-    if (e != cudaSuccess) { cudaFree(blk); set_cuda_error("graph solve state", e); return 1; }
+    if (e != cudaSuccess) { cudaFree(blk); cudaFree(stamps); set_cuda_error("graph solve state", e); return 1; }
   }
   cudaStream_t st = nullptr, st2 = nullptr;
   cudaStreamSynchronize(ops.stream);
   e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking);
-  if (e != cudaSuccess) { cudaFree(blk); cudaFree(xpart); set_cuda_error("graph solve streams", e); return 1; }
+  if (e != cudaSuccess) {
+    cudaFree(blk); cudaFree(xpart); cudaFree(stamps);
+    set_cuda_error("graph solve streams", e);
+    return 1;
+  }
   Engine<T>& eng = *io.eng;
   const cudaStream_t eng_st = eng.stream;
   MvArgs<T> mv;
@@ -716,6 +743,7 @@ static int qmr_graph_loop(BatchIO<T>& io, BatchOps<T>& ops, std::vector<int>& nc
     const unsigned long long c0 = launch_total();
     if (e == cudaSuccess) {
       // body of iteration k: its p/q/v step ran at the end of k-1 (or in the prologue)
+      stamp(st, 0, 0);
       mv.x = vt; mv.y = atw; mv.mask = S.I;
       if (xpart) {  // vt^T A vt summed inside the last MATVEC pass
         mv.dot_out = ops.d_out; mv.dot_part = xpart; mv.dot_cnt = ops.d_cnt; mv.dot_k = 0;
@@ -728,13 +756,17 @@ static int qmr_graph_loop(BatchIO<T>& io, BatchOps<T>& ops, std::vector<int>& nc
         kb_dots<T><<<dim3(ops.nb, R), BT, 0, st>>>(n, sp, S.I, ops.d_part, ops.d_out, ops.d_cnt);
         note_launch();
       }
+      stamp(st, 1, 0);
       k_qg_scalars<<<1, 256, 0, st>>>(R, S, ops.d_out);
       note_launch();
+      stamp(st, 2, 0);
       kq_dsxr_pqv<C><<<dim3(ops.nb, R), BT, 0, st>>>(n, d, s, xs, r, p, q, vt, atw, S.co, S.I, ops.d_part,
                                                      ops.d_out, ops.d_cnt);
       note_launch();
+      stamp(st, 3, 0);
       k_qg_post<<<1, 32, 0, st>>>(R, tol, S, ops.d_out, h);
       note_launch();
+      stamp(st, 4, 0);
       kernels_a = launch_total() - c0;
       // IF node: the reliable-residual check
       e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps);
@@ -770,8 +802,10 @@ static int qmr_graph_loop(BatchIO<T>& io, BatchOps<T>& ops, std::vector<int>& nc
         }
       }
       if (e == cudaSuccess) {
+        stamp(st, 5, 0);
         k_qg_next<<<1, 32, 0, st>>>(R, maxit, tol, S);
         note_launch();
+        stamp(st, 6, 1);
         kernels_a += 1;
       }
     }
@@ -802,6 +836,27 @@ static int qmr_graph_loop(BatchIO<T>& io, BatchOps<T>& ops, std::vector<int>& nc
     if (e == cudaSuccess) e = cudaMemcpy(&checks, S.checks, sizeof(int), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) { set_cuda_error("graph solve", e); rc = 1; }
     note_launch((unsigned long long)launches * kernels_a + (unsigned long long)checks * kernels_b);
+    if (stamps && e == cudaSuccess) {
+      std::vector<unsigned long long> hs((size_t)8 * scap + 1);
+      if (cudaMemcpy(hs.data(), stamps, hs.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost) ==
+          cudaSuccess) {
+        const long long nit = (long long)std::min<unsigned long long>(hs[(size_t)8 * scap], (unsigned long long)scap);
+        double ph[7] = {0, 0, 0, 0, 0, 0, 0};
+        long long cntv = 0;
+        for (long long i = 0; i + 1 < nit; ++i) {
+          const unsigned long long* a = &hs[(size_t)8 * i];
+          for (int k = 0; k < 6; ++k) ph[k] += (double)(a[k + 1] - a[k]) * 1e-3;
+          ph[6] += (double)(hs[(size_t)8 * (i + 1)] - a[6]) * 1e-3;
+          ++cntv;
+        }
+        if (cntv > 0)
+          std::printf("batched QMRCCG, %d RHS, %lld iterations (us per iteration): MATVEC + vt^T A vt %.1f | "
+                      "scalars %.1f | d/s/x/r + p/q/v %.1f | residual bookkeeping %.1f | reliable-residual check "
+                      "(IF node) %.1f | next-iteration start %.1f | gap %.1f\n",
+                      R, cntv, ph[0] / cntv, ph[1] / cntv, ph[2] / cntv, ph[3] / cntv, ph[4] / cntv, ph[5] / cntv,
+                      ph[6] / cntv);
+      }
+    }
     cudaFreeHost(h_active);
     if (!rc) {
       std::vector<double> hd(nd);
@@ -830,6 +885,7 @@ static int qmr_graph_loop(BatchIO<T>& io, BatchOps<T>& ops, std::vector<int>& nc
   cudaStreamDestroy(st2);
   cudaFree(blk);
   cudaFree(xpart);
+  cudaFree(stamps);
   return rc;
 }
 
