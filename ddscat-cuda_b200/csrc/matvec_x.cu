@@ -97,23 +97,31 @@ __device__ __forceinline__ void store_pairs(C* g, int ld, int valid, const C* ti
     }
   }
 }
-// Global -> tile move of the column passes (the inverse of store_pairs): all
-// of a thread's copies are issued asynchronously at once (8-byte cp.async,
-// zero-filled beyond `valid`), so the block waits for one memory round trip;
-// completed by cp_async_wait_all + __syncthreads.
+// Global -> tile move of the column passes (the inverse of store_pairs),
+// staged through registers: all of a thread's 16-byte loads are issued before
+// its shared-memory stores (one memory round trip per block, fewer
+// instructions than 8-byte cp.async copies); rows hold `valid` elements, an even count, and the global
+// base and ld are even in elements, so every pair is 16-byte aligned.
 template <int RL, int N, typename C>
-__device__ __forceinline__ void load_tile_async(const C* g, int ld, int valid, C* tile) {
-  static_assert(sizeof(C) == 8 && (N * RL) % 256 == 0, "complex-float tiles of whole 256-thread rounds");
+__device__ __forceinline__ void load_tile_pairs(const C* g, int ld, int valid, C* tile) {
+  static_assert(sizeof(C) == 8 && (N * RL / 2) % 256 == 0, "complex-float tiles of whole 256-thread rounds");
+  constexpr int RP = RL / 2, K = N * RP / 256;
+  float4 q[K];
 #pragma unroll
-  for (int k = 0; k < N * RL / 256; ++k) {
-    const int u = threadIdx.x + 256 * k, r = u / RL, ll = u - r * RL;
-    const bool ok = ll < valid;
-    cp_async8(tile + r * (RL + 1) + ll, ok ? g + (size_t)r * ld + ll : g, ok);
+  for (int k = 0; k < K; ++k) {
+    const int u = threadIdx.x + 256 * k, r = u / RP, ll = 2 * (u - r * RP);
+    q[k] = ll < valid ? __ldg(reinterpret_cast<const float4*>(g + (size_t)r * ld + ll)) : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int u = threadIdx.x + 256 * k, r = u / RP, ll = 2 * (u - r * RP);
+    tile[r * (RL + 1) + ll] = mk<C>(q[k].x, q[k].y);
+    tile[r * (RL + 1) + ll + 1] = mk<C>(q[k].z, q[k].w);
   }
 }
 
 // Asynchronous copy of cnt (<= MAXC) contiguous elements from global to shared
-// memory with the whole 256-thread block (completed like load_tile_async).
+// memory with the whole 256-thread block (completed by cp_async_wait_all).
 template <int MAXC, typename C> __device__ __forceinline__ void stage_chunk_async(C* dst, const C* src, int cnt) {
   static_assert(sizeof(C) == 8, "complex float");
 #pragma unroll
@@ -475,8 +483,7 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_yi(XParam
   load_tw<T, N>(tws, P.twy);
   const int nz = P.nz;
   const C* B = P.B + ((size_t)(rb * 3 + c) * P.nkx + kxl) * (size_t)P.My * nz + iz0;
-  load_tile_async<RL, N>(B, nz, nz - iz0, tile);
-  cp_async_wait_all();
+  load_tile_pairs<RL, N>(B, nz, nz - iz0, tile);
   __syncthreads();
   C v[E];
 #pragma unroll
@@ -587,8 +594,8 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_xi(XParam
     stage_chunk_async<MAXC>(as, ad + q0, cnt);
   }
   const C* A = P.A + (size_t)rl * P.A_rs + ((size_t)(c * P.nz + iz) * P.Mx) * ny + iy0;
-  load_tile_async<RL, N>(A, ny, ny - iy0, tile);
-  cp_async_wait_all();
+  load_tile_pairs<RL, N>(A, ny, ny - iy0, tile);
+  cp_async_wait_all();  // the x and CXADIA chunks
   __syncthreads();
   C v[E];
 #pragma unroll
