@@ -118,6 +118,10 @@ __device__ __forceinline__ void cp_async8(void* dst, const void* src, bool ok) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(smem_addr(dst)), "l"(src), "r"(ok ? 8 : 0)
                : "memory");
 }
+// 16-byte form (both addresses 16-byte aligned)
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 // Wait for the phase of parity `par` to complete, at most `limit` polls;
 // returns false if it did not complete in that time.

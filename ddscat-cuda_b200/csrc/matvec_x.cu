@@ -71,7 +71,7 @@ template <int N> struct XShape {
   static constexpr int E = RegShape<N>::E, TT = RegShape<N>::T, H = E / 2;
   static constexpr int RL = 256 / TT;
   static constexpr int RZ = (128 / TT) > 1 ? 128 / TT : 1;  // ZG lines per block (3*TT*RZ threads)
-  static constexpr int ZG_MINB = E >= 24 ? 2 : 3;             // ZG blocks per SM the registers must allow
+  static constexpr int ZG_MINB = E >= 24 ? 2 : 3;             // ZG blocks per SM the registers must allow (FP32)
   static constexpr bool PAIR = TT >= 8;                      // 128-bit transpose stores (conflict-free for TT >= 8)
 };
 
@@ -100,34 +100,53 @@ __device__ __forceinline__ void store_pairs(C* g, int ld, int valid, const C* ti
 // Global -> tile move of the column passes (the inverse of store_pairs),
 // staged through registers: all of a thread's 16-byte loads are issued before
 // its shared-memory stores (one memory round trip per block, fewer
-// instructions than 8-byte cp.async copies); rows hold `valid` elements, an even count, and the global
-// base and ld are even in elements, so every pair is 16-byte aligned.
+// instructions than 8-byte cp.async copies).  Rows hold `valid` elements, an
+// even count, and the global base and ld are even in elements, so every
+// complex-float pair is 16-byte aligned.
 template <int RL, int N, typename C>
 __device__ __forceinline__ void load_tile_pairs(const C* g, int ld, int valid, C* tile) {
-  static_assert(sizeof(C) == 8 && (N * RL / 2) % 256 == 0, "complex-float tiles of whole 256-thread rounds");
-  constexpr int RP = RL / 2, K = N * RP / 256;
-  float4 q[K];
+  static_assert((N * RL / 2) % 256 == 0, "tiles of whole 256-thread rounds");
+  if constexpr (sizeof(C) == 8) {
+    constexpr int RP = RL / 2, K = N * RP / 256;
+    float4 q[K];
 #pragma unroll
-  for (int k = 0; k < K; ++k) {
-    const int u = threadIdx.x + 256 * k, r = u / RP, ll = 2 * (u - r * RP);
-    q[k] = ll < valid ? __ldg(reinterpret_cast<const float4*>(g + (size_t)r * ld + ll)) : make_float4(0.f, 0.f, 0.f, 0.f);
-  }
+    for (int k = 0; k < K; ++k) {
+      const int u = threadIdx.x + 256 * k, r = u / RP, ll = 2 * (u - r * RP);
+      q[k] = ll < valid ? __ldg(reinterpret_cast<const float4*>(g + (size_t)r * ld + ll))
+                        : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
 #pragma unroll
-  for (int k = 0; k < K; ++k) {
-    const int u = threadIdx.x + 256 * k, r = u / RP, ll = 2 * (u - r * RP);
-    tile[r * (RL + 1) + ll] = mk<C>(q[k].x, q[k].y);
-    tile[r * (RL + 1) + ll + 1] = mk<C>(q[k].z, q[k].w);
+    for (int k = 0; k < K; ++k) {
+      const int u = threadIdx.x + 256 * k, r = u / RP, ll = 2 * (u - r * RP);
+      tile[r * (RL + 1) + ll] = mk<C>(q[k].x, q[k].y);
+      tile[r * (RL + 1) + ll + 1] = mk<C>(q[k].z, q[k].w);
+    }
+  } else {  // complex double: one 16-byte element per load
+    constexpr int K = N * RL / 256;
+    C q[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int u = threadIdx.x + 256 * k, r = u / RL, ll = u - r * RL;
+      q[k] = ll < valid ? g[(size_t)r * ld + ll] : mk<C>(0, 0);
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int u = threadIdx.x + 256 * k, r = u / RL, ll = u - r * RL;
+      tile[r * (RL + 1) + ll] = q[k];
+    }
   }
 }
 
 // Asynchronous copy of cnt (<= MAXC) contiguous elements from global to shared
 // memory with the whole 256-thread block (completed by cp_async_wait_all).
 template <int MAXC, typename C> __device__ __forceinline__ void stage_chunk_async(C* dst, const C* src, int cnt) {
-  static_assert(sizeof(C) == 8, "complex float");
 #pragma unroll
   for (int k = 0; k < (MAXC + 255) / 256; ++k) {
     const int u = threadIdx.x + 256 * k;
-    if (u < cnt) cp_async8(dst + u, src + u, true);
+    if (u < cnt) {
+      if constexpr (sizeof(C) == 8) cp_async8(dst + u, src + u, true);
+      else cp_async16(dst + u, src + u);
+    }
   }
 }
 
@@ -259,7 +278,8 @@ __device__ __forceinline__ void green_apply(const C a[6], R sxy, R sxz, R syz, C
 // block: RZ lines x TT threads x 3 components, thread-fastest within a line;
 // lines are (kx, ky) pairs p = kxl*My + ky.  grid (nrb, ceil(nkx*My/RZ))
 template <typename T, int N>
-__global__ void __launch_bounds__(3 * XShape<N>::TT * XShape<N>::RZ, XShape<N>::ZG_MINB) kx_zg(XParams<T> P) {
+__global__ void __launch_bounds__(3 * XShape<N>::TT * XShape<N>::RZ, sizeof(T) == 8 ? 1 : XShape<N>::ZG_MINB)
+    kx_zg(XParams<T> P) {
   using C = cplx<T>;
   using R = T;
   using S_ = XShape<N>;
@@ -651,7 +671,7 @@ template <typename T, int N> static const void* xk(XPass p) {
     case XPass::YF: return (const void*)kx_yf<T, N>;
     case XPass::ZG: return (const void*)kx_zg<T, N>;
     case XPass::ZG3:
-      if constexpr (Z3Shape<N>::OK) return (const void*)kx_zg3<T, N>;
+      if constexpr (Z3Shape<N>::OK && sizeof(T) == 4) return (const void*)kx_zg3<T, N>;
       return nullptr;
     case XPass::YI: return (const void*)kx_yi<T, N>;
     default: return (const void*)kx_xi<T, N>;
@@ -659,21 +679,19 @@ template <typename T, int N> static const void* xk(XPass p) {
 }
 
 template <typename T> static const void* xkernel(XPass p, int n) {
-  if constexpr (sizeof(T) == 8) {
-    return nullptr;  // FP64 runs the z-first pipeline (xpipe_supported)
-  } else {
-    switch (n) {
-      case 16: return xk<T, 16>(p);
-      case 32: return xk<T, 32>(p);
-      case 48: return xk<T, 48>(p);
-      case 64: return xk<T, 64>(p);
-      case 96: return xk<T, 96>(p);
-      case 128: return xk<T, 128>(p);
-      case 192: return xk<T, 192>(p);
-      case 256: return xk<T, 256>(p);
-      case 512: return xk<T, 512>(p);
-      default: return nullptr;
-    }
+  switch (n) {
+    case 16: return xk<T, 16>(p);
+    case 32: return xk<T, 32>(p);
+    case 48: return xk<T, 48>(p);
+    case 64: return xk<T, 64>(p);
+    case 96: return xk<T, 96>(p);
+    case 128: return xk<T, 128>(p);
+    case 192: return xk<T, 192>(p);
+    case 256: return xk<T, 256>(p);
+    case 512:
+      if constexpr (sizeof(T) == 4) return xk<T, 512>(p);  // FP64: shared memory of the 512 passes too large
+      return nullptr;
+    default: return nullptr;
   }
 }
 
@@ -690,8 +708,8 @@ template <typename T> static int xlaunch(const void* f, dim3 g, int th, size_t s
 
 template <typename T> bool xpipe_supported(const Geometry& g) {
   if (std::getenv("DDSCAT_B200_ZFIRST")) return false;
-  if (sizeof(T) == 8) return false;  // the FP64 engine keeps the generic z-first pipeline
-  auto ok = [](int n) { return xreg_supported(n); };
+  // FP64: axis lengths up to 256 (the shared memory of the 512-point passes is too large in complex double)
+  auto ok = [](int n) { return xreg_supported(n) && (sizeof(T) == 4 || n <= 256); };
   return ok(g.Mx) && ok(g.My) && ok(g.Mz);
 }
 
