@@ -912,16 +912,25 @@ template <typename T> int solve_batch_qmrccg(BatchIO<T>& io, BatchResult& res) {
   const C* A1[3];
   const C* B1[3];
   int cj[3];
-  // ||b||
+  // ||b|| and ||x0||: A x0 is formed only for a nonzero x0 (for x0 = 0 it is
+  // exactly zero; the product still counts in NCOMPTE, as in the reference)
   A1[0] = io.b; B1[0] = io.b; cj[0] = 1;
-  if (ops.dots(1, A1, B1, cj, nullptr, o)) return 1;
+  A1[1] = xs; B1[1] = xs; cj[1] = 1;
+  if (ops.dots(2, A1, B1, cj, nullptr, o)) return 1;
+  std::vector<int> x0nz(R, 0), x0z(R, 0);
   for (int i = 0; i < R; ++i) {
-    bnorm[i] = std::sqrt(std::max(0.0, o[i].x));
+    bnorm[i] = std::sqrt(std::max(0.0, o[2 * i].x));
     if (bnorm[i] == 0.0) { res.status[i] = 52; live[i] = 0; }
+    x0nz[i] = live[i] && o[2 * i + 1].x != 0.0;
+    x0z[i] = live[i] && !x0nz[i];
   }
   const int* M = ops.mask(live);
-  int rc = c.mv(xs, sy, live);
+  int rc = c.mv(xs, sy, x0nz);
   if (rc) return rc;
+  if (any_of(x0z)) {
+    ops.zero(sy, ops.mask(x0z));
+    for (int i = 0; i < R; ++i) { c.nc[i] += x0z[i]; io.matvec_rhs += x0z[i]; }
+  }
   ops.lin(r, nullptr, io.b, one.data(), sy, mone.data(), M);
   for (C* v : {p, ap, q, d, s, atw}) ops.zero(v, M);
   ops.copy(vt, r, M);

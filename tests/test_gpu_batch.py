@@ -164,3 +164,31 @@ def test_batch_qmrccg_graph_matches_host_driven(n):
     ms, rhs, calls = dda.last_solve_stats()
     assert rhs == int(gr.ncompte.sum()) and ms > 0
     dda.release()
+
+
+@pytest.mark.gpu
+def test_batch_qmrccg_nonzero_initial_guess():
+    """A nonzero x0 enters through A x0 (formed only for the RHS whose x0 is
+    nonzero; for x0 = 0 the product is exactly zero and is skipped, still
+    counted in NCOMPTE): warm-started RHS converge in fewer iterations to the
+    same FP64-checked tolerance, zero-started ones as before."""
+    n = 16
+    prob = targets.make_problem(n, m=1.33 + 0.05j, x=3.0, orientations=targets.random_orientations(2, seed=21))
+    dda = D.DDA()
+    dda.prepare_green(n, n, n, prob.iocc, prob.incid[0].k)
+    b, adia = _batch_inputs(prob)
+    x = np.zeros_like(b)
+    first = dda.solve_batch("qmrccg", b, x, adia, maxit=500, tol=TOL, replace=True, symmetric=True, graph=True)
+    assert np.all(first.status == 0)
+    assert np.all(first.ncompte >= first.itno + 1)
+    x2 = np.zeros_like(b)
+    x2[0] = x[0] * (1.0 + 1e-3)  # warm start for RHS 0 only
+    x2[2] = x[2] * (1.0 - 1e-3)
+    second = dda.solve_batch("qmrccg", b, x2, adia, maxit=500, tol=TOL, replace=True, symmetric=True, graph=True)
+    assert np.all(second.status == 0) and np.all(second.tole <= TOL)
+    assert np.all(dda.residual_f64(b, x2, adia) <= 1.2 * TOL)
+    assert second.itno[0] < first.itno[0] and second.itno[2] < first.itno[2]
+    assert abs(int(second.itno[1]) - int(first.itno[1])) <= 1
+    ms, rhs, calls = dda.last_solve_stats()
+    assert rhs == int(second.ncompte.sum())
+    dda.release()
