@@ -71,7 +71,7 @@ template <int N> struct XShape {
   static constexpr int E = RegShape<N>::E, TT = RegShape<N>::T, H = E / 2;
   static constexpr int RL = 256 / TT;
   static constexpr int RZ = (128 / TT) > 1 ? 128 / TT : 1;  // ZG lines per block (3*TT*RZ threads)
-  static constexpr int ZG_MINB = E >= 24 ? 2 : 3;             // ZG blocks per SM the registers must allow (FP32)
+  static constexpr int ZG_MINB = E >= 32 ? 1 : (E >= 24 ? 2 : 3);  // ZG blocks per SM the registers must allow (FP32)
   static constexpr bool PAIR = TT >= 8;                      // 128-bit transpose stores (conflict-free for TT >= 8)
 };
 

@@ -54,8 +54,17 @@ int multi_solve(int nt, const int* dims, const int16_t* const* iocc, const float
     for (auto& t : T) t.release();
   };
   int first = 0;
+  double ph[4] = {0, 0, 0, 0};  // verbose: geometry, Green, workspace, inputs (s)
+  auto lap = [&](int k, std::chrono::steady_clock::time_point& a) {
+    if (!verbose) return;
+    cudaDeviceSynchronize();
+    const auto b = now();
+    ph[k] += std::chrono::duration<double>(b - a).count();
+    a = b;
+  };
   for (int i = 0; i < nt; ++i) {
     Target& t = T[i];
+    auto ta = now();
     const int nx = dims[3 * i], ny = dims[3 * i + 1], nz = dims[3 * i + 2];
     const int nat = nx * ny * nz;
     int nat0 = 0;
@@ -64,10 +73,12 @@ int multi_solve(int nt, const int* dims, const int16_t* const* iocc, const float
     if (cudaStreamCreate(&t.st) != cudaSuccess) { set_error("multi-target solve", "stream"); cleanup(); return 542; }
     int rc = t.eng.init_geometry(nx, ny, nz, 0, nat, nat0, iocc[i]);
     if (rc) { cleanup(); return 543; }
+    lap(0, ta);
     GreenArgs<float> ga;
     for (int k = 0; k < 3; ++k) ga.ak[k] = ak[3 * i + k];
     rc = t.eng.build_green(ga);
     if (rc) { cleanup(); return 543; }
+    lap(1, ta);
     if (autotune) {
       float d = 0.f, bst = 0.f;
       if (autotune_engine(t.eng, 3, &d, &bst)) { cleanup(); return 543; }
@@ -85,6 +96,7 @@ int multi_solve(int nt, const int* dims, const int16_t* const* iocc, const float
     if (e == cudaSuccess) e = cudaMalloc((void**)&t.full, full * sizeof(float2));
     if (e != cudaSuccess) { set_cuda_error("multi-target workspace", e); cleanup(); return 542; }
     if (t.ops.init(t.R, t.n, t.st)) { cleanup(); return 542; }
+    lap(2, ta);
     // inputs: full host vectors -> compact device slots
     const void* src[3] = {b[i], x[i], adia[i]};
     float2* dst[3] = {t.b, t.x, t.adia};
@@ -96,6 +108,7 @@ int multi_solve(int nt, const int* dims, const int16_t* const* iocc, const float
         v_gather<float>(t.full, dst[k] + (size_t)r * t.n, t.eng.occ, nat, nat0, t.st);
         if (check_launch("multi-target gather")) { cleanup(); return 544; }
       }
+    lap(3, ta);
   }
   cudaDeviceSynchronize();
   const auto t1 = now();
@@ -152,8 +165,10 @@ int multi_solve(int nt, const int* dims, const int16_t* const* iocc, const float
   const auto t2 = now();
   cleanup();
   if (verbose)
-    std::printf("multi-target solve: %d targets, setup (geometry, Green, inputs) %.3f s, solves %.3f s on %d threads\n",
-                nt, std::chrono::duration<double>(t1 - t0).count(), std::chrono::duration<double>(t2 - t1).count(), nw);
+    std::printf("multi-target solve: %d targets, setup %.3f s (geometry %.3f, Green %.3f, workspace %.3f, inputs "
+                "%.3f), solves %.3f s on %d threads\n",
+                nt, std::chrono::duration<double>(t1 - t0).count(), ph[0], ph[1], ph[2], ph[3],
+                std::chrono::duration<double>(t2 - t1).count(), nw);
   if (first_rc) {
     set_error("multi-target solve", first_msg.c_str());
     return first_rc;
