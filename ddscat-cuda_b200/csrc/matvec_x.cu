@@ -60,9 +60,6 @@ template <typename T> __device__ __forceinline__ bool xoff(const XParams<T>& P, 
   return P.mask != nullptr && P.mask[P.rhs0 + rl] == 0;
 }
 
-template <typename T, int N> __device__ __forceinline__ void load_tw(cplx<T>* tws, const cplx<T>* tw) {
-  for (int u = threadIdx.x; u < N; u += blockDim.x) tws[u] = tw[u];
-}
 
 // Compile-time shape of a pass over axis length N = 2n (M = 2n always in this
 // pipeline): E elements per thread, TT threads per line, H = E/2 elements per
@@ -158,14 +155,11 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_xf(XParam
   constexpr int E = S_::E, TT = S_::TT, H = S_::H, RL = S_::RL;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int t = threadIdx.x % TT, l = threadIdx.x / TT;
-  C* tws = reinterpret_cast<C*>(smem_raw);
-  C* tile = tws + N;   // [kx][RL+1], aliases the line scratch
-  C* lines = tws + N;  // RL * lsx
+  C* tile = reinterpret_cast<C*>(smem_raw);   // [kx][RL+1], aliases the line scratch
+  C* lines = reinterpret_cast<C*>(smem_raw);  // RL * lsx
   const int iy0 = blockIdx.x * RL, iy = iy0 + l, iz = blockIdx.y;
   const int rl = blockIdx.z / 3, c = blockIdx.z - 3 * (blockIdx.z / 3);
   if (xoff(P, rl)) return;
-  load_tw<T, N>(tws, P.twx);
-  __syncthreads();
   const int S = P.io_full ? P.nat : P.nat0;
   const C* x = P.x + (size_t)rl * P.x_rs + (size_t)c * S;
   const int jrow = P.nx * (iy + P.ny * iz);
@@ -194,7 +188,7 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_xf(XParam
 #pragma unroll
     for (int i = 0; i < H; ++i) v[i].y = -v[i].y;
   }
-  line_fft<E, TT, +1, false, true, S_::PAIR>(v, lines + (size_t)l * P.lsx, t, tws);
+  line_fft<E, TT, +1, false, true, S_::PAIR>(v, lines + (size_t)l * P.lsx, t, P.twx);
   __syncthreads();  // all line scratch consumed before the tile reuses it
 #pragma unroll
   for (int i = 0; i < E; ++i) tile[(t + TT * i) * (RL + 1) + l] = v[i];
@@ -211,20 +205,17 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_yf(XParam
   constexpr int E = S_::E, TT = S_::TT, H = S_::H, RL = S_::RL;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int t = threadIdx.x % TT, l = threadIdx.x / TT;
-  C* tws = reinterpret_cast<C*>(smem_raw);
-  C* tile = tws + N;
-  C* lines = tws + N;
+  C* tile = reinterpret_cast<C*>(smem_raw);
+  C* lines = reinterpret_cast<C*>(smem_raw);
   const int iz0 = blockIdx.x * RL, iz = iz0 + l, kxl = blockIdx.y, kx = P.kx0 + kxl;
   const int rb = blockIdx.z / 3, c = blockIdx.z - 3 * (blockIdx.z / 3), rl = P.b_rhs0 + rb;
   if (xoff(P, rl)) return;
-  load_tw<T, N>(tws, P.twy);
-  __syncthreads();
   const C* A = P.A + (size_t)rl * P.A_rs + ((size_t)(c * P.nz + iz) * P.Mx + kx) * P.ny;
   C v[E];
   const bool zin = iz < P.nz;
 #pragma unroll
   for (int i = 0; i < H; ++i) v[i] = zin ? A[t + TT * i] : mk<C>(0, 0);  // iy < ny = N/2
-  line_fft<E, TT, +1, false, true, S_::PAIR>(v, lines + (size_t)l * P.lsy, t, tws);
+  line_fft<E, TT, +1, false, true, S_::PAIR>(v, lines + (size_t)l * P.lsy, t, P.twy);
   __syncthreads();
 #pragma unroll
   for (int i = 0; i < E; ++i) tile[(t + TT * i) * (RL + 1) + l] = v[i];
@@ -287,13 +278,10 @@ __global__ void __launch_bounds__(3 * XShape<N>::TT * XShape<N>::RZ, sizeof(T) =
   constexpr int GT = 3 * TT;  // Green-phase threads per line
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int t = threadIdx.x % TT, l = (threadIdx.x / TT) % RL, c = threadIdx.x / (TT * RL);
-  C* tws = reinterpret_cast<C*>(smem_raw);
-  C* lines = tws + N;  // [3][RL][lsz]
+  C* lines = reinterpret_cast<C*>(smem_raw);  // [3][RL][lsz]
   C* my = lines + (size_t)(c * RL + l) * P.lsz;
   const int rb = blockIdx.x, rl = P.b_rhs0 + rb;
   if (xoff(P, rl)) return;
-  load_tw<T, N>(tws, P.twz);
-  __syncthreads();
   const int nlines = P.nkx * P.My;
   const int p = blockIdx.y * RL + l;
   const bool live = p < nlines;
@@ -301,7 +289,7 @@ __global__ void __launch_bounds__(3 * XShape<N>::TT * XShape<N>::RZ, sizeof(T) =
   C v[E];
 #pragma unroll
   for (int i = 0; i < H; ++i) v[i] = live ? row[t + TT * i] : mk<C>(0, 0);  // iz < nz = N/2
-  line_fft<E, TT, +1, false, true, S_::PAIR>(v, my, t, tws);
+  line_fft<E, TT, +1, false, true, S_::PAIR>(v, my, t, P.twz);
 #pragma unroll
   for (int i = 0; i < E; ++i) my[t + TT * i] = v[i];
   __syncthreads();
@@ -352,7 +340,7 @@ __global__ void __launch_bounds__(3 * XShape<N>::TT * XShape<N>::RZ, sizeof(T) =
 #pragma unroll
   for (int i = 0; i < E; ++i) v[i] = my[t + TT * i];
   __syncwarp();
-  line_fft<E, TT, -1, false, false, S_::PAIR>(v, my, t, tws);
+  line_fft<E, TT, -1, false, false, S_::PAIR>(v, my, t, P.twz);
   if (live) {
 #pragma unroll
     for (int i = 0; i < H; ++i) row[t + TT * i] = v[i];  // keep iz < nz
@@ -370,7 +358,7 @@ __global__ void __launch_bounds__(3 * XShape<N>::TT * XShape<N>::RZ, sizeof(T) =
 // records of its own kz values there (kz > N/2 reads the record of N - kz).
 // For E <= 16 (registers: 3E complex per thread).
 // block: RZ lines x TT threads, thread-fastest; grid (nrb, ceil(nkx*My/RZ))
-// shared memory: twiddles [N] | FFT scratch [RZ][lsz] | Green [RZ][NR][6] | mbarrier
+// shared memory: FFT scratch [RZ][lsz] | Green [RZ][NR][6] | mbarrier
 template <int N> struct Z3Shape {
   static constexpr int RZ = 128 / XShape<N>::TT;  // lines per 128-thread block
   static constexpr int NR = N / 2 + 1;            // octant records per line
@@ -402,9 +390,8 @@ template <typename T, int N> __global__ void __launch_bounds__(128, 3) kx_zg3(XP
   static_assert(Z3Shape<N>::OK, "kx_zg3 holds 3*E complex values per thread");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int t = threadIdx.x % TT, l = threadIdx.x / TT;
-  C* tws = reinterpret_cast<C*>(smem_raw);
-  C* my = tws + N + (size_t)l * P.lsz;
-  C* sg = tws + N + (size_t)RL * P.lsz;  // 16-byte aligned: N and RL*lsz are even
+  C* my = reinterpret_cast<C*>(smem_raw) + (size_t)l * P.lsz;
+  C* sg = reinterpret_cast<C*>(smem_raw) + (size_t)RL * P.lsz;  // 16-byte aligned: RL*lsz is even
   uint64_t* bar = reinterpret_cast<uint64_t*>(sg + (size_t)RL * NR * 6);
   const int rb = blockIdx.x, rl = P.b_rhs0 + rb;
   if (xoff(P, rl)) return;
@@ -422,8 +409,6 @@ template <typename T, int N> __global__ void __launch_bounds__(128, 3) kx_zg3(XP
                (uint32_t)(NR * 6 * sizeof(C)), bar);
     }
   }
-  load_tw<T, N>(tws, P.twz);
-  __syncthreads();
   const int p = p0 + l;
   const bool live = p < nlines;
   const size_t cs = (size_t)nlines * P.nz;  // component stride of B
@@ -436,10 +421,11 @@ template <typename T, int N> __global__ void __launch_bounds__(128, 3) kx_zg3(XP
   }
   // one twiddle set for the six transforms: forward, and conjugated for the inverse
   C w[E];
-  line_twiddles<E, +1>(w, t, tws);
+  line_twiddles<E, +1>(w, t, P.twz);
 #pragma unroll
   for (int c = 0; c < 3; ++c) line_fft_w<E, TT, +1, false, true, S_::PAIR>(v[c], my, t, w);
   bool ok = true;
+  __syncthreads();  // the mbarrier initialisation is visible before any thread waits on it
   if (live) {
     const int kxl = p / P.My;
     const int kx = P.kx0 + kxl, ky = p - kxl * P.My;
@@ -494,13 +480,11 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_yi(XParam
   constexpr int E = S_::E, TT = S_::TT, H = S_::H, RL = S_::RL;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int t = threadIdx.x % TT, l = threadIdx.x / TT;
-  C* tws = reinterpret_cast<C*>(smem_raw);
-  C* tile = tws + N;
-  C* lines = tws + N;
+  C* tile = reinterpret_cast<C*>(smem_raw);
+  C* lines = reinterpret_cast<C*>(smem_raw);
   const int iz0 = blockIdx.x * RL, iz = iz0 + l, kxl = blockIdx.y, kx = P.kx0 + kxl;
   const int rb = blockIdx.z / 3, c = blockIdx.z - 3 * (blockIdx.z / 3), rl = P.b_rhs0 + rb;
   if (xoff(P, rl)) return;
-  load_tw<T, N>(tws, P.twy);
   const int nz = P.nz;
   const C* B = P.B + ((size_t)(rb * 3 + c) * P.nkx + kxl) * (size_t)P.My * nz + iz0;
   load_tile_pairs<RL, N>(B, nz, nz - iz0, tile);
@@ -509,7 +493,7 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_yi(XParam
 #pragma unroll
   for (int i = 0; i < E; ++i) v[i] = tile[(t + TT * i) * (RL + 1) + l];
   __syncthreads();  // the tile is consumed before the line scratch reuses it
-  line_fft<E, TT, -1, false, false, S_::PAIR>(v, lines + (size_t)l * P.lsy, t, tws);
+  line_fft<E, TT, -1, false, false, S_::PAIR>(v, lines + (size_t)l * P.lsy, t, P.twy);
   if (iz < nz) {
     C* A = P.A + (size_t)rl * P.A_rs + ((size_t)(c * nz + iz) * P.Mx + kx) * P.ny;
 #pragma unroll
@@ -577,15 +561,13 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_xi(XParam
   constexpr bool STAGE = MAXC <= XI_STAGE_MAX;  // larger rows keep direct loads (shared memory)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int t = threadIdx.x % TT, l = threadIdx.x / TT;
-  C* tws = reinterpret_cast<C*>(smem_raw);
-  C* tile = tws + N;
-  C* lines = tws + N;
-  C* xs = tws + N + P.tlx;
+  C* tile = reinterpret_cast<C*>(smem_raw);
+  C* lines = reinterpret_cast<C*>(smem_raw);
+  C* xs = reinterpret_cast<C*>(smem_raw) + P.tlx;
   C* as = xs + MAXC;
   const int iy0 = blockIdx.x * RL, iy = iy0 + l, iz = blockIdx.y;
   const int rl = blockIdx.z / 3, c = blockIdx.z - 3 * (blockIdx.z / 3);
   if (xoff(P, rl)) return;
-  load_tw<T, N>(tws, P.twx);
   const int ny = P.ny;
   const int S = P.io_full ? P.nat : P.nat0;
   const int SA = P.a_full ? P.nat : P.nat0;
@@ -621,7 +603,7 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_xi(XParam
 #pragma unroll
   for (int i = 0; i < E; ++i) v[i] = tile[(t + TT * i) * (RL + 1) + l];
   __syncthreads();
-  line_fft<E, TT, -1, false, false, S_::PAIR>(v, lines + (size_t)l * P.lsx, t, tws);
+  line_fft<E, TT, -1, false, false, S_::PAIR>(v, lines + (size_t)l * P.lsx, t, P.twx);
   // finish (cu:116-118): y = CXADIA x - w/ngrid [+ CXAOFF terms], conj for 'C'
   C* y = P.y + (size_t)rl * P.y_rs + (size_t)c * S;
   const C* ao = P.aoff ? P.aoff + (size_t)rl * P.a_rs : nullptr;
@@ -743,13 +725,13 @@ int matvec_xpipe(Engine<T>& E, const MvArgs<T>& a) {
                : std::max(line_stride(g.Mz / TZ, TZ, RZ, false, TZ >= 8), g.Mz);
   // the transpose tile and the line scratch share one region
   P.tlx = (int)std::max((size_t)g.Mx * (RX + 1), (size_t)RX * P.lsx);
-  const size_t smx = ((size_t)g.Mx + P.tlx) * sizeof(C);
+  const size_t smx = (size_t)P.tlx * sizeof(C);
   const size_t smxi = smx + ((size_t)RX * g.nx <= (size_t)XI_STAGE_MAX ? (size_t)2 * RX * g.nx * sizeof(C) : 0);
-  const size_t smy = ((size_t)g.My + std::max((size_t)g.My * (RY + 1), (size_t)RY * P.lsy)) * sizeof(C);
-  // ZG3: twiddles, FFT scratch, Green octant lines (IPBC = 0) and the mbarrier
+  const size_t smy = std::max((size_t)g.My * (RY + 1), (size_t)RY * P.lsy) * sizeof(C);
+  // ZG3: FFT scratch, Green octant lines (IPBC = 0) and the mbarrier
   const size_t smz =
-      fzg3 ? ((size_t)g.Mz + (size_t)RZ3 * P.lsz + (g.ipbc == 0 ? (size_t)RZ3 * 6 * (g.Mz / 2 + 1) : 0)) * sizeof(C) + 16
-           : ((size_t)g.Mz + (size_t)3 * RZ * P.lsz) * sizeof(C);
+      fzg3 ? ((size_t)RZ3 * P.lsz + (g.ipbc == 0 ? (size_t)RZ3 * 6 * (g.Mz / 2 + 1) : 0)) * sizeof(C) + 16
+           : (size_t)3 * RZ * P.lsz * sizeof(C);
   const void* fxf = xkernel<T>(XPass::XF, g.Mx);
   const void* fyf = xkernel<T>(XPass::YF, g.My);
   const void* fzg = xkernel<T>(XPass::ZG, g.Mz);
