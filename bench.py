@@ -385,8 +385,33 @@ def run_ours(args):
             q64 = dda.evalq(k, use_resident=0, e=ec, p=compact(x64[r]).astype(np.complex64), adia=ac, aoff=zero)
             for key, a, c in zip(("cabs", "cext", "cpha"), q32, q64):
                 worst[key] = max(worst[key], abs(a - c) / max(abs(c), 1e-300))
+        # S_ij on 0..180 deg at 1 deg in two scattering planes per orientation:
+        # FP32 (SCAT amplitudes of the FP32 solutions) against FP64 (FP64
+        # amplitudes of the FP64 solutions), both through the Mueller entry points
+        from ddscat_b200 import targets as T
+        s11_err, sij_err, ndir = 0.0, 0.0, 0
+        for o in range(R // 2):
+            r0, r1 = 2 * o, 2 * o + 1
+            k = prob.incid[r0].k
+            aks, em1, em2 = T.scattering_planes(k, prob.incid[r0].e)
+            ndir = aks.shape[0]
+            f32 = []
+            for r in (r0, r1):
+                dda.evalq(k, use_resident=0, e=compact(b[r]), p=compact(x32[r]), adia=compact(adia[r]), aoff=zero)
+                sc = dda.scat(k, prob.incid[r].e, prob.x0, etasca=0.5, aks=aks.astype(np.float32),
+                              em1=em1.astype(np.float32), em2=em2.astype(np.float32))
+                f32.append((sc["f1"], sc["f2"]))
+            _, m32 = dda.mueller(k, prob.incid[r0].e, prob.incid[r1].e, em2.astype(np.float32),
+                                 f32[0][0], f32[0][1], f32[1][0], f32[1][1])
+            g1, g2 = dda.scat_amplitudes_f64(np.ascontiguousarray(x64[r0:r1 + 1]), k, aks, em1, em2, prob.x0)
+            _, m64 = dda.mueller_f64(k, prob.incid[r0].e, prob.incid[r1].e, em2, g1[0], g2[0], g1[1], g2[1])
+            s11 = m64[:, 0, 0]
+            s11_err = max(s11_err, float(np.max(np.abs(m32[:, 0, 0] - s11) / s11)))
+            sij_err = max(sij_err, float(np.max(np.abs(m32 - m64) / s11[:, None, None])))
         qerr = {"cabs_max_rel": worst["cabs"], "cext_max_rel": worst["cext"], "cpha_max_rel": worst["cpha"],
-                "rhs": R, "fp64_solve": f"{args.solver.upper()} all-FP64 on the GPU, tol 1e-8",
+                "s11_max_rel": s11_err, "sij_max_abs_over_s11": sij_err,
+                "s_ij_directions": f"theta 0..180 deg at 1 deg in 2 planes ({ndir}) x {R // 2} orientations",
+                "rhs": R, "fp64_solve": f"{args.solver.upper()} all-FP64 on the GPU, tol 1e-8, FP64 far-field sums",
                 "fp64_iterations_mean": float(np.mean(o64.itno))}
 
     if rank == 0:

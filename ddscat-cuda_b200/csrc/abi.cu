@@ -851,6 +851,76 @@ extern "C" DDSCAT_CUDA_API int ddscat_b200_mueller_f32(int ndir, const float* ak
                          static_cast<float2*>(s1234), smat);
 }
 
+extern "C" DDSCAT_CUDA_API int ddscat_b200_mueller_f64(int ndir, const double* ak, const void* e01, const void* e02,
+                                                       const double* em2, const void* f11, const void* f21,
+                                                       const void* f12, const void* f22, void* s1234, double* smat) {
+  clear_error();
+  if (ndir <= 0 || !ak || !e01 || !e02 || !em2 || !f11 || !f21 || !f12 || !f22 || !smat) {
+    set_error("Mueller FP64", "invalid argument");
+    return 700;
+  }
+  return mueller_compute_f64(ndir, ak, static_cast<const double2*>(e01), static_cast<const double2*>(e02), em2,
+                             static_cast<const double2*>(f11), static_cast<const double2*>(f21),
+                             static_cast<const double2*>(f12), static_cast<const double2*>(f22),
+                             static_cast<double2*>(s1234), smat);
+}
+
+extern "C" DDSCAT_CUDA_API int ddscat_b200_scat_amplitudes_f64(int nrhs, const void* x, int ndir, const double* ak,
+                                                               const double* aks, const double* em1,
+                                                               const double* em2, const double* dx, const double* x0,
+                                                               double e02, void* f1, void* f2) {
+  clear_error();
+  if (!s.ready || nrhs <= 0 || ndir <= 0 || !x || !ak || !aks || !em1 || !em2 || !dx || !x0 || !(e02 > 0.0) || !f1 ||
+      !f2) {
+    set_error("FP64 amplitudes", "invalid argument or not prepared");
+    return 710;
+  }
+  const Geometry& g = s.eng.g;
+  const size_t full = (size_t)3 * g.nat, cn = (size_t)3 * g.nat0;
+  const bool dev = is_device_ptr(x);
+  double2 *d_full = nullptr, *d_p = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (!dev) e = cudaMalloc((void**)&d_full, full * sizeof(double2));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&d_p, cn * sizeof(double2));
+  if (e != cudaSuccess) {
+    cudaFree(d_full);
+    set_cuda_error("FP64 amplitudes workspace", e);
+    return 711;
+  }
+  const double kk = std::sqrt(ak[0] * ak[0] + ak[1] * ak[1] + ak[2] * ak[2]);
+  const double term = kk * kk * kk / std::sqrt(e02);
+  std::vector<double2> sums((size_t)3 * ndir);
+  double2* h1 = static_cast<double2*>(f1);
+  double2* h2 = static_cast<double2*>(f2);
+  int rc = 0;
+  for (int r = 0; r < nrhs && !rc; ++r) {
+    const double2* src = static_cast<const double2*>(x) + (size_t)r * full;
+    if (!dev) {
+      e = cudaMemcpyAsync(d_full, src, full * sizeof(double2), cudaMemcpyHostToDevice, s.stream);
+      if (e != cudaSuccess) { set_cuda_error("FP64 amplitudes H2D", e); rc = 711; break; }
+      src = d_full;
+    }
+    v_gather<double>(src, d_p, s.eng.occ, g.nat, g.nat0, s.stream);
+    if (check_launch("FP64 amplitudes gather")) { rc = 712; break; }
+    if (farfield_sums_f64(s.eng.occ, g.nx, g.ny, g.nz, g.nat0, d_p, aks, ndir, dx, x0, sums.data(), s.stream)) {
+      rc = 712;
+      break;
+    }
+    for (int i = 0; i < ndir; ++i) {
+      const double2 sx = sums[3 * i], sy = sums[3 * i + 1], sz = sums[3 * i + 2];
+      const double* a = em1 + 3 * i;
+      const double* b = em2 + 3 * i;
+      h1[(size_t)r * ndir + i] = make_double2(term * (a[0] * sx.x + a[1] * sy.x + a[2] * sz.x),
+                                              term * (a[0] * sx.y + a[1] * sy.y + a[2] * sz.y));
+      h2[(size_t)r * ndir + i] = make_double2(term * (b[0] * sx.x + b[1] * sy.x + b[2] * sz.x),
+                                              term * (b[0] * sx.y + b[1] * sy.y + b[2] * sz.y));
+    }
+  }
+  cudaFree(d_full);
+  cudaFree(d_p);
+  return rc;
+}
+
 extern "C" DDSCAT_CUDA_API int ddscat_b200_make_inputs_f32(int nrhs, const float* k, const void* e0, const float* x0,
                                                            int nmat, const void* m, const int16_t* icomp, void* b,
                                                            void* adia) {

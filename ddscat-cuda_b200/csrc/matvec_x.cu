@@ -552,7 +552,7 @@ template <typename T> __device__ __forceinline__ void xdot_reduce(const XParams<
 constexpr int XI_STAGE_MAX = 2048;  // largest staged chunk of the XI pass (elements)
 
 // block: RL rows (iy) x TT; grid (ceil(ny/RL), nz, 3*nr)
-// shared memory: twiddles [N] | tile / line scratch [tlx] | x chunk | CXADIA chunk
+// shared memory: tile / line scratch [tlx] | x chunk | CXADIA chunk
 template <typename T, int N> __global__ void __launch_bounds__(256) kx_xi(XParams<T> P) {
   using C = cplx<T>;
   using S_ = XShape<N>;

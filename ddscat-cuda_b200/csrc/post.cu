@@ -62,9 +62,12 @@ int evalq_compute(Engine<T>& eng, VecOps<T>& ops, const cplx<T>* e, const cplx<T
 constexpr int FF_THREADS = 256;
 constexpr int FF_DIRS = 8;
 
-// tables[d][0..nx) = exp(-i kx (ix+1+x0x) dx), then ny, then nz entries
+// tables[d][0..nx) = exp(-i kx (ix+1+x0x) dx), then ny, then nz entries;
+// phases in FP64, stored as complex float (SCAT) or complex double (the
+// all-FP64 amplitudes)
+template <typename TC>
 __global__ void k_ff_tables(const double* dirs, int ndir, int nx, int ny, int nz, double dx0, double dx1, double dx2,
-                            double x00, double x01, double x02, float2* tab) {
+                            double x00, double x01, double x02, TC* tab) {
   const int ntab = nx + ny + nz;
   const size_t tot = (size_t)ndir * ntab;
   for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < tot; t += (size_t)gridDim.x * blockDim.x) {
@@ -75,7 +78,7 @@ __global__ void k_ff_tables(const double* dirs, int ndir, int nx, int ny, int nz
     else ph = dirs[3 * d + 2] * ((u - nx - ny + 1) + x02) * dx2;
     double s, c;
     sincos(ph, &s, &c);
-    tab[t] = make_float2((float)c, (float)-s);
+    tab[t] = mk<TC>(c, -s);
   }
 }
 
@@ -87,36 +90,39 @@ __global__ void k_pack_coords(const int* occ, int nat0, int nx, int ny, unsigned
   packed[q] = ix | (iy << 11) | (iz << 22);
 }
 
-template <typename C>
+// Partial sums of ND directions per block: phase products and per-thread
+// accumulation in TR (float for SCAT, double for the all-FP64 amplitudes),
+// block reduction in FP64.
+template <typename C, typename TR, int ND>
 __global__ void __launch_bounds__(FF_THREADS) k_ff_partial(const C* p, const unsigned* coords, int nat0, int ndir,
-                                                           int nx, int ny, int nz, const float2* tab, int sites_per_block,
-                                                           double2* partials) {
+                                                           int nx, int ny, int nz, const cplx<TR>* tab,
+                                                           int sites_per_block, double2* partials) {
+  using TC = cplx<TR>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2* st = reinterpret_cast<float2*>(smem_raw);
+  TC* st = reinterpret_cast<TC*>(smem_raw);
   const int ntab = nx + ny + nz;
-  const int d0 = blockIdx.y * FF_DIRS;
-  const int nd = min(FF_DIRS, ndir - d0);
+  const int d0 = blockIdx.y * ND;
+  const int nd = min(ND, ndir - d0);
   for (int t = threadIdx.x; t < nd * ntab; t += blockDim.x) st[t] = tab[(size_t)d0 * ntab + t];
   __syncthreads();
-  float acc[FF_DIRS][6];
+  TR acc[ND][6];
 #pragma unroll
-  for (int d = 0; d < FF_DIRS; ++d)
+  for (int d = 0; d < ND; ++d)
 #pragma unroll
-    for (int k = 0; k < 6; ++k) acc[d][k] = 0.f;
+    for (int k = 0; k < 6; ++k) acc[d][k] = (TR)0;
   const int q0 = blockIdx.x * sites_per_block;
   const int q1 = min(nat0, q0 + sites_per_block);
   for (int q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
     const unsigned pk = coords[q];
     const int ix = pk & 2047u, iy = (pk >> 11) & 2047u, iz = pk >> 22;
     const double2 a = to_d(p[q]), b = to_d(p[q + nat0]), c = to_d(p[q + 2 * (size_t)nat0]);
-    const float2 px = make_float2((float)a.x, (float)a.y), py = make_float2((float)b.x, (float)b.y),
-                 pz = make_float2((float)c.x, (float)c.y);
+    const TC px = mk<TC>(a.x, a.y), py = mk<TC>(b.x, b.y), pz = mk<TC>(c.x, c.y);
 #pragma unroll
-    for (int d = 0; d < FF_DIRS; ++d) {
+    for (int d = 0; d < ND; ++d) {
       if (d < nd) {
-        const float2* td = st + d * ntab;
-        const float2 e = cmul(cmul(td[ix], td[nx + iy]), td[nx + ny + iz]);
-        const float2 sx = cmul(px, e), sy = cmul(py, e), sz = cmul(pz, e);
+        const TC* td = st + d * ntab;
+        const TC e = cmul(cmul(td[ix], td[nx + iy]), td[nx + ny + iz]);
+        const TC sx = cmul(px, e), sy = cmul(py, e), sz = cmul(pz, e);
         acc[d][0] += sx.x; acc[d][1] += sx.y;
         acc[d][2] += sy.x; acc[d][3] += sy.y;
         acc[d][4] += sz.x; acc[d][5] += sz.y;
@@ -124,10 +130,10 @@ __global__ void __launch_bounds__(FF_THREADS) k_ff_partial(const C* p, const uns
     }
   }
   // block reduction in FP64: warp shuffles then shared memory
-  __shared__ double red[FF_THREADS / 32][FF_DIRS * 6];
+  __shared__ double red[FF_THREADS / 32][ND * 6];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
-  for (int d = 0; d < FF_DIRS; ++d)
+  for (int d = 0; d < ND; ++d)
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
       double v = (double)acc[d][k];
@@ -158,10 +164,12 @@ __global__ void k_ff_final(const double2* partials, int nblocks, int rows, doubl
   sums[r] = s;
 }
 
-template <typename T>
-int farfield_sums(Engine<T>& eng, const cplx<T>* p, const float* dirs_host, int ndir, const float dx[3], const float x0[3],
-                  double2* sums_host, cudaStream_t s) {
-  const int nx = eng.g.nx, ny = eng.g.ny, nz = eng.g.nz, nat0 = eng.g.nat0;
+// Far-field sums of a compact polarisation p (device) over ndir directions,
+// phases and per-thread sums in TR, ND directions per block.
+template <typename C, typename TR, int ND>
+static int ff_sums_impl(const int* occ, int nx, int ny, int nz, int nat0, const C* p, const double* dirs_host, int ndir,
+                        const double dx[3], const double x0[3], double2* sums_host, cudaStream_t s) {
+  using TC = cplx<TR>;
   if (nx > 2047 || ny > 2047 || nz > 1023) { set_error("GPU SCAT", "grid too large for packed coordinates"); return 322; }
   const int chunk = 4096;  // directions per launch
   const int sites_per_block = FF_THREADS * 32;
@@ -169,30 +177,29 @@ int farfield_sums(Engine<T>& eng, const cplx<T>* p, const float* dirs_host, int 
   const int ntab = nx + ny + nz;
   unsigned* coords = nullptr;
   double* d_dirs = nullptr;
-  float2* tab = nullptr;
+  TC* tab = nullptr;
   double2 *partials = nullptr, *sums = nullptr;
   int rc = 0;
   cudaError_t e = cudaMalloc((void**)&coords, (size_t)nat0 * sizeof(unsigned));
   if (e == cudaSuccess) e = cudaMalloc((void**)&d_dirs, (size_t)3 * chunk * sizeof(double));
-  if (e == cudaSuccess) e = cudaMalloc((void**)&tab, (size_t)chunk * ntab * sizeof(float2));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&tab, (size_t)chunk * ntab * sizeof(TC));
   if (e == cudaSuccess) e = cudaMalloc((void**)&partials, (size_t)chunk * 3 * nblocks * sizeof(double2));
   if (e == cudaSuccess) e = cudaMalloc((void**)&sums, (size_t)chunk * 3 * sizeof(double2));
   if (e != cudaSuccess) { set_cuda_error("SCAT workspace", e); rc = 322; }
   if (!rc) {
-    k_pack_coords<<<(unsigned)ceil_div(nat0, 256), 256, 0, s>>>(eng.occ, nat0, nx, ny, coords);
+    k_pack_coords<<<(unsigned)ceil_div(nat0, 256), 256, 0, s>>>(occ, nat0, nx, ny, coords);
     note_launch();
-    std::vector<double> hd((size_t)3 * chunk);
-    const size_t sm = (size_t)FF_DIRS * ntab * sizeof(float2);
-    cudaFuncSetAttribute((const void*)k_ff_partial<cplx<T>>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    const size_t sm = (size_t)ND * ntab * sizeof(TC);
+    cudaFuncSetAttribute((const void*)k_ff_partial<C, TR, ND>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     for (int off = 0; off < ndir && !rc; off += chunk) {
       const int cnt = std::min(chunk, ndir - off);
-      for (int i = 0; i < 3 * cnt; ++i) hd[i] = (double)dirs_host[(size_t)3 * off + i];
-      cudaMemcpyAsync(d_dirs, hd.data(), (size_t)3 * cnt * sizeof(double), cudaMemcpyHostToDevice, s);
-      k_ff_tables<<<(unsigned)std::min<size_t>(ceil_div((size_t)cnt * ntab, 256), 4096), 256, 0, s>>>(
+      cudaMemcpyAsync(d_dirs, dirs_host + (size_t)3 * off, (size_t)3 * cnt * sizeof(double), cudaMemcpyHostToDevice, s);
+      k_ff_tables<TC><<<(unsigned)std::min<size_t>(ceil_div((size_t)cnt * ntab, 256), 4096), 256, 0, s>>>(
           d_dirs, cnt, nx, ny, nz, dx[0], dx[1], dx[2], x0[0], x0[1], x0[2], tab);
       note_launch();
-      dim3 grid((unsigned)nblocks, (unsigned)ceil_div(cnt, FF_DIRS));
-      k_ff_partial<cplx<T>><<<grid, FF_THREADS, sm, s>>>(p, coords, nat0, cnt, nx, ny, nz, tab, sites_per_block, partials);
+      dim3 grid((unsigned)nblocks, (unsigned)ceil_div(cnt, ND));
+      k_ff_partial<C, TR, ND><<<grid, FF_THREADS, sm, s>>>(p, coords, nat0, cnt, nx, ny, nz, tab, sites_per_block,
+                                                           partials);
       note_launch();
       k_ff_final<<<(unsigned)ceil_div((size_t)cnt * 3, 128), 128, 0, s>>>(partials, nblocks, cnt * 3, sums);
       note_launch();
@@ -204,6 +211,21 @@ int farfield_sums(Engine<T>& eng, const cplx<T>* p, const float* dirs_host, int 
   }
   cudaFree(coords); cudaFree(d_dirs); cudaFree(tab); cudaFree(partials); cudaFree(sums);
   return rc;
+}
+
+template <typename T>
+int farfield_sums(Engine<T>& eng, const cplx<T>* p, const float* dirs_host, int ndir, const float dx[3], const float x0[3],
+                  double2* sums_host, cudaStream_t s) {
+  std::vector<double> hd((size_t)3 * std::max(ndir, 0));
+  for (size_t i = 0; i < hd.size(); ++i) hd[i] = (double)dirs_host[i];
+  const double dxd[3] = {dx[0], dx[1], dx[2]}, x0d[3] = {x0[0], x0[1], x0[2]};
+  return ff_sums_impl<cplx<T>, float, FF_DIRS>(eng.occ, eng.g.nx, eng.g.ny, eng.g.nz, eng.g.nat0, p, hd.data(), ndir,
+                                               dxd, x0d, sums_host, s);
+}
+
+int farfield_sums_f64(const int* occ, int nx, int ny, int nz, int nat0, const double2* p, const double* dirs_host,
+                      int ndir, const double dx[3], const double x0[3], double2* sums_host, cudaStream_t s) {
+  return ff_sums_impl<double2, double, 4>(occ, nx, ny, nz, nat0, p, dirs_host, ndir, dx, x0, sums_host, s);
 }
 
 // --------------------------------------------------------------------------
@@ -224,8 +246,9 @@ struct MuellerIn {
 __device__ __forceinline__ double2 zmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
 __device__ __forceinline__ double2 zmulc(double2 a, double2 b) { return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y); }  // a conj(b)
 
-__global__ void k_mueller(int ndir, MuellerIn in, const float* em2, const float2* f11, const float2* f21,
-                          const float2* f12, const float2* f22, float2* s_out, double* m_out) {
+template <typename R>
+__global__ void k_mueller(int ndir, MuellerIn in, const R* em2, const cplx<R>* f11, const cplx<R>* f21,
+                          const cplx<R>* f12, const cplx<R>* f22, cplx<R>* s_out, double* m_out) {
   const int d = blockIdx.x * blockDim.x + threadIdx.x;
   if (d >= ndir) return;
   const double ep[3] = {-(double)em2[3 * d], -(double)em2[3 * d + 1], -(double)em2[3 * d + 2]};  // e_perp = -EM2
@@ -243,6 +266,7 @@ __global__ void k_mueller(int ndir, MuellerIn in, const float* em2, const float2
   const double2 a11 = to_d(f11[d]), a12 = to_d(f12[d]);
   const double2 a21 = make_double2(-(double)f21[d].x, -(double)f21[d].y);  // g_2l = -f_2l
   const double2 a22 = make_double2(-(double)f22[d].x, -(double)f22[d].y);
+  using C = cplx<R>;
   auto mi = [](double2 z) { return make_double2(z.y, -z.x); };  // -i z
   auto add = [](double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); };
   const double2 S2 = mi(add(zmul(a11, cpar[0]), zmul(a12, cpar[1])));
@@ -250,10 +274,10 @@ __global__ void k_mueller(int ndir, MuellerIn in, const float* em2, const float2
   const double2 S4 = mi(add(zmul(a21, cpar[0]), zmul(a22, cpar[1])));
   const double2 S1 = mi(add(zmul(a21, cperp[0]), zmul(a22, cperp[1])));
   if (s_out) {
-    s_out[4 * d] = make_float2((float)S1.x, (float)S1.y);
-    s_out[4 * d + 1] = make_float2((float)S2.x, (float)S2.y);
-    s_out[4 * d + 2] = make_float2((float)S3.x, (float)S3.y);
-    s_out[4 * d + 3] = make_float2((float)S4.x, (float)S4.y);
+    s_out[4 * d] = mk<C>(S1.x, S1.y);
+    s_out[4 * d + 1] = mk<C>(S2.x, S2.y);
+    s_out[4 * d + 2] = mk<C>(S3.x, S3.y);
+    s_out[4 * d + 3] = mk<C>(S4.x, S4.y);
   }
   const double q1 = zabs2(S1), q2 = zabs2(S2), q3 = zabs2(S3), q4 = zabs2(S4);
   const double2 s23 = zmulc(S2, S3), s14 = zmulc(S1, S4), s24 = zmulc(S2, S4), s13 = zmulc(S1, S3);
@@ -277,9 +301,10 @@ __global__ void k_mueller(int ndir, MuellerIn in, const float* em2, const float2
   M[15] = s12.x - s34.x;
 }
 
-int mueller_compute(int ndir, const float* ak, const float2* e01, const float2* e02, const float* em2,
-                    const float2* f11, const float2* f21, const float2* f12, const float2* f22, float2* s_out,
-                    double* m_out) {
+template <typename R>
+static int mueller_impl(int ndir, const R* ak, const cplx<R>* e01, const cplx<R>* e02, const R* em2, const cplx<R>* f11,
+                        const cplx<R>* f21, const cplx<R>* f12, const cplx<R>* f22, cplx<R>* s_out, double* m_out) {
+  using C = cplx<R>;
   MuellerIn in{};
   const double kk = std::sqrt((double)ak[0] * ak[0] + (double)ak[1] * ak[1] + (double)ak[2] * ak[2]);
   if (!(kk > 0.0)) { set_error("Mueller", "zero incident wave vector"); return 700; }
@@ -288,29 +313,41 @@ int mueller_compute(int ndir, const float* ak, const float2* e01, const float2* 
     in.e0c[0][k] = make_double2(e01[k].x, -e01[k].y);
     in.e0c[1][k] = make_double2(e02[k].x, -e02[k].y);
   }
-  const size_t off_f = ((size_t)ndir * 3 * sizeof(float) + 15) & ~(size_t)15;  // 16-byte aligned f block
-  const size_t nb = off_f + (size_t)ndir * (8 * sizeof(float2) + 16 * sizeof(double));
+  const size_t off_f = ((size_t)ndir * 3 * sizeof(R) + 15) & ~(size_t)15;  // 16-byte aligned f block
+  const size_t nb = off_f + (size_t)ndir * (8 * sizeof(C) + 16 * sizeof(double));
   unsigned char* buf = nullptr;
   cudaError_t e = cudaMalloc((void**)&buf, nb);
   if (e != cudaSuccess) { set_cuda_error("Mueller workspace", e); return 701; }
-  float* d_em2 = reinterpret_cast<float*>(buf);
-  float2* d_f = reinterpret_cast<float2*>(buf + off_f);
-  float2* d_s = d_f + (size_t)4 * ndir;
+  R* d_em2 = reinterpret_cast<R*>(buf);
+  C* d_f = reinterpret_cast<C*>(buf + off_f);
+  C* d_s = d_f + (size_t)4 * ndir;
   double* d_m = reinterpret_cast<double*>(d_s + (size_t)4 * ndir);
-  const float2* hf[4] = {f11, f21, f12, f22};
-  e = cudaMemcpy(d_em2, em2, (size_t)ndir * 3 * sizeof(float), cudaMemcpyHostToDevice);
+  const C* hf[4] = {f11, f21, f12, f22};
+  e = cudaMemcpy(d_em2, em2, (size_t)ndir * 3 * sizeof(R), cudaMemcpyHostToDevice);
   for (int k = 0; k < 4 && e == cudaSuccess; ++k)
-    e = cudaMemcpy(d_f + (size_t)k * ndir, hf[k], (size_t)ndir * sizeof(float2), cudaMemcpyHostToDevice);
+    e = cudaMemcpy(d_f + (size_t)k * ndir, hf[k], (size_t)ndir * sizeof(C), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) { cudaFree(buf); set_cuda_error("Mueller H2D", e); return 702; }
-  k_mueller<<<(unsigned)ceil_div(ndir, 128), 128>>>(ndir, in, d_em2, d_f, d_f + ndir, d_f + 2 * (size_t)ndir,
-                                                    d_f + 3 * (size_t)ndir, d_s, d_m);
+  k_mueller<R><<<(unsigned)ceil_div(ndir, 128), 128>>>(ndir, in, d_em2, d_f, d_f + ndir, d_f + 2 * (size_t)ndir,
+                                                       d_f + 3 * (size_t)ndir, d_s, d_m);
   note_launch();
   if (check_launch("Mueller kernel")) { cudaFree(buf); return 703; }
-  if (s_out) e = cudaMemcpy(s_out, d_s, (size_t)ndir * 4 * sizeof(float2), cudaMemcpyDeviceToHost);
+  if (s_out) e = cudaMemcpy(s_out, d_s, (size_t)ndir * 4 * sizeof(C), cudaMemcpyDeviceToHost);
   if (e == cudaSuccess) e = cudaMemcpy(m_out, d_m, (size_t)ndir * 16 * sizeof(double), cudaMemcpyDeviceToHost);
   cudaFree(buf);
   if (e != cudaSuccess) { set_cuda_error("Mueller D2H", e); return 702; }
   return 0;
+}
+
+int mueller_compute(int ndir, const float* ak, const float2* e01, const float2* e02, const float* em2,
+                    const float2* f11, const float2* f21, const float2* f12, const float2* f22, float2* s_out,
+                    double* m_out) {
+  return mueller_impl<float>(ndir, ak, e01, e02, em2, f11, f21, f12, f22, s_out, m_out);
+}
+
+int mueller_compute_f64(int ndir, const double* ak, const double2* e01, const double2* e02, const double* em2,
+                        const double2* f11, const double2* f21, const double2* f12, const double2* f22,
+                        double2* s_out, double* m_out) {
+  return mueller_impl<double>(ndir, ak, e01, e02, em2, f11, f21, f12, f22, s_out, m_out);
 }
 
 template int evalq_compute<float>(Engine<float>&, VecOps<float>&, const float2*, const float2*, const float2*,

@@ -46,9 +46,17 @@ template <typename T>
 int farfield_sums(Engine<T>& eng, const cplx<T>* p, const float* dirs_host, int ndir, const float dx[3], const float x0[3],
                   double2* sums_host, cudaStream_t s);
 
+// The same sums with FP64 phases and FP64 accumulation (all-FP64 amplitudes);
+// occ: compact -> site map of the grid, p: compact complex-double polarisation.
+int farfield_sums_f64(const int* occ, int nx, int ny, int nz, int nat0, const double2* p, const double* dirs_host,
+                      int ndir, const double dx[3], const double x0[3], double2* sums_host, cudaStream_t s);
+
 // Amplitude and Mueller matrices per scattering direction from f_ml (host in / out).
 int mueller_compute(int ndir, const float* ak, const float2* e01, const float2* e02, const float* em2,
                     const float2* f11, const float2* f21, const float2* f12, const float2* f22, float2* s_out,
                     double* m_out);
+int mueller_compute_f64(int ndir, const double* ak, const double2* e01, const double2* e02, const double* em2,
+                        const double2* f11, const double2* f21, const double2* f12, const double2* f22,
+                        double2* s_out, double* m_out);
 
 }  // namespace ddb

@@ -30,7 +30,7 @@ EXPORTS = (
        "ddscat_b200_last_solve_stats", "ddscat_b200_residual_f64", "ddscat_b200_launch_count",
        "ddscat_b200_apply_noalloc_f32", "ddscat_b200_mueller_f32", "ddscat_b200_make_inputs_f32",
        "ddscat_b200_solve_batch_f64", "ddscat_b200_adjoint_f32", "ddscat_b200_multi_solve_f32",
-       "ddscat_b200_autotune_f32"]
+       "ddscat_b200_autotune_f32", "ddscat_b200_mueller_f64", "ddscat_b200_scat_amplitudes_f64"]
 )
 
 
@@ -102,6 +102,10 @@ def _declare(lib):
     lib.ddscat_b200_multi_solve_f32.restype = _I
     lib.ddscat_b200_autotune_f32.argtypes = [_I, _P, _P]
     lib.ddscat_b200_autotune_f32.restype = _I
+    lib.ddscat_b200_mueller_f64.argtypes = [_I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _D]
+    lib.ddscat_b200_mueller_f64.restype = _I
+    lib.ddscat_b200_scat_amplitudes_f64.argtypes = [_I, _P, _I, _P, _P, _P, _P, _P, _P, _D2, _P, _P]
+    lib.ddscat_b200_scat_amplitudes_f64.restype = _I
     lib.ddscat_b200_launch_count.argtypes = []
     lib.ddscat_b200_launch_count.restype = ct.c_ulonglong
 
@@ -405,6 +409,44 @@ class DDA:
                                               _ptr(s), m.ctypes.data_as(_D))
         self._check("mueller", rc)
         return s, m
+
+    def mueller_f64(self, ak, e01, e02, em2, f11, f21, f12, f22):
+        """mueller() with complex-double amplitudes (e.g. from scat_amplitudes_f64):
+        (S1..S4 (ndir, 4) complex128, S_ij (ndir, 4, 4))."""
+        f = [np.ascontiguousarray(v, dtype=np.complex128) for v in (f11, f21, f12, f22)]
+        ndir = f[0].size
+        akd = np.ascontiguousarray(ak, dtype=np.float64)
+        e1 = np.ascontiguousarray(e01, dtype=np.complex128)
+        e2 = np.ascontiguousarray(e02, dtype=np.complex128)
+        em2d = np.ascontiguousarray(em2, dtype=np.float64).reshape(ndir, 3)
+        s = np.zeros((ndir, 4), dtype=np.complex128)
+        m = np.zeros((ndir, 4, 4), dtype=np.float64)
+        rc = self.lib.ddscat_b200_mueller_f64(ndir, _ptr(akd), _ptr(e1), _ptr(e2), _ptr(em2d),
+                                              *[_ptr(v) for v in f], _ptr(s), m.ctypes.data_as(_D))
+        self._check("mueller_f64", rc)
+        return s, m
+
+    def scat_amplitudes_f64(self, x, ak, aks, em1, em2, x0, dx=(1.0, 1.0, 1.0), e02=1.0):
+        """All-FP64 scattering amplitudes (f1, f2), each (nrhs, ndir) complex128,
+        of the polarisations x ((nrhs, 3*NAT) complex128, NumPy or CUDA tensor),
+        normalised like the f1/f2 of scat()."""
+        nrhs = int(x.shape[0])
+        if not hasattr(x, "data_ptr") and (x.dtype != np.complex128 or not x.flags.c_contiguous):
+            raise ValueError("x must be a C-contiguous complex128 array")
+        aksd = np.ascontiguousarray(aks, dtype=np.float64).reshape(-1, 3)
+        ndir = aksd.shape[0]
+        em1d = np.ascontiguousarray(em1, dtype=np.float64).reshape(ndir, 3)
+        em2d = np.ascontiguousarray(em2, dtype=np.float64).reshape(ndir, 3)
+        akd = np.ascontiguousarray(ak, dtype=np.float64)
+        dxd = np.ascontiguousarray(dx, dtype=np.float64)
+        x0d = np.ascontiguousarray(x0, dtype=np.float64)
+        f1 = np.zeros((nrhs, ndir), dtype=np.complex128)
+        f2 = np.zeros((nrhs, ndir), dtype=np.complex128)
+        rc = self.lib.ddscat_b200_scat_amplitudes_f64(nrhs, _vptr(x), ndir, _ptr(akd), _ptr(aksd), _ptr(em1d),
+                                                      _ptr(em2d), _ptr(dxd), _ptr(x0d), float(e02), _ptr(f1),
+                                                      _ptr(f2))
+        self._check("scat_amplitudes_f64", rc)
+        return f1, f2
 
     def autotune(self, iters=5):
         """Tune the prepared target's FFT launch shapes; returns (default ms, best ms) per MATVEC."""

@@ -166,6 +166,30 @@ def embed_ellipsoid(sides, semi, grid="fast"):
     return (gx, gy, gz), occ.reshape(-1)
 
 
+def scattering_planes(k, e01, step_deg=1.0, phis_deg=(0.0, 90.0)):
+    """Scattering directions theta = 0..180 deg (step_deg) in the planes
+    phi = phis_deg, phi measured from the incident polarisation e01 about k,
+    with DDSCAT's SCAT basis: AKS = |k| n, EM1 = theta-hat, EM2 = n x EM1.
+    Returns float64 arrays (ndir, 3) aks, em1, em2."""
+    k = np.asarray(k, dtype=np.float64)
+    kk = float(np.linalg.norm(k))
+    kh = k / kk
+    e1 = np.real(np.asarray(e01)).astype(np.float64)
+    e1 = e1 - kh * float(kh @ e1)
+    e1 /= np.linalg.norm(e1)
+    e2 = np.cross(kh, e1)
+    aks, em1, em2 = [], [], []
+    for phi in np.deg2rad(np.asarray(phis_deg, dtype=np.float64)):
+        u = math.cos(phi) * e1 + math.sin(phi) * e2
+        for t in np.deg2rad(np.arange(0.0, 180.0 + 0.5 * step_deg, step_deg)):
+            n = math.cos(t) * kh + math.sin(t) * u
+            th = -math.sin(t) * kh + math.cos(t) * u
+            aks.append(kk * n)
+            em1.append(th)
+            em2.append(np.cross(n, th))
+    return np.array(aks), np.array(em1), np.array(em2)
+
+
 def make_problem(nx, ny=None, nz=None, m=1.5 + 0.01j, x=5.0, semi=None, orientations=None, iocc=None):
     """Ellipsoid (sphere by default) of size parameter x = k*aeff; one RHS per
     (orientation, polarisation) with k along x before rotation and

@@ -125,6 +125,27 @@ DDSCAT_CUDA_API int ddscat_b200_mueller_f32(int ndir, const float *ak, const voi
                                             const float *em2, const void *f11, const void *f21, const void *f12,
                                             const void *f22, void *s1234, double *smat);
 
+/* The same with complex-double amplitudes and FP64 vectors (s1234 ndir x 4
+ * complex doubles): the Mueller matrix of an all-FP64 reference solve.  No
+ * counterpart in the reference.  Codes as ddscat_b200_mueller_f32. */
+DDSCAT_CUDA_API int ddscat_b200_mueller_f64(int ndir, const double *ak, const void *e01, const void *e02,
+                                            const double *em2, const void *f11, const void *f21, const void *f12,
+                                            const void *f22, void *s1234, double *smat);
+
+/* All-FP64 scattering amplitudes f1, f2 of nrhs polarisations at ndir
+ * directions, with the normalisation of the f1/f2 outputs of
+ * ddscat_cuda_scat_f32 (|k|^3/sqrt(E02) sum_j EM . P_j exp(-i AKS . r_j),
+ * r_j = ((i+1)+X0)*DX), but FP64 phases and FP64 sums: the reference values the
+ * S_ij of an FP32 solve are checked against.  No counterpart in the reference
+ * (its SCAT sums FP32 phases).  x: nrhs full component-major complex-double
+ * polarisations (3*NAT each, host or device) of the prepared target; aks, em1,
+ * em2: ndir x 3; f1, f2: nrhs x ndir complex doubles (host).  Codes: 710
+ * invalid argument or not prepared, 711 allocation, 712 far-field sums. */
+DDSCAT_CUDA_API int ddscat_b200_scat_amplitudes_f64(int nrhs, const void *x, int ndir, const double *ak,
+                                                    const double *aks, const double *em1, const double *em2,
+                                                    const double *dx, const double *x0, double e02, void *f1,
+                                                    void *f2);
+
 /* Right-hand sides and CXADIA for nrhs incident waves, generated on the GPU
  * for the prepared target (DDSCAT computes them on the host in EVALE and
  * ALPHADIAG; no counterpart in the reference ABI).  k: nrhs x 3 wave vectors in

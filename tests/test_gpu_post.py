@@ -150,3 +150,50 @@ def test_mueller_of_dda_sphere():
     assert abs(m[0, 2, 2] - s11[0]) <= 1e-4 * s11[0] and abs(m[0, 0, 1]) <= 1e-4 * s11[0]
     assert np.allclose(np.sum(m ** 2, axis=(1, 2)), 4 * s11 ** 2, rtol=1e-5)
     dda.release()
+
+
+@pytest.mark.gpu
+def test_scat_amplitudes_f64_matches_oracle_and_fp32_scat():
+    """ddscat_b200_scat_amplitudes_f64 equals the FP64 oracle far-field sums
+    (1e-11 relative) and the FP32 SCAT amplitudes of the same polarisation to
+    the FP32 phase-table tolerance (1e-5 of the largest amplitude)."""
+    prob, dda, out, occ, b, adia = _solved()
+    k = prob.incid[0].k
+    e01 = prob.incid[0].e
+    aks, em1, em2 = targets.scattering_planes(k, e01, step_deg=5.0)
+    x64 = out.x.astype(np.complex128)[None, :]
+    f1, f2 = dda.scat_amplitudes_f64(x64, k, aks, em1, em2, prob.x0)
+    pc = O.gather_compact(x64[0], occ, prob.nat)
+    sums = O.farfield_sums(pc, occ, prob.nx, prob.ny, aks, (1.0, 1.0, 1.0), prob.x0)
+    term = np.linalg.norm(k) ** 3
+    r1 = term * np.einsum("dc,dc->d", em1, sums)
+    r2 = term * np.einsum("dc,dc->d", em2, sums)
+    scale = max(np.abs(r1).max(), np.abs(r2).max())
+    assert np.abs(f1[0] - r1).max() <= 1e-11 * scale
+    assert np.abs(f2[0] - r2).max() <= 1e-11 * scale
+    sc = dda.scat(k, e01, prob.x0, etasca=0.5, aks=aks.astype(np.float32), em1=em1.astype(np.float32),
+                  em2=em2.astype(np.float32))
+    assert np.abs(sc["f1"] - f1[0]).max() <= 1e-5 * scale
+    assert np.abs(sc["f2"] - f2[0]).max() <= 1e-5 * scale
+    dda.release()
+
+
+@pytest.mark.gpu
+def test_mueller_f64_matches_oracle_and_f32():
+    """ddscat_b200_mueller_f64 equals the oracle's Bohren & Huffman amplitude and
+    Mueller matrices to 1e-12 and agrees with the complex-float entry point on
+    the same (rounded) amplitudes to 1e-6 of S11."""
+    rng = np.random.default_rng(4)
+    k = np.array([0.3, -0.2, 0.5])
+    e01, e02 = np.array([0.0, 1.0, 0.0], dtype=np.complex128), np.array([0.0, 0.0, 1.0], dtype=np.complex128)
+    aks, em1, em2 = targets.scattering_planes(k, np.cross(k, [1.0, 0.0, 0.0]), step_deg=10.0)
+    nd = aks.shape[0]
+    f = [rng.normal(size=nd) + 1j * rng.normal(size=nd) for _ in range(4)]
+    dda = D.DDA()
+    s64, m64 = dda.mueller_f64(k, e01, e02, em2, *f)
+    S = O.amplitude_matrix(k, e01, e02, em2, *f)
+    M = O.mueller_from_amplitude(S)
+    assert np.abs(s64 - S).max() <= 1e-12 * np.abs(S).max()
+    assert np.abs(m64 - M).max() <= 1e-12 * np.abs(M).max()
+    s32, m32 = dda.mueller(k.astype(np.float32), e01, e02, em2.astype(np.float32), *[v.astype(np.complex64) for v in f])
+    assert np.abs(m32 - m64).max() <= 1e-6 * np.abs(m64[:, 0, 0]).max()
