@@ -520,9 +520,17 @@ struct QGState {
 };
 
 __device__ __forceinline__ double2 dmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+// a / b by Smith's scaled algorithm (R. L. Smith, CACM 5(8), 1962), which
+// avoids the overflow and underflow of |b|^2 the way the host's complex
+// division does, so a stagnating recurrence with extreme scalars takes the same
+// breakdown decisions on the device as on the host
 __device__ __forceinline__ double2 ddiv(double2 a, double2 b) {
-  const double d = b.x * b.x + b.y * b.y;
-  return make_double2((a.x * b.x + a.y * b.y) / d, (a.y * b.x - a.x * b.y) / d);
+  if (fabs(b.x) >= fabs(b.y)) {
+    const double r = b.y / b.x, d = b.x + b.y * r;
+    return make_double2((a.x + a.y * r) / d, (a.y - a.x * r) / d);
+  }
+  const double r = b.x / b.y, d = b.y + b.x * r;
+  return make_double2((a.x * r + a.y) / d, (a.y * r - a.x) / d);
 }
 __device__ __forceinline__ double2 dsc(double s, double2 a) { return make_double2(s * a.x, s * a.y); }
 __device__ __forceinline__ bool dz0(double2 a) { return a.x == 0.0 && a.y == 0.0; }
@@ -677,28 +685,23 @@ static int qmr_graph_loop(BatchIO<T>& io, BatchOps<T>& ops, std::vector<int>& nc
   for (int k = 0; k < 7; ++k) *ip[k] = ii + (size_t)k * R;
   S.active = ii + (size_t)7 * R;
   S.checks = S.active + 1;
-  {
-    std::vector<double2> hz(nz2, make_double2(0, 0));
-    for (int k = 0; k < 9; ++k)
-      for (int i = 0; i < R; ++i) hz[(size_t)k * R + i] = dz(sc[k][i]);
-    for (int i = 0; i < R; ++i) { hz[(size_t)16 * R + i] = make_double2(1, 0); hz[(size_t)17 * R + i] = make_double2(-1, 0); }
-    std::vector<double> hd(nd);
-    for (int i = 0; i < R; ++i) { hd[i] = bnorm[i]; hd[R + i] = resid[i]; }
-    std::vector<int> hi(ni, 0);
-    for (int i = 0; i < R; ++i) {
-      hi[i] = it[i]; hi[R + i] = live[i]; hi[2 * R + i] = status[i]; hi[3 * R + i] = nc[i];
-    }
-    e = cudaMemcpy(z, hz.data(), nz2 * sizeof(double2), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(dd, hd.data(), nd * sizeof(double), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(ii, hi.data(), ni * sizeof(int), cudaMemcpyHostToDevice);
-    if (e != cudaSuccess) { cudaFree(blk); set_cuda_error("graph solve state", e); return 1; }
+  // initial device state (uploaded on the solve's own stream below)
+  std::vector<double2> hz(nz2, make_double2(0, 0));
+  for (int k = 0; k < 9; ++k)
+    for (int i = 0; i < R; ++i) hz[(size_t)k * R + i] = dz(sc[k][i]);
+  for (int i = 0; i < R; ++i) { hz[(size_t)16 * R + i] = make_double2(1, 0); hz[(size_t)17 * R + i] = make_double2(-1, 0); }
+  std::vector<double> hd0(nd);
+  for (int i = 0; i < R; ++i) { hd0[i] = bnorm[i]; hd0[R + i] = resid[i]; }
+  std::vector<int> hi0(ni, 0);
+  for (int i = 0; i < R; ++i) {
+    hi0[i] = it[i]; hi0[R + i] = live[i]; hi0[2 * R + i] = status[i]; hi0[3 * R + i] = nc[i];
   }
   // phase stamps of the iterations (verbose only)
   const bool verbose = std::getenv("DDSCAT_B200_VERBOSE") != nullptr;
   const int scap = io.maxit + 64;
   unsigned long long* stamps = nullptr;
-  if (verbose && cudaMalloc((void**)&stamps, (size_t)(8 * scap + 1) * sizeof(unsigned long long)) == cudaSuccess)
-    cudaMemset(stamps, 0, (size_t)(8 * scap + 1) * sizeof(unsigned long long));
+  if (verbose && cudaMalloc((void**)&stamps, (size_t)(8 * scap + 1) * sizeof(unsigned long long)) != cudaSuccess)
+    stamps = nullptr;
   auto stamp = [&](cudaStream_t s_, int slot, int bump) {
     if (stamps) k_qg_stamp<<<1, 1, 0, s_>>>(stamps, scap, slot, bump);
   };
@@ -712,9 +715,21 @@ static int qmr_graph_loop(BatchIO<T>& io, BatchOps<T>& ops, std::vector<int>& nc
   cudaStreamSynchronize(ops.stream);
   e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking);
+  // Every upload is ordered on st: st does not synchronise with the legacy
+  // default stream, so a plain cudaMemcpy (whose DMA from pageable memory may
+  // still be in flight when it returns) or cudaMemset could land after the
+  // first kernels on st read the state.
+  if (e == cudaSuccess) e = cudaMemcpyAsync(z, hz.data(), nz2 * sizeof(double2), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dd, hd0.data(), nd * sizeof(double), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ii, hi0.data(), ni * sizeof(int), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && stamps)
+    e = cudaMemsetAsync(stamps, 0, (size_t)(8 * scap + 1) * sizeof(unsigned long long), st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // the host vectors may be released afterwards
   if (e != cudaSuccess) {
+    if (st) cudaStreamDestroy(st);
+    if (st2) cudaStreamDestroy(st2);
     cudaFree(blk); cudaFree(xpart); cudaFree(stamps);
-    set_cuda_error("graph solve streams", e);
+    set_cuda_error("graph solve streams and state", e);
     return 1;
   }
   Engine<T>& eng = *io.eng;

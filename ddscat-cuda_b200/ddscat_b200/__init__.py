@@ -322,7 +322,7 @@ class DDA:
         return grad, lam, it, tole
 
     def multi_solve(self, targets_, name="qmrccg", maxit=1000, tol=1e-5, replace=True, symmetric=True, nthreads=0,
-                    check=True, autotune=False):
+                    check=True, autotune=False, graph=False):
         """Solve many targets of uneven size together.  targets_: list of dicts
         with dims (nx, ny, nz), iocc (NAT int16), ak (3,), b, x, adia
         ((nrhs, 3*NAT) complex64 host arrays; x in/out).  Returns BatchOut over
@@ -349,6 +349,7 @@ class DDA:
         st = np.zeros(total, dtype=np.int32)
         code = BATCH_SOLVERS[name] | (REPLACE_RESIDUAL if replace else 0) | (QMR_SYMMETRIC if symmetric else 0)
         code |= AUTOTUNE if autotune else 0
+        code |= GRAPH if graph else 0
         rc = self.lib.ddscat_b200_multi_solve_f32(nt, _ptr(dims), ct.cast(po, ct.c_void_p), _ptr(aks), _ptr(nr),
                                                   ct.cast(pb, ct.c_void_p), ct.cast(px, ct.c_void_p),
                                                   ct.cast(pa, ct.c_void_p), code, maxit, tol, nthreads, _ptr(it),

@@ -52,3 +52,30 @@ def test_c4_uneven_multi_target():
         for r in range(2):
             assert np.linalg.norm(xs[r] - it["x"][r]) / np.linalg.norm(xs[r]) < 20 * TOL
     dda.release()
+
+
+@pytest.mark.gpu
+def test_multi_target_graph_solves_concurrent_equal_serial():
+    """The graph-driven QMRCCG of several targets run by concurrent host threads
+    (one CUDA stream each) gives the same iterations and solutions as the same
+    solves run one after another: every target's state reaches the GPU in its
+    own stream order."""
+    probs = c4_targets(count=8, seed=3)
+
+    def items():
+        out = []
+        for p in probs:
+            b = np.stack([p.rhs(r) for r in range(2)])
+            out.append({"dims": (p.nx, p.ny, p.nz), "iocc": p.iocc, "ak": p.incid[0].k, "b": b,
+                        "x": np.zeros_like(b), "adia": np.stack([p.adia(r) for r in range(2)])})
+        return out
+
+    dda = D.DDA()
+    one, eight = items(), items()
+    a = dda.multi_solve(one, "qmrccg", maxit=3000, tol=TOL, symmetric=True, graph=True, nthreads=1, check=False)
+    b = dda.multi_solve(eight, "qmrccg", maxit=3000, tol=TOL, symmetric=True, graph=True, nthreads=8, check=False)
+    assert np.all(a.status == 0) and np.all(b.status == 0)
+    np.testing.assert_array_equal(a.itno, b.itno)
+    for u, v in zip(one, eight):
+        np.testing.assert_array_equal(u["x"], v["x"])
+    dda.release()
