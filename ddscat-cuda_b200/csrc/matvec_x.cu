@@ -12,10 +12,14 @@
 //   YI : B (transposed load)       -> y-FFT(-i), keep n_y -> A
 //   XI : A (transposed load)       -> x-FFT(-i), keep n_x -> finish -> y
 // The Green octant is stored z-fastest, [irx][iry][irz][6], so a z-line reads
-// contiguous 48-byte records, and each record is loaded once for kz and its
-// mirror M_z - kz.  The ZG grid runs RHS-fastest so consecutive blocks reuse
-// the Green tile from L2.  The middle passes run over kx batches (all of M_x for
-// the FFT3D build, 4 columns for the SLICES build).
+// contiguous 48-byte records: kx_zg3 (the ZG pass for E <= 16, FP32) copies a
+// block's octant lines to shared memory with bulk asynchronous copies and
+// keeps the three components of a z position in one thread; kx_zg (larger E,
+// FP64) loads each record once for kz and its mirror M_z - kz and exchanges
+// the components through shared memory.  The ZG grid runs RHS-fastest so
+// consecutive blocks reuse the Green tile from L2.  Twiddles are read from
+// global memory (L1/L2 resident tables).  The middle passes run over kx
+// batches (all of M_x for the FFT3D build, a few columns for the SLICES build).
 #include <algorithm>
 #include <cstdlib>
 #include "engine.h"
