@@ -94,6 +94,9 @@ template <typename T> struct Engine {
   // prepare, changed by the autotuner): register-pass block sizes, y-pass
   // columns per block, complex elements per generic-pass tile (0: default)
   int tune_thz = 256, tune_thx = 256, tune_ly = 4, tune_tile = 0;
+  // x-first z pass: 0 = three components per thread (kx_zg3, where it applies),
+  // 1 = components exchanged through shared memory (kx_zg)
+  int tune_zg = 0;
   cudaStream_t stream = 0;
   size_t bytes_allocated = 0;
 
@@ -145,6 +148,8 @@ template <typename T> bool xpipe_supported(const Geometry& g);
 // to its grid and keeps the fastest; default_ms / best_ms per call.
 int autotune_engine(Engine<float>& e, int iters, float* default_ms, float* best_ms);
 template <typename T> int matvec_xpipe(Engine<T>& E, const MvArgs<T>& a);
+// whether the FP32 x-first pipeline has the components-per-thread z pass for length Mz
+bool xzg3_supported(int Mz);
 // partials per RHS of the fused x*y sum of the x-first pipeline (MvArgs::dot_out)
 size_t xdot_blocks(const Geometry& g);
 template <typename T> int interleave_green_zfast(Engine<T>& E, const cplx<T>* planar);

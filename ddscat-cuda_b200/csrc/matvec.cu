@@ -590,6 +590,7 @@ int Engine<T>::init_geometry(int nx, int ny, int nz, int ipbc, int nat, int nat0
   tune_thx = env_int("DDSCAT_B200_TH_X", 256);
   tune_ly = std::max(1, env_int("DDSCAT_B200_LY", 4));
   tune_tile = env_int("DDSCAT_B200_TILE", 0);
+  tune_zg = std::getenv("DDSCAT_B200_ZG") ? 1 : 0;
   if (px.nstages < 0 || py.nstages < 0 || pz.nstages < 0) {
     set_error("prepare", "FFT length has too many prime factors");
     return 1;
@@ -850,10 +851,13 @@ int autotune_engine(Engine<float>& e, int iters, float* default_ms, float* best_
     *ms /= iters;
     return 0;
   };
-  struct Shape { int thz, thx, ly, tile; };
-  const Shape def{e.tune_thz, e.tune_thx, e.tune_ly, e.tune_tile};
+  struct Shape { int thz, thx, ly, tile, zg; };
+  const Shape def{e.tune_thz, e.tune_thx, e.tune_ly, e.tune_tile, e.tune_zg};
   std::vector<Shape> cands{def};
-  if (!e.xpipe) {
+  if (e.xpipe) {
+    // the two z passes of the x-first pipeline, where both apply (E <= 16)
+    if (xzg3_supported(g.Mz)) cands.push_back({def.thz, def.thx, def.ly, def.tile, 1 - def.zg});
+  } else {
     const bool rz = reg_supported(g.Mz), rx = reg_supported(g.Mx), ry = reg_supported(g.My);
     const std::vector<int> thzs = rz ? std::vector<int>{128, 256} : std::vector<int>{def.thz};
     const std::vector<int> thxs = rx ? std::vector<int>{128, 256} : std::vector<int>{def.thx};
@@ -866,13 +870,14 @@ int autotune_engine(Engine<float>& e, int iters, float* default_ms, float* best_
     for (int a1 : thzs)
       for (int a2 : thxs)
         for (int a3 : lys)
-          for (int a4 : tiles) cands.push_back({a1, a2, a3, a4});
+          for (int a4 : tiles) cands.push_back({a1, a2, a3, a4, def.zg});
   }
   int rc = 0;
   float dms = 0.f, bms = 0.f;
   Shape best = def;
   for (size_t k = 0; k < cands.size() && !rc; ++k) {
     e.tune_thz = cands[k].thz; e.tune_thx = cands[k].thx; e.tune_ly = cands[k].ly; e.tune_tile = cands[k].tile;
+    e.tune_zg = cands[k].zg;
     float ms = 0.f;
     if (time_it(&ms)) {
       if (k == 0) { rc = 1; break; }  // the default shape must run
@@ -883,6 +888,7 @@ int autotune_engine(Engine<float>& e, int iters, float* default_ms, float* best_
     if (ms < bms) { bms = ms; best = cands[k]; }
   }
   e.tune_thz = best.thz; e.tune_thx = best.thx; e.tune_ly = best.ly; e.tune_tile = best.tile;
+  e.tune_zg = best.zg;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   cudaFree(x); cudaFree(y); cudaFree(ad);

@@ -692,6 +692,8 @@ template <typename T> static int xlaunch(const void* f, dim3 g, int th, size_t s
   return 0;
 }
 
+bool xzg3_supported(int Mz) { return xkernel<float>(XPass::ZG3, Mz) != nullptr; }
+
 template <typename T> bool xpipe_supported(const Geometry& g) {
   if (std::getenv("DDSCAT_B200_ZFIRST")) return false;
   // FP64: axis lengths up to 256 (the shared memory of the 512-point passes is too large in complex double)
@@ -719,8 +721,9 @@ int matvec_xpipe(Engine<T>& E, const MvArgs<T>& a) {
   const int TX = rT(g.Mx), TY = rT(g.My), TZ = rT(g.Mz);
   const int RX = 256 / TX, RY = 256 / TY;
   const int RZ = std::max(1, 128 / TZ);  // ZG: 3*TZ*RZ threads
-  // ZG3 (components in registers, E <= 16) unless DDSCAT_B200_ZG=1 selects ZG
-  const void* fzg3 = std::getenv("DDSCAT_B200_ZG") ? nullptr : xkernel<T>(XPass::ZG3, g.Mz);
+  // ZG3 (components in registers, E <= 16) unless the engine's tunable (autotuner
+  // or DDSCAT_B200_ZG=1) selects ZG
+  const void* fzg3 = E.tune_zg ? nullptr : xkernel<T>(XPass::ZG3, g.Mz);
   const int RZ3 = 128 / TZ;  // ZG3: RZ3 lines of TZ threads
   // must match XShape<N>::PAIR
   P.lsx = line_stride(g.Mx / TX, TX, RX, false, TX >= 8);

@@ -1,7 +1,8 @@
 """FFT launch-shape autotuner (ddscat_b200_autotune_f32): on grids that run the
-z-first pipeline (non-power-of-two and mixed axes) the chosen shape is never
-slower than the default (the default is a candidate) and the MATVEC still
-matches the FP64 oracle (relative L2 <= 2e-5)."""
+z-first pipeline (non-power-of-two and mixed axes) it picks launch shapes, on
+grids of the x-first pipeline (24^3: 48-point axes; 32x24x16) it picks between
+the two z passes; the choice is never slower than the default (the default is
+a candidate) and the MATVEC still matches the FP64 oracle (relative L2 <= 2e-5)."""
 import numpy as np
 import pytest
 
