@@ -269,13 +269,17 @@ def run_ours(args):
     xd = torch.zeros_like(bd)
     stats = {"iters": [], "ncompte": [], "res64": [], "resolves": 0, "mv_ms": 0.0, "mv_rhs": 0, "mv_calls": 0}
 
-    def solve_to_fp64(bx, xx, ax, on_device):
-        """One step: batched solve, FP64 true residuals, re-solve failures."""
+    def solve_to_fp64(bx, xx, ax, on_device, on_solved=None):
+        """One step: batched solve, FP64 true residuals, re-solve failures.
+        on_solved() runs once the first solve has returned (its x is final
+        unless an RHS fails the FP64 check); returns (out, res, re-solve rounds)."""
         rep = args.policy == "replace"
         sym = args.solver == "qmrccg" and args.qmr_form == "symmetric"
         gr = sym and rep and args.graph == "on"
         out = dda.solve_batch(args.solver, bx, xx, ax, None, maxit=args.maxit, tol=args.tol, replace=rep,
                               symmetric=sym, graph=gr)
+        if on_solved is not None:
+            on_solved()
         ms, rhs, calls = dda.last_solve_stats()
         stats["mv_ms"] += ms
         stats["mv_rhs"] += rhs
@@ -296,11 +300,11 @@ def run_ours(args):
             res[bad] = dda.residual_f64(sub(bx), xs, sub(ax))
             stats["resolves"] += len(bad)
             rounds += 1
-        return out, res
+        return out, res, rounds
 
     def step_dev(record):
         xd.zero_()
-        out, res = solve_to_fp64(bd, xd, ad, True)
+        out, res, _ = solve_to_fp64(bd, xd, ad, True)
         if record:
             stats["iters"] += list(out.itno)
             stats["ncompte"] += list(out.ncompte)
@@ -339,12 +343,26 @@ def run_ours(args):
     xo = torch.empty_like(bh).pin_memory()
     be, ae, xe = torch.empty_like(bd), torch.empty_like(ad), torch.empty_like(bd)
 
+    # the read-back of x runs on a side stream, overlapped with the FP64
+    # residual check of the same x (both only read it); it is repeated if a
+    # re-solve changed x, and every step waits for it
+    d2h = torch.cuda.Stream(device=dev)
+
+    def start_d2h():
+        ev = torch.cuda.Event()
+        ev.record()
+        d2h.wait_event(ev)
+        with torch.cuda.stream(d2h):
+            xo.copy_(xe, non_blocking=True)
+
     def step_host():
         be.copy_(bh, non_blocking=True)
         ae.copy_(ah, non_blocking=True)
         xe.copy_(xh, non_blocking=True)
-        solve_to_fp64(be, xe, ae, True)
-        xo.copy_(xe)
+        _, _, rounds = solve_to_fp64(be, xe, ae, True, start_d2h)
+        torch.cuda.current_stream().wait_stream(d2h)
+        if rounds:
+            xo.copy_(xe)
 
     step_host()  # warm-up of the host path
     barrier(pg, local)
