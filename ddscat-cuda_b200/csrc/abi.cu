@@ -338,7 +338,7 @@ template <typename Src> __global__ void k_to_f64(const Src* a, double2* b, size_
 static int ensure_f64() {
   if (f64.ready) return 0;
   const Geometry& g = s.eng.g;
-  int rc = f64.eng.init_geometry(g.nx, g.ny, g.nz, g.ipbc, g.nat, g.nat0, s.h_iocc);
+  int rc = f64.eng.init_geometry(g.nx, g.ny, g.nz, g.ipbc, g.nat, g.nat0, s.h_iocc, s.prep_kind == 1);
   if (rc) { release_f64(); return 1; }
   if (s.prep_kind == 1) {
     GreenArgs<double> ga;
@@ -464,7 +464,7 @@ DDSCAT_CUDA_API int ddscat_cuda_prepare_green_f32(int nx, int ny, int nz, int ip
   if (ipbc && gamma <= 0.f) { set_error("prepare_green", "GAMMA must be >0 for PBC"); return 202; }
   if (!s.verbose) s.verbose = env_verbose();
   release_state();
-  int rc = s.eng.init_geometry(nx, ny, nz, ipbc, nat, nat0, iocc);
+  int rc = s.eng.init_geometry(nx, ny, nz, ipbc, nat, nat0, iocc, true);
   if (rc) { release_state(); return rc == 2 ? 208 : 204; }
   GreenArgs<float> ga;
   ga.idipint = idipint; ga.gamma = gamma; ga.pyd = pyd; ga.pzd = pzd;

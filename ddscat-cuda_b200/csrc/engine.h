@@ -32,11 +32,17 @@ unsigned long long launch_total();     // kernels launched so far (note_launch c
 void note_launch(unsigned long long k = 1);
 
 // ---------------------------------------------------------------- geometry
+// M_a is the padded FFT length of axis a: 2 n_a as in the reference, or, for
+// a library-built Green tensor with IPBC = 0, the next length >= 2 n_a that the
+// register-FFT pipeline runs (the circulant embedding of the lags -(n-1)..n-1
+// is exact for any M >= 2n - 1; the spectrum is still even per axis, so the
+// octant k_a = 0..M_a/2 holds it).
 struct Geometry {
   int nx = 0, ny = 0, nz = 0, Mx = 0, My = 0, Mz = 0;
   int nat = 0, nat0 = 0, ipbc = 0;
   size_t ngrid() const { return (size_t)Mx * My * Mz; }
-  size_t octant() const { return (size_t)(nx + 1) * (ny + 1) * (nz + 1); }
+  size_t octant() const { return (size_t)(Mx / 2 + 1) * (My / 2 + 1) * (Mz / 2 + 1); }
+  bool padded() const { return Mx != 2 * nx || My != 2 * ny || Mz != 2 * nz; }
   size_t green_count() const { return ipbc == 0 ? 6 * octant() : 6 * ngrid(); }
 };
 
@@ -97,10 +103,17 @@ template <typename T> struct Engine {
   // x-first z pass: 0 = three components per thread (kx_zg3, where it applies),
   // 1 = components exchanged through shared memory (kx_zg)
   int tune_zg = 0;
+  // elements per RHS of the first-pass grid: the z-transformed grid (z-first)
+  // or the x-transformed grid A (x-first)
+  size_t zhat_per_rhs() const {
+    return xpipe ? (size_t)3 * g.nz * g.Mx * g.ny : (size_t)3 * g.Mz * g.ny * g.nx;
+  }
   cudaStream_t stream = 0;
   size_t bytes_allocated = 0;
 
-  int init_geometry(int nx, int ny, int nz, int ipbc, int nat, int nat0, const int16_t* iocc_host);
+  // pad: the Green tensor will be built here (build_green), so the FFT lengths
+  // may be padded beyond 2n onto the register-FFT pipeline
+  int init_geometry(int nx, int ny, int nz, int ipbc, int nat, int nat0, const int16_t* iocc_host, bool pad = false);
   int build_green(const GreenArgs<T>& ga);          // on-GPU direct sum + FFT to the octant
   int upload_green(const void* host_green);         // CPU-supplied CXZC (ddscat_cuda_prepare_f32)
   int interleave_green(const C* planar_dev);        // planar [6][P] -> green [P][6]
@@ -144,6 +157,8 @@ template <typename T> void v_scatter(const cplx<T>* compact, cplx<T>* full, cons
 
 // x-first transposed pipeline (matvec_x.cu)
 template <typename T> bool xpipe_supported(const Geometry& g);
+// smallest register-pipeline FFT length >= m for T (0 if none)
+template <typename T> int xpipe_len(int m);
 // Times the MATVEC of a prepared FP32 engine under the launch shapes that apply
 // to its grid and keeps the fastest; default_ms / best_ms per call.
 int autotune_engine(Engine<float>& e, int iters, float* default_ms, float* best_ms);

@@ -14,7 +14,7 @@
 namespace ddb {
 
 struct GreenDev {
-  int nx, ny, nz, ipbc, idipint;
+  int nx, ny, nz, Mx, My, Mz, ipbc, idipint;
   double gamma, akx, aky, akz, dx1, dx2, dx3, akd, akd2, pyddx, pzddx;
 };
 
@@ -216,13 +216,17 @@ __device__ void green_sum_lag(int lx, int ly, int lz, const GreenDev& p, double2
 __global__ void __launch_bounds__(256) k_green_x(GreenDev p, FftPlan plan, const double2* tw, double2* out, int nxo,
                                                  int* status) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int Mx = 2 * p.nx, My = 2 * p.ny, Mz = 2 * p.nz, LD = Mx + 1;
+  const int Mx = p.Mx, My = p.My, Mz = p.Mz, LD = Mx + 1;
   double2* A = reinterpret_cast<double2*>(smem_raw);
   double2* B = A + 6 * LD;
   const int iy = blockIdx.x, iz = blockIdx.y;
   for (int ix = threadIdx.x; ix < Mx; ix += blockDim.x) {
     double2 c[6];
-    if (ix == p.nx || iy == p.ny || iz == p.nz) {
+    // lags -(n-1)..n-1 at FFT indices 0..n-1 and M-n+1..M-1; the indices
+    // between (lag n for M = 2n, cu:644) are zero
+    const bool gap = (ix >= p.nx && ix <= Mx - p.nx) || (iy >= p.ny && iy <= My - p.ny) ||
+                     (iz >= p.nz && iz <= Mz - p.nz);
+    if (gap) {
       for (int m = 0; m < 6; ++m) c[m] = make_double2(0.0, 0.0);
     } else {
       const int lx = ix < p.nx ? ix : ix - Mx, ly = iy < p.ny ? iy : iy - My, lz = iz < p.nz ? iz : iz - Mz;
@@ -274,7 +278,8 @@ static double2* twiddles_d(int n) {
 
 template <typename T> int Engine<T>::build_green(const GreenArgs<T>& ga) {
   GreenDev p{};
-  p.nx = g.nx; p.ny = g.ny; p.nz = g.nz; p.ipbc = g.ipbc; p.idipint = ga.idipint;
+  p.nx = g.nx; p.ny = g.ny; p.nz = g.nz; p.Mx = g.Mx; p.My = g.My; p.Mz = g.Mz;
+  p.ipbc = g.ipbc; p.idipint = ga.idipint;
   p.gamma = ga.gamma;
   p.akx = ga.ak[0]; p.aky = ga.ak[1]; p.akz = ga.ak[2];
   p.dx1 = ga.dx[0]; p.dx2 = ga.dx[1]; p.dx3 = ga.dx[2];
@@ -283,7 +288,7 @@ template <typename T> int Engine<T>::build_green(const GreenArgs<T>& ga) {
   p.pyddx = ga.pyd * ga.dx[1];
   p.pzddx = ga.pzd * ga.dx[2];
   const int Mx = g.Mx, My = g.My, Mz = g.Mz;
-  const int nxo = g.ipbc == 0 ? g.nx + 1 : Mx, nyo = g.ipbc == 0 ? g.ny + 1 : My, nzo = g.ipbc == 0 ? g.nz + 1 : Mz;
+  const int nxo = g.ipbc == 0 ? Mx / 2 + 1 : Mx, nyo = g.ipbc == 0 ? My / 2 + 1 : My, nzo = g.ipbc == 0 ? Mz / 2 + 1 : Mz;
   double2 *twx_d = twiddles_d(Mx), *twy_d = twiddles_d(My), *twz_d = twiddles_d(Mz);
   double2 *a1 = nullptr, *a2 = nullptr;
   int* d_status = nullptr;

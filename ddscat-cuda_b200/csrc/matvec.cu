@@ -125,9 +125,9 @@ __device__ __forceinline__ void green_at(const MvParams<T>& P, int kx, int ky, i
   size_t b;
   T sxy = (T)1, sxz = (T)1, syz = (T)1;
   if (P.ipbc == 0) {
-    const T sx = kx <= P.nx ? (T)1 : (T)-1, sy = ky <= P.ny ? (T)1 : (T)-1, sz = kz <= P.nz ? (T)1 : (T)-1;
+    const T sx = 2 * kx <= P.Mx ? (T)1 : (T)-1, sy = 2 * ky <= P.My ? (T)1 : (T)-1, sz = 2 * kz <= P.Mz ? (T)1 : (T)-1;
     const int irx = min(kx, P.Mx - kx), iry = min(ky, P.My - ky), irz = min(kz, P.Mz - kz);
-    b = (size_t)irx + (size_t)(P.nx + 1) * ((size_t)iry + (size_t)(P.ny + 1) * irz);
+    b = (size_t)irx + (size_t)(P.Mx / 2 + 1) * ((size_t)iry + (size_t)(P.My / 2 + 1) * irz);
     sxy = sx * sy; sxz = sx * sz; syz = sy * sz;
   } else {
     b = (size_t)kx + (size_t)P.Mx * ((size_t)ky + (size_t)P.My * kz);
@@ -578,10 +578,19 @@ template <typename T> static cplx<T>* upload_twiddles(int n, size_t& bytes) {
 }
 
 template <typename T>
-int Engine<T>::init_geometry(int nx, int ny, int nz, int ipbc, int nat, int nat0, const int16_t* iocc_host) {
+int Engine<T>::init_geometry(int nx, int ny, int nz, int ipbc, int nat, int nat0, const int16_t* iocc_host, bool pad) {
   g.nx = nx; g.ny = ny; g.nz = nz;
   g.Mx = 2 * nx; g.My = 2 * ny; g.Mz = 2 * nz;
   g.nat = nat; g.nat0 = nat0; g.ipbc = ipbc;
+  if (pad && ipbc == 0 && nx % 2 == 0 && ny % 2 == 0 && nz % 2 == 0 && !std::getenv("DDSCAT_B200_NOPAD") &&
+      !xpipe_supported<T>(g)) {
+    // pad to the register-FFT lengths when the padded grid has at most 2.5x the
+    // points of the 2n grid (the register pipeline is ~4x faster per point);
+    // even n only (the row passes move element pairs of 16 bytes)
+    Geometry p = g;
+    p.Mx = xpipe_len<T>(2 * nx); p.My = xpipe_len<T>(2 * ny); p.Mz = xpipe_len<T>(2 * nz);
+    if (p.Mx && p.My && p.Mz && (double)p.ngrid() <= 2.5 * (double)g.ngrid() && xpipe_supported<T>(p)) g = p;
+  }
   px = make_fft_plan(g.Mx);
   py = make_fft_plan(g.My);
   pz = make_fft_plan(g.Mz);
@@ -641,7 +650,7 @@ int Engine<T>::init_geometry(int nx, int ny, int nz, int ipbc, int nat, int nat0
 }
 
 template <typename T> int Engine<T>::ensure_workspace(int nrhs) {
-  const size_t per_rhs_z = (size_t)3 * g.Mz * g.ny * g.nx;
+  const size_t per_rhs_z = zhat_per_rhs();
   // one middle-stage plane, 3 comps, one RHS: a kz plane (z-first) or a kx column plane (x-first)
   const size_t per_plane = xpipe ? (size_t)3 * g.My * g.nz : (size_t)3 * g.ny * g.Mx;
   const int nplanes_all = xpipe ? g.Mx : g.Mz;
@@ -677,7 +686,7 @@ template <typename T> int Engine<T>::matvec(const MvArgs<T>& a) {
   raise_smem_limit((const void*)k_zinv_fin<T>);
   {
     // z-spectrum capacity: all RHS of the call if they fit the budget
-    const size_t per_rhs_z = (size_t)3 * g.Mz * g.ny * g.nx * sizeof(C);
+    const size_t per_rhs_z = zhat_per_rhs() * sizeof(C);
     const size_t budget = (size_t)env_int("DDSCAT_B200_ZHAT_MB", 16384) * 1024 * 1024;
     const int want = (int)std::max<size_t>(1, std::min<size_t>((size_t)a.nrhs, budget / per_rhs_z));
     if (ensure_workspace(want)) return 1;

@@ -65,9 +65,10 @@ template <typename T> __device__ __forceinline__ bool xoff(const XParams<T>& P, 
 }
 
 
-// Compile-time shape of a pass over axis length N = 2n (M = 2n always in this
-// pipeline): E elements per thread, TT threads per line, H = E/2 elements per
-// thread inside the n real points, RL lines per 256-thread row block.
+// Compile-time shape of a pass over the padded axis length N >= 2n: E elements
+// per thread, TT threads per line, H = E/2 elements per thread in the first
+// half N/2 >= n (those with index >= n are masked), RL lines per 256-thread
+// row block.
 template <int N> struct XShape {
   static constexpr int E = RegShape<N>::E, TT = RegShape<N>::T, H = E / 2;
   static constexpr int RL = 256 / TT;
@@ -79,7 +80,7 @@ template <int N> struct XShape {
 // Tile <-> global moves of the row passes: N rows of RL consecutive elements
 // (row stride ld in global, RL+1 in the tile), two elements per 16-byte access.
 // Rows hold `valid` elements (RL or fewer at the grid edge; always even,
-// since every axis length n = N/2 >= 8 and RL are even).  The global base and
+// since every axis length n is even here and RL is even).  The global base and
 // ld are even in elements, so every pair is 16-byte aligned.
 template <int RL, int N, typename C>
 __device__ __forceinline__ void store_pairs(C* g, int ld, int valid, const C* tile) {
@@ -170,7 +171,7 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_xf(XParam
   C v[E];
   if (P.io_full) {
 #pragma unroll
-    for (int i = 0; i < H; ++i) v[i] = iy < P.ny ? x[jrow + t + TT * i] : mk<C>(0, 0);  // ix < nx = N/2
+    for (int i = 0; i < H; ++i) v[i] = iy < P.ny && t + TT * i < P.nx ? x[jrow + t + TT * i] : mk<C>(0, 0);  // ix < nx <= N/2
   } else {
     // the block's rows hold one contiguous compact range [q0, q0 + cnt): copy
     // it to shared memory (coalesced) while the inv lookups are in flight,
@@ -179,7 +180,7 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_xf(XParam
     const int q0 = P.rowq[r0], cnt = P.rowq[r0 + nrows] - q0;
     int qi[H];
 #pragma unroll
-    for (int i = 0; i < H; ++i) qi[i] = iy < P.ny ? P.inv[jrow + t + TT * i] : -1;
+    for (int i = 0; i < H; ++i) qi[i] = iy < P.ny && t + TT * i < P.nx ? P.inv[jrow + t + TT * i] : -1;
     C* chunk = lines;  // at most RL*nx elements; consumed before the FFT uses the scratch
     stage_chunk_async<RL * (N / 2)>(chunk, x + q0, cnt);
     cp_async_wait_all();
@@ -218,7 +219,7 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_yf(XParam
   C v[E];
   const bool zin = iz < P.nz;
 #pragma unroll
-  for (int i = 0; i < H; ++i) v[i] = zin ? A[t + TT * i] : mk<C>(0, 0);  // iy < ny = N/2
+  for (int i = 0; i < H; ++i) v[i] = zin && t + TT * i < P.ny ? A[t + TT * i] : mk<C>(0, 0);  // iy < ny <= N/2
   line_fft<E, TT, +1, false, true, S_::PAIR>(v, lines + (size_t)l * P.lsy, t, P.twy);
   __syncthreads();
 #pragma unroll
@@ -234,9 +235,9 @@ __device__ __forceinline__ const cplx<T>* green_rec(const XParams<T>& P, int kx,
                                                     T& syz) {
   size_t b;
   if (P.ipbc == 0) {
-    const T sx = kx <= P.nx ? (T)1 : (T)-1, sy = ky <= P.ny ? (T)1 : (T)-1;
+    const T sx = 2 * kx <= P.Mx ? (T)1 : (T)-1, sy = 2 * ky <= P.My ? (T)1 : (T)-1;
     const int irx = min(kx, P.Mx - kx), iry = min(ky, P.My - ky);
-    b = ((size_t)irx * (P.ny + 1) + iry) * (P.nz + 1) + kz;
+    b = ((size_t)irx * (P.My / 2 + 1) + iry) * (P.Mz / 2 + 1) + kz;
     sxy = sx * sy; sxz = sx; syz = sy;  // times sz, applied by the caller
   } else {
     b = ((size_t)kx * P.My + ky) * P.Mz + kz;
@@ -292,7 +293,7 @@ __global__ void __launch_bounds__(3 * XShape<N>::TT * XShape<N>::RZ, sizeof(T) =
   C* row = P.B + ((size_t)(rb * 3 + c) * P.nkx) * (size_t)P.My * P.nz + (size_t)p * P.nz;
   C v[E];
 #pragma unroll
-  for (int i = 0; i < H; ++i) v[i] = live ? row[t + TT * i] : mk<C>(0, 0);  // iz < nz = N/2
+  for (int i = 0; i < H; ++i) v[i] = live && t + TT * i < P.nz ? row[t + TT * i] : mk<C>(0, 0);  // iz < nz <= N/2
   line_fft<E, TT, +1, false, true, S_::PAIR>(v, my, t, P.twz);
 #pragma unroll
   for (int i = 0; i < E; ++i) my[t + TT * i] = v[i];
@@ -347,7 +348,8 @@ __global__ void __launch_bounds__(3 * XShape<N>::TT * XShape<N>::RZ, sizeof(T) =
   line_fft<E, TT, -1, false, false, S_::PAIR>(v, my, t, P.twz);
   if (live) {
 #pragma unroll
-    for (int i = 0; i < H; ++i) row[t + TT * i] = v[i];  // keep iz < nz
+    for (int i = 0; i < H; ++i)
+      if (t + TT * i < P.nz) row[t + TT * i] = v[i];  // keep iz < nz
   }
 }
 
@@ -421,7 +423,8 @@ template <typename T, int N> __global__ void __launch_bounds__(128, 3) kx_zg3(XP
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
 #pragma unroll
-    for (int i = 0; i < H; ++i) v[c][i] = live ? row[c * cs + t + TT * i] : mk<C>(0, 0);  // iz < nz = N/2
+    for (int i = 0; i < H; ++i)
+      v[c][i] = live && t + TT * i < P.nz ? row[c * cs + t + TT * i] : mk<C>(0, 0);  // iz < nz <= N/2
   }
   // one twiddle set for the six transforms: forward, and conjugated for the inverse
   C w[E];
@@ -470,7 +473,8 @@ template <typename T, int N> __global__ void __launch_bounds__(128, 3) kx_zg3(XP
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
 #pragma unroll
-      for (int i = 0; i < H; ++i) row[c * cs + t + TT * i] = v[c][i];  // keep iz < nz
+      for (int i = 0; i < H; ++i)
+        if (t + TT * i < P.nz) row[c * cs + t + TT * i] = v[c][i];  // keep iz < nz
     }
   }
   if (!ok) mbar_wait(bar, 0, ZG3_WAIT_POLLS);  // no copy may land after the block exits
@@ -501,7 +505,8 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_yi(XParam
   if (iz < nz) {
     C* A = P.A + (size_t)rl * P.A_rs + ((size_t)(c * nz + iz) * P.Mx + kx) * P.ny;
 #pragma unroll
-    for (int i = 0; i < H; ++i) A[t + TT * i] = v[i];  // keep iy < ny
+    for (int i = 0; i < H; ++i)
+      if (t + TT * i < P.ny) A[t + TT * i] = v[i];  // keep iy < ny
   }
 }
 
@@ -593,7 +598,7 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_xi(XParam
 #pragma unroll
   for (int i = 0; i < H; ++i) {
     const int j = jrow + t + TT * i;  // ix < nx
-    qi[i] = iy < ny ? (P.io_full ? (P.iocc[j] != 0 ? j : -1) : P.inv[j]) : -1;
+    qi[i] = iy < ny && t + TT * i < P.nx ? (P.io_full ? (P.iocc[j] != 0 ? j : -1) : P.inv[j]) : -1;
   }
   if (chunked) {
     stage_chunk_async<MAXC>(xs, x + (size_t)c * S + q0, cnt);
@@ -615,6 +620,7 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_xi(XParam
 #pragma unroll
   for (int i = 0; i < H; ++i) {
     if (iy >= ny) break;
+    if (t + TT * i >= P.nx) continue;  // padded FFT length: ix beyond the row
     const int j = jrow + t + TT * i;
     const int q = qi[i];
     if (q < 0) {
@@ -733,7 +739,10 @@ int matvec_xpipe(Engine<T>& E, const MvArgs<T>& a) {
   // the transpose tile and the line scratch share one region
   P.tlx = (int)std::max((size_t)g.Mx * (RX + 1), (size_t)RX * P.lsx);
   const size_t smx = (size_t)P.tlx * sizeof(C);
-  const size_t smxi = smx + ((size_t)RX * g.nx <= (size_t)XI_STAGE_MAX ? (size_t)2 * RX * g.nx * sizeof(C) : 0);
+  // XI: the x and CXADIA chunks of RX rows, each sized as the kernel lays them
+  // out (MAXC = RL * N/2 elements, which is RX * nx only when Mx = 2 nx)
+  const size_t xi_maxc = (size_t)RX * (g.Mx / 2);
+  const size_t smxi = smx + (xi_maxc <= (size_t)XI_STAGE_MAX ? 2 * xi_maxc * sizeof(C) : 0);
   const size_t smy = std::max((size_t)g.My * (RY + 1), (size_t)RY * P.lsy) * sizeof(C);
   // ZG3: FFT scratch, Green octant lines (IPBC = 0) and the mbarrier
   const size_t smz =
@@ -792,7 +801,8 @@ template <typename C> __global__ void k_interleave6_zfast(const C* src, C* dst, 
 
 template <typename T> int interleave_green_zfast(Engine<T>& E, const cplx<T>* planar) {
   const Geometry& g = E.g;
-  const int X = g.ipbc == 0 ? g.nx + 1 : g.Mx, Y = g.ipbc == 0 ? g.ny + 1 : g.My, Z = g.ipbc == 0 ? g.nz + 1 : g.Mz;
+  const int X = g.ipbc == 0 ? g.Mx / 2 + 1 : g.Mx, Y = g.ipbc == 0 ? g.My / 2 + 1 : g.My,
+            Z = g.ipbc == 0 ? g.Mz / 2 + 1 : g.Mz;
   const size_t n = (size_t)6 * X * Y * Z;
   k_interleave6_zfast<cplx<T>><<<(unsigned)std::min<size_t>(ceil_div(n, 256), 148 * 32), 256, 0, E.stream>>>(
       planar, E.green, X, Y, Z);
@@ -800,6 +810,14 @@ template <typename T> int interleave_green_zfast(Engine<T>& E, const cplx<T>* pl
   return check_launch("Green interleave (z-fastest)");
 }
 
+template <typename T> int xpipe_len(int m) {
+  for (int L : {16, 32, 48, 64, 96, 128, 192, 256, 512})
+    if (L >= m && xreg_supported(L) && (sizeof(T) == 4 || L <= 256)) return L;
+  return 0;
+}
+
+template int xpipe_len<float>(int);
+template int xpipe_len<double>(int);
 template bool xpipe_supported<float>(const Geometry&);
 template bool xpipe_supported<double>(const Geometry&);
 template int matvec_xpipe<float>(Engine<float>&, const MvArgs<float>&);

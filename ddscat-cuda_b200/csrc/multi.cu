@@ -71,7 +71,7 @@ int multi_solve(int nt, const int* dims, const int16_t* const* iocc, const float
     for (int j = 0; j < nat; ++j) nat0 += iocc[i][j] != 0;
     if (nat0 == 0) { set_error("multi-target solve", "a target has no occupied site"); cleanup(); return 540; }
     if (cudaStreamCreate(&t.st) != cudaSuccess) { set_error("multi-target solve", "stream"); cleanup(); return 542; }
-    int rc = t.eng.init_geometry(nx, ny, nz, 0, nat, nat0, iocc[i]);
+    int rc = t.eng.init_geometry(nx, ny, nz, 0, nat, nat0, iocc[i], true);
     if (rc) { cleanup(); return 543; }
     lap(0, ta);
     GreenArgs<float> ga;

@@ -83,10 +83,15 @@ extern "C" DDSCAT_CUDA_API int ddscat_b200_apply_noalloc_f32(int cwhat, const vo
   // A shallow copy of the prepared engine whose workspace is the fixed array:
   // one RHS, every middle-stage plane in one batch.
   Engine<float> e = *prep;
-  const size_t nat = (size_t)e.g.nat;
+  const size_t za = e.zhat_per_rhs();
+  const size_t sb = e.xpipe ? (size_t)3 * e.g.My * e.g.nz * e.g.Mx : (size_t)3 * e.g.ny * e.g.Mx * e.g.Mz;
+  if (za + sb > (size_t)NOALLOC_SCRATCH_ELEMS) {
+    set_error("apply_noalloc", "the padded FFT grid of this target does not fit the fixed scratch (48 MiB)");
+    return 601;
+  }
   e.zhat = scratch;
   e.zcap = 1;
-  e.slab = scratch + 6 * nat;
+  e.slab = scratch + za;
   e.slab_nr = 1;
   e.slab_B = e.xpipe ? e.g.Mx : e.g.Mz;
   e.stream = static_cast<cudaStream_t>(stream);

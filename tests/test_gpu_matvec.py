@@ -41,7 +41,10 @@ def _err(y, yr):
                                           ((32, 32, 32), 0), ((16, 8, 32), 1), ((64, 32, 16), 0), ((8, 64, 16), 0),
                                           ((128, 16, 8), 1), ((64, 64, 64), 0),
                                           # 3 * 2^k padded lengths (x-first pipeline with 12/24-point DFTs)
-                                          ((24, 24, 24), 0), ((48, 24, 96), 1), ((96, 32, 24), 0), ((48, 48, 48), 0)])
+                                          ((24, 24, 24), 0), ((48, 24, 96), 1), ((96, 32, 24), 0), ((48, 48, 48), 0),
+                                          # even n whose 2n is no register-FFT length: padded FFT lengths
+                                          # (40, 52, 28 -> 48, 64, 32; 100, 20, 60 -> 128, 32, 64)
+                                          ((20, 26, 14), 1), ((50, 10, 30), 0)])
 def test_apply_matches_oracle(layout, dims, idipint):
     iocc, ak, x, adia, aoff, gp = _case(dims, idipint)
     dda = D.DDA(layout)
@@ -114,4 +117,21 @@ def test_apply_is_linear_and_symmetric():
     s1 = np.dot(z.astype(np.complex128), ax.astype(np.complex128))
     s2 = np.dot(x.astype(np.complex128), az.astype(np.complex128))
     assert abs(s1 - s2) / abs(s1) < 1e-5
+    dda.release()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dims", [(20, 26, 14), (40, 36, 32)])
+def test_padded_fft_lengths_equal_2n(dims, monkeypatch):
+    """With a library-built Green tensor, even grids whose 2n is no register-FFT
+    length run on padded FFT lengths (next register length >= 2n); the operator
+    equals the one on the 2n grid (DDSCAT_B200_NOPAD=1) to FP32 rounding."""
+    iocc, ak, x, adia, aoff, gp = _case(dims, 0, seed=6)
+    dda = D.DDA()
+    dda.prepare_green(*dims, iocc, ak)
+    y_pad = dda.apply(x, adia, aoff)
+    monkeypatch.setenv("DDSCAT_B200_NOPAD", "1")
+    dda.prepare_green(*dims, iocc, ak)
+    y_2n = dda.apply(x, adia, aoff)
+    assert _err(y_pad, y_2n)[0] <= 1e-5
     dda.release()
