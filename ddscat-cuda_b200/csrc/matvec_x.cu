@@ -11,6 +11,10 @@
 //   ZG : B z-rows (n_z)            -> z-FFT(+i) * Green * z-FFT(-i), keep n_z
 //   YI : B (transposed load)       -> y-FFT(-i), keep n_y -> A
 //   XI : A (transposed load)       -> x-FFT(-i), keep n_x -> finish -> y
+// Optionally (DDSCAT_B200_FUSEXY=1; FP32, M_x and M_y up to 256, FFT3D build)
+// the x and y passes of a z plane run fused in one cluster of four CTAs (XYF,
+// XYI below): the plane meets in distributed shared memory instead of an HBM
+// round trip of A, and B is laid out [c][kx][iz][ky] for them.
 // The Green octant is stored z-fastest, [irx][iry][irz][6], so a z-line reads
 // contiguous 48-byte records: kx_zg3 (the ZG pass for E <= 16, FP32) copies a
 // block's octant lines to shared memory with bulk asynchronous copies and
@@ -22,6 +26,7 @@
 // batches (all of M_x for the FFT3D build, a few columns for the SLICES build).
 #include <algorithm>
 #include <cstdlib>
+#include <cooperative_groups.h>
 #include "engine.h"
 #include "fftreg.cuh"
 
@@ -44,7 +49,7 @@ template <typename T> struct XParams {
   int rhs0;
   cplx<T>* A;  // [rl][c][iz][kx][iy]
   size_t A_rs;
-  cplx<T>* B;  // [rb][c][kxl][ky][iz] for kx in [kx0, kx0 + nkx)
+  cplx<T>* B;  // [rb][c][kxl][ky][iz] for kx in [kx0, kx0 + nkx); fused xy passes: [rb][c][kx][iz][ky]
   int kx0, nkx, b_rhs0;
   const cplx<T>* green;  // [irx][iry][irz][6] (IPBC=0) or [kx][ky][kz][6] (IPBC=1)
   int ipbc;
@@ -270,10 +275,24 @@ __device__ __forceinline__ void green_apply(const C a[6], R sxy, R sxz, R syz, C
   pz = cadd(cadd(cmul(a13, x), cmul(a23, y)), cmul(a[5], z));
 }
 
+// Offset of z position 0 of line p = kxl*My + ky in one component of B, and
+// the z stride: [kxl][ky][iz] (five-pass schedule, BTY = 0) or [kx][iz][ky]
+// (the fused xy passes, BTY = M_y: a compile-time stride keeps the z offsets
+// immediate).
+template <int BTY, typename T> __device__ __forceinline__ size_t zline_base(const XParams<T>& P, int p) {
+  if constexpr (BTY > 0) {
+    const int kxl = p / BTY;
+    return (size_t)kxl * P.nz * BTY + (p - kxl * BTY);
+  } else {
+    return (size_t)p * P.nz;
+  }
+}
+template <int BTY> constexpr int zline_stride() { return BTY > 0 ? BTY : 1; }
+
 // ------------------------------------------------------------- ZG: z * Green * z^-1
 // block: RZ lines x TT threads x 3 components, thread-fastest within a line;
 // lines are (kx, ky) pairs p = kxl*My + ky.  grid (nrb, ceil(nkx*My/RZ))
-template <typename T, int N>
+template <typename T, int N, int BTY = 0>
 __global__ void __launch_bounds__(3 * XShape<N>::TT * XShape<N>::RZ, sizeof(T) == 8 ? 1 : XShape<N>::ZG_MINB)
     kx_zg(XParams<T> P) {
   using C = cplx<T>;
@@ -290,10 +309,12 @@ __global__ void __launch_bounds__(3 * XShape<N>::TT * XShape<N>::RZ, sizeof(T) =
   const int nlines = P.nkx * P.My;
   const int p = blockIdx.y * RL + l;
   const bool live = p < nlines;
-  C* row = P.B + ((size_t)(rb * 3 + c) * P.nkx) * (size_t)P.My * P.nz + (size_t)p * P.nz;
+  constexpr int zs = zline_stride<BTY>();
+  C* row = P.B + ((size_t)(rb * 3 + c) * P.nkx) * (size_t)P.My * P.nz + zline_base<BTY>(P, live ? p : 0);
   C v[E];
 #pragma unroll
-  for (int i = 0; i < H; ++i) v[i] = live && t + TT * i < P.nz ? row[t + TT * i] : mk<C>(0, 0);  // iz < nz <= N/2
+  for (int i = 0; i < H; ++i)
+    v[i] = live && t + TT * i < P.nz ? row[(t + TT * i) * zs] : mk<C>(0, 0);  // iz < nz <= N/2
   line_fft<E, TT, +1, false, true, S_::PAIR>(v, my, t, P.twz);
 #pragma unroll
   for (int i = 0; i < E; ++i) my[t + TT * i] = v[i];
@@ -349,7 +370,7 @@ __global__ void __launch_bounds__(3 * XShape<N>::TT * XShape<N>::RZ, sizeof(T) =
   if (live) {
 #pragma unroll
     for (int i = 0; i < H; ++i)
-      if (t + TT * i < P.nz) row[t + TT * i] = v[i];  // keep iz < nz
+      if (t + TT * i < P.nz) row[(t + TT * i) * zs] = v[i];  // keep iz < nz
   }
 }
 
@@ -388,7 +409,7 @@ __device__ __forceinline__ void load_rec_s(const cplx<T>* sp, cplx<T> a[6]) {
   }
 }
 
-template <typename T, int N> __global__ void __launch_bounds__(128, 3) kx_zg3(XParams<T> P) {
+template <typename T, int N, int BTY = 0> __global__ void __launch_bounds__(128, 3) kx_zg3(XParams<T> P) {
   using C = cplx<T>;
   using R = T;
   using S_ = XShape<N>;
@@ -418,13 +439,14 @@ template <typename T, int N> __global__ void __launch_bounds__(128, 3) kx_zg3(XP
   const int p = p0 + l;
   const bool live = p < nlines;
   const size_t cs = (size_t)nlines * P.nz;  // component stride of B
-  C* row = P.B + (size_t)rb * 3 * cs + (size_t)(live ? p : 0) * P.nz;
+  constexpr int zs = zline_stride<BTY>();
+  C* row = P.B + (size_t)rb * 3 * cs + zline_base<BTY>(P, live ? p : 0);
   C v[3][E];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
 #pragma unroll
     for (int i = 0; i < H; ++i)
-      v[c][i] = live && t + TT * i < P.nz ? row[c * cs + t + TT * i] : mk<C>(0, 0);  // iz < nz <= N/2
+      v[c][i] = live && t + TT * i < P.nz ? row[c * cs + (t + TT * i) * zs] : mk<C>(0, 0);  // iz < nz <= N/2
   }
   // one twiddle set for the six transforms: forward, and conjugated for the inverse
   C w[E];
@@ -474,7 +496,7 @@ template <typename T, int N> __global__ void __launch_bounds__(128, 3) kx_zg3(XP
     for (int c = 0; c < 3; ++c) {
 #pragma unroll
       for (int i = 0; i < H; ++i)
-        if (t + TT * i < P.nz) row[c * cs + t + TT * i] = v[c][i];  // keep iz < nz
+        if (t + TT * i < P.nz) row[c * cs + (t + TT * i) * zs] = v[c][i];  // keep iz < nz
     }
   }
   if (!ok) mbar_wait(bar, 0, ZG3_WAIT_POLLS);  // no copy may land after the block exits
@@ -654,10 +676,225 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_xi(XParam
                 3 * (int)gridDim.y * (int)gridDim.x);
 }
 
-// ------------------------------------------------------------- host side
-enum class XPass { XF, YF, ZG, ZG3, YI, XI };
+// ------------------------------------------------------------- XYF / XYI: fused xy passes of a z plane
+// One cluster of four CTAs per (RHS, component, iz).  The plane of the
+// x-transformed rows, ny x M_x complex (256 KB at 128 x 256), is spread over
+// the four CTAs' shared memory by kx mod 4: CTA q holds the columns
+// kx = 4m + q as [iy][m] with the odd row stride M_x/4 + 1, so that column
+// reads are free of bank conflicts.  A row transform's thread t owns the
+// outputs kx = t + TX*i (line_fft), all in the plane of CTA t % 4.
+//   XYF: CTA q transforms rows iy in [q*rpc, (q+1)*rpc) along x and stores
+//        the outputs in the owning planes (distributed shared memory); after
+//        the cluster barrier each CTA transforms its M_x/4 columns along y
+//        and writes B[c][kx][iz][ky] (ky contiguous, coalesced from
+//        registers).
+//   XYI: each CTA reads its columns of B, transforms them back along y
+//        keeping iy < ny into its plane; after the cluster barrier CTA q
+//        reads rows iy in [q*rpc, (q+1)*rpc) from the four planes, transforms
+//        them back along x keeping ix < nx and finishes as the XI pass does.
+// Peer shared memory is touched only between cluster barriers that every
+// thread of the four CTAs reaches (the CTAs of a cluster share RHS,
+// component and iz, so a masked RHS returns in all four before the first).
+template <int NX, int NY> struct XYShape {
+  static constexpr int EX = RegShape<NX>::E, TX = RegShape<NX>::T, HX = EX / 2, RX = 256 / TX;
+  static constexpr int EY = RegShape<NY>::E, TY = RegShape<NY>::T, HY = EY / 2, CY = 256 / TY;
+  static constexpr int MQ = NX / 4;                    // plane columns per CTA
+  static constexpr int PR = NY / 2;                    // plane rows (ny <= NY/2)
+  static constexpr int PS = MQ + 1;                    // plane row stride (odd)
+  static constexpr int PLANE = (PR * PS + 1) / 2 * 2;  // elements; even, so the scratch after it is 16-byte aligned
+  static constexpr bool OK = TX % 4 == 0 && MQ % 2 == 0;
+};
 
-template <typename T, int N> static const void* xk(XPass p) {
+template <int NX, int NY> __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(256, 2) kxy_f(XParams<float> P) {
+  using C = float2;
+  using S = XYShape<NX, NY>;
+  constexpr int EX = S::EX, TX = S::TX, HX = S::HX, RX = S::RX;
+  constexpr int EY = S::EY, TY = S::TY, HY = S::HY, CY = S::CY, MQ = S::MQ, PS = S::PS;
+  static_assert(S::OK, "row outputs of one thread must share kx mod 4");
+  cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* plane = reinterpret_cast<C*>(smem_raw);  // [PR][PS]
+  C* lines = plane + S::PLANE;                // row / column FFT scratch
+  const int q = (int)cl.block_rank();
+  const int iz = blockIdx.y, rb = blockIdx.z / 3, c = blockIdx.z - 3 * (blockIdx.z / 3), rl = P.b_rhs0 + rb;
+  if (xoff(P, rl)) return;  // all four CTAs of the cluster
+  const int nx = P.nx, ny = P.ny;
+  const int rpc = (ny + 3) / 4, row0 = q * rpc, row1 = min(ny, row0 + rpc);
+  {
+    const int t = threadIdx.x % TX, l = threadIdx.x / TX;
+    C* dst = cl.map_shared_rank(plane, t & 3);  // kx = t + TX*i: kx % 4 = t % 4
+    C* ln = lines + (size_t)l * P.lsx;
+    const int S_ = P.io_full ? P.nat : P.nat0;
+    const C* x = P.x + (size_t)rl * P.x_rs + (size_t)c * S_;
+    cl.sync();  // every CTA of the cluster runs before a peer writes its plane
+    for (int r0 = row0; r0 < row1; r0 += RX) {
+      const int iy = r0 + l;
+      const bool live = iy < row1;
+      const int jrow = nx * (iy + ny * iz);
+      C v[EX];
+      if (P.io_full) {
+#pragma unroll
+        for (int i = 0; i < HX; ++i) v[i] = live && t + TX * i < nx ? x[jrow + t + TX * i] : mk<C>(0, 0);
+      } else {
+        int qi[HX];
+#pragma unroll
+        for (int i = 0; i < HX; ++i) qi[i] = live && t + TX * i < nx ? P.inv[jrow + t + TX * i] : -1;
+#pragma unroll
+        for (int i = 0; i < HX; ++i) v[i] = qi[i] >= 0 ? x[qi[i]] : mk<C>(0, 0);
+      }
+      if (P.conj) {
+#pragma unroll
+        for (int i = 0; i < HX; ++i) v[i].y = -v[i].y;
+      }
+      line_fft<EX, TX, +1, false, true, XShape<NX>::PAIR>(v, ln, t, P.twx);
+      if (live) {
+#pragma unroll
+        for (int i = 0; i < EX; ++i) dst[iy * PS + (t >> 2) + (TX / 4) * i] = v[i];
+      }
+    }
+  }
+  cl.sync();  // the four planes are complete (and the row scratch is free)
+  {
+    const int t = threadIdx.x % TY, l = threadIdx.x / TY;
+    C* ln = lines + (size_t)l * P.lsy;
+    const size_t cs = (size_t)NX * P.nz * NY;  // component stride of B
+    C* Bc = P.B + (size_t)(rb * 3 + c) * cs + (size_t)iz * NY;
+    for (int m0 = 0; m0 < MQ; m0 += CY) {
+      const int m = m0 + l;
+      const bool live = m < MQ;
+      C v[EY];
+#pragma unroll
+      for (int i = 0; i < HY; ++i) v[i] = live && t + TY * i < ny ? plane[(t + TY * i) * PS + m] : mk<C>(0, 0);
+      line_fft<EY, TY, +1, false, true, XShape<NY>::PAIR>(v, ln, t, P.twy);
+      if (live) {
+        C* b = Bc + (size_t)(4 * m + q) * P.nz * NY;
+#pragma unroll
+        for (int i = 0; i < EY; ++i) b[t + TY * i] = v[i];
+      }
+    }
+  }
+}
+
+template <int NX, int NY> __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(256, 2) kxy_i(XParams<float> P) {
+  using C = float2;
+  using S = XYShape<NX, NY>;
+  constexpr int EX = S::EX, TX = S::TX, HX = S::HX, RX = S::RX;
+  constexpr int EY = S::EY, TY = S::TY, HY = S::HY, CY = S::CY, MQ = S::MQ, PS = S::PS;
+  static_assert(S::OK, "row inputs of one thread must share kx mod 4");
+  cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* plane = reinterpret_cast<C*>(smem_raw);
+  C* lines = plane + S::PLANE;
+  const int q = (int)cl.block_rank();
+  const int iz = blockIdx.y, rb = blockIdx.z / 3, c = blockIdx.z - 3 * (blockIdx.z / 3), rl = P.b_rhs0 + rb;
+  if (xoff(P, rl)) return;  // all four CTAs of the cluster
+  const int nx = P.nx, ny = P.ny;
+  {
+    const int t = threadIdx.x % TY, l = threadIdx.x / TY;
+    C* ln = lines + (size_t)l * P.lsy;
+    const size_t cs = (size_t)NX * P.nz * NY;
+    const C* Bc = P.B + (size_t)(rb * 3 + c) * cs + (size_t)iz * NY;
+    for (int m0 = 0; m0 < MQ; m0 += CY) {
+      const int m = m0 + l;
+      const bool live = m < MQ;
+      const C* b = Bc + (size_t)(4 * (live ? m : 0) + q) * P.nz * NY;
+      C v[EY];
+#pragma unroll
+      for (int i = 0; i < EY; ++i) v[i] = live ? b[t + TY * i] : mk<C>(0, 0);
+      line_fft<EY, TY, -1, false, false, XShape<NY>::PAIR>(v, ln, t, P.twy);
+      if (live) {
+#pragma unroll
+        for (int i = 0; i < HY; ++i)
+          if (t + TY * i < ny) plane[(t + TY * i) * PS + m] = v[i];  // keep iy < ny
+      }
+    }
+  }
+  cl.sync();  // the four planes are complete (and the column scratch is free)
+  double2 dacc = make_double2(0.0, 0.0);  // x*y of this thread's sites (dot_out)
+  {
+    const int t = threadIdx.x % TX, l = threadIdx.x / TX;
+    const C* src = cl.map_shared_rank(plane, t & 3);
+    C* ln = lines + (size_t)l * P.lsx;
+    const int rpc = (ny + 3) / 4, row0 = q * rpc, row1 = min(ny, row0 + rpc);
+    const int S_ = P.io_full ? P.nat : P.nat0;
+    const int SA = P.a_full ? P.nat : P.nat0;
+    const C* x = P.x + (size_t)rl * P.x_rs;
+    const C* ad = P.adia + (size_t)rl * P.a_rs + (size_t)c * SA;
+    C* y = P.y + (size_t)rl * P.y_rs + (size_t)c * S_;
+    const C* ao = P.aoff ? P.aoff + (size_t)rl * P.a_rs : nullptr;
+    for (int r0 = row0; r0 < row1; r0 += RX) {
+      const int iy = r0 + l;
+      const bool live = iy < row1;
+      const int jrow = nx * (iy + ny * iz);
+      int qi[HX];  // x / y index of each kept element, -1 for vacuum
+#pragma unroll
+      for (int i = 0; i < HX; ++i) {
+        const int j = jrow + t + TX * i;
+        qi[i] = live && t + TX * i < nx ? (P.io_full ? (P.iocc[j] != 0 ? j : -1) : P.inv[j]) : -1;
+      }
+      C v[EX];
+#pragma unroll
+      for (int i = 0; i < EX; ++i) v[i] = live ? src[iy * PS + (t >> 2) + (TX / 4) * i] : mk<C>(0, 0);
+      line_fft<EX, TX, -1, false, false, XShape<NX>::PAIR>(v, ln, t, P.twx);
+      // finish (cu:116-118): y = CXADIA x - w/ngrid [+ CXAOFF terms], conj for 'C'
+#pragma unroll
+      for (int i = 0; i < HX; ++i) {
+        if (!live || t + TX * i >= nx) continue;
+        const int j = jrow + t + TX * i;
+        const int qx = qi[i];
+        if (qx < 0) {
+          if (P.io_full) y[j] = mk<C>(0, 0);
+          continue;
+        }
+        const int qa = P.a_full == P.io_full ? qx : (P.a_full ? j : P.inv[j]);
+        C xc = x[(size_t)c * S_ + qx];
+        if (P.conj) xc.y = -xc.y;
+        C yv = csub(cmul(ad[qa], xc), cscale(v[i], P.inv_ngrid));
+        if (ao) {
+          C x1 = x[qx], x2 = x[S_ + qx], x3 = x[2 * (size_t)S_ + qx];
+          if (P.conj) { x1.y = -x1.y; x2.y = -x2.y; x3.y = -x3.y; }
+          const C a23 = ao[qa], a31 = ao[SA + qa], a12 = ao[2 * (size_t)SA + qa];
+          if (c == 0) yv = cadd(yv, cadd(cmul(a31, x3), cmul(a12, x2)));
+          else if (c == 1) yv = cadd(yv, cadd(cmul(a12, x1), cmul(a23, x3)));
+          else yv = cadd(yv, cadd(cmul(a23, x2), cmul(a31, x1)));
+        }
+        if (P.conj) yv.y = -yv.y;
+        y[qx] = yv;
+        if (P.dot_out) {  // conj = 0 here: xc is x
+          const double2 xd = to_d(xc), yd = to_d(yv);
+          dacc.x += xd.x * yd.x - xd.y * yd.y;
+          dacc.y += xd.x * yd.y + xd.y * yd.x;
+        }
+      }
+    }
+  }
+  cl.sync();  // no CTA leaves while a peer still reads its plane
+  if (P.dot_out) xdot_reduce(P, dacc, P.rhs0 + rl, (c * P.nz + iz) * 4 + q, 12 * P.nz);
+}
+
+// ------------------------------------------------------------- host side
+// ZGT / ZG3T: the z passes on the B layout of the fused xy passes
+enum class XPass { XF, YF, ZG, ZG3, YI, XI, ZGT, ZG3T };
+
+// z passes on the B layout of the fused xy passes (z stride M_y = BTY)
+template <typename T, int N, int BTY> static const void* xkt(XPass p) {
+  if constexpr (sizeof(T) == 4) {
+    if (p == XPass::ZGT) return (const void*)kx_zg<T, N, BTY>;
+    if constexpr (Z3Shape<N>::OK)
+      if (p == XPass::ZG3T) return (const void*)kx_zg3<T, N, BTY>;
+  }
+  return nullptr;
+}
+
+template <typename T, int N> static const void* xk(XPass p, int my = 0) {
+  if (p == XPass::ZGT || p == XPass::ZG3T) {
+    switch (my) {
+      case 64: return xkt<T, N, 64>(p);
+      case 128: return xkt<T, N, 128>(p);
+      case 256: return xkt<T, N, 256>(p);
+      default: return nullptr;
+    }
+  }
   switch (p) {
     case XPass::XF: return (const void*)kx_xf<T, N>;
     case XPass::YF: return (const void*)kx_yf<T, N>;
@@ -665,29 +902,46 @@ template <typename T, int N> static const void* xk(XPass p) {
     case XPass::ZG3:
       if constexpr (Z3Shape<N>::OK && sizeof(T) == 4) return (const void*)kx_zg3<T, N>;
       return nullptr;
+
     case XPass::YI: return (const void*)kx_yi<T, N>;
     default: return (const void*)kx_xi<T, N>;
   }
 }
 
-template <typename T> static const void* xkernel(XPass p, int n) {
+// my: M_y, for the z passes on the fused layout (ZGT, ZG3T)
+template <typename T> static const void* xkernel(XPass p, int n, int my = 0) {
   switch (n) {
-    case 16: return xk<T, 16>(p);
-    case 32: return xk<T, 32>(p);
-    case 48: return xk<T, 48>(p);
-    case 64: return xk<T, 64>(p);
-    case 96: return xk<T, 96>(p);
-    case 128: return xk<T, 128>(p);
-    case 192: return xk<T, 192>(p);
-    case 256: return xk<T, 256>(p);
+    case 16: return xk<T, 16>(p, my);
+    case 32: return xk<T, 32>(p, my);
+    case 48: return xk<T, 48>(p, my);
+    case 64: return xk<T, 64>(p, my);
+    case 96: return xk<T, 96>(p, my);
+    case 128: return xk<T, 128>(p, my);
+    case 192: return xk<T, 192>(p, my);
+    case 256: return xk<T, 256>(p, my);
     case 512:
-      if constexpr (sizeof(T) == 4) return xk<T, 512>(p);  // FP64: shared memory of the 512 passes too large
+      if constexpr (sizeof(T) == 4) return xk<T, 512>(p, my);  // FP64: shared memory of the 512 passes too large
       return nullptr;
     default: return nullptr;
   }
 }
 
 static int rT(int n) { return reg_threads(n); }
+
+// fused xy kernels for (M_x, M_y); nullptr where none is built
+static const void* xykernel(bool fwd, int nxl, int nyl) {
+#define DDB_XY(a, b) \
+  if (nxl == a && nyl == b) return fwd ? (const void*)kxy_f<a, b> : (const void*)kxy_i<a, b>;
+  DDB_XY(64, 64) DDB_XY(128, 128) DDB_XY(256, 256) DDB_XY(128, 256) DDB_XY(256, 128)
+#undef DDB_XY
+  return nullptr;
+}
+// shared memory of kxy_f / kxy_i: plane (XYShape::PLANE) + row or column FFT scratch
+static size_t xy_smem(int nxl, int nyl, int lsx, int lsy) {
+  const int TX = reg_threads(nxl), TY = reg_threads(nyl);
+  const int PS = nxl / 4 + 1, PLANE = ((nyl / 2) * PS + 1) / 2 * 2;
+  return ((size_t)PLANE + std::max((size_t)(256 / TX) * lsx, (size_t)(256 / TY) * lsy)) * sizeof(float2);
+}
 
 template <typename T> static int xlaunch(const void* f, dim3 g, int th, size_t sm, cudaStream_t st, XParams<T>& P) {
   raise_smem_limit(f);
@@ -753,6 +1007,44 @@ int matvec_xpipe(Engine<T>& E, const MvArgs<T>& a) {
   const void* fzg = xkernel<T>(XPass::ZG, g.Mz);
   const void* fyi = xkernel<T>(XPass::YI, g.My);
   const void* fxi = xkernel<T>(XPass::XI, g.Mx);
+  // DDSCAT_B200_FUSEXY=1, FP32 with all kx planes of a slab batch resident
+  // (FFT3D): the x and y passes fused per z plane (kxy_f / kxy_i), three
+  // launches per slab batch.  Opt-in: at 128^3 it moves 41 % fewer DRAM bytes
+  // in the xy passes but runs slower than the five-pass schedule (16 warps per
+  // SM at 101 KB of shared memory per CTA, and half-used sectors in the z
+  // pass on the ky-contiguous layout).
+  const void* fxyf = nullptr;
+  const void* fxyi = nullptr;
+  if constexpr (sizeof(T) == 4) {
+    if (E.slab_B == g.Mx && std::getenv("DDSCAT_B200_FUSEXY")) {
+      fxyf = xykernel(true, g.Mx, g.My);
+      fxyi = xykernel(false, g.Mx, g.My);
+    }
+  }
+  const void* fzt = fxyf ? xkernel<T>(fzg3 ? XPass::ZG3T : XPass::ZGT, g.Mz, g.My) : nullptr;
+  if (fxyf && fxyi && fzt) {
+    const size_t smxy = xy_smem(g.Mx, g.My, P.lsx, P.lsy);
+    P.kx0 = 0;
+    P.nkx = g.Mx;
+    P.b_rhs0 = 0;
+    for (int r0 = 0; r0 < a.nrhs; r0 += E.slab_nr) {
+      const int nr = std::min(E.slab_nr, a.nrhs - r0);
+      P.rhs0 = r0;
+      P.x = a.x + (size_t)r0 * a.x_rs;
+      P.y = a.y + (size_t)r0 * a.y_rs;
+      P.adia = a.adia + (size_t)r0 * a.a_rs;
+      P.aoff = a.aoff ? a.aoff + (size_t)r0 * a.a_rs : nullptr;
+      const dim3 gxy(4u, (unsigned)g.nz, (unsigned)(3 * nr));
+      if (xlaunch<T>(fxyf, gxy, 256, smxy, E.stream, P)) return 21;
+      if (fzg3 ? xlaunch<T>(fzt, dim3((unsigned)nr, (unsigned)ceil_div((size_t)g.Mx * g.My, RZ3)), 128, smz,
+                            E.stream, P)
+               : xlaunch<T>(fzt, dim3((unsigned)nr, (unsigned)ceil_div((size_t)g.Mx * g.My, RZ)), 3 * TZ * RZ, smz,
+                            E.stream, P))
+        return 23;
+      if (xlaunch<T>(fxyi, gxy, 256, smxy, E.stream, P)) return 25;
+    }
+    return 0;
+  }
   for (int r0 = 0; r0 < a.nrhs; r0 += E.zcap) {
     const int nr = std::min(E.zcap, a.nrhs - r0);
     P.rhs0 = r0;
@@ -787,7 +1079,11 @@ int matvec_xpipe(Engine<T>& E, const MvArgs<T>& a) {
   return 0;
 }
 
-size_t xdot_blocks(const Geometry& g) { return (size_t)3 * g.nz * ceil_div(g.ny, 256 / reg_threads(g.Mx)); }
+// partial sums per RHS of the fused x*y sum: XI blocks, or the 4 CTAs per
+// (component, iz) of the fused XYI pass
+size_t xdot_blocks(const Geometry& g) {
+  return std::max((size_t)3 * g.nz * ceil_div(g.ny, 256 / reg_threads(g.Mx)), (size_t)12 * g.nz);
+}
 
 // planar [6][Z][Y][X] (build / CXZC layout) -> [X][Y][Z][6]
 template <typename C> __global__ void k_interleave6_zfast(const C* src, C* dst, int X, int Y, int Z) {

@@ -192,3 +192,26 @@ def test_batch_qmrccg_nonzero_initial_guess():
     ms, rhs, calls = dda.last_solve_stats()
     assert rhs == int(second.ncompte.sum())
     dda.release()
+
+
+@pytest.mark.gpu
+def test_batch_qmrccg_graph_fused_xy_passes(monkeypatch):
+    """The graph-driven QMRCCG on the fused xy passes (DDSCAT_B200_FUSEXY=1,
+    32^3: M_x = M_y = 64), whose inverse pass also forms the fused vt^T A vt
+    sum over its four-CTA clusters: same iteration counts within one and
+    solutions within 20*TOL of the five-pass schedule, FP64 residual <= 1.2*TOL."""
+    n = 32
+    prob = targets.make_problem(n, m=1.33 + 0.05j, x=5.0, orientations=targets.random_orientations(2, seed=5))
+    dda = D.DDA()
+    dda.prepare_green(n, n, n, prob.iocc, prob.incid[0].k)
+    b, adia = _batch_inputs(prob)
+    x5, xf = np.zeros_like(b), np.zeros_like(b)
+    r5 = dda.solve_batch("qmrccg", b, x5, adia, maxit=2000, tol=TOL, replace=True, symmetric=True, graph=True)
+    monkeypatch.setenv("DDSCAT_B200_FUSEXY", "1")
+    rf = dda.solve_batch("qmrccg", b, xf, adia, maxit=2000, tol=TOL, replace=True, symmetric=True, graph=True)
+    assert np.all(rf.status == 0) and np.all(rf.tole <= TOL)
+    assert np.all(np.abs(rf.itno - r5.itno) <= 1), (rf.itno, r5.itno)
+    assert np.all(dda.residual_f64(b, xf, adia) <= 1.2 * TOL)
+    for r in range(b.shape[0]):
+        assert np.linalg.norm(xf[r] - x5[r]) / np.linalg.norm(x5[r]) < 20 * TOL
+    dda.release()

@@ -44,7 +44,10 @@ def _err(y, yr):
                                           ((24, 24, 24), 0), ((48, 24, 96), 1), ((96, 32, 24), 0), ((48, 48, 48), 0),
                                           # even n whose 2n is no register-FFT length: padded FFT lengths
                                           # (40, 52, 28 -> 48, 64, 32; 100, 20, 60 -> 128, 32, 64)
-                                          ((20, 26, 14), 1), ((50, 10, 30), 0)])
+                                          ((20, 26, 14), 1), ((50, 10, 30), 0),
+                                          # (M_x, M_y) = (256, 256), (128, 256), (256, 128), full and padded rows
+                                          ((128, 128, 8), 0), ((100, 120, 6), 1), ((64, 128, 10), 0),
+                                          ((128, 60, 8), 0)])
 def test_apply_matches_oracle(layout, dims, idipint):
     iocc, ak, x, adia, aoff, gp = _case(dims, idipint)
     dda = D.DDA(layout)
@@ -134,4 +137,23 @@ def test_padded_fft_lengths_equal_2n(dims, monkeypatch):
     dda.prepare_green(*dims, iocc, ak)
     y_2n = dda.apply(x, adia, aoff)
     assert _err(y_pad, y_2n)[0] <= 1e-5
+    dda.release()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dims", [(32, 32, 12), (64, 64, 20), (120, 128, 16)])
+def test_fused_xy_passes_equal_five_pass(dims, monkeypatch):
+    """With DDSCAT_B200_FUSEXY=1, FP32 grids with (M_x, M_y) in the fused set
+    run the x and y passes of a z plane in one four-CTA cluster (distributed
+    shared memory, B laid out ky-contiguous): the same transforms in the same
+    order as the five-pass schedule, so both give the same y to rounding, for
+    'N' and 'C' and with CXAOFF."""
+    iocc, ak, x, adia, aoff, gp = _case(dims, 0, seed=9)
+    dda = D.DDA()
+    dda.prepare_green(*dims, iocc, ak)
+    y_5 = [dda.apply(x, adia, aoff, cw) for cw in "NC"]
+    monkeypatch.setenv("DDSCAT_B200_FUSEXY", "1")
+    y_f = [dda.apply(x, adia, aoff, cw) for cw in "NC"]
+    for a, b in zip(y_f, y_5):
+        assert _err(a, b)[0] <= 1e-6
     dda.release()
