@@ -1159,6 +1159,475 @@ template <typename T> int solve_batch_qmrccg(BatchIO<T>& io, BatchResult& res) {
 }
 
 // --------------------------------------------------------------------------
+// Device-driven PBCGS2 iteration (residual replacement), captured in a CUDA
+// graph: the host-driven recurrence of solve_batch_pbcgs2 below, with its
+// per-RHS FP64 scalars (rho, alpha, beta, omega, the 3 x 3 minimal-residual
+// system of the BiCGStab(2) step, the reliable-update tests) in single-thread
+// kernels on state held on the GPU.  Two IF conditional nodes hold the
+// reliable-residual check (every 20 iterations and at convergence) and the
+// reliable update of the solution (cu:474), armed on the device only when some
+// RHS needs them.  The host launches the graph repeatedly and reads the active
+// count every few launches.
+struct PGState {
+  double2 *alpha, *omega, *sigma, *rho0, *rho1, *beta;
+  double2* co;           // [7][R]: -beta, alpha, -alpha, y1, y2, -y1, -y2
+  double2 *one, *mone;   // [R]
+  double *rnrm0, *rnrm, *mxx, *mxr, *resid;
+  int *it, *live, *status, *nc, *I, *CK, *RP, *RC, *XD, *RCMP, *XPDT;
+  int *active, *checks, *updates;  // [1] each
+};
+
+__device__ __forceinline__ double2 dconj(double2 a) { return make_double2(a.x, -a.y); }
+__device__ __forceinline__ double2 dadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double dabs(double2 a) { return hypot(a.x, a.y); }
+
+// start of an iteration: I = live, resid > tol, it < maxit; rho0 = -(omega rho0)
+__global__ void k_pg_begin(int R, int maxit, double tol, PGState S) {
+  for (int r = threadIdx.x; r < R; r += blockDim.x) {
+    const int on = S.live[r] && S.resid[r] > tol && S.it[r] < maxit;
+    S.I[r] = on;
+    if (!on) continue;
+    S.it[r] += 1;
+    S.rho0[r] = dsc(-1.0, dmul(S.omega[r], S.rho0[r]));
+  }
+}
+
+// rho1 = rr^H r_{k-1} (out slot 0), beta and the coefficient -beta of the u update
+__global__ void k_pg_rho(int R, PGState S, const double2* out) {
+  for (int r = threadIdx.x; r < R; r += blockDim.x) {
+    if (!S.I[r]) continue;
+    const double2 rho1 = out[(size_t)r * 8];
+    S.rho1[r] = rho1;
+    if (dz0(S.rho0[r])) { S.status[r] = 95; S.live[r] = 0; S.I[r] = 0; continue; }
+    const double2 beta = dmul(S.alpha[r], ddiv(rho1, S.rho0[r]));
+    S.beta[r] = beta;
+    S.rho0[r] = rho1;
+    S.co[r] = dsc(-1.0, beta);
+    S.nc[r] += 1;  // the MATVEC u_{k-1} -> u_k that follows
+  }
+}
+
+// sigma = rr^H u_k (out slot 0), alpha and the coefficients alpha, -alpha
+__global__ void k_pg_sigma(int R, PGState S, const double2* out) {
+  for (int r = threadIdx.x; r < R; r += blockDim.x) {
+    if (!S.I[r]) continue;
+    const double2 sg = out[(size_t)r * 8];
+    S.sigma[r] = sg;
+    if (dz0(sg)) { S.status[r] = 98; S.live[r] = 0; S.I[r] = 0; continue; }
+    const double2 al = ddiv(S.rho1[r], sg);
+    S.alpha[r] = al;
+    S.co[R + r] = al;
+    S.co[2 * R + r] = dsc(-1.0, al);
+    S.nc[r] += 1;  // the MATVEC r_{k-1} -> r_k that follows
+  }
+}
+
+// |r_0| (out slot 0) and its running maxima
+__global__ void k_pg_rnrm(int R, PGState S, const double2* out) {
+  for (int r = threadIdx.x; r < R; r += blockDim.x) {
+    if (!S.I[r]) continue;
+    const double v = sqrt(fmax(0.0, out[(size_t)r * 8].x));
+    S.rnrm[r] = v;
+    S.mxx[r] = fmax(S.mxx[r], v);
+    S.mxr[r] = fmax(S.mxr[r], v);
+  }
+}
+
+// the BiCGStab(2) minimal-residual step from the Gram matrix of r_0, r_1, r_2
+// (out slots 0..5: (0,0), (1,0), (1,1), (2,0), (2,1), (2,2), conjugated first
+// argument), as in the host form (cu:1168-1278 via solvers.cu)
+__global__ void k_pg_gram(int R, PGState S, const double2* out) {
+  for (int r = threadIdx.x; r < R; r += blockDim.x) {
+    if (!S.I[r]) continue;
+    const double2* o = out + (size_t)r * 8;
+    double2 Zm[3][3];
+    Zm[0][0] = o[0]; Zm[1][0] = o[1]; Zm[1][1] = o[2];
+    Zm[2][0] = o[3]; Zm[2][1] = o[4]; Zm[2][2] = o[5];
+    Zm[0][1] = dconj(Zm[1][0]); Zm[0][2] = dconj(Zm[2][0]); Zm[1][2] = dconj(Zm[2][1]);
+    auto matv = [&](const double2* v, double2* w) {
+      for (int a = 0; a < 3; ++a) {
+        w[a] = make_double2(0.0, 0.0);
+        for (int b = 0; b < 3; ++b) w[a] = dadd(w[a], dmul(Zm[a][b], v[b]));
+      }
+    };
+    auto inner = [](const double2* a, const double2* b) {
+      double2 s = make_double2(0.0, 0.0);
+      for (int k = 0; k < 3; ++k) s = dadd(s, dmul(dconj(a[k]), b[k]));
+      return s;
+    };
+    bool fail = dz0(Zm[1][1]);
+    double2 y0[3], yl[3], zy0[3], zyl[3];
+    double k0 = 0.0, kl = 0.0;
+    if (!fail) {
+      y0[0] = make_double2(-1.0, 0.0); y0[1] = ddiv(Zm[1][0], Zm[1][1]); y0[2] = make_double2(0.0, 0.0);
+      yl[0] = make_double2(0.0, 0.0); yl[1] = ddiv(Zm[1][2], Zm[1][1]); yl[2] = make_double2(-1.0, 0.0);
+      matv(y0, zy0);
+      matv(yl, zyl);
+      k0 = sqrt(dabs(inner(y0, zy0)));
+      kl = sqrt(dabs(inner(yl, zyl)));
+      fail = k0 == 0.0 || kl == 0.0;
+    }
+    double2 vr = make_double2(0.0, 0.0);
+    double avr = 0.0;
+    if (!fail) {
+      const double2 q = inner(yl, zy0);
+      const double den = k0 * kl;
+      vr = make_double2(q.x / den, q.y / den);
+      avr = dabs(vr);
+      fail = avr == 0.0;
+    }
+    if (fail) { S.status[r] = 102; S.live[r] = 0; S.I[r] = 0; continue; }
+    const double s1 = fmax(avr, 0.7) / avr, s2 = k0 / kl;
+    const double2 fac = dsc(s2, dsc(s1, vr));
+    for (int a = 0; a < 3; ++a) {
+      const double2 f = dmul(fac, yl[a]);
+      y0[a] = make_double2(y0[a].x - f.x, y0[a].y - f.y);
+    }
+    S.omega[r] = y0[2];
+    matv(y0, zy0);
+    const double rn = sqrt(dabs(inner(y0, zy0)));
+    S.rnrm[r] = rn;
+    S.mxx[r] = fmax(S.mxx[r], rn);
+    S.mxr[r] = fmax(S.mxr[r], rn);
+    S.co[3 * R + r] = y0[1];
+    S.co[4 * R + r] = y0[2];
+    S.co[5 * R + r] = dsc(-1.0, y0[1]);
+    S.co[6 * R + r] = dsc(-1.0, y0[2]);
+    const double r0n = S.rnrm0[r];
+    const int xpdt = rn < 1.0e-2 * r0n && r0n < S.mxx[r];
+    S.XPDT[r] = xpdt;
+    S.RCMP[r] = (rn < 1.0e-2 * S.mxr[r] && r0n < S.mxr[r]) || xpdt;
+    S.resid[r] = r0n > 0.0 ? rn / r0n : 0.0;
+  }
+}
+
+// reliable-residual check mask (every 20 iterations and at convergence) and its IF condition
+__global__ void k_pg_post(int R, double tol, PGState S, cudaGraphConditionalHandle h) {
+  if (threadIdx.x != 0) return;
+  int any = 0;
+  for (int r = 0; r < R; ++r) {
+    const int ck = S.I[r] && ((S.it[r] % 20) == 0 || S.resid[r] <= tol);
+    S.CK[r] = ck;
+    S.RP[r] = 0;
+    if (ck) S.nc[r] += 1;
+    any |= ck;
+  }
+  if (any) *S.checks += 1;
+  cudaGraphSetConditional(h, any ? 1u : 0u);
+}
+
+// decisions of the check from |b' - A x|^2, |b' - A x - r_0|^2 (b' the shifted RHS)
+__global__ void k_pg_check(int R, double tol, PGState S, const double2* out) {
+  for (int r = threadIdx.x; r < R; r += blockDim.x) {
+    if (!S.CK[r]) continue;
+    const double tr = sqrt(fmax(0.0, out[(size_t)r * 8].x)), gapn = sqrt(fmax(0.0, out[(size_t)r * 8 + 1].x));
+    const double tres = tr / S.rnrm0[r];
+    const double gap = tr > 0.0 ? gapn / tr : (gapn == 0.0 ? 0.0 : INFINITY);
+    const bool conv = tres <= tol;
+    const bool rest = gap >= 1.0e-3 || (S.resid[r] <= tol && !conv);
+    if (conv) { S.resid[r] = tres; S.live[r] = 0; S.I[r] = 0; continue; }
+    if (rest) {
+      S.RP[r] = 1;
+      S.resid[r] = tres;
+      S.rnrm[r] = tres * S.rnrm0[r];
+      S.mxr[r] = fmax(S.mxr[r], S.rnrm[r]);
+    }
+  }
+}
+
+// reliable-update masks (RC: recompute r_0; XD: also shift the solution) and their IF condition
+__global__ void k_pg_rc(int R, PGState S, cudaGraphConditionalHandle h) {
+  if (threadIdx.x != 0) return;
+  int any = 0;
+  for (int r = 0; r < R; ++r) {
+    const int rc = S.I[r] && S.RCMP[r];
+    S.RC[r] = rc;
+    S.XD[r] = rc && S.XPDT[r];
+    if (rc) S.nc[r] += 1;
+    any |= rc;
+  }
+  if (any) *S.updates += 1;
+  cudaGraphSetConditional(h, any ? 1u : 0u);
+}
+
+__global__ void k_pg_rcpost(int R, PGState S) {
+  for (int r = threadIdx.x; r < R; r += blockDim.x) {
+    if (!S.RC[r]) continue;
+    S.mxr[r] = S.rnrm[r];
+    if (S.XD[r]) S.mxx[r] = S.rnrm[r];
+  }
+}
+
+// RHS that will run another iteration
+__global__ void k_pg_count(int R, int maxit, double tol, PGState S) {
+  if (threadIdx.x != 0) return;
+  int c = 0;
+  for (int r = 0; r < R; ++r) c += S.live[r] && S.resid[r] > tol && S.it[r] < maxit;
+  *S.active = c;
+}
+
+// host copy of the PBCGS2 state handed between the host-driven and the graph-driven iterations
+struct PGHost {
+  std::vector<Z> alpha, omega, sigma, rho0, rho1, beta;
+  std::vector<double> rnrm0, rnrm, mxx, mxr, resid;
+  std::vector<int> it, live, status;
+};
+
+// Runs the PBCGS2 iterations (residual replacement) from the host state hs
+// until no RHS is active; w: rr, r0, r1, r2, u0, u1, u2, XP, BP, X, sy.
+template <typename T>
+static int pbcgs2_graph_loop(BatchIO<T>& io, BatchOps<T>& ops, std::vector<int>& nc, cplx<T>* const* w, PGHost& hs,
+                             double mv_ms_per_rhs) {
+  using C = cplx<T>;
+  const int R = io.R, n = io.n;
+  C *rr = w[0], *r[3] = {w[1], w[2], w[3]}, *u[3] = {w[4], w[5], w[6]}, *XP = w[7], *BP = w[8], *X = w[9], *sy = w[10];
+  const size_t nz2 = (size_t)(6 + 7 + 2) * R, nd = (size_t)5 * R, ni = (size_t)11 * R + 3;
+  unsigned char* blk = nullptr;
+  cudaError_t e = cudaMalloc((void**)&blk, nz2 * sizeof(double2) + nd * sizeof(double) + ni * sizeof(int));
+  if (e != cudaSuccess) { set_cuda_error("graph solve state", e); return 1; }
+  PGState S;
+  double2* z = reinterpret_cast<double2*>(blk);
+  double2** zp[6] = {&S.alpha, &S.omega, &S.sigma, &S.rho0, &S.rho1, &S.beta};
+  for (int k = 0; k < 6; ++k) *zp[k] = z + (size_t)k * R;
+  S.co = z + (size_t)6 * R;
+  S.one = z + (size_t)13 * R;
+  S.mone = z + (size_t)14 * R;
+  double* dd = reinterpret_cast<double*>(z + nz2);
+  double** dp[5] = {&S.rnrm0, &S.rnrm, &S.mxx, &S.mxr, &S.resid};
+  for (int k = 0; k < 5; ++k) *dp[k] = dd + (size_t)k * R;
+  int* ii = reinterpret_cast<int*>(dd + nd);
+  int** ip[11] = {&S.it, &S.live, &S.status, &S.nc, &S.I, &S.CK, &S.RP, &S.RC, &S.XD, &S.RCMP, &S.XPDT};
+  for (int k = 0; k < 11; ++k) *ip[k] = ii + (size_t)k * R;
+  S.active = ii + (size_t)11 * R;
+  S.checks = S.active + 1;
+  S.updates = S.active + 2;
+  std::vector<double2> hz(nz2, make_double2(0, 0));
+  const std::vector<Z>* zs[6] = {&hs.alpha, &hs.omega, &hs.sigma, &hs.rho0, &hs.rho1, &hs.beta};
+  for (int k = 0; k < 6; ++k)
+    for (int i = 0; i < R; ++i) hz[(size_t)k * R + i] = dz((*zs[k])[i]);
+  for (int i = 0; i < R; ++i) { hz[(size_t)13 * R + i] = make_double2(1, 0); hz[(size_t)14 * R + i] = make_double2(-1, 0); }
+  std::vector<double> hd0(nd);
+  const std::vector<double>* ds[5] = {&hs.rnrm0, &hs.rnrm, &hs.mxx, &hs.mxr, &hs.resid};
+  for (int k = 0; k < 5; ++k)
+    for (int i = 0; i < R; ++i) hd0[(size_t)k * R + i] = (*ds[k])[i];
+  std::vector<int> hi0(ni, 0);
+  for (int i = 0; i < R; ++i) {
+    hi0[i] = hs.it[i]; hi0[R + i] = hs.live[i]; hi0[2 * R + i] = hs.status[i]; hi0[3 * R + i] = nc[i];
+  }
+  cudaStream_t st = nullptr, st2 = nullptr;
+  cudaStreamSynchronize(ops.stream);
+  e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking);
+  // uploads ordered on st (see qmr_graph_loop)
+  if (e == cudaSuccess) e = cudaMemcpyAsync(z, hz.data(), nz2 * sizeof(double2), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dd, hd0.data(), nd * sizeof(double), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ii, hi0.data(), ni * sizeof(int), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    if (st) cudaStreamDestroy(st);
+    if (st2) cudaStreamDestroy(st2);
+    cudaFree(blk);
+    set_cuda_error("graph solve streams and state", e);
+    return 1;
+  }
+  Engine<T>& eng = *io.eng;
+  const cudaStream_t eng_st = eng.stream;
+  MvArgs<T> mv;
+  mv.x_rs = n; mv.y_rs = n; mv.io_full = 0;
+  mv.adia = io.adia; mv.aoff = io.aoff; mv.a_rs = n; mv.a_full = 0; mv.conj = 0; mv.nrhs = R;
+  const double tol = io.tol;
+  const int maxit = io.maxit;
+  const unsigned gb = (unsigned)std::max<size_t>(1, std::min<size_t>(ceil_div(n, BT), std::max(1, 2368 / R)));
+  auto lin = [&](cudaStream_t s_, C* d, const double2* cd, const C* a, const double2* ca, const C* b,
+                 const double2* cb, const int* m) {
+    kb_lin<C><<<dim3(gb, R), BT, 0, s_>>>(n, d, cd, a, ca, b, cb, m);
+    note_launch();
+  };
+  auto dots = [&](cudaStream_t s_, int K, const C* const* a, const C* const* b, const int* m) {
+    BDot<T> sp{};
+    sp.K = K; sp.mode = 0;
+    for (int k = 0; k < K; ++k) { sp.a[k] = a[k]; sp.b[k] = b[k]; sp.conj[k] = 1; }
+    kb_dots<T><<<dim3(ops.nb, R), BT, 0, s_>>>(n, sp, m, ops.d_part, ops.d_out, ops.d_cnt);
+    note_launch();
+  };
+  auto matvec = [&](const C* in, C* out, const int* m) {
+    mv.x = in; mv.y = out; mv.mask = m;
+    return eng.matvec(mv);
+  };
+  // an IF node at the capture point of st whose body is captured on st2 by body()
+  auto if_node = [&](cudaGraphConditionalHandle h, auto body) -> cudaError_t {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    cudaError_t e_ = cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &ndeps);
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cnode = nullptr;
+    if (e_ == cudaSuccess) e_ = cudaGraphAddNode(&cnode, g, deps, ndeps, &cp);
+    if (e_ == cudaSuccess) e_ = cudaStreamUpdateCaptureDependencies(st, &cnode, 1, cudaStreamSetCaptureDependencies);
+    if (e_ != cudaSuccess) return e_;
+    e_ = cudaStreamBeginCaptureToGraph(st2, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                       cudaStreamCaptureModeThreadLocal);
+    if (e_ != cudaSuccess) return e_;
+    eng.stream = st2;
+    body();
+    eng.stream = st;
+    cudaGraph_t body_out = nullptr;
+    return cudaStreamEndCapture(st2, &body_out);
+  };
+  int rc = 0;
+  eng.stream = st;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  unsigned long long kernels_a = 0, kernels_b = 0, kernels_c = 0;
+  {
+    e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    cudaGraphConditionalHandle hck = 0, hrc = 0;
+    if (e == cudaSuccess) e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &ndeps);
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&hck, g, 0, cudaGraphCondAssignDefault);
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&hrc, g, 0, cudaGraphCondAssignDefault);
+    unsigned long long c0 = launch_total();
+    if (e == cudaSuccess) {
+      k_pg_begin<<<1, 256, 0, st>>>(R, maxit, tol, S);
+      note_launch();
+      for (int k = 1; k <= 2 && !rc; ++k) {
+        {
+          const C* A1[1] = {rr};
+          const C* B1[1] = {r[k - 1]};
+          dots(st, 1, A1, B1, S.I);
+        }
+        k_pg_rho<<<1, 256, 0, st>>>(R, S, ops.d_out);
+        note_launch();
+        for (int j = 0; j < k; ++j) lin(st, u[j], S.co, r[j], S.one, nullptr, nullptr, S.I);
+        if ((rc = matvec(u[k - 1], u[k], S.I))) break;
+        {
+          const C* A1[1] = {rr};
+          const C* B1[1] = {u[k]};
+          dots(st, 1, A1, B1, S.I);
+        }
+        k_pg_sigma<<<1, 256, 0, st>>>(R, S, ops.d_out);
+        note_launch();
+        lin(st, X, S.one, u[0], S.co + R, nullptr, nullptr, S.I);
+        for (int j = 0; j < k; ++j) lin(st, r[j], S.one, u[j + 1], S.co + 2 * R, nullptr, nullptr, S.I);
+        if ((rc = matvec(r[k - 1], r[k], S.I))) break;
+        {
+          const C* A1[1] = {r[0]};
+          dots(st, 1, A1, A1, S.I);
+        }
+        k_pg_rnrm<<<1, 256, 0, st>>>(R, S, ops.d_out);
+        note_launch();
+      }
+      if (!rc) {
+        const C* A6[6] = {r[0], r[1], r[1], r[2], r[2], r[2]};
+        const C* B6[6] = {r[0], r[0], r[1], r[0], r[1], r[2]};
+        dots(st, 6, A6, B6, S.I);
+        k_pg_gram<<<1, 64, 0, st>>>(R, S, ops.d_out);
+        note_launch();
+        lin(st, u[0], S.one, u[1], S.co + 5 * R, u[2], S.co + 6 * R, S.I);
+        lin(st, X, S.one, r[0], S.co + 3 * R, r[1], S.co + 4 * R, S.I);
+        lin(st, r[0], S.one, r[1], S.co + 5 * R, r[2], S.co + 6 * R, S.I);
+        k_pg_post<<<1, 32, 0, st>>>(R, tol, S, hck);
+        note_launch();
+        kernels_a = launch_total() - c0;
+        // IF node 1: the reliable-residual check with residual replacement
+        const unsigned long long c1 = launch_total();
+        e = if_node(hck, [&]() {
+          if (!rc) rc = matvec(X, sy, S.CK);
+          BDot<T> dn{};
+          dn.K = 2; dn.mode = 1; dn.a[0] = BP; dn.b[0] = sy; dn.c[0] = r[0];
+          kb_dots<T><<<dim3(ops.nb, R), BT, 0, st2>>>(n, dn, S.CK, ops.d_part, ops.d_out, ops.d_cnt);
+          note_launch();
+          k_pg_check<<<1, 256, 0, st2>>>(R, tol, S, ops.d_out);
+          note_launch();
+          lin(st2, r[0], nullptr, BP, S.one, sy, S.mone, S.RP);
+        });
+        kernels_b = launch_total() - c1;
+        if (e == cudaSuccess) {
+          const unsigned long long c2 = launch_total();
+          k_pg_rc<<<1, 32, 0, st>>>(R, S, hrc);
+          note_launch();
+          kernels_a += launch_total() - c2;
+          // IF node 2: the reliable update of r_0 (and of the solution shift)
+          const unsigned long long c3 = launch_total();
+          e = if_node(hrc, [&]() {
+            if (!rc) rc = matvec(X, sy, S.RC);
+            lin(st2, r[0], nullptr, BP, S.one, sy, S.mone, S.RC);
+            lin(st2, XP, S.one, X, S.one, nullptr, nullptr, S.XD);
+            lin(st2, X, nullptr, nullptr, nullptr, nullptr, nullptr, S.XD);
+            lin(st2, BP, nullptr, r[0], S.one, nullptr, nullptr, S.XD);
+            k_pg_rcpost<<<1, 256, 0, st2>>>(R, S);
+            note_launch();
+          });
+          kernels_c = launch_total() - c3;
+        }
+        if (e == cudaSuccess) {
+          k_pg_count<<<1, 32, 0, st>>>(R, maxit, tol, S);
+          note_launch();
+          kernels_a += 1;
+        }
+      }
+    }
+    cudaGraph_t g_out = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(st, &g_out);
+    if (e == cudaSuccess) e = e2;
+    graph = g_out;
+    if (e == cudaSuccess && !rc) e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e != cudaSuccess) { set_cuda_error("graph solve capture", e); rc = 1; }
+  }
+  long long launches = 0;
+  int checks = 0, updates = 0;
+  if (!rc) {
+    int* h_cnt = nullptr;
+    e = cudaMallocHost((void**)&h_cnt, 3 * sizeof(int));
+    const long long cap = (long long)maxit + 64;  // every RHS stops at maxit; the loop is bounded
+    while (e == cudaSuccess && launches < cap) {
+      for (int k = 0; k < 4 && e == cudaSuccess; ++k, ++launches) e = cudaGraphLaunch(exec, st);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(h_cnt, S.active, 3 * sizeof(int), cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess || h_cnt[0] == 0) break;
+    }
+    if (e == cudaSuccess) { checks = h_cnt[1]; updates = h_cnt[2]; }
+    cudaFreeHost(h_cnt);
+    if (e != cudaSuccess) { set_cuda_error("graph solve", e); rc = 1; }
+    note_launch((unsigned long long)launches * kernels_a + (unsigned long long)checks * kernels_b +
+                (unsigned long long)updates * kernels_c);
+  }
+  if (!rc) {
+    std::vector<double> hd(nd);
+    std::vector<int> hi(ni);
+    e = cudaMemcpy(hd.data(), dd, nd * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(hi.data(), ii, ni * sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) { set_cuda_error("graph solve state", e); rc = 1; }
+    long long mv_rhs = 0;
+    for (int i = 0; i < R && !rc; ++i) {
+      hs.resid[i] = hd[(size_t)4 * R + i];
+      hs.it[i] = hi[i]; hs.live[i] = hi[R + i]; hs.status[i] = hi[2 * R + i];
+      mv_rhs += hi[3 * R + i] - nc[i];
+      nc[i] = hi[3 * R + i];
+    }
+    io.matvec_rhs += mv_rhs;
+    io.matvec_calls += (int)(4 * launches + checks + updates);
+    io.matvec_ms += mv_ms_per_rhs * (double)mv_rhs;
+  }
+  if (exec) cudaGraphExecDestroy(exec);
+  if (graph) cudaGraphDestroy(graph);
+  eng.stream = eng_st;
+  cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
+  cudaStreamDestroy(st2);
+  cudaFree(blk);
+  return rc;
+}
+
+// --------------------------------------------------------------------------
 // PBCGS2 (per RHS: solvers.cu solve_pbcgs2, reference cu:459-480, cu:1168-1278)
 template <typename T> int solve_batch_pbcgs2(BatchIO<T>& io, BatchResult& res) {
   using C = cplx<T>;
@@ -1189,10 +1658,30 @@ template <typename T> int solve_batch_pbcgs2(BatchIO<T>& io, BatchResult& res) {
   }
   std::vector<int> it(R, 0);
   int rc;
+  // DDSCAT_B200_GRAPH with residual replacement: the first iteration runs
+  // host-driven (it sizes the workspace and times the MATVEC), the rest as a
+  // captured graph per iteration
+  const bool use_graph = io.graph && io.replace;
+  int host_iters = 0;
   for (;;) {
     std::vector<int> I(R, 0);
     for (int i = 0; i < R; ++i) I[i] = live[i] && resid[i] > io.tol && it[i] < io.maxit;
     if (!any_of(I)) break;
+    if (use_graph && host_iters >= 1) {
+      float t = 0.f;
+      cudaStreamSynchronize(ops.stream);
+      if (!c.ev.empty()) cudaEventElapsedTime(&t, c.ev.back().first, c.ev.back().second);
+      const double per_rhs = c.last_cnt > 0 ? (double)t / c.last_cnt : 0.0;
+      PGHost hs{alpha, omega, sigma, rho0, rho1, beta, rnrm0, rnrm, mxx, mxr, resid, it, live, res.status};
+      C* wv[11] = {rr, r[0], r[1], r[2], u[0], u[1], u[2], XP, BP, X, sy};
+      if ((rc = pbcgs2_graph_loop<T>(io, ops, c.nc, wv, hs, per_rhs))) return rc;
+      resid = hs.resid;
+      it = hs.it;
+      live = hs.live;
+      res.status = hs.status;
+      break;
+    }
+    ++host_iters;
     for (int i = 0; i < R; ++i)
       if (I[i]) { it[i]++; rho0[i] = -(omega[i] * rho0[i]); }
     const int* MI = ops.mask(I);

@@ -263,7 +263,8 @@ class DDA:
         replace=True selects residual replacement instead of restarts at the
         reliable-residual checks; symmetric=True (QMRCCG) uses one MATVEC per
         iteration (left Lanczos vectors equal to the right ones); graph=True
-        (with both) runs the iterations device-driven as a CUDA graph."""
+        (QMRCCG with both, PBCGS2 with replace) runs the iterations
+        device-driven as a CUDA graph."""
         nrhs = int(b.shape[0])
         for a in (b, x, adia) + (() if aoff is None else (aoff,)):
             if tuple(a.shape) != (nrhs, 3 * self.nat):

@@ -167,6 +167,34 @@ def test_batch_qmrccg_graph_matches_host_driven(n):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("n", [16, 24])
+def test_batch_pbcgs2_graph_matches_host_driven(n):
+    """Device-driven PBCGS2 iterations (DDSCAT_B200_GRAPH with residual
+    replacement: FP64 scalars and the 3 x 3 minimal-residual step in
+    single-thread kernels, the reliable-residual check and the reliable update
+    in IF conditional nodes) follow the host-driven batched PBCGS2: iteration
+    counts within one, solutions within 20*TOL, FP64 residual <= 1.2*TOL."""
+    prob = targets.make_problem(n, m=1.5 + 0.02j, x=5.0, orientations=targets.random_orientations(3, seed=7))
+    dda = D.DDA()
+    dda.prepare_green(n, n, n, prob.iocc, prob.incid[0].k)
+    b, adia = _batch_inputs(prob)
+    xh, xg = np.zeros_like(b), np.zeros_like(b)
+    host = dda.solve_batch("pbcgs2", b, xh, adia, maxit=2000, tol=TOL, replace=True)
+    l0 = dda.launch_count()
+    gr = dda.solve_batch("pbcgs2", b, xg, adia, maxit=2000, tol=TOL, replace=True, graph=True)
+    assert dda.launch_count() > l0
+    assert np.all(gr.status == 0) and np.all(gr.tole <= TOL), (gr.status, gr.tole)
+    assert np.all(np.abs(gr.itno - host.itno) <= 1), (gr.itno, host.itno)
+    assert np.all(np.abs(gr.ncompte - host.ncompte) <= 6), (gr.ncompte, host.ncompte)
+    assert np.all(dda.residual_f64(b, xg, adia) <= 1.2 * TOL)
+    for r in range(b.shape[0]):
+        assert np.linalg.norm(xg[r] - xh[r]) / np.linalg.norm(xh[r]) < 20 * TOL
+    ms, rhs, calls = dda.last_solve_stats()
+    assert rhs == int(gr.ncompte.sum()) and ms > 0
+    dda.release()
+
+
+@pytest.mark.gpu
 def test_batch_qmrccg_nonzero_initial_guess():
     """A nonzero x0 enters through A x0 (formed only for the RHS whose x0 is
     nonzero; for x0 = 0 the product is exactly zero and is skipped, still

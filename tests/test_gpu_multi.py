@@ -31,7 +31,10 @@ def c4_targets(count=40, seed=0, grid="fast"):
 
 
 @pytest.mark.gpu
-def test_c4_uneven_multi_target():
+@pytest.mark.parametrize("graph", [False, True])
+def test_c4_uneven_multi_target(graph):
+    """graph=True: each target's PBCGS2 iterations run device-driven (one
+    captured graph per iteration and target)."""
     probs = c4_targets()
     items = []
     for p in probs:
@@ -39,7 +42,7 @@ def test_c4_uneven_multi_target():
         items.append({"dims": (p.nx, p.ny, p.nz), "iocc": p.iocc, "ak": p.incid[0].k, "b": b,
                       "x": np.zeros_like(b), "adia": np.stack([p.adia(r) for r in range(2)])})
     dda = D.DDA()
-    out = dda.multi_solve(items, "pbcgs2", maxit=3000, tol=TOL, symmetric=False)
+    out = dda.multi_solve(items, "pbcgs2", maxit=3000, tol=TOL, symmetric=False, graph=graph)
     assert out.itno.size == 80 and np.all(out.status == 0) and np.all(out.tole <= TOL)
     sizes = [p.nat for p in probs]
     for t in (int(np.argmin(sizes)), int(np.argsort(sizes)[len(sizes) // 2]), int(np.argmax(sizes))):
