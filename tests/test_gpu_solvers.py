@@ -96,7 +96,7 @@ def test_initial_guess_and_maxit_semantics():
 @pytest.mark.gpu
 def test_config_c1_sphere_q_parity():
     """32^3 sphere, m=1.50+0.01i, x=5, PBCGS2 at 1e-5, two polarisations:
-    Qext/Qabs within 1e-4 of the FP64 oracle solve."""
+    Qext/Qabs within 1e-4 of the FP64 oracle solve (the accuracy bar for Q values)."""
     prob = targets.make_problem(32, m=1.5 + 0.01j, x=5.0)
     dda = D.DDA()
     dda.prepare_green(32, 32, 32, prob.iocc, prob.incid[0].k)
