@@ -81,9 +81,13 @@ __global__ void __launch_bounds__(BT) kb_dots(int n, BDot<T> sp, const int* mask
       acc[1].x += er * er + ei * ei;
     }
   }
+  // the loops over k stay unrolled with compile-time indices so that acc
+  // lives in registers
   const int K = sp.mode == 0 ? sp.K : 2;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int k = 0; k < K; ++k) {
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    if (k >= K) break;
     const double2 v = wsum2(acc[k]);
     if (lane == 0) ws[k][wid] = v;
   }

@@ -67,7 +67,9 @@ __global__ void __launch_bounds__(RED_THREADS) k_dots(int n, DotSpec<T> sp, doub
     }
   }
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int q = 0; q < sp.k; ++q) {
+#pragma unroll
+  for (int q = 0; q < RED_MAXK; ++q) {  // compile-time indices: acc stays in registers
+    if (q >= sp.k) break;
     double2 v = warp_sum(acc[q]);
     if (lane == 0) wsum[q][wid] = v;
   }
