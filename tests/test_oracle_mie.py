@@ -1,0 +1,55 @@
+"""Physics checks of the oracle against the Mie series of a homogeneous sphere
+(CPU).  The Mie code (oracle/mie.py) is first checked against the Rayleigh
+limit; the oracle's FP64 DDA of a lattice sphere (LDR polarisability, volume-
+equivalent radius from NAT0) must then reproduce Mie's Q_ext and Q_abs within
+the DDA discretisation error, which is about 1 % at |m| k d < 0.5."""
+import math
+
+import numpy as np
+import pytest
+
+from ddscat_b200 import targets
+from oracle import ddscat_oracle as O
+from oracle.mie import mie_efficiencies
+
+
+@pytest.mark.parametrize("x,m", [(0.02, 1.5 + 0.1j), (0.05, 1.33 + 0.01j)])
+def test_mie_rayleigh_limit(x, m):
+    """Q_abs -> 4x Im(alpha), Q_sca -> 8/3 x^4 |alpha|^2, alpha = (m^2-1)/(m^2+2),
+    with relative corrections of order x^2."""
+    qext, qsca, qabs, g = mie_efficiencies(x, m)
+    al = (m * m - 1) / (m * m + 2)
+    assert qabs == pytest.approx(4 * x * al.imag, rel=2e-3)
+    assert qsca == pytest.approx(8.0 / 3.0 * x ** 4 * abs(al) ** 2, rel=2e-3)
+    assert abs(g) < 1e-3
+
+
+def test_mie_real_index_does_not_absorb():
+    qext, qsca, qabs, g = mie_efficiencies(5.0, 1.5 + 0.0j)
+    assert abs(qabs) < 1e-10 * qext
+    assert 0.0 < g < 1.0
+
+
+@pytest.mark.parametrize("n,m,x,tol_ext,tol_abs", [
+    (16, 1.33 + 0.1j, 1.0, 0.01, 0.01),
+    # the small plain-path configuration: 32^3 sphere, m = 1.50 + 0.01i, x = 5
+    (32, 1.5 + 0.01j, 5.0, 0.01, 0.03),
+])
+def test_oracle_dda_sphere_matches_mie(n, m, x, tol_ext, tol_abs):
+    prob = targets.make_problem(n, m=m, x=x)
+    gp = O.GreenParams(n, n, n, ak=tuple(prob.incid[0].k))
+    op = O.Operator.from_params(gp, prob.iocc)
+    area = math.pi * prob.aeff ** 2
+    qext, qabs = [], []
+    for r in range(2):  # both incident polarisations
+        b = O.gather_compact(prob.rhs(r), op.occ, prob.nat)
+        adia = O.gather_compact(prob.adia(r), op.occ, prob.nat)
+        aoff = np.zeros_like(adia)
+        res = O.solve_qmrccg(lambda v: op.apply_compact(v, adia, aoff), b, np.zeros_like(b), 1000, 1e-6)
+        assert res.status == 0
+        cabs, cext, _ = O.evalq(b, res.x, adia, aoff, prob.incid[r].k, 1.0)
+        qext.append(cext / area)
+        qabs.append(cabs / area)
+    me, _, ma, _ = mie_efficiencies(x, m)
+    assert np.mean(qext) == pytest.approx(me, rel=tol_ext)
+    assert np.mean(qabs) == pytest.approx(ma, rel=tol_abs)
