@@ -61,3 +61,42 @@ def mie_efficiencies(x: float, m: complex):
     gq = 4.0 / x ** 2 * float(np.sum(n * (n + 2) / (n + 1) * (an * np.conj(an1) + bn * np.conj(bn1)).real
                                      + (2 * n + 1) / (n * (n + 1)) * (an * np.conj(bn)).real))
     return qext, qsca, qext - qsca, gq / qsca
+
+
+def mie_amplitudes(x: float, m: complex, theta):
+    """Amplitude functions S1(theta), S2(theta) of the sphere (Bohren & Huffman
+    eq. 4.74) with the angular functions pi_n, tau_n of their eq. 4.47:
+    pi_0 = 0, pi_1 = 1, pi_n = (2n-1)/(n-1) mu pi_{n-1} - n/(n-1) pi_{n-2},
+    tau_n = n mu pi_n - (n+1) pi_{n-1}, mu = cos(theta)."""
+    x = float(x)
+    m = complex(m)
+    y = m * x
+    nstop = int(round(x + 4.0 * x ** (1.0 / 3.0) + 2.0))
+    nmx = int(round(max(nstop, abs(y)))) + 15
+    d = np.zeros(nmx + 1, dtype=complex)
+    for n in range(nmx, 0, -1):
+        d[n - 1] = n / y - 1.0 / (d[n] + n / y)
+    mu = np.cos(np.asarray(theta, dtype=np.float64))
+    s1 = np.zeros(mu.shape, dtype=complex)
+    s2 = np.zeros(mu.shape, dtype=complex)
+    psi0, psi1 = math.cos(x), math.sin(x)
+    chi0, chi1 = -math.sin(x), math.cos(x)
+    xi1 = complex(psi1, -chi1)
+    pi0, pi1 = np.zeros_like(mu), np.ones_like(mu)  # pi_{n-1}, pi_n for n = 1
+    for n in range(1, nstop + 1):
+        psi = (2.0 * n - 1.0) / x * psi1 - psi0
+        chi = (2.0 * n - 1.0) / x * chi1 - chi0
+        xi = complex(psi, -chi)
+        ta = d[n] / m + n / x
+        tb = m * d[n] + n / x
+        an = (ta * psi - psi1) / (ta * xi - xi1)
+        bn = (tb * psi - psi1) / (tb * xi - xi1)
+        tau = n * mu * pi1 - (n + 1) * pi0
+        fn = (2.0 * n + 1.0) / (n * (n + 1.0))
+        s1 += fn * (an * pi1 + bn * tau)
+        s2 += fn * (an * tau + bn * pi1)
+        psi0, psi1 = psi1, psi
+        chi0, chi1 = chi1, chi
+        xi1 = complex(psi1, -chi1)
+        pi0, pi1 = pi1, ((2.0 * n + 1.0) / n) * mu * pi1 - ((n + 1.0) / n) * pi0
+    return s1, s2
