@@ -38,23 +38,32 @@ def test_mie_real_index_does_not_absorb():
     (32, 1.5 + 0.01j, 5.0, 0.01, 0.03),
 ])
 def test_oracle_dda_sphere_matches_mie(n, m, x, tol_ext, tol_abs):
+    """Q_ext, Q_abs (EVALQ) and Q_sca, g (SCAT's angular integration at
+    ETASCA = 0.5) of the lattice sphere, averaged over both polarisations."""
     prob = targets.make_problem(n, m=m, x=x)
     gp = O.GreenParams(n, n, n, ak=tuple(prob.incid[0].k))
     op = O.Operator.from_params(gp, prob.iocc)
+    k = prob.incid[0].k
+    khat = np.asarray(k) / np.linalg.norm(k)
     area = math.pi * prob.aeff ** 2
-    qext, qabs = [], []
+    qext, qabs, qsca, g = [], [], [], []
     for r in range(2):  # both incident polarisations
         b = O.gather_compact(prob.rhs(r), op.occ, prob.nat)
         adia = O.gather_compact(prob.adia(r), op.occ, prob.nat)
         aoff = np.zeros_like(adia)
         res = O.solve_qmrccg(lambda v: op.apply_compact(v, adia, aoff), b, np.zeros_like(b), 1000, 1e-6)
         assert res.status == 0
-        cabs, cext, _ = O.evalq(b, res.x, adia, aoff, prob.incid[r].k, 1.0)
+        cabs, cext, _ = O.evalq(b, res.x, adia, aoff, k, 1.0)
+        sc = O.scat(res.x, op.occ, prob.nx, prob.ny, 0, k, [], (1, 1, 1), [], [], 1.0, 0.5, prob.incid[r].e, prob.x0)
         qext.append(cext / area)
         qabs.append(cabs / area)
-    me, _, ma, _ = mie_efficiencies(x, m)
+        qsca.append(sc["csca"] / area)
+        g.append(float(np.dot(sc["cscag"], khat)) / sc["csca"])
+    me, ms, ma, mg = mie_efficiencies(x, m)
     assert np.mean(qext) == pytest.approx(me, rel=tol_ext)
     assert np.mean(qabs) == pytest.approx(ma, rel=tol_abs)
+    assert np.mean(qsca) == pytest.approx(ms, rel=0.02)
+    assert abs(np.mean(g) - mg) < 0.01
 
 
 def test_mie_forward_amplitude_optical_theorem():
