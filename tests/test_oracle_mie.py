@@ -32,34 +32,39 @@ def test_mie_real_index_does_not_absorb():
     assert 0.0 < g < 1.0
 
 
-@pytest.mark.parametrize("n,m,x,tol_ext,tol_abs", [
-    (16, 1.33 + 0.1j, 1.0, 0.01, 0.01),
+@pytest.mark.parametrize("n,m,x,tol_ext,tol_abs,tol_pha", [
+    (16, 1.33 + 0.1j, 1.0, 0.01, 0.01, 0.01),
     # the small plain-path configuration: 32^3 sphere, m = 1.50 + 0.01i, x = 5
-    (32, 1.5 + 0.01j, 5.0, 0.01, 0.03),
+    (32, 1.5 + 0.01j, 5.0, 0.01, 0.03, 0.03),
 ])
-def test_oracle_dda_sphere_matches_mie(n, m, x, tol_ext, tol_abs):
-    """Q_ext, Q_abs (EVALQ) and Q_sca, g (SCAT's angular integration at
-    ETASCA = 0.5) of the lattice sphere, averaged over both polarisations."""
+def test_oracle_dda_sphere_matches_mie(n, m, x, tol_ext, tol_abs, tol_pha):
+    """Q_ext, Q_abs, Q_pha (EVALQ) and Q_sca, g (SCAT's angular integration at
+    ETASCA = 0.5) of the lattice sphere, averaged over both polarisations.
+    Q_pha is DDSCAT's phase-lag efficiency, -2/x^2 Im S(0) in Bohren &
+    Huffman's convention (positive for a small sphere with Re m > 1)."""
     prob = targets.make_problem(n, m=m, x=x)
     gp = O.GreenParams(n, n, n, ak=tuple(prob.incid[0].k))
     op = O.Operator.from_params(gp, prob.iocc)
     k = prob.incid[0].k
     khat = np.asarray(k) / np.linalg.norm(k)
     area = math.pi * prob.aeff ** 2
-    qext, qabs, qsca, g = [], [], [], []
+    qext, qabs, qpha, qsca, g = [], [], [], [], []
     for r in range(2):  # both incident polarisations
         b = O.gather_compact(prob.rhs(r), op.occ, prob.nat)
         adia = O.gather_compact(prob.adia(r), op.occ, prob.nat)
         aoff = np.zeros_like(adia)
         res = O.solve_qmrccg(lambda v: op.apply_compact(v, adia, aoff), b, np.zeros_like(b), 1000, 1e-6)
         assert res.status == 0
-        cabs, cext, _ = O.evalq(b, res.x, adia, aoff, k, 1.0)
+        cabs, cext, cpha = O.evalq(b, res.x, adia, aoff, k, 1.0)
         sc = O.scat(res.x, op.occ, prob.nx, prob.ny, 0, k, [], (1, 1, 1), [], [], 1.0, 0.5, prob.incid[r].e, prob.x0)
         qext.append(cext / area)
         qabs.append(cabs / area)
+        qpha.append(cpha / area)
         qsca.append(sc["csca"] / area)
         g.append(float(np.dot(sc["cscag"], khat)) / sc["csca"])
     me, ms, ma, mg = mie_efficiencies(x, m)
+    s1, _ = mie_amplitudes(x, m, np.array([0.0]))
+    assert np.mean(qpha) == pytest.approx(-2.0 / x ** 2 * s1[0].imag, rel=tol_pha)
     assert np.mean(qext) == pytest.approx(me, rel=tol_ext)
     assert np.mean(qabs) == pytest.approx(ma, rel=tol_abs)
     assert np.mean(qsca) == pytest.approx(ms, rel=0.02)
