@@ -32,23 +32,26 @@ def test_mie_real_index_does_not_absorb():
     assert 0.0 < g < 1.0
 
 
-@pytest.mark.parametrize("n,m,x,tol_ext,tol_abs,tol_pha", [
-    (16, 1.33 + 0.1j, 1.0, 0.01, 0.01, 0.01),
+@pytest.mark.parametrize("n,m,x,tol_ext,tol_abs,tol_pha,tol_bk", [
+    (16, 1.33 + 0.1j, 1.0, 0.01, 0.01, 0.01, 0.02),
     # the small plain-path configuration: 32^3 sphere, m = 1.50 + 0.01i, x = 5
-    (32, 1.5 + 0.01j, 5.0, 0.01, 0.03, 0.03),
+    # (the backscatter of a lattice sphere carries the largest DDA error)
+    (32, 1.5 + 0.01j, 5.0, 0.01, 0.03, 0.03, 0.15),
 ])
-def test_oracle_dda_sphere_matches_mie(n, m, x, tol_ext, tol_abs, tol_pha):
-    """Q_ext, Q_abs, Q_pha (EVALQ) and Q_sca, g (SCAT's angular integration at
-    ETASCA = 0.5) of the lattice sphere, averaged over both polarisations.
-    Q_pha is DDSCAT's phase-lag efficiency, -2/x^2 Im S(0) in Bohren &
-    Huffman's convention (positive for a small sphere with Re m > 1)."""
+def test_oracle_dda_sphere_matches_mie(n, m, x, tol_ext, tol_abs, tol_pha, tol_bk):
+    """Q_ext, Q_abs, Q_pha (EVALQ) and Q_sca, g, the backscatter (SCAT's
+    angular integration at ETASCA = 0.5, whose last direction is -k) of the
+    lattice sphere, averaged over both polarisations.  Q_pha is DDSCAT's
+    phase-lag efficiency, -2/x^2 Im S(0) in Bohren & Huffman's convention
+    (positive for a small sphere with Re m > 1); CBKSCA is the differential
+    cross section at 180 deg, |S1(pi)|^2 / k^2."""
     prob = targets.make_problem(n, m=m, x=x)
     gp = O.GreenParams(n, n, n, ak=tuple(prob.incid[0].k))
     op = O.Operator.from_params(gp, prob.iocc)
     k = prob.incid[0].k
     khat = np.asarray(k) / np.linalg.norm(k)
     area = math.pi * prob.aeff ** 2
-    qext, qabs, qpha, qsca, g = [], [], [], [], []
+    qext, qabs, qpha, qsca, g, qbk = [], [], [], [], [], []
     for r in range(2):  # both incident polarisations
         b = O.gather_compact(prob.rhs(r), op.occ, prob.nat)
         adia = O.gather_compact(prob.adia(r), op.occ, prob.nat)
@@ -61,10 +64,12 @@ def test_oracle_dda_sphere_matches_mie(n, m, x, tol_ext, tol_abs, tol_pha):
         qabs.append(cabs / area)
         qpha.append(cpha / area)
         qsca.append(sc["csca"] / area)
+        qbk.append(sc["cbksca"] / area)
         g.append(float(np.dot(sc["cscag"], khat)) / sc["csca"])
     me, ms, ma, mg = mie_efficiencies(x, m)
-    s1, _ = mie_amplitudes(x, m, np.array([0.0]))
+    s1, _ = mie_amplitudes(x, m, np.array([0.0, math.pi]))
     assert np.mean(qpha) == pytest.approx(-2.0 / x ** 2 * s1[0].imag, rel=tol_pha)
+    assert np.mean(qbk) == pytest.approx(abs(s1[1]) ** 2 / (math.pi * x ** 2), rel=tol_bk)
     assert np.mean(qext) == pytest.approx(me, rel=tol_ext)
     assert np.mean(qabs) == pytest.approx(ma, rel=tol_abs)
     assert np.mean(qsca) == pytest.approx(ms, rel=0.02)
