@@ -47,7 +47,7 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=128)
-    ap.add_argument("--orient", type=int, default=8, help="orientations per rank (x2 polarisations = RHS per step)")
+    ap.add_argument("--orient", type=int, default=64, help="orientations per rank (x2 polarisations = RHS per step)")
     ap.add_argument("--solver", default="qmrccg", choices=["qmrccg", "pbcgs2"])
     ap.add_argument("--tol", type=float, default=1e-5)
     ap.add_argument("--maxit", type=int, default=4000)
@@ -58,7 +58,9 @@ def parse_args():
                          "reference's two-product form")
     ap.add_argument("--graph", default="on", choices=["on", "off"],
                     help="QMRCCG symmetric form with replacement: device-driven iterations launched as a CUDA graph")
-    ap.add_argument("--ref-rhs", type=int, default=0, help="RHS per step of the reference arm (0: the whole batch)")
+    ap.add_argument("--ref-rhs", type=int, default=2,
+                    help="RHS per step of the reference arm: a bounded sample of the batch, a different orientation's "
+                         "pair of RHS each step (0: the whole batch)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-q-check", action="store_true", help="skip the all-FP64 reference solve and Q errors")
     return ap.parse_args()
@@ -185,6 +187,7 @@ def config(args, prob, R, world):
     return {"workload": f"{args.n}^3 sphere, m=1.33+0.05i, x=20, {args.solver.upper()} tol {args.tol:g}, "
                         f"{args.orient} orientations x 2 polarisations per rank",
             "n": args.n, "nat": prob.nat, "nat0": prob.nat0, "rhs_per_rank": R, "solver": args.solver,
+            "polarisability": f"{prob.cmdpol} (isotropic material; CXAOFF = 0)",
             "tol": args.tol, "fp64_check": "GPU all-FP64 MATVEC true residual, every RHS, every step",
             "l2": "inputs larger than L2 (each RHS vector 3*NAT*8 B > 50 MB; working set > 1 GB)",
             "parallelism": f"replicas x{world} (independent RHS batches per GPU)",
@@ -217,6 +220,17 @@ def load_profile_traffic(n):
     return None
 
 
+def cpu_model():
+    """Host CPU model name (Linux /proc/cpuinfo), for the CPU baseline record."""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def measured_peak():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -247,9 +261,40 @@ def cpu_baseline(prob, ncompte_mean):
         op.apply_compact(xc, ac, oc)
     t_mv = (time.perf_counter() - t0) / nmv
     per_rhs = t_mv * ncompte_mean
-    return {"value": 1.0 / per_rhs, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+    return {"value": 1.0 / per_rhs, "unit": UNIT, "cores": os.cpu_count(), "cpu_model": cpu_model(), "kind": "port",
             "sample": f"{nmv} MATVECs of the complex64 oracle FFT operator at {nx}^3 (scipy.fft, "
-                      f"{os.cpu_count()} threads), {t_mv:.3f} s each, scaled by {ncompte_mean:.1f} MATVECs per RHS"}
+                      f"{os.cpu_count()} threads), {t_mv:.3f} s each, scaled by {ncompte_mean:.1f} MATVECs per RHS",
+            "c1_full_solve": cpu_c1_solve()}
+
+
+def cpu_c1_solve():
+    """A whole CPU solve timed end to end on the small sphere workload (32^3,
+    m = 1.50+0.01i, x = 5, PBCGS2 at tol 1e-5, both polarisations): the
+    oracle's complex64 FFT operator (scipy.fft, all host threads) inside the
+    oracle's PBCGS2 recurrence (FP64 vectors and scalars)."""
+    from ddscat_b200 import targets
+    from oracle import ddscat_oracle as O
+
+    prob = targets.make_problem(32, m=1.5 + 0.01j, x=5.0)
+    k = prob.incid[0].k
+    t0 = time.perf_counter()
+    op = O.Operator.from_params(O.GreenParams(32, 32, 32, ak=tuple(float(np.float32(a)) for a in k)), prob.iocc,
+                                dtype=np.complex64)
+    t_green = time.perf_counter() - t0
+    occ = op.occ
+    zero = np.zeros(3 * op.nat0, dtype=np.complex64)
+    its, times = [], []
+    for r in range(len(prob.incid)):
+        bc = O.gather_compact(prob.rhs(r), occ, prob.nat)
+        ac = O.gather_compact(prob.adia(r), occ, prob.nat).astype(np.complex64)
+        t0 = time.perf_counter()
+        res = O.solve_pbcgs2(lambda v: op.apply_compact(v.astype(np.complex64), ac, zero).astype(np.complex128),
+                             bc, np.zeros_like(bc), 500, 1e-5)
+        times.append(time.perf_counter() - t0)
+        its.append(res.itno)
+    return {"workload": "32^3 sphere, m=1.50+0.01i, x=5, PBCGS2 tol 1e-5, 1 orientation x 2 polarisations",
+            "s_per_rhs": float(np.mean(times)), "rhs_per_s": 1.0 / float(np.mean(times)),
+            "iterations": its, "green_build_s": t_green, "threads": os.cpu_count(), "cpu_model": cpu_model()}
 
 
 # ------------------------------------------------------------------ our arm
@@ -379,6 +424,37 @@ def run_ours(args):
     h2d = R * vec * 3  # b, x0 and CXADIA
     d2h = R * vec      # x
 
+    # The drop-in path as unchanged DDSCAT calls it: this library's own
+    # ddscat_cuda_solve_<solver>_f32 (the reference's entry point, its
+    # recurrence and restart rule) with host buffers, one RHS per call, on the
+    # same bounded sample as the reference arm (--ref-rhs RHS per step, a
+    # different orientation each step); console lines off, as in benchmarks.
+    abi = None
+    if rank == 0 and world == 1:
+        nref = R if args.ref_rhs <= 0 else min(args.ref_rhs, R)
+        aoff0 = np.zeros(b.shape[1], dtype=np.complex64)
+        dda.lib.ddscat_b200_set_verbose(0)
+        dda.solve(args.solver, b[0], adia[0], aoff0, maxit=args.maxit, tol=args.tol)  # warm-up
+        its, ncs = [], []
+        torch.cuda.synchronize()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record()
+        for st in range(args.steps):
+            for j in range(nref):
+                r = (nref * st + j) % R
+                o = dda.solve(args.solver, b[r], adia[r], aoff0, maxit=args.maxit, tol=args.tol)
+                its.append(o.itno)
+                ncs.append(o.ncompte)
+        g1.record()
+        torch.cuda.synchronize()
+        dda.lib.ddscat_b200_set_verbose(-1)
+        abi_s = g0.elapsed_time(g1) / 1000.0
+        abi = {"value": nref * args.steps / abi_s, "unit": UNIT,
+               "entry_point": f"ddscat_cuda_solve_{args.solver}_f32 (the reference's C ABI, host buffers, one RHS per call)",
+               "rhs_per_step": nref, "steps": args.steps, "iterations_mean": float(np.mean(its)),
+               "matvecs_per_rhs_mean": float(np.mean(ncs)),
+               "sample": "the reference arm's sample: step s solves RHS nref*s .. nref*s+nref-1 (mod the batch)"}
+
     # Q errors of the FP32 solutions against the same batch solved all-FP64 on
     # the GPU (outside the timed regions; every rank checks its own batch)
     qerr = None
@@ -408,6 +484,7 @@ def run_ours(args):
         # amplitudes of the FP64 solutions), both through the Mueller entry points
         from ddscat_b200 import targets as T
         s11_err, sij_err, ndir = 0.0, 0.0, 0
+        csca_err, g_err, navg = 0.0, 0.0, 0
         for o in range(R // 2):
             r0, r1 = 2 * o, 2 * o + 1
             k = prob.incid[r0].k
@@ -419,6 +496,13 @@ def run_ours(args):
                 sc = dda.scat(k, prob.incid[r].e, prob.x0, etasca=0.5, aks=aks.astype(np.float32),
                               em1=em1.astype(np.float32), em2=em2.astype(np.float32))
                 f32.append((sc["f1"], sc["f2"]))
+                # Qsca and g of the FP32 solution (FP32 phases, FP64 sums) against the
+                # FP64 solution's (FP64 phases and sums), same directions and weights
+                s64 = dda.scat_csca_f64(np.ascontiguousarray(x64[r:r + 1]), k, prob.incid[r].e, prob.x0, etasca=0.5)
+                c64 = float(s64["csca"][0])
+                csca_err = max(csca_err, abs(sc["csca"] - c64) / c64)
+                g_err = max(g_err, abs(sc["cscag"][0] / sc["csca"] - float(s64["cscag"][0, 0]) / c64))
+                navg = int(s64["navg"][0])
             _, m32 = dda.mueller(k, prob.incid[r0].e, prob.incid[r1].e, em2.astype(np.float32),
                                  f32[0][0], f32[0][1], f32[1][0], f32[1][1])
             g1, g2 = dda.scat_amplitudes_f64(np.ascontiguousarray(x64[r0:r1 + 1]), k, aks, em1, em2, prob.x0)
@@ -427,6 +511,8 @@ def run_ours(args):
             s11_err = max(s11_err, float(np.max(np.abs(m32[:, 0, 0] - s11) / s11)))
             sij_err = max(sij_err, float(np.max(np.abs(m32 - m64) / s11[:, None, None])))
         qerr = {"cabs_max_rel": worst["cabs"], "cext_max_rel": worst["cext"], "cpha_max_rel": worst["cpha"],
+                "csca_max_rel": csca_err, "g_max_abs": g_err,
+                "csca_g_quadrature": f"SCAT integration at ETASCA 0.5, NAVG {navg} directions",
                 "s11_max_rel": s11_err, "sij_max_abs_over_s11": sij_err,
                 "s_ij_directions": f"theta 0..180 deg at 1 deg in 2 planes ({ndir}) x {R // 2} orientations",
                 "rhs": R, "fp64_solve": f"{args.solver.upper()} all-FP64 on the GPU, tol 1e-8, FP64 far-field sums",
@@ -460,7 +546,7 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "e2e": {"value": total_rhs / e2e_elapsed, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
-            "gpu_launches": launches, "clocks": clk,
+            "gpu_launches": launches, "clocks": clk, "abi_single_rhs": abi,
             "q_error_vs_fp64": qerr,
         }
         print(json.dumps(line), flush=True)
@@ -500,9 +586,15 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": f"reference prepare_green failed with status {rc}"}))
         return
     iters = []
+    R = b.shape[0]
+    nstep = [0]
 
     def step(record, count=nref):
-        for r in range(count):
+        # a different orientation's RHS each step, so the sample spreads over the batch
+        first = nref * nstep[0]
+        nstep[0] += 1
+        for j in range(count):
+            r = (first + j) % R
             x = np.zeros(b.shape[1], dtype=np.complex64)
             it, tole, nc = ct.c_int(), ct.c_float(), ct.c_int()
             rr = fn(P(b[r]), P(x), P(adia[r]), P(aoff), b.shape[1], args.maxit, args.tol, ct.byref(it),
@@ -515,6 +607,7 @@ def run_reference(args):
     with quiet_stdout():
         for _ in range(args.warmup):
             step(False, 1)  # warm-up: one RHS per step
+        nstep[0] = 0
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -525,19 +618,28 @@ def run_reference(args):
     elapsed = e0.elapsed_time(e1) / 1000.0
     value = nref * args.steps / elapsed
     sample = (f"reference ddscat_matvec_cuda.cu built unmodified (oracle/Makefile), {args.solver.upper()} through its "
-              f"own C ABI with host buffers, one RHS at a time, {nref} RHS per step (RHS 0..{nref - 1} of the "
-              f"workload), its own restart policy; the reference implementation of this path runs on the GPU, its host side on 1 thread")
-    cfg = config(args, prob, b.shape[0], world)
+              f"own C ABI with host buffers, one RHS at a time, {nref} RHS per step (step s solves RHS "
+              f"{nref}s..{nref}s+{nref - 1} mod {R} of the workload's batch), its own restart policy; the reference "
+              f"implementation of this path runs on the GPU, its host side on 1 thread")
+    cfg = config(args, prob, R, world)
     cfg["reference_rhs_per_step"] = nref
     cfg["reliable_residual_policy"] = "restart (the reference's own)"
     cfg["qmr_form"] = "two-product (the reference's own)" if args.solver == "qmrccg" else None
+    cfg["fp64_check"] = "none: the reference returns its own FP32 residual TOLE (true residual at its reliable checks)"
+    cfg["iteration_launch"] = ("host-driven, one RHS per call, a host round trip per inner-product group "
+                               "(the reference's own)")
+    vec = b.shape[1] * 8
+    h2d = nref * 4 * vec  # b, x0, CXADIA and CXAOFF copied in by every solve call
+    d2h = nref * vec      # x copied out
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed * 1000.0 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c64 (FP32 complex bulk, FP64 dots)",
             "data": "synthetic (seeded sphere target and incident fields)", "config": cfg, "impl": "reference",
             "iterations_mean": float(np.mean(iters)),
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference", "sample": sample},
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "cpu_model": cpu_model(), "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "copies": "inside the reference's solve call (host buffers in, solution out), every step"}}
     print(json.dumps(line), flush=True)
 
 

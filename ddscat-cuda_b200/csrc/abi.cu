@@ -58,12 +58,12 @@ struct State {
   C *d_xf = nullptr, *d_yf = nullptr, *d_adia = nullptr, *d_aoff = nullptr;  // full 3*NAT
   C *d_b = nullptr, *d_sx = nullptr, *d_sy = nullptr, *d_work = nullptr;     // compact
   bool aoff_zero = false;
-  int verbose = 0;
   // how the target was prepared (for the all-FP64 engine built on demand)
   int prep_kind = 0;  // 1 prepare_green, 2 prepare (CPU Green)
   GreenArgs<float> green_args;
   std::vector<float2> cpu_green;  // CXZC copy for prepare_f32
   int16_t* h_iocc = nullptr;
+  int device = -1;  // the CUDA device current at prepare, which holds the state's buffers
 };
 static State s;
 
@@ -129,15 +129,22 @@ static void release_state() {
     s.ops.release();
     s.eng.release();
   }
-  const int verbose = s.verbose;
   s.cpu_green.clear();
   s = State{};
-  s.verbose = verbose;
 }
 
-static int env_verbose() {
+// Console output level.  1 (the default, as the reference prints for DDSCAT
+// users): the per-MATVEC and per-iteration lines of the 15 reference entry
+// points (cu:417, e.g. cu:1085-1092); 0: silent; 2: also the library
+// extensions' diagnostics (batched-solve phase times, multi-target set-up).
+// DDSCAT_B200_VERBOSE=0/1/2 sets it; ddscat_b200_set_verbose overrides it.
+static int g_verbose = -1;
+int verbose_level() {
+  if (g_verbose >= 0) return g_verbose;
   const char* v = std::getenv("DDSCAT_B200_VERBOSE");
-  return (v && *v && *v != '0') ? 1 : 0;
+  if (!v || !*v) return 1;
+  const int l = std::atoi(v);
+  return l < 0 ? 0 : (l > 2 ? 2 : l);
 }
 
 static int slices_build() {
@@ -225,8 +232,9 @@ static int run_solver(const SolverCodes& sc, SolveFn fn, const void* b, void* x,
   io.b = s.d_b; io.x = s.d_sx;
   io.adia = s.d_adia; io.aoff = s.aoff_zero ? nullptr : s.d_aoff; io.a_full = 1;
   io.work = s.d_work; io.sy = s.d_sy;
-  io.maxit = maxit; io.tol = (double)tol; io.verbose = s.verbose;
+  io.maxit = maxit; io.tol = (double)tol; io.verbose = verbose_level() >= 1;
   const int rc = fn(io);
+  if (io.verbose) std::fflush(stdout);
   if (rc != 0 && !(rc == 87 && sc.publish_on_maxit)) return rc;
   std::string keep = g_last_error;
   if (download_compact_to_full(s.d_sx, x)) return sc.d2h;
@@ -281,6 +289,34 @@ static int make_integration_dirs(const float ak[3], const C e01[3], float etasca
     }
   }
   return 0;
+}
+
+// Csca, Csca*g (3), Csca*<cos^2>, and the backscatter term (last direction)
+// from the far-field sums F(n) = sum_j P_j exp(-i k_s . r_j) at the
+// integration directions: |F - n (n . F)|^2 weighted by the quadrature
+// (ddscat_matvec_cuda.cu:975-1002), times |k|^4 / E02.
+static void scat_integrate(const std::vector<IntDir>& dirs, const double2* sums, double ak2, double e02,
+                           double* cbksca, double* csca, double* cscag, double* cscag2) {
+  const double akk = std::sqrt(ak2);
+  const int nd = (int)dirs.size();
+  double acc[5] = {0, 0, 0, 0, 0}, back = 0.0;
+  for (int i = 0; i < nd; ++i) {
+    const double nx = dirs[i].k[0] / akk, ny = dirs[i].k[1] / akk, nz = dirs[i].k[2] / akk;
+    const double2 sx = sums[3 * i], sy = sums[3 * i + 1], sz = sums[3 * i + 2];
+    const double ndr = nx * sx.x + ny * sy.x + nz * sz.x, ndi = nx * sx.y + ny * sy.y + nz * sz.y;
+    const double exr = sx.x - nx * ndr, exi = sx.y - nx * ndi, eyr = sy.x - ny * ndr, eyi = sy.y - ny * ndi;
+    const double ezr = sz.x - nz * ndr, ezi = sz.y - nz * ndi;
+    const double es2 = exr * exr + exi * exi + eyr * eyr + eyi * eyi + ezr * ezr + ezi * ezi;
+    for (int k = 0; k < 5; ++k) acc[k] += es2 * dirs[i].w[k];
+    if (i == nd - 1) back = es2;
+  }
+  const double fac = ak2 * ak2 / e02;
+  *csca = fac * acc[0];
+  cscag[0] = fac * acc[1];
+  cscag[1] = fac * acc[2];
+  cscag[2] = fac * acc[3];
+  *cscag2 = fac * acc[4];
+  *cbksca = fac * back;
 }
 
 // ---- batched solve ----
@@ -413,16 +449,19 @@ static int widen_to_compact(const void* src, bool dev, int r, double2* dst) {
 // g[r][site j] = -sum_c lam_c(j) dadia_c(j) p_c(j): the derivative of s^T P
 // with respect to a parameter that enters A only through CXADIA at site j
 // (A^T = A, so lam = A^-1 s is the adjoint solution).  FP64 accumulation.
-__global__ void k_adjoint_grad(int n, int nat0, const C* lam, const C* dad, const C* p, const int* occ, C* g,
-                               size_t g_rs) {
+// grad[r][occ[q]] = -sum_c lam_r[c][q] dad_r[c][q] p_r[c][q]; the per-RHS
+// strides of dad and p may be 0 (one forward solution / derivative shared by
+// every adjoint source)
+__global__ void k_adjoint_grad(int n, int nat0, const C* lam, const C* dad, size_t dad_rs, const C* p, size_t p_rs,
+                               const int* occ, C* g, size_t g_rs) {
   const int r = blockIdx.y;
-  const size_t off = (size_t)r * n;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nat0; q += gridDim.x * blockDim.x) {
     double gr = 0.0, gi = 0.0;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const size_t i = off + (size_t)c * nat0 + q;
-      const double2 l = to_d(lam[i]), d = to_d(dad[i]), v = to_d(p[i]);
+      const size_t i = (size_t)c * nat0 + q;
+      const double2 l = to_d(lam[(size_t)r * n + i]), d = to_d(dad[(size_t)r * dad_rs + i]),
+                    v = to_d(p[(size_t)r * p_rs + i]);
       const double tr = l.x * d.x - l.y * d.y, ti = l.x * d.y + l.y * d.x;
       gr -= tr * v.x - ti * v.y;
       gi -= tr * v.y + ti * v.x;
@@ -434,9 +473,11 @@ __global__ void k_adjoint_grad(int n, int nat0, const C* lam, const C* dad, cons
 // The prepared FP32 engine, or null before a successful prepare (read-only
 // access for entry points defined in other translation units).
 const Engine<float>* prepared_engine() { return s.ready ? &s.eng : nullptr; }
+// The device the prepared state lives on (-1 before a successful prepare).
+int prepared_device() { return s.ready ? s.device : -1; }
 
-int make_inputs(const Engine<float>& eng, int nrhs, const float* k, const float2* e0, const float* x0, int nmat,
-                const float2* mref, const int16_t* icomp_host, float2* b, float2* adia, cudaStream_t st);
+int make_inputs(const Engine<float>& eng, int cmdpol, int nrhs, const float* k, const float2* e0, const float* x0,
+                int nmat, const float2* mref, const int16_t* icomp_host, float2* b, float2* adia, cudaStream_t st);
 
 }  // namespace ddb
 
@@ -462,7 +503,6 @@ DDSCAT_CUDA_API int ddscat_cuda_prepare_green_f32(int nx, int ny, int nz, int ip
     return 201;
   }
   if (ipbc && gamma <= 0.f) { set_error("prepare_green", "GAMMA must be >0 for PBC"); return 202; }
-  if (!s.verbose) s.verbose = env_verbose();
   release_state();
   int rc = s.eng.init_geometry(nx, ny, nz, ipbc, nat, nat0, iocc, true);
   if (rc) { release_state(); return rc == 2 ? 208 : 204; }
@@ -478,6 +518,7 @@ DDSCAT_CUDA_API int ddscat_cuda_prepare_green_f32(int nx, int ny, int nz, int ip
   s.green_args = ga;
   s.h_iocc = new int16_t[nat];
   std::memcpy(s.h_iocc, iocc, (size_t)nat * sizeof(int16_t));
+  cudaGetDevice(&s.device);
   s.ready = true;
   return 0;
 }
@@ -490,7 +531,6 @@ DDSCAT_CUDA_API int ddscat_cuda_prepare_f32(int nx, int ny, int nz, int ipbc, in
     set_error("prepare", "invalid argument");
     return 1;
   }
-  if (!s.verbose) s.verbose = env_verbose();
   release_state();
   int rc = s.eng.init_geometry(nx, ny, nz, ipbc, nat, nat0, iocc);
   if (rc) { release_state(); return rc == 2 ? 6 : 2; }
@@ -500,6 +540,7 @@ DDSCAT_CUDA_API int ddscat_cuda_prepare_f32(int nx, int ny, int nz, int ipbc, in
   s.cpu_green.assign((const float2*)green, (const float2*)green + s.eng.g.green_count());
   s.h_iocc = new int16_t[nat];
   std::memcpy(s.h_iocc, iocc, (size_t)nat * sizeof(int16_t));
+  cudaGetDevice(&s.device);
   s.ready = true;
   return 0;
 }
@@ -519,11 +560,24 @@ DDSCAT_CUDA_API int ddscat_cuda_apply_f32(int cwhat, const void* x, void* y, con
   a.x = s.d_xf; a.y = s.d_yf; a.io_full = 1;
   a.adia = s.d_adia; a.aoff = s.aoff_zero ? nullptr : s.d_aoff; a.a_full = 1;
   a.conj = (cwhat == 'C'); a.nrhs = 1;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  const bool timed = verbose_level() >= 1 && cudaEventCreate(&ev[0]) == cudaSuccess &&
+                     cudaEventCreate(&ev[1]) == cudaSuccess;
+  if (timed) cudaEventRecord(ev[0], s.stream);
   int rc = s.eng.matvec(a);
-  if (rc) return rc;
-  e = cudaMemcpy(y, s.d_yf, b, cudaMemcpyDeviceToHost);
-  if (e != cudaSuccess) { set_cuda_error("y D2H", e); return 15; }
-  return 0;
+  if (timed) cudaEventRecord(ev[1], s.stream);
+  if (!rc) {
+    e = cudaMemcpy(y, s.d_yf, b, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) { set_cuda_error("y D2H", e); rc = 15; }
+  }
+  if (timed) {
+    float ms = 0.f;
+    if (!rc && cudaEventElapsedTime(&ms, ev[0], ev[1]) == cudaSuccess) report_matvec_line(cwhat, "host-copy", ms);
+  }
+  if (ev[0]) cudaEventDestroy(ev[0]);
+  if (ev[1]) cudaEventDestroy(ev[1]);
+  cudaGetLastError();  // a failed event creation leaves no sticky error behind
+  return rc;
 }
 
 #define SOLVER_ENTRY(fname, fn, nm, inv, ws, h2d, d2h, pub)                                                          \
@@ -613,24 +667,7 @@ DDSCAT_CUDA_API int ddscat_cuda_scat_f32(int jpbc, int ndir, const float* ak, co
     std::vector<double2> sums((size_t)3 * nd);
     int rc = farfield_sums<float>(s.eng, s.d_sx, hd.data(), nd, dx, x0, sums.data(), s.stream);
     if (rc) return rc;
-    double acc[5] = {0, 0, 0, 0, 0}, back = 0.0;
-    for (int i = 0; i < nd; ++i) {
-      const double nx = hd[3 * i] / akk, ny = hd[3 * i + 1] / akk, nz = hd[3 * i + 2] / akk;
-      const double2 sx = sums[3 * i], sy = sums[3 * i + 1], sz = sums[3 * i + 2];
-      const double ndr = nx * sx.x + ny * sy.x + nz * sz.x, ndi = nx * sx.y + ny * sy.y + nz * sz.y;
-      const double exr = sx.x - nx * ndr, exi = sx.y - nx * ndi, eyr = sy.x - ny * ndr, eyi = sy.y - ny * ndi;
-      const double ezr = sz.x - nz * ndr, ezi = sz.y - nz * ndi;
-      const double es2 = exr * exr + exi * exi + eyr * eyr + eyi * eyi + ezr * ezr + ezi * ezi;
-      for (int k = 0; k < 5; ++k) acc[k] += es2 * idirs[i].w[k];
-      if (i == nd - 1) back = es2;
-    }
-    const double fac = ak2 * ak2 / (double)e02;
-    *csca = fac * acc[0];
-    cscag[0] = fac * acc[1];
-    cscag[1] = fac * acc[2];
-    cscag[2] = fac * acc[3];
-    *cscag2 = fac * acc[4];
-    *cbksca = fac * back;
+    scat_integrate(idirs, sums.data(), ak2, (double)e02, cbksca, csca, cscag, cscag2);
   }
   if (ndir > 0) {
     std::vector<double2> sums((size_t)3 * ndir);
@@ -654,7 +691,7 @@ DDSCAT_CUDA_API int ddscat_cuda_scat_f32(int jpbc, int ndir, const float* ak, co
 
 // ---- library extensions (declared in ddscat_b200.h) ----
 DDSCAT_CUDA_API int ddscat_b200_set_verbose(int level) {
-  s.verbose = level;
+  g_verbose = level < 0 ? -1 : (level > 2 ? 2 : level);
   return 0;
 }
 
@@ -700,7 +737,7 @@ DDSCAT_CUDA_API int ddscat_b200_solve_batch_f32(int solver, int nrhs, const void
   io.eng = &s.eng; io.ops = &bs.ops; io.R = nrhs; io.n = bs.n;
   io.b = bs.b; io.x = bs.x; io.adia = bs.adia; io.aoff = use_aoff ? bs.aoff : nullptr;
   io.work = bs.work; io.nwork = BATCH_WORK_VECTORS;
-  io.maxit = maxit; io.tol = (double)tol; io.verbose = s.verbose; io.replace = replace; io.sym = sym;
+  io.maxit = maxit; io.tol = (double)tol; io.verbose = verbose_level() >= 2; io.replace = replace; io.sym = sym;
   io.graph = graph;
   BatchResult res;
   const int rc = solver == DDSCAT_B200_QMRCCG ? solve_batch_qmrccg<float>(io, res) : solve_batch_pbcgs2<float>(io, res);
@@ -921,9 +958,62 @@ extern "C" DDSCAT_CUDA_API int ddscat_b200_scat_amplitudes_f64(int nrhs, const v
   return rc;
 }
 
-extern "C" DDSCAT_CUDA_API int ddscat_b200_make_inputs_f32(int nrhs, const float* k, const void* e0, const float* x0,
-                                                           int nmat, const void* m, const int16_t* icomp, void* b,
-                                                           void* adia) {
+extern "C" DDSCAT_CUDA_API int ddscat_b200_scat_csca_f64(int nrhs, const void* x, const float* ak, const void* e01,
+                                                        float etasca, const float* dx, const float* x0, float e02,
+                                                        double* cbksca, double* csca, double* cscag,
+                                                        double* cscag2, int* navg) {
+  clear_error();
+  if (!s.ready || nrhs <= 0 || !x || !ak || !e01 || !(etasca > 0.f) || !dx || !x0 || !(e02 > 0.f) || !cbksca ||
+      !csca || !cscag || !cscag2 || !navg) {
+    set_error("FP64 SCAT", "invalid argument or not prepared");
+    return 710;
+  }
+  const Geometry& g = s.eng.g;
+  const size_t full = (size_t)3 * g.nat, cn = (size_t)3 * g.nat0;
+  const bool dev = is_device_ptr(x);
+  double2 *d_full = nullptr, *d_p = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (!dev) e = cudaMalloc((void**)&d_full, full * sizeof(double2));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&d_p, cn * sizeof(double2));
+  if (e != cudaSuccess) {
+    cudaFree(d_full);
+    set_cuda_error("FP64 SCAT workspace", e);
+    return 711;
+  }
+  const double ak2 = (double)ak[0] * ak[0] + (double)ak[1] * ak[1] + (double)ak[2] * ak[2];
+  const double dxd[3] = {dx[0], dx[1], dx[2]}, x0d[3] = {x0[0], x0[1], x0[2]};
+  int rc = 0;
+  for (int r = 0; r < nrhs && !rc; ++r) {
+    std::vector<IntDir> idirs;
+    if (make_integration_dirs(ak, static_cast<const C*>(e01) + 3 * r, etasca, g.nat0, idirs)) { rc = 710; break; }
+    const int nd = (int)idirs.size();
+    navg[r] = nd;
+    std::vector<double> hd((size_t)3 * nd);
+    for (int i = 0; i < nd; ++i)
+      for (int k = 0; k < 3; ++k) hd[3 * i + k] = (double)idirs[i].k[k];
+    const double2* src = static_cast<const double2*>(x) + (size_t)r * full;
+    if (!dev) {
+      e = cudaMemcpyAsync(d_full, src, full * sizeof(double2), cudaMemcpyHostToDevice, s.stream);
+      if (e != cudaSuccess) { set_cuda_error("FP64 SCAT H2D", e); rc = 711; break; }
+      src = d_full;
+    }
+    v_gather<double>(src, d_p, s.eng.occ, g.nat, g.nat0, s.stream);
+    if (check_launch("FP64 SCAT gather")) { rc = 712; break; }
+    std::vector<double2> sums((size_t)3 * nd);
+    if (farfield_sums_f64(s.eng.occ, g.nx, g.ny, g.nz, g.nat0, d_p, hd.data(), nd, dxd, x0d, sums.data(),
+                          s.stream)) {
+      rc = 712;
+      break;
+    }
+    scat_integrate(idirs, sums.data(), ak2, (double)e02, cbksca + r, csca + r, cscag + 3 * r, cscag2 + r);
+  }
+  cudaFree(d_full);
+  cudaFree(d_p);
+  return rc;
+}
+
+static int make_inputs_entry(int cmdpol, int nrhs, const float* k, const void* e0, const float* x0, int nmat,
+                             const void* m, const int16_t* icomp, void* b, void* adia) {
   clear_error();
   if (!s.ready || nrhs <= 0 || nmat <= 0 || !k || !e0 || !x0 || !m || (!b && !adia)) {
     set_error("make_inputs", "invalid argument or not prepared");
@@ -944,8 +1034,8 @@ extern "C" DDSCAT_CUDA_API int ddscat_b200_make_inputs_f32(int nrhs, const float
     db = b ? tmp : nullptr;
     da = adia ? tmp + (b ? per : 0) : nullptr;
   }
-  int rc = make_inputs(s.eng, nrhs, k, static_cast<const float2*>(e0), x0, nmat, static_cast<const float2*>(m),
-                       icomp, db, da, s.stream);
+  int rc = make_inputs(s.eng, cmdpol, nrhs, k, static_cast<const float2*>(e0), x0, nmat,
+                       static_cast<const float2*>(m), icomp, db, da, s.stream);
   if (!rc && !dev) {
     const size_t bytes = (size_t)nrhs * full * sizeof(float2);
     cudaError_t e = cudaSuccess;
@@ -955,6 +1045,18 @@ extern "C" DDSCAT_CUDA_API int ddscat_b200_make_inputs_f32(int nrhs, const float
   }
   cudaFree(tmp);
   return rc;
+}
+
+extern "C" DDSCAT_CUDA_API int ddscat_b200_make_inputs_f32(int nrhs, const float* k, const void* e0, const float* x0,
+                                                           int nmat, const void* m, const int16_t* icomp, void* b,
+                                                           void* adia) {
+  return make_inputs_entry(DDSCAT_B200_LATTDR, nrhs, k, e0, x0, nmat, m, icomp, b, adia);
+}
+
+extern "C" DDSCAT_CUDA_API int ddscat_b200_make_inputs_pol_f32(int cmdpol, int nrhs, const float* k, const void* e0,
+                                                               const float* x0, int nmat, const void* m,
+                                                               const int16_t* icomp, void* b, void* adia) {
+  return make_inputs_entry(cmdpol, nrhs, k, e0, x0, nmat, m, icomp, b, adia);
 }
 
 extern "C" DDSCAT_CUDA_API int ddscat_b200_solve_batch_f64(int solver, int nrhs, const void* b, void* x,
@@ -1012,7 +1114,7 @@ extern "C" DDSCAT_CUDA_API int ddscat_b200_solve_batch_f64(int solver, int nrhs,
   io.eng = &f64.eng; io.ops = &b64.ops; io.R = nrhs; io.n = b64.n;
   io.b = b64.b; io.x = b64.x; io.adia = b64.adia; io.aoff = aoff ? b64.aoff : nullptr;
   io.work = b64.work; io.nwork = BATCH_WORK_VECTORS;
-  io.maxit = maxit; io.tol = tol; io.verbose = s.verbose; io.replace = replace; io.sym = sym;
+  io.maxit = maxit; io.tol = tol; io.verbose = verbose_level() >= 2; io.replace = replace; io.sym = sym;
   BatchResult res;
   const int rc = solver == DDSCAT_B200_QMRCCG ? solve_batch_qmrccg<double>(io, res) : solve_batch_pbcgs2<double>(io, res);
   if (rc) return rc == 1 ? 525 : rc;
@@ -1074,7 +1176,7 @@ extern "C" DDSCAT_CUDA_API int ddscat_b200_adjoint_f32(int nrhs, const void* p, 
   io.eng = &s.eng; io.ops = &bs.ops; io.R = nrhs; io.n = bs.n;
   io.b = bs.b; io.x = bs.x; io.adia = bs.adia; io.aoff = nullptr;
   io.work = bs.work; io.nwork = BATCH_WORK_VECTORS - 2;
-  io.maxit = maxit; io.tol = (double)tol; io.verbose = s.verbose; io.replace = 1; io.sym = 1;
+  io.maxit = maxit; io.tol = (double)tol; io.verbose = verbose_level() >= 2; io.replace = 1; io.sym = 1;
   BatchResult res;
   const int rc = solve_batch_qmrccg<float>(io, res);
   if (rc) return rc == 1 ? 534 : rc;
@@ -1109,8 +1211,8 @@ extern "C" DDSCAT_CUDA_API int ddscat_b200_adjoint_f32(int nrhs, const void* p, 
     e = cudaMemsetAsync(gd + (dev ? 0 : 0), 0, (size_t)nr * nat * sizeof(C), s.stream);
     if (e != cudaSuccess) { set_cuda_error("adjoint", e); return 535; }
     k_adjoint_grad<<<dim3(gx, (unsigned)nr), 256, 0, s.stream>>>(bs.n, s.eng.g.nat0, bs.x + (size_t)r0 * bs.n,
-                                                                 dc + (size_t)r0 * bs.n, pc + (size_t)r0 * bs.n,
-                                                                 s.eng.occ, gd, nat);
+                                                                 dc + (size_t)r0 * bs.n, bs.n, pc + (size_t)r0 * bs.n,
+                                                                 bs.n, s.eng.occ, gd, nat);
     note_launch();
     if (check_launch("adjoint gradient")) return 535;
     if (!dev) {
@@ -1136,4 +1238,150 @@ extern "C" DDSCAT_CUDA_API int ddscat_b200_adjoint_f32(int nrhs, const void* p, 
   e = cudaStreamSynchronize(s.stream);
   if (e != cudaSuccess) { set_cuda_error("adjoint", e); return 535; }
   return 0;
+}
+
+// ---- adjoint gradient with the forward field recomputed (library extension) ----
+extern "C" DDSCAT_CUDA_API int ddscat_b200_adjoint_fwd_f32(int nsrc, const void* e, const void* src,
+                                                           const void* adia, const void* dadia, int maxit, float tol,
+                                                           void* grad, void* p, int* itno, float* tole) {
+  clear_error();
+  if (!s.ready || nsrc <= 0 || !e || !src || !adia || !dadia || !grad || maxit <= 0 || !(tol > 0.f) || !itno ||
+      !tole) {
+    set_error("adjoint (forward recomputed)", "invalid argument or not prepared");
+    return 530;
+  }
+  const bool dev = is_device_ptr(e);
+  if (is_device_ptr(src) != dev || is_device_ptr(adia) != dev || is_device_ptr(dadia) != dev ||
+      is_device_ptr(grad) != dev || (p && is_device_ptr(p) != dev)) {
+    set_error("adjoint (forward recomputed)", "all arrays must be host or all device pointers");
+    return 531;
+  }
+  const int R = nsrc + 1;  // slot 0: the forward system A P = E; slots 1..nsrc: A lam_k = s_k
+  if (ensure_batch(R)) return 532;
+  const size_t full = (size_t)3 * s.eng.g.nat, nat = (size_t)s.eng.g.nat;
+  C* dc = bs.aoff;  // compact dCXADIA (one vector, shared by every source)
+  if (to_compact(e, dev, 0, bs.b) || to_compact(adia, dev, 0, bs.adia) || to_compact(dadia, dev, 0, dc)) return 533;
+  for (int k = 0; k < nsrc; ++k)
+    if (to_compact(src, dev, k, bs.b + bs.n)) return 533;
+  cudaError_t ce = cudaSuccess;
+  for (int r = 1; r < R && ce == cudaSuccess; ++r)
+    ce = cudaMemcpyAsync(bs.adia + (size_t)r * bs.n, bs.adia, (size_t)bs.n * sizeof(C), cudaMemcpyDeviceToDevice,
+                         s.stream);
+  if (ce == cudaSuccess) ce = cudaMemsetAsync(bs.x, 0, (size_t)R * bs.n * sizeof(C), s.stream);
+  if (ce != cudaSuccess) { set_cuda_error("adjoint (forward recomputed)", ce); return 533; }
+  // the forward and the adjoint systems share the operator: one batched
+  // one-MATVEC QMRCCG solve with residual replacement over all of them
+  BatchIO<float> io;
+  io.eng = &s.eng; io.ops = &bs.ops; io.R = R; io.n = bs.n;
+  io.b = bs.b; io.x = bs.x; io.adia = bs.adia; io.aoff = nullptr;
+  io.work = bs.work; io.nwork = BATCH_WORK_VECTORS;
+  io.maxit = maxit; io.tol = (double)tol; io.verbose = verbose_level() >= 2; io.replace = 1; io.sym = 1;
+  BatchResult res;
+  const int rc = solve_batch_qmrccg<float>(io, res);
+  if (rc) return rc == 1 ? 534 : rc;
+  for (int r = 0; r < R; ++r) {
+    itno[r] = res.itno[r];
+    tole[r] = (float)res.tole[r];
+    if (res.status[r]) {
+      set_error("adjoint (forward recomputed)", "a forward or adjoint solve broke down");
+      return res.status[r];
+    }
+  }
+  // gradient per site and source (zero on vacuum)
+  C* gd = dev ? static_cast<C*>(grad) : s.d_xf;  // host: stage up to 3 sources in the full-vector buffer
+  const unsigned gx = (unsigned)std::min<size_t>(ceil_div((size_t)s.eng.g.nat0, 256), 1184);
+  for (int k0 = 0; k0 < nsrc; k0 += dev ? nsrc : 3) {
+    const int nk = dev ? nsrc : std::min(3, nsrc - k0);
+    ce = cudaMemsetAsync(gd, 0, (size_t)nk * nat * sizeof(C), s.stream);
+    if (ce != cudaSuccess) { set_cuda_error("adjoint (forward recomputed)", ce); return 535; }
+    k_adjoint_grad<<<dim3(gx, (unsigned)nk), 256, 0, s.stream>>>(bs.n, s.eng.g.nat0, bs.x + (size_t)(1 + k0) * bs.n,
+                                                                 dc, 0, bs.x, 0, s.eng.occ, gd, nat);
+    note_launch();
+    if (check_launch("adjoint gradient")) return 535;
+    if (!dev) {
+      ce = cudaMemcpyAsync((C*)grad + (size_t)k0 * nat, gd, (size_t)nk * nat * sizeof(C), cudaMemcpyDeviceToHost,
+                           s.stream);
+      if (ce == cudaSuccess) ce = cudaStreamSynchronize(s.stream);
+      if (ce != cudaSuccess) { set_cuda_error("adjoint D2H", ce); return 535; }
+    }
+  }
+  if (p) {  // the forward solution, full layout
+    C* dst = dev ? static_cast<C*>(p) : s.d_xf;
+    ce = cudaMemsetAsync(dst, 0, full * sizeof(C), s.stream);
+    if (ce != cudaSuccess) { set_cuda_error("adjoint (forward recomputed)", ce); return 535; }
+    v_scatter<float>(bs.x, dst, s.eng.occ, s.eng.g.nat, s.eng.g.nat0, s.stream);
+    if (check_launch("adjoint scatter")) return 535;
+    if (!dev) {
+      ce = cudaMemcpyAsync(p, s.d_xf, full * sizeof(C), cudaMemcpyDeviceToHost, s.stream);
+      if (ce != cudaSuccess) { set_cuda_error("adjoint D2H", ce); return 535; }
+    }
+  }
+  ce = cudaStreamSynchronize(s.stream);
+  if (ce != cudaSuccess) { set_cuda_error("adjoint (forward recomputed)", ce); return 535; }
+  return 0;
+}
+
+// far-field weights: w_k[c][j] = |aks_k|^3 / sqrt(E02) em_k[c] exp(-i aks_k . r_j) on occupied sites
+__global__ void k_ffweights(int nw, int nx, int ny, int nat, const double* aks, const double* em, double x00,
+                            double x01, double x02, double term_scale, const int16_t* iocc, C* out) {
+  const int k = blockIdx.y;
+  const double kx = aks[3 * k], ky = aks[3 * k + 1], kz = aks[3 * k + 2];
+  const double kk = sqrt(kx * kx + ky * ky + kz * kz), term = kk * kk * kk * term_scale;
+  const double e0 = em[3 * k] * term, e1 = em[3 * k + 1] * term, e2 = em[3 * k + 2] * term;
+  C* w = out + (size_t)k * 3 * nat;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nat; j += gridDim.x * blockDim.x) {
+    C a = make_float2(0.f, 0.f), b = a, c = a;
+    if (iocc[j]) {
+      const int ix = j % nx, iy = (j / nx) % ny, iz = j / (nx * ny);
+      const double ph = -(kx * (ix + 1 + x00) + ky * (iy + 1 + x01) + kz * (iz + 1 + x02));
+      double sn, cs;
+      sincos(ph, &sn, &cs);
+      a = make_float2((float)(e0 * cs), (float)(e0 * sn));
+      b = make_float2((float)(e1 * cs), (float)(e1 * sn));
+      c = make_float2((float)(e2 * cs), (float)(e2 * sn));
+    }
+    w[j] = a;
+    w[(size_t)nat + j] = b;
+    w[2 * (size_t)nat + j] = c;
+  }
+}
+
+extern "C" DDSCAT_CUDA_API int ddscat_b200_ffweights_f32(int nw, const double* aks, const double* em,
+                                                         const double* x0, double e02, void* w) {
+  clear_error();
+  if (!s.ready || nw <= 0 || !aks || !em || !x0 || !(e02 > 0.0) || !w) {
+    set_error("far-field weights", "invalid argument or not prepared");
+    return 720;
+  }
+  const Geometry& g = s.eng.g;
+  const bool dev = is_device_ptr(w);
+  const size_t full = (size_t)3 * g.nat;
+  double* d_par = nullptr;
+  C* d_w = dev ? static_cast<C*>(w) : nullptr;
+  cudaError_t ce = cudaMalloc((void**)&d_par, (size_t)6 * nw * sizeof(double));
+  if (ce == cudaSuccess && !dev) ce = cudaMalloc((void**)&d_w, (size_t)nw * full * sizeof(C));
+  if (ce == cudaSuccess) ce = cudaMemcpyAsync(d_par, aks, (size_t)3 * nw * sizeof(double), cudaMemcpyHostToDevice,
+                                              s.stream);
+  if (ce == cudaSuccess) ce = cudaMemcpyAsync(d_par + 3 * (size_t)nw, em, (size_t)3 * nw * sizeof(double),
+                                              cudaMemcpyHostToDevice, s.stream);
+  int rc = 0;
+  if (ce != cudaSuccess) {
+    set_cuda_error("far-field weights", ce);
+    rc = 721;
+  } else {
+    const unsigned gx = (unsigned)std::min<size_t>(ceil_div((size_t)g.nat, 256), std::max(1, 2368 / nw));
+    k_ffweights<<<dim3(gx, (unsigned)nw), 256, 0, s.stream>>>(nw, g.nx, g.ny, g.nat, d_par, d_par + 3 * (size_t)nw,
+                                                              x0[0], x0[1], x0[2], 1.0 / std::sqrt(e02),
+                                                              s.eng.iocc, d_w);
+    note_launch();
+    if (check_launch("far-field weights")) rc = 722;
+    if (!rc && !dev) {
+      ce = cudaMemcpyAsync(w, d_w, (size_t)nw * full * sizeof(C), cudaMemcpyDeviceToHost, s.stream);
+      if (ce != cudaSuccess) { set_cuda_error("far-field weights D2H", ce); rc = 721; }
+    }
+    if (!rc && (ce = cudaStreamSynchronize(s.stream)) != cudaSuccess) { set_cuda_error("far-field weights", ce); rc = 722; }
+  }
+  cudaFree(d_par);
+  if (!dev) cudaFree(d_w);
+  return rc;
 }

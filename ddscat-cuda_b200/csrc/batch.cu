@@ -701,7 +701,7 @@ static int qmr_graph_loop(BatchIO<T>& io, BatchOps<T>& ops, std::vector<int>& nc
     hi0[i] = it[i]; hi0[R + i] = live[i]; hi0[2 * R + i] = status[i]; hi0[3 * R + i] = nc[i];
   }
   // phase stamps of the iterations (verbose only)
-  const bool verbose = std::getenv("DDSCAT_B200_VERBOSE") != nullptr;
+  const bool verbose = verbose_level() >= 2;
   const int scap = io.maxit + 64;
   unsigned long long* stamps = nullptr;
   if (verbose && cudaMalloc((void**)&stamps, (size_t)(8 * scap + 1) * sizeof(unsigned long long)) != cudaSuccess)

@@ -26,6 +26,8 @@ void set_cuda_error(const char* where, cudaError_t e);
 const char* last_error_text();
 void clear_error();
 int check_launch(const char* where);
+// console output level of the library (0 silent, 1 reference-style lines, 2 diagnostics)
+int verbose_level();
 void raise_smem_limit(const void* f);  // thread-safe, once per kernel
 unsigned long long launch_total();     // kernels launched so far (note_launch counter)
 // count of kernels this library launched (reported by ddscat_b200_launch_count)

@@ -6,16 +6,23 @@
 // polarisation e_r, and each lattice site j = ix + nx*(iy + ny*iz):
 //   b[r][c][j]    = e_r[c] exp(i k_r . r_j) on occupied sites, 0 on vacuum,
 //                   r_j = (ix+1, iy+1, iz+1) + x0 (the SCAT convention, cu:805)
-//   adia[r][c][j] = 1/alpha_LDR(m of the site's material, |k_r|, khat_r, e_r)
-// with the lattice-dispersion-relation polarisability of Draine & Goodman
-// (1993, ApJ 405, 685): alpha = alpha_CM / (1 + alpha_CM [(b1 + m^2 b2 +
-// m^2 b3 S)(kd)^2 - (2/3) i (kd)^3]), alpha_CM = (3/4pi)(m^2-1)/(m^2+2),
-// S = sum_a (khat_a Re e_a)^2, b1 = -1.891531, b2 = 0.1648469, b3 = -1.7700004.
-// The 1/alpha table (nrhs x materials) is computed in FP64 on the host; the
-// phases are evaluated in FP64 on the GPU.
+//   adia[r][c][j] = 1/alpha_c(m of the site's material, |k_r|, khat_r, e_r)
+// with one of DDSCAT's polarisability prescriptions (CMDPOL), lattice units
+// d = 1, 1/alpha_CM = (4pi/3)(m^2+2)/(m^2-1):
+//   LATTDR (Draine & Goodman 1993, ApJ 405, 685): 1/alpha = 1/alpha_CM +
+//     (b1 + m^2 b2 + m^2 b3 S)(kd)^2 - (2/3) i (kd)^3, S = sum_a (khat_a Re e_a)^2,
+//     b1 = -1.891531, b2 = 0.1648469, b3 = -1.7700004, the same for c = 1..3;
+//   GKDLDR (Gutkowicz-Krusin & Draine 2004): the same with S replaced by
+//     khat_c^2 for component c (independent of the polarisation);
+//   FLTRCD (filtered coupled dipoles; Piller & Martin 1998, Gay-Balmaz &
+//     Martin 2002): 1/alpha = 1/alpha_CM - (4/3)(kd)^2
+//     - (2/(3 pi)) ln((pi - kd)/(pi + kd)) (kd)^3 - (2/3) i (kd)^3, kd < pi.
+// The 1/alpha table (nrhs x materials x 3 components) is computed in FP64 on
+// the host; the phases are evaluated in FP64 on the GPU.
 #include <cmath>
 #include <complex>
 #include <vector>
+#include "ddscat_b200.h"
 #include "engine.h"
 
 namespace ddb {
@@ -47,35 +54,48 @@ __global__ void k_make_inputs(int nx, int ny, int nat, int nrhs, const double* k
     }
     if (ar) {
       const int mat = (occ && icomp) ? icomp[j] : 1;
-      const float2 a = adtab[(size_t)r * nmat1 + mat];
-      ar[j] = a;
-      ar[(size_t)nat + j] = a;
-      ar[2 * (size_t)nat + j] = a;
+      const float2* a = adtab + ((size_t)r * nmat1 + mat) * 3;
+      ar[j] = a[0];
+      ar[(size_t)nat + j] = a[1];
+      ar[2 * (size_t)nat + j] = a[2];
     }
   }
 }
 
-// host: 1/alpha_LDR per (rhs, material); material 0 is unused (vacuum)
-static std::complex<double> inv_alpha_ldr(std::complex<double> m, double kd, const double* khat,
-                                          const std::complex<double>* e) {
+// host: 1/alpha per Cartesian component c for one (rhs, material); material 0
+// is unused (vacuum).  Returns false for FLTRCD with kd >= pi.
+static bool inv_alpha(int cmdpol, std::complex<double> m, double kd, const double* khat,
+                      const std::complex<double>* e, std::complex<double> out[3]) {
   const double b1 = -1.891531, b2 = 0.1648469, b3 = -1.7700004;
   const double pi = 3.14159265358979323846;
   const std::complex<double> eps = m * m;
-  const std::complex<double> acm = (3.0 / (4.0 * pi)) * (eps - 1.0) / (eps + 2.0);
+  const std::complex<double> base =
+      (4.0 * pi / 3.0) * (eps + 2.0) / (eps - 1.0) - std::complex<double>(0.0, 2.0 / 3.0) * kd * kd * kd;
+  if (cmdpol == DDSCAT_B200_FLTRCD) {
+    if (!(kd < pi)) return false;
+    const double corr = -(4.0 / 3.0) * kd * kd - (2.0 / (3.0 * pi)) * std::log((pi - kd) / (pi + kd)) * kd * kd * kd;
+    for (int c = 0; c < 3; ++c) out[c] = base + corr;
+    return true;
+  }
   double S = 0.0;
   for (int a = 0; a < 3; ++a) S += (khat[a] * e[a].real()) * (khat[a] * e[a].real());
-  const std::complex<double> corr =
-      (b1 + eps * b2 + eps * b3 * S) * kd * kd - std::complex<double>(0.0, 2.0 / 3.0) * kd * kd * kd;
-  const std::complex<double> alpha = acm / (1.0 + acm * corr);
-  return 1.0 / alpha;
+  for (int c = 0; c < 3; ++c) {
+    const double Sc = cmdpol == DDSCAT_B200_GKDLDR ? khat[c] * khat[c] : S;
+    out[c] = base + (b1 + eps * b2 + eps * b3 * Sc) * kd * kd;
+  }
+  return true;
 }
 
-int make_inputs(const Engine<float>& eng, int nrhs, const float* k, const float2* e0, const float* x0, int nmat,
-                const float2* mref, const int16_t* icomp_host, float2* b, float2* adia, cudaStream_t st) {
+int make_inputs(const Engine<float>& eng, int cmdpol, int nrhs, const float* k, const float2* e0, const float* x0,
+                int nmat, const float2* mref, const int16_t* icomp_host, float2* b, float2* adia, cudaStream_t st) {
   const Geometry& g = eng.g;
+  if (cmdpol != DDSCAT_B200_LATTDR && cmdpol != DDSCAT_B200_GKDLDR && cmdpol != DDSCAT_B200_FLTRCD) {
+    set_error("make_inputs", "unknown polarisability prescription (LATTDR=0, GKDLDR=1, FLTRCD=2)");
+    return 610;
+  }
   std::vector<double> kv((size_t)3 * nrhs);
   std::vector<double2> ev((size_t)3 * nrhs);
-  std::vector<float2> tab((size_t)nrhs * (nmat + 1), make_float2(0.f, 0.f));
+  std::vector<float2> tab((size_t)nrhs * (nmat + 1) * 3, make_float2(0.f, 0.f));
   for (int r = 0; r < nrhs; ++r) {
     double kh[3], kk = 0.0;
     std::complex<double> e[3];
@@ -89,9 +109,13 @@ int make_inputs(const Engine<float>& eng, int nrhs, const float* k, const float2
     if (!(kk > 0.0)) { set_error("make_inputs", "zero wave vector"); return 610; }
     for (int a = 0; a < 3; ++a) kh[a] = kv[3 * r + a] / kk;
     for (int mi = 1; mi <= nmat; ++mi) {
-      const std::complex<double> ia =
-          inv_alpha_ldr(std::complex<double>(mref[mi - 1].x, mref[mi - 1].y), kk, kh, e);
-      tab[(size_t)r * (nmat + 1) + mi] = make_float2((float)ia.real(), (float)ia.imag());
+      std::complex<double> ia[3];
+      if (!inv_alpha(cmdpol, std::complex<double>(mref[mi - 1].x, mref[mi - 1].y), kk, kh, e, ia)) {
+        set_error("make_inputs", "FLTRCD needs |k| d < pi");
+        return 610;
+      }
+      for (int c = 0; c < 3; ++c)
+        tab[((size_t)r * (nmat + 1) + mi) * 3 + c] = make_float2((float)ia[c].real(), (float)ia[c].imag());
     }
   }
   if (icomp_host) {

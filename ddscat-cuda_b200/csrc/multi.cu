@@ -46,7 +46,7 @@ int multi_solve(int nt, const int* dims, const int16_t* const* iocc, const float
                 const void* const* b, void* const* x, const void* const* adia, int solver, int replace, int sym,
                 int autotune, int graph, int maxit, float tol, int nthreads, int* itno, float* tole, int* ncompte,
                 int* status) {
-  const bool verbose = std::getenv("DDSCAT_B200_VERBOSE") != nullptr;
+  const bool verbose = verbose_level() >= 2;
   auto now = []() { return std::chrono::steady_clock::now(); };
   const auto t0 = now();
   std::vector<Target> T(nt);

@@ -9,11 +9,42 @@
 // and the same error codes.  Scalars are combined on the host from the
 // device-reduced inner products (one small D2H per product, no full-vector
 // transfers inside the loops).
+#include <chrono>
 #include <complex>
 #include "engine.h"
 #include "solvers.h"
 
 namespace ddb {
+
+// Console line per MATVEC of the reference entry points (the reference's
+// report_matvec, cu:417): a running count, CWHAT, the solver, the GPU time of
+// the MATVEC (CUDA events, waited for) and the wall time since the previous
+// MATVEC ended, minus the previous line's own printing time.
+struct MatvecReport {
+  unsigned long long count = 0;
+  bool have_prev = false;
+  std::chrono::steady_clock::time_point prev_end;
+  double last_print_ms = 0.0;
+  void line(char cw, const char* path, float gpu_ms) {
+    ++count;
+    const auto now = std::chrono::steady_clock::now();
+    const auto p0 = now;
+    if (have_prev) {
+      double dt = std::chrono::duration<double, std::milli>(now - prev_end).count() - last_print_ms;
+      if (dt < 0) dt = 0;
+      std::printf("CUDA MATVEC %llu [%c,%s]: GPU=%.6f ms  prev_end->end=%.6f ms  outside=%.6f ms\n", count, cw, path,
+                  (double)gpu_ms, dt, dt - gpu_ms);
+    } else {
+      std::printf("CUDA MATVEC %llu [%c,%s]: GPU=%.6f ms  prev_end->end=N/A\n", count, cw, path, (double)gpu_ms);
+    }
+    std::fflush(stdout);
+    last_print_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - p0).count();
+    prev_end = now;
+    have_prev = true;
+  }
+};
+static MatvecReport g_mv_report;
+void report_matvec_line(int cwhat, const char* path, float gpu_ms) { g_mv_report.line((char)cwhat, path, gpu_ms); }
 
 using Z = std::complex<double>;
 static inline double2 dz(Z z) { return make_double2(z.real(), z.imag()); }
@@ -28,15 +59,35 @@ template <typename T> struct Ctx {
   int n;
   int nc = 0;
   int err = 0;
-  explicit Ctx(SolveIO<T>& s) : io(s), n(s.n) {}
+  const char* label = "device";
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  explicit Ctx(SolveIO<T>& s, const char* solver = "device") : io(s), n(s.n), label(solver) {
+    if (io.verbose && (cudaEventCreate(&ev[0]) != cudaSuccess || cudaEventCreate(&ev[1]) != cudaSuccess)) {
+      cudaGetLastError();
+      ev[0] = ev[1] = nullptr;
+    }
+  }
+  ~Ctx() {
+    if (ev[0]) cudaEventDestroy(ev[0]);
+    if (ev[1]) cudaEventDestroy(ev[1]);
+  }
   cudaStream_t st() const { return io.stream; }
   int mv(const C* in, C* out, int conj = 0) {
     MvArgs<T> a;
     a.x = in; a.y = out; a.io_full = 0;
     a.adia = io.adia; a.aoff = io.aoff; a.a_full = io.a_full; a.conj = conj; a.nrhs = 1;
+    const bool timed = io.verbose && ev[0];
+    if (timed) cudaEventRecord(ev[0], st());
     int rc = io.eng->matvec(a);
     if (!rc) ++nc;
-    if (!rc && io.verbose) std::printf("CUDA MATVEC %d [%c]\n", nc, conj ? 'C' : 'N');
+    if (!rc && timed) {
+      float ms = 0.f;
+      cudaEventRecord(ev[1], st());
+      if (cudaEventSynchronize(ev[1]) == cudaSuccess && cudaEventElapsedTime(&ms, ev[0], ev[1]) == cudaSuccess)
+        g_mv_report.line(conj ? 'C' : 'N', label, ms);
+      else
+        cudaGetLastError();
+    }
     return rc;
   }
   Z dotc(const C* a, const C* b) { return zd(io.ops->dotc(n, a, b, &err)); }
@@ -83,7 +134,7 @@ template <typename T> struct Ctx {
 template <typename T> int solve_pbcgs2(SolveIO<T>& io) {
   using C = cplx<T>;
   const char* name = "PBCGS2";
-  Ctx<T> c(io);
+  Ctx<T> c(io, name);
   C *rr = c.w(0), *r[3] = {c.w(1), c.w(2), c.w(3)}, *u[3] = {c.w(4), c.w(5), c.w(6)};
   C *XP = c.w(7), *BP = c.w(8), *X = c.w(9);
   // init: rr=r0=BP=b, XP=x0, the rest 0 (cu:462)
@@ -215,7 +266,7 @@ template <typename T> int solve_pbcgs2(SolveIO<T>& io) {
 template <typename T> int solve_qmrccg(SolveIO<T>& io) {
   using C = cplx<T>;
   const char* name = "QMRCCG";
-  Ctx<T> c(io);
+  Ctx<T> c(io, name);
   C *r = c.w(0), *p = c.w(1), *ap = c.w(2), *q = c.w(3), *d = c.w(4), *s = c.w(5);
   C *vt = c.w(6), *wt = c.w(7), *atw = c.w(8), *xs = c.w(9);
   const double bnorm = c.nrm(io.b);
@@ -350,7 +401,7 @@ template <typename T> int solve_qmrccg(SolveIO<T>& io) {
 template <typename T> int solve_pbcgst(SolveIO<T>& io) {
   using C = cplx<T>;
   const char* name = "PBCGST";
-  Ctx<T> c(io);
+  Ctx<T> c(io, name);
   C *r = c.w(0), *rt = c.w(1), *p = c.w(2), *sv = c.w(3), *v = c.w(4), *t = c.w(5), *xs = c.w(6), *rtrue = c.w(7);
   const Engine<T>& E = *io.eng;
   auto precon = [&](C* dst, const C* src) { v_precon<T>(dst, src, io.adia, E.occ, E.g.nat, E.g.nat0, c.st()); };
@@ -441,7 +492,7 @@ template <typename T> int solve_pbcgst(SolveIO<T>& io) {
 template <typename T> int solve_petrkp(SolveIO<T>& io) {
   using C = cplx<T>;
   const char* name = "PETRKP";
-  Ctx<T> c(io);
+  Ctx<T> c(io, name);
   C *ace = c.w(0), *gi = c.w(1), *pi = c.w(2), *qi = c.w(3), *axi = c.w(4), *rv = c.w(5), *xs = c.w(6);
   c.copy(xs, io.x);
   const double bb = c.dotc(io.b, io.b).real();
@@ -504,7 +555,7 @@ template <typename T> int solve_petrkp(SolveIO<T>& io) {
 template <typename T> int solve_gpbicg(SolveIO<T>& io) {
   using C = cplx<T>;
   const char* name = "GPBICG";
-  Ctx<T> c(io);
+  Ctx<T> c(io, name);
   C *r0 = c.w(0), *p = c.w(1), *r = c.w(2), *yv = c.w(3), *t = c.w(4), *ap = c.w(5), *at = c.w(6);
   C *u = c.w(7), *wv = c.w(8), *zv = c.w(9), *xsol = c.w(10), *told = c.w(11), *tmp = c.w(12);
   c.copy(xsol, io.x);
@@ -621,7 +672,7 @@ template <typename T> int solve_gpbicg(SolveIO<T>& io) {
 template <typename T> int solve_bicgstab4(SolveIO<T>& io) {
   using C = cplx<T>;
   const char* name = "BiCGStab4";
-  Ctx<T> c(io);
+  Ctx<T> c(io, name);
   C* r[5] = {c.w(0), c.w(3), c.w(4), c.w(5), c.w(6)};
   C* u[5] = {c.w(1), c.w(7), c.w(8), c.w(9), c.w(10)};
   C* rtil = c.w(2);
@@ -755,7 +806,7 @@ static bool solve_small(Z* a, Z* b, int n, int ld) {
 template <typename T> int solve_gpbicgstab2(SolveIO<T>& io) {
   using C = cplx<T>;
   const char* name = "GPBiCGStab2";
-  Ctx<T> c(io);
+  Ctx<T> c(io, name);
   C *r0 = c.w(0), *p0 = c.w(1), *rt = c.w(2), *z = c.w(3), *yv = c.w(4), *u = c.w(5), *hs = c.w(6), *hq0 = c.w(7),
     *hq1 = c.w(8), *work = c.w(9);
   C* x = io.x;
@@ -915,7 +966,7 @@ template <typename T> int solve_gpbicgstab2(SolveIO<T>& io) {
 template <typename T> int solve_gpbicgstab4(SolveIO<T>& io) {
   using C = cplx<T>;
   const char* name = "GPBiCGStab4";
-  Ctx<T> c(io);
+  Ctx<T> c(io, name);
   C *r0 = c.w(0), *p0 = c.w(1), *rt = c.w(2), *z = c.w(3), *yv = c.w(4), *u = c.w(5);
   C* hs[3] = {c.w(6), c.w(7), c.w(8)};
   C* hq[4] = {c.w(9), c.w(10), c.w(11), c.w(12)};

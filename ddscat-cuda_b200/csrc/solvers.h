@@ -24,6 +24,9 @@ template <typename T> struct SolveIO {
   int ncompte = 0;
 };
 
+// one reference-style console line for a MATVEC of GPU time gpu_ms (cu:417)
+void report_matvec_line(int cwhat, const char* path, float gpu_ms);
+
 template <typename T> int solve_pbcgs2(SolveIO<T>& io);
 template <typename T> int solve_qmrccg(SolveIO<T>& io);
 template <typename T> int solve_pbcgst(SolveIO<T>& io);

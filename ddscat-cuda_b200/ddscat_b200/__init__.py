@@ -30,7 +30,9 @@ EXPORTS = (
        "ddscat_b200_last_solve_stats", "ddscat_b200_residual_f64", "ddscat_b200_launch_count",
        "ddscat_b200_apply_noalloc_f32", "ddscat_b200_mueller_f32", "ddscat_b200_make_inputs_f32",
        "ddscat_b200_solve_batch_f64", "ddscat_b200_adjoint_f32", "ddscat_b200_multi_solve_f32",
-       "ddscat_b200_autotune_f32", "ddscat_b200_mueller_f64", "ddscat_b200_scat_amplitudes_f64"]
+       "ddscat_b200_autotune_f32", "ddscat_b200_mueller_f64", "ddscat_b200_scat_amplitudes_f64",
+       "ddscat_b200_scat_csca_f64", "ddscat_b200_make_inputs_pol_f32", "ddscat_b200_adjoint_fwd_f32",
+       "ddscat_b200_ffweights_f32"]
 )
 
 
@@ -94,6 +96,12 @@ def _declare(lib):
     lib.ddscat_b200_mueller_f32.restype = _I
     lib.ddscat_b200_make_inputs_f32.argtypes = [_I, _P, _P, _P, _I, _P, _P, _P, _P]
     lib.ddscat_b200_make_inputs_f32.restype = _I
+    lib.ddscat_b200_make_inputs_pol_f32.argtypes = [_I, _I, _P, _P, _P, _I, _P, _P, _P, _P]
+    lib.ddscat_b200_make_inputs_pol_f32.restype = _I
+    lib.ddscat_b200_adjoint_fwd_f32.argtypes = [_I, _P, _P, _P, _P, _I, _F, _P, _P, _P, _P]
+    lib.ddscat_b200_adjoint_fwd_f32.restype = _I
+    lib.ddscat_b200_ffweights_f32.argtypes = [_I, _P, _P, _P, _D2, _P]
+    lib.ddscat_b200_ffweights_f32.restype = _I
     lib.ddscat_b200_solve_batch_f64.argtypes = [_I, _I, _P, _P, _P, _P, _I, _D2, _P, _P, _P, _P]
     lib.ddscat_b200_solve_batch_f64.restype = _I
     lib.ddscat_b200_adjoint_f32.argtypes = [_I, _P, _P, _P, _P, _I, _F, _P, _P, _P, _P]
@@ -106,6 +114,8 @@ def _declare(lib):
     lib.ddscat_b200_mueller_f64.restype = _I
     lib.ddscat_b200_scat_amplitudes_f64.argtypes = [_I, _P, _I, _P, _P, _P, _P, _P, _P, _D2, _P, _P]
     lib.ddscat_b200_scat_amplitudes_f64.restype = _I
+    lib.ddscat_b200_scat_csca_f64.argtypes = [_I, _P, _P, _P, _F, _P, _P, _F, _P, _P, _P, _P, _P]
+    lib.ddscat_b200_scat_csca_f64.restype = _I
     lib.ddscat_b200_launch_count.argtypes = []
     lib.ddscat_b200_launch_count.restype = ct.c_ulonglong
 
@@ -143,6 +153,7 @@ QMR_SYMMETRIC = 0x200  # DDSCAT_B200_QMR_SYMMETRIC
 INPUTS_F64 = 0x400  # DDSCAT_B200_INPUTS_F64
 AUTOTUNE = 0x800  # DDSCAT_B200_AUTOTUNE
 GRAPH = 0x1000  # DDSCAT_B200_GRAPH
+CMDPOL = {"LATTDR": 0, "GKDLDR": 1, "FLTRCD": 2}  # DDSCAT_B200_LATTDR, _GKDLDR, _FLTRCD
 
 
 def _vptr(a):
@@ -175,6 +186,8 @@ class SolveOut:
 class DDA:
     """One prepared target on the current CUDA device (the library keeps a
     single global state, like the reference)."""
+
+    takes_device_pointers = True  # the batched / adjoint entry points accept CUDA tensors
 
     def __init__(self, layout="fft3d"):
         self.lib = load(layout)
@@ -322,6 +335,47 @@ class DDA:
         self._check("adjoint", rc)
         return grad, lam, it, tole
 
+    def adjoint_fwd(self, e, src, adia, dadia, maxit=1000, tol=1e-5, want_p=False):
+        """Per-site derivatives of s_k^T P with the forward solution P of A P = e
+        recomputed inside the call (ddscat_b200_adjoint_fwd_f32).  e, adia,
+        dadia: (3*NAT,) complex64; src: (nsrc, 3*NAT) complex64; NumPy arrays
+        or CUDA tensors (all of one kind).  Returns (grad (nsrc, NAT), p or None,
+        itno, tole) with itno / tole of the forward solve first."""
+        dev = hasattr(e, "data_ptr")
+        if not dev:
+            e, adia, dadia = (np.ascontiguousarray(a, dtype=np.complex64).reshape(-1) for a in (e, adia, dadia))
+            src = np.ascontiguousarray(src, dtype=np.complex64).reshape(-1, 3 * self.nat)
+        nsrc = int(src.shape[0])
+        if dev:
+            import torch
+
+            grad = torch.zeros((nsrc, self.nat), dtype=torch.complex64, device=e.device)
+            p = torch.zeros(3 * self.nat, dtype=torch.complex64, device=e.device) if want_p else None
+        else:
+            grad = np.zeros((nsrc, self.nat), dtype=np.complex64)
+            p = np.zeros(3 * self.nat, dtype=np.complex64) if want_p else None
+        it = np.zeros(nsrc + 1, dtype=np.int32)
+        tole = np.zeros(nsrc + 1, dtype=np.float32)
+        rc = self.lib.ddscat_b200_adjoint_fwd_f32(nsrc, _vptr(e), _vptr(src), _vptr(adia), _vptr(dadia), maxit, tol,
+                                                  _vptr(grad), _vptr(p), _ptr(it), _ptr(tole))
+        self._check("adjoint_fwd", rc)
+        return grad, p, it, tole
+
+    def ffweights(self, aks, ems, x0, e02=1.0, out=None):
+        """Far-field adjoint sources (nw, 3*NAT) complex64 built on the GPU
+        (ddscat_b200_ffweights_f32): w_k^T P is SCAT's amplitude along ems[k]
+        at scattering wave vector aks[k].  out: optional CUDA tensor or NumPy
+        array to fill; a NumPy array is returned when none is given."""
+        aksd = np.ascontiguousarray(aks, dtype=np.float64).reshape(-1, 3)
+        emd = np.ascontiguousarray(ems, dtype=np.float64).reshape(-1, 3)
+        x0d = np.ascontiguousarray(x0, dtype=np.float64)
+        nw = aksd.shape[0]
+        if out is None:
+            out = np.zeros((nw, 3 * self.nat), dtype=np.complex64)
+        rc = self.lib.ddscat_b200_ffweights_f32(nw, _ptr(aksd), _ptr(emd), _ptr(x0d), float(e02), _vptr(out))
+        self._check("ffweights", rc)
+        return out
+
     def multi_solve(self, targets_, name="qmrccg", maxit=1000, tol=1e-5, replace=True, symmetric=True, nthreads=0,
                     check=True, autotune=False, graph=False):
         """Solve many targets of uneven size together.  targets_: list of dicts
@@ -377,10 +431,11 @@ class DDA:
         self._check("matvec_timing", self.lib.ddscat_b200_matvec_timing(nrhs, iters, ord(cwhat), ct.byref(ms)))
         return ms.value
 
-    def make_inputs(self, ks, es, x0, m, icomp=None, b=None, adia=None):
+    def make_inputs(self, ks, es, x0, m, icomp=None, b=None, adia=None, cmdpol="LATTDR"):
         """b and CXADIA (nrhs, 3*NAT) for wave vectors ks (nrhs, 3) and
         polarisations es (nrhs, 3) on the GPU.  m: refractive index or list of
-        them; icomp: NAT material indices (1-based, 0 vacuum) or None.  b / adia:
+        them; icomp: NAT material indices (1-based, 0 vacuum) or None; cmdpol:
+        the polarisability prescription, "LATTDR", "GKDLDR" or "FLTRCD".  b / adia:
         optional preallocated outputs (NumPy arrays or CUDA tensors); NumPy
         arrays are returned when none are given."""
         kf = np.ascontiguousarray(ks, dtype=np.float32).reshape(-1, 3)
@@ -392,8 +447,13 @@ class DDA:
         if b is None and adia is None:
             b = np.zeros((nrhs, 3 * self.nat), dtype=np.complex64)
             adia = np.zeros_like(b)
-        rc = self.lib.ddscat_b200_make_inputs_f32(nrhs, _ptr(kf), _ptr(ef), _ptr(x0f), int(mf.size), _ptr(mf),
-                                                  _ptr(ic), _vptr(b), _vptr(adia))
+        pol = CMDPOL[cmdpol]
+        if pol == CMDPOL["LATTDR"]:
+            rc = self.lib.ddscat_b200_make_inputs_f32(nrhs, _ptr(kf), _ptr(ef), _ptr(x0f), int(mf.size), _ptr(mf),
+                                                      _ptr(ic), _vptr(b), _vptr(adia))
+        else:
+            rc = self.lib.ddscat_b200_make_inputs_pol_f32(pol, nrhs, _ptr(kf), _ptr(ef), _ptr(x0f), int(mf.size),
+                                                          _ptr(mf), _ptr(ic), _vptr(b), _vptr(adia))
         self._check("make_inputs", rc)
         return b, adia
 
@@ -449,6 +509,27 @@ class DDA:
                                                       _ptr(f2))
         self._check("scat_amplitudes_f64", rc)
         return f1, f2
+
+    def scat_csca_f64(self, x, ak, e01, x0, dx=(1.0, 1.0, 1.0), etasca=0.5, e02=1.0):
+        """All-FP64 Csca, Csca*g, Csca*<cos^2>, backscatter and NAVG of the
+        polarisations x ((nrhs, 3*NAT) complex128, NumPy or CUDA tensor) over
+        SCAT's integration directions for incident polarisations e01 ((nrhs, 3)
+        or (3,)): the FP64 counterpart of scat()'s cross sections."""
+        nrhs = int(x.shape[0])
+        if not hasattr(x, "data_ptr") and (x.dtype != np.complex128 or not x.flags.c_contiguous):
+            raise ValueError("x must be a C-contiguous complex128 array")
+        e01c = np.ascontiguousarray(np.broadcast_to(np.asarray(e01, dtype=np.complex64).reshape(-1, 3), (nrhs, 3)))
+        akf = np.ascontiguousarray(ak, dtype=np.float32)
+        dxf = np.ascontiguousarray(dx, dtype=np.float32)
+        x0f = np.ascontiguousarray(x0, dtype=np.float32)
+        cb, cs, cg2 = (np.zeros(nrhs) for _ in range(3))
+        cg = np.zeros((nrhs, 3))
+        navg = np.zeros(nrhs, dtype=np.int32)
+        rc = self.lib.ddscat_b200_scat_csca_f64(nrhs, _vptr(x), _ptr(akf), _ptr(e01c), float(etasca), _ptr(dxf),
+                                                _ptr(x0f), float(e02), _ptr(cb), _ptr(cs), _ptr(cg), _ptr(cg2),
+                                                _ptr(navg))
+        self._check("scat_csca_f64", rc)
+        return {"cbksca": cb, "csca": cs, "cscag": cg, "cscag2": cg2, "navg": navg}
 
     def autotune(self, iters=5):
         """Tune the prepared target's FFT launch shapes; returns (default ms, best ms) per MATVEC."""

@@ -5,9 +5,13 @@ The DDA matrix A(eps) = diag(CXADIA(eps)) - G is complex symmetric, so the
 derivative of any holomorphic functional F = s^T P of the polarisation P =
 A^-1 E costs one adjoint solve A lam = s and a per-site product:
 dF/deps_j = -sum_c lam_c(j) dCXADIA_c(j)/deps_j P_c(j).  With the lattice
-dispersion relation polarisability (Draine & Goodman 1993)
-    1/alpha = (4 pi / 3)(eps + 2)/(eps - 1) + (b1 + eps b2 + eps b3 S)(kd)^2 - (2/3) i (kd)^3
-the site derivative is d(1/alpha)/deps = -4 pi/(eps - 1)^2 + (b2 + b3 S)(kd)^2.
+dispersion relation polarisabilities (Draine & Goodman 1993; the per-component
+form of Gutkowicz-Krusin & Draine 2004)
+    1/alpha_c = (4 pi / 3)(eps + 2)/(eps - 1) + (b1 + eps b2 + eps b3 S_c)(kd)^2 - (2/3) i (kd)^3
+the site derivative is d(1/alpha_c)/deps = -4 pi/(eps - 1)^2 + (b2 + b3 S_c)(kd)^2
+(S_c = sum_j (a_j e_j)^2 for LATTDR, a_c^2 for GKDLDR); the filtered coupled
+dipole form (FLTRCD) has only the first term.  The problem's prescription
+(Problem.cmdpol) is used.
 
 * Cext = 4 pi k Im(E^H P)/E02 -> F = conj(E)^T P;
   dCext/dRe eps = 4 pi k Im(g)/E02, dCext/dIm eps = 4 pi k Re(g)/E02.
@@ -25,7 +29,7 @@ import math
 
 import numpy as np
 
-from .targets import B1, B2, B3
+from .targets import B1, B2, B3, dinv_alpha_deps, inv_alpha_eps
 
 
 def ldr_inv_alpha(eps, kd, khat, e):
@@ -44,20 +48,25 @@ def ldr_dinv_alpha(eps, kd, khat, e):
 
 
 def _full(prob, site_vals, fill):
-    """3*NAT vector with site_vals (NAT0, compact order) on occupied sites."""
-    v = np.full(prob.nat, fill, dtype=np.complex128)
-    v[prob.occ] = site_vals
-    return np.tile(v, 3)
+    """3*NAT vector with site_vals ((3, NAT0): per component, compact order) on
+    occupied sites and fill[c] on vacuum sites."""
+    v = np.empty((3, prob.nat), dtype=np.complex128)
+    for c in range(3):
+        v[c] = fill[c]
+        v[c, prob.occ] = site_vals[c]
+    return v.reshape(-1)
 
 
 def site_inputs(prob, r, eps):
-    """(b, CXADIA, dCXADIA/deps) full vectors of RHS r for per-site permittivity eps (NAT0)."""
+    """(b, CXADIA, dCXADIA/deps) full vectors of RHS r for per-site permittivity
+    eps (NAT0), with the problem's polarisability prescription."""
     inc = prob.incid[r]
     khat = inc.k / np.linalg.norm(inc.k)
     kd = float(np.linalg.norm(inc.k))
-    ia = ldr_inv_alpha(eps, kd, khat, inc.e)
-    dia = ldr_dinv_alpha(eps, kd, khat, inc.e)
-    return prob.rhs(r), _full(prob, ia, ia[0]), _full(prob, dia, 0.0)
+    cmdpol = getattr(prob, "cmdpol", "LATTDR")
+    ia = inv_alpha_eps(eps, kd, khat, inc.e, cmdpol)
+    dia = dinv_alpha_deps(eps, kd, khat, inc.e, cmdpol)
+    return prob.rhs(r), _full(prob, ia, ia[:, 0]), _full(prob, dia, np.zeros(3))
 
 
 def farfield_weights(prob, r, aks, ems, e02=1.0):
@@ -79,14 +88,36 @@ def _solve(dda, b, adia, tol, maxit):
     return x, out
 
 
+def _on_gpu(dda):
+    """Device tensors for the adjoint inputs when torch has a CUDA device and
+    the library object is the real one (it takes device pointers)."""
+    if not getattr(dda, "takes_device_pointers", False):
+        return None
+    try:
+        import torch
+    except ImportError:
+        return None
+    return torch if torch.cuda.is_available() else None
+
+
 def cext_and_grad(dda, prob, r, eps, tol=1e-5, maxit=2000, e02=1.0):
     """Cext of RHS r for per-site permittivity eps (NAT0 complex) and its
-    gradient (dRe, dIm) per occupied site, FP32 forward and adjoint solves."""
+    gradient (dRe, dIm) per occupied site: FP32 forward and adjoint solves in
+    one call (ddscat_b200_adjoint_fwd_f32, which recomputes the forward field
+    instead of taking it from the caller)."""
     b, adia, dadia = site_inputs(prob, r, eps)
-    x, _ = _solve(dda, b[None, :], adia[None, :], tol, maxit)
+    b64, a64, d64 = (v.astype(np.complex64) for v in (b, adia, dadia))
+    src = np.conj(b64)[None, :]
+    torch = _on_gpu(dda)
+    if torch is not None:
+        dev = torch.device("cuda", torch.cuda.current_device())
+        t = lambda v: torch.from_numpy(np.ascontiguousarray(v)).to(dev)  # noqa: E731
+        g, p, _, _ = dda.adjoint_fwd(t(b64), t(src), t(a64), t(d64), maxit=maxit, tol=tol, want_p=True)
+        g, p = g.cpu().numpy(), p.cpu().numpy()
+    else:
+        g, p, _, _ = dda.adjoint_fwd(b64, src, a64, d64, maxit=maxit, tol=tol, want_p=True)
     kk = float(np.linalg.norm(prob.incid[r].k))
-    cext = 4.0 * math.pi * kk * np.vdot(b.astype(np.complex128), x[0].astype(np.complex128)).imag / e02
-    g, _, _, _ = dda.adjoint(x, np.conj(b)[None, :], adia[None, :], dadia[None, :], maxit=maxit, tol=tol)
+    cext = 4.0 * math.pi * kk * np.vdot(b.astype(np.complex128), p.astype(np.complex128)).imag / e02
     gs = g[0][prob.occ].astype(np.complex128)
     fac = 4.0 * math.pi * kk / e02
     return cext, fac * gs.imag, fac * gs.real
@@ -94,17 +125,29 @@ def cext_and_grad(dda, prob, r, eps, tol=1e-5, maxit=2000, e02=1.0):
 
 def intensity_and_grad(dda, prob, r, eps, aks, em1, em2, tol=1e-5, maxit=2000, e02=1.0):
     """I(n) = |f_1|^2 + |f_2|^2 at each scattering wave vector of aks and its
-    gradient (dRe, dIm) per occupied site: arrays (ndir,), (ndir, NAT0), (ndir, NAT0)."""
+    gradient (dRe, dIm) per occupied site: arrays (ndir,), (ndir, NAT0), (ndir, NAT0).
+    The far-field adjoint sources are built by the library
+    (ddscat_b200_ffweights_f32; on the GPU, in device memory when torch has a
+    CUDA device) and the forward field is recomputed inside the adjoint call."""
     b, adia, dadia = site_inputs(prob, r, eps)
-    x, _ = _solve(dda, b[None, :], adia[None, :], tol, maxit)
+    b64, a64, d64 = (v.astype(np.complex64) for v in (b, adia, dadia))
     nd = len(aks)
-    w = farfield_weights(prob, r, list(aks) + list(aks), list(em1) + list(em2), e02)
-    W = np.stack(w)
-    f = W @ x[0].astype(np.complex128)  # f_1 for every direction, then f_2
-    R = 2 * nd
-    g, _, _, _ = dda.adjoint(np.repeat(x, R, axis=0), W, np.repeat(adia[None, :], R, axis=0),
-                             np.repeat(dadia[None, :], R, axis=0), maxit=maxit, tol=tol)
-    gs = g[:, prob.occ].astype(np.complex128)
+    aks2 = np.concatenate([np.asarray(aks, dtype=np.float64)] * 2)
+    ems = np.concatenate([np.asarray(em1, dtype=np.float64), np.asarray(em2, dtype=np.float64)])
+    torch = _on_gpu(dda)
+    if torch is not None:
+        dev = torch.device("cuda", torch.cuda.current_device())
+        W = torch.empty((2 * nd, 3 * prob.nat), dtype=torch.complex64, device=dev)
+        dda.ffweights(aks2, ems, prob.x0, e02, out=W)
+        t = lambda v: torch.from_numpy(np.ascontiguousarray(v)).to(dev)  # noqa: E731
+        g, p, _, _ = dda.adjoint_fwd(t(b64), W, t(a64), t(d64), maxit=maxit, tol=tol, want_p=True)
+        f = (W.to(torch.complex128) @ p.to(torch.complex128)).cpu().numpy()  # f_1 for every direction, then f_2
+        gs = g[:, torch.from_numpy(prob.occ).to(dev)].to(torch.complex128).cpu().numpy()
+    else:
+        W = dda.ffweights(aks2, ems, prob.x0, e02)
+        g, p, _, _ = dda.adjoint_fwd(b64, W, a64, d64, maxit=maxit, tol=tol, want_p=True)
+        f = W.astype(np.complex128) @ p.astype(np.complex128)
+        gs = g[:, prob.occ].astype(np.complex128)
     inten = np.abs(f[:nd]) ** 2 + np.abs(f[nd:]) ** 2
     h = np.conj(f[:nd])[:, None] * gs[:nd] + np.conj(f[nd:])[:, None] * gs[nd:]
     return inten, 2.0 * h.real, -2.0 * h.imag

@@ -8,10 +8,23 @@ configurations:
 
 * occupancy: site (i,j,k) is occupied iff sum_a ((i_a + 1/2 - n_a/2)/r_a)^2 <= 1
   (r_a = semi-axes in lattice units);
-* lattice-dispersion-relation polarisability (Draine & Goodman 1993, ApJ 405,
-  685): alpha = alpha_CM / (1 + (alpha_CM/d^3) [(b1 + m^2 b2 + m^2 b3 S)(kd)^2
-  - (2/3) i (kd)^3]), b1=-1.891531, b2=0.1648469, b3=-1.7700004,
-  S = sum_j (a_j e_j)^2, alpha_CM = (3/4pi)(m^2-1)/(m^2+2); CXADIA = 1/alpha;
+* polarisabilities (CXADIA = 1/alpha per Cartesian component, lattice units
+  d = 1, alpha_CM = (3/4pi)(m^2-1)/(m^2+2), a = unit propagation vector,
+  e = unit polarisation vector), DDSCAT's CMDPOL choices:
+  - LATTDR, the lattice dispersion relation of Draine & Goodman (1993, ApJ 405,
+    685): 1/alpha = 1/alpha_CM + (b1 + m^2 b2 + m^2 b3 S)(kd)^2 - (2/3) i (kd)^3,
+    S = sum_j (a_j e_j)^2, b1 = -1.891531, b2 = 0.1648469, b3 = -1.7700004, the
+    same for the three components;
+  - GKDLDR, the corrected lattice dispersion relation of Gutkowicz-Krusin &
+    Draine (2004, arXiv:astro-ph/0403082): a diagonal tensor whose component j
+    has S replaced by a_j^2, so it depends on the direction of propagation but
+    not on the polarisation: 1/alpha_jj = 1/alpha_CM + (b1 + m^2 b2 +
+    m^2 b3 a_j^2)(kd)^2 - (2/3) i (kd)^3 (the prescription of the synthetic
+    workloads, as in DDSCAT's own parameter files);
+  - FLTRCD, the filtered coupled dipole polarisability (Piller & Martin 1998;
+    Gay-Balmaz & Martin 2002; Yurkin, Min & Hoekstra 2010): 1/alpha =
+    1/alpha_CM - (4/3)(kd)^2 - (2/(3 pi)) ln((pi - kd)/(pi + kd)) (kd)^3
+    - (2/3) i (kd)^3, for kd < pi;
 * incident field E_j = e0 exp(i k.r_j), r_j = ((i+1)+x0)*d, x0 = -(n+1)/2
   (target centred at the origin).
 """
@@ -23,6 +36,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 B1, B2, B3 = -1.891531, 0.1648469, -1.7700004
+PRESCRIPTIONS = ("LATTDR", "GKDLDR", "FLTRCD")
 
 
 def ellipsoid_occupancy(nx, ny, nz, semi=None):
@@ -43,6 +57,43 @@ def ldr_alpha(m, kd, khat, ehat):
     S = float(np.sum((np.asarray(khat) * np.real(np.asarray(ehat))) ** 2))
     corr = (B1 + eps * B2 + eps * B3 * S) * kd ** 2 - (2.0 / 3.0) * 1j * kd ** 3
     return acm / (1.0 + acm * corr)
+
+
+def _shape_factor(khat, ehat, cmdpol):
+    """The (kd)^2 term's S per Cartesian component (3,): LATTDR's sum_j (a_j e_j)^2
+    for all three, GKDLDR's a_j^2; None for FLTRCD."""
+    a = np.asarray(khat, dtype=np.float64)
+    if cmdpol == "LATTDR":
+        return np.full(3, float(np.sum((a * np.real(np.asarray(ehat))) ** 2)))
+    if cmdpol == "GKDLDR":
+        return a ** 2
+    if cmdpol == "FLTRCD":
+        return None
+    raise ValueError(f"unknown polarisability prescription {cmdpol!r} (one of {PRESCRIPTIONS})")
+
+
+def inv_alpha_eps(eps, kd, khat, ehat, cmdpol="GKDLDR"):
+    """1/alpha (lattice units) per Cartesian component for permittivity eps
+    (scalar or array): shape (3,) + eps.shape."""
+    eps = np.asarray(eps, dtype=np.complex128)
+    base = (4.0 * math.pi / 3.0) * (eps + 2.0) / (eps - 1.0) - (2.0 / 3.0) * 1j * kd ** 3
+    S = _shape_factor(khat, ehat, cmdpol)
+    if S is None:
+        if not kd < math.pi:
+            raise ValueError("FLTRCD needs kd < pi")
+        corr = -(4.0 / 3.0) * kd ** 2 - (2.0 / (3.0 * math.pi)) * math.log((math.pi - kd) / (math.pi + kd)) * kd ** 3
+        return np.stack([base + corr] * 3)
+    return np.stack([base + (B1 + eps * B2 + eps * B3 * S[j]) * kd ** 2 for j in range(3)])
+
+
+def dinv_alpha_deps(eps, kd, khat, ehat, cmdpol="GKDLDR"):
+    """d(1/alpha)/d eps per Cartesian component: shape (3,) + eps.shape."""
+    eps = np.asarray(eps, dtype=np.complex128)
+    base = -4.0 * math.pi / (eps - 1.0) ** 2
+    S = _shape_factor(khat, ehat, cmdpol)
+    if S is None:
+        return np.stack([base] * 3)
+    return np.stack([base + (B2 + B3 * S[j]) * kd ** 2 for j in range(3)])
 
 
 def euler_rotation(beta, theta, phi):
@@ -88,6 +139,7 @@ class Problem:
     aeff: float
     x0: tuple
     incid: list = field(default_factory=list)
+    cmdpol: str = "GKDLDR"
 
     @property
     def nat(self):
@@ -114,11 +166,13 @@ class Problem:
         return b.reshape(-1).astype(np.complex64)
 
     def adia(self, r, m=None):
-        """Full CXADIA (3*NAT) for right-hand side r (uniform 1/alpha, homogeneous)."""
+        """Full CXADIA (3*NAT) for right-hand side r: 1/alpha of the problem's
+        prescription per component, the same on every site (homogeneous)."""
         inc = self.incid[r]
         khat = inc.k / np.linalg.norm(inc.k)
-        a = ldr_alpha(self.m if m is None else m, self.kd, khat, inc.e)
-        return np.full(3 * self.nat, 1.0 / a, dtype=np.complex64)
+        eps = complex(self.m if m is None else m) ** 2
+        ia = inv_alpha_eps(eps, self.kd, khat, inc.e, self.cmdpol)
+        return np.repeat(ia.astype(np.complex64), self.nat)
 
     def aoff(self):
         return np.zeros(3 * self.nat, dtype=np.complex64)
@@ -190,10 +244,12 @@ def scattering_planes(k, e01, step_deg=1.0, phis_deg=(0.0, 90.0)):
     return np.array(aks), np.array(em1), np.array(em2)
 
 
-def make_problem(nx, ny=None, nz=None, m=1.5 + 0.01j, x=5.0, semi=None, orientations=None, iocc=None):
+def make_problem(nx, ny=None, nz=None, m=1.5 + 0.01j, x=5.0, semi=None, orientations=None, iocc=None,
+                 cmdpol="GKDLDR"):
     """Ellipsoid (sphere by default) of size parameter x = k*aeff; one RHS per
     (orientation, polarisation) with k along x before rotation and
-    polarisations y and z."""
+    polarisations y and z; polarisability prescription cmdpol."""
+    _shape_factor((1.0, 0.0, 0.0), (0.0, 1.0, 0.0), cmdpol)  # validates the name
     ny = nx if ny is None else ny
     nz = nx if nz is None else nz
     if iocc is None:
@@ -202,7 +258,7 @@ def make_problem(nx, ny=None, nz=None, m=1.5 + 0.01j, x=5.0, semi=None, orientat
     aeff = (3.0 * nat0 / (4.0 * math.pi)) ** (1.0 / 3.0)
     kd = x / aeff
     x0 = (-(nx + 1) / 2.0, -(ny + 1) / 2.0, -(nz + 1) / 2.0)
-    p = Problem(nx, ny, nz, np.asarray(iocc, dtype=np.int16), complex(m), kd, aeff, x0)
+    p = Problem(nx, ny, nz, np.asarray(iocc, dtype=np.int16), complex(m), kd, aeff, x0, cmdpol=cmdpol)
     if orientations is None:
         orientations = [(0.0, 0.0, 0.0)]
     for ang in orientations:
@@ -213,11 +269,11 @@ def make_problem(nx, ny=None, nz=None, m=1.5 + 0.01j, x=5.0, semi=None, orientat
     return p
 
 
-def voxel_problem(n, p_occ=0.6, m1=1.5 + 0.01j, m2=1.2 + 0.0j, x=8.0, seed=0):
+def voxel_problem(n, p_occ=0.6, m1=1.5 + 0.01j, m2=1.2 + 0.0j, x=8.0, seed=0, cmdpol="GKDLDR"):
     """Two-material random voxel target: each voxel occupied with probability
     p_occ, material 1 with probability 1/2.  Returns (Problem, material map)."""
     rng = np.random.default_rng(seed)
     occ = rng.random(n ** 3) < p_occ
     mat = np.where(rng.random(n ** 3) < 0.5, 1, 2) * occ
-    prob = make_problem(n, m=m1, x=x, iocc=occ.astype(np.int16))
+    prob = make_problem(n, m=m1, x=x, iocc=occ.astype(np.int16), cmdpol=cmdpol)
     return prob, mat

@@ -75,6 +75,12 @@ DDSCAT_CUDA_API int ddscat_b200_autotune_f32(int iters, float *default_ms, float
 #define DDSCAT_B200_INPUTS_F64 0x400
 #define DDSCAT_B200_AUTOTUNE 0x800
 #define DDSCAT_B200_GRAPH 0x1000
+
+/* Polarisability prescriptions of ddscat_b200_make_inputs_pol_f32 (DDSCAT's
+ * CMDPOL values). */
+#define DDSCAT_B200_LATTDR 0
+#define DDSCAT_B200_GKDLDR 1
+#define DDSCAT_B200_FLTRCD 2
 DDSCAT_CUDA_API int ddscat_b200_solve_batch_f32(int solver, int nrhs, const void *b, void *x, const void *adia,
                                                 const void *aoff, int maxit, float tol, int *itno, float *tole,
                                                 int *ncompte, int *status);
@@ -91,21 +97,25 @@ DDSCAT_CUDA_API int ddscat_b200_residual_f64(int nrhs, const void *b, const void
                                              const void *aoff, double *resid);
 
 /* MATVEC that allocates no device memory; no counterpart in the reference.
- * For callers that cannot call cudaMalloc where they need the operator (inside
- * CUDA stream capture, in allocation-free real-time loops, or with all device
- * memory handed to their own pool): y = A x (cwhat 'N') or A^H x ('C') for the
- * prepared target, with x, y, adia and aoff caller-owned DEVICE vectors in the
- * full layout of ddscat_cuda_apply_f32 (3*NAT complex floats; aoff may be
- * NULL), launched on `stream` (a cudaStream_t, NULL for the legacy default
- * stream).  The MATVEC scratch is a fixed 48 MiB array in the library's device
- * image, so only targets with NAT <= 349,525 sites (e.g. 64^3) are accepted;
- * every GPU that loads the library holds that array until exit.  All calls
- * share it and it keeps the last call's contents (nothing needs to start at
- * zero); calls that overlap on the GPU race, so serialise them.  The first call
- * on a device (and the first after each prepare) does one-time set-up and
- * should come before any stream capture.  Codes: 600 invalid argument or not
- * prepared, 601 target larger than the fixed scratch, 602 scratch address
- * lookup failed, 21-25 kernel launch failure. */
+ * For callers that cannot call cudaMalloc where they need the operator
+ * (real-time loops that forbid allocation once started, or applications that
+ * hand all device memory to their own pool): y = A x (cwhat 'N') or A^H x
+ * ('C') for the prepared target, with x, y, adia and aoff caller-owned DEVICE
+ * vectors in the full layout of ddscat_cuda_apply_f32 (3*NAT complex floats;
+ * aoff may be NULL), launched on `stream` (a cudaStream_t, NULL for the legacy
+ * default stream), with the device of the prepare current.  The MATVEC
+ * scratch is a fixed 48 MiB array (6,291,456 complex floats) in the library's
+ * device image; every GPU that loads the library holds it until exit.  It must
+ * hold 3*nz*Mx*ny + 3*My*nz*Mx complex floats for the padded FFT lengths Mx,
+ * My of the prepared grid (18*NAT when M = 2n: unpadded targets up to
+ * NAT = 349,525 sites, e.g. 64^3; padded grids need more), else the call
+ * returns 601.  All calls share the array and it keeps the last call's
+ * contents (nothing needs to start at zero); calls that overlap on the GPU
+ * race, so serialise them.  The first call on a device (and the first after
+ * each prepare) does one-time set-up and should come before any stream
+ * capture.  Codes: 600 invalid argument, not prepared or another device
+ * current, 601 target larger than the fixed scratch, 602 scratch address lookup
+ * failed, 21-25 kernel launch failure. */
 DDSCAT_CUDA_API int ddscat_b200_apply_noalloc_f32(int cwhat, const void *x, void *y, const void *adia,
                                                   const void *aoff, void *stream);
 
@@ -146,6 +156,23 @@ DDSCAT_CUDA_API int ddscat_b200_scat_amplitudes_f64(int nrhs, const void *x, int
                                                     const double *dx, const double *x0, double e02, void *f1,
                                                     void *f2);
 
+/* All-FP64 cross sections of SCAT's angular integration for nrhs
+ * polarisations: Csca, Csca*g (3 per RHS), Csca*<cos^2 theta> and the
+ * backscatter term, with the direction set and quadrature weights that
+ * ddscat_cuda_scat_f32 builds from AK, CXE01 and ETASCA
+ * (ddscat_matvec_cuda.cu:849-875, :957-1002), but FP64 phases and FP64 sums of
+ * complex-double polarisations: the reference values that the Qsca and g of
+ * an FP32 solve are checked against.  No counterpart in the reference.
+ * x: nrhs full component-major complex-double polarisations (3*NAT each, host
+ * or device) of the prepared target; e01: nrhs x 3 complex floats (CXE01_TF of
+ * each RHS); outputs per RHS (host): cbksca[nrhs], csca[nrhs], cscag[3*nrhs],
+ * cscag2[nrhs], navg[nrhs].  Codes: 710 invalid argument or not prepared, 711
+ * allocation or transfer, 712 far-field sums. */
+DDSCAT_CUDA_API int ddscat_b200_scat_csca_f64(int nrhs, const void *x, const float *ak, const void *e01,
+                                              float etasca, const float *dx, const float *x0, float e02,
+                                              double *cbksca, double *csca, double *cscag, double *cscag2,
+                                              int *navg);
+
 /* Right-hand sides and CXADIA for nrhs incident waves, generated on the GPU
  * for the prepared target (DDSCAT computes them on the host in EVALE and
  * ALPHADIAG; no counterpart in the reference ABI).  k: nrhs x 3 wave vectors in
@@ -160,6 +187,26 @@ DDSCAT_CUDA_API int ddscat_b200_scat_amplitudes_f64(int nrhs, const void *x, int
  * index out of range, 612 allocation or transfer, 613 kernel failure. */
 DDSCAT_CUDA_API int ddscat_b200_make_inputs_f32(int nrhs, const float *k, const void *e0, const float *x0, int nmat,
                                                 const void *m, const int16_t *icomp, void *b, void *adia);
+
+/* ddscat_b200_make_inputs_f32 with a choice of polarisability prescription
+ * (DDSCAT's CMDPOL; ALPHADIAG is not part of the reference, so the formulas
+ * are restated from the publications; lattice units d = 1, 1/alpha_CM =
+ * (4 pi/3)(m^2+2)/(m^2-1), b1 = -1.891531, b2 = 0.1648469, b3 = -1.7700004):
+ *   DDSCAT_B200_LATTDR  1/alpha = 1/alpha_CM + (b1 + m^2 b2 + m^2 b3 S)(kd)^2
+ *                       - (2/3) i (kd)^3, S = sum_a (khat_a Re e_a)^2 (Draine &
+ *                       Goodman 1993), the same for the three components;
+ *   DDSCAT_B200_GKDLDR  component c with S replaced by khat_c^2
+ *                       (Gutkowicz-Krusin & Draine 2004): CXADIA differs per
+ *                       component and does not depend on the polarisation;
+ *   DDSCAT_B200_FLTRCD  1/alpha = 1/alpha_CM - (4/3)(kd)^2 - (2/(3 pi))
+ *                       ln((pi - kd)/(pi + kd)) (kd)^3 - (2/3) i (kd)^3, kd < pi
+ *                       (filtered coupled dipoles, Piller & Martin 1998,
+ *                       Gay-Balmaz & Martin 2002).
+ * Other arguments and codes as ddscat_b200_make_inputs_f32 (610 also for an
+ * unknown cmdpol or FLTRCD with kd >= pi). */
+DDSCAT_CUDA_API int ddscat_b200_make_inputs_pol_f32(int cmdpol, int nrhs, const float *k, const void *e0,
+                                                    const float *x0, int nmat, const void *m, const int16_t *icomp,
+                                                    void *b, void *adia);
 
 /* All-FP64 batched solve: the recurrence of ddscat_b200_solve_batch_f32 (same
  * solver codes and flags) with complex-double vectors, an FP64 Green tensor and
@@ -196,6 +243,36 @@ DDSCAT_CUDA_API int ddscat_b200_solve_batch_f64(int solver, int nrhs, const void
 DDSCAT_CUDA_API int ddscat_b200_adjoint_f32(int nrhs, const void *p, const void *src, const void *adia,
                                             const void *dadia, int maxit, float tol, void *grad, void *lam, int *itno,
                                             float *tole);
+
+/* Adjoint gradient with the forward field recomputed, not stored (no
+ * counterpart in the reference).  For one incident field E (full vector) and
+ * nsrc adjoint sources s_k, solves the forward system A P = E and the adjoint
+ * systems A lam_k = s_k together (they share the operator; one batched
+ * one-MATVEC QMRCCG solve with residual replacement, nsrc + 1 right-hand
+ * sides) and returns grad[k][j] = -sum_c lam_k[c][j] dadia[c][j] P[c][j], the
+ * derivative of F_k = s_k^T P with respect to a site parameter entering only
+ * CXADIA.  The caller never holds P: for large grids it costs one extra
+ * right-hand side inside the call instead of a stored full vector.  e, adia,
+ * dadia: one full vector each (3*NAT complex floats); src: nsrc full vectors;
+ * grad: nsrc x NAT complex floats (zero on vacuum sites); p: optional output of
+ * the forward solution (full vector) or NULL; itno / tole: nsrc + 1 entries,
+ * the forward solve first.  All host or all device pointers.  Codes as
+ * ddscat_b200_adjoint_f32. */
+DDSCAT_CUDA_API int ddscat_b200_adjoint_fwd_f32(int nsrc, const void *e, const void *src, const void *adia,
+                                                const void *dadia, int maxit, float tol, void *grad, void *p,
+                                                int *itno, float *tole);
+
+/* Far-field adjoint sources built on the GPU (no counterpart in the
+ * reference): for nw scattering wave vectors aks (nw x 3, |aks| = |k|) and
+ * basis vectors em (nw x 3), the full vectors
+ *   w_k[c][j] = |aks_k|^3 / sqrt(e02) em_k[c] exp(-i aks_k . r_j)
+ * on occupied sites (0 on vacuum), r_j = (ix+1, iy+1, iz+1) + x0 (unit
+ * spacing), so that w_k^T P is the scattering amplitude f of
+ * ddscat_cuda_scat_f32 along em_k (cu:957-1002).  FP64 phases, complex-float
+ * output: w is nw x 3*NAT complex floats, host or device.  Codes: 720 invalid
+ * argument or not prepared, 721 allocation or transfer, 722 kernel failure. */
+DDSCAT_CUDA_API int ddscat_b200_ffweights_f32(int nw, const double *aks, const double *em, const double *x0,
+                                              double e02, void *w);
 
 /* Many targets of uneven size solved together (no counterpart in the
  * reference, whose state holds one target).  Target t has lattice dims[3t..3t+2],

@@ -7,7 +7,14 @@ tests/golden/reference_fixtures.npz.  tests/test_oracle_pinned.py then checks
 the CPU oracle against these outputs (no GPU needed), which pins the oracle to
 the reference's actual behaviour.
 
-Run on a GPU machine:  python tests/golden/make_reference_fixtures.py
+A second set at configuration size (reference_fixtures_c1.npz): the whole
+small-sphere workload (32^3 sphere, m = 1.50+0.01i, x = 5, PBCGS2 at tol 1e-5
+for both polarisations, EVALQ, SCAT at ETASCA 0.5 with f1/f2 on 0..180 deg at
+1 deg in two scattering planes) and a 64^3 MATVEC ('N' and 'C').  Its inputs
+are regenerated from seeds by c1_problem() and mv64_inputs() below, so only
+outputs are stored (the 64^3 MATVEC as seeded samples and projections).
+
+Run on a GPU machine:  python tests/golden/make_reference_fixtures.py [base|c1|all]
 """
 import ctypes as ct
 import os
@@ -25,6 +32,47 @@ import ddscat_b200 as D  # noqa: E402
 from oracle import ddscat_oracle as O  # noqa: E402
 
 OUT = os.path.join(HERE, "reference_fixtures.npz")
+OUT_C1 = os.path.join(HERE, "reference_fixtures_c1.npz")
+C1_TOL, C1_MAXIT, C1_ETASCA = 1e-5, 500, 0.5
+MV64_SAMPLES, MV64_PROJ = 8192, 4
+
+
+def c1_problem():
+    """The small-sphere workload: 32^3 sphere, m = 1.50+0.01i, x = 5, one
+    orientation, polarisations e01 = y and e02 = z (seeded, deterministic)."""
+    return targets.make_problem(32, m=1.5 + 0.01j, x=5.0)
+
+
+def c1_directions(prob, r):
+    """SCAT's selected directions for RHS r: theta 0..180 deg at 1 deg in the
+    phi = 0 and 90 deg planes (362 directions), float32 AKS, EM1, EM2."""
+    k = prob.incid[r].k
+    aks, em1, em2 = targets.scattering_planes(k, prob.incid[r].e)
+    return aks.astype(np.float32), em1.astype(np.float32), em2.astype(np.float32)
+
+
+def mv64_inputs():
+    """A 64^3 MATVEC case from seed 64: 70 % random occupancy, random x (zero
+    on vacuum sites), CXADIA and CXAOFF, k of modulus ~0.7; and the sample
+    indices and projection vectors its output is stored as."""
+    rng = np.random.default_rng(64)
+    n = 64
+    nat = n ** 3
+    iocc = (rng.random(nat) < 0.7).astype(np.int16)
+    ak = (rng.normal(size=3) * 0.4).astype(np.float32)
+    c = lambda s=1.0: (s * (rng.normal(size=3 * nat) + 1j * rng.normal(size=3 * nat))).astype(np.complex64)  # noqa: E731
+    x, adia, aoff = c(), c(), c(0.3)
+    x[np.tile(iocc == 0, 3)] = 0
+    idx = np.sort(rng.choice(3 * nat, MV64_SAMPLES, replace=False))
+    proj = (rng.normal(size=(MV64_PROJ, 3 * nat)) + 1j * rng.normal(size=(MV64_PROJ, 3 * nat))) / np.sqrt(3 * nat)
+    return (n, n, n), iocc, ak, x, adia, aoff, idx, proj
+
+
+def mv64_summary(y, idx, proj):
+    """What the 64^3 MATVEC output is stored as: seeded samples, the L2 norm and
+    projections onto seeded random vectors (complex128)."""
+    y = np.asarray(y)
+    return y[idx], np.array([np.linalg.norm(y.astype(np.complex128))]), proj @ y.astype(np.complex128)
 
 
 def ref_lib(layout="fft3d"):
@@ -138,5 +186,67 @@ def main():
     print("wrote", OUT, len(fx), "arrays")
 
 
+def main_c1():
+    lib = ref_lib("fft3d")
+    fx = {}
+    # ---- 64^3 MATVEC, both CWHAT
+    dims, iocc, ak, x, adia, aoff, idx, proj = mv64_inputs()
+    nat = int(np.prod(dims))
+    rc = lib.ddscat_cuda_prepare_green_f32(*dims, 0, nat, int(iocc.sum()), 0, 0.0, 0.0, 0.0, *map(float, ak), 1.0, 1.0,
+                                           1.0, _p(iocc))
+    assert rc == 0, lib.ddscat_cuda_last_error()
+    for cw in "NC":
+        y = np.empty_like(x)
+        assert lib.ddscat_cuda_apply_f32(ord(cw), _p(x), _p(y), _p(adia), _p(aoff)) == 0
+        smp, nrm, prj = mv64_summary(y, idx, proj)
+        fx.update({f"M64_{cw}_samples": smp, f"M64_{cw}_norm": nrm, f"M64_{cw}_proj": prj})
+    lib.ddscat_cuda_release()
+    # ---- the small-sphere workload, PBCGS2 per polarisation, EVALQ, SCAT
+    prob = c1_problem()
+    k = prob.incid[0].k.astype(np.float32)
+    rc = lib.ddscat_cuda_prepare_green_f32(32, 32, 32, 0, prob.nat, prob.nat0, 0, 0.0, 0.0, 0.0, *map(float, k), 1.0,
+                                           1.0, 1.0, _p(prob.iocc))
+    assert rc == 0, lib.ddscat_cuda_last_error()
+    aoff = prob.aoff()
+    dx = np.ones(3, dtype=np.float32)
+    x0 = np.array(prob.x0, dtype=np.float32)
+    for r in range(len(prob.incid)):
+        b, adia = prob.rhs(r), prob.adia(r)
+        xs = np.zeros_like(b)
+        it, tole, nc = ct.c_int(), ct.c_float(), ct.c_int()
+        rc = lib.ddscat_cuda_solve_pbcgs2_f32(_p(b), _p(xs), _p(adia), _p(aoff), b.size, C1_MAXIT, C1_TOL,
+                                              ct.byref(it), ct.byref(tole), ct.byref(nc))
+        assert rc == 0, lib.ddscat_cuda_last_error()
+        fx[f"C1_{r}_x"] = np.concatenate([xs[c * prob.nat:(c + 1) * prob.nat][prob.occ] for c in range(3)])
+        fx[f"C1_{r}_meta"] = np.array([it.value, tole.value, nc.value], dtype=np.float64)
+        fx[f"C1_{r}_inputs"] = np.array([b.astype(np.complex128).sum(), adia.astype(np.complex128).sum()])
+        cabs, cext, cpha = ct.c_double(), ct.c_double(), ct.c_double()
+        assert lib.ddscat_cuda_evalq_f32(1, None, None, None, None, *map(float, k), 1.0, ct.byref(cabs),
+                                         ct.byref(cext), ct.byref(cpha)) == 0
+        fx[f"C1_{r}_evalq"] = np.array([cabs.value, cext.value, cpha.value])
+        aks, em1, em2 = c1_directions(prob, r)
+        e01 = prob.incid[r].e.astype(np.complex64)
+        f1 = np.zeros(len(aks), dtype=np.complex64)
+        f2 = np.zeros(len(aks), dtype=np.complex64)
+        cb, cs, cg2 = ct.c_double(), ct.c_double(), ct.c_double()
+        cg = (ct.c_double * 3)()
+        navg = ct.c_int()
+        rc = lib.ddscat_cuda_scat_f32(0, len(aks), _p(k), _p(aks), _p(dx), _p(em1), _p(em2), 1.0, C1_ETASCA,
+                                      _p(e01), _p(x0), ct.byref(cb), ct.byref(cs),
+                                      ct.cast(cg, ct.POINTER(ct.c_double)), ct.byref(cg2), ct.byref(navg), _p(f1),
+                                      _p(f2))
+        assert rc == 0, lib.ddscat_cuda_last_error()
+        fx[f"C1_{r}_scat"] = np.array([cb.value, cs.value, cg[0], cg[1], cg[2], cg2.value, navg.value])
+        fx[f"C1_{r}_f1"] = f1
+        fx[f"C1_{r}_f2"] = f2
+    lib.ddscat_cuda_release()
+    np.savez_compressed(OUT_C1, **fx)
+    print("wrote", OUT_C1, len(fx), "arrays")
+
+
 if __name__ == "__main__":
-    main()
+    which = sys.argv[1] if len(sys.argv) > 1 else "all"
+    if which in ("base", "all"):
+        main()
+    if which in ("c1", "all"):
+        main_c1()

@@ -129,3 +129,36 @@ def test_cext_autograd():
     _, gre, gim = G.cext_and_grad(dda, prob, 0, eps0)
     assert np.allclose(g.numpy().real, gre) and np.allclose(g.numpy().imag, gim)
     dda.release()
+
+
+@pytest.mark.gpu
+def test_ffweights_and_recomputed_forward_adjoint():
+    """ddscat_b200_ffweights_f32 equals the host restatement of the far-field
+    weights (1e-6 of max |w|, host and device outputs), and the adjoint with
+    the forward field recomputed inside the call (ddscat_b200_adjoint_fwd_f32)
+    gives the gradient of the adjoint with a caller-held forward solution
+    (ddscat_b200_adjoint_f32) to 1e-4 of its largest entry."""
+    torch = pytest.importorskip("torch")
+    n = 12
+    prob, mat = targets.voxel_problem(n, x=2.0, seed=5)
+    eps = np.where(mat[prob.occ] == 1, (1.5 + 0.01j) ** 2, (1.2 + 0.0j) ** 2).astype(np.complex128)
+    dda = D.DDA()
+    dda.prepare_green(n, n, n, prob.iocc, prob.incid[0].k)
+    k = prob.incid[0].k
+    aks, em1, em2 = targets.scattering_planes(k, prob.incid[0].e, 45.0, (0.0,))
+    aks2, ems = np.concatenate([aks, aks]), np.concatenate([em1, em2])
+    W = dda.ffweights(aks2, ems, prob.x0)
+    Wh = np.stack(G.farfield_weights(prob, 0, list(aks2), list(ems)))
+    assert np.abs(W - Wh).max() <= 1e-6 * np.abs(Wh).max()
+    Wd = torch.empty(W.shape, dtype=torch.complex64, device="cuda")
+    dda.ffweights(aks2, ems, prob.x0, out=Wd)
+    assert np.abs(Wd.cpu().numpy() - Wh).max() <= 1e-6 * np.abs(Wh).max()
+    b, adia, dadia = (v.astype(np.complex64) for v in G.site_inputs(prob, 0, eps))
+    g2, p, it, tole = dda.adjoint_fwd(b, W, adia, dadia, maxit=2000, tol=1e-6, want_p=True)
+    assert it.shape == (W.shape[0] + 1,) and np.all(tole <= 1e-6)
+    R = W.shape[0]
+    g1, _, _, _ = dda.adjoint(np.repeat(p[None, :], R, axis=0), W, np.repeat(adia[None, :], R, axis=0),
+                              np.repeat(dadia[None, :], R, axis=0), maxit=2000, tol=1e-6)
+    assert np.abs(g2 - g1).max() <= 1e-4 * np.abs(g1).max()
+    assert np.all(g2[:, prob.iocc == 0] == 0)
+    dda.release()

@@ -197,3 +197,33 @@ def test_mueller_f64_matches_oracle_and_f32():
     assert np.abs(m64 - M).max() <= 1e-12 * np.abs(M).max()
     s32, m32 = dda.mueller(k.astype(np.float32), e01, e02, em2.astype(np.float32), *[v.astype(np.complex64) for v in f])
     assert np.abs(m32 - m64).max() <= 1e-6 * np.abs(m64[:, 0, 0]).max()
+
+
+@pytest.mark.gpu
+def test_scat_csca_f64_matches_oracle_and_fp32_scat():
+    """ddscat_b200_scat_csca_f64 gives the oracle's SCAT cross sections (same
+    directions and weights, FP64 sums) to 1e-10 relative, two RHS per call,
+    and agrees with the FP32 SCAT of the same polarisation to the FP32
+    phase-table tolerance (1e-5 relative for Csca, 1e-5 absolute for g)."""
+    prob, dda, out, occ, b, adia = _solved()
+    k = prob.incid[0].k
+    e01 = prob.incid[0].e
+    x64 = np.stack([out.x.astype(np.complex128), 0.5j * out.x.astype(np.complex128)])
+    e01s = np.stack([e01, e01])
+    got = dda.scat_csca_f64(x64, k, e01s, prob.x0, etasca=0.5)
+    pc = O.gather_compact(x64[0], occ, prob.nat)
+    ref = O.scat(pc, occ, prob.nx, prob.ny, 0, k, np.zeros((0, 3)), (1.0, 1.0, 1.0), None, None, 1.0, 0.5, e01,
+                 prob.x0)
+    assert got["navg"][0] == ref["navg"] == got["navg"][1]
+    assert abs(got["csca"][0] - ref["csca"]) <= 1e-10 * ref["csca"]
+    assert np.abs(got["cscag"][0] - np.array(ref["cscag"])).max() <= 1e-10 * ref["csca"]
+    assert abs(got["cscag2"][0] - ref["cscag2"]) <= 1e-10 * ref["csca"]
+    assert abs(got["cbksca"][0] - ref["cbksca"]) <= 1e-10 * ref["csca"]
+    # the second RHS is 0.5i times the first: |0.5|^2 of every cross section
+    assert abs(got["csca"][1] - 0.25 * got["csca"][0]) <= 1e-12 * got["csca"][0]
+    dda.evalq(k, use_resident=1)
+    sc = dda.scat(k, e01, prob.x0, etasca=0.5)
+    assert sc["navg"] == got["navg"][0]
+    assert abs(sc["csca"] - got["csca"][0]) <= 1e-5 * got["csca"][0]
+    assert abs(sc["cscag"][0] / sc["csca"] - got["cscag"][0, 0] / got["csca"][0]) <= 1e-5
+    dda.release()

@@ -9,6 +9,8 @@ Checks per solver, on a seeded 12^3 sphere and a 10x8x6 ellipsoid:
   * iteration count within max(3, 30 %) of the FP64 oracle's;
   * NCOMPTE >= the MATVECs the iteration count implies.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -116,3 +118,32 @@ def test_config_c1_sphere_q_parity():
         assert abs(cext - qe) / abs(qe) < 1e-4
         assert abs(cabs - qa) / abs(qa) < 1e-4
     dda.release()
+
+
+@pytest.mark.gpu
+def test_abi_console_lines_on_by_default(capfd):
+    """The reference entry points print the reference's console lines by
+    default (one per MATVEC with its GPU time, cu:417, and one per iteration,
+    e.g. cu:1085-1092), which DDSCAT users see; level 0 silences them."""
+    prob = targets.make_problem(12, m=1.5 + 0.01j, x=2.0)
+    dda = D.DDA()
+    dda.prepare_green(12, 12, 12, prob.iocc, prob.incid[0].k)
+    b, adia, aoff = prob.rhs(0), prob.adia(0), prob.aoff()
+    try:
+        dda.lib.ddscat_b200_set_verbose(-1)  # the default (DDSCAT_B200_VERBOSE unset: on)
+        if os.environ.get("DDSCAT_B200_VERBOSE", "1") == "0":
+            pytest.skip("DDSCAT_B200_VERBOSE=0 in this environment")
+        capfd.readouterr()
+        out = dda.solve("qmrccg", b, adia, aoff, maxit=200, tol=1e-5)
+        text = capfd.readouterr().out
+        assert " QMRCCG iteration=" in text
+        assert "CUDA MATVEC" in text and "[N,QMRCCG]: GPU=" in text
+        assert text.count("[N,QMRCCG]") == out.ncompte
+        dda.apply(b, adia, aoff)
+        assert "[N,host-copy]: GPU=" in capfd.readouterr().out
+        dda.lib.ddscat_b200_set_verbose(0)
+        dda.solve("qmrccg", b, adia, aoff, maxit=200, tol=1e-5)
+        assert "CUDA MATVEC" not in capfd.readouterr().out
+    finally:
+        dda.lib.ddscat_b200_set_verbose(-1)
+        dda.release()

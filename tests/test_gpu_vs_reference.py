@@ -73,3 +73,76 @@ def test_solver_vs_reference(fx, name):
         fmax = np.abs(fx["B_f1"]).max()
         assert np.abs(sc["f1"] - fx["B_f1"]).max() <= 1e-4 * fmax
     dda.release()
+
+
+# ---- configuration-size fixtures: the small-sphere workload (32^3, PBCGS2,
+# EVALQ, SCAT at ETASCA 0.5 on 362 directions) and a 64^3 MATVEC
+FIX_C1 = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_fixtures_c1.npz")
+
+
+def _gen():
+    import importlib.util
+
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "make_reference_fixtures.py")
+    spec = importlib.util.spec_from_file_location("make_reference_fixtures", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+@pytest.fixture(scope="module")
+def fc1():
+    if not os.path.exists(FIX_C1):
+        pytest.skip("configuration-size reference fixtures not generated")
+    return dict(np.load(FIX_C1))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("layout", ["fft3d", "slices"])
+def test_matvec64_vs_reference(fc1, layout):
+    G = _gen()
+    dims, iocc, ak, x, adia, aoff, idx, proj = G.mv64_inputs()
+    dda = D.DDA(layout)
+    dda.prepare_green(*dims, iocc, ak)
+    for cw in "NC":
+        y = dda.apply(x, adia, aoff, cw)
+        smp, nrm, prj = G.mv64_summary(y, idx, proj)
+        assert _rel(smp, fc1[f"M64_{cw}_samples"]) < 2e-5
+        assert abs(nrm[0] - fc1[f"M64_{cw}_norm"][0]) <= 2e-5 * nrm[0]
+        assert np.abs(prj - fc1[f"M64_{cw}_proj"]).max() <= 2e-5 * nrm[0]
+    dda.release()
+
+
+@pytest.mark.gpu
+def test_c1_workload_vs_reference(fc1):
+    """This library's ABI on the small-sphere workload against the reference's
+    outputs on the same inputs: iteration and MATVEC counts within 20 %,
+    solutions within 20 tol, EVALQ's Q and SCAT's Csca within 1e-4 relative,
+    g within 1e-4, f1/f2 within 1e-4 of max|f| (two converged FP32 iterates of
+    the same recurrence)."""
+    G = _gen()
+    prob = G.c1_problem()
+    k = prob.incid[0].k.astype(np.float32)
+    dda = D.DDA()
+    dda.prepare_green(32, 32, 32, prob.iocc, k)
+    for r in range(2):
+        b, adia = prob.rhs(r), prob.adia(r)
+        out = dda.solve("pbcgs2", b, adia, prob.aoff(), maxit=G.C1_MAXIT, tol=G.C1_TOL)
+        it_ref, tole_ref, nc_ref = fc1[f"C1_{r}_meta"]
+        assert out.rc == 0 and out.tole <= G.C1_TOL
+        assert abs(out.itno - it_ref) <= max(1, 0.2 * it_ref), (out.itno, it_ref)
+        assert abs(out.ncompte - nc_ref) <= max(2, 0.2 * nc_ref), (out.ncompte, nc_ref)
+        xc = np.concatenate([out.x[c * prob.nat:(c + 1) * prob.nat][prob.occ] for c in range(3)])
+        assert _rel(xc, fc1[f"C1_{r}_x"]) < 20 * G.C1_TOL
+        for g, w in zip(dda.evalq(k), fc1[f"C1_{r}_evalq"]):
+            assert abs(g - w) <= 1e-4 * abs(w)
+        aks, em1, em2 = G.c1_directions(prob, r)
+        sc = dda.scat(k, prob.incid[r].e, prob.x0, etasca=G.C1_ETASCA, aks=aks, em1=em1, em2=em2)
+        cb, cs, g0, g1, g2, cg2, navg = fc1[f"C1_{r}_scat"]
+        assert sc["navg"] == int(navg)
+        assert sc["csca"] == pytest.approx(cs, rel=1e-4)
+        assert abs(sc["cscag"][0] / sc["csca"] - g0 / cs) <= 1e-4
+        fmax = max(np.abs(fc1[f"C1_{r}_f1"]).max(), np.abs(fc1[f"C1_{r}_f2"]).max())
+        assert np.abs(sc["f1"] - fc1[f"C1_{r}_f1"]).max() <= 1e-4 * fmax
+        assert np.abs(sc["f2"] - fc1[f"C1_{r}_f2"]).max() <= 1e-4 * fmax
+    dda.release()

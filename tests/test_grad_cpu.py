@@ -36,6 +36,22 @@ class OracleDDA:
             x[r] = self._solve(b[r], adia[r])
         return None
 
+    def adjoint_fwd(self, e, src, adia, dadia, maxit=1000, tol=1e-5, want_p=False):
+        """ddscat_b200_adjoint_fwd_f32: the forward solution of A P = e is
+        recomputed inside; grad[k][j] = -sum_c lam_k[c][j] dadia[c][j] P[c][j]."""
+        p = self._solve(e, adia)
+        nat = self.prob.nat
+        out = np.zeros((src.shape[0], nat), dtype=np.complex128)
+        for k in range(src.shape[0]):
+            lam = self._solve(src[k], adia)
+            t = -(lam * dadia.astype(np.complex128) * p).reshape(3, nat)
+            out[k] = t.sum(axis=0)
+        return out, (p if want_p else None), None, None
+
+    def ffweights(self, aks, ems, x0, e02=1.0, out=None):
+        """ddscat_b200_ffweights_f32: w_k = |aks_k|^3/sqrt(E02) em_k exp(-i aks_k . r_j)."""
+        return np.stack(G.farfield_weights(self.prob, 0, list(aks), list(ems), e02))
+
     def adjoint(self, p, src, adia, dadia, maxit=1000, tol=1e-5):
         """grad[r][j] = -sum_c lam[c][j] dadia[c][j] p[c][j], A lam = src (A^T = A)."""
         nat = self.prob.nat
@@ -64,6 +80,21 @@ def test_ldr_derivative_matches_finite_difference():
     fdi = (G.ldr_inv_alpha(eps0 + 1j * h, kd, khat, inc.e) - G.ldr_inv_alpha(eps0 - 1j * h, kd, khat, inc.e)) / (2j * h)
     an = G.ldr_dinv_alpha(eps0, kd, khat, inc.e)
     assert np.allclose(fd, an, rtol=1e-7) and np.allclose(fdi, an, rtol=1e-7)  # holomorphic in eps
+
+
+@pytest.mark.parametrize("cmdpol", targets.PRESCRIPTIONS)
+def test_prescription_derivative_matches_finite_difference(cmdpol):
+    prob, eps0 = _problem()
+    inc = prob.incid[0]
+    khat = inc.k / np.linalg.norm(inc.k)
+    kd = float(np.linalg.norm(inc.k))
+    f = lambda e: targets.inv_alpha_eps(e, kd, khat, inc.e, cmdpol)  # noqa: E731
+    h = 1e-6
+    fd = (f(eps0 + h) - f(eps0 - h)) / (2 * h)
+    fdi = (f(eps0 + 1j * h) - f(eps0 - 1j * h)) / (2j * h)
+    an = targets.dinv_alpha_deps(eps0, kd, khat, inc.e, cmdpol)
+    assert an.shape == (3, eps0.size)
+    assert np.allclose(fd, an, rtol=1e-7) and np.allclose(fdi, an, rtol=1e-7)
 
 
 def _cext(dda, prob, eps):

@@ -101,3 +101,74 @@ def test_oracle_evalq_and_scat_match_reference(fx):
     fmax = np.abs(fx["B_f1"]).max()
     assert np.abs(sc["f1"] - fx["B_f1"]).max() <= 2e-5 * fmax
     assert np.abs(sc["f2"] - fx["B_f2"]).max() <= 2e-5 * fmax
+
+
+# ---- configuration-size fixtures (reference_fixtures_c1.npz): the small-sphere
+# workload and a 64^3 MATVEC, inputs regenerated from seeds by the fixture script
+FIX_C1 = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_fixtures_c1.npz")
+
+
+def _gen():
+    import importlib.util
+
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "make_reference_fixtures.py")
+    spec = importlib.util.spec_from_file_location("make_reference_fixtures", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+@pytest.fixture(scope="module")
+def fc1():
+    if not os.path.exists(FIX_C1):
+        pytest.skip("configuration-size reference fixtures not generated")
+    return dict(np.load(FIX_C1))
+
+
+def test_oracle_matvec64_matches_reference(fc1):
+    """64^3 MATVEC, 'N' and 'C': the seeded samples, the norm and the random
+    projections of the reference's output (2e-5, complex FP32 reference)."""
+    G = _gen()
+    dims, iocc, ak, x, adia, aoff, idx, proj = G.mv64_inputs()
+    op = O.Operator.from_params(O.GreenParams(*dims, ak=tuple(float(v) for v in ak)), iocc)
+    for cw in "NC":
+        y = op.apply_full(x, adia, aoff, cw)
+        smp, nrm, prj = G.mv64_summary(y, idx, proj)
+        assert _rel(smp, fc1[f"M64_{cw}_samples"]) < 2e-5
+        assert abs(nrm[0] - fc1[f"M64_{cw}_norm"][0]) <= 2e-5 * nrm[0]
+        assert np.abs(prj - fc1[f"M64_{cw}_proj"]).max() <= 2e-5 * nrm[0]
+
+
+def test_oracle_c1_matches_reference(fc1):
+    """The small-sphere workload solved by the reference (PBCGS2, both
+    polarisations): its solutions have FP64 true residuals <= 1.2 tol under
+    the oracle's operator, and the oracle's EVALQ (1e-6) and SCAT (2e-5:
+    Csca, g, f1/f2 on 362 directions) of those solutions equal the
+    reference's."""
+    G = _gen()
+    prob = G.c1_problem()
+    k = prob.incid[0].k
+    op = O.Operator.from_params(O.GreenParams(32, 32, 32, ak=tuple(float(np.float32(a)) for a in k)), prob.iocc)
+    occ = op.occ
+    for r in range(2):
+        b, adia = prob.rhs(r), prob.adia(r)
+        assert np.allclose(fc1[f"C1_{r}_inputs"], [b.astype(np.complex128).sum(), adia.astype(np.complex128).sum()],
+                           rtol=1e-12), "the fixture was made from other inputs"
+        bc = O.gather_compact(b, occ, prob.nat).astype(np.complex128)
+        ac = O.gather_compact(adia, occ, prob.nat).astype(np.complex128)
+        oc = np.zeros_like(ac)
+        xr = fc1[f"C1_{r}_x"].astype(np.complex128)
+        it_ref, tole_ref, nc_ref = fc1[f"C1_{r}_meta"]
+        assert tole_ref <= G.C1_TOL
+        assert np.linalg.norm(bc - op.apply_compact(xr, ac, oc)) / np.linalg.norm(bc) <= 1.2 * G.C1_TOL
+        for g, w in zip(O.evalq(bc, xr, ac, oc, k, 1.0), fc1[f"C1_{r}_evalq"]):
+            assert abs(g - w) <= 1e-6 * abs(w)
+        aks, em1, em2 = G.c1_directions(prob, r)
+        sc = O.scat(xr, occ, 32, 32, 0, k, aks, (1, 1, 1), em1, em2, 1.0, G.C1_ETASCA, prob.incid[r].e, prob.x0)
+        cb, cs, g0, g1, g2, cg2, navg = fc1[f"C1_{r}_scat"]
+        assert sc["navg"] == int(navg)
+        assert sc["csca"] == pytest.approx(cs, rel=2e-5)
+        assert abs(sc["cscag"][0] / sc["csca"] - g0 / cs) <= 2e-5
+        fmax = max(np.abs(fc1[f"C1_{r}_f1"]).max(), np.abs(fc1[f"C1_{r}_f2"]).max())
+        assert np.abs(sc["f1"] - fc1[f"C1_{r}_f1"]).max() <= 2e-5 * fmax
+        assert np.abs(sc["f2"] - fc1[f"C1_{r}_f2"]).max() <= 2e-5 * fmax

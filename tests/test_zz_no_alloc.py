@@ -1,12 +1,12 @@
 """The allocation-free MATVEC entry point, ddscat_b200_apply_noalloc_f32.
 
 It exists for callers that cannot allocate device memory where they need the
-operator (code inside CUDA stream capture, allocation-free real-time loops,
-applications that give all device memory to their own pool).  It must return
+operator: real-time loops that forbid allocation once they run, and
+applications that give all device memory to their own pool.  It must return
 the same y as ddscat_cuda_apply_f32 on the same inputs (FP32 tolerance 2e-5
 relative, as in test_gpu_matvec.py) on two calls in a row, leave the free
-device memory unchanged, and reject targets larger than its fixed scratch.
-This file is named to be collected last."""
+device memory unchanged, and reject targets whose padded FFT grid does not fit
+its fixed scratch.  This file is named to be collected last."""
 import ctypes as ct
 
 import numpy as np
@@ -28,8 +28,10 @@ def _inputs(dims, seed):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("dims", [(16, 16, 16), (12, 10, 9)])
+@pytest.mark.parametrize("dims", [(16, 16, 16), (12, 10, 9), (18, 18, 18)])
 def test_apply_noalloc_matches_apply(dims):
+    """16^3: x-first pipeline with M = 2n; 12x10x9: z-first pipeline; 18^3: x-first
+    on padded FFT lengths (36 -> 48)."""
     torch = pytest.importorskip("torch")
     iocc, ak, x1, x2, adia, aoff = _inputs(dims, 7)
     dda = D.DDA()
@@ -57,9 +59,12 @@ def test_apply_noalloc_matches_apply(dims):
 
 
 @pytest.mark.gpu
-def test_apply_noalloc_rejects_large_target():
+@pytest.mark.parametrize("dims", [(72, 72, 72), (72, 72, 64)])
+def test_apply_noalloc_rejects_large_target(dims):
+    """72^3 has NAT = 373,248 > 349,525; 72x72x64 (NAT = 331,776) is under that
+    bound but its x and y axes are padded from 144 to 192, so its scratch
+    (9.7 M complex floats) exceeds the fixed 6.29 M as well."""
     torch = pytest.importorskip("torch")
-    dims = (72, 72, 72)  # NAT = 373,248 > 349,525
     nat = int(np.prod(dims))
     dda = D.DDA()
     dda.prepare_green(*dims, np.ones(nat, dtype=np.int16), (0.3, 0.0, 0.0))
