@@ -4,6 +4,8 @@
 // small D2H per group of inner products) are shared by all RHS of the batch.
 #include <algorithm>
 #include <complex>
+#include <condition_variable>
+#include <mutex>
 #include "batch.h"
 #include <cstdio>
 #include <cstdlib>
@@ -1377,130 +1379,145 @@ struct PGHost {
   std::vector<int> it, live, status;
 };
 
-// Runs the PBCGS2 iterations (residual replacement) from the host state hs
-// until no RHS is active; w: rr, r0, r1, r2, u0, u1, u2, XP, BP, X, sy.
-template <typename T>
-static int pbcgs2_graph_loop(BatchIO<T>& io, BatchOps<T>& ops, std::vector<int>& nc, cplx<T>* const* w, PGHost& hs,
-                             double mv_ms_per_rhs) {
+// One target's device-driven PBCGS2 iterations (residual replacement) as a
+// graph body: init() moves the host state hs onto the GPU, capture() records one
+// iteration into the capture its stream st has joined (its IF-node bodies on
+// st2), pg_run() launches the captured iteration until no RHS is active, and
+// readback() brings the state back; w: rr, r0, r1, r2, u0, u1, u2, XP, BP, X, sy.
+template <typename T> struct PGGraph {
   using C = cplx<T>;
-  const int R = io.R, n = io.n;
-  C *rr = w[0], *r[3] = {w[1], w[2], w[3]}, *u[3] = {w[4], w[5], w[6]}, *XP = w[7], *BP = w[8], *X = w[9], *sy = w[10];
-  const size_t nz2 = (size_t)(6 + 7 + 2) * R, nd = (size_t)5 * R, ni = (size_t)11 * R + 3;
+  BatchIO<T>* io = nullptr;
+  BatchOps<T>* ops = nullptr;
+  std::vector<int>* nc = nullptr;
+  PGHost* hs = nullptr;
+  C* w[11] = {};
+  double mv_ms_per_rhs = 0.0;
+  int R = 0, n = 0;
+  size_t nz2 = 0, nd = 0, ni = 0;
   unsigned char* blk = nullptr;
-  cudaError_t e = cudaMalloc((void**)&blk, nz2 * sizeof(double2) + nd * sizeof(double) + ni * sizeof(int));
-  if (e != cudaSuccess) { set_cuda_error("graph solve state", e); return 1; }
-  PGState S;
-  double2* z = reinterpret_cast<double2*>(blk);
-  double2** zp[6] = {&S.alpha, &S.omega, &S.sigma, &S.rho0, &S.rho1, &S.beta};
-  for (int k = 0; k < 6; ++k) *zp[k] = z + (size_t)k * R;
-  S.co = z + (size_t)6 * R;
-  S.one = z + (size_t)13 * R;
-  S.mone = z + (size_t)14 * R;
-  double* dd = reinterpret_cast<double*>(z + nz2);
-  double** dp[5] = {&S.rnrm0, &S.rnrm, &S.mxx, &S.mxr, &S.resid};
-  for (int k = 0; k < 5; ++k) *dp[k] = dd + (size_t)k * R;
-  int* ii = reinterpret_cast<int*>(dd + nd);
-  int** ip[11] = {&S.it, &S.live, &S.status, &S.nc, &S.I, &S.CK, &S.RP, &S.RC, &S.XD, &S.RCMP, &S.XPDT};
-  for (int k = 0; k < 11; ++k) *ip[k] = ii + (size_t)k * R;
-  S.active = ii + (size_t)11 * R;
-  S.checks = S.active + 1;
-  S.updates = S.active + 2;
-  std::vector<double2> hz(nz2, make_double2(0, 0));
-  const std::vector<Z>* zs[6] = {&hs.alpha, &hs.omega, &hs.sigma, &hs.rho0, &hs.rho1, &hs.beta};
-  for (int k = 0; k < 6; ++k)
-    for (int i = 0; i < R; ++i) hz[(size_t)k * R + i] = dz((*zs[k])[i]);
-  for (int i = 0; i < R; ++i) { hz[(size_t)13 * R + i] = make_double2(1, 0); hz[(size_t)14 * R + i] = make_double2(-1, 0); }
-  std::vector<double> hd0(nd);
-  const std::vector<double>* ds[5] = {&hs.rnrm0, &hs.rnrm, &hs.mxx, &hs.mxr, &hs.resid};
-  for (int k = 0; k < 5; ++k)
-    for (int i = 0; i < R; ++i) hd0[(size_t)k * R + i] = (*ds[k])[i];
-  std::vector<int> hi0(ni, 0);
-  for (int i = 0; i < R; ++i) {
-    hi0[i] = hs.it[i]; hi0[R + i] = hs.live[i]; hi0[2 * R + i] = hs.status[i]; hi0[3 * R + i] = nc[i];
-  }
-  cudaStream_t st = nullptr, st2 = nullptr;
-  cudaStreamSynchronize(ops.stream);
-  e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking);
-  // uploads ordered on st (see qmr_graph_loop)
-  if (e == cudaSuccess) e = cudaMemcpyAsync(z, hz.data(), nz2 * sizeof(double2), cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(dd, hd0.data(), nd * sizeof(double), cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(ii, hi0.data(), ni * sizeof(int), cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) {
-    if (st) cudaStreamDestroy(st);
-    if (st2) cudaStreamDestroy(st2);
-    cudaFree(blk);
-    set_cuda_error("graph solve streams and state", e);
-    return 1;
-  }
-  Engine<T>& eng = *io.eng;
-  const cudaStream_t eng_st = eng.stream;
-  MvArgs<T> mv;
-  mv.x_rs = n; mv.y_rs = n; mv.io_full = 0;
-  mv.adia = io.adia; mv.aoff = io.aoff; mv.a_rs = n; mv.a_full = 0; mv.conj = 0; mv.nrhs = R;
-  const double tol = io.tol;
-  const int maxit = io.maxit;
-  const unsigned gb = (unsigned)std::max<size_t>(1, std::min<size_t>(ceil_div(n, BT), std::max(1, 2368 / R)));
-  auto lin = [&](cudaStream_t s_, C* d, const double2* cd, const C* a, const double2* ca, const C* b,
-                 const double2* cb, const int* m) {
-    kb_lin<C><<<dim3(gb, R), BT, 0, s_>>>(n, d, cd, a, ca, b, cb, m);
-    note_launch();
-  };
-  auto dots = [&](cudaStream_t s_, int K, const C* const* a, const C* const* b, const int* m) {
-    BDot<T> sp{};
-    sp.K = K; sp.mode = 0;
-    for (int k = 0; k < K; ++k) { sp.a[k] = a[k]; sp.b[k] = b[k]; sp.conj[k] = 1; }
-    kb_dots<T><<<dim3(ops.nb, R), BT, 0, s_>>>(n, sp, m, ops.d_part, ops.d_out, ops.d_cnt);
-    note_launch();
-  };
-  auto matvec = [&](const C* in, C* out, const int* m) {
-    mv.x = in; mv.y = out; mv.mask = m;
-    return eng.matvec(mv);
-  };
-  // an IF node at the capture point of st whose body is captured on st2 by body()
-  auto if_node = [&](cudaGraphConditionalHandle h, auto body) -> cudaError_t {
-    cudaStreamCaptureStatus cs;
-    cudaGraph_t g = nullptr;
-    const cudaGraphNode_t* deps = nullptr;
-    size_t ndeps = 0;
-    cudaError_t e_ = cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &ndeps);
-    cudaGraphNodeParams cp{};
-    cp.type = cudaGraphNodeTypeConditional;
-    cp.conditional.handle = h;
-    cp.conditional.type = cudaGraphCondTypeIf;
-    cp.conditional.size = 1;
-    cudaGraphNode_t cnode = nullptr;
-    if (e_ == cudaSuccess) e_ = cudaGraphAddNode(&cnode, g, deps, ndeps, &cp);
-    if (e_ == cudaSuccess) e_ = cudaStreamUpdateCaptureDependencies(st, &cnode, 1, cudaStreamSetCaptureDependencies);
-    if (e_ != cudaSuccess) return e_;
-    e_ = cudaStreamBeginCaptureToGraph(st2, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
-                                       cudaStreamCaptureModeThreadLocal);
-    if (e_ != cudaSuccess) return e_;
-    eng.stream = st2;
-    body();
-    eng.stream = st;
-    cudaGraph_t body_out = nullptr;
-    return cudaStreamEndCapture(st2, &body_out);
-  };
-  int rc = 0;
-  eng.stream = st;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
+  double* dd = nullptr;
+  int* ii = nullptr;
+  PGState S{};
+  cudaStream_t st = nullptr, st2 = nullptr, eng_st = nullptr;
   unsigned long long kernels_a = 0, kernels_b = 0, kernels_c = 0;
-  {
-    e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+  long long launches = 0;  // set by pg_run
+
+  int init(BatchIO<T>& io_, BatchOps<T>& ops_, std::vector<int>& nc_, C* const* w_, PGHost& hs_, double per_rhs) {
+    io = &io_; ops = &ops_; nc = &nc_; hs = &hs_; mv_ms_per_rhs = per_rhs;
+    for (int k = 0; k < 11; ++k) w[k] = w_[k];
+    R = io->R; n = io->n;
+    nz2 = (size_t)(6 + 7 + 2) * R; nd = (size_t)5 * R; ni = (size_t)11 * R + 3;
+    cudaError_t e = cudaMalloc((void**)&blk, nz2 * sizeof(double2) + nd * sizeof(double) + ni * sizeof(int));
+    if (e != cudaSuccess) { set_cuda_error("graph solve state", e); return 1; }
+    double2* z = reinterpret_cast<double2*>(blk);
+    double2** zp[6] = {&S.alpha, &S.omega, &S.sigma, &S.rho0, &S.rho1, &S.beta};
+    for (int k = 0; k < 6; ++k) *zp[k] = z + (size_t)k * R;
+    S.co = z + (size_t)6 * R;
+    S.one = z + (size_t)13 * R;
+    S.mone = z + (size_t)14 * R;
+    dd = reinterpret_cast<double*>(z + nz2);
+    double** dp[5] = {&S.rnrm0, &S.rnrm, &S.mxx, &S.mxr, &S.resid};
+    for (int k = 0; k < 5; ++k) *dp[k] = dd + (size_t)k * R;
+    ii = reinterpret_cast<int*>(dd + nd);
+    int** ip[11] = {&S.it, &S.live, &S.status, &S.nc, &S.I, &S.CK, &S.RP, &S.RC, &S.XD, &S.RCMP, &S.XPDT};
+    for (int k = 0; k < 11; ++k) *ip[k] = ii + (size_t)k * R;
+    S.active = ii + (size_t)11 * R;
+    S.checks = S.active + 1;
+    S.updates = S.active + 2;
+    std::vector<double2> hz(nz2, make_double2(0, 0));
+    const std::vector<Z>* zs[6] = {&hs->alpha, &hs->omega, &hs->sigma, &hs->rho0, &hs->rho1, &hs->beta};
+    for (int k = 0; k < 6; ++k)
+      for (int i = 0; i < R; ++i) hz[(size_t)k * R + i] = dz((*zs[k])[i]);
+    for (int i = 0; i < R; ++i) { hz[(size_t)13 * R + i] = make_double2(1, 0); hz[(size_t)14 * R + i] = make_double2(-1, 0); }
+    std::vector<double> hd0(nd);
+    const std::vector<double>* ds[5] = {&hs->rnrm0, &hs->rnrm, &hs->mxx, &hs->mxr, &hs->resid};
+    for (int k = 0; k < 5; ++k)
+      for (int i = 0; i < R; ++i) hd0[(size_t)k * R + i] = (*ds[k])[i];
+    std::vector<int> hi0(ni, 0);
+    for (int i = 0; i < R; ++i) {
+      hi0[i] = hs->it[i]; hi0[R + i] = hs->live[i]; hi0[2 * R + i] = hs->status[i]; hi0[3 * R + i] = (*nc)[i];
+    }
+    cudaStreamSynchronize(ops->stream);
+    e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking);
+    // uploads ordered on st (see qmr_graph_loop)
+    if (e == cudaSuccess) e = cudaMemcpyAsync(z, hz.data(), nz2 * sizeof(double2), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dd, hd0.data(), nd * sizeof(double), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ii, hi0.data(), ni * sizeof(int), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) { set_cuda_error("graph solve streams and state", e); return 1; }
+    eng_st = io->eng->stream;
+    return 0;
+  }
+
+  // one iteration into the capture stream st has joined
+  int capture() {
+    const int R_ = R, n_ = n;
+    Engine<T>& eng = *io->eng;
+    C *rr = w[0], *r[3] = {w[1], w[2], w[3]}, *u[3] = {w[4], w[5], w[6]}, *XP = w[7], *BP = w[8], *X = w[9],
+      *sy = w[10];
+    MvArgs<T> mv;
+    mv.x_rs = n_; mv.y_rs = n_; mv.io_full = 0;
+    mv.adia = io->adia; mv.aoff = io->aoff; mv.a_rs = n_; mv.a_full = 0; mv.conj = 0; mv.nrhs = R_;
+    const double tol = io->tol;
+    const int maxit = io->maxit;
+    const unsigned gb = (unsigned)std::max<size_t>(1, std::min<size_t>(ceil_div(n_, BT), std::max(1, 2368 / R_)));
+    BatchOps<T>& op = *ops;
+    auto lin = [&](cudaStream_t s_, C* d, const double2* cd, const C* a, const double2* ca, const C* b,
+                   const double2* cb, const int* m) {
+      kb_lin<C><<<dim3(gb, R_), BT, 0, s_>>>(n_, d, cd, a, ca, b, cb, m);
+      note_launch();
+    };
+    auto dots = [&](cudaStream_t s_, int K, const C* const* a, const C* const* b, const int* m) {
+      BDot<T> sp{};
+      sp.K = K; sp.mode = 0;
+      for (int k = 0; k < K; ++k) { sp.a[k] = a[k]; sp.b[k] = b[k]; sp.conj[k] = 1; }
+      kb_dots<T><<<dim3(op.nb, R_), BT, 0, s_>>>(n_, sp, m, op.d_part, op.d_out, op.d_cnt);
+      note_launch();
+    };
+    auto matvec = [&](const C* in, C* out, const int* m) {
+      mv.x = in; mv.y = out; mv.mask = m;
+      return eng.matvec(mv);
+    };
+    // an IF node at the capture point of st whose body is captured on st2 by body()
+    auto if_node = [&](cudaGraphConditionalHandle h, auto body) -> cudaError_t {
+      cudaStreamCaptureStatus cs;
+      cudaGraph_t g = nullptr;
+      const cudaGraphNode_t* deps = nullptr;
+      size_t ndeps = 0;
+      cudaError_t e_ = cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &ndeps);
+      cudaGraphNodeParams cp{};
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = h;
+      cp.conditional.type = cudaGraphCondTypeIf;
+      cp.conditional.size = 1;
+      cudaGraphNode_t cnode = nullptr;
+      if (e_ == cudaSuccess) e_ = cudaGraphAddNode(&cnode, g, deps, ndeps, &cp);
+      if (e_ == cudaSuccess) e_ = cudaStreamUpdateCaptureDependencies(st, &cnode, 1, cudaStreamSetCaptureDependencies);
+      if (e_ != cudaSuccess) return e_;
+      e_ = cudaStreamBeginCaptureToGraph(st2, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                         cudaStreamCaptureModeThreadLocal);
+      if (e_ != cudaSuccess) return e_;
+      eng.stream = st2;
+      body();
+      eng.stream = st;
+      cudaGraph_t body_out = nullptr;
+      return cudaStreamEndCapture(st2, &body_out);
+    };
+    int rc = 0;
+    eng.stream = st;
     cudaStreamCaptureStatus cs;
     cudaGraph_t g = nullptr;
     const cudaGraphNode_t* deps = nullptr;
     size_t ndeps = 0;
     cudaGraphConditionalHandle hck = 0, hrc = 0;
-    if (e == cudaSuccess) e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &ndeps);
+    cudaError_t e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &ndeps);
+    if (e == cudaSuccess && cs != cudaStreamCaptureStatusActive) e = cudaErrorStreamCaptureInvalidated;
     if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&hck, g, 0, cudaGraphCondAssignDefault);
     if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&hrc, g, 0, cudaGraphCondAssignDefault);
     unsigned long long c0 = launch_total();
     if (e == cudaSuccess) {
-      k_pg_begin<<<1, 256, 0, st>>>(R, maxit, tol, S);
+      k_pg_begin<<<1, 256, 0, st>>>(R_, maxit, tol, S);
       note_launch();
       for (int k = 1; k <= 2 && !rc; ++k) {
         {
@@ -1508,7 +1525,7 @@ static int pbcgs2_graph_loop(BatchIO<T>& io, BatchOps<T>& ops, std::vector<int>&
           const C* B1[1] = {r[k - 1]};
           dots(st, 1, A1, B1, S.I);
         }
-        k_pg_rho<<<1, 256, 0, st>>>(R, S, ops.d_out);
+        k_pg_rho<<<1, 256, 0, st>>>(R_, S, op.d_out);
         note_launch();
         for (int j = 0; j < k; ++j) lin(st, u[j], S.co, r[j], S.one, nullptr, nullptr, S.I);
         if ((rc = matvec(u[k - 1], u[k], S.I))) break;
@@ -1517,28 +1534,28 @@ static int pbcgs2_graph_loop(BatchIO<T>& io, BatchOps<T>& ops, std::vector<int>&
           const C* B1[1] = {u[k]};
           dots(st, 1, A1, B1, S.I);
         }
-        k_pg_sigma<<<1, 256, 0, st>>>(R, S, ops.d_out);
+        k_pg_sigma<<<1, 256, 0, st>>>(R_, S, op.d_out);
         note_launch();
-        lin(st, X, S.one, u[0], S.co + R, nullptr, nullptr, S.I);
-        for (int j = 0; j < k; ++j) lin(st, r[j], S.one, u[j + 1], S.co + 2 * R, nullptr, nullptr, S.I);
+        lin(st, X, S.one, u[0], S.co + R_, nullptr, nullptr, S.I);
+        for (int j = 0; j < k; ++j) lin(st, r[j], S.one, u[j + 1], S.co + 2 * R_, nullptr, nullptr, S.I);
         if ((rc = matvec(r[k - 1], r[k], S.I))) break;
         {
           const C* A1[1] = {r[0]};
           dots(st, 1, A1, A1, S.I);
         }
-        k_pg_rnrm<<<1, 256, 0, st>>>(R, S, ops.d_out);
+        k_pg_rnrm<<<1, 256, 0, st>>>(R_, S, op.d_out);
         note_launch();
       }
       if (!rc) {
         const C* A6[6] = {r[0], r[1], r[1], r[2], r[2], r[2]};
         const C* B6[6] = {r[0], r[0], r[1], r[0], r[1], r[2]};
         dots(st, 6, A6, B6, S.I);
-        k_pg_gram<<<1, 64, 0, st>>>(R, S, ops.d_out);
+        k_pg_gram<<<1, 64, 0, st>>>(R_, S, op.d_out);
         note_launch();
-        lin(st, u[0], S.one, u[1], S.co + 5 * R, u[2], S.co + 6 * R, S.I);
-        lin(st, X, S.one, r[0], S.co + 3 * R, r[1], S.co + 4 * R, S.I);
-        lin(st, r[0], S.one, r[1], S.co + 5 * R, r[2], S.co + 6 * R, S.I);
-        k_pg_post<<<1, 32, 0, st>>>(R, tol, S, hck);
+        lin(st, u[0], S.one, u[1], S.co + 5 * R_, u[2], S.co + 6 * R_, S.I);
+        lin(st, X, S.one, r[0], S.co + 3 * R_, r[1], S.co + 4 * R_, S.I);
+        lin(st, r[0], S.one, r[1], S.co + 5 * R_, r[2], S.co + 6 * R_, S.I);
+        k_pg_post<<<1, 32, 0, st>>>(R_, tol, S, hck);
         note_launch();
         kernels_a = launch_total() - c0;
         // IF node 1: the reliable-residual check with residual replacement
@@ -1547,16 +1564,16 @@ static int pbcgs2_graph_loop(BatchIO<T>& io, BatchOps<T>& ops, std::vector<int>&
           if (!rc) rc = matvec(X, sy, S.CK);
           BDot<T> dn{};
           dn.K = 2; dn.mode = 1; dn.a[0] = BP; dn.b[0] = sy; dn.c[0] = r[0];
-          kb_dots<T><<<dim3(ops.nb, R), BT, 0, st2>>>(n, dn, S.CK, ops.d_part, ops.d_out, ops.d_cnt);
+          kb_dots<T><<<dim3(op.nb, R_), BT, 0, st2>>>(n_, dn, S.CK, op.d_part, op.d_out, op.d_cnt);
           note_launch();
-          k_pg_check<<<1, 256, 0, st2>>>(R, tol, S, ops.d_out);
+          k_pg_check<<<1, 256, 0, st2>>>(R_, tol, S, op.d_out);
           note_launch();
           lin(st2, r[0], nullptr, BP, S.one, sy, S.mone, S.RP);
         });
         kernels_b = launch_total() - c1;
         if (e == cudaSuccess) {
           const unsigned long long c2 = launch_total();
-          k_pg_rc<<<1, 32, 0, st>>>(R, S, hrc);
+          k_pg_rc<<<1, 32, 0, st>>>(R_, S, hrc);
           note_launch();
           kernels_a += launch_total() - c2;
           // IF node 2: the reliable update of r_0 (and of the solution shift)
@@ -1567,67 +1584,191 @@ static int pbcgs2_graph_loop(BatchIO<T>& io, BatchOps<T>& ops, std::vector<int>&
             lin(st2, XP, S.one, X, S.one, nullptr, nullptr, S.XD);
             lin(st2, X, nullptr, nullptr, nullptr, nullptr, nullptr, S.XD);
             lin(st2, BP, nullptr, r[0], S.one, nullptr, nullptr, S.XD);
-            k_pg_rcpost<<<1, 256, 0, st2>>>(R, S);
+            k_pg_rcpost<<<1, 256, 0, st2>>>(R_, S);
             note_launch();
           });
           kernels_c = launch_total() - c3;
         }
         if (e == cudaSuccess) {
-          k_pg_count<<<1, 32, 0, st>>>(R, maxit, tol, S);
+          k_pg_count<<<1, 32, 0, st>>>(R_, maxit, tol, S);
           note_launch();
           kernels_a += 1;
         }
       }
     }
-    cudaGraph_t g_out = nullptr;
-    const cudaError_t e2 = cudaStreamEndCapture(st, &g_out);
-    if (e == cudaSuccess) e = e2;
-    graph = g_out;
-    if (e == cudaSuccess && !rc) e = cudaGraphInstantiate(&exec, graph, 0);
-    if (e != cudaSuccess) { set_cuda_error("graph solve capture", e); rc = 1; }
+    eng.stream = eng_st;
+    if (e != cudaSuccess) { set_cuda_error("graph solve capture", e); return 1; }
+    return rc;
   }
-  long long launches = 0;
-  int checks = 0, updates = 0;
-  if (!rc) {
-    int* h_cnt = nullptr;
-    e = cudaMallocHost((void**)&h_cnt, 3 * sizeof(int));
-    const long long cap = (long long)maxit + 64;  // every RHS stops at maxit; the loop is bounded
-    while (e == cudaSuccess && launches < cap) {
-      for (int k = 0; k < 4 && e == cudaSuccess; ++k, ++launches) e = cudaGraphLaunch(exec, st);
-      if (e == cudaSuccess) e = cudaMemcpyAsync(h_cnt, S.active, 3 * sizeof(int), cudaMemcpyDeviceToHost, st);
-      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-      if (e != cudaSuccess || h_cnt[0] == 0) break;
-    }
-    if (e == cudaSuccess) { checks = h_cnt[1]; updates = h_cnt[2]; }
-    cudaFreeHost(h_cnt);
-    if (e != cudaSuccess) { set_cuda_error("graph solve", e); rc = 1; }
-    note_launch((unsigned long long)launches * kernels_a + (unsigned long long)checks * kernels_b +
-                (unsigned long long)updates * kernels_c);
-  }
-  if (!rc) {
+
+  // state back to the host after pg_run
+  int readback() {
     std::vector<double> hd(nd);
     std::vector<int> hi(ni);
-    e = cudaMemcpy(hd.data(), dd, nd * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaError_t e = cudaMemcpy(hd.data(), dd, nd * sizeof(double), cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(hi.data(), ii, ni * sizeof(int), cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) { set_cuda_error("graph solve state", e); rc = 1; }
+    if (e != cudaSuccess) { set_cuda_error("graph solve state", e); return 1; }
+    const int checks = hi[(size_t)11 * R + 1], updates = hi[(size_t)11 * R + 2];
+    note_launch((unsigned long long)launches * kernels_a + (unsigned long long)checks * kernels_b +
+                (unsigned long long)updates * kernels_c);
     long long mv_rhs = 0;
-    for (int i = 0; i < R && !rc; ++i) {
-      hs.resid[i] = hd[(size_t)4 * R + i];
-      hs.it[i] = hi[i]; hs.live[i] = hi[R + i]; hs.status[i] = hi[2 * R + i];
-      mv_rhs += hi[3 * R + i] - nc[i];
-      nc[i] = hi[3 * R + i];
+    for (int i = 0; i < R; ++i) {
+      hs->resid[i] = hd[(size_t)4 * R + i];
+      hs->it[i] = hi[i]; hs->live[i] = hi[R + i]; hs->status[i] = hi[2 * R + i];
+      mv_rhs += hi[3 * R + i] - (*nc)[i];
+      (*nc)[i] = hi[3 * R + i];
     }
-    io.matvec_rhs += mv_rhs;
-    io.matvec_calls += (int)(4 * launches + checks + updates);
-    io.matvec_ms += mv_ms_per_rhs * (double)mv_rhs;
+    io->matvec_rhs += mv_rhs;
+    io->matvec_calls += (int)(4 * launches + checks + updates);
+    io->matvec_ms += mv_ms_per_rhs * (double)mv_rhs;
+    return 0;
   }
+
+  void release() {
+    if (st) { cudaStreamSynchronize(st); cudaStreamDestroy(st); }
+    if (st2) cudaStreamDestroy(st2);
+    cudaFree(blk);
+    st = st2 = nullptr;
+    blk = nullptr;
+  }
+};
+
+// sum of the active-RHS counts of every branch
+__global__ void k_pg_sum_active(int* const* act, int nb, int* out) {
+  if (threadIdx.x != 0) return;
+  int c = 0;
+  for (int b = 0; b < nb; ++b) c += *act[b];
+  *out = c;
+}
+
+// One CUDA graph whose branches are the iterations of the given targets
+// (independent of one another: fork from a root stream, join back), launched
+// once per Krylov step until no RHS of any branch is active; the host reads the
+// summed active count every 4 launches.  Bounded by the largest maxit + 64
+// launches (every RHS stops at its maxit).
+template <typename T> int pg_run(const std::vector<PGGraph<T>*>& gs) {
+  if (gs.empty()) return 0;
+  const int nb = (int)gs.size();
+  cudaStream_t root = nullptr;
+  int** d_act = nullptr;
+  int* d_sum = nullptr;
+  int* h_sum = nullptr;
+  std::vector<cudaEvent_t> evs;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int rc = 0;
+  cudaError_t e = cudaStreamCreateWithFlags(&root, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&d_act, (size_t)nb * sizeof(int*) + sizeof(int));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&h_sum, sizeof(int));
+  if (e == cudaSuccess) {
+    d_sum = reinterpret_cast<int*>(d_act + nb);
+    std::vector<int*> ha(nb);
+    for (int b = 0; b < nb; ++b) ha[b] = gs[b]->S.active;
+    e = cudaMemcpy(d_act, ha.data(), (size_t)nb * sizeof(int*), cudaMemcpyHostToDevice);
+  }
+  for (int b = 0; b <= nb && e == cudaSuccess; ++b) {
+    cudaEvent_t ev = nullptr;
+    e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    evs.push_back(ev);
+  }
+  if (e == cudaSuccess) {
+    e = cudaStreamBeginCapture(root, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) e = cudaEventRecord(evs[nb], root);
+    for (int b = 0; b < nb && e == cudaSuccess && !rc; ++b) {
+      e = cudaStreamWaitEvent(gs[b]->st, evs[nb], 0);
+      if (e == cudaSuccess) rc = gs[b]->capture();
+      if (e == cudaSuccess && !rc) e = cudaEventRecord(evs[b], gs[b]->st);
+      if (e == cudaSuccess && !rc) e = cudaStreamWaitEvent(root, evs[b], 0);
+    }
+    if (e == cudaSuccess && !rc) {
+      k_pg_sum_active<<<1, 32, 0, root>>>(d_act, nb, d_sum);
+      note_launch();
+    }
+    const cudaError_t e2 = cudaStreamEndCapture(root, &graph);
+    if (e == cudaSuccess) e = e2;
+    if (e == cudaSuccess && !rc) e = cudaGraphInstantiate(&exec, graph, 0);
+  }
+  if (e != cudaSuccess && !rc) { set_cuda_error("graph solve capture", e); rc = 1; }
+  long long launches = 0;
+  if (!rc) {
+    int cap = 0;
+    for (auto* g : gs) cap = std::max(cap, g->io->maxit);
+    const long long lim = (long long)cap + 64;
+    while (e == cudaSuccess && launches < lim) {
+      for (int k = 0; k < 4 && e == cudaSuccess; ++k, ++launches) e = cudaGraphLaunch(exec, root);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(h_sum, d_sum, sizeof(int), cudaMemcpyDeviceToHost, root);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(root);
+      if (e != cudaSuccess || *h_sum == 0) break;
+    }
+    if (e != cudaSuccess) { set_cuda_error("graph solve", e); rc = 1; }
+    note_launch((unsigned long long)launches);  // the summing kernel
+  }
+  for (auto* g : gs) g->launches = launches;
   if (exec) cudaGraphExecDestroy(exec);
   if (graph) cudaGraphDestroy(graph);
-  eng.stream = eng_st;
-  cudaStreamSynchronize(st);
-  cudaStreamDestroy(st);
-  cudaStreamDestroy(st2);
-  cudaFree(blk);
+  if (root) { cudaStreamSynchronize(root); cudaStreamDestroy(root); }
+  for (auto ev : evs)
+    if (ev) cudaEventDestroy(ev);
+  cudaFree(d_act);
+  cudaFreeHost(h_sum);
+  return rc;
+}
+
+// Targets of a multi-target solve hand their graph iterations to one
+// coordinator, which runs all of them as branches of one graph (pg_run).  Each
+// target's solve calls join() at the hand-over point and blocks until the
+// combined run ends; a target that finishes or fails without handing over calls
+// leave().  run() (the coordinator's thread) waits until every target has done
+// one of the two.
+template <typename T> struct PGGroup {
+  std::mutex m;
+  std::condition_variable cv;
+  int expected = 0, arrived = 0;
+  bool done = false;
+  int rc = 0;
+  std::vector<PGGraph<T>*> graphs;
+  int join(PGGraph<T>* g) {
+    std::unique_lock<std::mutex> lk(m);
+    graphs.push_back(g);
+    ++arrived;
+    cv.notify_all();
+    cv.wait(lk, [&] { return done; });
+    return rc;
+  }
+  void leave() {
+    std::lock_guard<std::mutex> lk(m);
+    ++arrived;
+    cv.notify_all();
+  }
+  int run() {
+    std::unique_lock<std::mutex> lk(m);
+    cv.wait(lk, [&] { return arrived >= expected; });
+    rc = pg_run<T>(graphs);
+    done = true;
+    cv.notify_all();
+    return rc;
+  }
+};
+
+template <typename T>
+static int pbcgs2_graph_loop(BatchIO<T>& io, BatchOps<T>& ops, std::vector<int>& nc, cplx<T>* const* w, PGHost& hs,
+                             double mv_ms_per_rhs) {
+  PGGraph<T> g;
+  int rc = g.init(io, ops, nc, w, hs, mv_ms_per_rhs);
+  if (!rc) {
+    PGGroup<T>* grp = static_cast<PGGroup<T>*>(io.group);
+    if (grp) {
+      io.group_joined = 1;
+      rc = grp->join(&g);
+    } else {
+      rc = pg_run<T>({&g});
+    }
+  } else if (io.group) {
+    io.group_joined = 1;
+    static_cast<PGGroup<T>*>(io.group)->leave();
+  }
+  if (!rc) rc = g.readback();
+  g.release();
   return rc;
 }
 
@@ -1861,5 +2002,14 @@ template int solve_batch_qmrccg<float>(BatchIO<float>&, BatchResult&);
 template int solve_batch_qmrccg<double>(BatchIO<double>&, BatchResult&);
 template int solve_batch_pbcgs2<float>(BatchIO<float>&, BatchResult&);
 template int solve_batch_pbcgs2<double>(BatchIO<double>&, BatchResult&);
+
+void* pg_group_create(int expected) {
+  auto* g = new PGGroup<float>();
+  g->expected = expected;
+  return g;
+}
+int pg_group_run(void* grp) { return static_cast<PGGroup<float>*>(grp)->run(); }
+void pg_group_leave(void* grp) { static_cast<PGGroup<float>*>(grp)->leave(); }
+void pg_group_destroy(void* grp) { delete static_cast<PGGroup<float>*>(grp); }
 
 }  // namespace ddb

@@ -88,12 +88,27 @@ template <typename T> struct BatchIO {
   // QMRCCG with sym and replace: 1 = device-driven iterations launched as a
   // CUDA graph (no host round trip per iteration)
   int graph = 0;
+  // PBCGS2 with graph (FP32): a multi-target group (pg_group_create) whose
+  // coordinator runs the device-driven iterations of every member target as
+  // branches of one graph; group_joined is set once this solve handed over (or
+  // left the group)
+  void* group = nullptr;
+  int group_joined = 0;
   double matvec_ms = 0.0;         // CUDA-event time of the MATVECs inside the solve
   long long matvec_rhs = 0;       // RHS-MATVECs performed
   int matvec_calls = 0;
 };
 
 template <typename T> int solve_batch_qmrccg(BatchIO<T>& io, BatchResult& res);
+// Multi-target graph group of FP32 batched PBCGS2 solves (see BatchIO::group):
+// every member solve runs on its own host thread and either hands its graph
+// iteration over (and blocks until the combined run ends) or leaves; the
+// coordinator's pg_group_run waits for all `expected` members, then launches
+// one graph whose branches are the members' iterations, once per Krylov step.
+void* pg_group_create(int expected);
+int pg_group_run(void* group);
+void pg_group_leave(void* group);
+void pg_group_destroy(void* group);
 template <typename T> int solve_batch_pbcgs2(BatchIO<T>& io, BatchResult& res);
 constexpr int BATCH_WORK_VECTORS = 12;
 

@@ -3,11 +3,17 @@
 //
 // Every target gets its own engine (geometry, Green tensor, FFT plans, MATVEC
 // workspace), its own batched-solver state and its own CUDA stream.  The Green
-// tensors are built first, one target after another; then a pool of host
+// tensors are built first, one target after another.  With the device-driven
+// PBCGS2 (DDSCAT_B200_GRAPH) every target's solve runs its first, host-driven
+// iteration on a host thread of its own and then hands its iteration over to a
+// coordinator: one CUDA graph holds the iterations of all targets as
+// independent branches and is launched once per Krylov step until no RHS of
+// any target is active, so the GPU runs the kernels of all targets side by
+// side and the host does one launch per step.  Otherwise a pool of host
 // threads drives the targets' batched Krylov solves, each thread taking the
-// largest target not yet started.  A solve synchronises only its own stream,
-// so while one target waits for its inner products the kernels of the others
-// keep the GPU busy: small targets that could not fill 148 SMs alone overlap.
+// largest target not yet started; a solve synchronises only its own stream, so
+// while one target waits for its inner products the kernels of the others keep
+// the GPU busy.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -30,11 +36,13 @@ struct Target {
   BatchOps<float> ops;
   cudaStream_t st = nullptr;
   int R = 0, n = 0, first = 0;  // RHS count, compact length, index of the first RHS
+  int nat = 0;                  // lattice sites of the caller's grid (its full-vector layout)
+  int* occ = nullptr;           // compact index -> site of the caller's grid
   float2 *b = nullptr, *x = nullptr, *adia = nullptr, *work = nullptr, *full = nullptr;
   void release() {
     ops.release();
     eng.release();
-    cudaFree(b); cudaFree(x); cudaFree(adia); cudaFree(work); cudaFree(full);
+    cudaFree(b); cudaFree(x); cudaFree(adia); cudaFree(work); cudaFree(full); cudaFree(occ);
     if (st) cudaStreamDestroy(st);
     *this = Target{};
   }
@@ -71,7 +79,32 @@ int multi_solve(int nt, const int* dims, const int16_t* const* iocc, const float
     for (int j = 0; j < nat; ++j) nat0 += iocc[i][j] != 0;
     if (nat0 == 0) { set_error("multi-target solve", "a target has no occupied site"); cleanup(); return 540; }
     if (cudaStreamCreate(&t.st) != cudaSuccess) { set_error("multi-target solve", "stream"); cleanup(); return 542; }
-    int rc = t.eng.init_geometry(nx, ny, nz, 0, nat, nat0, iocc[i], true);
+    // The engine's grid: each odd side extended by one vacuum plane, so that
+    // every axis runs on the register-FFT pipeline (padded lengths need even
+    // sides).  The occupied sites, their order (z, then y, then x) and so the
+    // compact vectors are those of the caller's grid; the Green tensor depends
+    // on the lags only, so the operator on them is unchanged.
+    const int ex = nx + (nx & 1), ey = ny + (ny & 1), ez = nz + (nz & 1);
+    const int enat = ex * ey * ez;
+    std::vector<int16_t> eocc((size_t)enat, 0);
+    std::vector<int> occ_h;
+    occ_h.reserve(nat0);
+    for (int z = 0; z < nz; ++z)
+      for (int y = 0; y < ny; ++y)
+        for (int x = 0; x < nx; ++x) {
+          const int j = x + nx * (y + ny * z);
+          if (iocc[i][j] == 0) continue;
+          eocc[(size_t)x + ex * ((size_t)y + ey * z)] = iocc[i][j];
+          occ_h.push_back(j);
+        }
+    t.nat = nat;
+    if (cudaMalloc((void**)&t.occ, (size_t)nat0 * sizeof(int)) != cudaSuccess ||
+        cudaMemcpy(t.occ, occ_h.data(), (size_t)nat0 * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess) {
+      set_error("multi-target solve", "index map");
+      cleanup();
+      return 542;
+    }
+    int rc = t.eng.init_geometry(ex, ey, ez, 0, enat, nat0, eocc.data(), true);
     if (rc) { cleanup(); return 543; }
     lap(0, ta);
     GreenArgs<float> ga;
@@ -105,7 +138,7 @@ int multi_solve(int nt, const int* dims, const int16_t* const* iocc, const float
         e = cudaMemcpyAsync(t.full, (const float2*)src[k] + (size_t)r * full, full * sizeof(float2),
                             cudaMemcpyHostToDevice, t.st);
         if (e != cudaSuccess) { set_cuda_error("multi-target H2D", e); cleanup(); return 544; }
-        v_gather<float>(t.full, dst[k] + (size_t)r * t.n, t.eng.occ, nat, nat0, t.st);
+        v_gather<float>(t.full, dst[k] + (size_t)r * t.n, t.occ, nat, nat0, t.st);
         if (check_launch("multi-target gather")) { cleanup(); return 544; }
       }
     lap(3, ta);
@@ -120,9 +153,12 @@ int multi_solve(int nt, const int* dims, const int16_t* const* iocc, const float
   std::mutex mu;
   int first_rc = 0;
   std::string first_msg;
-  auto worker = [&]() {
+  // one graph for all targets: PBCGS2 with device-driven iterations (replacement)
+  const bool grouped = graph && replace && solver == DDSCAT_B200_PBCGS2;
+  void* group = grouped ? pg_group_create(nt) : nullptr;
+  auto worker = [&](int fixed) {
     for (;;) {
-      const int k = next++;
+      const int k = fixed >= 0 ? fixed : next++;
       if (k >= nt) return;
       Target& t = T[order[k]];
       BatchIO<float> io;
@@ -130,14 +166,16 @@ int multi_solve(int nt, const int* dims, const int16_t* const* iocc, const float
       io.b = t.b; io.x = t.x; io.adia = t.adia; io.aoff = nullptr;
       io.work = t.work; io.nwork = BATCH_WORK_VECTORS;
       io.maxit = maxit; io.tol = (double)tol; io.replace = replace; io.sym = sym; io.graph = graph;
+      io.group = group;
       BatchResult res;
       int rc = solver == DDSCAT_B200_QMRCCG ? solve_batch_qmrccg<float>(io, res) : solve_batch_pbcgs2<float>(io, res);
+      if (group && !io.group_joined) pg_group_leave(group);  // solved (or failed) without handing over
       const int i = order[k];
-      const size_t full = (size_t)3 * t.eng.g.nat;
+      const size_t full = (size_t)3 * t.nat;
       for (int r = 0; !rc && r < t.R; ++r) {
         cudaError_t e = cudaMemsetAsync(t.full, 0, full * sizeof(float2), t.st);
         if (e == cudaSuccess) {
-          v_scatter<float>(t.x + (size_t)r * t.n, t.full, t.eng.occ, t.eng.g.nat, t.eng.g.nat0, t.st);
+          v_scatter<float>(t.x + (size_t)r * t.n, t.full, t.occ, t.nat, t.eng.g.nat0, t.st);
           e = cudaMemcpyAsync((float2*)x[i] + (size_t)r * full, t.full, full * sizeof(float2), cudaMemcpyDeviceToHost,
                               t.st);
         }
@@ -155,13 +193,23 @@ int multi_solve(int nt, const int* dims, const int16_t* const* iocc, const float
         std::lock_guard<std::mutex> lock(mu);
         if (!first_rc) { first_rc = rc == 1 ? 545 : rc; first_msg = last_error_text(); }
       }
+      if (fixed >= 0) return;
     }
   };
-  const int nw = std::max(1, std::min(nthreads, nt));
+  const int nw = grouped ? nt : std::max(1, std::min(nthreads, nt));
   std::vector<std::thread> pool;
-  for (int w = 1; w < nw; ++w) pool.emplace_back(worker);
-  worker();
-  for (auto& th : pool) th.join();
+  if (grouped) {
+    // a thread per target up to the hand-over; this thread coordinates
+    for (int k = 0; k < nt; ++k) pool.emplace_back(worker, k);
+    const int grc = pg_group_run(group);
+    for (auto& th : pool) th.join();
+    pg_group_destroy(group);
+    if (grc && !first_rc) { first_rc = 545; first_msg = last_error_text(); }
+  } else {
+    for (int w = 1; w < nw; ++w) pool.emplace_back(worker, -1);
+    worker(-1);
+    for (auto& th : pool) th.join();
+  }
   const auto t2 = now();
   cleanup();
   if (verbose)

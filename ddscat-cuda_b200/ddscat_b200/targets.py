@@ -210,9 +210,9 @@ def embed_ellipsoid(sides, semi, grid="fast"):
     """(grid dims, IOCC) of an ellipsoid filling a box of the given lattice
     sides, placed in a grid extended with vacuum: grid='fast' picks the sides
     of the fast MATVEC path (fast_side), grid='friendly' DDSCAT's 2^a 3^b 5^c
-    sizes (fft_friendly)."""
+    sizes (fft_friendly), grid='exact' keeps the sides themselves."""
     sx, sy, sz = (int(v) for v in sides)
-    ext = fast_side if grid == "fast" else fft_friendly
+    ext = {"fast": fast_side, "friendly": fft_friendly, "exact": (lambda v: v)}[grid]
     gx, gy, gz = ext(sx), ext(sy), ext(sz)
     box = ellipsoid_occupancy(sx, sy, sz, semi).reshape(sz, sy, sx)
     occ = np.zeros((gz, gy, gx), dtype=np.int16)

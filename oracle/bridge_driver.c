@@ -82,8 +82,8 @@ static int run(const char* in_path, const char* out_path) {
   FILE* f = fopen(in_path, "rb");
   if (!f) { perror(in_path); return 2; }
   int32_t hi[10];
-  float hf[17];
-  if (fread(hi, sizeof(int32_t), 10, f) != 10 || fread(hf, sizeof(float), 17, f) != 17) {
+  float hf[15];
+  if (fread(hi, sizeof(int32_t), 10, f) != 10 || fread(hf, sizeof(float), 15, f) != 15) {
     fprintf(stderr, "bridge_driver: short header\n");
     return 2;
   }

@@ -2,11 +2,12 @@
 the C4 configuration, 40 seeded random ellipsoids with lattice sides drawn
 uniformly from 24 to 96 per axis, semi-axes filling 0.6-1.0 of the box,
 Re m ~ U[1.2, 1.8], Im m ~ U[0.001, 0.1], x = 0.15 * (largest side), two
-polarisations each (80 RHS), PBCGS2.  Each target's grid is extended with
-vacuum to the nearest sides whose padded FFT lengths run on the fast x-first
-pipeline (2^k and 3*2^k), as DDSCAT extends its grids to FFT-friendly sizes.  Every
-RHS converges; for three targets the FP64 true residual is <= 1.2*TOL and the
-solutions match the single-target batched solve to 20*TOL."""
+polarisations each (80 RHS), PBCGS2.  Each target is solved on its drawn
+lattice sides (even sides run on padded register-FFT lengths, odd ones on
+the generic z-first pipeline).  Every RHS converges; for three targets the
+FP64 true residual is <= 1.2*TOL, the solutions match the single-target
+batched solve to 20*TOL, and Cext, Cabs (EVALQ) and Csca (SCAT) of the FP32
+solutions are within 1e-4 of those of the all-FP64 batched solve."""
 import numpy as np
 import pytest
 
@@ -16,7 +17,7 @@ from ddscat_b200 import targets
 TOL = 1e-5
 
 
-def c4_targets(count=40, seed=0, grid="fast"):
+def c4_targets(count=40, seed=0, grid="exact"):
     rng = np.random.default_rng(seed)
     out = []
     for _ in range(count):
@@ -33,8 +34,8 @@ def c4_targets(count=40, seed=0, grid="fast"):
 @pytest.mark.gpu
 @pytest.mark.parametrize("graph", [False, True])
 def test_c4_uneven_multi_target(graph):
-    """graph=True: each target's PBCGS2 iterations run device-driven (one
-    captured graph per iteration and target)."""
+    """graph=True: the PBCGS2 iterations of all targets run device-driven as
+    branches of one captured graph, launched once per Krylov step."""
     probs = c4_targets()
     items = []
     for p in probs:
@@ -54,6 +55,23 @@ def test_c4_uneven_multi_target(graph):
         dda.solve_batch("pbcgs2", it["b"], xs, it["adia"], maxit=3000, tol=TOL, replace=True)
         for r in range(2):
             assert np.linalg.norm(xs[r] - it["x"][r]) / np.linalg.norm(xs[r]) < 20 * TOL
+        # Q values of the FP32 solutions against the all-FP64 batched solve
+        x64 = np.zeros(it["b"].shape, dtype=np.complex128)
+        o64 = dda.solve_batch_f64("pbcgs2", it["b"], x64, it["adia"], maxit=4000, tol=1e-9, replace=True)
+        assert np.all(o64.status == 0)
+        nat, occ = p.nat, p.occ
+        comp = lambda v: np.concatenate([v[c * nat:(c + 1) * nat][occ] for c in range(3)])  # noqa: E731
+        zero = np.zeros(3 * p.nat0, dtype=np.complex64)
+        k = p.incid[0].k
+        for r in range(2):
+            e, a = comp(it["b"][r]), comp(it["adia"][r])
+            q32 = dda.evalq(k, use_resident=0, e=e, p=comp(it["x"][r]), adia=a, aoff=zero)
+            sc32 = dda.scat(k, p.incid[r].e, p.x0, etasca=0.5)
+            q64 = dda.evalq(k, use_resident=0, e=e, p=comp(x64[r]).astype(np.complex64), adia=a, aoff=zero)
+            s64 = dda.scat_csca_f64(np.ascontiguousarray(x64[r:r + 1]), k, p.incid[r].e, p.x0, etasca=0.5)
+            for g, w in zip(q32[:2], q64[:2]):
+                assert abs(g - w) <= 1e-4 * abs(w), (t, r, g, w)
+            assert abs(sc32["csca"] - s64["csca"][0]) <= 1e-4 * s64["csca"][0], (t, r)
     dda.release()
 
 
