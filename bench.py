@@ -496,7 +496,7 @@ def run_ours(args):
         # FP32 (SCAT amplitudes of the FP32 solutions) against FP64 (FP64
         # amplitudes of the FP64 solutions), both through the Mueller entry points
         from ddscat_b200 import targets as T
-        s11_err, sij_err, ndir = 0.0, 0.0, 0
+        s11_err, sij_err, sij_glob, ndir = 0.0, 0.0, 0.0, 0
         csca_err, g_err, navg = 0.0, 0.0, 0
         for o in range(R // 2):
             r0, r1 = 2 * o, 2 * o + 1
@@ -523,10 +523,11 @@ def run_ours(args):
             s11 = m64[:, 0, 0]
             s11_err = max(s11_err, float(np.max(np.abs(m32[:, 0, 0] - s11) / s11)))
             sij_err = max(sij_err, float(np.max(np.abs(m32 - m64) / s11[:, None, None])))
+            sij_glob = max(sij_glob, float(np.max(np.abs(m32 - m64)) / np.max(s11)))
         qerr = {"cabs_max_rel": worst["cabs"], "cext_max_rel": worst["cext"], "cpha_max_rel": worst["cpha"],
                 "csca_max_rel": csca_err, "g_max_abs": g_err,
                 "csca_g_quadrature": f"SCAT integration at ETASCA 0.5, NAVG {navg} directions",
-                "s11_max_rel": s11_err, "sij_max_abs_over_s11": sij_err,
+                "s11_max_rel": s11_err, "sij_max_abs_over_s11": sij_err, "sij_max_abs_over_max_s11": sij_glob,
                 "s_ij_directions": f"theta 0..180 deg at 1 deg in 2 planes ({ndir}) x {R // 2} orientations",
                 "rhs": R, "fp64_solve": f"{args.solver.upper()} all-FP64 on the GPU, tol 1e-8, FP64 far-field sums",
                 "fp64_iterations_mean": float(np.mean(its64))}

@@ -1180,7 +1180,7 @@ struct PGState {
   double2 *one, *mone;   // [R]
   double *rnrm0, *rnrm, *mxx, *mxr, *resid;
   int *it, *live, *status, *nc, *I, *CK, *RP, *RC, *XD, *RCMP, *XPDT;
-  int *active, *checks, *updates;  // [1] each
+  int *active, *checks, *updates, *loops;  // [1] each
 };
 
 __device__ __forceinline__ double2 dconj(double2 a) { return make_double2(a.x, -a.y); }
@@ -1370,6 +1370,18 @@ __global__ void k_pg_count(int R, int maxit, double tol, PGState S) {
   int c = 0;
   for (int r = 0; r < R; ++r) c += S.live[r] && S.resid[r] > tol && S.it[r] < maxit;
   *S.active = c;
+  *S.loops += 1;
+}
+// the same as the last kernel of an iteration that runs as the body of a WHILE
+// node: the loop continues while some RHS is active (each pass raises `it` of
+// every active RHS, so it ends after at most maxit passes)
+__global__ void k_pg_count_while(int R, int maxit, double tol, PGState S, cudaGraphConditionalHandle h) {
+  if (threadIdx.x != 0) return;
+  int c = 0;
+  for (int r = 0; r < R; ++r) c += S.live[r] && S.resid[r] > tol && S.it[r] < maxit;
+  *S.active = c;
+  *S.loops += 1;
+  cudaGraphSetConditional(h, c > 0 ? 1u : 0u);
 }
 
 // host copy of the PBCGS2 state handed between the host-driven and the graph-driven iterations
@@ -1398,7 +1410,7 @@ template <typename T> struct PGGraph {
   double* dd = nullptr;
   int* ii = nullptr;
   PGState S{};
-  cudaStream_t st = nullptr, st2 = nullptr, eng_st = nullptr;
+  cudaStream_t st = nullptr, st2 = nullptr, stw = nullptr, eng_st = nullptr;
   unsigned long long kernels_a = 0, kernels_b = 0, kernels_c = 0;
   long long launches = 0;  // set by pg_run
 
@@ -1406,7 +1418,7 @@ template <typename T> struct PGGraph {
     io = &io_; ops = &ops_; nc = &nc_; hs = &hs_; mv_ms_per_rhs = per_rhs;
     for (int k = 0; k < 11; ++k) w[k] = w_[k];
     R = io->R; n = io->n;
-    nz2 = (size_t)(6 + 7 + 2) * R; nd = (size_t)5 * R; ni = (size_t)11 * R + 3;
+    nz2 = (size_t)(6 + 7 + 2) * R; nd = (size_t)5 * R; ni = (size_t)11 * R + 4;
     cudaError_t e = cudaMalloc((void**)&blk, nz2 * sizeof(double2) + nd * sizeof(double) + ni * sizeof(int));
     if (e != cudaSuccess) { set_cuda_error("graph solve state", e); return 1; }
     double2* z = reinterpret_cast<double2*>(blk);
@@ -1424,6 +1436,7 @@ template <typename T> struct PGGraph {
     S.active = ii + (size_t)11 * R;
     S.checks = S.active + 1;
     S.updates = S.active + 2;
+    S.loops = S.active + 3;
     std::vector<double2> hz(nz2, make_double2(0, 0));
     const std::vector<Z>* zs[6] = {&hs->alpha, &hs->omega, &hs->sigma, &hs->rho0, &hs->rho1, &hs->beta};
     for (int k = 0; k < 6; ++k)
@@ -1440,6 +1453,7 @@ template <typename T> struct PGGraph {
     cudaStreamSynchronize(ops->stream);
     e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&stw, cudaStreamNonBlocking);
     // uploads ordered on st (see qmr_graph_loop)
     if (e == cudaSuccess) e = cudaMemcpyAsync(z, hz.data(), nz2 * sizeof(double2), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dd, hd0.data(), nd * sizeof(double), cudaMemcpyHostToDevice, st);
@@ -1450,8 +1464,9 @@ template <typename T> struct PGGraph {
     return 0;
   }
 
-  // one iteration into the capture stream st has joined
-  int capture() {
+  // one iteration into the capture stream st has joined; hwhile: the WHILE
+  // node whose body this is (0: none, the host relaunches the graph)
+  int capture(cudaGraphConditionalHandle hwhile = 0) {
     const int R_ = R, n_ = n;
     Engine<T>& eng = *io->eng;
     C *rr = w[0], *r[3] = {w[1], w[2], w[3]}, *u[3] = {w[4], w[5], w[6]}, *XP = w[7], *BP = w[8], *X = w[9],
@@ -1590,7 +1605,8 @@ template <typename T> struct PGGraph {
           kernels_c = launch_total() - c3;
         }
         if (e == cudaSuccess) {
-          k_pg_count<<<1, 32, 0, st>>>(R_, maxit, tol, S);
+          if (hwhile) k_pg_count_while<<<1, 32, 0, st>>>(R_, maxit, tol, S, hwhile);
+          else k_pg_count<<<1, 32, 0, st>>>(R_, maxit, tol, S);
           note_launch();
           kernels_a += 1;
         }
@@ -1609,6 +1625,7 @@ template <typename T> struct PGGraph {
     if (e == cudaSuccess) e = cudaMemcpy(hi.data(), ii, ni * sizeof(int), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) { set_cuda_error("graph solve state", e); return 1; }
     const int checks = hi[(size_t)11 * R + 1], updates = hi[(size_t)11 * R + 2];
+    launches = hi[(size_t)11 * R + 3];  // iterations run by the graph
     note_launch((unsigned long long)launches * kernels_a + (unsigned long long)checks * kernels_b +
                 (unsigned long long)updates * kernels_c);
     long long mv_rhs = 0;
@@ -1627,8 +1644,9 @@ template <typename T> struct PGGraph {
   void release() {
     if (st) { cudaStreamSynchronize(st); cudaStreamDestroy(st); }
     if (st2) cudaStreamDestroy(st2);
+    if (stw) cudaStreamDestroy(stw);
     cudaFree(blk);
-    st = st2 = nullptr;
+    st = st2 = stw = nullptr;
     blk = nullptr;
   }
 };
@@ -1642,13 +1660,19 @@ __global__ void k_pg_sum_active(int* const* act, int nb, int* out) {
 }
 
 // One CUDA graph whose branches are the iterations of the given targets
-// (independent of one another: fork from a root stream, join back), launched
-// once per Krylov step until no RHS of any branch is active; the host reads the
-// summed active count every 4 launches.  Bounded by the largest maxit + 64
-// launches (every RHS stops at its maxit).
+// (independent of one another: fork from a root stream, join back).  With one
+// target the graph is one iteration, launched once per Krylov step until no
+// RHS is active (the host reads the active count every 4 launches).  With
+// several, each branch is a WHILE node whose body is that target's iteration
+// and whose condition its last kernel sets (some RHS still active): every
+// target iterates on the device at its own pace, and the host launches the
+// graph once.  Every pass raises the iteration count of each active RHS, so a
+// branch ends after at most its maxit passes; the host relaunches (bounded)
+// only if some branch is still active afterwards.
 template <typename T> int pg_run(const std::vector<PGGraph<T>*>& gs) {
   if (gs.empty()) return 0;
   const int nb = (int)gs.size();
+  const bool loops = nb > 1;
   cudaStream_t root = nullptr;
   int** d_act = nullptr;
   int* d_sum = nullptr;
@@ -1671,12 +1695,45 @@ template <typename T> int pg_run(const std::vector<PGGraph<T>*>& gs) {
     e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
     evs.push_back(ev);
   }
+  // branch b's WHILE node at the capture point of its stream, its body captured on stw
+  auto while_branch = [&](PGGraph<T>* g) -> cudaError_t {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t cg = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    cudaError_t e_ = cudaStreamGetCaptureInfo(g->st, &cs, nullptr, &cg, &deps, &ndeps);
+    cudaGraphConditionalHandle hw = 0;
+    if (e_ == cudaSuccess) e_ = cudaGraphConditionalHandleCreate(&hw, cg, 1, cudaGraphCondAssignDefault);
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = hw;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t wnode = nullptr;
+    if (e_ == cudaSuccess) e_ = cudaGraphAddNode(&wnode, cg, deps, ndeps, &cp);
+    if (e_ == cudaSuccess) e_ = cudaStreamUpdateCaptureDependencies(g->st, &wnode, 1, cudaStreamSetCaptureDependencies);
+    if (e_ == cudaSuccess)
+      e_ = cudaStreamBeginCaptureToGraph(g->stw, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                         cudaStreamCaptureModeThreadLocal);
+    if (e_ != cudaSuccess) return e_;
+    cudaStream_t outer = g->st;
+    g->st = g->stw;  // the body's kernels and IF nodes go into the WHILE body
+    const int brc = g->capture(hw);
+    g->st = outer;
+    cudaGraph_t body = nullptr;
+    e_ = cudaStreamEndCapture(g->stw, &body);
+    if (brc && e_ == cudaSuccess) e_ = cudaErrorUnknown;
+    return e_;
+  };
   if (e == cudaSuccess) {
     e = cudaStreamBeginCapture(root, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) e = cudaEventRecord(evs[nb], root);
     for (int b = 0; b < nb && e == cudaSuccess && !rc; ++b) {
       e = cudaStreamWaitEvent(gs[b]->st, evs[nb], 0);
-      if (e == cudaSuccess) rc = gs[b]->capture();
+      if (e == cudaSuccess) {
+        if (loops) e = while_branch(gs[b]);
+        else rc = gs[b]->capture();
+      }
       if (e == cudaSuccess && !rc) e = cudaEventRecord(evs[b], gs[b]->st);
       if (e == cudaSuccess && !rc) e = cudaStreamWaitEvent(root, evs[b], 0);
     }
@@ -1693,9 +1750,11 @@ template <typename T> int pg_run(const std::vector<PGGraph<T>*>& gs) {
   if (!rc) {
     int cap = 0;
     for (auto* g : gs) cap = std::max(cap, g->io->maxit);
-    const long long lim = (long long)cap + 64;
+    // one launch per Krylov step (one target) or per whole solve (WHILE branches)
+    const long long lim = loops ? 4 : (long long)cap + 64;
+    const int per_poll = loops ? 1 : 4;
     while (e == cudaSuccess && launches < lim) {
-      for (int k = 0; k < 4 && e == cudaSuccess; ++k, ++launches) e = cudaGraphLaunch(exec, root);
+      for (int k = 0; k < per_poll && e == cudaSuccess; ++k, ++launches) e = cudaGraphLaunch(exec, root);
       if (e == cudaSuccess) e = cudaMemcpyAsync(h_sum, d_sum, sizeof(int), cudaMemcpyDeviceToHost, root);
       if (e == cudaSuccess) e = cudaStreamSynchronize(root);
       if (e != cudaSuccess || *h_sum == 0) break;
@@ -1703,7 +1762,6 @@ template <typename T> int pg_run(const std::vector<PGGraph<T>*>& gs) {
     if (e != cudaSuccess) { set_cuda_error("graph solve", e); rc = 1; }
     note_launch((unsigned long long)launches);  // the summing kernel
   }
-  for (auto* g : gs) g->launches = launches;
   if (exec) cudaGraphExecDestroy(exec);
   if (graph) cudaGraphDestroy(graph);
   if (root) { cudaStreamSynchronize(root); cudaStreamDestroy(root); }

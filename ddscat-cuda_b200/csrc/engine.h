@@ -137,6 +137,8 @@ template <typename T> struct VecOps {
   void release();
   // results of up to 8 dots, each sum over conj(a)*b (conj=1) or a*b (conj=0)
   int dots(int n, int k, const C* const* a, const C* const* b, const int* conjf, double2* host_out);
+  // the same products left in d_out[0..k) on the device (stream-ordered, no host copy)
+  int dots_dev(int n, int k, const C* const* a, const C* const* b, const int* conjf);
   double2 dotc(int n, const C* a, const C* b, int* err);
   double2 dotu(int n, const C* a, const C* b, int* err);
   double nrm2(int n, const C* a, int* err);

@@ -16,11 +16,11 @@
 // XYI below): the plane meets in distributed shared memory instead of an HBM
 // round trip of A, and B is laid out [c][kx][iz][ky] for them.
 // The Green octant is stored z-fastest, [irx][iry][irz][6], so a z-line reads
-// contiguous 48-byte records: kx_zg3 (the ZG pass for E <= 16, FP32) copies a
-// block's octant lines to shared memory with bulk asynchronous copies and
-// keeps the three components of a z position in one thread; kx_zg (larger E,
-// FP64) loads each record once for kz and its mirror M_z - kz and exchanges
-// the components through shared memory.  The ZG grid runs RHS-fastest so
+// contiguous 48-byte records: kx_zg3 (the ZG pass for E <= 16, FP32) reads
+// its records straight from global memory (the octant stays L2-resident
+// across the RHS of a call) and keeps the three components of a z position in
+// one thread; kx_zg (larger E, FP64) loads each record once for kz and its
+// mirror M_z - kz and exchanges the components through shared memory.  The ZG grid runs RHS-fastest so
 // consecutive blocks reuse the Green tile from L2.  Twiddles are read from
 // global memory (L1/L2 resident tables).  The middle passes run over kx
 // batches (all of M_x for the FFT3D build, a few columns for the SLICES build).
@@ -275,6 +275,32 @@ __device__ __forceinline__ void green_apply(const C a[6], R sxy, R sxz, R syz, C
   pz = cadd(cadd(cmul(a13, x), cmul(a23, y)), cmul(a[5], z));
 }
 
+// y = G x for one octant record a = (xx, xy, xz, yy, yz, zz) with the
+// off-diagonal signs SXY, SXZ, SYZ (+1 or -1, compile-time, so they fold into
+// the operands): each real and imaginary output is one multiply and five
+// fused multiply-adds.
+template <int SXY, int SXZ, int SYZ, typename C>
+__device__ __forceinline__ void green_apply_s(const C a[6], C& px, C& py, C& pz) {
+  using R = decltype(px.x);
+  const C x = px, y = py, z = pz;
+  const R kxy = (R)SXY, kxz = (R)SXZ, kyz = (R)SYZ;
+  // row x: a0 x + SXY a1 y + SXZ a2 z
+  px.x = fma(kxz * a[2].x, z.x, fma(-kxz * a[2].y, z.y, fma(kxy * a[1].x, y.x, fma(-kxy * a[1].y, y.y,
+         fma(a[0].x, x.x, -a[0].y * x.y)))));
+  px.y = fma(kxz * a[2].x, z.y, fma(kxz * a[2].y, z.x, fma(kxy * a[1].x, y.y, fma(kxy * a[1].y, y.x,
+         fma(a[0].x, x.y, a[0].y * x.x)))));
+  // row y: SXY a1 x + a3 y + SYZ a4 z
+  py.x = fma(kyz * a[4].x, z.x, fma(-kyz * a[4].y, z.y, fma(a[3].x, y.x, fma(-a[3].y, y.y,
+         fma(kxy * a[1].x, x.x, -kxy * a[1].y * x.y)))));
+  py.y = fma(kyz * a[4].x, z.y, fma(kyz * a[4].y, z.x, fma(a[3].x, y.y, fma(a[3].y, y.x,
+         fma(kxy * a[1].x, x.y, kxy * a[1].y * x.x)))));
+  // row z: SXZ a2 x + SYZ a4 y + a5 z
+  pz.x = fma(a[5].x, z.x, fma(-a[5].y, z.y, fma(kyz * a[4].x, y.x, fma(-kyz * a[4].y, y.y,
+         fma(kxz * a[2].x, x.x, -kxz * a[2].y * x.y)))));
+  pz.y = fma(a[5].x, z.y, fma(a[5].y, z.x, fma(kyz * a[4].x, y.y, fma(kyz * a[4].y, y.x,
+         fma(kxz * a[2].x, x.y, kxz * a[2].y * x.x)))));
+}
+
 // Offset of z position 0 of line p = kxl*My + ky in one component of B, and
 // the z stride: [kxl][ky][iz] (five-pass schedule, BTY = 0) or [kx][iz][ky]
 // (the fused xy passes, BTY = M_y: a compile-time stride keeps the z offsets
@@ -378,34 +404,49 @@ __global__ void __launch_bounds__(3 * XShape<N>::TT * XShape<N>::RZ, sizeof(T) =
 // Each thread holds the same z positions of all three components of its
 // (kx, ky) line, so the Green multiply runs in registers: shared memory only
 // carries the FFT transposes (half the shared-memory traffic of kx_zg, no
-// block barriers after the start).  With IPBC = 0 one thread copies the
-// block's Green octant lines (kz = 0..N/2, contiguous 48-byte records) into
-// shared memory with bulk asynchronous copies at the start, so they arrive
-// while the data loads and forward FFTs run; each thread then reads the
-// records of its own kz values there (kz > N/2 reads the record of N - kz).
-// For E <= 16 (registers: 3E complex per thread).
+// block barriers).  The Green octant records (48 bytes, kz > N/2 reads the
+// record of N - kz with the kz sign) come straight from global memory, four
+// per thread at a time; consecutive blocks work on the same lines for
+// successive RHS (the grid runs RHS-fastest), so the records are L2 hits.
+// Staging the block's octant lines in shared memory by bulk asynchronous
+// copies instead measured 7 % slower at 128^3 (66 KB more shared memory per
+// block, a smaller L1).  For E <= 16 (registers: 3E complex per thread).
 // block: RZ lines x TT threads, thread-fastest; grid (nrb, ceil(nkx*My/RZ))
-// shared memory: FFT scratch [RZ][lsz] | Green [RZ][NR][6] | mbarrier
+// shared memory: FFT scratch [RZ][lsz]
 template <int N> struct Z3Shape {
   static constexpr int RZ = 128 / XShape<N>::TT;  // lines per 128-thread block
-  static constexpr int NR = N / 2 + 1;            // octant records per line
   static constexpr bool OK = XShape<N>::E <= 16;
 };
-constexpr int ZG3_WAIT_POLLS = 1 << 20;  // bound on the mbarrier polls of one wait
 
-template <typename T>
-__device__ __forceinline__ void load_rec_s(const cplx<T>* sp, cplx<T> a[6]) {
-  if constexpr (sizeof(cplx<T>) == 8) {
-    const float4* s4 = reinterpret_cast<const float4*>(sp);
+// The Green multiply of kx_zg3 on data whose x and y components carry the
+// line signs sx (kx) and sy (ky) already (the off-diagonal signs of the octant,
+// cu:112, are s_a s_b, i.e. G = D G' D with D = diag(sx, sy, sz)); what is left
+// is the kz sign of the xz and yz entries, compile-time for every element but
+// the one at i = E/2, whose kz = N/2 + t has sign +1 only for t = 0.
+template <int N, int TT, int E, typename C>
+__device__ __forceinline__ void zg3_green(const C* rec0, int t, C (&v)[3][E]) {
+  constexpr int GB = 4;  // records in flight per thread (2 measured 9 % slower at 128^3)
 #pragma unroll
-    for (int m = 0; m < 3; ++m) {
-      const float4 q = s4[m];
-      a[2 * m] = mk<cplx<T>>(q.x, q.y);
-      a[2 * m + 1] = mk<cplx<T>>(q.z, q.w);
+  for (int i0 = 0; i0 < E; i0 += GB) {
+    C a[GB][6];
+#pragma unroll
+    for (int j = 0; j < GB; ++j) {
+      const int kz = t + TT * (i0 + j);
+      load_rec<decltype(a[0][0].x)>(rec0 + 6 * (kz <= N / 2 ? kz : N - kz), a[j]);
     }
-  } else {
 #pragma unroll
-    for (int m = 0; m < 6; ++m) a[m] = sp[m];
+    for (int j = 0; j < GB; ++j) {
+      const int i = i0 + j;
+      // i is a constant after unrolling: these tests fold
+      if (TT * i + TT - 1 <= N / 2) {
+        green_apply_s<1, 1, 1>(a[j], v[0][i], v[1][i], v[2][i]);
+      } else if (TT * i > N / 2) {
+        green_apply_s<1, -1, -1>(a[j], v[0][i], v[1][i], v[2][i]);
+      } else {
+        if (t + TT * i <= N / 2) green_apply_s<1, 1, 1>(a[j], v[0][i], v[1][i], v[2][i]);
+        else green_apply_s<1, -1, -1>(a[j], v[0][i], v[1][i], v[2][i]);
+      }
+    }
   }
 }
 
@@ -413,72 +454,41 @@ template <typename T, int N, int BTY = 0> __global__ void __launch_bounds__(128,
   using C = cplx<T>;
   using R = T;
   using S_ = XShape<N>;
-  constexpr int E = S_::E, TT = S_::TT, H = S_::H, RL = Z3Shape<N>::RZ, NR = Z3Shape<N>::NR;
+  constexpr int E = S_::E, TT = S_::TT, H = S_::H;
   static_assert(Z3Shape<N>::OK, "kx_zg3 holds 3*E complex values per thread");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int t = threadIdx.x % TT, l = threadIdx.x / TT;
   C* my = reinterpret_cast<C*>(smem_raw) + (size_t)l * P.lsz;
-  C* sg = reinterpret_cast<C*>(smem_raw) + (size_t)RL * P.lsz;  // 16-byte aligned: RL*lsz is even
-  uint64_t* bar = reinterpret_cast<uint64_t*>(sg + (size_t)RL * NR * 6);
   const int rb = blockIdx.x, rl = P.b_rhs0 + rb;
   if (xoff(P, rl)) return;
   const int nlines = P.nkx * P.My;
-  const int p0 = blockIdx.y * RL;
-  const bool pre = P.ipbc == 0;
-  if (pre && threadIdx.x == 0) {
-    const int nl = min(RL, nlines - p0);  // >= 1
-    mbar_init(bar, 1);
-    mbar_arrive_expect_tx(bar, (uint32_t)(nl * NR * 6 * sizeof(C)));
-    for (int j = 0; j < nl; ++j) {
-      const int pj = p0 + j, kxl = pj / P.My;
-      R s0, s1, s2;
-      bulk_g2s(sg + (size_t)j * NR * 6, green_rec(P, P.kx0 + kxl, pj - kxl * P.My, 0, s0, s1, s2),
-               (uint32_t)(NR * 6 * sizeof(C)), bar);
-    }
-  }
-  const int p = p0 + l;
+  const int p = blockIdx.y * Z3Shape<N>::RZ + l;
   const bool live = p < nlines;
   const size_t cs = (size_t)nlines * P.nz;  // component stride of B
   constexpr int zs = zline_stride<BTY>();
   C* row = P.B + (size_t)rb * 3 * cs + zline_base<BTY>(P, live ? p : 0);
+  const int kxl = p / P.My;
+  const int kx = P.kx0 + kxl, ky = p - kxl * P.My;
+  // the octant's line signs sx (kx) and sy (ky) of cu:112, applied to the x and
+  // y components on the way in and out (the z transforms are linear)
+  const R sx = P.ipbc == 0 && 2 * kx > P.Mx ? (R)-1 : (R)1, sy = P.ipbc == 0 && 2 * ky > P.My ? (R)-1 : (R)1;
   C v[3][E];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
+    const R sc = c == 0 ? sx : (c == 1 ? sy : (R)1);
 #pragma unroll
     for (int i = 0; i < H; ++i)
-      v[c][i] = live && t + TT * i < P.nz ? row[c * cs + (t + TT * i) * zs] : mk<C>(0, 0);  // iz < nz <= N/2
+      v[c][i] = live && t + TT * i < P.nz ? cscale(row[c * cs + (t + TT * i) * zs], sc) : mk<C>(0, 0);  // iz < nz <= N/2
   }
   // one twiddle set for the six transforms: forward, and conjugated for the inverse
   C w[E];
   line_twiddles<E, +1>(w, t, P.twz);
 #pragma unroll
   for (int c = 0; c < 3; ++c) line_fft_w<E, TT, +1, false, true, S_::PAIR>(v[c], my, t, w);
-  bool ok = true;
-  __syncthreads();  // the mbarrier initialisation is visible before any thread waits on it
   if (live) {
-    const int kxl = p / P.My;
-    const int kx = P.kx0 + kxl, ky = p - kxl * P.My;
-    if (pre) {
+    if (P.ipbc == 0) {
       R sxy, sxz, syz;
-      const C* rec0 = green_rec(P, kx, ky, 0, sxy, sxz, syz);
-      const C* srec = sg + (size_t)l * NR * 6;
-      ok = mbar_wait(bar, 0, ZG3_WAIT_POLLS);  // else read the records from global memory
-#pragma unroll
-      for (int i0 = 0; i0 < E; i0 += 4) {
-        C a[4][6];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const int kz = t + TT * (i0 + j);
-          const int r = kz <= N / 2 ? kz : N - kz;
-          if (ok) load_rec_s<T>(srec + 6 * r, a[j]); else load_rec<T>(rec0 + 6 * r, a[j]);
-        }
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const int i = i0 + j;
-          const R s = t + TT * i <= N / 2 ? (R)1 : (R)-1;
-          green_apply(a[j], sxy, s * sxz, s * syz, v[0][i], v[1][i], v[2][i]);
-        }
-      }
+      zg3_green<N, TT, E>(green_rec(P, kx, ky, 0, sxy, sxz, syz), t, v);
     } else {
 #pragma unroll
       for (int i = 0; i < E; ++i) {
@@ -494,12 +504,12 @@ template <typename T, int N, int BTY = 0> __global__ void __launch_bounds__(128,
   if (live) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
+      const R sc = c == 0 ? sx : (c == 1 ? sy : (R)1);
 #pragma unroll
       for (int i = 0; i < H; ++i)
-        if (t + TT * i < P.nz) row[c * cs + (t + TT * i) * zs] = v[c][i];  // keep iz < nz
+        if (t + TT * i < P.nz) row[c * cs + (t + TT * i) * zs] = cscale(v[c][i], sc);  // keep iz < nz
     }
   }
-  if (!ok) mbar_wait(bar, 0, ZG3_WAIT_POLLS);  // no copy may land after the block exits
 }
 
 // ------------------------------------------------------------- YI: y inverse
@@ -998,10 +1008,8 @@ int matvec_xpipe(Engine<T>& E, const MvArgs<T>& a) {
   const size_t xi_maxc = (size_t)RX * (g.Mx / 2);
   const size_t smxi = smx + (xi_maxc <= (size_t)XI_STAGE_MAX ? 2 * xi_maxc * sizeof(C) : 0);
   const size_t smy = std::max((size_t)g.My * (RY + 1), (size_t)RY * P.lsy) * sizeof(C);
-  // ZG3: FFT scratch, Green octant lines (IPBC = 0) and the mbarrier
-  const size_t smz =
-      fzg3 ? ((size_t)RZ3 * P.lsz + (g.ipbc == 0 ? (size_t)RZ3 * 6 * (g.Mz / 2 + 1) : 0)) * sizeof(C) + 16
-           : (size_t)3 * RZ * P.lsz * sizeof(C);
+  // ZG3: FFT scratch
+  const size_t smz = fzg3 ? (size_t)RZ3 * P.lsz * sizeof(C) : (size_t)3 * RZ * P.lsz * sizeof(C);
   const void* fxf = xkernel<T>(XPass::XF, g.Mx);
   const void* fyf = xkernel<T>(XPass::YF, g.My);
   const void* fzg = xkernel<T>(XPass::ZG, g.Mz);

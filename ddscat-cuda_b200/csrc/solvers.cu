@@ -130,90 +130,350 @@ template <typename T> struct Ctx {
     if (_rc) return _rc;             \
   } while (0)
 
+// QMRCCG with the FP64 recurrence scalars held on the GPU: one iteration is
+// the p/q step, A p, the vt/wt step, A wt, one launch of the four inner
+// products, the scalar recurrence in a single thread, the d/s/x/r step and
+// |r|^2; the host waits once per iteration, for the residual it prints and
+// tests (the reference waits for every inner-product group, cu:1079-1092).
+// Same recurrence, reliable-residual checks, restart rule and MATVEC count as
+// the reference (cu:434-443, cu:1071-1103).
+struct DQState {
+  double2 gamma, ksi, rho, eps, mu, tau, lambda, kappa, theta;
+  // coefficients: p = co0 p + co1 vt, q = co2 q + co3 atw, vt = co4 vt + A p,
+  // wt = co5 wt + q, d = co6 d + co7 p, s = co6 s + co7 A p
+  double2 co[8];
+  double bnorm, resid;
+  int status, pad;
+};
+
+__host__ __device__ inline double2 dq_mul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__host__ __device__ inline double2 dq_div(double2 a, double2 b) {  // Smith's scaled complex division
+  if (fabs(b.x) >= fabs(b.y)) {
+    const double r = b.y / b.x, d = b.x + b.y * r;
+    return make_double2((a.x + a.y * r) / d, (a.y - a.x * r) / d);
+  }
+  const double r = b.x / b.y, d = b.y + b.x * r;
+  return make_double2((a.x * r + a.y) / d, (a.y * r - a.x) / d);
+}
+__host__ __device__ inline bool dq_zero(double2 a) { return a.x == 0.0 && a.y == 0.0; }
+__host__ __device__ inline double2 dq_neg(double2 a) { return make_double2(-a.x, -a.y); }
+
+// coefficients of the p/q and vt/wt steps from gamma, ksi, mu, tau
+__host__ __device__ inline void dq_step_coefficients(DQState& S) {
+  const double2 one = make_double2(1.0, 0.0);
+  S.co[0] = dq_neg(S.mu);
+  S.co[1] = dq_div(one, S.gamma);
+  S.co[2] = dq_neg(dq_div(dq_mul(S.gamma, S.mu), S.ksi));
+  S.co[3] = dq_div(one, S.ksi);
+  S.co[4] = dq_neg(dq_div(S.tau, S.gamma));
+  S.co[5] = dq_neg(dq_div(S.tau, S.ksi));
+}
+
+// the scalar recurrence of cu:442 from |vt|^2, |wt|^2, vt^T wt, vt^T A wt
+__global__ void k_dq_recur(DQState* SP, const double2* out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  DQState S = *SP;
+  const double2 gamma0 = S.gamma, ksi0 = S.ksi, rho0 = S.rho, tau0 = S.tau, kappa0 = S.kappa;
+  S.gamma = make_double2(sqrt(fmax(0.0, out[0].x)), 0.0);
+  S.ksi = make_double2(sqrt(fmax(0.0, out[1].x)), 0.0);
+  S.rho = out[2];
+  S.eps = out[3];
+  int st = 0;
+  if (dq_zero(S.gamma)) st = 6;
+  else if (dq_zero(S.ksi)) st = 7;
+  const double2 den = dq_mul(dq_mul(S.gamma, S.tau), rho0);
+  if (!st && dq_zero(den)) st = 12;
+  if (!st) {
+    S.mu = dq_div(dq_mul(dq_mul(gamma0, ksi0), S.rho), den);
+    if (dq_zero(S.rho)) st = 13;
+  }
+  if (!st) {
+    const double2 gm = dq_mul(S.gamma, S.mu), er = dq_div(S.eps, S.rho);
+    S.tau = make_double2(er.x - gm.x, er.y - gm.y);
+    const double at0 = tau0.x * tau0.x + tau0.y * tau0.y, ag = S.gamma.x * S.gamma.x + S.gamma.y * S.gamma.y;
+    const double2 den2 = make_double2(S.lambda.x * at0 + ag, S.lambda.y * at0);
+    if (dq_zero(den2)) st = 14;
+    else {
+      S.theta = dq_div(make_double2((1.0 - S.lambda.x) * at0, -S.lambda.y * at0), den2);
+      const double2 g0t = dq_mul(gamma0, make_double2(tau0.x, -tau0.y));
+      S.kappa = dq_neg(dq_div(dq_mul(g0t, kappa0), den2));
+      S.lambda = dq_div(make_double2(S.lambda.x * at0, S.lambda.y * at0), den2);
+    }
+  }
+  S.status = st;
+  S.co[6] = S.theta;
+  S.co[7] = S.kappa;
+  if (!st) dq_step_coefficients(S);
+  *SP = S;
+}
+__global__ void k_dq_resid(DQState* S, const double2* out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double v = out[0].x;
+  if (v < 0.0 && v > -1e-12) v = 0.0;
+  S->resid = sqrt(v > 0.0 ? v : 0.0) / S->bnorm;
+}
+
+// d = zd d + za a (k_lincomb's arithmetic: zmulv per term, a zero zd drops d)
+template <typename C> __device__ __forceinline__ C dq_lin(C d, double2 zd, C a, double2 za) {
+  C v = mk<C>(0, 0);
+  if (!dq_zero(zd)) v = zmulv(zd, d);
+  return cadd(v, zmulv(za, a));
+}
+template <typename C>
+__global__ void k_dq_pq(int n, C* p, C* q, const C* vt, const C* atw, const DQState* S) {
+  const double2 c0 = S->co[0], c1 = S->co[1], c2 = S->co[2], c3 = S->co[3];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    p[i] = dq_lin(p[i], c0, vt[i], c1);
+    q[i] = dq_lin(q[i], c2, atw[i], c3);
+  }
+}
+template <typename C>
+__global__ void k_dq_vw(int n, C* vt, C* wt, const C* ap, const C* q, const DQState* S) {
+  const double2 c4 = S->co[4], c5 = S->co[5], one = make_double2(1.0, 0.0);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    vt[i] = dq_lin(vt[i], c4, ap[i], one);
+    wt[i] = dq_lin(wt[i], c5, q[i], one);
+  }
+}
+template <typename C>
+__global__ void k_dq_dsxr(int n, C* d, C* s, C* x, C* r, const C* p, const C* ap, const DQState* S) {
+  if (S->status) return;
+  const double2 th = S->co[6], ka = S->co[7], one = make_double2(1.0, 0.0), mone = make_double2(-1.0, 0.0);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const C dn = dq_lin(d[i], th, p[i], ka);
+    const C sn = dq_lin(s[i], th, ap[i], ka);
+    d[i] = dn;
+    s[i] = sn;
+    x[i] = dq_lin(x[i], one, dn, one);
+    r[i] = dq_lin(r[i], one, sn, mone);
+  }
+}
+
+static inline unsigned dq_grid(int n) { return (unsigned)std::min<size_t>(ceil_div((size_t)std::max(n, 1), 256), 148 * 16); }
+
 // ---------------------------------------------------------------- PBCGS2 (cu:459-480, cu:1168-1278)
+// ZBCG2 = BiCGStab(2) with the reference's reliable updates and restarts, its
+// FP64 scalars held on the GPU (DPState): the inner products land in device
+// memory, single-thread kernels form rho/beta, sigma/alpha, the residual norm
+// and the 3 x 3 minimal-residual step, and the vector updates read their
+// coefficients from the state.  The host waits once per iteration (for the
+// residual, the breakdown status and the reliable-update tests); the
+// reference waits for every inner product (cu:1190-1255).
+struct DPState {
+  double2 alpha, omega, sigma, rho0, rho1, beta;
+  double2 one, mone;
+  double2 co[3];           // -beta, alpha, -alpha
+  double2 y1, y2, my1, my2;  // Y1, Y2 of the minimal-residual step and their negatives
+  double rnrm0, rnrm, mxnrmx, mxnrmr, resid;
+  int status, xpdt, rcmp, pad;
+};
+
+__host__ __device__ inline double dp_abs(double2 a) { return hypot(a.x, a.y); }
+__host__ __device__ inline double2 dp_conj(double2 a) { return make_double2(a.x, -a.y); }
+__host__ __device__ inline double2 dp_add(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__host__ __device__ inline double2 dp_sc(double s, double2 a) { return make_double2(s * a.x, s * a.y); }
+
+__global__ void k_dp_begin(DPState* S) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  S->rho0 = dq_neg(dq_mul(S->omega, S->rho0));
+}
+// rho1 = rr^H r_{k-1}, beta = alpha rho1 / rho0, rho0 = rho1
+__global__ void k_dp_rho(DPState* S, const double2* out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0 || S->status) return;
+  S->rho1 = out[0];
+  if (dq_zero(S->rho0)) { S->status = 95; return; }
+  S->beta = dq_mul(S->alpha, dq_div(S->rho1, S->rho0));
+  S->rho0 = S->rho1;
+  S->co[0] = dq_neg(S->beta);
+}
+// sigma = rr^H u_k, alpha = rho1 / sigma
+__global__ void k_dp_sigma(DPState* S, const double2* out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0 || S->status) return;
+  S->sigma = out[0];
+  if (dq_zero(S->sigma)) { S->status = 98; return; }
+  S->alpha = dq_div(S->rho1, S->sigma);
+  S->co[1] = S->alpha;
+  S->co[2] = dq_neg(S->alpha);
+}
+__global__ void k_dp_rnrm(DPState* S, const double2* out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0 || S->status) return;
+  S->rnrm = sqrt(fmax(0.0, out[0].x));
+  S->mxnrmx = fmax(S->mxnrmx, S->rnrm);
+  S->mxnrmr = fmax(S->mxnrmr, S->rnrm);
+}
+// the convex polynomial of cu:471-472 from the Gram matrix r_i^H r_j (lower
+// triangle r0r0, r1r0, r1r1, r2r0, r2r1, r2r2 in out[0..5]) and the
+// reliable-update tests of cu:474
+__global__ void k_dp_gram(DPState* SP, const double2* out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0 || SP->status) return;
+  DPState S = *SP;
+  double2 Zm[3][3];
+  Zm[0][0] = out[0]; Zm[1][0] = out[1]; Zm[1][1] = out[2];
+  Zm[2][0] = out[3]; Zm[2][1] = out[4]; Zm[2][2] = out[5];
+  Zm[0][1] = dp_conj(Zm[1][0]); Zm[0][2] = dp_conj(Zm[2][0]); Zm[1][2] = dp_conj(Zm[2][1]);
+  if (dq_zero(Zm[1][1])) { SP->status = 102; return; }
+  double2 y0[3] = {make_double2(-1.0, 0.0), dq_div(Zm[1][0], Zm[1][1]), make_double2(0.0, 0.0)};
+  double2 yl[3] = {make_double2(0.0, 0.0), dq_div(Zm[1][2], Zm[1][1]), make_double2(-1.0, 0.0)};
+  auto matv = [&](const double2* v, double2* o) {
+    for (int i = 0; i < 3; ++i) {
+      o[i] = make_double2(0.0, 0.0);
+      for (int j = 0; j < 3; ++j) o[i] = dp_add(o[i], dq_mul(Zm[i][j], v[j]));
+    }
+  };
+  auto inner = [](const double2* a, const double2* b) {
+    double2 sum = make_double2(0.0, 0.0);
+    for (int i = 0; i < 3; ++i) sum = dp_add(sum, dq_mul(dp_conj(a[i]), b[i]));
+    return sum;
+  };
+  double2 zy0[3], zyl[3];
+  matv(y0, zy0);
+  matv(yl, zyl);
+  const double k0 = sqrt(dp_abs(inner(y0, zy0))), kl = sqrt(dp_abs(inner(yl, zyl)));
+  if (k0 == 0.0 || kl == 0.0) { SP->status = 102; return; }
+  const double2 vr = dp_sc(1.0 / (k0 * kl), inner(yl, zy0));
+  const double avr = dp_abs(vr);
+  if (avr == 0.0) { SP->status = 102; return; }
+  const double2 fac = dp_sc((fmax(avr, 0.7) / avr) * (k0 / kl), vr);
+  for (int i = 0; i < 3; ++i) y0[i] = make_double2(y0[i].x - dq_mul(fac, yl[i]).x, y0[i].y - dq_mul(fac, yl[i]).y);
+  S.y1 = y0[1]; S.y2 = y0[2]; S.my1 = dq_neg(y0[1]); S.my2 = dq_neg(y0[2]);
+  S.omega = y0[2];
+  matv(y0, zy0);
+  S.rnrm = sqrt(dp_abs(inner(y0, zy0)));
+  S.mxnrmx = fmax(S.mxnrmx, S.rnrm);
+  S.mxnrmr = fmax(S.mxnrmr, S.rnrm);
+  const double delta = 1.0e-2;
+  S.xpdt = S.rnrm < delta * S.rnrm0 && S.rnrm0 < S.mxnrmx;
+  S.rcmp = (S.rnrm < delta * S.mxnrmr && S.rnrm0 < S.mxnrmr) || S.xpdt;
+  S.resid = S.rnrm0 > 0.0 ? S.rnrm / S.rnrm0 : 0.0;
+  *SP = S;
+}
+// d = cd d + ca a + cb b with coefficients read from device memory (null:
+// term absent; a zero cd drops d), k_lincomb's arithmetic
+template <typename C>
+__global__ void k_dp_lin(int n, C* d, const double2* cd, const C* a, const double2* ca, const C* b,
+                         const double2* cb, const int* status) {
+  if (*status) return;
+  const double2 zd = cd ? *cd : make_double2(0.0, 0.0), za = ca ? *ca : make_double2(0.0, 0.0),
+                zb = cb ? *cb : make_double2(0.0, 0.0);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    C v = mk<C>(0, 0);
+    if (!dq_zero(zd)) v = zmulv(zd, d[i]);
+    if (a) v = cadd(v, zmulv(za, a[i]));
+    if (b) v = cadd(v, zmulv(zb, b[i]));
+    d[i] = v;
+  }
+}
+
 template <typename T> int solve_pbcgs2(SolveIO<T>& io) {
   using C = cplx<T>;
   const char* name = "PBCGS2";
   Ctx<T> c(io, name);
   C *rr = c.w(0), *r[3] = {c.w(1), c.w(2), c.w(3)}, *u[3] = {c.w(4), c.w(5), c.w(6)};
   C *XP = c.w(7), *BP = c.w(8), *X = c.w(9);
+  DPState* dS = nullptr;
+  DPState* hS = nullptr;
+  cudaEvent_t ev = nullptr;
+  struct Free {
+    DPState*& a; DPState*& b; cudaEvent_t& e;
+    ~Free() { cudaFree(a); if (b) cudaFreeHost(b); if (e) cudaEventDestroy(e); }
+  } release{dS, hS, ev};
+  if (cudaMalloc((void**)&dS, sizeof(DPState)) != cudaSuccess || cudaMallocHost((void**)&hS, sizeof(DPState)) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    set_error(name, "scalar state allocation");
+    return 29;
+  }
   // init: rr=r0=BP=b, XP=x0, the rest 0 (cu:462)
   c.copy(XP, io.x);
   c.copy(rr, io.b); c.copy(r[0], io.b); c.copy(BP, io.b);
   c.zero(r[1]); c.zero(r[2]); c.zero(u[0]); c.zero(u[1]); c.zero(u[2]); c.zero(X);
   const double rnrm0 = c.nrm(r[0]);
   CK(92);
-  double rnrm = rnrm0, mxnrmx = rnrm0, mxnrmr = rnrm0;
-  Z alpha = 0.0, omega = 1.0, sigma = 1.0, rho0 = 1.0, rho1 = 0.0, beta;
-  double resid = rnrm0 > 0.0 ? 1.0 : 0.0;
+  DPState S{};
+  S.alpha = make_double2(0.0, 0.0); S.omega = make_double2(1.0, 0.0); S.sigma = make_double2(1.0, 0.0);
+  S.rho0 = make_double2(1.0, 0.0); S.rho1 = make_double2(0.0, 0.0);
+  S.one = make_double2(1.0, 0.0); S.mone = make_double2(-1.0, 0.0);
+  S.rnrm0 = rnrm0; S.rnrm = S.mxnrmx = S.mxnrmr = rnrm0;
+  S.resid = rnrm0 > 0.0 ? 1.0 : 0.0;
+  auto upload = [&]() -> int {
+    *hS = S;
+    if (cudaMemcpyAsync(dS, hS, sizeof(DPState), cudaMemcpyHostToDevice, c.st()) != cudaSuccess ||
+        cudaStreamSynchronize(c.st()) != cudaSuccess) {
+      set_error(name, "scalar state upload");
+      return 1;
+    }
+    return 0;
+  };
+  if (upload()) return 93;
+  double resid = S.resid;
+  const int n = c.n;
+  const unsigned gb = dq_grid(n);
+  const int* dst = &dS->status;
+  auto lin = [&](C* d, const double2* cd, const C* a, const double2* ca, const C* b = nullptr,
+                 const double2* cb = nullptr) {
+    k_dp_lin<C><<<gb, 256, 0, c.st()>>>(n, d, cd, a, ca, b, cb, dst);
+    note_launch();
+  };
+  const double2 *one = &dS->one, *mbeta = &dS->co[0], *calpha = &dS->co[1], *cmalpha = &dS->co[2];
   int it = 0;
   while (resid > io.tol && it < io.maxit) {
     ++it;
-    rho0 = -(omega * rho0);
+    k_dp_begin<<<1, 32, 0, c.st()>>>(dS);
+    note_launch();
     for (int k = 1; k <= 2; ++k) {
-      rho1 = c.dotc(rr, r[k - 1]);
-      CK(94);
-      if (rho0 == Z(0.0)) { set_error(name, "ZBCG2 breakdown: RHO0 == 0"); return 95; }
-      beta = alpha * (rho1 / rho0);
-      rho0 = rho1;
-      for (int j = 0; j < k; ++j) c.lin(u[j], -beta, r[j], 1.0);
+      {
+        const C* A1[1] = {rr};
+        const C* B1[1] = {r[k - 1]};
+        const int cj[1] = {1};
+        if (io.ops->dots_dev(n, 1, A1, B1, cj)) return 94;
+      }
+      k_dp_rho<<<1, 32, 0, c.st()>>>(dS, io.ops->d_out);
+      note_launch();
+      for (int j = 0; j < k; ++j) lin(u[j], mbeta, r[j], one);  // u_j = r_j - beta u_j
       MV(u[k - 1], u[k], 96);
-      sigma = c.dotc(rr, u[k]);
-      CK(97);
-      if (sigma == Z(0.0)) { set_error(name, "ZBCG2 breakdown: SIGMA == 0"); return 98; }
-      alpha = rho1 / sigma;
-      c.lin(X, 1.0, u[0], alpha);
-      for (int j = 0; j < k; ++j) c.lin(r[j], 1.0, u[j + 1], -alpha);
+      {
+        const C* A1[1] = {rr};
+        const C* B1[1] = {u[k]};
+        const int cj[1] = {1};
+        if (io.ops->dots_dev(n, 1, A1, B1, cj)) return 97;
+      }
+      k_dp_sigma<<<1, 32, 0, c.st()>>>(dS, io.ops->d_out);
+      note_launch();
+      lin(X, one, u[0], calpha);                                                  // X += alpha u0
+      for (int j = 0; j < k; ++j) lin(r[j], one, u[j + 1], cmalpha);              // r_j -= alpha u_{j+1}
       MV(r[k - 1], r[k], 99);
-      rnrm = c.nrm(r[0]);
-      CK(100);
-      mxnrmx = std::max(mxnrmx, rnrm);
-      mxnrmr = std::max(mxnrmr, rnrm);
+      {
+        const C* A1[1] = {r[0]};
+        const int cj[1] = {1};
+        if (io.ops->dots_dev(n, 1, A1, A1, cj)) return 100;
+      }
+      k_dp_rnrm<<<1, 32, 0, c.st()>>>(dS, io.ops->d_out);
+      note_launch();
     }
-    // Hermitian Gram matrix Z[i][j] = r_i^H r_j (lower triangle computed, cu:1215-1220)
-    Z Zm[3][3];
-    {
+    {  // Hermitian Gram matrix r_i^H r_j, lower triangle (cu:1215-1220)
       const C* A6[6] = {r[0], r[1], r[1], r[2], r[2], r[2]};
       const C* B6[6] = {r[0], r[0], r[1], r[0], r[1], r[2]};
       const int cj[6] = {1, 1, 1, 1, 1, 1};
-      double2 o[6];
-      if (io.ops->dots(c.n, 6, A6, B6, cj, o)) return 101;
-      Zm[0][0] = zd(o[0]); Zm[1][0] = zd(o[1]); Zm[1][1] = zd(o[2]);
-      Zm[2][0] = zd(o[3]); Zm[2][1] = zd(o[4]); Zm[2][2] = zd(o[5]);
-      Zm[0][1] = std::conj(Zm[1][0]); Zm[0][2] = std::conj(Zm[2][0]); Zm[1][2] = std::conj(Zm[2][1]);
+      if (io.ops->dots_dev(n, 6, A6, B6, cj)) return 101;
     }
-    // convex polynomial (cu:471-472)
-    if (Zm[1][1] == Z(0.0)) { set_error(name, "ZBCG2 convex-polynomial breakdown"); return 102; }
-    Z y0[3] = {-1.0, Zm[1][0] / Zm[1][1], 0.0};
-    Z yl[3] = {0.0, Zm[1][2] / Zm[1][1], -1.0};
-    auto matv = [&](const Z* v, Z* o) { for (int i = 0; i < 3; ++i) { o[i] = 0.0; for (int j = 0; j < 3; ++j) o[i] += Zm[i][j] * v[j]; } };
-    auto inner = [](const Z* a, const Z* b) { Z s = 0.0; for (int i = 0; i < 3; ++i) s += std::conj(a[i]) * b[i]; return s; };
-    Z zy0[3], zyl[3];
-    matv(y0, zy0);
-    matv(yl, zyl);
-    const double k0 = std::sqrt(std::abs(inner(y0, zy0))), kl = std::sqrt(std::abs(inner(yl, zyl)));
-    if (k0 == 0.0 || kl == 0.0) { set_error(name, "ZBCG2 convex-polynomial breakdown"); return 102; }
-    const Z vr = inner(yl, zy0) / (k0 * kl);
-    const double avr = std::abs(vr);
-    if (avr == 0.0) { set_error(name, "ZBCG2 convex-polynomial breakdown"); return 102; }
-    const Z hg = vr * (std::max(avr, 0.7) / avr);
-    const Z fac = hg * (k0 / kl);
-    for (int i = 0; i < 3; ++i) y0[i] -= fac * yl[i];
-    const Z Y1 = y0[1], Y2 = y0[2];
-    omega = y0[2];
-    matv(y0, zy0);
-    rnrm = std::sqrt(std::abs(inner(y0, zy0)));
-    mxnrmx = std::max(mxnrmx, rnrm);
-    mxnrmr = std::max(mxnrmr, rnrm);
+    k_dp_gram<<<1, 32, 0, c.st()>>>(dS, io.ops->d_out);
+    note_launch();
     // u0 -= Y1 u1 + Y2 u2 ; X += Y1 r0 + Y2 r1 ; r0 -= Y1 r1 + Y2 r2
-    c.lin(u[0], 1.0, u[1], -Y1, u[2], -Y2);
-    c.lin(X, 1.0, r[0], Y1, r[1], Y2);
-    c.lin(r[0], 1.0, r[1], -Y1, r[2], -Y2);
-    CK(103);
-    const double delta = 1.0e-2;
-    const bool xpdt = rnrm < delta * rnrm0 && rnrm0 < mxnrmx;
-    const bool rcmp = (rnrm < delta * mxnrmr && rnrm0 < mxnrmr) || xpdt;
-    resid = rnrm0 > 0.0 ? rnrm / rnrm0 : 0.0;
+    lin(u[0], one, u[1], &dS->my1, u[2], &dS->my2);
+    lin(X, one, r[0], &dS->y1, r[1], &dS->y2);
+    lin(r[0], one, r[1], &dS->my1, r[2], &dS->my2);
+    if (check_launch(name)) return 103;
+    if (cudaMemcpyAsync(hS, dS, sizeof(DPState), cudaMemcpyDeviceToHost, c.st()) != cudaSuccess ||
+        cudaEventRecord(ev, c.st()) != cudaSuccess || cudaEventSynchronize(ev) != cudaSuccess) {
+      set_error(name, "scalar state read-back");
+      return 103;
+    }
+    S = *hS;
+    if (S.status == 95) { set_error(name, "ZBCG2 breakdown: RHO0 == 0"); return 95; }
+    if (S.status == 98) { set_error(name, "ZBCG2 breakdown: SIGMA == 0"); return 98; }
+    if (S.status == 102) { set_error(name, "ZBCG2 convex-polynomial breakdown"); return 102; }
+    resid = S.resid;
+    bool changed = false;
     if ((it % RELIABLE_PERIOD) == 0 || resid <= io.tol) {
       double tres;
       bool conv, rest;
@@ -227,33 +487,37 @@ template <typename T> int solve_pbcgs2(SolveIO<T>& io) {
         c.copy(BP, r[0]);
         c.copy(rr, r[0]);
         c.zero(r[1]); c.zero(r[2]); c.zero(u[0]); c.zero(u[1]); c.zero(u[2]);
-        rnrm = mxnrmx = mxnrmr = tres * rnrm0;
-        alpha = 0.0; omega = 1.0; sigma = 1.0; rho0 = 1.0;
-        resid = tres;
+        S.rnrm = S.mxnrmx = S.mxnrmr = tres * rnrm0;
+        S.alpha = make_double2(0.0, 0.0); S.omega = make_double2(1.0, 0.0); S.sigma = make_double2(1.0, 0.0);
+        S.rho0 = make_double2(1.0, 0.0);
+        resid = S.resid = tres;
         CK(104);
+        if (upload()) return 104;
         if (io.verbose) std::printf(" PBCGS2 reliable restart at iteration %d\n", it);
         continue;
       }
     }
-    if (rcmp) {
+    if (S.rcmp) {
       MV(X, io.sy, 104);
       c.diff(r[0], BP, io.sy);
-      if (xpdt) {
+      if (S.xpdt) {
         c.lin(XP, 1.0, X, 1.0);
         c.zero(X);
         c.copy(BP, r[0]);
       }
-      mxnrmr = rnrm;
-      if (xpdt) mxnrmx = rnrm;
+      S.mxnrmr = S.rnrm;
+      if (S.xpdt) S.mxnrmx = S.rnrm;
       CK(104);
+      changed = true;
     }
+    if (changed && upload()) return 104;
     if (io.verbose) std::printf(" PBCGS2 iteration=%6d residual=%14.6E\n", it, resid);
   }
   // X = X + XP and one final true residual against the original b (cu:1259-1264)
   c.lin(X, 1.0, XP, 1.0);
   MV(X, io.sy, 105);
   c.diff(r[0], io.b, io.sy);
-  rnrm = c.nrm(r[0]);
+  const double rnrm = c.nrm(r[0]);
   CK(106);
   resid = rnrm0 > 0.0 ? rnrm / rnrm0 : INFINITY;
   c.copy(io.x, X);
@@ -272,12 +536,27 @@ template <typename T> int solve_qmrccg(SolveIO<T>& io) {
   const double bnorm = c.nrm(io.b);
   CK(52);
   if (bnorm == 0.0) { set_error(name, "zero RHS norm"); return 52; }
+  DQState* dS = nullptr;
+  DQState* hS = nullptr;
+  cudaEvent_t ev = nullptr;
+  struct Free {
+    DQState*& a; DQState*& b; cudaEvent_t& e;
+    ~Free() { cudaFree(a); if (b) cudaFreeHost(b); if (e) cudaEventDestroy(e); }
+  } release{dS, hS, ev};
+  if (cudaMalloc((void**)&dS, sizeof(DQState)) != cudaSuccess || cudaMallocHost((void**)&hS, sizeof(DQState)) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    set_error(name, "scalar state allocation");
+    return 29;
+  }
   c.copy(xs, io.x);
   MV(xs, io.sy, 53);
   c.diff(r, io.b, io.sy);
   c.zero(p); c.zero(ap); c.zero(q); c.zero(d); c.zero(s); c.zero(atw);
   c.copy(vt, r); c.copy(wt, r);
-  Z lambda, kappa, theta, gamma, ksi, rho, eps, mu, tau;
+  DQState S{};
+  S.bnorm = bnorm;
+  // initial scalars (host, as at every restart), then uploaded with the step coefficients
   auto init_scalars = [&]() -> int {
     const C* A3[3] = {vt, wt, vt};
     const C* B3[3] = {vt, wt, wt};
@@ -285,88 +564,76 @@ template <typename T> int solve_qmrccg(SolveIO<T>& io) {
     double2 o[3];
     if (io.ops->dots(c.n, 3, A3, B3, cj, o)) return 54;
     const double gn = std::sqrt(std::max(0.0, o[0].x)), kn = std::sqrt(std::max(0.0, o[1].x));
-    rho = zd(o[2]);
-    int rc = c.mv(wt, io.sy);
+    const double2 rho = o[2];
+    int rc = c.mv(wt, atw);
     if (rc) return rc;
-    c.copy(atw, io.sy);
-    eps = c.dotu(vt, atw);
+    const double2 eps = dz(c.dotu(vt, atw));
     if (c.err) return 54;
-    lambda = 1.0; kappa = -1.0; theta = -1.0; gamma = gn; ksi = kn; mu = 0.0;
-    if (rho == Z(0.0) || gamma == Z(0.0) || ksi == Z(0.0)) {
+    if (dq_zero(rho) || gn == 0.0 || kn == 0.0) {
       char msg[80];
-      std::snprintf(msg, sizeof(msg), "breakdown at step %d", rho == Z(0.0) ? 5 : (gamma == Z(0.0) ? 6 : 7));
+      std::snprintf(msg, sizeof(msg), "breakdown at step %d", dq_zero(rho) ? 5 : (gn == 0.0 ? 6 : 7));
       set_error(name, msg);
       return 55;
     }
-    tau = eps / rho;
+    S.lambda = make_double2(1.0, 0.0); S.kappa = make_double2(-1.0, 0.0); S.theta = make_double2(-1.0, 0.0);
+    S.gamma = make_double2(gn, 0.0); S.ksi = make_double2(kn, 0.0); S.mu = make_double2(0.0, 0.0);
+    S.rho = rho; S.eps = eps;
+    S.tau = dq_div(eps, rho);
+    S.status = 0;
+    dq_step_coefficients(S);
+    *hS = S;
+    if (cudaMemcpyAsync(dS, hS, sizeof(DQState), cudaMemcpyHostToDevice, c.st()) != cudaSuccess ||
+        cudaStreamSynchronize(c.st()) != cudaSuccess) {
+      set_error(name, "scalar state upload");
+      return 54;
+    }
     return 0;
   };
   int rc = init_scalars();
   if (rc) return rc;
   double resid = c.nrm(r) / bnorm;
   CK(55);
+  const int n = c.n;
+  const unsigned gb = dq_grid(n);
   int it = 0;
   while (it < io.maxit && resid > io.tol) {
     ++it;
-    // p = vt/gamma - mu p ; q = (atw - gamma mu q)/ksi
-    c.lin(p, -mu, vt, 1.0 / gamma);
-    c.lin(q, -(gamma * mu) / ksi, atw, 1.0 / ksi);
-    MV(p, io.sy, 56);
-    c.copy(ap, io.sy);
-    c.lin(vt, -(tau / gamma), io.sy, 1.0);
-    c.lin(wt, -(tau / ksi), q, 1.0);
-    double gn, kn;
-    Z new_rho;
+    k_dq_pq<C><<<gb, 256, 0, c.st()>>>(n, p, q, vt, atw, dS);
+    note_launch();
+    MV(p, ap, 56);
+    k_dq_vw<C><<<gb, 256, 0, c.st()>>>(n, vt, wt, ap, q, dS);
+    note_launch();
+    MV(wt, atw, 57);
     {
-      const C* A3[3] = {vt, wt, vt};
-      const C* B3[3] = {vt, wt, wt};
-      const int cj[3] = {1, 1, 0};
-      double2 o[3];
-      if (io.ops->dots(c.n, 3, A3, B3, cj, o)) return 57;
-      gn = std::sqrt(std::max(0.0, o[0].x));
-      kn = std::sqrt(std::max(0.0, o[1].x));
-      new_rho = zd(o[2]);
+      const C* A4[4] = {vt, wt, vt, vt};
+      const C* B4[4] = {vt, wt, wt, atw};
+      const int cj[4] = {1, 1, 0, 0};
+      if (io.ops->dots_dev(n, 4, A4, B4, cj)) return 57;
     }
-    MV(wt, io.sy, 57);
-    c.copy(atw, io.sy);
-    const Z new_eps = c.dotu(vt, atw);
-    CK(57);
-    // scalar recurrence (cu:442)
-    const Z gamma0 = gamma, ksi0 = ksi, rho0 = rho, tau0 = tau, kappa0 = kappa;
-    gamma = gn; ksi = kn; rho = new_rho; eps = new_eps;
-    int st = 0;
-    if (gamma == Z(0.0)) st = 6;
-    else if (ksi == Z(0.0)) st = 7;
-    Z den = gamma * tau * rho0;
-    if (!st && den == Z(0.0)) st = 12;
-    if (!st) {
-      mu = gamma0 * ksi0 * rho / den;
-      if (rho == Z(0.0)) st = 13;
+    k_dq_recur<<<1, 32, 0, c.st()>>>(dS, io.ops->d_out);
+    note_launch();
+    k_dq_dsxr<C><<<gb, 256, 0, c.st()>>>(n, d, s, xs, r, p, ap, dS);
+    note_launch();
+    {
+      const C* A1[1] = {r};
+      const int cj[1] = {1};
+      if (io.ops->dots_dev(n, 1, A1, A1, cj)) return 59;
     }
-    if (!st) {
-      tau = eps / rho - gamma * mu;
-      const double at0 = std::norm(tau0), ag = std::norm(gamma);
-      const Z den2 = lambda * at0 + ag;
-      if (den2 == Z(0.0)) st = 14;
-      else {
-        theta = ((1.0 - lambda) * at0) / den2;
-        kappa = -(gamma0 * std::conj(tau0) * kappa0) / den2;
-        lambda = (lambda * at0) / den2;
-      }
+    k_dq_resid<<<1, 32, 0, c.st()>>>(dS, io.ops->d_out);
+    note_launch();
+    if (check_launch(name)) return 59;
+    if (cudaMemcpyAsync(hS, dS, sizeof(DQState), cudaMemcpyDeviceToHost, c.st()) != cudaSuccess ||
+        cudaEventRecord(ev, c.st()) != cudaSuccess || cudaEventSynchronize(ev) != cudaSuccess) {
+      set_error(name, "scalar state read-back");
+      return 59;
     }
-    if (st) {
+    if (hS->status) {
       char msg[80];
-      std::snprintf(msg, sizeof(msg), "breakdown at step %d", st);
+      std::snprintf(msg, sizeof(msg), "breakdown at step %d", hS->status);
       set_error(name, msg);
       return 58;
     }
-    // d = theta d + kappa p ; s = theta s + kappa ap ; x += d ; r -= s
-    c.lin(d, theta, p, kappa);
-    c.lin(s, theta, ap, kappa);
-    c.lin(xs, 1.0, d, 1.0);
-    c.lin(r, 1.0, s, -1.0);
-    resid = c.nrm(r) / bnorm;
-    CK(59);
+    resid = hS->resid;
     if (io.verbose) std::printf(" QMRCCG iteration=%6d residual=%14.6E\n", it, resid);
     if ((it % RELIABLE_PERIOD) == 0 || resid <= io.tol) {
       double tres;

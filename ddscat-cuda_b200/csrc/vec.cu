@@ -148,6 +148,20 @@ int VecOps<T>::dots(int n, int k, const C* const* a, const C* const* b, const in
   return run_dots(*this, n, sp, host_out);
 }
 
+template <typename T>
+int VecOps<T>::dots_dev(int n, int k, const C* const* a, const C* const* b, const int* conjf) {
+  DotSpec<T> sp{};
+  sp.k = k;
+  sp.mode = 0;
+  for (int q = 0; q < k; ++q) { sp.a[q] = a[q]; sp.b[q] = b[q]; sp.conj[q] = conjf[q]; }
+  int nb = nblocks;
+  const int need = (int)ceil_div((size_t)std::max(n, 1), RED_THREADS);
+  if (need < nb) nb = need;
+  k_dots<T><<<nb, RED_THREADS, 0, stream>>>(n, sp, d_red, d_out, d_count);
+  note_launch();
+  return check_launch("FP64 inner product");
+}
+
 template <typename T> double2 VecOps<T>::dotc(int n, const C* a, const C* b, int* err) {
   double2 r = make_double2(0, 0);
   const int cj = 1;
