@@ -689,6 +689,73 @@ DDSCAT_CUDA_API int ddscat_cuda_scat_f32(int jpbc, int ndir, const float* ak, co
   return 0;
 }
 
+// Torque cross sections of the resident solution (DDSCAT's DOTORQ branch of
+// SCAT, getfml_cuda.f90:1135-1144, whose torque sums the reference leaves to
+// DDSCAT's CPU SCAT).  Physics restated in the oracle (scat_torque):
+//   C_inc  = 8 pi k / E02 sum_j [1/2 Re(P_j x E_j*) + (1/2) Im(P_j . E_j*) r_j x k]
+//   C_flux = k^4 / E02 sum_d w_d Im[-i k n x V - (n.S)(n x e*) + e* x e]
+// with e = S - n (n.S), V_b = sum_a e_a* U_ab over SCAT's integration directions.
+extern "C" DDSCAT_CUDA_API int ddscat_b200_scat_torque_f32(const float* ak, const float* dx, float e02, float etasca,
+                                                          const void* e01v, const float* x0, double* ctrq_inc,
+                                                          double* ctrq_flux, int* navg) {
+  clear_error();
+  if (!s.ready || !s.solution_valid || !ak || !dx || !x0 || !e01v || !ctrq_inc || !ctrq_flux || !navg ||
+      !(e02 > 0.f) || !(etasca > 0.f)) {
+    set_error("GPU torque", "invalid state/argument");
+    return 340;
+  }
+  const double ak2 = (double)ak[0] * ak[0] + (double)ak[1] * ak[1] + (double)ak[2] * ak[2], akk = std::sqrt(ak2);
+  const double pi = 4.0 * std::atan(1.0);
+  const double kd[3] = {ak[0], ak[1], ak[2]};
+  double gam[6];
+  int rc = incident_torque<float>(s.eng, s.d_sx, s.d_b, dx, x0, kd, gam, s.stream);
+  if (rc) return rc;
+  for (int k = 0; k < 3; ++k) ctrq_inc[k] = 8.0 * pi * akk * (gam[k] + gam[3 + k]) / (double)e02;
+  std::vector<IntDir> idirs;
+  if (make_integration_dirs(ak, (const C*)e01v, etasca, s.eng.g.nat0, idirs)) return 344;
+  const int nd = (int)idirs.size();
+  *navg = nd;
+  std::vector<double> hd((size_t)3 * nd);
+  for (int i = 0; i < nd; ++i)
+    for (int k = 0; k < 3; ++k) hd[3 * i + k] = idirs[i].k[k];
+  std::vector<double2> sums((size_t)12 * nd);
+  rc = farfield_torque_sums<float>(s.eng, s.d_sx, hd.data(), nd, dx, x0, sums.data(), s.stream);
+  if (rc) return rc == 325 ? 345 : rc;
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (int i = 0; i < nd; ++i) {
+    const double2* q = &sums[(size_t)12 * i];
+    double n[3];
+    for (int k = 0; k < 3; ++k) n[k] = hd[3 * i + k] / akk;
+    const double nsr = n[0] * q[0].x + n[1] * q[1].x + n[2] * q[2].x, nsi = n[0] * q[0].y + n[1] * q[1].y + n[2] * q[2].y;
+    double er[3], ei[3];
+    for (int a = 0; a < 3; ++a) { er[a] = q[a].x - n[a] * nsr; ei[a] = q[a].y - n[a] * nsi; }
+    // V_b = sum_a conj(e_a) U_ab
+    double vr[3], vi[3];
+    for (int b = 0; b < 3; ++b) {
+      vr[b] = vi[b] = 0.0;
+      for (int a = 0; a < 3; ++a) {
+        const double2 u = q[3 + 3 * a + b];
+        vr[b] += er[a] * u.x + ei[a] * u.y;
+        vi[b] += er[a] * u.y - ei[a] * u.x;
+      }
+    }
+    for (int c = 0; c < 3; ++c) {
+      const int c1 = (c + 1) % 3, c2 = (c + 2) % 3;
+      // Im(-i k (n x V)_c) = -k Re((n x V)_c)
+      const double t1 = -akk * (n[c1] * vr[c2] - n[c2] * vr[c1]);
+      // Im(-(n.S)(n x e*)_c), (n x e*)_c = n_c1 conj(e_c2) - n_c2 conj(e_c1)
+      const double xr = n[c1] * er[c2] - n[c2] * er[c1], xi = -(n[c1] * ei[c2] - n[c2] * ei[c1]);
+      const double t2 = -(nsr * xi + nsi * xr);
+      // Im((e* x e)_c) = Im(conj(e_c1) e_c2 - conj(e_c2) e_c1) = 2 (er_c1 ei_c2 - ei_c1 er_c2)
+      const double t3 = 2.0 * (er[c1] * ei[c2] - ei[c1] * er[c2]);
+      acc[c] += idirs[i].w[0] * (t1 + t2 + t3);
+    }
+  }
+  const double fac = ak2 * ak2 / (double)e02;
+  for (int k = 0; k < 3; ++k) ctrq_flux[k] = fac * acc[k];
+  return 0;
+}
+
 // ---- library extensions (declared in ddscat_b200.h) ----
 DDSCAT_CUDA_API int ddscat_b200_set_verbose(int level) {
   g_verbose = level < 0 ? -1 : (level > 2 ? 2 : level);

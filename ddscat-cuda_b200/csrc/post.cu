@@ -90,13 +90,20 @@ __global__ void k_pack_coords(const int* occ, int nat0, int nx, int ny, unsigned
   packed[q] = ix | (iy << 11) | (iz << 22);
 }
 
+// Site position r_j = ((i+1) + x0) * dx of the far-field sums, per axis
+struct SitePos {
+  float x0[3], dx[3];
+};
+
 // Partial sums of ND directions per block: phase products and per-thread
 // accumulation in TR (float for SCAT, double for the all-FP64 amplitudes),
-// block reduction in FP64.
-template <typename C, typename TR, int ND>
+// block reduction in FP64.  NS = 3: S_a = sum_j P_ja exp(-i k.r_j); NS = 12
+// adds the position moments U_ab = sum_j P_ja r_jb exp(-i k.r_j) (a-major)
+// that the scattered angular-momentum flux needs.
+template <typename C, typename TR, int ND, int NS = 3>
 __global__ void __launch_bounds__(FF_THREADS) k_ff_partial(const C* p, const unsigned* coords, int nat0, int ndir,
                                                            int nx, int ny, int nz, const cplx<TR>* tab,
-                                                           int sites_per_block, double2* partials) {
+                                                           int sites_per_block, double2* partials, SitePos pos) {
   using TC = cplx<TR>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   TC* st = reinterpret_cast<TC*>(smem_raw);
@@ -105,11 +112,12 @@ __global__ void __launch_bounds__(FF_THREADS) k_ff_partial(const C* p, const uns
   const int nd = min(ND, ndir - d0);
   for (int t = threadIdx.x; t < nd * ntab; t += blockDim.x) st[t] = tab[(size_t)d0 * ntab + t];
   __syncthreads();
-  TR acc[ND][6];
+  constexpr int NA = 2 * NS;  // real accumulators per direction
+  TR acc[ND][NA];
 #pragma unroll
   for (int d = 0; d < ND; ++d)
 #pragma unroll
-    for (int k = 0; k < 6; ++k) acc[d][k] = (TR)0;
+    for (int k = 0; k < NA; ++k) acc[d][k] = (TR)0;
   const int q0 = blockIdx.x * sites_per_block;
   const int q1 = min(nat0, q0 + sites_per_block);
   for (int q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
@@ -117,37 +125,54 @@ __global__ void __launch_bounds__(FF_THREADS) k_ff_partial(const C* p, const uns
     const int ix = pk & 2047u, iy = (pk >> 11) & 2047u, iz = pk >> 22;
     const double2 a = to_d(p[q]), b = to_d(p[q + nat0]), c = to_d(p[q + 2 * (size_t)nat0]);
     const TC px = mk<TC>(a.x, a.y), py = mk<TC>(b.x, b.y), pz = mk<TC>(c.x, c.y);
+    TR rr[3] = {(TR)0, (TR)0, (TR)0};
+    if constexpr (NS == 12) {
+      rr[0] = ((TR)(ix + 1) + (TR)pos.x0[0]) * (TR)pos.dx[0];
+      rr[1] = ((TR)(iy + 1) + (TR)pos.x0[1]) * (TR)pos.dx[1];
+      rr[2] = ((TR)(iz + 1) + (TR)pos.x0[2]) * (TR)pos.dx[2];
+    }
 #pragma unroll
     for (int d = 0; d < ND; ++d) {
       if (d < nd) {
         const TC* td = st + d * ntab;
         const TC e = cmul(cmul(td[ix], td[nx + iy]), td[nx + ny + iz]);
-        const TC sx = cmul(px, e), sy = cmul(py, e), sz = cmul(pz, e);
-        acc[d][0] += sx.x; acc[d][1] += sx.y;
-        acc[d][2] += sy.x; acc[d][3] += sy.y;
-        acc[d][4] += sz.x; acc[d][5] += sz.y;
+        const TC sa[3] = {cmul(px, e), cmul(py, e), cmul(pz, e)};
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+          acc[d][2 * m] += sa[m].x;
+          acc[d][2 * m + 1] += sa[m].y;
+        }
+        if constexpr (NS == 12) {
+#pragma unroll
+          for (int m = 0; m < 3; ++m)
+#pragma unroll
+            for (int b2 = 0; b2 < 3; ++b2) {
+              acc[d][6 + 6 * m + 2 * b2] += sa[m].x * rr[b2];
+              acc[d][7 + 6 * m + 2 * b2] += sa[m].y * rr[b2];
+            }
+        }
       }
     }
   }
   // block reduction in FP64: warp shuffles then shared memory
-  __shared__ double red[FF_THREADS / 32][ND * 6];
+  __shared__ double red[FF_THREADS / 32][ND * NA];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
   for (int d = 0; d < ND; ++d)
 #pragma unroll
-    for (int k = 0; k < 6; ++k) {
+    for (int k = 0; k < NA; ++k) {
       double v = (double)acc[d][k];
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-      if (lane == 0) red[wid][d * 6 + k] = v;
+      if (lane == 0) red[wid][d * NA + k] = v;
     }
   __syncthreads();
-  for (int t = threadIdx.x; t < nd * 6; t += blockDim.x) {
+  for (int t = threadIdx.x; t < nd * NA; t += blockDim.x) {
     double v = 0.0;
     for (int w = 0; w < FF_THREADS / 32; ++w) v += red[w][t];
-    const int d = t / 6, k = t % 6;
-    // partials[(dir)*3 + comp][block] as (re, im)
-    double* dst = reinterpret_cast<double*>(&partials[((size_t)(d0 + d) * 3 + k / 2) * gridDim.x + blockIdx.x]);
+    const int d = t / NA, k = t % NA;
+    // partials[(dir)*NS + sum][block] as (re, im)
+    double* dst = reinterpret_cast<double*>(&partials[((size_t)(d0 + d) * NS + k / 2) * gridDim.x + blockIdx.x]);
     dst[k & 1] = v;
   }
 }
@@ -165,8 +190,9 @@ __global__ void k_ff_final(const double2* partials, int nblocks, int rows, doubl
 }
 
 // Far-field sums of a compact polarisation p (device) over ndir directions,
-// phases and per-thread sums in TR, ND directions per block.
-template <typename C, typename TR, int ND>
+// phases and per-thread sums in TR, ND directions per block; NS sums per
+// direction (3: S, 12: S and the position moments U), sums_host[dir][NS].
+template <typename C, typename TR, int ND, int NS = 3>
 static int ff_sums_impl(const int* occ, int nx, int ny, int nz, int nat0, const C* p, const double* dirs_host, int ndir,
                         const double dx[3], const double x0[3], double2* sums_host, cudaStream_t s) {
   using TC = cplx<TR>;
@@ -183,14 +209,17 @@ static int ff_sums_impl(const int* occ, int nx, int ny, int nz, int nat0, const 
   cudaError_t e = cudaMalloc((void**)&coords, (size_t)nat0 * sizeof(unsigned));
   if (e == cudaSuccess) e = cudaMalloc((void**)&d_dirs, (size_t)3 * chunk * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc((void**)&tab, (size_t)chunk * ntab * sizeof(TC));
-  if (e == cudaSuccess) e = cudaMalloc((void**)&partials, (size_t)chunk * 3 * nblocks * sizeof(double2));
-  if (e == cudaSuccess) e = cudaMalloc((void**)&sums, (size_t)chunk * 3 * sizeof(double2));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&partials, (size_t)chunk * NS * nblocks * sizeof(double2));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&sums, (size_t)chunk * NS * sizeof(double2));
   if (e != cudaSuccess) { set_cuda_error("SCAT workspace", e); rc = 322; }
   if (!rc) {
     k_pack_coords<<<(unsigned)ceil_div(nat0, 256), 256, 0, s>>>(occ, nat0, nx, ny, coords);
     note_launch();
     const size_t sm = (size_t)ND * ntab * sizeof(TC);
-    cudaFuncSetAttribute((const void*)k_ff_partial<C, TR, ND>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute((const void*)k_ff_partial<C, TR, ND, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         200 * 1024);
+    SitePos pos;
+    for (int k = 0; k < 3; ++k) { pos.x0[k] = (float)x0[k]; pos.dx[k] = (float)dx[k]; }
     for (int off = 0; off < ndir && !rc; off += chunk) {
       const int cnt = std::min(chunk, ndir - off);
       cudaMemcpyAsync(d_dirs, dirs_host + (size_t)3 * off, (size_t)3 * cnt * sizeof(double), cudaMemcpyHostToDevice, s);
@@ -198,13 +227,14 @@ static int ff_sums_impl(const int* occ, int nx, int ny, int nz, int nat0, const 
           d_dirs, cnt, nx, ny, nz, dx[0], dx[1], dx[2], x0[0], x0[1], x0[2], tab);
       note_launch();
       dim3 grid((unsigned)nblocks, (unsigned)ceil_div(cnt, ND));
-      k_ff_partial<C, TR, ND><<<grid, FF_THREADS, sm, s>>>(p, coords, nat0, cnt, nx, ny, nz, tab, sites_per_block,
-                                                           partials);
+      k_ff_partial<C, TR, ND, NS><<<grid, FF_THREADS, sm, s>>>(p, coords, nat0, cnt, nx, ny, nz, tab,
+                                                               sites_per_block, partials, pos);
       note_launch();
-      k_ff_final<<<(unsigned)ceil_div((size_t)cnt * 3, 128), 128, 0, s>>>(partials, nblocks, cnt * 3, sums);
+      k_ff_final<<<(unsigned)ceil_div((size_t)cnt * NS, 128), 128, 0, s>>>(partials, nblocks, cnt * NS, sums);
       note_launch();
       if (check_launch("SCAT far-field sums")) { rc = 325; break; }
-      e = cudaMemcpyAsync(sums_host + (size_t)3 * off, sums, (size_t)3 * cnt * sizeof(double2), cudaMemcpyDeviceToHost, s);
+      e = cudaMemcpyAsync(sums_host + (size_t)NS * off, sums, (size_t)NS * cnt * sizeof(double2), cudaMemcpyDeviceToHost,
+                          s);
       if (e == cudaSuccess) e = cudaStreamSynchronize(s);
       if (e != cudaSuccess) { set_cuda_error("SCAT sums D2H", e); rc = 329; }
     }
@@ -222,6 +252,95 @@ int farfield_sums(Engine<T>& eng, const cplx<T>* p, const float* dirs_host, int 
   return ff_sums_impl<cplx<T>, float, FF_DIRS>(eng.occ, eng.g.nx, eng.g.ny, eng.g.nz, eng.g.nat0, p, hd.data(), ndir,
                                                dxd, x0d, sums_host, s);
 }
+
+template <typename T>
+int farfield_torque_sums(Engine<T>& eng, const cplx<T>* p, const double* dirs_host, int ndir, const float dx[3],
+                         const float x0[3], double2* sums_host, cudaStream_t s) {
+  const double dxd[3] = {dx[0], dx[1], dx[2]}, x0d[3] = {x0[0], x0[1], x0[2]};
+  return ff_sums_impl<cplx<T>, float, 2, 12>(eng.occ, eng.g.nx, eng.g.ny, eng.g.nz, eng.g.nat0, p, dirs_host, ndir, dxd,
+                                             x0d, sums_host, s);
+}
+
+// Torque of the incident field E on the dipoles P (compact), per block:
+// sum_j 1/2 Re(P_j x conj(E_j)) and sum_j (k/2) Im(P_j . conj(E_j)) r_j x k-hat*|k|,
+// six FP64 partials per block, folded in block order by k_torque_final.
+template <typename C>
+__global__ void __launch_bounds__(256) k_torque_inc(const C* p, const C* e, const int* occ, int nat0, int nx, int ny,
+                                                    SitePos pos, double kx, double ky, double kz, double* partials) {
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nat0; q += gridDim.x * blockDim.x) {
+    const int j = occ[q];
+    const double r0 = ((j % nx) + 1 + (double)pos.x0[0]) * pos.dx[0];
+    const double r1 = (((j / nx) % ny) + 1 + (double)pos.x0[1]) * pos.dx[1];
+    const double r2 = ((j / (nx * ny)) + 1 + (double)pos.x0[2]) * pos.dx[2];
+    const double2 p0 = to_d(p[q]), p1 = to_d(p[q + nat0]), p2 = to_d(p[q + 2 * (size_t)nat0]);
+    const double2 e0 = to_d(e[q]), e1 = to_d(e[q + nat0]), e2 = to_d(e[q + 2 * (size_t)nat0]);
+    // Re(a conj(b)) and Im(a conj(b))
+    auto rc = [](double2 a, double2 b) { return a.x * b.x + a.y * b.y; };
+    auto ic = [](double2 a, double2 b) { return a.y * b.x - a.x * b.y; };
+    acc[0] += 0.5 * (rc(p1, e2) - rc(p2, e1));
+    acc[1] += 0.5 * (rc(p2, e0) - rc(p0, e2));
+    acc[2] += 0.5 * (rc(p0, e1) - rc(p1, e0));
+    const double w = 0.5 * (ic(p0, e0) + ic(p1, e1) + ic(p2, e2));
+    acc[3] += w * (r1 * kz - r2 * ky);
+    acc[4] += w * (r2 * kx - r0 * kz);
+    acc[5] += w * (r0 * ky - r1 * kx);
+  }
+  __shared__ double red[8][6];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    double v = acc[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) red[wid][k] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    double v = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[w][threadIdx.x];
+    partials[(size_t)blockIdx.x * 6 + threadIdx.x] = v;
+  }
+}
+
+__global__ void k_torque_final(const double* partials, int nblocks, double* out) {
+  const int k = threadIdx.x;
+  if (k >= 6) return;
+  double v = 0.0;
+  for (int b = 0; b < nblocks; ++b) v += partials[(size_t)b * 6 + k];
+  out[k] = v;
+}
+
+// gamma[0..2]: spin part, gamma[3..5]: orbital part of the incident-field torque
+template <typename T>
+int incident_torque(Engine<T>& eng, const cplx<T>* p, const cplx<T>* e, const float dx[3], const float x0[3],
+                    const double k[3], double gamma[6], cudaStream_t s) {
+  const int nat0 = eng.g.nat0;
+  const int nblocks = (int)std::min<size_t>(ceil_div((size_t)nat0, 256), 1184);
+  double* d = nullptr;
+  cudaError_t e1 = cudaMalloc((void**)&d, ((size_t)nblocks * 6 + 6) * sizeof(double));
+  if (e1 != cudaSuccess) { set_cuda_error("torque workspace", e1); return 341; }
+  SitePos pos;
+  for (int i = 0; i < 3; ++i) { pos.x0[i] = x0[i]; pos.dx[i] = dx[i]; }
+  k_torque_inc<<<(unsigned)nblocks, 256, 0, s>>>(p, e, eng.occ, nat0, eng.g.nx, eng.g.ny, pos, k[0], k[1], k[2], d + 6);
+  note_launch();
+  k_torque_final<<<1, 32, 0, s>>>(d + 6, nblocks, d);
+  note_launch();
+  int rc = 0;
+  if (check_launch("torque sums")) rc = 342;
+  if (!rc) {
+    e1 = cudaMemcpyAsync(gamma, d, 6 * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e1 == cudaSuccess) e1 = cudaStreamSynchronize(s);
+    if (e1 != cudaSuccess) { set_cuda_error("torque sums D2H", e1); rc = 343; }
+  }
+  cudaFree(d);
+  return rc;
+}
+
+template int farfield_torque_sums<float>(Engine<float>&, const float2*, const double*, int, const float*, const float*,
+                                         double2*, cudaStream_t);
+template int incident_torque<float>(Engine<float>&, const float2*, const float2*, const float*, const float*,
+                                    const double*, double*, cudaStream_t);
 
 int farfield_sums_f64(const int* occ, int nx, int ny, int nz, int nat0, const double2* p, const double* dirs_host,
                       int ndir, const double dx[3], const double x0[3], double2* sums_host, cudaStream_t s) {

@@ -49,6 +49,18 @@ template <typename T>
 int farfield_sums(Engine<T>& eng, const cplx<T>* p, const float* dirs_host, int ndir, const float dx[3], const float x0[3],
                   double2* sums_host, cudaStream_t s);
 
+// S and the position moments of the scattered angular-momentum flux:
+// sums[d][0..2] = S_a, sums[d][3 + 3a + b] = U_ab = sum_j P_a(j) r_jb exp(-i k_d . r_j)
+// (k_d given in FP64); FP32 phases and per-thread sums, FP64 block sums.
+template <typename T>
+int farfield_torque_sums(Engine<T>& eng, const cplx<T>* p, const double* dirs_host, int ndir, const float dx[3],
+                         const float x0[3], double2* sums_host, cudaStream_t s);
+// Torque of the incident field e on the dipoles p (both compact, device):
+// gamma[0..2] = sum 1/2 Re(P x conj(E)), gamma[3..5] = sum (1/2) Im(P.conj(E)) r x k.
+template <typename T>
+int incident_torque(Engine<T>& eng, const cplx<T>* p, const cplx<T>* e, const float dx[3], const float x0[3],
+                    const double k[3], double gamma[6], cudaStream_t s);
+
 // The same sums with FP64 phases and FP64 accumulation (all-FP64 amplitudes);
 // occ: compact -> site map of the grid, p: compact complex-double polarisation.
 int farfield_sums_f64(const int* occ, int nx, int ny, int nz, int nat0, const double2* p, const double* dirs_host,

@@ -32,7 +32,7 @@ EXPORTS = (
        "ddscat_b200_solve_batch_f64", "ddscat_b200_adjoint_f32", "ddscat_b200_multi_solve_f32",
        "ddscat_b200_autotune_f32", "ddscat_b200_mueller_f64", "ddscat_b200_scat_amplitudes_f64",
        "ddscat_b200_scat_csca_f64", "ddscat_b200_make_inputs_pol_f32", "ddscat_b200_adjoint_fwd_f32",
-       "ddscat_b200_ffweights_f32"]
+       "ddscat_b200_ffweights_f32", "ddscat_b200_scat_torque_f32"]
 )
 
 
@@ -116,6 +116,8 @@ def _declare(lib):
     lib.ddscat_b200_scat_amplitudes_f64.restype = _I
     lib.ddscat_b200_scat_csca_f64.argtypes = [_I, _P, _P, _P, _F, _P, _P, _F, _P, _P, _P, _P, _P]
     lib.ddscat_b200_scat_csca_f64.restype = _I
+    lib.ddscat_b200_scat_torque_f32.argtypes = [_P, _P, _F, _F, _P, _P, _P, _P, ct.POINTER(_I)]
+    lib.ddscat_b200_scat_torque_f32.restype = _I
     lib.ddscat_b200_launch_count.argtypes = []
     lib.ddscat_b200_launch_count.restype = ct.c_ulonglong
 
@@ -268,6 +270,22 @@ class DDA:
         self._check("scat", rc)
         return {"cbksca": cb.value, "csca": cs.value, "cscag": [cg[0], cg[1], cg[2]], "cscag2": cg2.value,
                 "navg": navg.value, "f1": f1[:ndir], "f2": f2[:ndir]}
+
+    def scat_torque(self, ak, e01, x0, dx=(1.0, 1.0, 1.0), etasca=0.5, e02=1.0):
+        """Radiative torque cross sections of the resident solution (DDSCAT's
+        DOTORQ): dict with ctrq_inc (incident-field torque), ctrq_flux (angular
+        momentum carried off by the scattered light), ctrq = ctrq_inc - ctrq_flux
+        (net), each a 3-vector in the frame of ak, and navg."""
+        akf = np.ascontiguousarray(ak, dtype=np.float32)
+        dxf = np.ascontiguousarray(dx, dtype=np.float32)
+        x0f = np.ascontiguousarray(x0, dtype=np.float32)
+        e01c = _c64(e01, 3)
+        cinc, cflux = np.zeros(3), np.zeros(3)
+        navg = _I(0)
+        rc = self.lib.ddscat_b200_scat_torque_f32(_ptr(akf), _ptr(dxf), e02, etasca, _ptr(e01c), _ptr(x0f),
+                                                  _ptr(cinc), _ptr(cflux), ct.byref(navg))
+        self._check("scat_torque", rc)
+        return {"ctrq_inc": cinc, "ctrq_flux": cflux, "ctrq": cinc - cflux, "navg": navg.value}
 
     def solve_batch(self, name, b, x, adia, aoff=None, maxit=300, tol=1e-5, check=True, replace=False,
                     symmetric=False, graph=False):

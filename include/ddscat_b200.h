@@ -173,6 +173,26 @@ DDSCAT_CUDA_API int ddscat_b200_scat_csca_f64(int nrhs, const void *x, const flo
                                               double *cbksca, double *csca, double *cscag, double *cscag2,
                                               int *navg);
 
+/* Radiative torque of the resident solution, DDSCAT's CMDTRQ = 'DOTORQ'
+ * branch of SCAT (getfml_cuda.f90:1135-1144 sends it to DDSCAT's CPU SCAT,
+ * whose torque sums are not part of the reference).  Requires a resident
+ * solution P and incident field E (after a solver call or a non-resident
+ * EVALQ).  Outputs torque cross sections C = 8 pi k Gamma / E02 in the frame of
+ * AK (divide by pi a_eff^2 for DDSCAT's Q_Gamma):
+ *   ctrq_inc[3]  torque of the incident field on the induced dipoles,
+ *                sum_j 1/2 Re(P_j x E_j*) + (1/2) Im(P_j . E_j*) r_j x k
+ *                (the angular momentum removed from the incident beam);
+ *   ctrq_flux[3] angular momentum carried off by the scattered light, the
+ *                far-field flux integrated over SCAT's ETASCA direction set;
+ *   net radiative torque = ctrq_inc - ctrq_flux.
+ * r_j = ((i+1)+X0)*DX as in SCAT; the direction set and navg as in
+ * ddscat_cuda_scat_f32 for AK, CXE01 and ETASCA.  Codes: 340 invalid
+ * state/argument, 341-343 incident-torque workspace/kernel/transfer, 344 bad
+ * CXE01, 345/322/329 far-field sums. */
+DDSCAT_CUDA_API int ddscat_b200_scat_torque_f32(const float *ak, const float *dx, float e02, float etasca,
+                                                const void *e01, const float *x0, double *ctrq_inc,
+                                                double *ctrq_flux, int *navg);
+
 /* Right-hand sides and CXADIA for nrhs incident waves, generated on the GPU
  * for the prepared target (DDSCAT computes them on the host in EVALE and
  * ALPHADIAG; no counterpart in the reference ABI).  k: nrhs x 3 wave vectors in

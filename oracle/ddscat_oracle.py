@@ -1502,6 +1502,90 @@ def scat(p_c, occ, nx, ny, jpbc, ak, aks, dx, em1, em2, e02, etasca, e01, x0):
 
 
 # --------------------------------------------------------------------------
+# Radiative torque (DDSCAT's CMDTRQ = 'DOTORQ' branch of SCAT,
+# getfml_cuda.f90:1135-1144; DDSCAT's own SCAT torque sums are not vendored in
+# the reference, so this restates the physics from first principles).
+#
+# Units as in EVALQ/SCAT: P in the solver's normalisation (A P = E), the torque
+# reported as a cross section C = 8 pi k Gamma / E02 (Q = C / (pi a_eff^2) is
+# DDSCAT's Q_Gamma = Gamma / (pi a_eff^2 u_rad / k) with u_rad = E02 / 8 pi).
+#   incident part  Gamma_inc = sum_j 1/2 Re(P_j x E_j*) + r_j x (k/2) Im(P_j . E_j*)
+#                  (time-averaged torque of the incident plane wave on the
+#                  induced dipoles: the angular momentum it loses, whose
+#                  momentum counterpart is C_ext k-hat)
+#   scattered flux L_sca = 1/(8 pi k) Int dOmega Im[F_a* (n x grad_n) F_a + F* x F]
+#                  with F = k^2 (S - n (n.S)), S = sum_j P_j exp(-i k n.r_j):
+#                  (n x grad_n) F_a expands to -i k n x U_a . and -(n x F*)(n.S)
+#                  terms, U_ab = sum_j P_ja r_jb exp(-i k n.r_j)
+#   net torque     C_net = C_inc - C_flux
+# r_j as in SCAT: ((i+1) + x0) * dx.  The angular integration uses SCAT's
+# ETASCA quadrature (scat_integration_dirs, first weight column).
+# --------------------------------------------------------------------------
+def site_positions(occ, nx, ny, dx, x0):
+    ix = occ % nx
+    iy = (occ // nx) % ny
+    iz = occ // (nx * ny)
+    return np.stack([(ix + 1 + float(x0[0])) * float(dx[0]),
+                     (iy + 1 + float(x0[1])) * float(dx[1]),
+                     (iz + 1 + float(x0[2])) * float(dx[2])], axis=1)
+
+
+def torque_incident(p_c, e_c, r, ak, e02):
+    """C_inc (3,) of the incident field E (compact) on the dipoles P at r."""
+    nat0 = r.shape[0]
+    p = np.asarray(p_c, dtype=np.complex128).reshape(3, nat0).T
+    e = np.asarray(e_c, dtype=np.complex128).reshape(3, nat0).T
+    ak = np.asarray([float(a) for a in ak])
+    akk = float(np.linalg.norm(ak))
+    spin = 0.5 * np.real(np.cross(p, np.conj(e))).sum(axis=0)
+    w = 0.5 * np.imag(np.sum(p * np.conj(e), axis=1))
+    orb = (np.cross(r, ak[None, :]) * w[:, None]).sum(axis=0)
+    return 8.0 * math.pi * akk * (spin + orb) / e02
+
+
+def torque_flux_sums(p_c, r, dirs):
+    """S (ndir,3) and U (ndir,3,3), U[:,a,b] = sum_j P_ja r_jb exp(-i k_s . r_j)."""
+    nat0 = r.shape[0]
+    p = np.asarray(p_c, dtype=np.complex128).reshape(3, nat0).T
+    d64 = np.asarray(dirs, dtype=np.float64)
+    S = np.empty((len(d64), 3), dtype=np.complex128)
+    U = np.empty((len(d64), 3, 3), dtype=np.complex128)
+    pr = (p[:, :, None] * r[:, None, :]).reshape(nat0, 9)
+    chunk = max(1, 2_000_000 // max(nat0, 1))
+    for s in range(0, len(d64), chunk):
+        ph = np.exp(-1j * (d64[s:s + chunk] @ r.T))
+        S[s:s + chunk] = ph @ p
+        U[s:s + chunk] = (ph @ pr).reshape(-1, 3, 3)
+    return S, U
+
+
+def torque_flux_integrand(n, S, U, akk):
+    """Im[-i k n x V - (n.S)(n x e*) + e* x e] per direction, e = S - n(n.S),
+    V_b = sum_a e_a* U_ab (the bracket of L_sca without the k^4 factor)."""
+    nS = np.sum(n * S, axis=1)
+    e = S - n * nS[:, None]
+    V = np.einsum("da,dab->db", np.conj(e), U)
+    val = -1j * akk * np.cross(n, V) - nS[:, None] * np.cross(n, np.conj(e)) + np.cross(np.conj(e), e)
+    return np.imag(val)
+
+
+def scat_torque(p_c, e_c, occ, nx, ny, ak, dx, e02, etasca, e01, x0):
+    """Torque cross sections of the resident solution: dict with ctrq_inc (3),
+    ctrq_flux (3), ctrq (3) = inc - flux, navg."""
+    nat0 = occ.size
+    ak = [float(np.float32(a)) for a in ak]
+    akk = math.sqrt(sum(a * a for a in ak))
+    r = site_positions(occ, nx, ny, dx, x0)
+    cinc = torque_incident(p_c, e_c, r, ak, e02)
+    dirs, w = scat_integration_dirs(ak, e01, etasca, nat0)
+    S, U = torque_flux_sums(p_c, r, dirs)
+    n = dirs.astype(np.float64) / akk
+    f = torque_flux_integrand(n, S, U, akk)
+    cflux = akk ** 4 / e02 * (w[:, 0] @ f)
+    return {"ctrq_inc": cinc, "ctrq_flux": cflux, "ctrq": cinc - cflux, "navg": len(dirs)}
+
+
+# --------------------------------------------------------------------------
 # Amplitude and Mueller matrices (the S_ij step DDSCAT's GETMUELLER performs
 # after SCAT; GETMUELLER itself is not in the reference).  Restated from the
 # definitions of Bohren & Huffman (1983), "Absorption and Scattering of Light by
