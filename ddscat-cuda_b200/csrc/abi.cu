@@ -12,6 +12,7 @@
 #include <vector>
 #include <atomic>
 #include <mutex>
+#include <thread>
 #include "ddscat_b200.h"
 #include "batch.h"
 #include "solvers.h"
@@ -57,6 +58,7 @@ struct State {
   cudaStream_t stream = 0;
   C *d_xf = nullptr, *d_yf = nullptr, *d_adia = nullptr, *d_aoff = nullptr;  // full 3*NAT
   C *d_b = nullptr, *d_sx = nullptr, *d_sy = nullptr, *d_work = nullptr;     // compact
+  C *d_adia_c = nullptr, *d_aoff_c = nullptr;  // compact CXADIA / CXAOFF of the current solve
   bool aoff_zero = false;
   // how the target was prepared (for the all-FP64 engine built on demand)
   int prep_kind = 0;  // 1 prepare_green, 2 prepare (CPU Green)
@@ -126,6 +128,7 @@ static void release_state() {
   if (s.ready || s.eng.green) {
     cudaFree(s.d_xf); cudaFree(s.d_yf); cudaFree(s.d_adia); cudaFree(s.d_aoff);
     cudaFree(s.d_b); cudaFree(s.d_sx); cudaFree(s.d_sy); cudaFree(s.d_work);
+    cudaFree(s.d_adia_c); cudaFree(s.d_aoff_c);
     s.ops.release();
     s.eng.release();
   }
@@ -162,6 +165,7 @@ static int allocate_runtime() {
   auto M = [&](C** p, size_t cnt) { if (e == cudaSuccess) e = cudaMalloc((void**)p, cnt * sizeof(C)); };
   M(&s.d_xf, n); M(&s.d_yf, n); M(&s.d_adia, n); M(&s.d_aoff, n);
   M(&s.d_b, cn); M(&s.d_sx, cn); M(&s.d_sy, cn); M(&s.d_work, 13 * cn);
+  M(&s.d_adia_c, cn); M(&s.d_aoff_c, cn);
   if (e != cudaSuccess) { set_cuda_error("allocate runtime", e); return 204; }
   if (s.ops.init(s.stream)) return 204;
   s.eng.stream = s.stream;
@@ -170,24 +174,61 @@ static int allocate_runtime() {
   return 0;
 }
 
+// True when every byte of the host array is zero: 64-bit words, large arrays
+// split over up to 8 host threads (a full DDSCAT vector at 128^3 is 50 MB).
+static bool zero_words(const unsigned char* c, size_t bytes) {
+  size_t i = 0;
+  for (; i < bytes && ((uintptr_t)(c + i) & 7u); ++i)
+    if (c[i]) return false;
+  const uint64_t* w = reinterpret_cast<const uint64_t*>(c + i);
+  const size_t nw = (bytes - i) / 8;
+  for (size_t k = 0; k < nw; k += 64) {
+    uint64_t acc = 0;
+    const size_t e = std::min(nw, k + 64);
+    for (size_t j = k; j < e; ++j) acc |= w[j];
+    if (acc) return false;
+  }
+  for (i += nw * 8; i < bytes; ++i)
+    if (c[i]) return false;
+  return true;
+}
 static bool all_zero(const void* p, size_t bytes) {
   const unsigned char* c = (const unsigned char*)p;
-  for (size_t i = 0; i < bytes; ++i)
-    if (c[i]) return false;
+  const size_t part = (size_t)8 << 20;
+  const int nt = (int)std::min<size_t>(8, (bytes + part - 1) / part);
+  if (nt <= 1) return zero_words(c, bytes);
+  std::vector<std::thread> th;
+  std::vector<char> res(nt, 0);
+  const size_t chunk = (bytes + nt - 1) / nt;
+  for (int k = 0; k < nt; ++k) {
+    const size_t off = (size_t)k * chunk, len = std::min(chunk, bytes - std::min(bytes, off));
+    th.emplace_back([&, k, off, len]() { res[k] = zero_words(c + off, len) ? 1 : 0; });
+  }
+  for (auto& t : th) t.join();
+  for (char r : res)
+    if (!r) return false;
   return true;
 }
 
 static int upload_operators(const void* adia, const void* aoff) {
   const size_t b = (size_t)3 * s.eng.g.nat * sizeof(C);
+  // zero CXAOFF (isotropic materials) contributes nothing: neither copied nor read
+  s.aoff_zero = all_zero(aoff, b);
   cudaError_t e = cudaMemcpy(s.d_adia, adia, b, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(s.d_aoff, aoff, b, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && !s.aoff_zero) e = cudaMemcpy(s.d_aoff, aoff, b, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) { set_cuda_error("operator H2D", e); return 1; }
-  s.aoff_zero = all_zero(aoff, b);  // zero CXAOFF contributes nothing: skip its reads
   return 0;
 }
 
-static int upload_full_to_compact(const void* host, C* compact) {
+// maybe_zero: the array may be all zero (an initial guess): then the compact
+// vector is cleared on the device instead of copied
+static int upload_full_to_compact(const void* host, C* compact, bool maybe_zero = false) {
   const size_t b = (size_t)3 * s.eng.g.nat * sizeof(C);
+  if (maybe_zero && all_zero(host, b)) {
+    const cudaError_t z = cudaMemsetAsync(compact, 0, (size_t)3 * s.eng.g.nat0 * sizeof(C), s.stream);
+    if (z != cudaSuccess) { set_cuda_error("zero initial guess", z); return 1; }
+    return 0;
+  }
   cudaError_t e = cudaMemcpy(s.d_xf, host, b, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) { set_cuda_error("full vector H2D", e); return 1; }
   v_gather<float>(s.d_xf, compact, s.eng.occ, s.eng.g.nat, s.eng.g.nat0, s.stream);
@@ -224,13 +265,19 @@ static int run_solver(const SolverCodes& sc, SolveFn fn, const void* b, void* x,
   if (!s.d_work) { set_error(sc.name, "Krylov workspace missing"); return sc.workspace; }
   s.solution_valid = false;
   if (upload_full_to_compact(b, s.d_b)) return sc.h2d;
-  if (upload_full_to_compact(x, s.d_sx)) return sc.h2d;
+  if (upload_full_to_compact(x, s.d_sx, true)) return sc.h2d;
   if (upload_operators(adia, aoff)) return sc.h2d;
+  // the MATVEC's finish reads CXADIA / CXAOFF in the layout of x: compact
+  // copies let it stage them with x in shared memory
+  v_gather<float>(s.d_adia, s.d_adia_c, s.eng.occ, s.eng.g.nat, s.eng.g.nat0, s.stream);
+  if (!s.aoff_zero) v_gather<float>(s.d_aoff, s.d_aoff_c, s.eng.occ, s.eng.g.nat, s.eng.g.nat0, s.stream);
+  if (check_launch("CXADIA/CXAOFF gather")) return sc.h2d;
   SolveIO<float> io;
   io.eng = &s.eng; io.ops = &s.ops; io.stream = s.stream;
   io.n = 3 * s.eng.g.nat0;
   io.b = s.d_b; io.x = s.d_sx;
-  io.adia = s.d_adia; io.aoff = s.aoff_zero ? nullptr : s.d_aoff; io.a_full = 1;
+  io.adia = s.d_adia_c; io.aoff = s.aoff_zero ? nullptr : s.d_aoff_c; io.a_full = 0;
+  io.adia_full = s.d_adia;
   io.work = s.d_work; io.sy = s.d_sy;
   io.maxit = maxit; io.tol = (double)tol; io.verbose = verbose_level() >= 1;
   const int rc = fn(io);
@@ -553,9 +600,9 @@ DDSCAT_CUDA_API int ddscat_cuda_apply_f32(int cwhat, const void* x, void* y, con
   if (e != cudaSuccess) { set_cuda_error("x H2D", e); return 12; }
   e = cudaMemcpy(s.d_adia, adia, b, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) { set_cuda_error("adia H2D", e); return 13; }
-  e = cudaMemcpy(s.d_aoff, aoff, b, cudaMemcpyHostToDevice);
+  s.aoff_zero = all_zero(aoff, b);  // zero CXAOFF: neither copied nor read
+  if (!s.aoff_zero) e = cudaMemcpy(s.d_aoff, aoff, b, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) { set_cuda_error("aoff H2D", e); return 14; }
-  s.aoff_zero = all_zero(aoff, b);
   MvArgs<float> a;
   a.x = s.d_xf; a.y = s.d_yf; a.io_full = 1;
   a.adia = s.d_adia; a.aoff = s.aoff_zero ? nullptr : s.d_aoff; a.a_full = 1;

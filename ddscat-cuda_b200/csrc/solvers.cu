@@ -671,7 +671,8 @@ template <typename T> int solve_pbcgst(SolveIO<T>& io) {
   Ctx<T> c(io, name);
   C *r = c.w(0), *rt = c.w(1), *p = c.w(2), *sv = c.w(3), *v = c.w(4), *t = c.w(5), *xs = c.w(6), *rtrue = c.w(7);
   const Engine<T>& E = *io.eng;
-  auto precon = [&](C* dst, const C* src) { v_precon<T>(dst, src, io.adia, E.occ, E.g.nat, E.g.nat0, c.st()); };
+  const C* adia_full = io.adia_full ? io.adia_full : io.adia;  // the DIAGL preconditioner reads the full layout
+  auto precon = [&](C* dst, const C* src) { v_precon<T>(dst, src, adia_full, E.occ, E.g.nat, E.g.nat0, c.st()); };
   c.copy(xs, io.x);
   const double bnorm = c.nrm(io.b);
   CK(72);

@@ -14,6 +14,7 @@ template <typename T> struct SolveIO {
   const cplx<T>* adia = nullptr;    // CXADIA (layout a_full)
   const cplx<T>* aoff = nullptr;    // CXAOFF or null
   int a_full = 1;
+  const cplx<T>* adia_full = nullptr;  // CXADIA in the full layout (PBCGST's DIAGL preconditioner)
   cplx<T>* work = nullptr;          // 13*n scratch
   cplx<T>* sy = nullptr;            // n: MATVEC output staging
   int maxit = 0;

@@ -33,42 +33,64 @@ __device__ __forceinline__ double2 warp_sum(double2 v) {
   return v;
 }
 
-template <typename T>
+// KM: the largest product count of the launch (registers scale with it)
+template <typename T, int KM>
 __global__ void __launch_bounds__(RED_THREADS) k_dots(int n, DotSpec<T> sp, double2* partials, double2* out,
                                                       unsigned* count) {
   __shared__ double2 wsum[RED_MAXK][RED_THREADS / 32];
   __shared__ bool last;
-  double2 acc[RED_MAXK];
+  double2 acc[KM];
 #pragma unroll
-  for (int q = 0; q < RED_MAXK; ++q) acc[q] = make_double2(0.0, 0.0);
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-#pragma unroll
-    for (int q = 0; q < RED_MAXK; ++q) {
-      if (q >= sp.k) break;
-      const double2 a = to_d(sp.a[q][i]);
-      const double2 b = to_d(sp.b[q][i]);
-      if (sp.mode == 0) {
-        if (sp.conj[q]) {
-          acc[q].x += a.x * b.x + a.y * b.y;
-          acc[q].y += a.x * b.y - a.y * b.x;
-        } else {
-          acc[q].x += a.x * b.x - a.y * b.y;
-          acc[q].y += a.x * b.y + a.y * b.x;
-        }
+  for (int q = 0; q < KM; ++q) acc[q] = make_double2(0.0, 0.0);
+  // two elements per thread and round, all of a round's loads issued before
+  // its products, so that a thread keeps several loads in flight
+  auto term = [&](int q, const cplx<T>& av, const cplx<T>& bv, const cplx<T>* cp, int i) {
+    const double2 a = to_d(av), b = to_d(bv);
+    if (sp.mode == 0) {
+      if (sp.conj[q]) {
+        acc[q].x += a.x * b.x + a.y * b.y;
+        acc[q].y += a.x * b.y - a.y * b.x;
       } else {
-        double dr = a.x - b.x, di = a.y - b.y;
-        if (sp.mode == 2) {
-          const double2 c = to_d(sp.c[q][i]);
-          dr -= c.x;
-          di -= c.y;
-        }
-        acc[q].x += dr * dr + di * di;
+        acc[q].x += a.x * b.x - a.y * b.y;
+        acc[q].y += a.x * b.y + a.y * b.x;
       }
+    } else {
+      double dr = a.x - b.x, di = a.y - b.y;
+      if (sp.mode == 2) {
+        const double2 c = to_d(cp[i]);
+        dr -= c.x;
+        di -= c.y;
+      }
+      acc[q].x += dr * dr + di * di;
+    }
+  };
+  const int stride = gridDim.x * blockDim.x;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  for (; i + stride < n; i += 2 * stride) {
+    cplx<T> a0[KM], b0[KM], a1[KM], b1[KM];
+#pragma unroll
+    for (int q = 0; q < KM; ++q) {
+      if (q >= sp.k) break;
+      a0[q] = sp.a[q][i]; b0[q] = sp.b[q][i];
+      a1[q] = sp.a[q][i + stride]; b1[q] = sp.b[q][i + stride];
+    }
+#pragma unroll
+    for (int q = 0; q < KM; ++q) {
+      if (q >= sp.k) break;
+      term(q, a0[q], b0[q], sp.c[q], i);
+      term(q, a1[q], b1[q], sp.c[q], i + stride);
+    }
+  }
+  if (i < n) {
+#pragma unroll
+    for (int q = 0; q < KM; ++q) {
+      if (q >= sp.k) break;
+      term(q, sp.a[q][i], sp.b[q][i], sp.c[q], i);
     }
   }
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
-  for (int q = 0; q < RED_MAXK; ++q) {  // compile-time indices: acc stays in registers
+  for (int q = 0; q < KM; ++q) {  // compile-time indices: acc stays in registers
     if (q >= sp.k) break;
     double2 v = warp_sum(acc[q]);
     if (lane == 0) wsum[q][wid] = v;
@@ -109,7 +131,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_dots(int n, DotSpec<T> sp, doub
 
 template <typename T> int VecOps<T>::init(cudaStream_t s) {
   stream = s;
-  nblocks = 2 * 148;
+  nblocks = 8 * 148;  // capacity of the partials buffer; launch_dots sizes each launch to one resident wave
   cudaError_t e = cudaMalloc((void**)&d_red, (size_t)RED_MAXK * nblocks * sizeof(double2));
   if (e == cudaSuccess) e = cudaMalloc((void**)&d_out, RED_MAXK * sizeof(double2));
   if (e == cudaSuccess) e = cudaMalloc((void**)&d_count, sizeof(unsigned));
@@ -125,12 +147,25 @@ template <typename T> void VecOps<T>::release() {
   d_red = d_out = nullptr; d_count = nullptr; h_out = nullptr;
 }
 
+// One launch of KM-product blocks, as many as are resident at once (the
+// register count grows with KM; nb caps them at the partials buffer), so the
+// grid-stride loop runs in a single wave.
+template <typename T>
+static void launch_dots(int nb, cudaStream_t st, int n, DotSpec<T>& sp, double2* red, double2* out, unsigned* cnt) {
+  const int per_sm = sp.k <= 1 ? 8 : (sp.k <= 2 ? 6 : (sp.k <= 4 ? 3 : 2));
+  nb = std::min(nb, 148 * per_sm);
+  if (sp.k <= 1) k_dots<T, 1><<<nb, RED_THREADS, 0, st>>>(n, sp, red, out, cnt);
+  else if (sp.k <= 2) k_dots<T, 2><<<nb, RED_THREADS, 0, st>>>(n, sp, red, out, cnt);
+  else if (sp.k <= 4) k_dots<T, 4><<<nb, RED_THREADS, 0, st>>>(n, sp, red, out, cnt);
+  else k_dots<T, RED_MAXK><<<nb, RED_THREADS, 0, st>>>(n, sp, red, out, cnt);
+  note_launch();
+}
+
 template <typename T> static int run_dots(VecOps<T>& o, int n, DotSpec<T>& sp, double2* host_out) {
   int nb = o.nblocks;
   const int need = (int)ceil_div((size_t)std::max(n, 1), RED_THREADS);
   if (need < nb) nb = need;
-  k_dots<T><<<nb, RED_THREADS, 0, o.stream>>>(n, sp, o.d_red, o.d_out, o.d_count);
-  note_launch();
+  launch_dots<T>(nb, o.stream, n, sp, o.d_red, o.d_out, o.d_count);
   if (check_launch("FP64 inner product")) return 1;
   cudaError_t e = cudaMemcpyAsync(o.h_out, o.d_out, sp.k * sizeof(double2), cudaMemcpyDeviceToHost, o.stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(o.stream);
@@ -157,8 +192,7 @@ int VecOps<T>::dots_dev(int n, int k, const C* const* a, const C* const* b, cons
   int nb = nblocks;
   const int need = (int)ceil_div((size_t)std::max(n, 1), RED_THREADS);
   if (need < nb) nb = need;
-  k_dots<T><<<nb, RED_THREADS, 0, stream>>>(n, sp, d_red, d_out, d_count);
-  note_launch();
+  launch_dots<T>(nb, stream, n, sp, d_red, d_out, d_count);
   return check_launch("FP64 inner product");
 }
 
