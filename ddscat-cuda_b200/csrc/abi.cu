@@ -210,12 +210,85 @@ static bool all_zero(const void* p, size_t bytes) {
   return true;
 }
 
+// ---- copies of the caller's pageable host arrays ----
+// DDSCAT passes pageable Fortran arrays (a full vector is 50 MB at 128^3).  A
+// pageable cudaMemcpy is staged by the driver at a few GB/s; here the host side
+// of the staging is split over up to 8 threads into two pinned 8 MB buffers
+// that alternate with their DMA on the library stream.  Same semantics as the
+// synchronous copy for the caller: its array is read (or written) completely
+// before the call returns.
+constexpr size_t PIN_CHUNK = (size_t)8 << 20;
+struct PinnedStage {
+  char* buf[2] = {nullptr, nullptr};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  bool ok = false, tried = false;
+};
+static PinnedStage g_pin;
+
+static void par_copy(void* dst, const void* src, size_t bytes) {
+  const int nt = (int)std::min<size_t>(8, bytes >> 20);
+  if (nt <= 1) { std::memcpy(dst, src, bytes); return; }
+  const size_t ch = (bytes + nt - 1) / nt;
+  std::vector<std::thread> th;
+  for (int k = 0; k < nt; ++k) {
+    const size_t off = (size_t)k * ch, len = std::min(ch, bytes - std::min(bytes, off));
+    if (len) th.emplace_back([=]() { std::memcpy((char*)dst + off, (const char*)src + off, len); });
+  }
+  for (auto& t : th) t.join();
+}
+
+static bool pin_ready() {
+  if (g_pin.tried) return g_pin.ok;
+  g_pin.tried = true;
+  bool ok = true;
+  for (int k = 0; k < 2 && ok; ++k)
+    ok = cudaMallocHost((void**)&g_pin.buf[k], PIN_CHUNK) == cudaSuccess &&
+         cudaEventCreateWithFlags(&g_pin.ev[k], cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) cudaGetLastError();  // fall back to pageable copies
+  g_pin.ok = ok;
+  return ok;
+}
+
+static cudaError_t copy_h2d(void* dev, const void* host, size_t bytes) {
+  if (bytes < 2 * PIN_CHUNK || !pin_ready()) return cudaMemcpy(dev, host, bytes, cudaMemcpyHostToDevice);
+  cudaError_t e = cudaSuccess;
+  int k = 0;
+  for (size_t off = 0; off < bytes && e == cudaSuccess; off += PIN_CHUNK, k ^= 1) {
+    const size_t n = std::min(PIN_CHUNK, bytes - off);
+    e = cudaEventSynchronize(g_pin.ev[k]);  // the DMA that last read buf[k] has finished
+    if (e != cudaSuccess) break;
+    par_copy(g_pin.buf[k], (const char*)host + off, n);
+    e = cudaMemcpyAsync((char*)dev + off, g_pin.buf[k], n, cudaMemcpyHostToDevice, s.stream);
+    if (e == cudaSuccess) e = cudaEventRecord(g_pin.ev[k], s.stream);
+  }
+  return e;
+}
+
+static cudaError_t copy_d2h(void* host, const void* dev, size_t bytes) {
+  if (bytes < 2 * PIN_CHUNK || !pin_ready()) return cudaMemcpy(host, dev, bytes, cudaMemcpyDeviceToHost);
+  const size_t nch = (bytes + PIN_CHUNK - 1) / PIN_CHUNK;
+  auto issue = [&](size_t i) {
+    const size_t off = i * PIN_CHUNK, n = std::min(PIN_CHUNK, bytes - off);
+    cudaError_t e = cudaMemcpyAsync(g_pin.buf[i & 1], (const char*)dev + off, n, cudaMemcpyDeviceToHost, s.stream);
+    return e == cudaSuccess ? cudaEventRecord(g_pin.ev[i & 1], s.stream) : e;
+  };
+  cudaError_t e = issue(0);
+  for (size_t i = 0; i < nch && e == cudaSuccess; ++i) {
+    if (i + 1 < nch) e = issue(i + 1);  // buf[(i+1)&1] was drained to the host in round i-1
+    if (e == cudaSuccess) e = cudaEventSynchronize(g_pin.ev[i & 1]);
+    if (e != cudaSuccess) break;
+    const size_t off = i * PIN_CHUNK;
+    par_copy((char*)host + off, g_pin.buf[i & 1], std::min(PIN_CHUNK, bytes - off));
+  }
+  return e;
+}
+
 static int upload_operators(const void* adia, const void* aoff) {
   const size_t b = (size_t)3 * s.eng.g.nat * sizeof(C);
   // zero CXAOFF (isotropic materials) contributes nothing: neither copied nor read
   s.aoff_zero = all_zero(aoff, b);
-  cudaError_t e = cudaMemcpy(s.d_adia, adia, b, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess && !s.aoff_zero) e = cudaMemcpy(s.d_aoff, aoff, b, cudaMemcpyHostToDevice);
+  cudaError_t e = copy_h2d(s.d_adia, adia, b);
+  if (e == cudaSuccess && !s.aoff_zero) e = copy_h2d(s.d_aoff, aoff, b);
   if (e != cudaSuccess) { set_cuda_error("operator H2D", e); return 1; }
   return 0;
 }
@@ -229,7 +302,7 @@ static int upload_full_to_compact(const void* host, C* compact, bool maybe_zero 
     if (z != cudaSuccess) { set_cuda_error("zero initial guess", z); return 1; }
     return 0;
   }
-  cudaError_t e = cudaMemcpy(s.d_xf, host, b, cudaMemcpyHostToDevice);
+  cudaError_t e = copy_h2d(s.d_xf, host, b);
   if (e != cudaSuccess) { set_cuda_error("full vector H2D", e); return 1; }
   v_gather<float>(s.d_xf, compact, s.eng.occ, s.eng.g.nat, s.eng.g.nat0, s.stream);
   return check_launch("full->compact gather");
@@ -241,7 +314,7 @@ static int download_compact_to_full(const C* compact, void* host) {
   if (e != cudaSuccess) { set_cuda_error("solution compact D2H", e); return 1; }
   v_scatter<float>(compact, s.d_xf, s.eng.occ, s.eng.g.nat, s.eng.g.nat0, s.stream);
   if (check_launch("compact->full scatter")) return 1;
-  e = cudaMemcpy(host, s.d_xf, b, cudaMemcpyDeviceToHost);
+  e = copy_d2h(host, s.d_xf, b);
   if (e != cudaSuccess) { set_cuda_error("solution compact D2H", e); return 1; }
   return 0;
 }
@@ -596,12 +669,12 @@ DDSCAT_CUDA_API int ddscat_cuda_apply_f32(int cwhat, const void* x, void* y, con
   if (!s.ready) { set_error("apply", "not prepared"); return 10; }
   if ((cwhat != 'N' && cwhat != 'C') || !x || !y || !adia || !aoff) { set_error("apply", "invalid argument"); return 11; }
   const size_t b = (size_t)3 * s.eng.g.nat * sizeof(C);
-  cudaError_t e = cudaMemcpy(s.d_xf, x, b, cudaMemcpyHostToDevice);
+  cudaError_t e = copy_h2d(s.d_xf, x, b);
   if (e != cudaSuccess) { set_cuda_error("x H2D", e); return 12; }
-  e = cudaMemcpy(s.d_adia, adia, b, cudaMemcpyHostToDevice);
+  e = copy_h2d(s.d_adia, adia, b);
   if (e != cudaSuccess) { set_cuda_error("adia H2D", e); return 13; }
   s.aoff_zero = all_zero(aoff, b);  // zero CXAOFF: neither copied nor read
-  if (!s.aoff_zero) e = cudaMemcpy(s.d_aoff, aoff, b, cudaMemcpyHostToDevice);
+  if (!s.aoff_zero) e = copy_h2d(s.d_aoff, aoff, b);
   if (e != cudaSuccess) { set_cuda_error("aoff H2D", e); return 14; }
   MvArgs<float> a;
   a.x = s.d_xf; a.y = s.d_yf; a.io_full = 1;
@@ -614,7 +687,7 @@ DDSCAT_CUDA_API int ddscat_cuda_apply_f32(int cwhat, const void* x, void* y, con
   int rc = s.eng.matvec(a);
   if (timed) cudaEventRecord(ev[1], s.stream);
   if (!rc) {
-    e = cudaMemcpy(y, s.d_yf, b, cudaMemcpyDeviceToHost);
+    e = copy_d2h(y, s.d_yf, b);
     if (e != cudaSuccess) { set_cuda_error("y D2H", e); rc = 15; }
   }
   if (timed) {
