@@ -14,7 +14,12 @@ for both polarisations, EVALQ, SCAT at ETASCA 0.5 with f1/f2 on 0..180 deg at
 are regenerated from seeds by c1_problem() and mv64_inputs() below, so only
 outputs are stored (the 64^3 MATVEC as seeded samples and projections).
 
-Run on a GPU machine:  python tests/golden/make_reference_fixtures.py [base|c1|all]
+A third set (reference_fixtures_edge.npz) holds the edge cases of
+edge_cases.py: every solver with a nonzero CXAOFF, the single-site target
+(PBCGS2 and QMRCCG return codes) and the MATVEC of hollow targets with vacant
+rows and planes.
+
+Run on a GPU machine:  python tests/golden/make_reference_fixtures.py [base|c1|edge|all]
 """
 import ctypes as ct
 import os
@@ -31,8 +36,12 @@ from ddscat_b200 import targets  # noqa: E402
 import ddscat_b200 as D  # noqa: E402
 from oracle import ddscat_oracle as O  # noqa: E402
 
+sys.path.insert(0, HERE)
+import edge_cases as EC  # noqa: E402
+
 OUT = os.path.join(HERE, "reference_fixtures.npz")
 OUT_C1 = os.path.join(HERE, "reference_fixtures_c1.npz")
+OUT_EDGE = os.path.join(HERE, "reference_fixtures_edge.npz")
 C1_TOL, C1_MAXIT, C1_ETASCA = 1e-5, 500, 0.5
 MV64_SAMPLES, MV64_PROJ = 8192, 4
 
@@ -244,9 +253,54 @@ def main_c1():
     print("wrote", OUT_C1, len(fx), "arrays")
 
 
+def _ref_solve(lib, name, b, adia, aoff, maxit, tol):
+    xs = np.zeros_like(b)
+    it, tole, nc = ct.c_int(), ct.c_float(), ct.c_int()
+    rc = getattr(lib, f"ddscat_cuda_solve_{name}_f32")(_p(b), _p(xs), _p(adia), _p(aoff), b.size, maxit, tol,
+                                                       ct.byref(it), ct.byref(tole), ct.byref(nc))
+    return rc, xs, np.array([it.value, tole.value, nc.value], dtype=np.float64)
+
+
+def main_edge():
+    lib = ref_lib("fft3d")
+    fx = {}
+    # ---- nonzero CXAOFF through every solver of edge_cases.SOLVERS_AOFF
+    prob, b, adia, aoff = EC.aoff_problem()
+    k = prob.incid[0].k.astype(np.float32)
+    rc = lib.ddscat_cuda_prepare_green_f32(prob.nx, prob.ny, prob.nz, 0, prob.nat, prob.nat0, 0, 0.0, 0.0, 0.0,
+                                           *map(float, k), 1.0, 1.0, 1.0, _p(prob.iocc))
+    assert rc == 0, lib.ddscat_cuda_last_error()
+    for s in EC.SOLVERS_AOFF:
+        rc, xs, meta = _ref_solve(lib, s, b, adia, aoff, EC.MAXIT, EC.TOL)
+        fx[f"O_{s}_rc"] = np.array([rc])
+        fx[f"O_{s}_x"] = xs
+        fx[f"O_{s}_meta"] = meta
+    lib.ddscat_cuda_release()
+    # ---- sparse targets: MATVEC ('N', 'C'), PBCGS2 and QMRCCG return codes and meta
+    for case in ("single_site",) + EC.HOLLOW:
+        prob, b, adia, aoff, x = EC.sparse_problem(case)
+        k = prob.incid[0].k.astype(np.float32)
+        rc = lib.ddscat_cuda_prepare_green_f32(prob.nx, prob.ny, prob.nz, 0, prob.nat, prob.nat0, 0, 0.0, 0.0, 0.0,
+                                               *map(float, k), 1.0, 1.0, 1.0, _p(prob.iocc))
+        assert rc == 0, lib.ddscat_cuda_last_error()
+        for cw in "NC":
+            y = np.empty_like(x)
+            assert lib.ddscat_cuda_apply_f32(ord(cw), _p(x), _p(y), _p(adia), _p(aoff)) == 0
+            fx[f"S_{case}_y{cw}"] = y
+        for s in ("pbcgs2", "qmrccg"):
+            rc, xs, meta = _ref_solve(lib, s, b, adia, aoff, 400, EC.TOL)
+            fx[f"S_{case}_{s}_rc"] = np.array([rc])
+            fx[f"S_{case}_{s}_meta"] = meta
+        lib.ddscat_cuda_release()
+    np.savez_compressed(OUT_EDGE, **fx)
+    print("wrote", OUT_EDGE, len(fx), "arrays")
+
+
 if __name__ == "__main__":
     which = sys.argv[1] if len(sys.argv) > 1 else "all"
     if which in ("base", "all"):
         main()
     if which in ("c1", "all"):
         main_c1()
+    if which in ("edge", "all"):
+        main_edge()

@@ -100,3 +100,33 @@ def test_multi_target_graph_solves_concurrent_equal_serial():
     for u, v in zip(one, eight):
         np.testing.assert_array_equal(u["x"], v["x"])
     dda.release()
+
+
+@pytest.mark.gpu
+def test_multi_wavelength_one_target():
+    """Many wavelengths of one target in one call: each wavelength has its own
+    Green tensor, so it enters as a target of its own (same lattice and
+    occupancy, wave number x / a_eff); 3 wavelengths x 2 orientations x 2
+    polarisations, PBCGS2 as graph branches.  Every RHS converges and matches
+    the single-target batched solve of its wavelength to 20*TOL."""
+    base = targets.make_problem(24, 20, 16, m=1.5 + 0.02j, x=2.0)
+    probs = [targets.make_problem(24, 20, 16, m=1.5 + 0.02j, x=x, iocc=base.iocc,
+                                  orientations=targets.random_orientations(2, seed=7)) for x in (2.0, 3.5, 5.0)]
+    items = []
+    for p in probs:
+        b = np.stack([p.rhs(r) for r in range(4)])
+        items.append({"dims": (p.nx, p.ny, p.nz), "iocc": p.iocc, "ak": p.incid[0].k, "b": b,
+                      "x": np.zeros_like(b), "adia": np.stack([p.adia(r) for r in range(4)])})
+    # the orientations rotate k: every RHS of a target must share |k| (one Green tensor per target)
+    for p in probs:
+        assert np.allclose([np.linalg.norm(i.k) for i in p.incid], np.linalg.norm(p.incid[0].k))
+    dda = D.DDA()
+    out = dda.multi_solve(items, "pbcgs2", maxit=2000, tol=TOL, symmetric=False, graph=True)
+    assert out.itno.size == 12 and np.all(out.status == 0) and np.all(out.tole <= TOL)
+    for p, it in zip(probs, items):
+        dda.prepare_green(p.nx, p.ny, p.nz, p.iocc, p.incid[0].k)
+        xs = np.zeros_like(it["b"])
+        dda.solve_batch("pbcgs2", it["b"], xs, it["adia"], maxit=2000, tol=TOL, replace=True)
+        for r in range(4):
+            assert np.linalg.norm(xs[r] - it["x"][r]) / np.linalg.norm(xs[r]) < 20 * TOL
+    dda.release()

@@ -172,3 +172,55 @@ def test_oracle_c1_matches_reference(fc1):
         fmax = max(np.abs(fc1[f"C1_{r}_f1"]).max(), np.abs(fc1[f"C1_{r}_f2"]).max())
         assert np.abs(sc["f1"] - fc1[f"C1_{r}_f1"]).max() <= 2e-5 * fmax
         assert np.abs(sc["f2"] - fc1[f"C1_{r}_f2"]).max() <= 2e-5 * fmax
+
+
+# ---- edge cases (reference_fixtures_edge.npz; inputs from tests/golden/edge_cases.py)
+FIX_EDGE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_fixtures_edge.npz")
+
+
+@pytest.fixture(scope="module")
+def fedge():
+    return dict(np.load(FIX_EDGE))
+
+
+def _edge_cases():
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    import edge_cases
+    return edge_cases
+
+
+@pytest.mark.parametrize("name", ["pbcgs2", "qmrccg", "pbcgst", "petrkp", "gpbicg"])
+def test_oracle_solvers_with_cxaoff_match_reference(fedge, name):
+    """Anisotropic sites (nonzero CXAOFF): the oracle's solution of each solver
+    equals the reference's within 20*TOL, from the same recurrence."""
+    EC = _edge_cases()
+    prob, b, adia, aoff = EC.aoff_problem()
+    gp = O.GreenParams(prob.nx, prob.ny, prob.nz, ak=tuple(float(np.float32(a)) for a in prob.incid[0].k))
+    op = O.Operator.from_params(gp, prob.iocc)
+    c = lambda v: O.gather_compact(v, op.occ, prob.nat).astype(np.complex128)  # noqa: E731
+    bc, ac, oc = c(b), c(adia), c(aoff)
+    mv = lambda v: op.apply_compact(v, ac, oc)  # noqa: E731
+    mvh = lambda v: op.apply_compact(v, ac, oc, "C")  # noqa: E731
+    x0 = np.zeros_like(bc)
+    if name == "pbcgst":
+        res = O.solve_pbcgst(mv, bc, x0, EC.MAXIT, EC.TOL, ac)
+    elif name == "petrkp":
+        res = O.solve_petrkp(mv, mvh, bc, x0, EC.MAXIT, EC.TOL)
+    else:
+        res = O.SOLVERS[name](mv, bc, x0, EC.MAXIT, EC.TOL)
+    assert res.status == int(fedge[f"O_{name}_rc"][0]) == 0
+    ref = c(fedge[f"O_{name}_x"])
+    assert np.linalg.norm(res.x - ref) / np.linalg.norm(ref) < 20 * EC.TOL
+
+
+@pytest.mark.parametrize("case", ["single_site", "hollow16", "hollow18x12x10"])
+def test_oracle_sparse_matvec_matches_reference(fedge, case):
+    EC = _edge_cases()
+    prob, b, adia, aoff, x = EC.sparse_problem(case)
+    gp = O.GreenParams(prob.nx, prob.ny, prob.nz, ak=tuple(float(np.float32(a)) for a in prob.incid[0].k))
+    op = O.Operator.from_params(gp, prob.iocc)
+    for cw in "NC":
+        y = op.apply_full(x, adia, aoff, cw)
+        ref = fedge[f"S_{case}_y{cw}"]
+        assert np.linalg.norm(y - ref) / np.linalg.norm(ref) < 2e-5
