@@ -353,8 +353,12 @@ static int run_solver(const SolverCodes& sc, SolveFn fn, const void* b, void* x,
   io.adia_full = s.d_adia;
   io.work = s.d_work; io.sy = s.d_sy;
   io.maxit = maxit; io.tol = (double)tol; io.verbose = verbose_level() >= 1;
-  const int rc = fn(io);
+  int rc = fn(io);
   if (io.verbose) std::fflush(stdout);
+  if (rc == 0 || (rc == 87 && sc.publish_on_maxit)) {
+    const int mc = matvec_check(s.eng);
+    if (mc) return mc;
+  }
   if (rc != 0 && !(rc == 87 && sc.publish_on_maxit)) return rc;
   std::string keep = g_last_error;
   if (download_compact_to_full(s.d_sx, x)) return sc.d2h;
@@ -685,6 +689,7 @@ DDSCAT_CUDA_API int ddscat_cuda_apply_f32(int cwhat, const void* x, void* y, con
                      cudaEventCreate(&ev[1]) == cudaSuccess;
   if (timed) cudaEventRecord(ev[0], s.stream);
   int rc = s.eng.matvec(a);
+  if (!rc) rc = matvec_check(s.eng);
   if (timed) cudaEventRecord(ev[1], s.stream);
   if (!rc) {
     e = copy_d2h(y, s.d_yf, b);
@@ -927,7 +932,8 @@ DDSCAT_CUDA_API int ddscat_b200_solve_batch_f32(int solver, int nrhs, const void
   io.maxit = maxit; io.tol = (double)tol; io.verbose = verbose_level() >= 2; io.replace = replace; io.sym = sym;
   io.graph = graph;
   BatchResult res;
-  const int rc = solver == DDSCAT_B200_QMRCCG ? solve_batch_qmrccg<float>(io, res) : solve_batch_pbcgs2<float>(io, res);
+  int rc = solver == DDSCAT_B200_QMRCCG ? solve_batch_qmrccg<float>(io, res) : solve_batch_pbcgs2<float>(io, res);
+  if (!rc) rc = matvec_check(s.eng);
   bs.matvec_ms = io.matvec_ms;
   bs.matvec_rhs = io.matvec_rhs;
   bs.matvec_calls = io.matvec_calls;
@@ -1055,6 +1061,7 @@ DDSCAT_CUDA_API int ddscat_b200_matvec_timing(int nrhs, int iters, int cwhat, fl
   cudaEventDestroy(e1);
   cudaFree(x); cudaFree(y); cudaFree(ad);
   if (!rc && e != cudaSuccess) { set_cuda_error("matvec_timing", e); rc = 402; }
+  if (!rc) rc = matvec_check(s.eng);
   *ms_per_call = ms / iters;
   return rc;
 }

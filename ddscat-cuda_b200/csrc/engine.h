@@ -112,6 +112,12 @@ template <typename T> struct Engine {
   }
   cudaStream_t stream = 0;
   size_t bytes_allocated = 0;
+  // device status word of the MATVEC kernels (0 = ok): a kernel whose bounded
+  // wait for an asynchronous tile copy ran out sets it (matvec_check)
+  int* d_err = nullptr;
+  // tile moves of the FP32 256-point y passes by the tensor memory accelerator
+  // (DDSCAT_B200_NOTMA=1 selects the per-thread copies)
+  int use_tma = 1;
 
   // pad: the Green tensor will be built here (build_green), so the FFT lengths
   // may be padded beyond 2n onto the register-FFT pipeline
@@ -172,5 +178,8 @@ bool xzg3_supported(int Mz);
 // partials per RHS of the fused x*y sum of the x-first pipeline (MvArgs::dot_out)
 size_t xdot_blocks(const Geometry& g);
 template <typename T> int interleave_green_zfast(Engine<T>& E, const cplx<T>* planar);
+// 0, or 26 with the error text when a MATVEC kernel reported a timed-out tile
+// copy since the last check (synchronises the engine's stream)
+template <typename T> int matvec_check(Engine<T>& E);
 
 }  // namespace ddb

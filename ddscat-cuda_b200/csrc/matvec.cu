@@ -600,6 +600,11 @@ int Engine<T>::init_geometry(int nx, int ny, int nz, int ipbc, int nat, int nat0
   tune_ly = std::max(1, env_int("DDSCAT_B200_LY", 4));
   tune_tile = env_int("DDSCAT_B200_TILE", 0);
   tune_zg = std::getenv("DDSCAT_B200_ZG") ? 1 : 0;
+  use_tma = std::getenv("DDSCAT_B200_NOTMA") ? 0 : 1;
+  if (!d_err) {
+    if (cudaMalloc((void**)&d_err, sizeof(int)) != cudaSuccess) { set_error("prepare", "status word"); return 1; }
+    cudaMemset(d_err, 0, sizeof(int));
+  }
   if (px.nstages < 0 || py.nstages < 0 || pz.nstages < 0) {
     set_error("prepare", "FFT length has too many prime factors");
     return 1;
@@ -821,7 +826,7 @@ template <typename T> int Engine<T>::upload_green(const void* host_green) {
 template <typename T> void Engine<T>::release() {
   cudaFree(twx); cudaFree(twy); cudaFree(twz);
   cudaFree(green); cudaFree(occ); cudaFree(inv); cudaFree(iocc); cudaFree(rowq);
-  cudaFree(zhat); cudaFree(slab);
+  cudaFree(zhat); cudaFree(slab); cudaFree(d_err);
   *this = Engine<T>{};
 }
 

@@ -27,12 +27,23 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cooperative_groups.h>
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include "engine.h"
 #include "fftreg.cuh"
 
 namespace ddb {
 
 template <typename T> struct XParams {
+  // B as a 2-D tensor of rows of n_z 8-byte complex floats, box {16, 256},
+  // 128-byte swizzle: the tiles of the 256-point y passes (tma != 0)
+  alignas(64) CUtensorMap tmB;
+  // A as rows of n_y complex floats, box {16, 256}: the tiles of the 256-point
+  // x passes (tma_x != 0)
+  alignas(64) CUtensorMap tmA;
+  int tma;
+  int tma_x;
+  int* err;  // status word (Engine::d_err)
   int nx, ny, nz, Mx, My, Mz, nat, nat0;
   const cplx<T>* x;
   size_t x_rs;
@@ -81,6 +92,40 @@ template <int N> struct XShape {
   static constexpr int ZG_MINB = E >= 32 ? 1 : (E >= 24 ? 2 : 3);  // ZG blocks per SM the registers must allow (FP32)
   static constexpr bool PAIR = TT >= 8;                      // 128-bit transpose stores (conflict-free for TT >= 8)
 };
+
+// ---- tensor-memory-accelerator tiles of the 256-point y passes (FP32)
+// A y-pass tile holds 256 rows (ky) of 16 consecutive z positions: 128 bytes
+// per row, stored with the 128-byte swizzle (16-byte chunk j of row r at chunk
+// j ^ (r & 7)), the layout a box of {16, 256} 8-byte elements has in shared
+// memory.  The tile base is 1024-byte aligned.  Threads write and read it
+// through tma_slot; the tensor map covers this GPU's own B buffer and no
+// multicast is used.
+constexpr int TMA_ROWS = 256, TMA_COLS = 16;
+constexpr unsigned TMA_TILE_BYTES = TMA_ROWS * TMA_COLS * 8;
+constexpr int TMA_WAIT_POLLS = 1 << 24;  // bounded wait for a tile load (seconds at most)
+__device__ __forceinline__ int tma_slot(int r, int col) {
+  return r * TMA_COLS + (((col >> 1) ^ (r & 7)) << 1) + (col & 1);
+}
+__device__ __forceinline__ float2* tma_tile(unsigned char* smem) {
+  const uintptr_t a = reinterpret_cast<uintptr_t>(smem);
+  return reinterpret_cast<float2*>((a + 1023) & ~(uintptr_t)1023);
+}
+// store the tile at (x = z position, y = row) of the map; the issuing thread
+// waits until the copy has read the tile (the CTA keeps its shared memory)
+__device__ __forceinline__ void tma_store_tile(const CUtensorMap* map, const void* tile, int x, int y) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(map), "r"(x), "r"(y),
+               "r"(smem_addr(tile))
+               : "memory");
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+__device__ __forceinline__ void tma_load_tile(const CUtensorMap* map, void* tile, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_addr(tile)),
+      "l"(map), "r"(x), "r"(y), "r"(smem_addr(bar))
+      : "memory");
+}
 
 // Tile <-> global moves of the row passes: N rows of RL consecutive elements
 // (row stride ld in global, RL+1 in the tile), two elements per 16-byte access.
@@ -159,7 +204,7 @@ template <int MAXC, typename C> __device__ __forceinline__ void stage_chunk_asyn
 
 // ------------------------------------------------------------- XF: x forward
 // block: RL rows (iy) x TT threads, thread-fastest; grid (ceil(ny/RL), nz, 3*nr)
-template <typename T, int N> __global__ void __launch_bounds__(256) kx_xf(XParams<T> P) {
+template <typename T, int N> __global__ void __launch_bounds__(256) kx_xf(const __grid_constant__ XParams<T> P) {
   using C = cplx<T>;
   using S_ = XShape<N>;
   constexpr int E = S_::E, TT = S_::TT, H = S_::H, RL = S_::RL;
@@ -200,6 +245,19 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_xf(XParam
   }
   line_fft<E, TT, +1, false, true, S_::PAIR>(v, lines + (size_t)l * P.lsx, t, P.twx);
   __syncthreads();  // all line scratch consumed before the tile reuses it
+  if constexpr (N == TMA_ROWS && RL == TMA_COLS && sizeof(C) == 8) {
+    if (P.tma_x) {
+      // swizzled tile, then one tensor store of its 256 x 16 elements (rows
+      // beyond n_y are clipped by the map)
+      C* tt = tma_tile(smem_raw);
+#pragma unroll
+      for (int i = 0; i < E; ++i) tt[tma_slot(t + TT * i, l)] = v[i];
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncthreads();
+      if (threadIdx.x == 0) tma_store_tile(&P.tmA, tt, iy0, ((rl * 3 + c) * P.nz + iz) * P.Mx);
+      return;
+    }
+  }
 #pragma unroll
   for (int i = 0; i < E; ++i) tile[(t + TT * i) * (RL + 1) + l] = v[i];
   __syncthreads();
@@ -209,7 +267,7 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_xf(XParam
 
 // ------------------------------------------------------------- YF: y forward
 // block: RL z-lines (iz) x TT; grid (ceil(nz/RL), nkx, 3*nrb)
-template <typename T, int N> __global__ void __launch_bounds__(256) kx_yf(XParams<T> P) {
+template <typename T, int N> __global__ void __launch_bounds__(256) kx_yf(const __grid_constant__ XParams<T> P) {
   using C = cplx<T>;
   using S_ = XShape<N>;
   constexpr int E = S_::E, TT = S_::TT, H = S_::H, RL = S_::RL;
@@ -227,6 +285,19 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_yf(XParam
   for (int i = 0; i < H; ++i) v[i] = zin && t + TT * i < P.ny ? A[t + TT * i] : mk<C>(0, 0);  // iy < ny <= N/2
   line_fft<E, TT, +1, false, true, S_::PAIR>(v, lines + (size_t)l * P.lsy, t, P.twy);
   __syncthreads();
+  if constexpr (N == TMA_ROWS && RL == TMA_COLS && sizeof(C) == 8) {
+    if (P.tma) {
+      // swizzled tile, then one tensor store of its 256 x 16 elements (z
+      // positions beyond n_z are clipped by the map)
+      C* tt = tma_tile(smem_raw);
+#pragma unroll
+      for (int i = 0; i < E; ++i) tt[tma_slot(t + TT * i, l)] = v[i];
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncthreads();
+      if (threadIdx.x == 0) tma_store_tile(&P.tmB, tt, iz0, ((rb * 3 + c) * P.nkx + kxl) * P.My);
+      return;
+    }
+  }
 #pragma unroll
   for (int i = 0; i < E; ++i) tile[(t + TT * i) * (RL + 1) + l] = v[i];
   __syncthreads();
@@ -514,7 +585,7 @@ template <typename T, int N, int BTY = 0> __global__ void __launch_bounds__(128,
 
 // ------------------------------------------------------------- YI: y inverse
 // block: RL z-lines x TT; grid (ceil(nz/RL), nkx, 3*nrb)
-template <typename T, int N> __global__ void __launch_bounds__(256) kx_yi(XParams<T> P) {
+template <typename T, int N> __global__ void __launch_bounds__(256) kx_yi(const __grid_constant__ XParams<T> P) {
   using C = cplx<T>;
   using S_ = XShape<N>;
   constexpr int E = S_::E, TT = S_::TT, H = S_::H, RL = S_::RL;
@@ -526,13 +597,41 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_yi(XParam
   const int rb = blockIdx.z / 3, c = blockIdx.z - 3 * (blockIdx.z / 3), rl = P.b_rhs0 + rb;
   if (xoff(P, rl)) return;
   const int nz = P.nz;
-  const C* B = P.B + ((size_t)(rb * 3 + c) * P.nkx + kxl) * (size_t)P.My * nz + iz0;
-  load_tile_pairs<RL, N>(B, nz, nz - iz0, tile);
-  __syncthreads();
   C v[E];
+  bool loaded = false;
+  if constexpr (N == TMA_ROWS && RL == TMA_COLS && sizeof(C) == 8) {
+    if (P.tma) {
+      // one tensor load of the 256 x 16 tile (z positions beyond n_z read as 0)
+      __shared__ __align__(8) uint64_t bar;
+      C* tt = tma_tile(smem_raw);
+      if (threadIdx.x == 0) mbar_init(&bar, 1);
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        mbar_arrive_expect_tx(&bar, TMA_TILE_BYTES);
+        tma_load_tile(&P.tmB, tt, iz0, ((rb * 3 + c) * P.nkx + kxl) * P.My, &bar);
+      }
+      // one decision for the whole block: every thread's bounded wait succeeded
+      if (!__syncthreads_and(mbar_wait(&bar, 0, TMA_WAIT_POLLS))) {
+        // the copy did not complete in the allowed time: report it, wait once
+        // more (bounded) for the copy in flight, and leave this block's lines
+        if (threadIdx.x == 0) atomicOr(P.err, 1);
+        mbar_wait(&bar, 0, TMA_WAIT_POLLS);
+        return;
+      }
 #pragma unroll
-  for (int i = 0; i < E; ++i) v[i] = tile[(t + TT * i) * (RL + 1) + l];
-  __syncthreads();  // the tile is consumed before the line scratch reuses it
+      for (int i = 0; i < E; ++i) v[i] = tt[tma_slot(t + TT * i, l)];
+      __syncthreads();  // the tile is consumed before the line scratch reuses it
+      loaded = true;
+    }
+  }
+  if (!loaded) {
+    const C* B = P.B + ((size_t)(rb * 3 + c) * P.nkx + kxl) * (size_t)P.My * nz + iz0;
+    load_tile_pairs<RL, N>(B, nz, nz - iz0, tile);
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < E; ++i) v[i] = tile[(t + TT * i) * (RL + 1) + l];
+    __syncthreads();  // the tile is consumed before the line scratch reuses it
+  }
   line_fft<E, TT, -1, false, false, S_::PAIR>(v, lines + (size_t)l * P.lsy, t, P.twy);
   if (iz < nz) {
     C* A = P.A + (size_t)rl * P.A_rs + ((size_t)(c * nz + iz) * P.Mx + kx) * P.ny;
@@ -594,7 +693,7 @@ constexpr int XI_STAGE_MAX = 2048;  // largest staged chunk of the XI pass (elem
 
 // block: RL rows (iy) x TT; grid (ceil(ny/RL), nz, 3*nr)
 // shared memory: tile / line scratch [tlx] | x chunk | CXADIA chunk
-template <typename T, int N> __global__ void __launch_bounds__(256) kx_xi(XParams<T> P) {
+template <typename T, int N> __global__ void __launch_bounds__(256) kx_xi(const __grid_constant__ XParams<T> P) {
   using C = cplx<T>;
   using S_ = XShape<N>;
   constexpr int E = S_::E, TT = S_::TT, H = S_::H, RL = S_::RL;
@@ -636,14 +735,45 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_xi(XParam
     stage_chunk_async<MAXC>(xs, x + (size_t)c * S + q0, cnt);
     stage_chunk_async<MAXC>(as, ad + q0, cnt);
   }
-  const C* A = P.A + (size_t)rl * P.A_rs + ((size_t)(c * P.nz + iz) * P.Mx) * ny + iy0;
-  load_tile_pairs<RL, N>(A, ny, ny - iy0, tile);
-  cp_async_wait_all();  // the x and CXADIA chunks
-  __syncthreads();
   C v[E];
+  bool loaded = false;
+  if constexpr (N == TMA_ROWS && RL == TMA_COLS && sizeof(C) == 8) {
+    if (P.tma_x) {
+      // one tensor load of the 256 x 16 tile of A (rows beyond n_y read as 0),
+      // while the x and CXADIA chunks arrive by per-thread copies
+      __shared__ __align__(8) uint64_t bar;
+      C* tt = tma_tile(smem_raw);
+      if (threadIdx.x == 0) mbar_init(&bar, 1);
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        mbar_arrive_expect_tx(&bar, TMA_TILE_BYTES);
+        tma_load_tile(&P.tmA, tt, iy0, ((rl * 3 + c) * P.nz + iz) * P.Mx, &bar);
+      }
+      cp_async_wait_all();  // the x and CXADIA chunks
+      // one decision for the whole block (the barrier also publishes every
+      // thread's chunk copies): every thread's bounded wait succeeded
+      if (!__syncthreads_and(mbar_wait(&bar, 0, TMA_WAIT_POLLS))) {
+        // the copy did not complete in the allowed time: report it, wait once
+        // more (bounded) for the copy in flight, and leave this block's rows
+        if (threadIdx.x == 0) atomicOr(P.err, 1);
+        mbar_wait(&bar, 0, TMA_WAIT_POLLS);
+        return;
+      }
 #pragma unroll
-  for (int i = 0; i < E; ++i) v[i] = tile[(t + TT * i) * (RL + 1) + l];
-  __syncthreads();
+      for (int i = 0; i < E; ++i) v[i] = tt[tma_slot(t + TT * i, l)];
+      __syncthreads();
+      loaded = true;
+    }
+  }
+  if (!loaded) {
+    const C* A = P.A + (size_t)rl * P.A_rs + ((size_t)(c * P.nz + iz) * P.Mx) * ny + iy0;
+    load_tile_pairs<RL, N>(A, ny, ny - iy0, tile);
+    cp_async_wait_all();  // the x and CXADIA chunks
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < E; ++i) v[i] = tile[(t + TT * i) * (RL + 1) + l];
+    __syncthreads();
+  }
   line_fft<E, TT, -1, false, false, S_::PAIR>(v, lines + (size_t)l * P.lsx, t, P.twx);
   // finish (cu:116-118): y = CXADIA x - w/ngrid [+ CXAOFF terms], conj for 'C'
   C* y = P.y + (size_t)rl * P.y_rs + (size_t)c * S;
@@ -971,11 +1101,57 @@ template <typename T> bool xpipe_supported(const Geometry& g) {
   return ok(g.Mx) && ok(g.My) && ok(g.Mz);
 }
 
+// cuTensorMapEncodeTiled of the driver, looked up once through the runtime
+// (no link against the driver library)
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = []() -> PFN_cuTensorMapEncodeTiled_v12000 {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+// Map of B (rows of n_z complex floats, row stride n_z * 8 bytes) for the
+// 256-point y passes' tiles, or of A (rows of n_y) for the x passes: box
+// {16, 256}, 128-byte swizzle, zero fill.
+static bool encode_b_map(CUtensorMap* m, void* base, size_t rows, int nz) {
+  const auto enc = tensor_map_encoder();
+  if (!enc || rows > 0xffffffffull || (nz & 1)) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)nz, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)nz * 8};
+  const cuuint32_t box[2] = {(cuuint32_t)TMA_COLS, (cuuint32_t)TMA_ROWS};
+  const cuuint32_t estr[2] = {1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <typename T> int matvec_check(Engine<T>& E) {
+  if (!E.d_err) return 0;
+  int h = 0;
+  cudaError_t e = cudaMemcpyAsync(&h, E.d_err, sizeof(int), cudaMemcpyDeviceToHost, E.stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(E.stream);
+  if (e != cudaSuccess) { set_cuda_error("MATVEC status", e); return 26; }
+  if (h == 0) return 0;
+  cudaMemsetAsync(E.d_err, 0, sizeof(int), E.stream);
+  set_error("MATVEC", "a tile copy of the y passes did not complete in the allowed time");
+  return 26;
+}
+template int matvec_check<float>(Engine<float>&);
+template int matvec_check<double>(Engine<double>&);
+
 template <typename T>
 int matvec_xpipe(Engine<T>& E, const MvArgs<T>& a) {
   using C = cplx<T>;
   const Geometry& g = E.g;
   XParams<T> P{};
+  P.err = E.d_err;
   P.nx = g.nx; P.ny = g.ny; P.nz = g.nz; P.Mx = g.Mx; P.My = g.My; P.Mz = g.Mz;
   P.nat = g.nat; P.nat0 = g.nat0;
   P.x_rs = a.x_rs; P.y_rs = a.y_rs; P.a_rs = a.a_rs;
@@ -1002,12 +1178,29 @@ int matvec_xpipe(Engine<T>& E, const MvArgs<T>& a) {
                : std::max(line_stride(g.Mz / TZ, TZ, RZ, false, TZ >= 8), g.Mz);
   // the transpose tile and the line scratch share one region
   P.tlx = (int)std::max((size_t)g.Mx * (RX + 1), (size_t)RX * P.lsx);
+  // a tensor tile of the x passes (32 KB at a 1024-byte boundary) fits in front of the XI chunks
+  if (g.Mx == TMA_ROWS) P.tlx = std::max(P.tlx, (int)((TMA_TILE_BYTES + 1024) / sizeof(C)));
   const size_t smx = (size_t)P.tlx * sizeof(C);
   // XI: the x and CXADIA chunks of RX rows, each sized as the kernel lays them
   // out (MAXC = RL * N/2 elements, which is RX * nx only when Mx = 2 nx)
   const size_t xi_maxc = (size_t)RX * (g.Mx / 2);
   const size_t smxi = smx + (xi_maxc <= (size_t)XI_STAGE_MAX ? 2 * xi_maxc * sizeof(C) : 0);
-  const size_t smy = std::max((size_t)g.My * (RY + 1), (size_t)RY * P.lsy) * sizeof(C);
+  size_t smy = std::max((size_t)g.My * (RY + 1), (size_t)RY * P.lsy) * sizeof(C);
+  // tensor tiles for the 256-point y passes (FP32, five-pass B layout): the
+  // slab as rows of n_z; the tile needs 32 KB at a 1024-byte boundary
+  P.tma = 0;
+  P.tma_x = 0;
+  if constexpr (sizeof(T) == 4) {
+    // the same for A (rows of n_y) in the 256-point x passes
+    if (E.use_tma && g.Mx == TMA_ROWS && RX == TMA_COLS && E.d_err &&
+        encode_b_map(&P.tmA, E.zhat, (size_t)E.zcap * 3 * g.nz * g.Mx, g.ny))
+      P.tma_x = 1;
+    if (E.use_tma && g.My == TMA_ROWS && RY == TMA_COLS && E.d_err &&
+        encode_b_map(&P.tmB, E.slab, (size_t)E.slab_nr * 3 * E.slab_B * g.My, g.nz)) {
+      P.tma = 1;
+      smy = std::max(smy, (size_t)TMA_TILE_BYTES + 1024);
+    }
+  }
   // ZG3: FFT scratch
   const size_t smz = fzg3 ? (size_t)RZ3 * P.lsz * sizeof(C) : (size_t)3 * RZ * P.lsz * sizeof(C);
   const void* fxf = xkernel<T>(XPass::XF, g.Mx);
