@@ -110,21 +110,31 @@ __device__ __forceinline__ float2* tma_tile(unsigned char* smem) {
   const uintptr_t a = reinterpret_cast<uintptr_t>(smem);
   return reinterpret_cast<float2*>((a + 1023) & ~(uintptr_t)1023);
 }
-// store the tile at (x = z position, y = row) of the map; the issuing thread
-// waits until the copy has read the tile (the CTA keeps its shared memory)
-__device__ __forceinline__ void tma_store_tile(const CUtensorMap* map, const void* tile, int x, int y) {
-  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(map), "r"(x), "r"(y),
-               "r"(smem_addr(tile))
-               : "memory");
+// A tile of N = 256 or 512 rows is N/256 boxes of 256 rows, each 32 KB and
+// 1024-byte aligned (the swizzle phase r & 7 is the same in every box).
+template <int N> constexpr bool tma_rows_ok() { return N == 256 || N == 512; }
+// store the tile's boxes at (x = inner position, y = first row) of the map;
+// the issuing thread waits until the copies have read the tile (the CTA keeps
+// its shared memory)
+template <int N> __device__ __forceinline__ void tma_store_tile(const CUtensorMap* map, const float2* tile, int x, int y) {
+#pragma unroll
+  for (int b = 0; b < N / TMA_ROWS; ++b)
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(map), "r"(x),
+                 "r"(y + b * TMA_ROWS), "r"(smem_addr(tile + (size_t)b * TMA_ROWS * TMA_COLS))
+                 : "memory");
   asm volatile("cp.async.bulk.commit_group;" ::: "memory");
   asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 }
-__device__ __forceinline__ void tma_load_tile(const CUtensorMap* map, void* tile, int x, int y, uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
-          smem_addr(tile)),
-      "l"(map), "r"(x), "r"(y), "r"(smem_addr(bar))
-      : "memory");
+// load the tile's boxes, completing on bar (which expects N/256 * 32 KB)
+template <int N>
+__device__ __forceinline__ void tma_load_tile(const CUtensorMap* map, float2* tile, int x, int y, uint64_t* bar) {
+#pragma unroll
+  for (int b = 0; b < N / TMA_ROWS; ++b)
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_addr(tile + (size_t)b * TMA_ROWS * TMA_COLS)),
+        "l"(map), "r"(x), "r"(y + b * TMA_ROWS), "r"(smem_addr(bar))
+        : "memory");
 }
 
 // Tile <-> global moves of the row passes: N rows of RL consecutive elements
@@ -245,7 +255,7 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_xf(const 
   }
   line_fft<E, TT, +1, false, true, S_::PAIR>(v, lines + (size_t)l * P.lsx, t, P.twx);
   __syncthreads();  // all line scratch consumed before the tile reuses it
-  if constexpr (N == TMA_ROWS && RL == TMA_COLS && sizeof(C) == 8) {
+  if constexpr (tma_rows_ok<N>() && RL == TMA_COLS && sizeof(C) == 8) {
     if (P.tma_x) {
       // swizzled tile, then one tensor store of its 256 x 16 elements (rows
       // beyond n_y are clipped by the map)
@@ -254,7 +264,7 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_xf(const 
       for (int i = 0; i < E; ++i) tt[tma_slot(t + TT * i, l)] = v[i];
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncthreads();
-      if (threadIdx.x == 0) tma_store_tile(&P.tmA, tt, iy0, ((rl * 3 + c) * P.nz + iz) * P.Mx);
+      if (threadIdx.x == 0) tma_store_tile<N>(&P.tmA, tt, iy0, ((rl * 3 + c) * P.nz + iz) * P.Mx);
       return;
     }
   }
@@ -285,7 +295,7 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_yf(const 
   for (int i = 0; i < H; ++i) v[i] = zin && t + TT * i < P.ny ? A[t + TT * i] : mk<C>(0, 0);  // iy < ny <= N/2
   line_fft<E, TT, +1, false, true, S_::PAIR>(v, lines + (size_t)l * P.lsy, t, P.twy);
   __syncthreads();
-  if constexpr (N == TMA_ROWS && RL == TMA_COLS && sizeof(C) == 8) {
+  if constexpr (tma_rows_ok<N>() && RL == TMA_COLS && sizeof(C) == 8) {
     if (P.tma) {
       // swizzled tile, then one tensor store of its 256 x 16 elements (z
       // positions beyond n_z are clipped by the map)
@@ -294,7 +304,7 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_yf(const 
       for (int i = 0; i < E; ++i) tt[tma_slot(t + TT * i, l)] = v[i];
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncthreads();
-      if (threadIdx.x == 0) tma_store_tile(&P.tmB, tt, iz0, ((rb * 3 + c) * P.nkx + kxl) * P.My);
+      if (threadIdx.x == 0) tma_store_tile<N>(&P.tmB, tt, iz0, ((rb * 3 + c) * P.nkx + kxl) * P.My);
       return;
     }
   }
@@ -599,7 +609,7 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_yi(const 
   const int nz = P.nz;
   C v[E];
   bool loaded = false;
-  if constexpr (N == TMA_ROWS && RL == TMA_COLS && sizeof(C) == 8) {
+  if constexpr (tma_rows_ok<N>() && RL == TMA_COLS && sizeof(C) == 8) {
     if (P.tma) {
       // one tensor load of the 256 x 16 tile (z positions beyond n_z read as 0)
       __shared__ __align__(8) uint64_t bar;
@@ -607,8 +617,8 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_yi(const 
       if (threadIdx.x == 0) mbar_init(&bar, 1);
       __syncthreads();
       if (threadIdx.x == 0) {
-        mbar_arrive_expect_tx(&bar, TMA_TILE_BYTES);
-        tma_load_tile(&P.tmB, tt, iz0, ((rb * 3 + c) * P.nkx + kxl) * P.My, &bar);
+        mbar_arrive_expect_tx(&bar, (N / TMA_ROWS) * TMA_TILE_BYTES);
+        tma_load_tile<N>(&P.tmB, tt, iz0, ((rb * 3 + c) * P.nkx + kxl) * P.My, &bar);
       }
       // one decision for the whole block: every thread's bounded wait succeeded
       if (!__syncthreads_and(mbar_wait(&bar, 0, TMA_WAIT_POLLS))) {
@@ -737,7 +747,7 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_xi(const 
   }
   C v[E];
   bool loaded = false;
-  if constexpr (N == TMA_ROWS && RL == TMA_COLS && sizeof(C) == 8) {
+  if constexpr (tma_rows_ok<N>() && RL == TMA_COLS && sizeof(C) == 8) {
     if (P.tma_x) {
       // one tensor load of the 256 x 16 tile of A (rows beyond n_y read as 0),
       // while the x and CXADIA chunks arrive by per-thread copies
@@ -746,8 +756,8 @@ template <typename T, int N> __global__ void __launch_bounds__(256) kx_xi(const 
       if (threadIdx.x == 0) mbar_init(&bar, 1);
       __syncthreads();
       if (threadIdx.x == 0) {
-        mbar_arrive_expect_tx(&bar, TMA_TILE_BYTES);
-        tma_load_tile(&P.tmA, tt, iy0, ((rl * 3 + c) * P.nz + iz) * P.Mx, &bar);
+        mbar_arrive_expect_tx(&bar, (N / TMA_ROWS) * TMA_TILE_BYTES);
+        tma_load_tile<N>(&P.tmA, tt, iy0, ((rl * 3 + c) * P.nz + iz) * P.Mx, &bar);
       }
       cp_async_wait_all();  // the x and CXADIA chunks
       // one decision for the whole block (the barrier also publishes every
@@ -1179,7 +1189,8 @@ int matvec_xpipe(Engine<T>& E, const MvArgs<T>& a) {
   // the transpose tile and the line scratch share one region
   P.tlx = (int)std::max((size_t)g.Mx * (RX + 1), (size_t)RX * P.lsx);
   // a tensor tile of the x passes (32 KB at a 1024-byte boundary) fits in front of the XI chunks
-  if (g.Mx == TMA_ROWS) P.tlx = std::max(P.tlx, (int)((TMA_TILE_BYTES + 1024) / sizeof(C)));
+  if (g.Mx == 256 || g.Mx == 512)
+    P.tlx = std::max(P.tlx, (int)(((size_t)(g.Mx / TMA_ROWS) * TMA_TILE_BYTES + 1024) / sizeof(C)));
   const size_t smx = (size_t)P.tlx * sizeof(C);
   // XI: the x and CXADIA chunks of RX rows, each sized as the kernel lays them
   // out (MAXC = RL * N/2 elements, which is RX * nx only when Mx = 2 nx)
@@ -1192,13 +1203,13 @@ int matvec_xpipe(Engine<T>& E, const MvArgs<T>& a) {
   P.tma_x = 0;
   if constexpr (sizeof(T) == 4) {
     // the same for A (rows of n_y) in the 256-point x passes
-    if (E.use_tma && g.Mx == TMA_ROWS && RX == TMA_COLS && E.d_err &&
+    if (E.use_tma && (g.Mx == 256 || g.Mx == 512) && RX == TMA_COLS && E.d_err &&
         encode_b_map(&P.tmA, E.zhat, (size_t)E.zcap * 3 * g.nz * g.Mx, g.ny))
       P.tma_x = 1;
-    if (E.use_tma && g.My == TMA_ROWS && RY == TMA_COLS && E.d_err &&
+    if (E.use_tma && (g.My == 256 || g.My == 512) && RY == TMA_COLS && E.d_err &&
         encode_b_map(&P.tmB, E.slab, (size_t)E.slab_nr * 3 * E.slab_B * g.My, g.nz)) {
       P.tma = 1;
-      smy = std::max(smy, (size_t)TMA_TILE_BYTES + 1024);
+      smy = std::max(smy, (size_t)(g.My / TMA_ROWS) * TMA_TILE_BYTES + 1024);
     }
   }
   // ZG3: FFT scratch
