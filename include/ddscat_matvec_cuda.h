@@ -39,7 +39,9 @@ DDSCAT_CUDA_API int ddscat_cuda_prepare_f32(int nx, int ny, int nz, int ipbc, in
 
 /* y = A x (cwhat='N') or A^H x (cwhat='C'), full host vectors.
  * Replaces ddscat_matvec_cuda.h:16-17 / ddscat_matvec_cuda.cu:1027-1029.
- * Codes: 10 not prepared, 11 invalid, 12-14 H2D, 15 D2H, 21-25 MATVEC launch. */
+ * Codes: 10 not prepared, 11 invalid, 12-14 H2D, 15 D2H, 21-25 MATVEC launch, 26 a tile copy of the
+ * MATVEC's x or y passes did not complete within its bounded wait (also returned by the solvers, the batched
+ * solve and the MATVEC timing entry point when it happens during their MATVECs). */
 DDSCAT_CUDA_API int ddscat_cuda_apply_f32(int cwhat, const void *x, void *y, const void *adia, const void *aoff);
 
 /* Krylov solvers: b, x (initial guess in, solution out), adia, aoff are full
