@@ -1372,7 +1372,8 @@ extern "C" DDSCAT_CUDA_API int ddscat_b200_adjoint_f32(int nrhs, const void* p, 
   io.work = bs.work; io.nwork = BATCH_WORK_VECTORS - 2;
   io.maxit = maxit; io.tol = (double)tol; io.verbose = verbose_level() >= 2; io.replace = 1; io.sym = 1;
   BatchResult res;
-  const int rc = solve_batch_qmrccg<float>(io, res);
+  int rc = solve_batch_qmrccg<float>(io, res);
+  if (!rc) rc = matvec_check(s.eng);
   if (rc) return rc == 1 ? 534 : rc;
   for (int r = 0; r < nrhs; ++r) {
     itno[r] = res.itno[r];
@@ -1471,7 +1472,8 @@ extern "C" DDSCAT_CUDA_API int ddscat_b200_adjoint_fwd_f32(int nsrc, const void*
   io.work = bs.work; io.nwork = BATCH_WORK_VECTORS;
   io.maxit = maxit; io.tol = (double)tol; io.verbose = verbose_level() >= 2; io.replace = 1; io.sym = 1;
   BatchResult res;
-  const int rc = solve_batch_qmrccg<float>(io, res);
+  int rc = solve_batch_qmrccg<float>(io, res);
+  if (!rc) rc = matvec_check(s.eng);
   if (rc) return rc == 1 ? 534 : rc;
   for (int r = 0; r < R; ++r) {
     itno[r] = res.itno[r];

@@ -182,6 +182,7 @@ int multi_solve(int nt, const int* dims, const int16_t* const* iocc, const float
         if (e == cudaSuccess) e = cudaStreamSynchronize(t.st);
         if (e != cudaSuccess) { set_cuda_error("multi-target output", e); rc = 546; }
       }
+      if (!rc) rc = matvec_check(t.eng);  // status word of the target's MATVEC kernels
       if (!rc) {
         for (int r = 0; r < t.R; ++r) {
           itno[t.first + r] = res.itno[r];
