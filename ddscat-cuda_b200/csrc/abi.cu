@@ -33,6 +33,10 @@ void clear_error() { g_last_error.clear(); }
 static std::atomic<unsigned long long> g_launches{0};
 void note_launch(unsigned long long k) { g_launches += k; }
 unsigned long long launch_total() { return g_launches.load(); }
+bool env_flag(const char* name) {
+  const char* v = std::getenv(name);
+  return v && *v && !(v[0] == '0' && v[1] == '\0');
+}
 // raise the dynamic shared-memory limit of kernel f once per process (thread-safe)
 void raise_smem_limit(const void* f) {
   static std::mutex mu;

@@ -29,6 +29,8 @@ int check_launch(const char* where);
 // console output level of the library (0 silent, 1 reference-style lines, 2 diagnostics)
 int verbose_level();
 void raise_smem_limit(const void* f);  // thread-safe, once per kernel
+// an on/off environment switch: on when set to a non-empty value other than "0"
+bool env_flag(const char* name);
 unsigned long long launch_total();     // kernels launched so far (note_launch counter)
 // count of kernels this library launched (reported by ddscat_b200_launch_count)
 void note_launch(unsigned long long k = 1);

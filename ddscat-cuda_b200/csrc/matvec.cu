@@ -531,7 +531,7 @@ template <typename T, int N> static const void* reg_kernel(Pass p) {
 
 // Register kernel for this pass and axis length, or null (generic path).
 template <typename T> static const void* pick_reg(Pass p, int n) {
-  if (std::getenv("DDSCAT_B200_GENERIC_FFT")) return nullptr;
+  if (env_flag("DDSCAT_B200_GENERIC_FFT")) return nullptr;
   if (sizeof(T) == 8) return nullptr;  // FP64 engine: generic path (register budget)
   if (p == Pass::YG && n == 512) return nullptr;
   switch (n) {
@@ -582,7 +582,7 @@ int Engine<T>::init_geometry(int nx, int ny, int nz, int ipbc, int nat, int nat0
   g.nx = nx; g.ny = ny; g.nz = nz;
   g.Mx = 2 * nx; g.My = 2 * ny; g.Mz = 2 * nz;
   g.nat = nat; g.nat0 = nat0; g.ipbc = ipbc;
-  if (pad && ipbc == 0 && nx % 2 == 0 && ny % 2 == 0 && nz % 2 == 0 && !std::getenv("DDSCAT_B200_NOPAD") &&
+  if (pad && ipbc == 0 && nx % 2 == 0 && ny % 2 == 0 && nz % 2 == 0 && !env_flag("DDSCAT_B200_NOPAD") &&
       !xpipe_supported<T>(g)) {
     // pad to the register-FFT lengths when the padded grid has at most 2.5x the
     // points of the 2n grid (the register pipeline is ~4x faster per point);
@@ -599,8 +599,8 @@ int Engine<T>::init_geometry(int nx, int ny, int nz, int ipbc, int nat, int nat0
   tune_thx = env_int("DDSCAT_B200_TH_X", 256);
   tune_ly = std::max(1, env_int("DDSCAT_B200_LY", 4));
   tune_tile = env_int("DDSCAT_B200_TILE", 0);
-  tune_zg = std::getenv("DDSCAT_B200_ZG") ? 1 : 0;
-  use_tma = std::getenv("DDSCAT_B200_NOTMA") ? 0 : 1;
+  tune_zg = env_flag("DDSCAT_B200_ZG") ? 1 : 0;
+  use_tma = env_flag("DDSCAT_B200_NOTMA") ? 0 : 1;
   if (!d_err) {
     if (cudaMalloc((void**)&d_err, sizeof(int)) != cudaSuccess) { set_error("prepare", "status word"); return 1; }
     cudaMemset(d_err, 0, sizeof(int));

@@ -1105,7 +1105,7 @@ template <typename T> static int xlaunch(const void* f, dim3 g, int th, size_t s
 bool xzg3_supported(int Mz) { return xkernel<float>(XPass::ZG3, Mz) != nullptr; }
 
 template <typename T> bool xpipe_supported(const Geometry& g) {
-  if (std::getenv("DDSCAT_B200_ZFIRST")) return false;
+  if (env_flag("DDSCAT_B200_ZFIRST")) return false;
   // FP64: axis lengths up to 256 (the shared memory of the 512-point passes is too large in complex double)
   auto ok = [](int n) { return xreg_supported(n) && (sizeof(T) == 4 || n <= 256); };
   return ok(g.Mx) && ok(g.My) && ok(g.Mz);
@@ -1228,7 +1228,7 @@ int matvec_xpipe(Engine<T>& E, const MvArgs<T>& a) {
   const void* fxyf = nullptr;
   const void* fxyi = nullptr;
   if constexpr (sizeof(T) == 4) {
-    if (E.slab_B == g.Mx && std::getenv("DDSCAT_B200_FUSEXY")) {
+    if (E.slab_B == g.Mx && env_flag("DDSCAT_B200_FUSEXY")) {
       fxyf = xykernel(true, g.Mx, g.My);
       fxyi = xykernel(false, g.Mx, g.My);
     }
