@@ -62,6 +62,8 @@ template <typename T> struct XParams {
   size_t A_rs;
   cplx<T>* B;  // [rb][c][kxl][ky][iz] for kx in [kx0, kx0 + nkx); fused xy passes: [rb][c][kx][iz][ky]
   int kx0, nkx, b_rhs0;
+  int nrb_mid;  // RHS of the current middle-stage batch
+  int zg_rch;   // RHS per ZG3R block (blockIdx.y = chunk)
   const cplx<T>* green;  // [irx][iry][irz][6] (IPBC=0) or [kx][ky][kz][6] (IPBC=1)
   int ipbc;
   const cplx<T>* twx;
@@ -593,6 +595,106 @@ template <typename T, int N, int BTY = 0> __global__ void __launch_bounds__(128,
   }
 }
 
+// ZG3R: ZG3 with the block's Green octant lines staged once in shared memory
+// and all RHS of the middle-stage batch processed by the same block (IPBC=0,
+// five-pass B layout): one L2 read of the octant lines per batch instead of
+// one per RHS, and the Green multiply reading shared memory.  Records of 48
+// bytes at consecutive kz are read with 16-byte loads at a 48-byte stride,
+// free of bank conflicts (3 is odd).
+// block: RZ lines x TT threads; grid (ceil(nkx*My/RZ), RHS chunks of zg_rch);
+// shared memory: FFT scratch [RZ][lsz] | Green [RZ][N/2+1][6]
+template <int N, int TT, int E, typename C>
+__device__ __forceinline__ void zg3_green_s(const C* rec, int t, C (&v)[3][E]) {
+#pragma unroll
+  for (int i = 0; i < E; ++i) {
+    const int kz = t + TT * i;
+    C a[6];
+    const float4* g4 = reinterpret_cast<const float4*>(rec + 6 * (kz <= N / 2 ? kz : N - kz));
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      const float4 q = g4[m];
+      a[2 * m] = mk2<C>(q.x, q.y);
+      a[2 * m + 1] = mk2<C>(q.z, q.w);
+    }
+    if (TT * i + TT - 1 <= N / 2) {
+      green_apply_s<1, 1, 1>(a, v[0][i], v[1][i], v[2][i]);
+    } else if (TT * i > N / 2) {
+      green_apply_s<1, -1, -1>(a, v[0][i], v[1][i], v[2][i]);
+    } else {
+      if (kz <= N / 2) green_apply_s<1, 1, 1>(a, v[0][i], v[1][i], v[2][i]);
+      else green_apply_s<1, -1, -1>(a, v[0][i], v[1][i], v[2][i]);
+    }
+  }
+}
+
+template <typename T, int N> __global__ void __launch_bounds__(128, 3) kx_zg3r(XParams<T> P) {
+  using C = cplx<T>;
+  using R = T;
+  using S_ = XShape<N>;
+  constexpr int E = S_::E, TT = S_::TT, H = S_::H, RZ = Z3Shape<N>::RZ;
+  constexpr int LREC = 6 * (N / 2 + 1);  // complex elements of a line's records
+  static_assert(Z3Shape<N>::OK && RZ * TT == 128 && sizeof(C) == 8, "kx_zg3r: FP32, 128-thread blocks");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int t = threadIdx.x % TT, l = threadIdx.x / TT;
+  C* my = reinterpret_cast<C*>(smem_raw) + (size_t)l * P.lsz;
+  C* gs = reinterpret_cast<C*>(smem_raw) + (size_t)RZ * P.lsz;  // [RZ][N/2+1][6]
+  const int nlines = P.nkx * P.My;
+  const int p = blockIdx.x * RZ + l;
+  const bool live = p < nlines;
+  const size_t cs = (size_t)nlines * P.nz;  // component stride of B
+  const int kxl = p / P.My;
+  const int kx = P.kx0 + kxl, ky = p - kxl * P.My;
+  // the block's octant lines: line ll is the contiguous record run of
+  // (irx, iry) = (min(kx, Mx - kx), min(ky, My - ky)), kz = 0..N/2
+  for (int u = threadIdx.x; u < RZ * (LREC / 2); u += 128) {
+    const int ll = u / (LREC / 2), o = u - ll * (LREC / 2);
+    const int pp = blockIdx.x * RZ + ll;
+    if (pp < nlines) {
+      const int kxl2 = pp / P.My, kx2 = P.kx0 + kxl2, ky2 = pp - kxl2 * P.My;
+      const int irx = min(kx2, P.Mx - kx2), iry = min(ky2, P.My - ky2);
+      const C* src = P.green + ((size_t)irx * (P.My / 2 + 1) + iry) * LREC;
+      cp_async16(gs + (size_t)ll * LREC + 2 * o, src + 2 * o);
+    }
+  }
+  const R sx = 2 * kx > P.Mx ? (R)-1 : (R)1, sy = 2 * ky > P.My ? (R)-1 : (R)1;
+  C w[E];
+  line_twiddles<E, +1>(w, t, P.twz);
+  bool staged = false;
+  const int rb1 = min(P.nrb_mid, ((int)blockIdx.y + 1) * P.zg_rch);
+  for (int rb = (int)blockIdx.y * P.zg_rch; rb < rb1; ++rb) {
+    if (xoff(P, P.b_rhs0 + rb)) continue;  // the same for every thread of the block
+    C* row = P.B + (size_t)rb * 3 * cs + (size_t)(live ? p : 0) * P.nz;
+    C v[3][E];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const R sc = c == 0 ? sx : (c == 1 ? sy : (R)1);
+#pragma unroll
+      for (int i = 0; i < H; ++i)
+        v[c][i] = live && t + TT * i < P.nz ? cscale(row[c * cs + (t + TT * i)], sc) : mk<C>(0, 0);  // iz < nz <= N/2
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) line_fft_w<E, TT, +1, false, true, S_::PAIR>(v[c], my, t, w);
+    if (!staged) {
+      cp_async_wait_all();
+      __syncthreads();  // every thread's Green copies have landed
+      staged = true;
+    }
+    if (live) zg3_green_s<N, TT, E>(gs + (size_t)l * LREC, t, v);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) line_fft_w<E, TT, -1, false, false, S_::PAIR, true>(v[c], my, t, w);
+    if (live) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const R sc = c == 0 ? sx : (c == 1 ? sy : (R)1);
+#pragma unroll
+        for (int i = 0; i < H; ++i)
+          if (t + TT * i < P.nz) row[c * cs + (t + TT * i)] = cscale(v[c][i], sc);  // keep iz < nz
+      }
+    }
+  }
+  cp_async_wait_all();  // no copy in flight at exit (every RHS masked)
+}
+
 // ------------------------------------------------------------- YI: y inverse
 // block: RL z-lines x TT; grid (ceil(nz/RL), nkx, 3*nrb)
 template <typename T, int N> __global__ void __launch_bounds__(256) kx_yi(const __grid_constant__ XParams<T> P) {
@@ -1024,7 +1126,7 @@ template <int NX, int NY> __global__ void __cluster_dims__(4, 1, 1) __launch_bou
 
 // ------------------------------------------------------------- host side
 // ZGT / ZG3T: the z passes on the B layout of the fused xy passes
-enum class XPass { XF, YF, ZG, ZG3, YI, XI, ZGT, ZG3T };
+enum class XPass { XF, YF, ZG, ZG3, YI, XI, ZGT, ZG3T, ZG3R };
 
 // z passes on the B layout of the fused xy passes (z stride M_y = BTY)
 template <typename T, int N, int BTY> static const void* xkt(XPass p) {
@@ -1051,6 +1153,10 @@ template <typename T, int N> static const void* xk(XPass p, int my = 0) {
     case XPass::ZG: return (const void*)kx_zg<T, N>;
     case XPass::ZG3:
       if constexpr (Z3Shape<N>::OK && sizeof(T) == 4) return (const void*)kx_zg3<T, N>;
+      return nullptr;
+    case XPass::ZG3R:
+      if constexpr (Z3Shape<N>::OK && sizeof(T) == 4 && 128 / RegShape<N>::T * RegShape<N>::T == 128)
+        return (const void*)kx_zg3r<T, N>;
       return nullptr;
 
     case XPass::YI: return (const void*)kx_yi<T, N>;
@@ -1214,6 +1320,10 @@ int matvec_xpipe(Engine<T>& E, const MvArgs<T>& a) {
   }
   // ZG3: FFT scratch
   const size_t smz = fzg3 ? (size_t)RZ3 * P.lsz * sizeof(C) : (size_t)3 * RZ * P.lsz * sizeof(C);
+  // ZG3R (Green lines staged once per block and reused for a chunk of RHS):
+  // IPBC=0, batches of at least 4 RHS (DDSCAT_B200_NOZG3R=1 keeps ZG3)
+  const void* fzg3r = fzg3 && g.ipbc == 0 && !env_flag("DDSCAT_B200_NOZG3R") ? xkernel<T>(XPass::ZG3R, g.Mz) : nullptr;
+  const size_t smzr = smz + (size_t)RZ3 * 6 * (g.Mz / 2 + 1) * sizeof(C);
   const void* fxf = xkernel<T>(XPass::XF, g.Mx);
   const void* fyf = xkernel<T>(XPass::YF, g.My);
   const void* fzg = xkernel<T>(XPass::ZG, g.Mz);
@@ -1269,13 +1379,21 @@ int matvec_xpipe(Engine<T>& E, const MvArgs<T>& a) {
     for (int rb0 = 0; rb0 < nr; rb0 += E.slab_nr) {
       const int nrb = std::min(E.slab_nr, nr - rb0);
       P.b_rhs0 = rb0;
+      P.nrb_mid = nrb;
       for (int kx0 = 0; kx0 < g.Mx; kx0 += E.slab_B) {
         P.kx0 = kx0;
         P.nkx = std::min(E.slab_B, g.Mx - kx0);
         if (xlaunch<T>(fyf, dim3((unsigned)ceil_div(g.nz, RY), (unsigned)P.nkx, (unsigned)(3 * nrb)), 256, smy,
                        E.stream, P))
           return 22;
-        if (fzg3 ? xlaunch<T>(fzg3, dim3((unsigned)nrb, (unsigned)ceil_div((size_t)P.nkx * g.My, RZ3)), 128, smz,
+        // ZG3R: RHS chunks so that the grid has at least 4 waves of 3 blocks per SM
+        const size_t nlb = ceil_div((size_t)P.nkx * g.My, RZ3);
+        const int nchunk = (int)std::min<size_t>((size_t)nrb, std::max<size_t>(1, ceil_div(4 * 3 * 148, nlb)));
+        P.zg_rch = (int)ceil_div((size_t)nrb, (size_t)nchunk);
+        const bool use_r = fzg3r && P.zg_rch >= 4;
+        if (use_r ? xlaunch<T>(fzg3r, dim3((unsigned)nlb, (unsigned)ceil_div((size_t)nrb, (size_t)P.zg_rch)), 128, smzr,
+                               E.stream, P)
+            : fzg3 ? xlaunch<T>(fzg3, dim3((unsigned)nrb, (unsigned)ceil_div((size_t)P.nkx * g.My, RZ3)), 128, smz,
                               E.stream, P)
                  : xlaunch<T>(fzg, dim3((unsigned)nrb, (unsigned)ceil_div((size_t)P.nkx * g.My, RZ)), 3 * TZ * RZ,
                               smz, E.stream, P))
