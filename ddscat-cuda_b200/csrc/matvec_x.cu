@@ -5,7 +5,8 @@
 // of its input with the T threads of a line inside one warp (register line
 // FFTs, fftreg.cuh), and the axis change is done by a shared-memory tile
 // transpose on the load or store side, keeping global accesses in 128-byte
-// segments:
+// segments (at the 256- and 512-point shapes the tiles move between shared and
+// global memory by the tensor memory accelerator):
 //   XF : x (compact or full) rows  -> x-FFT(+i), pad-skip -> A[c][iz][kx][iy]
 //   YF : A y-rows (n_y)            -> y-FFT(+i)           -> B[c][kx][ky][iz]
 //   ZG : B z-rows (n_z)            -> z-FFT(+i) * Green * z-FFT(-i), keep n_z
@@ -16,14 +17,16 @@
 // XYI below): the plane meets in distributed shared memory instead of an HBM
 // round trip of A, and B is laid out [c][kx][iz][ky] for them.
 // The Green octant is stored z-fastest, [irx][iry][irz][6], so a z-line reads
-// contiguous 48-byte records: kx_zg3 (the ZG pass for E <= 16, FP32) reads
-// its records straight from global memory (the octant stays L2-resident
-// across the RHS of a call) and keeps the three components of a z position in
-// one thread; kx_zg (larger E, FP64) loads each record once for kz and its
-// mirror M_z - kz and exchanges the components through shared memory.  The ZG grid runs RHS-fastest so
-// consecutive blocks reuse the Green tile from L2.  Twiddles are read from
-// global memory (L1/L2 resident tables).  The middle passes run over kx
-// batches (all of M_x for the FFT3D build, a few columns for the SLICES build).
+// contiguous 48-byte records.  kx_zg3 (the ZG pass for E <= 16, FP32) keeps
+// the three components of a z position in one thread and reads its records
+// straight from global memory, its grid RHS-fastest so that consecutive blocks
+// reuse the octant lines from L2; kx_zg3r (the default for batches of 4 RHS
+// or more, IPBC = 0) stages a block's octant lines in shared memory once and
+// runs the z pass for a chunk of RHS with them; kx_zg (larger E, FP64) loads
+// each record once for kz and its mirror M_z - kz and exchanges the
+// components through shared memory.  Twiddles are read from global memory
+// (L1/L2 resident tables).  The middle passes run over kx batches (all of M_x
+// for the FFT3D build, a few columns for the SLICES build).
 #include <algorithm>
 #include <cstdlib>
 #include <cooperative_groups.h>
