@@ -47,7 +47,9 @@ def _err(y, yr):
                                           ((20, 26, 14), 1), ((50, 10, 30), 0),
                                           # (M_x, M_y) = (256, 256), (128, 256), (256, 128), full and padded rows
                                           ((128, 128, 8), 0), ((100, 120, 6), 1), ((64, 128, 10), 0),
-                                          ((128, 60, 8), 0)])
+                                          ((128, 60, 8), 0),
+                                          # 512-point passes: z (kx_zg, E = 32), x and y (two TMA boxes per tile)
+                                          ((8, 8, 200), 0), ((200, 6, 8), 1), ((6, 200, 8), 0)])
 def test_apply_matches_oracle(layout, dims, idipint):
     iocc, ak, x, adia, aoff, gp = _case(dims, idipint)
     dda = D.DDA(layout)

@@ -59,6 +59,51 @@ def test_apply_noalloc_matches_apply(dims):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("dims", [(16, 16, 16), (18, 18, 18)])
+def test_apply_noalloc_in_cuda_graph(dims):
+    """The call captured into a CUDA graph on a caller's stream: every replay
+    reads the current contents of x and writes y, equal to ddscat_cuda_apply_f32
+    on the same inputs (the kernels' parameters, tensor maps included, are fixed
+    at capture; the scratch is the same fixed array)."""
+    torch = pytest.importorskip("torch")
+    iocc, ak, x1, x2, adia, aoff = _inputs(dims, 11)
+    dda = D.DDA()
+    dda.prepare_green(*dims, iocc, ak)
+    lib = dda.lib
+    dev = torch.device("cuda", torch.cuda.current_device())
+    xd = torch.from_numpy(x1).to(dev)
+    ad, od = torch.from_numpy(adia).to(dev), torch.from_numpy(aoff).to(dev)
+    yd = torch.empty_like(xd)
+    p = lambda t: ct.c_void_p(t.data_ptr())  # noqa: E731
+    s = torch.cuda.Stream()
+    sp = ct.c_void_p(s.cuda_stream)
+    s.wait_stream(torch.cuda.current_stream())
+    # uncaptured call first (one-time set-up), then the capture
+    assert lib.ddscat_b200_apply_noalloc_f32(ord("N"), p(xd), p(yd), p(ad), p(od), sp) == 0
+    s.synchronize()
+    g = torch.cuda.CUDAGraph()
+    rcs = []
+    with torch.cuda.graph(g, stream=s, capture_error_mode="thread_local"):
+        rcs.append(lib.ddscat_b200_apply_noalloc_f32(ord("N"), p(xd), p(yd), p(ad), p(od), sp))
+    assert rcs == [0]
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    got = []
+    for xh in (x2, x1):
+        xd.copy_(torch.from_numpy(xh))
+        yd.zero_()
+        g.replay()
+        torch.cuda.synchronize()
+        got.append(yd.cpu().numpy())
+    assert torch.cuda.mem_get_info()[0] == free0
+    del g
+    for xh, y in zip((x2, x1), got):
+        ref = dda.apply(xh, adia, aoff, "N")
+        assert np.linalg.norm(y - ref) / np.linalg.norm(ref) <= RTOL
+    dda.release()
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("dims", [(72, 72, 72), (72, 72, 64)])
 def test_apply_noalloc_rejects_large_target(dims):
     """72^3 has NAT = 373,248 > 349,525; 72x72x64 (NAT = 331,776) is under that
