@@ -555,6 +555,9 @@ def run_ours(args):
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": achieved / peak,
                          "traffic": None if traffic is None else traffic,
+                         # measured DRAM bytes (ncu, per RHS-MATVEC) over the event-timed MATVEC
+                         "traffic_gbs": None if traffic is None else traffic / (ms_per_rhs_mv * 1e-3) / 1e9,
+                         "traffic_frac": None if traffic is None else traffic / (ms_per_rhs_mv * 1e-3) / 1e9 / peak,
                          "algorithmic_bytes_per_rhs_matvec": alg, "ms_per_rhs_matvec": ms_per_rhs_mv,
                          "rhs_per_matvec_call": rhs_per_call},
             "cpu_baseline": cpu,
