@@ -1,6 +1,7 @@
-"""Seeded inputs of the edge cases that tests/golden/make_reference_fixtures.py
-runs through the reference library (reference_fixtures_edge.npz) and that
-tests/test_gpu_edge.py runs through this library (test inputs only)."""
+"""Seeded inputs of the edge cases and periodic targets that
+tests/golden/make_reference_fixtures.py runs through the reference library
+(reference_fixtures_edge.npz, reference_fixtures_pbc.npz) and that the tests
+run through the oracle and this library (test inputs only)."""
 import numpy as np
 
 from ddscat_b200 import targets
@@ -54,3 +55,40 @@ def sparse_problem(case):
     b, adia, aoff = prob.rhs(0), prob.adia(0), prob.aoff()
     x = (rng.normal(size=b.size) + 1j * rng.normal(size=b.size)).astype(np.complex64)
     return prob, b, adia, aoff, x
+
+
+def pbc_cases():
+    """Periodic MATVEC cases (name, dims, idipint, gamma, pyd, pzd, ak) and the
+    seeded inputs of each (80 % occupancy, random x zero on vacuum sites,
+    CXADIA shifted by 4 for a well-conditioned operator, CXAOFF); PYD and PZD are the periods in lattice units (dx = 1)."""
+    cases = [("y", (4, 3, 3), 0, 5e-2, 3.0, 0.0, (0.6, 0.25, 0.0)),
+             ("z", (6, 4, 4), 0, 5e-2, 0.0, 4.0, (0.5, 0.0, 0.3)),
+             ("yz", (6, 4, 4), 0, 5e-2, 4.0, 4.0, (0.6, 0.1, 0.05)),
+             ("yf", (5, 4, 4), 1, 5e-2, 4.0, 0.0, (0.55, 0.2, 0.1))]
+    out = []
+    rng = np.random.default_rng(4242)
+    for name, dims, idip, gamma, pyd, pzd, ak in cases:
+        nat = int(np.prod(dims))
+        iocc = (rng.random(nat) < 0.8).astype(np.int16)
+        iocc[0] = 1
+        c = lambda s=1.0: (s * (rng.normal(size=3 * nat) + 1j * rng.normal(size=3 * nat))).astype(np.complex64)  # noqa: E731
+        x, adia, aoff = c(), c(), c(0.3)
+        adia += np.complex64(4.0)
+        x[np.tile(iocc == 0, 3)] = 0
+        out.append(dict(name=name, dims=dims, idipint=idip, gamma=gamma, pyd=pyd, pzd=pzd,
+                        ak=np.array(ak, dtype=np.float32), iocc=iocc, x=x, adia=adia, aoff=aoff))
+    return out
+
+
+def pbc_solve_problem():
+    """A slab periodic in y and z: a 6 x 4 x 4 cell fully occupied, GKDLDR
+    CXADIA of m = 1.5+0.01i (targets.make_problem), incident along x
+    (k_perp = |k_x|), PBCGS2 at tol 1e-5; SCAT amplitudes in three directions.
+    Returns (prob, gamma, pyd, pzd, aks, em1, em2)."""
+    prob = targets.make_problem(6, 4, 4, m=1.5 + 0.01j, x=1.5, iocc=np.ones(96, dtype=np.int16))
+    th = np.deg2rad([0.0, 60.0, 180.0])
+    kk = float(np.linalg.norm(prob.incid[0].k))
+    aks = np.array([[kk * np.cos(t), kk * np.sin(t), 0.0] for t in th], dtype=np.float32)
+    em1 = np.array([[-np.sin(t), np.cos(t), 0.0] for t in th], dtype=np.float32)
+    em2 = np.array([[0.0, 0.0, 1.0] for t in th], dtype=np.float32)
+    return prob, 5e-2, 4.0, 4.0, aks, em1, em2

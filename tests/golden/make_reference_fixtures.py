@@ -19,7 +19,14 @@ edge_cases.py: every solver with a nonzero CXAOFF, the single-site target
 (PBCGS2 and QMRCCG return codes) and the MATVEC of hollow targets with vacant
 rows and planes.
 
-Run on a GPU machine:  python tests/golden/make_reference_fixtures.py [base|c1|edge|all]
+A fourth set (reference_fixtures_pbc.npz) holds periodic targets (IPBC = 1,
+the replica-sum Green tensor of cu:634-643 and the full-tensor MATVEC branch of
+cu:113): MATVECs for periodicity in y (JPBC 1), in z (JPBC 2) and in y and z
+(JPBC 3), one with IDIPINT = 1, and a PBCGS2 solve with EVALQ and SCAT's
+selected-direction amplitudes on a target periodic in y and z (the cases of
+edge_cases.pbc_cases and edge_cases.pbc_solve_problem).
+
+Run on a GPU machine:  python tests/golden/make_reference_fixtures.py [base|c1|edge|pbc|all]
 """
 import ctypes as ct
 import os
@@ -42,6 +49,7 @@ import edge_cases as EC  # noqa: E402
 OUT = os.path.join(HERE, "reference_fixtures.npz")
 OUT_C1 = os.path.join(HERE, "reference_fixtures_c1.npz")
 OUT_EDGE = os.path.join(HERE, "reference_fixtures_edge.npz")
+OUT_PBC = os.path.join(HERE, "reference_fixtures_pbc.npz")
 C1_TOL, C1_MAXIT, C1_ETASCA = 1e-5, 500, 0.5
 MV64_SAMPLES, MV64_PROJ = 8192, 4
 
@@ -296,6 +304,51 @@ def main_edge():
     print("wrote", OUT_EDGE, len(fx), "arrays")
 
 
+def main_pbc():
+    lib = ref_lib("fft3d")
+    fx = {}
+    for cs in EC.pbc_cases():
+        nx, ny, nz = cs["dims"]
+        nat = nx * ny * nz
+        rc = lib.ddscat_cuda_prepare_green_f32(nx, ny, nz, 1, nat, int(cs["iocc"].sum()), cs["idipint"], cs["gamma"],
+                                               cs["pyd"], cs["pzd"], *map(float, cs["ak"]), 1.0, 1.0, 1.0,
+                                               _p(cs["iocc"]))
+        assert rc == 0, lib.ddscat_cuda_last_error()
+        for cw in "NC":
+            y = np.empty_like(cs["x"])
+            assert lib.ddscat_cuda_apply_f32(ord(cw), _p(cs["x"]), _p(y), _p(cs["adia"]), _p(cs["aoff"])) == 0
+            fx[f"M_{cs['name']}_y{cw}"] = y
+        lib.ddscat_cuda_release()
+    prob, gamma, pyd, pzd, aks, em1, em2 = EC.pbc_solve_problem()
+    k = prob.incid[0].k.astype(np.float32)
+    rc = lib.ddscat_cuda_prepare_green_f32(prob.nx, prob.ny, prob.nz, 1, prob.nat, prob.nat0, 0, gamma, pyd, pzd,
+                                           *map(float, k), 1.0, 1.0, 1.0, _p(prob.iocc))
+    assert rc == 0, lib.ddscat_cuda_last_error()
+    b, adia, aoff = prob.rhs(0), prob.adia(0), prob.aoff()
+    rc, xs, meta = _ref_solve(lib, "pbcgs2", b, adia, aoff, 300, 1e-5)
+    fx.update({"P_rc": np.array([rc]), "P_x": xs, "P_meta": meta})
+    cabs, cext, cpha = ct.c_double(), ct.c_double(), ct.c_double()
+    assert lib.ddscat_cuda_evalq_f32(1, None, None, None, None, *map(float, k), 1.0, ct.byref(cabs), ct.byref(cext),
+                                     ct.byref(cpha)) == 0
+    fx["P_evalq"] = np.array([cabs.value, cext.value, cpha.value])
+    dx = np.ones(3, dtype=np.float32)
+    x0 = np.array(prob.x0, dtype=np.float32)
+    f1 = np.zeros(len(aks), dtype=np.complex64)
+    f2 = np.zeros(len(aks), dtype=np.complex64)
+    cb, csc, cg2 = ct.c_double(), ct.c_double(), ct.c_double()
+    cg = (ct.c_double * 3)()
+    navg = ct.c_int()
+    rc = lib.ddscat_cuda_scat_f32(3, len(aks), _p(k), _p(aks), _p(dx), _p(em1), _p(em2), 1.0, 0.0, None, _p(x0),
+                                  ct.byref(cb), ct.byref(csc), ct.cast(cg, ct.POINTER(ct.c_double)), ct.byref(cg2),
+                                  ct.byref(navg), _p(f1), _p(f2))
+    assert rc == 0, lib.ddscat_cuda_last_error()
+    fx.update({"P_scat": np.array([cb.value, csc.value, cg[0], cg[1], cg[2], cg2.value, navg.value]),
+               "P_f1": f1, "P_f2": f2})
+    lib.ddscat_cuda_release()
+    np.savez_compressed(OUT_PBC, **fx)
+    print("wrote", OUT_PBC, len(fx), "arrays")
+
+
 if __name__ == "__main__":
     which = sys.argv[1] if len(sys.argv) > 1 else "all"
     if which in ("base", "all"):
@@ -304,3 +357,5 @@ if __name__ == "__main__":
         main_c1()
     if which in ("edge", "all"):
         main_edge()
+    if which in ("pbc", "all"):
+        main_pbc()

@@ -146,3 +146,62 @@ def test_c1_workload_vs_reference(fc1):
         assert np.abs(sc["f1"] - fc1[f"C1_{r}_f1"]).max() <= 1e-4 * fmax
         assert np.abs(sc["f2"] - fc1[f"C1_{r}_f2"]).max() <= 1e-4 * fmax
     dda.release()
+
+
+# ---- periodic targets (IPBC = 1) against tests/golden/reference_fixtures_pbc.npz;
+# the inputs are regenerated by tests/golden/edge_cases.py
+FIX_PBC = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_fixtures_pbc.npz")
+
+
+def _edge_cases():
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    import edge_cases
+    return edge_cases
+
+
+@pytest.fixture(scope="module")
+def fpbc():
+    return dict(np.load(FIX_PBC))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("layout", ["fft3d", "slices"])
+@pytest.mark.parametrize("case", ["y", "z", "yz", "yf"])
+def test_periodic_matvec_vs_reference(fpbc, case, layout):
+    """Periodicity in y (JPBC 1), z (JPBC 2), y and z (JPBC 3), and in y with
+    IDIPINT = 1: the replica-sum Green build and the full-tensor MATVEC."""
+    cs = {c["name"]: c for c in _edge_cases().pbc_cases()}[case]
+    dda = D.DDA(layout)
+    dda.prepare_green(*cs["dims"], cs["iocc"], cs["ak"], ipbc=1, idipint=cs["idipint"], gamma=cs["gamma"],
+                      pyd=cs["pyd"], pzd=cs["pzd"])
+    for cw in "NC":
+        y = dda.apply(cs["x"], cs["adia"], cs["aoff"], cw)
+        assert _rel(y, fpbc[f"M_{case}_y{cw}"]) < 2e-5
+        assert np.all(y.reshape(3, -1)[:, cs["iocc"] == 0] == 0)
+    dda.release()
+
+
+@pytest.mark.gpu
+def test_periodic_solve_evalq_scat_vs_reference(fpbc):
+    """A slab periodic in y and z: PBCGS2 return code, ITNO, NCOMPTE and
+    solution, EVALQ, and SCAT with JPBC = 3 (no finite-target integration:
+    zero sums and NAVG = 0; amplitudes in the selected directions, within
+    2e-5 of the largest)."""
+    prob, gamma, pyd, pzd, aks, em1, em2 = _edge_cases().pbc_solve_problem()
+    k = prob.incid[0].k.astype(np.float32)
+    dda = D.DDA()
+    dda.prepare_green(prob.nx, prob.ny, prob.nz, prob.iocc, k, ipbc=1, gamma=gamma, pyd=pyd, pzd=pzd)
+    out = dda.solve("pbcgs2", prob.rhs(0), prob.adia(0), prob.aoff(), maxit=300, tol=TOL, check=False)
+    it_ref, tole_ref, nc_ref = fpbc["P_meta"]
+    assert out.rc == int(fpbc["P_rc"][0]) == 0 and out.tole <= TOL
+    assert abs(out.itno - it_ref) <= 1 and abs(out.ncompte - nc_ref) <= 2, (out.itno, out.ncompte)
+    assert _rel(out.x, fpbc["P_x"]) < 20 * TOL
+    for g, r in zip(dda.evalq(k), fpbc["P_evalq"]):
+        assert abs(g - r) <= 1e-5 * abs(r)
+    sc = dda.scat(k, prob.incid[0].e, prob.x0, etasca=0.0, jpbc=3, aks=aks, em1=em1, em2=em2)
+    assert sc["navg"] == 0 and sc["csca"] == 0.0 and sc["cbksca"] == 0.0 and sc["cscag2"] == 0.0
+    fmax = np.abs(fpbc["P_f1"]).max()
+    assert np.abs(sc["f1"] - fpbc["P_f1"]).max() <= 2e-5 * fmax
+    assert np.abs(sc["f2"] - fpbc["P_f2"]).max() <= 2e-5 * fmax
+    dda.release()

@@ -224,3 +224,57 @@ def test_oracle_sparse_matvec_matches_reference(fedge, case):
         y = op.apply_full(x, adia, aoff, cw)
         ref = fedge[f"S_{case}_y{cw}"]
         assert np.linalg.norm(y - ref) / np.linalg.norm(ref) < 2e-5
+
+
+# ---- periodic targets (reference_fixtures_pbc.npz, IPBC = 1): replica-sum Green
+# tensor and full-tensor MATVEC for periodicity in y, z and y+z, with IDIPINT 0
+# and 1, and a PBCGS2 solve with EVALQ and SCAT amplitudes on a slab periodic in
+# y and z; inputs regenerated by tests/golden/edge_cases.py
+FIX_PBC = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_fixtures_pbc.npz")
+
+
+@pytest.fixture(scope="module")
+def fpbc():
+    return dict(np.load(FIX_PBC))
+
+
+def _pbc_operator(cs):
+    gp = O.GreenParams(*cs["dims"], ipbc=1, idipint=cs["idipint"], gamma=cs["gamma"], pyd=cs["pyd"], pzd=cs["pzd"],
+                       ak=tuple(float(a) for a in cs["ak"]))
+    return O.Operator.from_params(gp, cs["iocc"])
+
+
+@pytest.mark.parametrize("case", ["y", "z", "yz", "yf"])
+def test_oracle_periodic_matvec_matches_reference(fpbc, case):
+    cs = {c["name"]: c for c in _edge_cases().pbc_cases()}[case]
+    op = _pbc_operator(cs)
+    for cw in "NC":
+        y = op.apply_full(cs["x"], cs["adia"], cs["aoff"], cw)
+        assert _rel(y, fpbc[f"M_{case}_y{cw}"]) < 2e-5
+
+
+def test_oracle_periodic_solve_matches_reference(fpbc):
+    EC = _edge_cases()
+    prob, gamma, pyd, pzd, aks, em1, em2 = EC.pbc_solve_problem()
+    k = prob.incid[0].k.astype(np.float32).astype(np.float64)
+    gp = O.GreenParams(prob.nx, prob.ny, prob.nz, ipbc=1, gamma=gamma, pyd=pyd, pzd=pzd, ak=tuple(k))
+    op = O.Operator.from_params(gp, prob.iocc)
+    occ = op.occ
+    c = lambda v: O.gather_compact(v, occ, prob.nat).astype(np.complex128)  # noqa: E731
+    bc, ac, oc = c(prob.rhs(0)), c(prob.adia(0)), c(prob.aoff())
+    mv = lambda v: op.apply_compact(v, ac, oc)  # noqa: E731
+    it_ref, tole_ref, nc_ref = fpbc["P_meta"]
+    assert int(fpbc["P_rc"][0]) == 0 and tole_ref <= TOL
+    res = O.solve_pbcgs2(mv, bc, np.zeros_like(bc), 300, TOL)
+    assert res.status == 0 and abs(res.itno - it_ref) <= 1 and abs(res.ncompte - nc_ref) <= 2
+    xr = c(fpbc["P_x"])
+    assert np.linalg.norm(res.x - xr) / np.linalg.norm(xr) < 20 * TOL
+    for g, r in zip(O.evalq(bc, xr, ac, oc, k, 1.0), fpbc["P_evalq"]):
+        assert abs(g - r) <= 1e-6 * abs(r)
+    # JPBC = 3: SCAT skips the finite-target integration (zero sums, NAVG = 0)
+    # and returns the amplitudes in the selected directions
+    sc = O.scat(xr, occ, prob.nx, prob.ny, 3, k, aks, (1, 1, 1), em1, em2, 1.0, 0.0, None, prob.x0)
+    assert sc["navg"] == 0 and np.all(fpbc["P_scat"] == 0)
+    fmax = np.abs(fpbc["P_f1"]).max()
+    assert np.abs(sc["f1"] - fpbc["P_f1"]).max() <= 2e-5 * fmax
+    assert np.abs(sc["f2"] - fpbc["P_f2"]).max() <= 2e-5 * fmax
