@@ -92,3 +92,21 @@ def pbc_solve_problem():
     em1 = np.array([[-np.sin(t), np.cos(t), 0.0] for t in th], dtype=np.float32)
     em2 = np.array([[0.0, 0.0, 1.0] for t in th], dtype=np.float32)
     return prob, 5e-2, 4.0, 4.0, aks, em1, em2
+
+
+def pbc_cpu_green_case():
+    """prepare_f32 with IPBC = 1: a caller-supplied full-grid spectrum of the
+    six tensor components, planar (6, 2nz, 2ny, 2nx) complex64 (random, seeded:
+    the MATVEC's full-tensor branch and the spectrum's layout do not depend on
+    its values being a Green tensor), on a 6 x 5 x 4 grid with random inputs."""
+    rng = np.random.default_rng(777)
+    dims = (6, 5, 4)
+    nat = int(np.prod(dims))
+    shape = (6, 2 * dims[2], 2 * dims[1], 2 * dims[0])
+    green = (rng.normal(size=shape) + 1j * rng.normal(size=shape)).astype(np.complex64)
+    iocc = (rng.random(nat) < 0.8).astype(np.int16)
+    iocc[0] = 1
+    c = lambda s=1.0: (s * (rng.normal(size=3 * nat) + 1j * rng.normal(size=3 * nat))).astype(np.complex64)  # noqa: E731
+    x, adia, aoff = c(), c(), c(0.3)
+    x[np.tile(iocc == 0, 3)] = 0
+    return dict(dims=dims, green=green, iocc=iocc, x=x, adia=adia, aoff=aoff)

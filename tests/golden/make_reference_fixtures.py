@@ -22,7 +22,8 @@ rows and planes.
 A fourth set (reference_fixtures_pbc.npz) holds periodic targets (IPBC = 1,
 the replica-sum Green tensor of cu:634-643 and the full-tensor MATVEC branch of
 cu:113): MATVECs for periodicity in y (JPBC 1), in z (JPBC 2) and in y and z
-(JPBC 3), one with IDIPINT = 1, and a PBCGS2 solve with EVALQ and SCAT's
+(JPBC 3), one with IDIPINT = 1, one on a caller-supplied full-grid spectrum
+(prepare_f32 with IPBC = 1), and a PBCGS2 solve with EVALQ and SCAT's
 selected-direction amplitudes on a target periodic in y and z (the cases of
 edge_cases.pbc_cases and edge_cases.pbc_solve_problem).
 
@@ -319,6 +320,15 @@ def main_pbc():
             assert lib.ddscat_cuda_apply_f32(ord(cw), _p(cs["x"]), _p(y), _p(cs["adia"]), _p(cs["aoff"])) == 0
             fx[f"M_{cs['name']}_y{cw}"] = y
         lib.ddscat_cuda_release()
+    cs = EC.pbc_cpu_green_case()
+    nx, ny, nz = cs["dims"]
+    nat = nx * ny * nz
+    assert lib.ddscat_cuda_prepare_f32(nx, ny, nz, 1, nat, int(cs["iocc"].sum()), _p(cs["green"]), _p(cs["iocc"])) == 0
+    for cw in "NC":
+        y = np.empty_like(cs["x"])
+        assert lib.ddscat_cuda_apply_f32(ord(cw), _p(cs["x"]), _p(y), _p(cs["adia"]), _p(cs["aoff"])) == 0
+        fx[f"M_cpu_y{cw}"] = y
+    lib.ddscat_cuda_release()
     prob, gamma, pyd, pzd, aks, em1, em2 = EC.pbc_solve_problem()
     k = prob.incid[0].k.astype(np.float32)
     rc = lib.ddscat_cuda_prepare_green_f32(prob.nx, prob.ny, prob.nz, 1, prob.nat, prob.nat0, 0, gamma, pyd, pzd,

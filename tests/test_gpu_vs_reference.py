@@ -205,3 +205,17 @@ def test_periodic_solve_evalq_scat_vs_reference(fpbc):
     assert np.abs(sc["f1"] - fpbc["P_f1"]).max() <= 2e-5 * fmax
     assert np.abs(sc["f2"] - fpbc["P_f2"]).max() <= 2e-5 * fmax
     dda.release()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("layout", ["fft3d", "slices"])
+def test_periodic_prepare_f32_vs_reference(fpbc, layout):
+    """ddscat_cuda_prepare_f32 with IPBC = 1 and a caller-supplied full-grid
+    spectrum (planar, six components), then the MATVEC in both CWHAT."""
+    cs = _edge_cases().pbc_cpu_green_case()
+    dda = D.DDA(layout)
+    dda.prepare(*cs["dims"], cs["iocc"], cs["green"], ipbc=1)
+    for cw in "NC":
+        y = dda.apply(cs["x"], cs["adia"], cs["aoff"], cw)
+        assert _rel(y, fpbc[f"M_cpu_y{cw}"]) < 2e-5
+    dda.release()

@@ -278,3 +278,13 @@ def test_oracle_periodic_solve_matches_reference(fpbc):
     fmax = np.abs(fpbc["P_f1"]).max()
     assert np.abs(sc["f1"] - fpbc["P_f1"]).max() <= 2e-5 * fmax
     assert np.abs(sc["f2"] - fpbc["P_f2"]).max() <= 2e-5 * fmax
+
+
+def test_oracle_periodic_cpu_green_matvec_matches_reference(fpbc):
+    """prepare_f32 with IPBC = 1: the full-tensor MATVEC on a caller-supplied
+    planar (6, 2nz, 2ny, 2nx) spectrum."""
+    cs = _edge_cases().pbc_cpu_green_case()
+    op = O.Operator(*cs["dims"], cs["green"].astype(np.complex128), cs["iocc"])
+    for cw in "NC":
+        y = op.apply_full(cs["x"], cs["adia"], cs["aoff"], cw)
+        assert _rel(y, fpbc[f"M_cpu_y{cw}"]) < 2e-5
