@@ -110,3 +110,42 @@ def pbc_cpu_green_case():
     x, adia, aoff = c(), c(), c(0.3)
     x[np.tile(iocc == 0, 3)] = 0
     return dict(dims=dims, green=green, iocc=iocc, x=x, adia=adia, aoff=aoff)
+
+
+DX = (1.0, 0.9, 1.1)
+
+
+def dx_cases():
+    """Rectangular lattices, DX = (1.0, 0.9, 1.1) (prepare_green's dx1..dx3):
+    MATVEC cases (name, dims, ipbc, idipint, gamma, pyd, ak) with seeded inputs
+    as in pbc_cases; the periodic one exercises the period PYD * DX(2) and the
+    replica offsets jpy * PYD * DX(2) * DX(2) of cu:642 and cu:1012."""
+    cases = [("iso", (7, 6, 5), 0, 0, 0.0, 0.0, (0.35, -0.2, 0.3)),
+             ("flt", (7, 6, 5), 0, 1, 0.0, 0.0, (0.35, -0.2, 0.3)),
+             ("pbc", (5, 4, 4), 1, 0, 5e-2, 4.0, (0.55, 0.2, 0.1))]
+    out = []
+    rng = np.random.default_rng(99)
+    for name, dims, ipbc, idip, gamma, pyd, ak in cases:
+        nat = int(np.prod(dims))
+        iocc = (rng.random(nat) < 0.8).astype(np.int16)
+        iocc[0] = 1
+        c = lambda s=1.0: (s * (rng.normal(size=3 * nat) + 1j * rng.normal(size=3 * nat))).astype(np.complex64)  # noqa: E731
+        x, adia, aoff = c(), c(), c(0.3)
+        adia += np.complex64(4.0)
+        x[np.tile(iocc == 0, 3)] = 0
+        out.append(dict(name=name, dims=dims, ipbc=ipbc, idipint=idip, gamma=gamma, pyd=pyd,
+                        ak=np.array(ak, dtype=np.float32), iocc=iocc, x=x, adia=adia, aoff=aoff))
+    return out
+
+
+def dx_solve_problem():
+    """A 10 x 8 x 6 ellipsoid on the DX lattice (m = 1.5+0.01i, x = 2), QMRCCG at
+    tol 1e-5, EVALQ, and SCAT at ETASCA 3.0 (site positions ((i+1)+x0)*DX) with
+    amplitudes in seven directions of the xy plane."""
+    prob = targets.make_problem(10, 8, 6, m=1.5 + 0.01j, x=2.0)
+    th = np.deg2rad(np.arange(0.0, 181.0, 30.0))
+    kk = float(np.linalg.norm(prob.incid[0].k))
+    aks = np.array([[kk * np.cos(t), kk * np.sin(t), 0.0] for t in th], dtype=np.float32)
+    em1 = np.array([[-np.sin(t), np.cos(t), 0.0] for t in th], dtype=np.float32)
+    em2 = np.array([[0.0, 0.0, 1.0] for t in th], dtype=np.float32)
+    return prob, aks, em1, em2

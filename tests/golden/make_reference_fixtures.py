@@ -27,7 +27,11 @@ cu:113): MATVECs for periodicity in y (JPBC 1), in z (JPBC 2) and in y and z
 selected-direction amplitudes on a target periodic in y and z (the cases of
 edge_cases.pbc_cases and edge_cases.pbc_solve_problem).
 
-Run on a GPU machine:  python tests/golden/make_reference_fixtures.py [base|c1|edge|pbc|all]
+A fifth set (reference_fixtures_dx.npz) holds rectangular lattices (dx1..dx3 =
+1.0, 0.9, 1.1): MATVECs with IDIPINT 0 and 1 and a periodic one, and a QMRCCG
+solve with EVALQ and SCAT (edge_cases.dx_cases, edge_cases.dx_solve_problem).
+
+Run on a GPU machine:  python tests/golden/make_reference_fixtures.py [base|c1|edge|pbc|dx|all]
 """
 import ctypes as ct
 import os
@@ -51,6 +55,7 @@ OUT = os.path.join(HERE, "reference_fixtures.npz")
 OUT_C1 = os.path.join(HERE, "reference_fixtures_c1.npz")
 OUT_EDGE = os.path.join(HERE, "reference_fixtures_edge.npz")
 OUT_PBC = os.path.join(HERE, "reference_fixtures_pbc.npz")
+OUT_DX = os.path.join(HERE, "reference_fixtures_dx.npz")
 C1_TOL, C1_MAXIT, C1_ETASCA = 1e-5, 500, 0.5
 MV64_SAMPLES, MV64_PROJ = 8192, 4
 
@@ -359,6 +364,52 @@ def main_pbc():
     print("wrote", OUT_PBC, len(fx), "arrays")
 
 
+def main_dx():
+    lib = ref_lib("fft3d")
+    fx = {}
+    dx = np.array(EC.DX, dtype=np.float32)
+    for cs in EC.dx_cases():
+        nx, ny, nz = cs["dims"]
+        nat = nx * ny * nz
+        rc = lib.ddscat_cuda_prepare_green_f32(nx, ny, nz, cs["ipbc"], nat, int(cs["iocc"].sum()), cs["idipint"],
+                                               cs["gamma"], cs["pyd"], 0.0, *map(float, cs["ak"]), *map(float, dx),
+                                               _p(cs["iocc"]))
+        assert rc == 0, lib.ddscat_cuda_last_error()
+        for cw in "NC":
+            y = np.empty_like(cs["x"])
+            assert lib.ddscat_cuda_apply_f32(ord(cw), _p(cs["x"]), _p(y), _p(cs["adia"]), _p(cs["aoff"])) == 0
+            fx[f"M_{cs['name']}_y{cw}"] = y
+        lib.ddscat_cuda_release()
+    prob, aks, em1, em2 = EC.dx_solve_problem()
+    k = prob.incid[0].k.astype(np.float32)
+    rc = lib.ddscat_cuda_prepare_green_f32(prob.nx, prob.ny, prob.nz, 0, prob.nat, prob.nat0, 0, 0.0, 0.0, 0.0,
+                                           *map(float, k), *map(float, dx), _p(prob.iocc))
+    assert rc == 0, lib.ddscat_cuda_last_error()
+    b, adia, aoff = prob.rhs(0), prob.adia(0), prob.aoff()
+    rc, xs, meta = _ref_solve(lib, "qmrccg", b, adia, aoff, 300, 1e-5)
+    fx.update({"Q_rc": np.array([rc]), "Q_x": xs, "Q_meta": meta})
+    cabs, cext, cpha = ct.c_double(), ct.c_double(), ct.c_double()
+    assert lib.ddscat_cuda_evalq_f32(1, None, None, None, None, *map(float, k), 1.0, ct.byref(cabs), ct.byref(cext),
+                                     ct.byref(cpha)) == 0
+    fx["Q_evalq"] = np.array([cabs.value, cext.value, cpha.value])
+    x0 = np.array(prob.x0, dtype=np.float32)
+    e01 = prob.incid[0].e.astype(np.complex64)
+    f1 = np.zeros(len(aks), dtype=np.complex64)
+    f2 = np.zeros(len(aks), dtype=np.complex64)
+    cb, csc, cg2 = ct.c_double(), ct.c_double(), ct.c_double()
+    cg = (ct.c_double * 3)()
+    navg = ct.c_int()
+    rc = lib.ddscat_cuda_scat_f32(0, len(aks), _p(k), _p(aks), _p(dx), _p(em1), _p(em2), 1.0, 3.0, _p(e01), _p(x0),
+                                  ct.byref(cb), ct.byref(csc), ct.cast(cg, ct.POINTER(ct.c_double)), ct.byref(cg2),
+                                  ct.byref(navg), _p(f1), _p(f2))
+    assert rc == 0, lib.ddscat_cuda_last_error()
+    fx.update({"Q_scat": np.array([cb.value, csc.value, cg[0], cg[1], cg[2], cg2.value, navg.value]),
+               "Q_f1": f1, "Q_f2": f2})
+    lib.ddscat_cuda_release()
+    np.savez_compressed(OUT_DX, **fx)
+    print("wrote", OUT_DX, len(fx), "arrays")
+
+
 if __name__ == "__main__":
     which = sys.argv[1] if len(sys.argv) > 1 else "all"
     if which in ("base", "all"):
@@ -369,3 +420,5 @@ if __name__ == "__main__":
         main_edge()
     if which in ("pbc", "all"):
         main_pbc()
+    if which in ("dx", "all"):
+        main_dx()

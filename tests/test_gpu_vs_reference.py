@@ -219,3 +219,57 @@ def test_periodic_prepare_f32_vs_reference(fpbc, layout):
         y = dda.apply(cs["x"], cs["adia"], cs["aoff"], cw)
         assert _rel(y, fpbc[f"M_cpu_y{cw}"]) < 2e-5
     dda.release()
+
+
+# ---- rectangular lattices (dx1..dx3 = 1.0, 0.9, 1.1) against
+# tests/golden/reference_fixtures_dx.npz
+FIX_DX = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_fixtures_dx.npz")
+
+
+@pytest.fixture(scope="module")
+def fdx():
+    return dict(np.load(FIX_DX))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("layout", ["fft3d", "slices"])
+@pytest.mark.parametrize("case", ["iso", "flt", "pbc"])
+def test_rectangular_lattice_matvec_vs_reference(fdx, case, layout):
+    EC = _edge_cases()
+    cs = {c["name"]: c for c in EC.dx_cases()}[case]
+    dda = D.DDA(layout)
+    dda.prepare_green(*cs["dims"], cs["iocc"], cs["ak"], dx=EC.DX, ipbc=cs["ipbc"], idipint=cs["idipint"],
+                      gamma=cs["gamma"], pyd=cs["pyd"], pzd=0.0)
+    for cw in "NC":
+        y = dda.apply(cs["x"], cs["adia"], cs["aoff"], cw)
+        assert _rel(y, fdx[f"M_{case}_y{cw}"]) < 2e-5
+    dda.release()
+
+
+@pytest.mark.gpu
+def test_rectangular_lattice_solve_evalq_scat_vs_reference(fdx):
+    """QMRCCG on an ellipsoid of the rectangular lattice (the padded register-FFT
+    grid), EVALQ, and SCAT with the site positions ((i+1)+x0)*DX."""
+    EC = _edge_cases()
+    prob, aks, em1, em2 = EC.dx_solve_problem()
+    k = prob.incid[0].k.astype(np.float32)
+    dda = D.DDA()
+    dda.prepare_green(prob.nx, prob.ny, prob.nz, prob.iocc, k, dx=EC.DX)
+    out = dda.solve("qmrccg", prob.rhs(0), prob.adia(0), prob.aoff(), maxit=300, tol=TOL)
+    it_ref, tole_ref, nc_ref = fdx["Q_meta"]
+    assert out.rc == int(fdx["Q_rc"][0]) == 0 and out.tole <= TOL
+    assert abs(out.itno - it_ref) <= max(1, 0.2 * it_ref) and abs(out.ncompte - nc_ref) <= max(2, 0.2 * nc_ref)
+    assert _rel(out.x, fdx["Q_x"]) < 20 * TOL
+    for g, r in zip(dda.evalq(k), fdx["Q_evalq"]):
+        assert abs(g - r) <= 1e-5 * abs(r)
+    sc = dda.scat(k, prob.incid[0].e, prob.x0, dx=EC.DX, etasca=3.0, aks=aks, em1=em1, em2=em2)
+    cb, cs, g0, g1, g2, cg2, navg = fdx["Q_scat"]
+    assert sc["navg"] == int(navg)
+    assert abs(sc["csca"] - cs) <= 1e-5 * cs and abs(sc["cscag2"] - cg2) <= 1e-5 * cs
+    for a, r in zip(sc["cscag"], (g0, g1, g2)):
+        assert abs(a - r) <= 1e-5 * cs
+    assert abs(sc["cbksca"] - cb) <= 1e-5 * cs
+    fmax = np.abs(fdx["Q_f1"]).max()
+    assert np.abs(sc["f1"] - fdx["Q_f1"]).max() <= 2e-5 * fmax
+    assert np.abs(sc["f2"] - fdx["Q_f2"]).max() <= 2e-5 * fmax
+    dda.release()

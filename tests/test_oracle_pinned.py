@@ -288,3 +288,55 @@ def test_oracle_periodic_cpu_green_matvec_matches_reference(fpbc):
     for cw in "NC":
         y = op.apply_full(cs["x"], cs["adia"], cs["aoff"], cw)
         assert _rel(y, fpbc[f"M_cpu_y{cw}"]) < 2e-5
+
+
+# ---- rectangular lattices (reference_fixtures_dx.npz): dx1..dx3 = 1.0, 0.9, 1.1
+FIX_DX = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_fixtures_dx.npz")
+
+
+@pytest.fixture(scope="module")
+def fdx():
+    return dict(np.load(FIX_DX))
+
+
+@pytest.mark.parametrize("case", ["iso", "flt", "pbc"])
+def test_oracle_rectangular_lattice_matvec_matches_reference(fdx, case):
+    EC = _edge_cases()
+    cs = {c["name"]: c for c in EC.dx_cases()}[case]
+    gp = O.GreenParams(*cs["dims"], ipbc=cs["ipbc"], idipint=cs["idipint"], gamma=cs["gamma"], pyd=cs["pyd"],
+                       pzd=0.0, dx=EC.DX, ak=tuple(float(a) for a in cs["ak"]))
+    op = O.Operator.from_params(gp, cs["iocc"])
+    for cw in "NC":
+        y = op.apply_full(cs["x"], cs["adia"], cs["aoff"], cw)
+        assert _rel(y, fdx[f"M_{case}_y{cw}"]) < 2e-5
+
+
+def test_oracle_rectangular_lattice_solve_matches_reference(fdx):
+    EC = _edge_cases()
+    prob, aks, em1, em2 = EC.dx_solve_problem()
+    k = prob.incid[0].k.astype(np.float32).astype(np.float64)
+    gp = O.GreenParams(prob.nx, prob.ny, prob.nz, dx=EC.DX, ak=tuple(k))
+    op = O.Operator.from_params(gp, prob.iocc)
+    occ = op.occ
+    c = lambda v: O.gather_compact(v, occ, prob.nat).astype(np.complex128)  # noqa: E731
+    bc, ac, oc = c(prob.rhs(0)), c(prob.adia(0)), c(prob.aoff())
+    mv = lambda v: op.apply_compact(v, ac, oc)  # noqa: E731
+    it_ref, tole_ref, nc_ref = fdx["Q_meta"]
+    assert int(fdx["Q_rc"][0]) == 0 and tole_ref <= TOL
+    res = O.SOLVERS["qmrccg"](mv, bc, np.zeros_like(bc), 300, TOL)
+    assert res.status == 0 and abs(res.itno - it_ref) <= 1 and abs(res.ncompte - nc_ref) <= 2
+    xr = c(fdx["Q_x"])
+    assert np.linalg.norm(res.x - xr) / np.linalg.norm(xr) < 20 * TOL
+    for g, r in zip(O.evalq(bc, xr, ac, oc, k, 1.0), fdx["Q_evalq"]):
+        assert abs(g - r) <= 1e-6 * abs(r)
+    sc = O.scat(xr, occ, prob.nx, prob.ny, 0, k, aks, EC.DX, em1, em2, 1.0, 3.0, prob.incid[0].e, prob.x0)
+    cb, cs, g0, g1, g2, cg2, navg = fdx["Q_scat"]
+    assert sc["navg"] == int(navg)
+    assert sc["csca"] == pytest.approx(cs, rel=2e-5)
+    assert sc["cscag2"] == pytest.approx(cg2, rel=2e-5)
+    for a, r in zip(sc["cscag"], (g0, g1, g2)):
+        assert abs(a - r) <= 2e-5 * cs
+    assert abs(sc["cbksca"] - cb) <= 2e-5 * cs
+    fmax = np.abs(fdx["Q_f1"]).max()
+    assert np.abs(sc["f1"] - fdx["Q_f1"]).max() <= 2e-5 * fmax
+    assert np.abs(sc["f2"] - fdx["Q_f2"]).max() <= 2e-5 * fmax
