@@ -149,3 +149,16 @@ def dx_solve_problem():
     em1 = np.array([[-np.sin(t), np.cos(t), 0.0] for t in th], dtype=np.float32)
     em2 = np.array([[0.0, 0.0, 1.0] for t in th], dtype=np.float32)
     return prob, aks, em1, em2
+
+
+def limits_problem():
+    """The solvers' limit cases on a 12^3 sphere (m = 1.5+0.01i, x = 2): MAXIT
+    reached (maxit 3 at tol 1e-12), a zero right-hand side (maxit 10), and a
+    nonzero initial guess (seeded, zero on vacuum sites; maxit 300, tol 1e-5).
+    Returns (prob, b, adia, aoff, x0)."""
+    prob = targets.make_problem(12, m=1.5 + 0.01j, x=2.0)
+    b, adia, aoff = prob.rhs(0), prob.adia(0), prob.aoff()
+    rng = np.random.default_rng(314)
+    x0 = (0.05 * (rng.normal(size=b.size) + 1j * rng.normal(size=b.size))).astype(np.complex64)
+    x0.reshape(3, -1)[:, prob.iocc == 0] = 0
+    return prob, b, adia, aoff, x0

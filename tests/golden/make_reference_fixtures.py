@@ -31,7 +31,11 @@ A fifth set (reference_fixtures_dx.npz) holds rectangular lattices (dx1..dx3 =
 1.0, 0.9, 1.1): MATVECs with IDIPINT 0 and 1 and a periodic one, and a QMRCCG
 solve with EVALQ and SCAT (edge_cases.dx_cases, edge_cases.dx_solve_problem).
 
-Run on a GPU machine:  python tests/golden/make_reference_fixtures.py [base|c1|edge|pbc|dx|all]
+A sixth set (reference_fixtures_limits.npz) holds the limit cases of all eight
+solvers (edge_cases.limits_problem): MAXIT reached, a zero right-hand side and
+a nonzero initial guess, with return codes, ITNO, TOLE, NCOMPTE and x.
+
+Run on a GPU machine:  python tests/golden/make_reference_fixtures.py [base|c1|edge|pbc|dx|limits|all]
 """
 import ctypes as ct
 import os
@@ -56,6 +60,7 @@ OUT_C1 = os.path.join(HERE, "reference_fixtures_c1.npz")
 OUT_EDGE = os.path.join(HERE, "reference_fixtures_edge.npz")
 OUT_PBC = os.path.join(HERE, "reference_fixtures_pbc.npz")
 OUT_DX = os.path.join(HERE, "reference_fixtures_dx.npz")
+OUT_LIM = os.path.join(HERE, "reference_fixtures_limits.npz")
 C1_TOL, C1_MAXIT, C1_ETASCA = 1e-5, 500, 0.5
 MV64_SAMPLES, MV64_PROJ = 8192, 4
 
@@ -410,6 +415,30 @@ def main_dx():
     print("wrote", OUT_DX, len(fx), "arrays")
 
 
+def main_limits():
+    lib = ref_lib("fft3d")
+    fx = {}
+    prob, b, adia, aoff, x0 = EC.limits_problem()
+    k = prob.incid[0].k.astype(np.float32)
+    rc = lib.ddscat_cuda_prepare_green_f32(prob.nx, prob.ny, prob.nz, 0, prob.nat, prob.nat0, 0, 0.0, 0.0, 0.0,
+                                           *map(float, k), 1.0, 1.0, 1.0, _p(prob.iocc))
+    assert rc == 0, lib.ddscat_cuda_last_error()
+    zero = np.zeros_like(b)
+    for s in D.SOLVERS:
+        for tag, bb, xx, maxit, tol in (("maxit", b, zero, 3, 1e-12), ("zero", zero, zero, 10, 1e-5),
+                                        ("x0", b, x0, 300, 1e-5)):
+            xs = xx.copy()
+            it, tole, nc = ct.c_int(), ct.c_float(), ct.c_int()
+            rc = getattr(lib, f"ddscat_cuda_solve_{s}_f32")(_p(bb), _p(xs), _p(adia), _p(aoff), bb.size, maxit, tol,
+                                                            ct.byref(it), ct.byref(tole), ct.byref(nc))
+            fx[f"L_{s}_{tag}_rc"] = np.array([rc])
+            fx[f"L_{s}_{tag}_x"] = xs
+            fx[f"L_{s}_{tag}_meta"] = np.array([it.value, tole.value, nc.value], dtype=np.float64)
+    lib.ddscat_cuda_release()
+    np.savez_compressed(OUT_LIM, **fx)
+    print("wrote", OUT_LIM, len(fx), "arrays")
+
+
 if __name__ == "__main__":
     which = sys.argv[1] if len(sys.argv) > 1 else "all"
     if which in ("base", "all"):
@@ -422,3 +451,5 @@ if __name__ == "__main__":
         main_pbc()
     if which in ("dx", "all"):
         main_dx()
+    if which in ("limits", "all"):
+        main_limits()

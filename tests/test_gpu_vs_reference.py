@@ -273,3 +273,41 @@ def test_rectangular_lattice_solve_evalq_scat_vs_reference(fdx):
     assert np.abs(sc["f1"] - fdx["Q_f1"]).max() <= 2e-5 * fmax
     assert np.abs(sc["f2"] - fdx["Q_f2"]).max() <= 2e-5 * fmax
     dda.release()
+
+
+# ---- limit cases of all eight solvers against tests/golden/reference_fixtures_limits.npz
+FIX_LIM = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_fixtures_limits.npz")
+
+
+@pytest.fixture(scope="module")
+def flim():
+    return dict(np.load(FIX_LIM))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", D.SOLVERS)
+def test_solver_limits_vs_reference(flim, name):
+    """MAXIT reached (maxit 3, tol 1e-12), a zero right-hand side and a nonzero
+    initial guess: the same return code, ITNO and NCOMPTE as the reference, TOLE
+    within 2 % + 1e-7 (FP32 stagnation near 1e-6 after three BiCGStab(4) steps
+    varies by a few per cent; both 0 or inf on the early exits), and the same
+    iterate."""
+    prob, b, adia, aoff, x0 = _edge_cases().limits_problem()
+    dda = D.DDA()
+    dda.prepare_green(prob.nx, prob.ny, prob.nz, prob.iocc, prob.incid[0].k.astype(np.float32))
+    for tag, bb, xx, maxit, tol in (("maxit", b, None, 3, 1e-12), ("zero", np.zeros_like(b), None, 10, 1e-5),
+                                    ("x0", b, x0, 300, 1e-5)):
+        out = dda.solve(name, bb, adia, aoff, x0=xx, maxit=maxit, tol=tol, check=False)
+        it_ref, tole_ref, nc_ref = flim[f"L_{name}_{tag}_meta"]
+        assert out.rc == int(flim[f"L_{name}_{tag}_rc"][0]), (tag, out.rc)
+        assert out.itno == int(it_ref) and out.ncompte == int(nc_ref), (tag, out.itno, out.ncompte)
+        if np.isfinite(tole_ref) and tole_ref > 0:
+            assert abs(out.tole - tole_ref) <= 0.02 * tole_ref + 1e-7, (tag, out.tole, tole_ref)
+        else:
+            assert out.tole == tole_ref, (tag, out.tole, tole_ref)
+        xr = flim[f"L_{name}_{tag}_x"]
+        if np.linalg.norm(xr) > 0:
+            assert _rel(out.x, xr) < 2 * TOL, tag
+        else:
+            assert np.all(out.x == 0), tag
+    dda.release()

@@ -340,3 +340,52 @@ def test_oracle_rectangular_lattice_solve_matches_reference(fdx):
     fmax = np.abs(fdx["Q_f1"]).max()
     assert np.abs(sc["f1"] - fdx["Q_f1"]).max() <= 2e-5 * fmax
     assert np.abs(sc["f2"] - fdx["Q_f2"]).max() <= 2e-5 * fmax
+
+
+# ---- limit cases of all eight solvers (reference_fixtures_limits.npz): MAXIT
+# reached, a zero right-hand side, a nonzero initial guess
+FIX_LIM = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_fixtures_limits.npz")
+LIMIT_CASES = (("maxit", 3, 1e-12), ("zero", 10, 1e-5), ("x0", 300, 1e-5))
+
+
+@pytest.fixture(scope="module")
+def flim():
+    return dict(np.load(FIX_LIM))
+
+
+@pytest.fixture(scope="module")
+def lim_operator():
+    prob, b, adia, aoff, x0 = _edge_cases().limits_problem()
+    gp = O.GreenParams(prob.nx, prob.ny, prob.nz, ak=tuple(float(np.float32(a)) for a in prob.incid[0].k))
+    op = O.Operator.from_params(gp, prob.iocc)
+    c = lambda v: O.gather_compact(v, op.occ, prob.nat).astype(np.complex128)  # noqa: E731
+    return op, c(b), c(adia), c(aoff), c(x0), c
+
+
+@pytest.mark.parametrize("name", SOLVER_NAMES)
+def test_oracle_solver_limits_match_reference(flim, lim_operator, name):
+    """Return code and ITNO in every case (the reference's codes for a zero
+    right-hand side: GPBICG 32, QMRCCG 52, PBCGST 78, PETRKP 115, BiCGStab(4)
+    133, GPBiCGStab(2) 153, GPBiCGStab(4) 183, PBCGS2 0 with TOLE = inf; MAXIT
+    reached: PBCGST 87, the others 0); NCOMPTE and the iterate where the solve
+    returns 0."""
+    op, bc, ac, oc, x0c, c = lim_operator
+    mv = lambda v: op.apply_compact(v, ac, oc)  # noqa: E731
+    mvh = lambda v: op.apply_compact(v, ac, oc, "C")  # noqa: E731
+    for tag, maxit, tol in LIMIT_CASES:
+        b = np.zeros_like(bc) if tag == "zero" else bc
+        x0 = x0c.copy() if tag == "x0" else np.zeros_like(bc)
+        if name == "pbcgst":
+            res = O.solve_pbcgst(mv, b, x0, maxit, tol, ac)
+        elif name == "petrkp":
+            res = O.solve_petrkp(mv, mvh, b, x0, maxit, tol)
+        else:
+            res = O.SOLVERS[name](mv, b, x0, maxit, tol)
+        rc = int(flim[f"L_{name}_{tag}_rc"][0])
+        it_ref, tole_ref, nc_ref = flim[f"L_{name}_{tag}_meta"]
+        assert res.status == rc and res.itno == int(it_ref), (tag, res.status, rc, res.itno, it_ref)
+        if rc == 0:
+            assert res.ncompte == int(nc_ref), (tag, res.ncompte, nc_ref)
+            xr = c(flim[f"L_{name}_{tag}_x"])
+            if np.linalg.norm(xr) > 0:
+                assert np.linalg.norm(res.x - xr) / np.linalg.norm(xr) < 2 * TOL, tag
