@@ -667,9 +667,15 @@ template <typename T> int Engine<T>::ensure_workspace(int nrhs) {
   if (e != cudaSuccess) { zcap = 0; set_cuda_error("malloc z-spectrum workspace", e); return 1; }
   bytes_allocated += (size_t)zcap * per_rhs_z * sizeof(C);
   if (slices_layout) {
-    // bounded memory: the middle stage holds max(4, planes/16) planes of one RHS
+    // bounded memory: the middle stage holds max(4, planes/16) planes of one
+    // RHS, and at least 32 MiB of them, so that its launches fill the GPU on
+    // small grids (128^3: 6 batches of 43 planes instead of 16 of 16); the
+    // batches are balanced
     slab_nr = 1;
-    slab_B = std::min(nplanes_all, std::max(4, nplanes_all / 16));
+    const size_t floor_planes = ceil_div((size_t)32 << 20, per_plane * sizeof(C));
+    const int want = (int)std::max<size_t>({(size_t)4, (size_t)nplanes_all / 16, floor_planes});
+    slab_B = std::min(nplanes_all, want);
+    slab_B = (int)ceil_div((size_t)nplanes_all, ceil_div((size_t)nplanes_all, (size_t)slab_B));
   } else {
     const size_t full_rhs = per_plane * nplanes_all;
     if (full_rhs * zcap <= slab_budget_elems) { slab_nr = zcap; slab_B = nplanes_all; }
