@@ -120,6 +120,9 @@ template <typename T> struct Engine {
   // tile moves of the FP32 256-point y passes by the tensor memory accelerator
   // (DDSCAT_B200_NOTMA=1 selects the per-thread copies)
   int use_tma = 1;
+  // smallest RHS chunk per block for which the z pass stages its Green lines
+  // in shared memory (kx_zg3r; DDSCAT_B200_ZG3R_MIN)
+  int zg3r_min = 4;
 
   // pad: the Green tensor will be built here (build_green), so the FFT lengths
   // may be padded beyond 2n onto the register-FFT pipeline

@@ -601,6 +601,7 @@ int Engine<T>::init_geometry(int nx, int ny, int nz, int ipbc, int nat, int nat0
   tune_tile = env_int("DDSCAT_B200_TILE", 0);
   tune_zg = env_flag("DDSCAT_B200_ZG") ? 1 : 0;
   use_tma = env_flag("DDSCAT_B200_NOTMA") ? 0 : 1;
+  zg3r_min = std::max(1, env_int("DDSCAT_B200_ZG3R_MIN", 4));
   if (!d_err) {
     if (cudaMalloc((void**)&d_err, sizeof(int)) != cudaSuccess) { set_error("prepare", "status word"); return 1; }
     cudaMemset(d_err, 0, sizeof(int));

@@ -1393,7 +1393,7 @@ int matvec_xpipe(Engine<T>& E, const MvArgs<T>& a) {
         const size_t nlb = ceil_div((size_t)P.nkx * g.My, RZ3);
         const int nchunk = (int)std::min<size_t>((size_t)nrb, std::max<size_t>(1, ceil_div(4 * 3 * 148, nlb)));
         P.zg_rch = (int)ceil_div((size_t)nrb, (size_t)nchunk);
-        const bool use_r = fzg3r && P.zg_rch >= 4;
+        const bool use_r = fzg3r && P.zg_rch >= E.zg3r_min;
         if (use_r ? xlaunch<T>(fzg3r, dim3((unsigned)nlb, (unsigned)ceil_div((size_t)nrb, (size_t)P.zg_rch)), 128, smzr,
                                E.stream, P)
             : fzg3 ? xlaunch<T>(fzg3, dim3((unsigned)nrb, (unsigned)ceil_div((size_t)P.nkx * g.My, RZ3)), 128, smz,
