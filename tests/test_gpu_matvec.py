@@ -159,3 +159,21 @@ def test_fused_xy_passes_equal_five_pass(dims, monkeypatch):
     for a, b in zip(y_f, y_5):
         assert _err(a, b)[0] <= 1e-6
     dda.release()
+
+
+@pytest.mark.gpu
+def test_slices_uneven_middle_batches_equal_fft3d():
+    """SLICES with middle-stage batches of unequal size: at 128 x 128 x 64 the
+    32 MiB floor gives batches of 86, 86 and 84 kx planes (the last one
+    shorter); the MATVEC equals the FFT3D layout's, whose middle stage holds
+    every plane at once, to FP32 rounding, in both CWHAT."""
+    dims = (128, 128, 64)
+    iocc, ak, x, adia, aoff, gp = _case(dims, 0, seed=21)
+    outs = {}
+    for layout in ("fft3d", "slices"):
+        dda = D.DDA(layout)
+        dda.prepare_green(*dims, iocc, ak)
+        outs[layout] = [dda.apply(x, adia, aoff, cw) for cw in "NC"]
+        dda.release()
+    for a, b in zip(outs["slices"], outs["fft3d"]):
+        assert np.linalg.norm(a - b) / np.linalg.norm(b) <= 1e-6
